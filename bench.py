@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Throughput of the lattice time-evolution hot path on B200.
+
+Workload (one "step" = one VV2 time step of the whole lattice): lphi4 with one real scalar,
+V = phi^4/4 in program variables, N = 512 periodic, kIR = 1, dt = 0.01, VV2, self-consistent
+expansion, phi0 = 1 (f* = 5.6964e18 GeV, MPl = 2.435e18 GeV), Gaussian vacuum-like fluctuations
+of relative amplitude 1e-3 cut at |k| <= N kIR / 4 (synthetic, seeded).
+
+Reported:
+  value            site-updates/s of the FP64 fused path (inputs resident in HBM), CUDA events
+                   on the library's stream, max over ranks
+  mixed            the FP32/FP64-split form on the same workload, with its Friedmann-constraint
+                   and energy differences against FP64
+  roofline         achieved HBM GB/s of the dominant kernel (the fused sweep) from its own
+                   per-launch CUDA events, against MEASURED_PEAKS.json
+  e2e              the same metric through the C ABI with host buffers: state upload from pinned
+                   host memory, evolve, per-step history read back, final state download
+  cpu_baseline     the FP64 CPU oracle (OpenMP, reference operation order) on a bounded sample
+
+--impl reference times the reference's CPU implementation of this path on the host cores.  The
+reference cannot be built here (its TempLat runtime is not vendored), so that arm runs the CPU
+restatement of the reference's algorithm (oracle/), with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_SITE = {"fp64": 32, "fp32": 16}  # state read once + written once per VV2 stage
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=512)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def workload_params(N, steps):
+    return {
+        "N": N, "kIR": 1.0, "dt": 0.01, "evolver": "VV2", "expansion": "true",
+        "lambda": 1.0, "initial_amplitudes": "5.6964e18", "initial_momenta": "0",
+        "fluct_amplitude": 1e-3, "kCutOff": N / 4.0, "baseSeed": "bench-512",
+        "tMax": steps * 0.01,
+    }
+
+
+def make_workload(N, steps):
+    from cosmolattice_b200 import ParameterParser, RunParameters, lphi4_1f
+
+    par = ParameterParser(params=workload_params(N, steps))
+    rp = RunParameters(par)
+    return rp, lphi4_1f(par, rp)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_tag, N, precision):
+    """dram bytes per launch of the fused sweep from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel_tag}.md")
+    if not os.path.exists(path):
+        return None
+    pat = re.compile(rf"^dram_bytes_per_launch\[{precision},N={N}\]\s*[:=]\s*([0-9.eE+]+)", re.M)
+    m = pat.search(open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"clb_clocks_{os.getpid()}_{device}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_form(rp, model, fields, momenta, sf, precision, warmup, steps, device, world, sample_clocks=True):
+    """Warm up, then time `steps` fused VV2 steps with the state resident in HBM."""
+    import torch
+
+    from cosmolattice_b200 import Lattice
+
+    lat = Lattice(model, rp, precision=precision, path="fused", device=device)
+    lat.set_state(fields, momenta, sf)
+    lat.initialize()
+    lat.sync()
+    m0 = lat.measure(1.0)
+    if warmup > 0:
+        lat.evolve(warmup)
+    lat.reset_stats()
+    lat.set_profiling(True)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    with ClockSampler(device) as clk:
+        lat.evolve(steps)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    ms = lat.last_evolve_ms()
+    stats = lat.kernel_stats()
+    lat.set_profiling(False)
+    lat.sync()
+    m1 = lat.measure(m0["energies"][-1])
+    hist = lat.history()
+    lat.close()
+    return {"ms": ms, "stats": stats, "clocks": clk.summary(), "m0": m0, "m1": m1, "hist_rows": len(hist)}
+
+
+def run_e2e(rp, model, fields, momenta, sf, steps, device):
+    """Through the C ABI with host buffers: upload from pinned memory, evolve, read back every
+    step's (a, aDot, averages) row and the final state."""
+    import numpy as np
+    import torch
+
+    from cosmolattice_b200 import Lattice
+
+    n = fields.size
+    hf = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hp = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hf[:] = fields.ravel()
+    hp[:] = momenta.ravel()
+    out_f = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    out_p = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    lat = Lattice(model, rp, precision="fp64", path="fused", device=device)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    lat.set_state(hf, hp, sf)
+    lat.initialize()
+    lat.evolve(steps)
+    hist = lat.history()
+    import ctypes as C
+
+    from cosmolattice_b200 import _capi
+
+    sfo = _capi.ScaleFactor()
+    lat._check(lat.lib.clb_get_state(lat.h, out_f.ctypes.data_as(C.POINTER(C.c_double)),
+                                     out_p.ctypes.data_as(C.POINTER(C.c_double)), C.byref(sfo)))
+    torch.cuda.synchronize(device)
+    dt = time.perf_counter() - t0
+    lat.close()
+    assert np.isfinite(hist).all() and len(hist) == steps
+    state_bytes = 2 * n * 8
+    return {
+        "value": rp.N ** 3 * steps / dt,
+        "seconds": dt,
+        "h2d_bytes_per_step": state_bytes / steps,
+        "d2h_bytes_per_step": (state_bytes + hist.nbytes) / steps,
+    }
+
+
+def cpu_baseline(rp, model, fields, momenta, sf, budget_s, max_steps=None):
+    """FP64 CPU oracle (reference operation order) timed on the host cores, bounded sample."""
+    from oracle.oracle import OracleLattice, num_threads
+
+    o = OracleLattice(model, rp)
+    o.set_state(fields, momenta, sf)
+    o.initialize()
+    t0 = time.perf_counter()
+    o.evolve(1)
+    one = time.perf_counter() - t0
+    steps = max(1, int(budget_s / max(one, 1e-9)) - 1)
+    if max_steps is not None:
+        steps = min(steps, max_steps)
+    t0 = time.perf_counter()
+    o.evolve(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {
+        "value": rp.N ** 3 * steps / dt, "unit": "site-updates/s", "cores": num_threads(), "kind": "port",
+        "sample": f"{steps} VV2 steps of the {rp.N}^3 lattice after 1 untimed step ({dt:.1f} s)",
+    }
+
+
+def roofline(stats, N, precision, peak, peak_kind):
+    st = stats["scalar_fused_sweep"]
+    if not st["timed_launches"]:
+        return None
+    per_launch_ms = st["total_ms"] / st["timed_launches"]
+    alg_bytes = BYTES_PER_SITE[precision] * N ** 3
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    return {
+        "bound": "hbm", "kernel": "scalar_fused_sweep", "achieved": round(achieved, 1), "peak": peak,
+        "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+        "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": round(per_launch_ms, 5),
+        "traffic": ncu_traffic("scalar_fused_sweep", N, precision),
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return main_reference(args)
+    world, rank, local = dist_setup(args)
+    import torch
+
+    torch.cuda.set_device(local)
+    from cosmolattice_b200.initializers import scalar_initial_state
+
+    N, K, W = args.N, args.steps, args.warmup
+    rp, model = make_workload(N, K)
+    fields, momenta, aI, aDot = scalar_initial_state(model, rp)
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aDot, "aDotSI": aDot}
+
+    r64 = run_form(rp, model, fields, momenta, sf, "fp64", W, K, local, world)
+    r32 = run_form(rp, model, fields, momenta, sf, "fp32", W, K, local, world)
+    ms64 = max_over_ranks(r64["ms"], world)
+    ms32 = max_over_ranks(r32["ms"], world)
+    sites = N ** 3
+    value64 = world * sites * K / (ms64 * 1e-3)
+    value32 = world * sites * K / (ms32 * 1e-3)
+    e2e = run_e2e(rp, model, fields, momenta, sf, K, local)
+    e2e_val = max_over_ranks(1.0 / e2e["value"], world)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(rp, model, fields, momenta, sf, args.cpu_seconds)
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    f64, f32 = r64["m1"], r32["m1"]
+    launches = sum(v["launches"] for v in r64["stats"].values())
+    line = {
+        "metric": "site-updates/s, mixed vs FP64 GPU at equal constraint error; HBM % of peak",
+        "value": value64,
+        "unit": "site-updates/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms64 / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Gaussian vacuum fluctuations, BASELINE recipe)",
+        "config": {
+            "workload": f"lphi4 1 real scalar {N}^3 VV2, self-consistent expansion, {K} steps, FP64 fused path",
+            "lattice": N, "evolver": "VV2", "dt": 0.01, "kIR": 1.0, "expansion": True,
+            "l2": "inputs larger than L2 (state %.1f GiB)" % (2 * sites * 8 / 2 ** 30),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+        },
+        "roofline": roofline(r64["stats"], N, "fp64", peak, peak_kind),
+        "mixed": {
+            "value": value32, "ms_per_step": ms32 / K, "speedup_vs_fp64": value32 / value64,
+            "roofline": roofline(r32["stats"], N, "fp32", peak, peak_kind),
+            "friedmann_fp32": f32["friedmann"][0], "friedmann_fp64": f64["friedmann"][0],
+            "friedmann_abs_diff": abs(f32["friedmann"][0] - f64["friedmann"][0]),
+            "energy_rel_diff": max(abs(a - b) / abs(b) for a, b in zip(f32["energies"], f64["energies"]) if b != 0),
+            "a_rel_diff": abs(f32["aI"] - f64["aI"]) / f64["aI"],
+        },
+        "e2e": {"value": 1.0 / e2e_val if world > 1 else e2e["value"], "unit": "site-updates/s",
+                "h2d_bytes_per_step": e2e["h2d_bytes_per_step"], "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
+                "seconds": e2e["seconds"], "timer": "host wall clock around the C-ABI calls"},
+        "gpu_launches": launches,
+        "kernel_launches": {k: v["launches"] for k, v in r64["stats"].items() if v["launches"]},
+        "clocks": r64["clocks"],
+        "clocks_mixed": r32["clocks"],
+        "cpu_baseline": cpu,
+        "history_rows": r64["hist_rows"],
+    }
+    print(json.dumps(line))
+
+
+def main_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cosmolattice_b200.initializers import scalar_initial_state
+
+    N, K, W = args.N, args.steps, args.warmup
+    rp, model = make_workload(N, K)
+    fields, momenta, aI, aDot = scalar_initial_state(model, rp)
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aDot, "aDotSI": aDot}
+    # the reference's CPU path on all host threads, bounded to a few minutes for K steps
+    budget = min(120.0, max(10.0, 2.0 * args.cpu_seconds))
+    cpu = cpu_baseline(rp, model, fields, momenta, sf, budget, max_steps=K)
+    line = {
+        "metric": "site-updates/s, mixed vs FP64 GPU at equal constraint error; HBM % of peak",
+        "value": cpu["value"], "unit": "site-updates/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": N ** 3 / cpu["value"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian vacuum fluctuations, BASELINE recipe)",
+        "config": {"workload": f"lphi4 1 real scalar {N}^3 VV2, self-consistent expansion, {K} steps, FP64",
+                   "lattice": N, "evolver": "VV2"},
+        "impl": "reference",
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference needs its un-vendored TempLat runtime (CMake FetchContent), so its CPU "
+                "algorithm runs as the FP64 restatement in oracle/ (reference operation order, OpenMP)",
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

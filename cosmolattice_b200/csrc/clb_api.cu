@@ -1,0 +1,839 @@
+// clb_api.cu - C ABI of libclb200: handle lifecycle, state transfer and the evolver schedules.
+//
+// The schedules restate the reference's composition loops:
+//   VelocityVerlet::evolve   evolvers/velocityverlet.h:51-114
+//   LeapFrog::evolve / sync  evolvers/leapfrog.h:42-116
+// Everything between host calls runs on one CUDA stream with the scale factor kept on the
+// device (DevState), so an evolve() of many steps issues kernels back to back with no host
+// synchronisation until its end.
+
+#include "../../include/clb200.h"
+#include "clb_internal.cuh"
+#include "clb_scalar.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace clb;
+
+namespace {
+
+thread_local std::string g_err;
+
+std::vector<double> vv_coeffs(int ev)
+{
+  // VelocityVerletParameters::getCoeffs (velocityverletparameters.h:23-46)
+  switch (ev) {
+  case CLB_VV2: return {1.0};
+  case CLB_VV4: return {1.351207191959657771818, -1.702414403875838200264};
+  case CLB_VV6: return {0.78451361047755726382, 0.23557321335935813368, -1.1776799841788710069, 1.3151863206839112189};
+  case CLB_VV6_2:
+    return {0.39216144400731413928, 0.33259913678935943860, -0.70624617255763935981, 0.082213596293550800230,
+            0.79854399093482996340};
+  case CLB_VV8:
+    return {0.74167036435061295345, -0.40910082580003159400, 0.19075471029623837995, -0.57386247111608226666,
+            0.29906418130365592384, 0.33462491824529818378,  0.31529309239676659663, -0.79688793935291635402};
+  case CLB_VV10:
+    return {-0.48159895600253002870, 0.0036303931544595926879, 0.50180317558723140279,  0.28298402624506254868,
+            0.80702967895372223806,  -0.026090580538592205447, -0.87286590146318071547, -0.52373568062510581643,
+            0.44521844299952789252,  0.18612289547097907887,   0.23137327866438360633,  -0.52191036590418628905,
+            0.74866113714499296793,  0.066736511890604057532,  -0.80360324375670830316, 0.91249037635867994571};
+  default: return {};
+  }
+}
+
+constexpr int kBZ = 32, kBY = 8;
+constexpr int kElemBlocks = 148 * 8; // elementwise grid: 8 resident 256-thread blocks per SM
+
+} // namespace
+
+struct clb_handle {
+  clb_config cfg;
+  clb_model_desc md;
+  int N = 0;
+  size_t n3 = 0;
+  int NS = 0;
+  bool fp32 = false;
+  size_t esz = 8;
+  void *fld[2] = {nullptr, nullptr};
+  void *pi[2] = {nullptr, nullptr};
+  int cf = 0, cp = 0; // current field / momentum buffer
+  DevState *d_st = nullptr;
+  double *d_part = nullptr;
+  double *d_sums = nullptr;
+  size_t part_rows = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<double> ws;
+  bool has_state = false, initialized = false, synced = true;
+  ScalarArgs sa{};
+  SFParams sp{};
+  dim3 sweep_grid;
+  int sweep_blocks = 0;
+  std::string err;
+
+  // instrumentation: launch counts always; per-launch CUDA events on the stream when prof
+  bool prof = false;
+  struct Pend {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<Pend> pend;
+  int64_t launches[16] = {};
+  int64_t timed[16] = {};
+  double kernel_ms[16] = {};
+  cudaEvent_t ev_call[2] = {nullptr, nullptr};
+  double last_evolve_ms = 0;
+  // per-step history rows of the last evolve call
+  double *d_hist = nullptr;
+  int64_t hist_cap = 0, hist_rows = 0;
+  // staging buffer for FP32 <-> FP64 host transfers
+  double *d_stage = nullptr;
+  size_t stage_n = 0;
+
+  int fail(int code, const std::string &m)
+  {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char *where)
+  {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    return CLB_ECUDA;
+  }
+};
+
+namespace {
+
+#define CLB_CHECK_LAUNCH(h, where)                                                                                     \
+  do {                                                                                                                 \
+    cudaError_t e_ = cudaGetLastError();                                                                               \
+    if (e_ != cudaSuccess) return (h)->cuda_fail(e_, where);                                                           \
+  } while (0)
+
+// z-marching geometry: BZ x BY columns per block, x split so the grid covers >= ~2 waves.
+void setup_geometry(clb_handle *h)
+{
+  const int N = h->N;
+  const int gx = (N + kBZ - 1) / kBZ, gy = (N + kBY - 1) / kBY;
+  const int target = 148 * 8 * 2;
+  int xs = (target + gx * gy - 1) / (gx * gy);
+  xs = std::max(1, std::min(xs, std::max(1, N / 4)));
+  int LX = (N + xs - 1) / xs;
+  xs = (N + LX - 1) / LX;
+  h->sa.LX = LX;
+  h->sweep_grid = dim3(gx, gy, xs);
+  h->sweep_blocks = gx * gy * xs;
+}
+
+template <class R> R *F(clb_handle *h, int b) { return static_cast<R *>(h->fld[b]); }
+template <class R> R *P(clb_handle *h, int b) { return static_cast<R *>(h->pi[b]); }
+
+enum KKind { K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_NKINDS };
+const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
+                                          "scalar_drift",       "reduce_pi2",        "reduce_fields",
+                                          "tail",               "measure",           "convert"};
+
+cudaEvent_t take_event(clb_handle *h)
+{
+  if (!h->ev_pool.empty()) {
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Counts a launch and, when profiling, brackets it with events on the handle's stream.
+struct ProfScope {
+  clb_handle *h;
+  int kind;
+  cudaEvent_t a = nullptr;
+  ProfScope(clb_handle *hh, int k) : h(hh), kind(k)
+  {
+    ++h->launches[kind];
+    if (h->prof) {
+      a = take_event(h);
+      cudaEventRecord(a, h->stream);
+    }
+  }
+  ~ProfScope()
+  {
+    if (h->prof) {
+      cudaEvent_t b = take_event(h);
+      cudaEventRecord(b, h->stream);
+      h->pend.push_back({kind, a, b});
+    }
+  }
+};
+#define CLB_LAUNCH(h, kind, ...)                                                                                       \
+  do {                                                                                                                 \
+    ProfScope ps_((h), (kind));                                                                                        \
+    __VA_ARGS__;                                                                                                       \
+  } while (0)
+
+void collect_profile(clb_handle *h)
+{
+  for (auto &p : h->pend) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      h->kernel_ms[p.kind] += ms;
+      ++h->timed[p.kind];
+    }
+    h->ev_pool.push_back(p.a);
+    h->ev_pool.push_back(p.b);
+  }
+  h->pend.clear();
+}
+
+// ---- kernel launchers (templated on storage type and field count) ----------------------------
+template <class R, int NS> struct Launch {
+  // kick in place: pi += h K(phi)
+  static void kick(clb_handle *h, double hk)
+  {
+    ScalarArgs a = h->sa;
+    a.h1 = hk;
+    a.h2 = 0.0;
+    CLB_LAUNCH(h, K_KICK,
+               k_scalar_sweep<R, NS, kBZ, kBY, false, true, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                   F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+  }
+  // fused: drift (dtw) + kick (h1, h2) + averages, ping-pong buffers
+  static void fused(clb_handle *h, double dtw, double h1, double h2, bool red)
+  {
+    ScalarArgs a = h->sa;
+    a.dtw = dtw;
+    a.h1 = h1;
+    a.h2 = h2;
+    const int nf = h->cf ^ 1, np = h->cp ^ 1;
+    if (red)
+      CLB_LAUNCH(h, K_FUSED,
+                 k_scalar_sweep<R, NS, kBZ, kBY, true, true, 3><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, np), a, h->d_st, h->d_part));
+    else
+      CLB_LAUNCH(h, K_FUSED,
+                 k_scalar_sweep<R, NS, kBZ, kBY, true, true, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, np), a, h->d_st, h->d_part));
+    h->cf = nf;
+    h->cp = np;
+  }
+  // drift (dtw) with optional field averages, writes the other field buffer
+  static void drift_fields(clb_handle *h, double dtw, bool red)
+  {
+    ScalarArgs a = h->sa;
+    a.dtw = dtw;
+    const int nf = h->cf ^ 1;
+    if (red)
+      CLB_LAUNCH(h, K_DRIFT_SWEEP,
+                 k_scalar_sweep<R, NS, kBZ, kBY, true, false, 2><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+    else
+      CLB_LAUNCH(h, K_DRIFT_SWEEP,
+                 k_scalar_sweep<R, NS, kBZ, kBY, true, false, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+    h->cf = nf;
+  }
+  // elementwise in-place drift (reference order)
+  static void drift(clb_handle *h, double dtw)
+  {
+    CLB_LAUNCH(h, K_DRIFT,
+               k_drift<R><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), (size_t)NS * h->n3,
+                                                               dtw, h->d_st));
+  }
+  // <pi^2> partials (elementwise grid)
+  static int reduce_pi2(clb_handle *h)
+  {
+    CLB_LAUNCH(h, K_RED_PI2, k_reduce_pi2<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(P<R>(h, h->cp), h->n3, h->d_part));
+    return kElemBlocks;
+  }
+  // <grad^2>, <V> (and <pi^2> with all=true) partials (sweep grid)
+  static int reduce_fields(clb_handle *h, bool all)
+  {
+    ScalarArgs a = h->sa;
+    if (all)
+      CLB_LAUNCH(h, K_RED_FIELDS,
+                 k_scalar_sweep<R, NS, kBZ, kBY, false, false, 3><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+    else
+      CLB_LAUNCH(h, K_RED_FIELDS,
+                 k_scalar_sweep<R, NS, kBZ, kBY, false, false, 2><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
+                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+    return h->sweep_blocks;
+  }
+  static void measure(clb_handle *h, double am)
+  {
+    CLB_LAUNCH(h, K_MEASURE,
+               k_measure<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->sa, am,
+                                                                    h->d_part));
+    CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeasSlots><<<1, 256, 0, h->stream>>>(h->d_part, kElemBlocks, h->d_sums));
+  }
+};
+
+void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1)
+{
+  TailOp op{flags, nblocks, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
+  CLB_LAUNCH(h, K_TAIL, k_tail<<<1, 256, 0, h->stream>>>(h->d_part, op, h->d_st, h->sp));
+}
+
+// Dispatch on (storage, field count).
+template <template <class, int> class Fn, class... Args> void dispatch(clb_handle *h, Args... args)
+{
+  if (h->fp32) {
+    if (h->NS == 1) Fn<float, 1>::run(h, args...);
+    else Fn<float, 2>::run(h, args...);
+  } else {
+    if (h->NS == 1) Fn<double, 1>::run(h, args...);
+    else Fn<double, 2>::run(h, args...);
+  }
+}
+
+// ---- schedules --------------------------------------------------------------------------------
+// VelocityVerlet::evolve, n steps (velocityverlet.h:51-114).
+template <class R, int NS> struct EvolveVV {
+  static void run(clb_handle *h, int64_t nsteps)
+  {
+    using L = Launch<R, NS>;
+    const double dt = h->cfg.dt;
+    const bool ex = h->cfg.expansion != 0;
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    if (h->cfg.path == CLB_PATH_REFERENCE) {
+      for (int64_t s = 0; s < nsteps; ++s)
+        for (size_t i = 0; i < S; ++i) {
+          const double w = wof(i);
+          if (ex) tail(h, T_VV_KICK_HALF, 0, 0, w);            // kickScaleFactorHalf
+          L::kick(h, w * dt / 2);                              // kickScalar
+          if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, L::reduce_pi2(h), 0, w); // <pi^2>, driftScaleFactor
+          L::drift(h, dt * w);                                 // driftScalar
+          if (ex) tail(h, T_STORE_FIELDS, L::reduce_fields(h, false));         // storeFieldsAverages
+          L::kick(h, w * dt / 2);                              // kickScalar
+          if (ex) // <pi^2>, kickScaleFactorOne; the last stage closes step s
+            tail(h, T_STORE_PI2_I | T_VV_KICK_ONE, L::reduce_pi2(h), w, 0, i + 1 == S ? s : -1);
+        }
+      return;
+    }
+    // Fused: the second kick of a stage and the first kick of the next one act with the same
+    // kernel K(phi', a) (no field or a update in between), so one sweep drifts phi, forms
+    // pi_mid = pi + h1 K and pi_next = pi_mid + h2 K, and reduces <pi_mid^2>, <grad^2>, <V>.
+    const int64_t total = nsteps * (int64_t)S;
+    const double w0 = wof(0);
+    if (ex) tail(h, T_VV_KICK_HALF, 0, 0, w0); // kickScaleFactorHalf
+    L::kick(h, w0 * dt / 2);                  // kickScalar with a(t) before the drift
+    if (ex) tail(h, T_VV_DRIFT, 0, 0, w0);     // driftScaleFactor
+    for (int64_t k = 0; k < total; ++k) {
+      const size_t i = (size_t)(k % (int64_t)S);
+      const double w = wof(i);
+      const bool more = k + 1 < total;
+      const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+      L::fused(h, dt * w, w * dt / 2, more ? wn * dt / 2 : 0.0, ex);
+      if (ex) {
+        uint32_t fl = T_STORE_PI2_I | T_STORE_FIELDS | T_VV_KICK_ONE;
+        if (more) fl |= T_VV_KICK_HALF | T_VV_DRIFT;
+        tail(h, fl, h->sweep_blocks, w, wn, i + 1 == S ? k / (int64_t)S : -1);
+      }
+    }
+  }
+};
+
+// LeapFrog::evolve, n steps (leapfrog.h:42-89).
+template <class R, int NS> struct EvolveLF {
+  static void run(clb_handle *h, int64_t nsteps)
+  {
+    using L = Launch<R, NS>;
+    const double dt = h->cfg.dt;
+    const bool ex = h->cfg.expansion != 0;
+    if (nsteps <= 0) return;
+    if (h->cfg.path == CLB_PATH_REFERENCE) {
+      for (int64_t s = 0; s < nsteps; ++s) {
+        const double weight = h->synced ? 0.5 : 1.0;
+        L::kick(h, weight * dt);
+        if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, L::reduce_pi2(h));
+        L::drift(h, dt);
+        if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY, L::reduce_fields(h, false), 0, 0, s);
+        h->synced = false;
+      }
+      return;
+    }
+    // Fused: drift of step n and kick of step n+1 in one sweep; the sweep's reductions are the
+    // field averages of phi_{n+1} and <pi_{n+3/2}^2>, which the tail books in LeapFrog order.
+    const double weight = h->synced ? 0.5 : 1.0;
+    L::kick(h, weight * dt);
+    if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, L::reduce_pi2(h));
+    for (int64_t s = 1; s < nsteps; ++s) {
+      L::fused(h, dt, dt, 0.0, ex);
+      if (ex)
+        tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, h->sweep_blocks, 0, 0, s - 1);
+    }
+    L::drift_fields(h, dt, ex);
+    if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY, h->sweep_blocks, 0, 0, nsteps - 1);
+    h->synced = false;
+  }
+};
+
+template <class R, int NS> struct SyncLF {
+  static void run(clb_handle *h)
+  {
+    using L = Launch<R, NS>;
+    if (!h->synced) {
+      L::kick(h, 0.5 * h->cfg.dt);
+      if (h->cfg.expansion) tail(h, T_STORE_PI2_I | T_LF_SYNC, L::reduce_pi2(h));
+    }
+    h->synced = true;
+  }
+};
+
+template <class R, int NS> struct Init {
+  static void run(clb_handle *h, int correct)
+  {
+    using L = Launch<R, NS>;
+    uint32_t fl = T_STORE_ALL;
+    if (h->cfg.expansion && correct) fl |= T_CORRECT_ADOT;
+    if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
+    tail(h, fl, L::reduce_fields(h, true));
+  }
+};
+
+template <class R, int NS> struct Measure {
+  static void run(clb_handle *h, double am) { Launch<R, NS>::measure(h, am); }
+};
+
+int sync_and_check(clb_handle *h, const char *where)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  collect_profile(h);
+  DevState s;
+  e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  if (s.status != 0) return h->fail(CLB_ENONFINITE, std::string(where) + ": a volume average or a(t) is not finite");
+  return CLB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *clb_version(void) { return "clb200 0.1 (sm_100a)"; }
+
+const char *clb_last_error(const clb_handle *h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out)
+{
+  if (!cfg || !md || !out) {
+    g_err = "clb_create: null argument";
+    return CLB_EINVAL;
+  }
+  *out = nullptr;
+  if (md->kind != CLB_MODEL_LPHI4) {
+    g_err = "clb_create: unknown model kind";
+    return CLB_EUNSUPPORTED;
+  }
+  if (md->n_scalars < 1 || md->n_scalars > 2) {
+    g_err = "clb_create: lphi4 supports 1 or 2 scalar singlets";
+    return CLB_EUNSUPPORTED;
+  }
+  if (cfg->N < 2 || cfg->N > 4096) {
+    g_err = "clb_create: N must be in [2, 4096]";
+    return CLB_EINVAL;
+  }
+  if (!(cfg->dx > 0) || !std::isfinite(cfg->dx)) {
+    g_err = "clb_create: dx must be positive";
+    return CLB_EINVAL;
+  }
+  if (cfg->dt == 0 || !std::isfinite(cfg->dt)) {
+    g_err = "clb_create: dt cannot be zero, abort.";  // runparameters.h:191
+    return CLB_EINVAL;
+  }
+  if (cfg->precision != CLB_PREC_FP64 && cfg->precision != CLB_PREC_FP32_SPLIT) {
+    g_err = "clb_create: unknown precision";
+    return CLB_EINVAL;
+  }
+  if (cfg->path != CLB_PATH_FUSED && cfg->path != CLB_PATH_REFERENCE) {
+    g_err = "clb_create: unknown path";
+    return CLB_EINVAL;
+  }
+  if (!(md->fStar > 0) || !(md->MPl > 0) || !(md->omegaStar > 0)) {
+    g_err = "clb_create: fStar, omegaStar and MPl must be positive";
+    return CLB_EINVAL;
+  }
+  std::vector<double> ws;
+  if (cfg->evolver != CLB_LF) {
+    ws = vv_coeffs(cfg->evolver);
+    if (ws.empty()) {
+      g_err = "clb_create: The evolver type you specified was not implemented in the Evolver class";  // evolver.h:366-368
+      return CLB_EUNSUPPORTED;
+    }
+  }
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) {
+    g_err = std::string("clb_create: cudaSetDevice: ") + cudaGetErrorString(e);
+    return CLB_ECUDA;
+  }
+  clb_handle *h = new clb_handle();
+  h->cfg = *cfg;
+  h->md = *md;
+  h->N = cfg->N;
+  h->n3 = (size_t)cfg->N * cfg->N * cfg->N;
+  h->NS = md->n_scalars;
+  h->fp32 = cfg->precision == CLB_PREC_FP32_SPLIT;
+  h->esz = h->fp32 ? sizeof(float) : sizeof(double);
+  h->ws = ws;
+  setup_geometry(h);
+  ScalarArgs &a = h->sa;
+  a.N = h->N;
+  a.inv_dx2 = 1.0 / (cfg->dx * cfg->dx);
+  a.c0 = md->couplings[0];
+  a.q = md->couplings[1];
+  a.c0_quarter = 0.25 * md->couplings[0];
+  a.q_half = 0.5 * md->couplings[1];
+  const double fm = md->fStar / md->MPl;
+  h->sp = SFParams{md->alpha, fm * fm, cfg->dt, 1.0 / (double)h->n3};
+  h->part_rows = (size_t)std::max(h->sweep_blocks, kElemBlocks);
+  const size_t bytes = (size_t)h->NS * h->n3 * h->esz;
+  const size_t nbuf = cfg->path == CLB_PATH_FUSED ? 2 : 1;
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (size_t b = 0; ok && b < nbuf; ++b) {
+    ok = cudaMalloc(&h->fld[b], bytes) == cudaSuccess && cudaMalloc(&h->pi[b], bytes) == cudaSuccess;
+    if (ok) ok = cudaMemset(h->fld[b], 0, bytes) == cudaSuccess && cudaMemset(h->pi[b], 0, bytes) == cudaSuccess;
+  }
+  ok = ok && cudaMalloc(&h->d_st, sizeof(DevState)) == cudaSuccess;
+  ok = ok && cudaMalloc(&h->d_part, h->part_rows * kMeasSlots * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&h->d_sums, kMeasSlots * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaEventCreate(&h->ev_call[0]) == cudaSuccess && cudaEventCreate(&h->ev_call[1]) == cudaSuccess;
+  if (ok && h->fp32) {
+    h->stage_n = std::min<size_t>((size_t)h->NS * h->n3, (size_t)1 << 23); // <= 64 MiB of doubles
+    ok = cudaMalloc(&h->d_stage, h->stage_n * sizeof(double)) == cudaSuccess;
+  }
+  if (!ok) {
+    g_err = std::string("clb_create: device allocation failed: ") + cudaGetErrorString(cudaGetLastError());
+    clb_destroy(h);
+    return CLB_ENOMEM;
+  }
+  DevState s{};
+  s.aI = s.aSI = s.aIM = 1.0;
+  s.drift_p = s.kick_A = s.kick_B = 1.0;
+  cudaMemcpy(h->d_st, &s, sizeof(s), cudaMemcpyHostToDevice);
+  *out = h;
+  return CLB_OK;
+}
+
+void clb_destroy(clb_handle *h)
+{
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int b = 0; b < 2; ++b) {
+    if (h->fld[b]) cudaFree(h->fld[b]);
+    if (h->pi[b]) cudaFree(h->pi[b]);
+  }
+  if (h->d_st) cudaFree(h->d_st);
+  if (h->d_part) cudaFree(h->d_part);
+  if (h->d_sums) cudaFree(h->d_sums);
+  if (h->d_hist) cudaFree(h->d_hist);
+  if (h->d_stage) cudaFree(h->d_stage);
+  for (auto &p : h->pend) {
+    h->ev_pool.push_back(p.a);
+    h->ev_pool.push_back(p.b);
+  }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  for (auto e : h->ev_call)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int clb_num_components(const clb_handle *h, int32_t *nf, int32_t *np)
+{
+  if (!h) return CLB_EINVAL;
+  if (nf) *nf = h->NS;
+  if (np) *np = h->NS;
+  return CLB_OK;
+}
+
+int clb_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
+{
+  if (!h || !fields || !momenta) return h ? h->fail(CLB_EINVAL, "clb_set_state: null argument") : CLB_EINVAL;
+  const size_t n = (size_t)h->NS * h->n3;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  h->cf = h->cp = 0;
+  if (h->fp32) {
+    // FP64 host arrays through a device staging buffer, converted on the GPU
+    auto up = [&](const double *src, float *dst) -> cudaError_t {
+      for (size_t off = 0; off < n; off += h->stage_n) {
+        const size_t c = std::min(h->stage_n, n - off);
+        cudaError_t r = cudaMemcpyAsync(h->d_stage, src + off, c * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        if (r != cudaSuccess) return r;
+        CLB_LAUNCH(h, K_CONVERT, k_convert<double, float><<<kElemBlocks, 256, 0, h->stream>>>(h->d_stage, dst + off, c));
+      }
+      return cudaGetLastError();
+    };
+    e = up(fields, static_cast<float *>(h->fld[0]));
+    if (e == cudaSuccess) e = up(momenta, static_cast<float *>(h->pi[0]));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  } else {
+    e = cudaMemcpyAsync(h->fld[0], fields, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->pi[0], momenta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  }
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  DevState s{};
+  s.aI = s.aSI = s.aIM = 1.0;
+  if (sf) {
+    s.aI = sf->aI;
+    s.aSI = sf->aSI;
+    s.aIM = sf->aIM;
+    s.aDotI = sf->aDotI;
+    s.aDotSI = sf->aDotSI;
+    s.aDotSIM = sf->aDotSIM;
+  }
+  const double al = h->md.alpha;
+  s.drift_p = std::pow(s.aSI, al - 3);
+  s.kick_A = std::pow(s.aI, 1 + al);
+  s.kick_B = std::pow(s.aI, 3 + al);
+  e = cudaMemcpy(h->d_st, &s, sizeof(s), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  h->has_state = true;
+  h->initialized = false;
+  h->synced = true;
+  return CLB_OK;
+}
+
+int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
+{
+  if (!h) return CLB_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
+  const size_t n = (size_t)h->NS * h->n3;
+  auto fetch = [&](void *src, double *dst) -> cudaError_t {
+    if (!dst) return cudaSuccess;
+    if (h->fp32) {
+      const float *fs = static_cast<const float *>(src);
+      for (size_t off = 0; off < n; off += h->stage_n) {
+        const size_t c = std::min(h->stage_n, n - off);
+        CLB_LAUNCH(h, K_CONVERT, k_convert<float, double><<<kElemBlocks, 256, 0, h->stream>>>(fs + off, h->d_stage, c));
+        cudaError_t r = cudaMemcpyAsync(dst + off, h->d_stage, c * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (r != cudaSuccess) return r;
+      }
+      return cudaStreamSynchronize(h->stream);
+    }
+    cudaError_t r = cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    return r == cudaSuccess ? cudaStreamSynchronize(h->stream) : r;
+  };
+  e = fetch(h->fld[h->cf], fields);
+  if (e == cudaSuccess) e = fetch(h->pi[h->cp], momenta);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
+  if (sf) {
+    DevState s;
+    e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
+    sf->aI = s.aI;
+    sf->aSI = s.aSI;
+    sf->aIM = s.aIM;
+    sf->aDotI = s.aDotI;
+    sf->aDotSI = s.aDotSI;
+    sf->aDotSIM = s.aDotSIM;
+  }
+  return CLB_OK;
+}
+
+int clb_initialize(clb_handle *h, int32_t correct_adot)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->has_state) return h->fail(CLB_ESTATE, "clb_initialize: no state uploaded");
+  dispatch<Init>(h, (int)correct_adot);
+  h->synced = true;
+  int r = sync_and_check(h, "clb_initialize");
+  if (r == CLB_OK) h->initialized = true;
+  return r;
+}
+
+int clb_evolve(clb_handle *h, int64_t n)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_evolve: call clb_initialize first");
+  if (n < 0) return h->fail(CLB_EINVAL, "clb_evolve: negative step count");
+  if (n == 0) return CLB_OK;
+  h->hist_rows = 0;
+  if (h->cfg.expansion && n > h->hist_cap) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && h->d_hist) e = cudaFree(h->d_hist);
+    h->d_hist = nullptr;
+    h->hist_cap = 0;
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_hist, (size_t)n * kHistCols * sizeof(double));
+    if (e != cudaSuccess) return h->fail(CLB_ENOMEM, std::string("clb_evolve: history buffer: ") + cudaGetErrorString(e));
+    h->hist_cap = n;
+  }
+  cudaEventRecord(h->ev_call[0], h->stream);
+  if (h->cfg.evolver == CLB_LF)
+    dispatch<EvolveLF>(h, n);
+  else
+    dispatch<EvolveVV>(h, n);
+  cudaEventRecord(h->ev_call[1], h->stream);
+  int r = sync_and_check(h, "clb_evolve");
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, h->ev_call[0], h->ev_call[1]) == cudaSuccess) h->last_evolve_ms = ms;
+  if (r == CLB_OK && h->cfg.expansion) h->hist_rows = n;
+  return r;
+}
+
+int clb_history(clb_handle *h, double *out, int64_t max_rows, int64_t *n_rows)
+{
+  if (!h || !n_rows) return h ? h->fail(CLB_EINVAL, "clb_history: null argument") : CLB_EINVAL;
+  const int64_t n = std::min(max_rows, h->hist_rows);
+  *n_rows = h->hist_rows;
+  if (n > 0 && out) {
+    cudaError_t e = cudaMemcpyAsync(out, h->d_hist, (size_t)n * kHistCols * sizeof(double), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_history");
+  }
+  return CLB_OK;
+}
+
+int clb_set_profiling(clb_handle *h, int32_t on)
+{
+  if (!h) return CLB_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_profiling");
+  collect_profile(h);
+  h->prof = on != 0;
+  return CLB_OK;
+}
+
+int clb_reset_stats(clb_handle *h)
+{
+  if (!h) return CLB_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_reset_stats");
+  collect_profile(h);
+  for (int k = 0; k < 16; ++k) {
+    h->launches[k] = 0;
+    h->timed[k] = 0;
+    h->kernel_ms[k] = 0;
+  }
+  return CLB_OK;
+}
+
+int clb_kernel_stats(clb_handle *h, clb_kernel_stat *out, int32_t max, int32_t *n)
+{
+  if (!h || !n) return h ? h->fail(CLB_EINVAL, "clb_kernel_stats: null argument") : CLB_EINVAL;
+  *n = K_NKINDS;
+  for (int k = 0; k < K_NKINDS && k < max && out; ++k) {
+    std::memset(&out[k], 0, sizeof(out[k]));
+    std::strncpy(out[k].name, kKindNames[k], sizeof(out[k].name) - 1);
+    out[k].launches = h->launches[k];
+    out[k].timed_launches = h->timed[k];
+    out[k].total_ms = h->kernel_ms[k];
+  }
+  return CLB_OK;
+}
+
+int clb_last_evolve_ms(clb_handle *h, double *ms)
+{
+  if (!h || !ms) return CLB_EINVAL;
+  *ms = h->last_evolve_ms;
+  return CLB_OK;
+}
+
+void *clb_cuda_stream(clb_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int clb_sync(clb_handle *h)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_sync: call clb_initialize first");
+  if (h->cfg.evolver == CLB_LF) dispatch<SyncLF>(h);
+  return sync_and_check(h, "clb_sync");
+}
+
+int clb_measure(clb_handle *h, double e0, clb_measurement *m)
+{
+  if (!h || !m) return h ? h->fail(CLB_EINVAL, "clb_measure: null argument") : CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_measure: call clb_initialize first");
+  DevState s;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  const double al = h->md.alpha;
+  const double am = std::pow(s.aI, al - 3);
+  dispatch<Measure>(h, am);
+  double sums[kMeasSlots];
+  e = cudaMemcpyAsync(sums, h->d_sums, sizeof(sums), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  std::memset(m, 0, sizeof(*m));
+  const double inv = 1.0 / (double)h->n3;
+  auto ipow = [](double x, int n) {
+    double r = x;
+    for (int i = 1; i < n; ++i) r = r * x;
+    return r;
+  };
+  const double am6 = 1.0 / ipow(s.aI, 6), am2 = 1.0 / ipow(s.aI, 2);
+  const int NS = h->NS;
+  double Etot = 0, pi2 = 0, g2 = 0, pot = 0;
+  int k = 0;
+  for (int f = 0; f < NS; ++f) {
+    // EnergiesMeasurer::measure (energiesmeasurer.h:56-59)
+    const double Ekin = 0.5 * (sums[6 * f + 0] * inv) * am6;
+    const double Egrad = 0.5 * (sums[6 * f + 1] * inv) * am2;
+    m->energies[k++] = Ekin;
+    m->energies[k++] = Egrad;
+    Etot += Ekin + Egrad;
+    pi2 += sums[6 * f + 0];
+    g2 += sums[6 * f + 1];
+  }
+  for (int t = 0; t < NS; ++t) {
+    const double v = sums[6 * NS + t] * inv;
+    m->energies[k++] = v;
+    Etot += v;
+    pot += sums[6 * NS + t];
+  }
+  m->energies[k++] = Etot;
+  m->n_energies = k;
+  if (h->cfg.expansion) {
+    // HubbleConstraint::get -> Energies::rho -> Averages::setAllAverages (energies.h:219): the
+    // cached averages are refreshed as a side effect, which later LF steps observe.
+    s.potAvI = pot * inv;
+    s.potAvSI = s.potAvI;
+    s.pi2AvI = pi2 * inv;
+    s.pi2AvSI = s.pi2AvI;
+    s.grad2AvI = g2 * inv;
+    const double rho = (0.5 * s.pi2AvI * am6 + 0.5 * s.grad2AvI * am2) + s.potAvI;
+    const double LHS = s.aDotI * s.aDotI;
+    const double RHS = std::pow(s.aI, 2 * al + 2) / 3. * h->sp.fm2 * rho;
+    m->friedmann[0] = (LHS - RHS) / (LHS + RHS);
+    m->friedmann[1] = LHS;
+    m->friedmann[2] = RHS;
+    e = cudaMemcpy(h->d_st, &s, sizeof(s), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  } else {
+    m->friedmann[0] = std::fabs(1.0 - Etot / e0);
+  }
+  for (int f = 0; f < NS; ++f) {
+    // MeansMeasurer::measure (meansmeasurer.h:28-48)
+    const double phi = sums[6 * f + 2] * inv, phi2 = sums[6 * f + 3] * inv;
+    const double mom = sums[6 * f + 4] * inv, mom2 = sums[6 * f + 5] * inv;
+    const double r1 = phi2 - phi * phi, r2 = mom2 - mom * mom;
+    m->means[f][0] = phi;
+    m->means[f][1] = mom;
+    m->means[f][2] = phi2;
+    m->means[f][3] = mom2;
+    m->means[f][4] = r1 > 0 ? std::sqrt(r1) : 0;
+    m->means[f][5] = r2 > 0 ? std::sqrt(r2) : 0;
+  }
+  m->n_means = NS;
+  m->aI = s.aI;
+  m->aDotI = s.aDotI;
+  m->hubble = s.aDotI / s.aI;
+  return CLB_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,131 @@
+// clb_internal.cuh - device-side state and helpers shared by the sm_100a kernels of libclb200.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace clb {
+
+// Number of reduction slots every sweep writes per block: <pi^2>, <grad^2>, <V>.
+constexpr int kRedSlots = 3;
+// Slots of the measurement reduction (per field: pi^2, grad^2, phi, phi^2, mom, mom^2; then V terms).
+constexpr int kMeasSlots = 16;
+
+// Scale-factor state, cached volume averages and the per-sweep coefficients, kept in device
+// memory so a whole evolve() call runs without host round trips.  Field names follow
+// ScaleFactorBase (abstractmodel/scalefactorbase.h:20-21) and ScalarBase (scalarbase.h).
+struct DevState {
+  double aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
+  double pi2AvI, pi2AvSI, pi2AvSIM, grad2AvI, potAvI, potAvSI;
+  // coefficients read by the sweeps
+  double drift_p; // pow(aSI, alpha - 3)              (velocityverlet.h:183)
+  double kick_A;  // pow(aI, 1 + alpha)               (scalarsingletkernels.h:266)
+  double kick_B;  // pow(aI, 3 + alpha)
+  int32_t status; // 0 ok, 1 non-finite average seen
+  int32_t pad;
+};
+
+// Constants of the scale-factor equation (scalefactorkernels.h:73-77) and Friedmann constraint.
+struct SFParams {
+  double alpha;
+  double fm2;     // (fStar / MPl)^2
+  double dt;
+  double inv_n3;  // 1 / N^3
+};
+
+// Operations of the one-thread tail that follows a reducing sweep.  Applied in field order.
+enum TailFlags : uint32_t {
+  T_STORE_PI2_I = 1u << 0,  // pi2AvI = <pi^2>                         (velocityverlet.h:251)
+  T_STORE_PI2_LF = 1u << 1, // pi2AvSIM = pi2AvSI; pi2AvSI = <pi^2>; pi2AvI = mean (leapfrog.h:241-245)
+  T_STORE_FIELDS = 1u << 2, // grad2AvI = <grad^2>; potAvI = <V>       (velocityverlet.h:258-266)
+  T_STORE_ALL = 1u << 3,    // Averages::setAllAverages                (averages.h:349-358)
+  T_VV_KICK_ONE = 1u << 4,  // aDotI = aDotSI + dt/2 F w               (velocityverlet.h:171-174)
+  T_VV_KICK_HALF = 1u << 5, // aDotSI = aDotI + dt/2 F w2              (velocityverlet.h:165-169)
+  T_VV_DRIFT = 1u << 6,     // a drift with weight w2                  (velocityverlet.h:239-242)
+  T_LF_KICK = 1u << 7,      // LeapFrog::kickScaleFactor               (leapfrog.h:124-129)
+  T_LF_DRIFT = 1u << 8,     // LeapFrog::driftScaleFactor              (leapfrog.h:180-183)
+  T_LF_SYNC = 1u << 9,      // aDotI = aDotSI + dt/2 F                 (leapfrog.h:111)
+  T_LF_CTOR = 1u << 10,     // aDotSI = aDotI - dt/2 F                 (leapfrog.h:35)
+  T_CORRECT_ADOT = 1u << 11,// aDotI = sqrt(Friedmann RHS)             (modelinitializer.h:77-78)
+  T_HIST_EARLY = 1u << 12   // history row right after the field averages (LF step end)
+};
+
+struct TailOp {
+  uint32_t flags;
+  int32_t nblocks; // number of partial rows to reduce (0: no reduction)
+  double w;        // weight of T_VV_KICK_ONE
+  double w2;       // weight of T_VV_KICK_HALF / T_VV_DRIFT
+  double *hist;    // per-step history rows (kHistCols doubles), or null
+  int64_t hist_row;// row written after this tail, -1 for none
+};
+
+// Columns of the per-step history: a, aDot, <pi^2>, <grad^2>, <V> at the end of each step.
+constexpr int kHistCols = 5;
+
+// Per-launch geometry of the z-marching stencil sweeps.
+struct SweepGeom {
+  int N;
+  int LX;         // x planes per block
+  dim3 grid;
+};
+
+// Arithmetic with a pinned rounding sequence.  The FP64 form uses the _rn intrinsics so the
+// compiler cannot contract a*b+c into an FMA: the FP64 path then rounds exactly where the
+// reference's expression templates round, which the 1e-12 parity bar relies on.  The FP32 form
+// lets the compiler fuse.
+template <class R> struct Ar;
+template <> struct Ar<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+};
+template <> struct Ar<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+  static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+  static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+};
+
+__device__ __forceinline__ double ipow_d(double x, int n)
+{
+  if (n == 0) return 1.0;
+  if (n < 0) return 1.0 / ipow_d(x, -n);
+  double r = x;
+  for (int i = 1; i < n; ++i) r = __dmul_rn(r, x);
+  return r;
+}
+
+// Deterministic block reduction of NV per-thread values; thread 0 of the block gets the sums.
+template <int NV, int NT>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double *smem /* [NT/32][NV] */)
+{
+  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int warp = tid >> 5;
+  // lanes are numbered along threadIdx.x first; blockDim.x is a multiple of 32 or the whole block
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    v[k] = s;
+  }
+  (void)lane;
+  if ((tid & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) smem[warp * NV + k] = v[k];
+  }
+  __syncthreads();
+  if (tid < 32) {
+    constexpr int NW = NT / 32;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = tid < NW ? smem[tid * NV + k] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      v[k] = s;
+    }
+  }
+}
+
+} // namespace clb

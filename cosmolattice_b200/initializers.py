@@ -1,0 +1,95 @@
+"""Initial conditions for scalar singlets and the scale factor (host, numpy FFT).
+
+Restates the reference recipe:
+* ScaleFactorInitializer::initializeScaleFactor (initializers/scalefactorinitializer.h:30-65):
+  a = a0, aDot = (fStar / MPl) sqrt(rho / 3) with rho from the homogeneous kinetic energy and pot0.
+* FluctuationsGenerator::getFluctuationsNorm / conjugateGaussianFluctuations
+  (initializers/fluctuationsgenerator.h:39-71, 130-150): per mode, left and right movers f_L, f_R
+  with Gaussian real and imaginary parts of rms
+      H(kCut - k) (omega*/f*) (L/dx^2)^(3/2) (2 omega_k)^(-1/2) / sqrt(2),
+  omega_k = sqrt(k^2 + max(m^2, 0)); phi_k = (f_L + f_R)/sqrt(2),
+  pi_k = i omega_k (f_L - f_R)/sqrt(2) - aDot phi_k; zero modes set to 0.
+* ScalarSingletInitializer::initializeScalars (scalarsingletinitializer.h:41-77): homogeneous
+  phi0/f* and pi0/(f* omega*) added afterwards.
+
+The random streams are numpy PCG64 streams seeded from (baseSeed, label, field); the reference's
+TempLat streams are not reproducible outside TempLat.  The configuration-space field is the
+normalised inverse real FFT (scipy.fft.irfftn, 1/N^3), consistent with the norm above giving the
+continuum vacuum variance.  ``fluct_amplitude`` (a model parameter) replaces omega*/f* when set.
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+
+import numpy as np
+import scipy.fft as sfft
+
+from .models import Model
+from .params import RunParameters
+
+
+def _rng(base_seed: str, label: str) -> np.random.Generator:
+    h = hashlib.sha256(f"{base_seed}|{label}".encode()).digest()
+    return np.random.Generator(np.random.PCG64(int.from_bytes(h[:16], "little")))
+
+
+def wave_numbers(N: int):
+    """Integer lattice wave numbers of the rfftn half spectrum, shape (N, N, N//2+1)."""
+    nx = np.fft.fftfreq(N, 1.0 / N)
+    nz = np.fft.rfftfreq(N, 1.0 / N)
+    return nx[:, None, None], nx[None, :, None], nz[None, None, :]
+
+
+def initial_scale_factor(model: Model, rp: RunParameters):
+    """(aI, aDotI) before fluctuations (scalefactorinitializer.h:58-65)."""
+    if not rp.expansion:
+        return 1.0, 0.0
+    kin = 0.0
+    for i in range(model.Ns):
+        # Energies::kineticS with the default a = 1 in force at that point
+        kin += 0.5 * (model.piS0[i] / model.fStar / model.omegaStar) ** 2
+    rho = kin + model.pot0
+    return rp.a0, model.fStar / model.MPl * math.sqrt(rho / 3.0)
+
+
+def scalar_fluctuations(model: Model, rp: RunParameters, field: int, aDot: float, dtype=np.float64):
+    """phi and pi fluctuations of scalar ``field`` in configuration space (no homogeneous part)."""
+    N = rp.N
+    nx, ny, nz = wave_numbers(N)
+    k = np.sqrt(nx * nx + ny * ny + nz * nz) * rp.kIR
+    m2 = model.masses2S[field]
+    omega = np.sqrt(k * k + (m2 if m2 > 0 else 0.0))
+    amp = model.omegaStar / model.fStar if model.fluct_amplitude is None else model.fluct_amplitude
+    with np.errstate(divide="ignore", invalid="ignore"):
+        norm = np.where(k <= rp.kCutoff, amp * (rp.lSide / rp.dx ** 2) ** 1.5 * (2 * omega) ** -0.5 / math.sqrt(2.0), 0.0)
+    norm[0, 0, 0] = 0.0
+    shape = norm.shape
+    name = f"scalar_{field}"
+
+    def gauss(label):
+        g = _rng(rp.baseSeed, f"{label}{name}")
+        return g.standard_normal(shape) + 1j * g.standard_normal(shape)
+
+    fL = norm * gauss("Random left")
+    fR = norm * gauss("Random right")
+    phik = (fL + fR) / math.sqrt(2.0)
+    phik[0, 0, 0] = 0.0
+    pik = 1j * omega * (fL - fR) / math.sqrt(2.0) - aDot * phik
+    pik[0, 0, 0] = 0.0
+    phi = sfft.irfftn(phik, s=(N, N, N), axes=(0, 1, 2), workers=-1)
+    pi = sfft.irfftn(pik, s=(N, N, N), axes=(0, 1, 2), workers=-1)
+    return phi.astype(dtype, copy=False), pi.astype(dtype, copy=False)
+
+
+def scalar_initial_state(model: Model, rp: RunParameters):
+    """Field and momentum arrays (Ns x N^3 each, float64) and the initial (aI, aDotI)."""
+    aI, aDot = initial_scale_factor(model, rp)
+    N = rp.N
+    fields = np.empty((model.Ns, N, N, N), dtype=np.float64)
+    momenta = np.empty_like(fields)
+    for f in range(model.Ns):
+        phi, pi = scalar_fluctuations(model, rp, f, aDot)
+        fields[f] = phi + model.fldS0[f] / model.fStar
+        momenta[f] = pi + model.piS0[f] / model.fStar / model.omegaStar
+    return fields, momenta, aI, aDot

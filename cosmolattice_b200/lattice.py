@@ -1,0 +1,275 @@
+"""Python handle over the C ABI, and the reference-shaped host API built on it.
+
+``Lattice`` owns one clb_handle (device state of one model on one GPU).  On top of it,
+``ModelInitializer``, ``Evolver`` and ``Measurer`` keep the reference's call shapes
+(initializers/modelinitializer.h:47-81, evolvers/evolver.h:45-155, measurements/measurer.h:87-178)
+so a driver reads like source/cosmolattice.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import _capi
+from .initializers import scalar_initial_state
+from .models import Model
+from .params import RunParameters
+
+PRECISIONS = {"fp64": _capi.PREC_FP64, "fp32": _capi.PREC_FP32_SPLIT}
+PATHS = {"fused": _capi.PATH_FUSED, "reference": _capi.PATH_REFERENCE}
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Lattice:
+    """One lattice of one model on one GPU (a clb_handle)."""
+
+    def __init__(self, model: Model, rp: RunParameters, precision: str = "fp64", path: str = "fused",
+                 device: int = 0):
+        self.lib = _capi.load()
+        self.model = model
+        self.rp = rp
+        cfg = _capi.Config()
+        cfg.N = rp.N
+        cfg.dx = rp.dx
+        cfg.dt = rp.dt
+        cfg.evolver = rp.eType
+        cfg.expansion = 1 if rp.expansion else 0
+        cfg.precision = PRECISIONS[precision]
+        cfg.path = PATHS[path]
+        cfg.device = device
+        self.cfg = cfg
+        self._desc = model.desc()
+        h = C.c_void_p()
+        rc = self.lib.clb_create(C.byref(cfg), C.byref(self._desc), C.byref(h))
+        if rc != _capi.CLB_OK:
+            raise _capi.ClbError(rc, self.lib.clb_last_error(None).decode())
+        self.h = h
+        nf, npm = C.c_int32(), C.c_int32()
+        self.lib.clb_num_components(self.h, C.byref(nf), C.byref(npm))
+        self.n_field_components, self.n_momentum_components = nf.value, npm.value
+
+    def _check(self, rc: int) -> None:
+        if rc != _capi.CLB_OK:
+            raise _capi.ClbError(rc, self.lib.clb_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.clb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, fields: np.ndarray, momenta: np.ndarray, sf: Optional[Dict[str, float]] = None) -> None:
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        p = np.ascontiguousarray(momenta, dtype=np.float64)
+        n3 = self.rp.N ** 3
+        if f.size != self.n_field_components * n3 or p.size != self.n_momentum_components * n3:
+            raise ValueError("state arrays do not match the model's component count")
+        s = None
+        if sf is not None:
+            s = _capi.ScaleFactor(**{k: float(sf.get(k, 0.0)) for k in ("aI", "aSI", "aIM", "aDotI", "aDotSI", "aDotSIM")})
+        self._check(self.lib.clb_set_state(self.h, _dp(f), _dp(p), C.byref(s) if s is not None else None))
+
+    def get_state(self, fields: bool = True, momenta: bool = True):
+        n = self.n_field_components * self.rp.N ** 3
+        f = np.empty(n) if fields else None
+        p = np.empty(n) if momenta else None
+        sf = _capi.ScaleFactor()
+        self._check(self.lib.clb_get_state(self.h, _dp(f) if fields else None, _dp(p) if momenta else None, C.byref(sf)))
+        sfd = {k: getattr(sf, k) for k, _ in _capi.ScaleFactor._fields_}
+        return f, p, sfd
+
+    def initialize(self, correct_adot: bool = True) -> None:
+        self._check(self.lib.clb_initialize(self.h, 1 if correct_adot else 0))
+
+    def evolve(self, n_steps: int) -> None:
+        self._check(self.lib.clb_evolve(self.h, int(n_steps)))
+
+    def sync(self) -> None:
+        self._check(self.lib.clb_sync(self.h))
+
+    def measure(self, e0: float = 1.0) -> Dict[str, object]:
+        m = _capi.Measurement()
+        self._check(self.lib.clb_measure(self.h, float(e0), C.byref(m)))
+        return measurement_to_dict(m)
+
+    def history(self) -> np.ndarray:
+        """Per-step rows (a, aDot, <pi^2>, <grad^2>, <V>) of the last evolve call."""
+        n = C.c_int64()
+        self._check(self.lib.clb_history(self.h, None, 0, C.byref(n)))
+        out = np.empty((n.value, _capi.HIST_COLS))
+        if n.value:
+            self._check(self.lib.clb_history(self.h, _dp(out), n.value, C.byref(n)))
+        return out
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.lib.clb_set_profiling(self.h, 1 if on else 0))
+
+    def reset_stats(self) -> None:
+        self._check(self.lib.clb_reset_stats(self.h))
+
+    def kernel_stats(self) -> Dict[str, Dict[str, float]]:
+        arr = (_capi.KernelStat * 16)()
+        n = C.c_int32()
+        self._check(self.lib.clb_kernel_stats(self.h, arr, 16, C.byref(n)))
+        return {arr[i].name.decode(): {"launches": arr[i].launches, "timed_launches": arr[i].timed_launches,
+                                       "total_ms": arr[i].total_ms} for i in range(min(n.value, 16))}
+
+    def last_evolve_ms(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.clb_last_evolve_ms(self.h, C.byref(v)))
+        return v.value
+
+    def cuda_stream(self) -> int:
+        return self.lib.clb_cuda_stream(self.h) or 0
+
+
+def measurement_to_dict(m: _capi.Measurement) -> Dict[str, object]:
+    return {
+        "aI": m.aI,
+        "aDotI": m.aDotI,
+        "hubble": m.hubble,
+        "energies": [m.energies[i] for i in range(m.n_energies)],
+        "friedmann": [m.friedmann[i] for i in range(3)],
+        "means": [[m.means[f][j] for j in range(6)] for f in range(m.n_means)],
+    }
+
+
+class ModelInitializer:
+    """ModelInitializer::initialize (modelinitializer.h:47-81) for scalar-singlet models."""
+
+    def __init__(self, model: Model, lSide: float, seed: str):
+        self.model = model
+
+    def initialize(self, model: Model, rp: RunParameters, lattice: Lattice) -> None:
+        fields, momenta, aI, aDot = scalar_initial_state(model, rp)
+        lattice.set_state(fields, momenta, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aDot, "aDotSI": aDot})
+        lattice.initialize(correct_adot=True)
+
+
+class Evolver:
+    """Evolver<Model> (evolver.h:45-155): LF and VV2-VV10 over a Lattice."""
+
+    def __init__(self, model: Model, rp: RunParameters, lattice: Lattice):
+        self.lattice = lattice
+
+    def evolve(self, model: Model, t_minus_t0: float) -> None:
+        self.lattice.evolve(1)
+
+    def evolve_n(self, n: int) -> None:
+        self.lattice.evolve(n)
+
+    def sync(self, model: Model, t_minus_t0: float) -> None:
+        self.lattice.sync()
+
+
+class Measurer:
+    """Frequent output of Measurer::measure (measurer.h:87-121) as reference text files:
+    average_energies.txt, average_energy_conservation.txt, average_scale_factor.txt and one
+    average_scalar_<i>.txt per singlet, numbers formatted with 15 significant digits
+    (measurementssaverstd.h:61-69)."""
+
+    def __init__(self, model: Model, rp: RunParameters, outdir: Optional[str] = None):
+        self.model = model
+        self.rp = rp
+        self.outdir = outdir if outdir is not None else rp.outFn
+        self.outputFreq = max(1, int(round(rp.tOutFreq / rp.dt)))
+        self.e0 = None
+        self.files: Dict[str, object] = {}
+        self.history: List[Dict[str, object]] = []
+        if self.outdir:
+            os.makedirs(self.outdir, exist_ok=True)
+
+    def _headers(self):
+        m = self.model
+        en = ["t"]
+        for i in range(m.Ns):
+            en += [f"E^kin_scal{i}", f"E^grad_scal{i}"]
+        en += [f"Vpot_term_{k}" for k in range(m.NPotTerms)] + ["E_tot"]
+        cons = ["t"] + (["rel_diff_friedmann", "LHS_friedmann", "RHS_friedmann"] if self.rp.expansion else ["energy_cons"])
+        return {
+            "energies": en,
+            "energy_conservation": cons,
+            "scale_factor": ["t", "a", "aDot", "H"],
+            **{f"scalar_{i}": ["t", "<phi>", "<pi>", "<phi^2>", "<pi^2>", "rms(phi)", "rms(pi)"] for i in range(m.Ns)},
+        }
+
+    def _write(self, name: str, values: List[float]) -> None:
+        if not self.outdir:
+            return
+        if name not in self.files:
+            path = os.path.join(self.outdir, f"average_{name}.txt")
+            if os.path.exists(path) and not self.rp.appendMode and not self.rp.overwriteMode:
+                raise FileExistsError(f'Refusing to overwrite existing output file "{path}". Set '
+                                      "'appendToFiles = true' to append, or 'overwriteFiles = true' to delete.")
+            fh = open(path, "a" if self.rp.appendMode else "w")
+            if self.rp.printHeaders and not self.rp.appendMode:
+                fh.write("#" + "    ".join(self._headers()[name]) + "\n")
+            self.files[name] = fh
+        fh = self.files[name]
+        fh.write("    ".join(f"{v:.15g}" for v in values) + "\n")
+        fh.flush()
+
+    def are_we_measuring(self, n: int) -> bool:
+        return n % self.outputFreq == 0
+
+    def measure(self, n: int, t: float, lattice: Lattice) -> Dict[str, object]:
+        first = self.e0 is None
+        m = lattice.measure(self.e0 if self.e0 is not None else 1.0)
+        etot = m["energies"][-1]
+        if first:
+            self.e0 = etot
+            if not self.rp.expansion:
+                m["friedmann"][0] = 0.0
+        m["t"] = t
+        self.history.append(m)
+        self._write("energies", [t] + m["energies"])
+        self._write("energy_conservation", [t] + (m["friedmann"] if self.rp.expansion else m["friedmann"][:1]))
+        if self.rp.expansion:
+            self._write("scale_factor", [t, m["aI"], m["aDotI"], m["hubble"]])
+        for i, row in enumerate(m["means"]):
+            self._write(f"scalar_{i}", [t] + row)
+        return m
+
+    def close(self) -> None:
+        for fh in self.files.values():
+            fh.close()
+        self.files = {}
+
+
+def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fused", outdir: Optional[str] = None):
+    """The reference main loop (source/cosmolattice.cpp:168-201) over the GPU library."""
+    from .models import MODELS
+    from .params import RunParameters
+
+    rp = RunParameters(par)
+    model = MODELS[model_name](par, rp)
+    lattice = Lattice(model, rp, precision=precision, path=path)
+    measurer = Measurer(model, rp, outdir)
+    ModelInitializer(model, rp.lSide, rp.baseSeed).initialize(model, rp, lattice)
+    evolver = Evolver(model, rp, lattice)
+    t = rp.t0
+    i = 0
+    while t < rp.tMax - rp.dt / 2.0:
+        if measurer.are_we_measuring(i):
+            evolver.sync(model, t - rp.t0)
+            measurer.measure(i, t, lattice)
+        # advance to the next measurement in one device call
+        n = measurer.outputFreq - (i % measurer.outputFreq)
+        n_left = int(round((rp.tMax - t) / rp.dt))
+        n = max(1, min(n, n_left))
+        evolver.evolve_n(n)
+        t += n * rp.dt
+        i += n
+    measurer.close()
+    return measurer.history, lattice

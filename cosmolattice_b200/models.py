@@ -1,0 +1,190 @@
+"""Host-side model descriptions in the reference's model API vocabulary.
+
+A model declares its field content, the program-unit rescaling (alpha, fStar, omegaStar), its
+potential terms and derivatives, and reads its couplings from the parameter file with the
+reference's keys.  ``desc()`` turns it into the C-ABI model descriptor; the per-site potential
+itself is compiled into the CUDA library (models/lphi4.h:154-226 restated in
+csrc/clb_scalar.cuh), the host copy below serves the homogeneous quantities (pot0, masses)
+that the reference computes in AbstractModel::setInitialPotentialAndMassesFromPotential
+(abstractmodel.h:220-248).
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Sequence
+
+from . import _capi
+from .params import ParameterParser, RunParameters
+
+# Reduced Planck mass in GeV.  TempLat's Constants::reducedMPlanck is not vendored with the
+# reference (scalefactorbase.h:18 uses it); this is the standard value, overridable with MPl=.
+REDUCED_MPLANCK_GEV = 2.435e18
+
+
+class CouplingsManager:
+    """Effective charges g*Q of matter fields under gauge fields (couplingsmanager.h:29-218).
+
+    ``pattern[m][g]`` says whether matter field m couples to gauge field g.  Charges are consumed
+    in order over the coupled pairs (row-major), couplings are picked by gauge index.
+    """
+
+    class NotEnoughCharges(ValueError):
+        """NotEnoughChargesForThisCouplingsManager"""
+
+    class NotEnoughCouplings(ValueError):
+        """NotEnoughCouplingsForThisCouplingsManager"""
+
+    def __init__(self, pattern: Sequence[Sequence[bool]]):
+        self.pattern = [list(map(bool, row)) for row in pattern]
+        self.n_matter = len(self.pattern)
+        self.n_gauge = len(self.pattern[0]) if self.pattern else 0
+        self._q = [[0.0] * self.n_gauge for _ in range(self.n_matter)]
+        self._g = [0.0] * self.n_gauge
+
+    def couples(self, m: int, g: int) -> bool:
+        return self.pattern[m][g]
+
+    def how_many_couples(self) -> int:
+        return sum(sum(r) for r in self.pattern)
+
+    def set_effective_charges(self, charges: Sequence[float], couplings: Sequence[float]) -> None:
+        if len(charges) != self.how_many_couples():
+            raise CouplingsManager.NotEnoughCharges(
+                f"{len(charges)} charges for {self.how_many_couples()} coupled pairs")
+        if len(couplings) != self.n_gauge:
+            raise CouplingsManager.NotEnoughCouplings(f"{len(couplings)} couplings for {self.n_gauge} gauge fields")
+        it = iter(charges)
+        for m in range(self.n_matter):
+            for g in range(self.n_gauge):
+                self._q[m][g] = next(it) * couplings[g] if self.pattern[m][g] else 0.0
+        self._g = list(couplings)
+
+    def __call__(self, m: int, g: int) -> float:
+        return self._q[m][g]
+
+    def coupling(self, g: int) -> float:
+        return self._g[g]
+
+
+class Model:
+    """Base of host model descriptions (the reference's AbstractModel, abstractmodel.h:84-318)."""
+
+    name = "model"
+    kind = 0
+    Ns = 0
+    NPotTerms = 1
+
+    def __init__(self, par: ParameterParser, rp: RunParameters):
+        self.rp = rp
+        self.alpha = 1.0
+        self.fStar = 1.0
+        self.omegaStar = 1.0
+        self.MPl = par.get_float("MPl", REDUCED_MPLANCK_GEV)
+        self.dx = rp.dx
+        self.kIR = rp.kIR
+        self.dt = rp.dt
+        self.fldS0: List[float] = [0.0] * self.Ns
+        self.piS0: List[float] = [0.0] * self.Ns
+        self.masses2S: List[float] = [0.0] * self.Ns
+        self.pot0 = 0.0
+        # fluctuation amplitude replacing omegaStar/fStar in the initial-spectrum norm
+        # (fluctuationsgenerator.h:64); the reference value when not given
+        self.fluct_amplitude = None
+
+    # ---- potential API on homogeneous program-unit values (numpy or float) ----
+    def potential_terms(self, k: int, phi):
+        raise NotImplementedError
+
+    def pot_deriv(self, n: int, phi):
+        raise NotImplementedError
+
+    def pot_deriv2(self, n: int, phi):
+        raise NotImplementedError
+
+    def potential(self, phi):
+        return sum(self.potential_terms(k, phi) for k in range(self.NPotTerms))
+
+    def couplings(self) -> List[float]:
+        raise NotImplementedError
+
+    def set_initial_potential_and_masses_from_potential(self) -> None:
+        """abstractmodel.h:220-248: pot0 and masses^2 at the homogeneous point phi0 / fStar."""
+        phi = [v / self.fStar for v in self.fldS0]
+        self.pot0 = self.potential(phi)
+        self.masses2S = [self.pot_deriv2(n, phi) for n in range(self.Ns)]
+
+    def desc(self) -> _capi.ModelDesc:
+        d = _capi.ModelDesc()
+        d.kind = self.kind
+        d.n_scalars = self.Ns
+        d.alpha = self.alpha
+        d.fStar = self.fStar
+        d.omegaStar = self.omegaStar
+        d.MPl = self.MPl
+        c = self.couplings()
+        for i, v in enumerate(c):
+            d.couplings[i] = v
+        return d
+
+
+class lphi4(Model):
+    """models/lphi4.h: two real scalars, V = phi^4/4 + q/2 phi^2 chi^2 in program variables.
+
+    Keys: lambda, q, initial_amplitudes (2 values, GeV), initial_momenta (2 values, GeV^2).
+    Rescaling (lphi4.h:125-127): alpha = 1, fStar = phi0, omegaStar = sqrt(lambda) fStar.
+    ``lambda_prog`` (default 1) multiplies the quartic term in program units, so a lattice can run
+    at a coupling other than the one that fixed omegaStar.
+    """
+
+    name = "lphi4"
+    kind = _capi.MODEL_LPHI4
+    Ns = 2
+    NPotTerms = 2
+
+    def __init__(self, par: ParameterParser, rp: RunParameters):
+        super().__init__(par, rp)
+        self.lam = par.get_float("lambda")
+        self.q = par.get_float("q", 0.0) if self.Ns == 2 else 0.0
+        self.c0 = par.get_float("lambda_prog", 1.0)
+        self.fldS0 = par.get_floats("initial_amplitudes", self.Ns)
+        self.piS0 = par.get_floats("initial_momenta", self.Ns, [0.0] * self.Ns)
+        self.alpha = 1.0
+        self.fStar = self.fldS0[0]
+        self.omegaStar = math.sqrt(self.lam) * self.fStar
+        if par.has("fluct_amplitude"):
+            self.fluct_amplitude = par.get_float("fluct_amplitude")
+        self.set_initial_potential_and_masses_from_potential()
+
+    def potential_terms(self, k, phi):
+        if k == 0:
+            return 0.25 * self.c0 * phi[0] ** 4
+        return 0.5 * self.q * (phi[0] * phi[1]) ** 2
+
+    def pot_deriv(self, n, phi):
+        if self.Ns == 1:
+            return self.c0 * phi[0] ** 3
+        if n == 0:
+            return self.c0 * phi[0] ** 3 + self.q * phi[0] * phi[1] ** 2
+        return self.q * phi[1] * phi[0] ** 2
+
+    def pot_deriv2(self, n, phi):
+        if self.Ns == 1:
+            return 3 * self.c0 * phi[0] ** 2
+        if n == 0:
+            return 3 * self.c0 * phi[0] ** 2 + self.q * phi[1] ** 2
+        return self.q * phi[0] ** 2
+
+    def couplings(self):
+        return [self.c0, self.q]
+
+
+class lphi4_1f(lphi4):
+    """One real scalar with V = lambda_prog/4 phi^4: the reference lphi4 header with its
+    daughter field removed (same keys; initial_amplitudes / initial_momenta take one value)."""
+
+    name = "lphi4_1f"
+    Ns = 1
+    NPotTerms = 1
+
+
+MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f}

@@ -1,0 +1,186 @@
+/* clb200.h - C ABI of the B200 lattice time-evolution library (libclb200.so).
+ *
+ * The reference has no FFI: its operator interface is the compile-time C++ template API
+ *   Evolver<Model>::Evolver / evolve / sync      (include/CosmoInterface/evolvers/evolver.h:45,102,132)
+ *   ModelInitializer<T>::initialize              (include/CosmoInterface/initializers/modelinitializer.h:47-81)
+ *   Measurer<Model,T>::measure                   (include/CosmoInterface/measurements/measurer.h:87-178)
+ * all called only from main (source/cosmolattice.cpp:134-188).  Each entry point below replaces
+ * one of those calls (cited per function).  Everything crossing this boundary is a plain C type:
+ * host arrays in, host arrays out; the library owns all device memory.
+ *
+ * Error convention: every int-returning function returns CLB_OK (0) or a negative CLB_E* code and
+ * records a message readable with clb_last_error().  No C++ exception crosses the boundary.
+ * Calls on one handle are not thread-safe; distinct handles are independent.
+ */
+#ifndef CLB200_H
+#define CLB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define CLB_OK            0
+#define CLB_EINVAL       -1 /* bad argument / inconsistent parameters (RunParametersInconsistent) */
+#define CLB_ECUDA        -2 /* CUDA runtime or cuFFT error */
+#define CLB_ENOMEM       -3 /* device allocation failed */
+#define CLB_ENONFINITE   -4 /* a volume average became NaN/Inf */
+#define CLB_ETIMEOUT     -5 /* a bounded device-side wait gave up */
+#define CLB_EUNSUPPORTED -6 /* combination not implemented (EvolverTypeNotInEvolver, ...) */
+#define CLB_ESTATE       -7 /* call out of order (e.g. evolve before initialize) */
+
+/* ---- evolver ids: same numbering as the reference enum EvolverType (evolvertype.h:37) ------ */
+#define CLB_LF     0
+#define CLB_VV2    1
+#define CLB_VV4    2
+#define CLB_VV6    3
+#define CLB_VV8    4
+#define CLB_VV10   5
+#define CLB_VV6_2  6
+
+/* ---- arithmetic forms -------------------------------------------------------------------- */
+#define CLB_PREC_FP64       0 /* fields, momenta, stencils, reductions and expansion in FP64 */
+#define CLB_PREC_FP32_SPLIT 1 /* fields/momenta/stencils FP32; reductions, a(t), constraints FP64 */
+
+/* ---- sweep schedule ---------------------------------------------------------------------- */
+#define CLB_PATH_FUSED     0 /* one drift+kick+averages sweep per VV stage (default)             */
+#define CLB_PATH_REFERENCE 1 /* the reference's operation order: kick, <pi^2>, drift, <grad^2>,<V>,
+                                kick, <pi^2> as separate sweeps (velocityverlet.h:69-113)           */
+
+/* ---- models ---------------------------------------------------------------------------------
+ * The model is chosen when the handle is created, as the reference chooses it at compile time
+ * (CMakeLists.txt:133-146).  Couplings are in program units.
+ *   CLB_MODEL_LPHI4   : n_scalars = 1 or 2 real singlets,
+ *                       V = c[0]/4 phi^4 + c[1]/2 phi^2 chi^2            (models/lphi4.h:154-177,
+ *                       with c[0] = 1 and c[1] = q reproducing the reference header exactly).
+ */
+#define CLB_MODEL_LPHI4 1
+
+#define CLB_MAX_COUPLINGS 8
+
+typedef struct clb_config {
+  int32_t N;          /* lattice points per dimension (RunParameters::N, runparameters.h:61)     */
+  double dx;          /* lattice spacing in program units (= 2 pi / (N kIR), runparameters.h:179-180) */
+  double dt;          /* time step (runparameters.h:64)                                         */
+  int32_t evolver;    /* CLB_LF, CLB_VV2 ... (runparameters.h:102)                              */
+  int32_t expansion;  /* 1: self-consistent expansion, 0: none (runparameters.h:66)             */
+  int32_t precision;  /* CLB_PREC_*                                                             */
+  int32_t path;       /* CLB_PATH_*                                                             */
+  int32_t device;     /* CUDA device ordinal                                                    */
+} clb_config;
+
+typedef struct clb_model_desc {
+  int32_t kind;       /* CLB_MODEL_*                                                            */
+  int32_t n_scalars;  /* Ns  (abstractmodel/scalarbase.h)                                       */
+  double alpha;       /* time-rescaling exponent (abstractmodel/modelparametersbase.h)          */
+  double fStar;       /* field rescaling f_*                                                    */
+  double omegaStar;   /* frequency rescaling omega_*                                            */
+  double MPl;         /* reduced Planck mass in the same units as fStar (scalefactorbase.h:18)  */
+  double couplings[CLB_MAX_COUPLINGS];
+} clb_model_desc;
+
+/* Scale-factor state in program units (abstractmodel/scalefactorbase.h:20-21). */
+typedef struct clb_scalefactor {
+  double aI, aSI, aIM;       /* a at integer time, at the half step, at the previous integer time */
+  double aDotI, aDotSI, aDotSIM;
+} clb_scalefactor;
+
+#define CLB_MAX_ENERGIES 32
+#define CLB_MAX_MEANS 8
+
+/* One measurement at the current (synchronised) time.
+ *  energies[] holds the columns of the reference's average_energies.txt after "t", in its order
+ *  (energiesmeasurer.h:45-101, headers :127-150): for each scalar singlet E^kin, E^grad; then each
+ *  potential term <V_k>; then E_tot.
+ *  friedmann[] holds (LHS-RHS)/(LHS+RHS), LHS, RHS with expansion (hubbleconstraint.h:27-36), or
+ *  energy_cons = |1 - E/E0| in friedmann[0] without expansion (energiesmeasurer.h:116-118).
+ *  means[f][] per scalar singlet: <phi>, <dphi/dt>, <phi^2>, <(dphi/dt)^2>, rms(phi), rms(dphi/dt)
+ *  with dphi/dt = a^(alpha-3) pi (meansmeasurer.h:28-48, scalarsingletmeasurer.h:61-66). */
+typedef struct clb_measurement {
+  double aI, aDotI, hubble;            /* scalefactormeasurer.h:37-48 */
+  int32_t n_energies;
+  double energies[CLB_MAX_ENERGIES];
+  double friedmann[3];
+  int32_t n_means;
+  double means[CLB_MAX_MEANS][6];
+} clb_measurement;
+
+typedef struct clb_handle clb_handle;
+
+/* Library version string. */
+const char *clb_version(void);
+
+/* Message of the last failed call on `h`; h == NULL gives the last failure of clb_create on the
+ * calling thread. */
+const char *clb_last_error(const clb_handle *h);
+
+/* Allocate a lattice and its device state.  Replaces the Model constructor's field allocation
+ * (abstractmodel.h:147-186, via MemoryToolBox::makeShared, source/cosmolattice.cpp:82-93) and the
+ * Evolver constructor's validation (evolvers/evolver.h:45-98). */
+int clb_create(const clb_config *cfg, const clb_model_desc *model, clb_handle **out);
+void clb_destroy(clb_handle *h);
+
+/* Number of real N^3 component arrays in the field and momentum buffers of clb_set_state. */
+int clb_num_components(const clb_handle *h, int32_t *n_field_components, int32_t *n_momentum_components);
+
+/* Upload a state from host memory.  fields: n_field_components x N^3 doubles, momenta likewise,
+ * each component row-major (x slowest, z fastest); order: scalar singlets 0..Ns-1.  The scale
+ * factor state sf may be NULL (a = 1, aDot = 0).  Mirrors the end state of the field-filling part
+ * of ModelInitializer::initialize (modelinitializer.h:54-69). */
+int clb_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf);
+
+/* Download the state (fields, momenta may be NULL to skip). */
+int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
+
+/* Finish initialisation: volume averages of the state (Averages::setAllAverages, averages.h:349-392),
+ * and with self-consistent expansion aDot_I = sqrt(Friedmann RHS) if correct_adot != 0
+ * (modelinitializer.h:74-80).  Then applies the evolver constructor: for LF,
+ * aDot_SI = aDot_I - dt/2 F (leapfrog.h:35) and the synced flag. */
+int clb_initialize(clb_handle *h, int32_t correct_adot);
+
+/* Advance n_steps time steps of dt: n_steps calls of Evolver::evolve (evolver.h:102-124). */
+int clb_evolve(clb_handle *h, int64_t n_steps);
+
+/* Evolver::sync (evolver.h:132-155): LF half-kicks the momenta to integer time; VV: no-op. */
+int clb_sync(clb_handle *h);
+
+/* Energies, Friedmann constraint and means at the current state (EnergiesMeasurer::measure,
+ * MeansMeasurer::measure, ScaleFactorMeasurer::measure).  Call after clb_sync.  e0 is the initial
+ * total energy used for energy_cons without expansion (ignored with expansion). */
+int clb_measure(clb_handle *h, double e0, clb_measurement *out);
+
+/* ---- per-step results and instrumentation (no reference counterpart: the reference writes these
+ *      averages to text files at its output cadence, measurer.h:87-121) -------------------------- */
+
+/* Columns of one history row: a, aDot, <pi^2>, <grad^2>, <V> at the end of each step. */
+#define CLB_HIST_COLS 5
+
+/* Rows recorded by the last clb_evolve (one per step; only with self-consistent expansion, where
+ * the averages are formed during the evolution).  Copies min(max_rows, rows) rows into out (may be
+ * NULL) and stores the number of rows in *n_rows. */
+int clb_history(clb_handle *h, double *out, int64_t max_rows, int64_t *n_rows);
+
+typedef struct clb_kernel_stat {
+  char name[40];
+  int64_t launches;       /* launches since the last reset                          */
+  int64_t timed_launches; /* launches bracketed by CUDA events while profiling was on */
+  double total_ms;        /* summed event time of the timed launches                */
+} clb_kernel_stat;
+
+/* Per-launch CUDA events on the handle's stream (on != 0), collected at each synchronising call. */
+int clb_set_profiling(clb_handle *h, int32_t on);
+int clb_reset_stats(clb_handle *h);
+/* Fills up to max entries, one per kernel kind; *n = number of kinds. */
+int clb_kernel_stats(clb_handle *h, clb_kernel_stat *out, int32_t max, int32_t *n);
+/* Device time of the last clb_evolve call, from events recorded on its stream around its launches. */
+int clb_last_evolve_ms(clb_handle *h, double *ms);
+/* The cudaStream_t the handle launches on (for callers that order their own work after it). */
+void *clb_cuda_stream(clb_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLB200_H */

@@ -1,0 +1,488 @@
+// oracle.cpp - FP64 CPU restatement of CosmoLattice's lattice time evolution.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: it is loaded by tests/, by
+// __graft_entry__.smoke() and by bench.py's CPU-baseline leg, never by the product path.
+//
+// It restates, in the reference's own operation order, the arithmetic of
+//   evolvers/velocityverlet.h:51-266, evolvers/velocityverletparameters.h:23-46,
+//   evolvers/leapfrog.h:29-277, evolvers/kernels/scalarsingletkernels.h:30-40,
+//   evolvers/kernels/scalefactorkernels.h:27-80, definitions/energies.h:37-239,
+//   definitions/averages.h:27-129, definitions/fieldfunctionals.h:52-67,
+//   definitions/gaugederivatives.h:36-73, definitions/hubbleconstraint.h:27-36,
+//   measurements/energiesmeasurer.h:45-122, measurements/meansmeasurer.h:28-48,
+//   initializers/modelinitializer.h:73-80 and models/lphi4.h:154-226
+// (paths relative to the reference's include/CosmoInterface or the reference root).
+//
+// Parity status: the operators that live in the un-vendored TempLat runtime (LatLapl, Grad2,
+// average, pow<N>) are restated from their in-tree definitions where one exists
+// (gaugederivatives.h:36-40 Laplacian, :70-73 forward gradient) and otherwise by a stated choice;
+// the reference's tests hold no golden vectors for this path, so the oracle is pinned only by
+// physics known-answer tests (see tests/test_oracle_*.py): parity unpinned against TempLat itself.
+//
+// Deterministic: every volume sum is formed per x-plane (fixed z, then y order), and the planes
+// are added in x order, independent of the OpenMP thread count.
+
+#include "../include/clb200.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// Integer power by repeated multiplication; negative exponents invert the positive power.
+// (TempLat pow<N>; restated choice.)
+inline double ipow(double x, int n)
+{
+  if (n == 0) return 1.0;
+  if (n < 0) return 1.0 / ipow(x, -n);
+  double r = x;
+  for (int i = 1; i < n; ++i) r = r * x;
+  return r;
+}
+
+// Composition coefficients, velocityverletparameters.h:23-46.
+std::vector<double> vvCoeffs(int ev)
+{
+  switch (ev) {
+  case CLB_VV2: return {1.0};
+  case CLB_VV4: return {1.351207191959657771818, -1.702414403875838200264};
+  case CLB_VV6: return {0.78451361047755726382, 0.23557321335935813368, -1.1776799841788710069, 1.3151863206839112189};
+  case CLB_VV6_2:
+    return {0.39216144400731413928, 0.33259913678935943860, -0.70624617255763935981, 0.082213596293550800230,
+            0.79854399093482996340};
+  case CLB_VV8:
+    return {0.74167036435061295345, -0.40910082580003159400, 0.19075471029623837995, -0.57386247111608226666,
+            0.29906418130365592384, 0.33462491824529818378,  0.31529309239676659663, -0.79688793935291635402};
+  case CLB_VV10:
+    return {-0.48159895600253002870, 0.0036303931544595926879, 0.50180317558723140279,  0.28298402624506254868,
+            0.80702967895372223806,  -0.026090580538592205447, -0.87286590146318071547, -0.52373568062510581643,
+            0.44521844299952789252,  0.18612289547097907887,   0.23137327866438360633,  -0.52191036590418628905,
+            0.74866113714499296793,  0.066736511890604057532,  -0.80360324375670830316, 0.91249037635867994571};
+  default: return {};
+  }
+}
+
+struct Oracle {
+  clb_config cfg;
+  clb_model_desc md;
+  int N;
+  size_t n3;
+  int Ns;
+  std::vector<double> fld, pi; // Ns x N^3 each
+
+  // ScaleFactorBase (scalefactorbase.h:20-21) and cached averages (scalarbase.h, abstractmodel.h:142)
+  double aI = 1, aSI = 1, aIM = 1, aDotI = 0, aDotSI = 0, aDotSIM = 0;
+  double pi2AvI = 0, pi2AvSI = 0, pi2AvSIM = 0, grad2AvI = 0, potAvI = 0, potAvSI = 0;
+  bool synced = true;   // LeapFrog::synced (leapfrog.h:31)
+  bool initialized = false;
+  std::vector<double> ws;
+  std::string err;
+
+  size_t at(int x, int y, int z) const { return ((size_t)x * N + y) * N + z; }
+  int up(int i) const { return i + 1 == N ? 0 : i + 1; }
+  int dn(int i) const { return i == 0 ? N - 1 : i - 1; }
+
+  double *F(int f) { return fld.data() + (size_t)f * n3; }
+  double *P(int f) { return pi.data() + (size_t)f * n3; }
+
+  // ---- model: lphi4 (models/lphi4.h:154-226), c0 = couplings[0] (1 in the reference), q = couplings[1]
+  double c0() const { return md.couplings[0]; }
+  double q() const { return md.couplings[1]; }
+
+  // potentialTerms(Tag<0>) = 0.25 * pow<4>(phi);  Tag<1> = 0.5 * q * pow<2>(phi * chi)
+  double potTerm(int k, size_t s) const
+  {
+    const double p = fld[s];
+    if (k == 0) return (0.25 * c0()) * ipow(p, 4);
+    const double c = fld[n3 + s];
+    return (0.5 * q()) * ipow(p * c, 2);
+  }
+  double potential(size_t s) const
+  {
+    double v = potTerm(0, s);
+    if (Ns > 1) v = v + potTerm(1, s);
+    return v;
+  }
+  // potDeriv(Tag<0>) = pow<3>(phi) + q * phi * pow<2>(chi);  Tag<1> = q * chi * pow<2>(phi)
+  double potDeriv(int f, size_t s) const
+  {
+    const double p = fld[s];
+    if (Ns == 1) return c0() * ipow(p, 3);
+    const double c = fld[n3 + s];
+    if (f == 0) return c0() * ipow(p, 3) + (q() * p) * ipow(c, 2);
+    return (q() * c) * ipow(p, 2);
+  }
+
+  // Lattice Laplacian: (1/dx^2) * sum_i [f(x+i) + f(x-i) - 2 f(x)]  (gaugederivatives.h:36-40)
+  double lapl(const double *f, int x, int y, int z) const
+  {
+    const double c = f[at(x, y, z)];
+    const double tx = (f[at(up(x), y, z)] + f[at(dn(x), y, z)]) - 2 * c;
+    const double ty = (f[at(x, up(y), z)] + f[at(x, dn(y), z)]) - 2 * c;
+    const double tz = (f[at(x, y, up(z))] + f[at(x, y, dn(z))]) - 2 * c;
+    return (1.0 / (md_dx() * md_dx())) * ((tx + ty) + tz);
+  }
+  double md_dx() const { return cfg.dx; }
+
+  // Sum over the forward-difference gradient squared, sum_i (f(x+i)-f(x))^2 / dx^2
+  // (Grad2 of fieldfunctionals.h:52-56 with the forward derivative of gaugederivatives.h:70-73).
+  double grad2(const double *f, int x, int y, int z) const
+  {
+    const double c = f[at(x, y, z)];
+    const double gx = f[at(up(x), y, z)] - c;
+    const double gy = f[at(x, up(y), z)] - c;
+    const double gz = f[at(x, y, up(z))] - c;
+    return ((gx * gx + gy * gy) + gz * gz) * (1.0 / (cfg.dx * cfg.dx));
+  }
+
+  // Deterministic volume average of a per-site functional g(x,y,z).
+  template <class G> double average(G g) const
+  {
+    std::vector<double> planes(N, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int x = 0; x < N; ++x) {
+      double sx = 0;
+      for (int y = 0; y < N; ++y) {
+        double sy = 0;
+        for (int z = 0; z < N; ++z) sy += g(x, y, z);
+        sx += sy;
+      }
+      planes[x] = sx;
+    }
+    double s = 0;
+    for (int x = 0; x < N; ++x) s += planes[x];
+    return s / (double)n3;
+  }
+
+  // ---- Averages (averages.h:290-298, velocityverlet.h:249-266)
+  double avPi2()
+  {
+    return average([&](int x, int y, int z) {
+      const size_t s = at(x, y, z);
+      double v = pi[s] * pi[s];
+      for (int f = 1; f < Ns; ++f) v = v + pi[f * n3 + s] * pi[f * n3 + s];
+      return v;
+    });
+  }
+  double avGrad2()
+  {
+    return average([&](int x, int y, int z) {
+      double v = grad2(F(0), x, y, z);
+      for (int f = 1; f < Ns; ++f) v = v + grad2(F(f), x, y, z);
+      return v;
+    });
+  }
+  double avPot()
+  {
+    return average([&](int x, int y, int z) { return potential(at(x, y, z)); });
+  }
+
+  // ---- Energies (energies.h:37-45): kineticS = 0.5 * <pi^2> * a^-6, gradientS = 0.5 * <grad^2> * a^-2
+  double kineticS(double fldf) const { return (0.5 * fldf) * ipow(aI, -6); }
+  double gradientS(double fldf) const { return (0.5 * fldf) * ipow(aI, -2); }
+
+  // ScaleFactorKernels::get (scalefactorkernels.h:73-77), scalar singlets only.
+  double sfKernel() const
+  {
+    const double al = md.alpha;
+    const double Eks = kineticS(pi2AvI);
+    const double Egs = gradientS(grad2AvI);
+    const double fm = md.fStar / md.MPl;
+    return std::pow(aI, 2 * al + 1) / 3.0 * (fm * fm) *
+           ((((al - 2) * Eks + al * Egs) + (al - 1) * 0.0) + (al + 1) * potAvI);
+  }
+
+  // ---- Sweeps
+  // Kick: pi += h * [a^(1+alpha) lapl(phi) - a^(3+alpha) dV/dphi]  (scalarsingletkernels.h:30-40)
+  void kick(double h)
+  {
+    // In place: the kick reads phi (stencil) and pi only at the site it writes.
+    const double A = std::pow(aI, 1 + md.alpha);
+    const double B = std::pow(aI, 3 + md.alpha);
+#pragma omp parallel for schedule(static)
+    for (int x = 0; x < N; ++x)
+      for (int y = 0; y < N; ++y)
+        for (int z = 0; z < N; ++z) {
+          const size_t s = at(x, y, z);
+          for (int f = 0; f < Ns; ++f) {
+            const double K = A * lapl(F(f), x, y, z) - B * potDeriv(f, s);
+            pi[f * n3 + s] = pi[f * n3 + s] + h * K;
+          }
+        }
+  }
+  // Drift: phi += pow(aSI, alpha-3) * (c * pi)  (velocityverlet.h:181-184, leapfrog.h:185-190)
+  void drift(double c)
+  {
+    const double p = std::pow(aSI, md.alpha - 3);
+#pragma omp parallel for schedule(static)
+    for (size_t s = 0; s < (size_t)Ns * n3; ++s) fld[s] = fld[s] + p * (c * pi[s]);
+  }
+
+  // ---- Averages::setAllAverages (averages.h:349-358)
+  void setAllAverages()
+  {
+    potAvI = avPot();
+    potAvSI = potAvI;
+    pi2AvI = avPi2();
+    pi2AvSI = pi2AvI;
+    grad2AvI = avGrad2();
+  }
+
+  // Energies::rho (energies.h:217-239) and HubbleConstraint::get (hubbleconstraint.h:27-36)
+  void hubble(double out[3])
+  {
+    setAllAverages();
+    const double rho = (kineticS(pi2AvI) + gradientS(grad2AvI)) + potAvI;
+    const double LHS = aDotI * aDotI;
+    const double fm = md.fStar / md.MPl;
+    const double RHS = std::pow(aI, 2 * md.alpha + 2) / 3. * (fm * fm) * rho;
+    out[0] = (LHS - RHS) / (LHS + RHS);
+    out[1] = LHS;
+    out[2] = RHS;
+  }
+
+  // ---- VelocityVerlet::evolve (velocityverlet.h:51-114), self-consistent or no expansion
+  void evolveVV()
+  {
+    const double dt = cfg.dt;
+    const size_t P = ws.size();
+    const size_t stages = (P - 1) * 2 + 1;
+    const bool ex = cfg.expansion != 0;
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < P ? i : stages - i - 1];
+      if (ex) aDotSI = aDotI + (dt / 2) * sfKernel() * w;   // kickScaleFactorHalf (:165-169)
+      kick(w * dt / 2);                                      // kickScalar (:129-132)
+      if (ex) {
+        pi2AvI = avPi2();                                    // storeMomentaAverages (:249-256)
+        aIM = aI;                                            // driftScaleFactor (:225-243)
+        aI += dt * aDotSI * w;
+        aSI = (aIM + aI) / 2.0;
+      }
+      drift(dt * w);                                         // driftScalar (:181-184)
+      if (ex) {                                              // storeFieldsAverages (:258-266)
+        grad2AvI = avGrad2();
+        potAvI = avPot();
+      }
+      kick(w * dt / 2);
+      if (ex) {
+        pi2AvI = avPi2();
+        aDotI = aDotSI + (dt / 2) * sfKernel() * w;          // kickScaleFactorOne (:171-174)
+      }
+    }
+  }
+
+  // ---- LeapFrog::evolve (leapfrog.h:42-89)
+  void evolveLF()
+  {
+    const double dt = cfg.dt;
+    const bool ex = cfg.expansion != 0;
+    const double weight = synced ? 0.5 : 1.0;
+    kick(weight * dt);                                      // kickScalar (:131-134)
+    if (ex) {
+      pi2AvSIM = pi2AvSI;                                   // storeMomentaAverages (:239-245)
+      pi2AvSI = avPi2();
+      pi2AvI = 0.5 * (pi2AvSIM + pi2AvSI);
+      aDotSIM = aDotSI;                                     // kickScaleFactor (:124-129)
+      aDotSI += dt * sfKernel();
+      aDotI = (aDotSIM + aDotSI) / 2.0;
+      aIM = aI;                                             // driftScaleFactor (:168-184)
+      aI += dt * aDotSI;
+      aSI = (aIM + aI) / 2.0;
+    }
+    drift(dt);                                              // driftScalar (:185-190)
+    if (ex) {                                               // storeFieldsAverages (:269-277)
+      grad2AvI = avGrad2();
+      potAvI = avPot();
+    }
+    synced = false;
+  }
+
+  // ---- LeapFrog::sync (leapfrog.h:96-116)
+  void syncLF()
+  {
+    if (!synced) {
+      kick(0.5 * cfg.dt);
+      if (cfg.expansion) {
+        pi2AvI = avPi2();
+        aDotI = aDotSI + cfg.dt / 2.0 * sfKernel();
+      }
+    }
+    synced = true;
+  }
+};
+
+thread_local std::string g_err;
+
+} // namespace
+
+extern "C" {
+
+typedef struct orc_handle orc_handle;
+
+const char *orc_last_error(orc_handle *h)
+{
+  return h ? reinterpret_cast<Oracle *>(h)->err.c_str() : g_err.c_str();
+}
+
+int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out)
+{
+  if (!cfg || !md || !out) { g_err = "null argument"; return CLB_EINVAL; }
+  if (md->kind != CLB_MODEL_LPHI4 || md->n_scalars < 1 || md->n_scalars > 2) {
+    g_err = "oracle: only lphi4 with 1 or 2 scalar singlets";
+    return CLB_EUNSUPPORTED;
+  }
+  if (cfg->N < 2) { g_err = "N must be >= 2"; return CLB_EINVAL; }
+  Oracle *o = new Oracle();
+  o->cfg = *cfg;
+  o->md = *md;
+  o->N = cfg->N;
+  o->n3 = (size_t)cfg->N * cfg->N * cfg->N;
+  o->Ns = md->n_scalars;
+  o->fld.assign((size_t)o->Ns * o->n3, 0.0);
+  o->pi.assign((size_t)o->Ns * o->n3, 0.0);
+  if (cfg->evolver != CLB_LF) {
+    o->ws = vvCoeffs(cfg->evolver);
+    if (o->ws.empty()) { delete o; g_err = "unsupported evolver"; return CLB_EUNSUPPORTED; }
+  }
+  *out = reinterpret_cast<orc_handle *>(o);
+  return CLB_OK;
+}
+
+void orc_destroy(orc_handle *h) { delete reinterpret_cast<Oracle *>(h); }
+
+int orc_set_state(orc_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  std::memcpy(o->fld.data(), fields, o->fld.size() * sizeof(double));
+  std::memcpy(o->pi.data(), momenta, o->pi.size() * sizeof(double));
+  if (sf) {
+    o->aI = sf->aI; o->aSI = sf->aSI; o->aIM = sf->aIM;
+    o->aDotI = sf->aDotI; o->aDotSI = sf->aDotSI; o->aDotSIM = sf->aDotSIM;
+  }
+  o->initialized = false;
+  return CLB_OK;
+}
+
+int orc_get_state(orc_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (fields) std::memcpy(fields, o->fld.data(), o->fld.size() * sizeof(double));
+  if (momenta) std::memcpy(momenta, o->pi.data(), o->pi.size() * sizeof(double));
+  if (sf) {
+    sf->aI = o->aI; sf->aSI = o->aSI; sf->aIM = o->aIM;
+    sf->aDotI = o->aDotI; sf->aDotSI = o->aDotSI; sf->aDotSIM = o->aDotSIM;
+  }
+  return CLB_OK;
+}
+
+// ModelInitializer tail (modelinitializer.h:74-80) then the evolver constructor (leapfrog.h:35).
+int orc_initialize(orc_handle *h, int32_t correct_adot)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  o->setAllAverages();
+  if (o->cfg.expansion && correct_adot) {
+    double hl[3];
+    o->hubble(hl);
+    o->aDotI = std::sqrt(hl[2]);
+  }
+  o->synced = true;
+  if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
+  o->initialized = true;
+  return CLB_OK;
+}
+
+int orc_evolve(orc_handle *h, int64_t n)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (!o->initialized) { o->err = "evolve before initialize"; return CLB_ESTATE; }
+  for (int64_t s = 0; s < n; ++s) {
+    if (o->cfg.evolver == CLB_LF)
+      o->evolveLF();
+    else
+      o->evolveVV();
+  }
+  return CLB_OK;
+}
+
+int orc_sync(orc_handle *h)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (o->cfg.evolver == CLB_LF) o->syncLF();
+  return CLB_OK;
+}
+
+// Measurer::measure frequent output: EnergiesMeasurer (energiesmeasurer.h:45-122), MeansMeasurer
+// (meansmeasurer.h:28-48), ScaleFactorMeasurer (scalefactormeasurer.h:37-48).
+int orc_measure(orc_handle *h, double e0, clb_measurement *m)
+{
+  Oracle *o = reinterpret_cast<Oracle *>(h);
+  std::memset(m, 0, sizeof(*m));
+  if (!o->cfg.expansion) o->potAvI = o->avPot();               // measurer.h:274-276
+  const double am6 = ipow(o->aI, -6), am2 = ipow(o->aI, -2);
+  double Etot = 0;
+  int k = 0;
+  for (int f = 0; f < o->Ns; ++f) {
+    const double *pf = o->P(f);
+    const double *ff = o->F(f);
+    const double Ekin = o->average([&](int x, int y, int z) {
+      const double p = pf[o->at(x, y, z)];
+      return (0.5 * (p * p)) * am6;
+    });
+    const double Egrad = o->average([&](int x, int y, int z) { return (0.5 * o->grad2(ff, x, y, z)) * am2; });
+    Etot += Ekin + Egrad;
+    m->energies[k++] = Ekin;
+    m->energies[k++] = Egrad;
+  }
+  const int nPot = o->Ns > 1 ? 2 : 1;
+  for (int t = 0; t < nPot; ++t) {
+    const double v = o->average([&](int x, int y, int z) { return o->potTerm(t, o->at(x, y, z)); });
+    m->energies[k++] = v;
+    Etot += v;
+  }
+  m->energies[k++] = Etot;
+  m->n_energies = k;
+  if (o->cfg.expansion) {
+    o->hubble(m->friedmann);
+  } else {
+    m->friedmann[0] = std::fabs(1.0 - Etot / e0);
+  }
+  const double am = std::pow(o->aI, o->md.alpha - 3);
+  for (int f = 0; f < o->Ns; ++f) {
+    const double *pf = o->P(f);
+    const double *ff = o->F(f);
+    const double phi = o->average([&](int x, int y, int z) { return ff[o->at(x, y, z)]; });
+    const double phi2 = o->average([&](int x, int y, int z) { const double v = ff[o->at(x, y, z)]; return v * v; });
+    const double mom = o->average([&](int x, int y, int z) { return pf[o->at(x, y, z)] * am; });
+    const double mom2 = o->average([&](int x, int y, int z) { const double v = pf[o->at(x, y, z)] * am; return v * v; });
+    const double r1 = phi2 - phi * phi, r2 = mom2 - mom * mom;
+    m->means[f][0] = phi;
+    m->means[f][1] = mom;
+    m->means[f][2] = phi2;
+    m->means[f][3] = mom2;
+    m->means[f][4] = r1 > 0 ? std::sqrt(r1) : 0;
+    m->means[f][5] = r2 > 0 ? std::sqrt(r2) : 0;
+  }
+  m->n_means = o->Ns;
+  m->aI = o->aI;
+  m->aDotI = o->aDotI;
+  m->hubble = o->aDotI / o->aI;
+  return CLB_OK;
+}
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+} // extern "C"

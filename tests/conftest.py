@@ -1,0 +1,47 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the product kernels")
+
+
+def make_scalar_case(N=16, evolver="VV2", expansion=True, model="lphi4_1f", dt=0.01, seed="t", amp=1e-3,
+                     kcut=None, extra=None):
+    """Parameter set, run parameters, model and initial state of a small lphi4 lattice."""
+    from cosmolattice_b200 import MODELS, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import scalar_initial_state
+
+    params = {
+        "N": N, "kIR": 1.0, "dt": dt, "evolver": evolver, "expansion": "true" if expansion else "false",
+        "lambda": 1.0, "initial_amplitudes": "5.6964e18" if model == "lphi4_1f" else "5.6964e18 0",
+        "initial_momenta": "0" if model == "lphi4_1f" else "0 0",
+        "fluct_amplitude": amp, "kCutOff": kcut if kcut is not None else N / 4.0, "baseSeed": seed,
+    }
+    if model == "lphi4":
+        params["q"] = 1.5
+        params["initial_amplitudes"] = "5.6964e18 1e17"
+    if extra:
+        params.update(extra)
+    par = ParameterParser(params=params)
+    rp = RunParameters(par)
+    m = MODELS[model](par, rp)
+    f, p, aI, aD = scalar_initial_state(m, rp)
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+    return par, rp, m, f, p, sf
+
+
+@pytest.fixture(scope="session")
+def gpu_available():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False

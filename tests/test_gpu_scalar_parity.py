@@ -1,0 +1,166 @@
+"""Parity of the CUDA scalar-singlet path with the FP64 CPU oracle (runs on a B200).
+
+Tolerances (BASELINE north star (a)): started from identical arrays, per-site fields and momenta
+within 1e-12 relative (to the array's max |value|) after 100 steps; a(t), aDot, volume averages
+and energies within 1e-10 relative.  The FP32/FP64-split form is checked against the same
+oracle with its own stated bounds.
+"""
+import numpy as np
+import pytest
+
+from conftest import make_scalar_case
+
+pytestmark = pytest.mark.gpu
+
+SITE_TOL = 1e-12
+AVG_TOL = 1e-10
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+def run_pair(N, evolver, expansion, nsteps, model="lphi4_1f", path="fused", precision="fp64", measure_every=None,
+             dt=0.01, amp=1e-3):
+    from cosmolattice_b200 import Lattice
+    from oracle.oracle import OracleLattice
+
+    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, expansion=expansion, model=model, dt=dt, amp=amp)
+    gpu = Lattice(m, rp, precision=precision, path=path)
+    cpu = OracleLattice(m, rp)
+    meas = {"gpu": [], "cpu": []}
+    for key, lat in (("gpu", gpu), ("cpu", cpu)):
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.sync()
+        m0 = lat.measure(1.0)
+        e0 = m0["energies"][-1]
+        meas[key].append(m0)
+        done = 0
+        while done < nsteps:
+            k = nsteps - done if measure_every is None else min(measure_every, nsteps - done)
+            lat.evolve(k)
+            done += k
+            if measure_every is not None:
+                lat.sync()
+                meas[key].append(lat.measure(e0))
+        lat.sync()
+        meas[key].append(lat.measure(e0))
+    out = (gpu.get_state(), cpu.get_state(), meas)
+    gpu.close()
+    cpu.close()
+    return out
+
+
+def check_state(g, c, site_tol=SITE_TOL, sf_tol=AVG_TOL):
+    (fg, pg, sg), (fc, pc, sc) = g, c
+    assert rel(fg, fc) < site_tol, rel(fg, fc)
+    assert rel(pg, pc) < site_tol, rel(pg, pc)
+    for k in ("aI", "aDotI"):
+        assert abs(sg[k] - sc[k]) <= sf_tol * max(abs(sc[k]), 1e-300), (k, sg[k], sc[k])
+
+
+def check_meas(mg, mc, tol=AVG_TOL):
+    for a, b in zip(mg, mc):
+        assert rel(a["energies"], b["energies"]) < tol
+        for ea, eb in zip(a["energies"], b["energies"]):
+            assert abs(ea - eb) <= tol * abs(eb) + 1e-300, (ea, eb)
+        assert abs(a["friedmann"][1] - b["friedmann"][1]) <= tol * abs(b["friedmann"][1]) + 1e-300
+        assert abs(a["friedmann"][2] - b["friedmann"][2]) <= tol * abs(b["friedmann"][2]) + 1e-300
+        for ra, rb in zip(a["means"], b["means"]):
+            for x, y in zip(ra[:4], rb[:4]):
+                assert abs(x - y) <= tol * max(abs(y), 1e-30), (x, y)
+
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+@pytest.mark.parametrize("expansion", [True, False])
+def test_lphi4_64_vv2_100_steps(path, expansion):
+    g, c, meas = run_pair(64, "VV2", expansion, 100, path=path)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("evolver", ["VV4", "VV6", "VV8", "VV10", "VV6_2"])
+def test_higher_order_vv(evolver):
+    g, c, meas = run_pair(24, evolver, True, 20)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+@pytest.mark.parametrize("expansion", [True, False])
+def test_leapfrog_with_syncs(path, expansion):
+    # LF momenta live at half steps; sync + measure every 7 steps exercises the half-kick restart
+    # and the averages refreshed by the Friedmann measurement (energies.h:219).
+    g, c, meas = run_pair(32, "LF", expansion, 50, path=path, measure_every=7)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("evolver", ["VV2", "LF"])
+def test_two_field_lphi4(evolver):
+    g, c, meas = run_pair(32, evolver, True, 40, model="lphi4")
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("N", [2, 3, 12, 20, 48, 40])
+def test_ragged_sizes(N):
+    # sizes that do not fill the 32 x 8 column tile, including the smallest periodic lattices
+    g, c, meas = run_pair(N, "VV2", True, 15, amp=1e-2)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_measure_cadence_vv():
+    g, c, meas = run_pair(32, "VV4", True, 30, measure_every=4)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_deterministic_reductions():
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = make_scalar_case(N=48, evolver="VV2", expansion=True)
+    outs = []
+    for _ in range(2):
+        lat = Lattice(m, rp)
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.evolve(25)
+        outs.append(lat.get_state())
+        lat.close()
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+
+
+def test_fp32_split_against_fp64():
+    # FP32 fields/momenta/stencils with FP64 reductions and a(t): field error bounded by FP32
+    # rounding accumulated over the run; a(t) and the Friedmann constraint follow FP64 closely.
+    g, c, meas = run_pair(64, "VV2", True, 100, precision="fp32")
+    (fg, pg, sg), (fc, pc, sc) = g, c
+    assert rel(fg, fc) < 1e-6
+    fluct_g = fg - fg.mean()
+    fluct_c = fc - fc.mean()
+    assert rel(fluct_g, fluct_c) < 1e-3
+    assert abs(sg["aI"] - sc["aI"]) / sc["aI"] < 1e-7
+    fr_g = meas["gpu"][-1]["friedmann"][0]
+    fr_c = meas["cpu"][-1]["friedmann"][0]
+    assert abs(fr_g - fr_c) < 1e-6
+
+
+def test_errors_surface_through_the_abi():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_scalar_case(N=8, evolver="VV2", expansion=True)
+    lat = Lattice(m, rp)
+    with pytest.raises(_capi.ClbError) as ei:
+        lat.evolve(1)
+    assert ei.value.code == _capi.CLB_ESTATE
+    bad = f.copy()
+    bad.ravel()[5] = np.nan
+    lat.set_state(bad, p, sf)
+    with pytest.raises(_capi.ClbError) as ei:
+        lat.initialize()
+    assert ei.value.code == _capi.CLB_ENONFINITE
+    lat.close()

@@ -1,0 +1,96 @@
+"""Host-side parameter handling and the couplings manager (no GPU)."""
+import math
+
+import pytest
+
+from cosmolattice_b200 import CouplingsManager, ParameterParser, RunParameters
+from cosmolattice_b200.params import NotAnEvolverType, RunParametersInconsistent, RunParametersMissing, parse_evolver
+
+
+def rp_of(**kw):
+    base = {"N": 32, "dt": 0.01}
+    base.update(kw)
+    return RunParameters(ParameterParser(params=base))
+
+
+def test_lattice_size_from_kir_lside_dx():
+    # runparameters.h:155-186: lSide = 2 pi / kIR = N dx
+    a = rp_of(kIR=1.0)
+    assert math.isclose(a.lSide, 2 * math.pi) and math.isclose(a.dx, 2 * math.pi / 32)
+    b = rp_of(lSide=2 * math.pi)
+    assert math.isclose(b.kIR, 1.0)
+    c = rp_of(dx=2 * math.pi / 32)
+    assert math.isclose(c.kIR, 1.0)
+    d = rp_of(kIR=1.0, lSide=2 * math.pi, dx=2 * math.pi / 32)
+    assert math.isclose(d.dx, a.dx)
+
+
+def test_lattice_size_errors():
+    with pytest.raises(RunParametersMissing):
+        rp_of()
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, lSide=3.0)
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, dx=0.5)
+
+
+def test_run_parameter_checks():
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, dt=0.0)
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, tMax=-1.0)
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, tOutputFreq=0.001)
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, appendToFiles="true", overwriteFiles="true")
+    with pytest.raises(RunParametersInconsistent):
+        rp_of(kIR=1.0, PS_type=3)
+
+
+def test_defaults_and_bins():
+    r = rp_of(kIR=0.7)
+    assert r.nBinsSpectra == math.floor(math.sqrt(3) / 2 * 32)  # runparameters.h:98
+    assert r.eType == 0 and r.expansion  # LF and expansion by default
+    kUV = math.sqrt(3) * math.pi / r.dx
+    assert math.isclose(r.kCutoff, 2 * kUV)  # no cutoff -> 2 kUV (runparameters.h:198-200)
+
+
+def test_evolver_names_and_numbers():
+    # evolvertype.h:37-82: names or integers
+    for i, name in enumerate(["LF", "VV2", "VV4", "VV6", "VV8", "VV10", "VV6_2"]):
+        assert parse_evolver(name) == i
+        assert parse_evolver(str(i)) == i
+    with pytest.raises(NotAnEvolverType):
+        parse_evolver("RK2")
+    with pytest.raises(NotAnEvolverType):
+        parse_evolver("banana")
+
+
+def test_parameter_file_syntax(tmp_path):
+    f = tmp_path / "p.in"
+    f.write_text("#Lattice\nN = 64\ndt = 0.01 # comment\nkIR = .7\ninitial_amplitudes = 5.6964e18 0  # GeV\n")
+    par = ParameterParser(filename=str(f), overrides=["N=32"])
+    assert par.get_int("N") == 32
+    assert par.get_floats("initial_amplitudes", 2) == [5.6964e18, 0.0]
+    assert math.isclose(par.get_float("kIR"), 0.7)
+
+
+def test_couplings_manager_golden():
+    # Golden values of the reference's only numeric test, tests/CosmoInterface/couplingsmanager.cpp:18-64:
+    # CouplingsManager<2, 4, true, false, true, false, true, true, true, false>
+    cm = CouplingsManager([[True, False, True, False], [True, True, True, False]])
+    assert cm.couples(0, 0) and not cm.couples(0, 1) and cm.couples(0, 2) and not cm.couples(0, 3)
+    assert cm.couples(1, 0) and cm.couples(1, 1) and cm.couples(1, 2) and not cm.couples(1, 3)
+    assert cm.how_many_couples() == 5
+    cm.set_effective_charges([1, 2, 3, 4, 5], [1, 2, 3, 4])
+    assert cm(0, 0) == 1
+    assert cm(0, 2) == 6
+    assert cm(1, 0) == 3
+    assert cm(1, 1) == 8
+    assert cm(1, 2) == 15
+    assert cm(0, 1) == 0 and cm(1, 3) == 0
+    assert cm.coupling(0) == 1 and cm.coupling(3) == 4
+    with pytest.raises(CouplingsManager.NotEnoughCharges):
+        cm.set_effective_charges([1, 1, 2, 3, 4, 5], [1, 2, 3, 4])
+    with pytest.raises(CouplingsManager.NotEnoughCouplings):
+        cm.set_effective_charges([1, 2, 3, 4, 5], [1, 3, 4])
