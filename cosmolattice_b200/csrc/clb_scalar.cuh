@@ -323,7 +323,7 @@ __device__ __forceinline__ double sf_kernel(const DevState &s, const SFParams &p
   return __dmul_rn(__dmul_rn(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
 }
 
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_tail(const double *__restrict__ partials, TailOp op, DevState *__restrict__ st, SFParams p)
 {
   __shared__ double smem[(256 / 32) * kRedSlots];
