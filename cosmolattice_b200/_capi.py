@@ -172,4 +172,5 @@ EXPORTED = [
     "clb_kernel_stats",
     "clb_last_evolve_ms",
     "clb_cuda_stream",
+    "clb_scalar_averages_noalloc",
 ]

@@ -11,8 +11,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libclb200.so")
 
-SOURCES = ["clb_api.cu"]
-DEPS = ["clb_api.cu", "clb_internal.cuh", "clb_scalar.cuh"]
+SOURCES = ["clb_api.cu", "clb_noalloc.cu"]
+DEPS = ["clb_api.cu", "clb_noalloc.cu", "clb_internal.cuh", "clb_scalar.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -51,6 +51,11 @@ constexpr int kElemBlocks = 148 * 8; // elementwise grid: 8 resident 256-thread 
 
 } // namespace
 
+namespace clb {
+// Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
+__attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
+} // namespace clb
+
 struct clb_handle {
   clb_config cfg;
   clb_model_desc md;

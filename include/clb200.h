@@ -179,6 +179,23 @@ int clb_last_evolve_ms(clb_handle *h, double *ms);
 /* The cudaStream_t the handle launches on (for callers that order their own work after it). */
 void *clb_cuda_stream(clb_handle *h);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
+ * For callers that cannot call cudaMalloc: a runtime that owns the whole device memory pool, code
+ * issued while a CUDA graph is being captured, or an embedding that forbids allocation after
+ * start-up.  Computes, for FP64 scalar-singlet lattices already in device memory, the volume
+ * averages d_out[0] = <sum_f pi_f^2>, d_out[1] = <sum_f grad^2 phi_f>, d_out[2] = <V> (lphi4:
+ * V = c0/4 phi^4 + q/2 phi^2 chi^2), the same sums clb_initialize and clb_measure form.
+ * d_fields / d_momenta: n_scalars x N^3 doubles each (layout of clb_set_state) on the current
+ * device; d_out: 3 doubles on the same device; stream: a cudaStream_t or NULL.
+ * Allocates nothing: the block partials live in a fixed 192 KiB device array that every GPU
+ * loading the library keeps until exit, so N is limited to 1024 (larger N returns CLB_EINVAL with
+ * the reason in clb_last_error(NULL)).  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) with the device current; make that first call before any stream capture.
+ * Calls return once their work is enqueued.  All calls share the array: calls that overlap on the
+ * GPU (other streams or host threads) race and must be serialised by the caller. */
+int clb_scalar_averages_noalloc(const double *d_fields, const double *d_momenta, int32_t N, int32_t n_scalars,
+                                double dx, double c0, double q, double *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
