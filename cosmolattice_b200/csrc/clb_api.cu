@@ -10,6 +10,9 @@
 #include "../../include/clb200.h"
 #include "clb_internal.cuh"
 #include "clb_scalar.cuh"
+#include "clb_sweep.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -46,8 +49,9 @@ std::vector<double> vv_coeffs(int ev)
   }
 }
 
-constexpr int kBZ = 32, kBY = 8;
 constexpr int kElemBlocks = 148 * 8; // elementwise grid: 8 resident 256-thread blocks per SM
+constexpr uint32_t kWaitTries = 1u << 24; // bound of each mbarrier wait in the sweeps
+constexpr size_t kStageMin = (size_t)1 << 23; // host-transfer staging: >= 64 MiB of doubles
 
 } // namespace
 
@@ -67,6 +71,11 @@ struct clb_handle {
   void *fld[2] = {nullptr, nullptr};
   void *pi[2] = {nullptr, nullptr};
   int cf = 0, cp = 0; // current field / momentum buffer
+  Pad pd{};           // padded component layout (clb_sweep.cuh)
+  CUtensorMap tm_f[2], tm_p[2];
+  int S = 3;          // sweep ring stages
+  size_t sweep_smem = 0;
+  int *d_err = nullptr; // set by a sweep whose bounded wait gave up
   DevState *d_st = nullptr;
   double *d_part = nullptr;
   double *d_sums = nullptr;
@@ -75,6 +84,7 @@ struct clb_handle {
   std::vector<double> ws;
   bool has_state = false, initialized = false, synced = true;
   ScalarArgs sa{};
+  SweepArgs sw{};
   SFParams sp{};
   dim3 sweep_grid;
   int sweep_blocks = 0;
@@ -120,12 +130,13 @@ namespace {
     if (e_ != cudaSuccess) return (h)->cuda_fail(e_, where);                                                           \
   } while (0)
 
-// z-marching geometry: BZ x BY columns per block, x split so the grid covers >= ~2 waves.
-void setup_geometry(clb_handle *h)
+// Sweep geometry: 64 x 8 (z, y) sites per block; the x direction is split so the grid holds about
+// two waves of resident blocks.
+void setup_geometry(clb_handle *h, int blocks_per_sm)
 {
   const int N = h->N;
-  const int gx = (N + kBZ - 1) / kBZ, gy = (N + kBY - 1) / kBY;
-  const int target = 148 * 8 * 2;
+  const int gx = (N + kTileZ - 1) / kTileZ, gy = (N + kTY - 1) / kTY;
+  const int target = 148 * std::max(1, blocks_per_sm) * 2;
   int xs = (target + gx * gy - 1) / (gx * gy);
   xs = std::max(1, std::min(xs, std::max(1, N / 4)));
   int LX = (N + xs - 1) / xs;
@@ -198,87 +209,158 @@ void collect_profile(clb_handle *h)
 }
 
 // ---- kernel launchers (templated on storage type and field count) ----------------------------
+template <class R, int NS, bool DRIFT, bool KICK, int RED> void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po,
+                                                                     double dtw, double h1, double h2)
+{
+  using TG = TileGeom<R>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_sweep<R, NS, DRIFT, KICK, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    attr_set = true;
+  }
+  (void)TG::SLOT;
+  SweepArgs a = h->sw;
+  a.dtw = dtw;
+  a.h1 = h1;
+  a.h2 = h2;
+  CLB_LAUNCH(h, kind,
+             k_sweep<R, NS, DRIFT, KICK, RED><<<h->sweep_grid, dim3(kTZ, kTY), h->sweep_smem, h->stream>>>(
+                 h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]), a, h->d_st,
+                 h->d_part, h->d_err));
+}
+
 template <class R, int NS> struct Launch {
   // kick in place: pi += h K(phi)
   static void kick(clb_handle *h, double hk)
   {
-    ScalarArgs a = h->sa;
-    a.h1 = hk;
-    a.h2 = 0.0;
-    CLB_LAUNCH(h, K_KICK,
-               k_scalar_sweep<R, NS, kBZ, kBY, false, true, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                   F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+    sweep<R, NS, false, true, 0>(h, K_KICK, h->cf, h->cp, h->cf, h->cp, 0.0, hk, 0.0);
   }
   // fused: drift (dtw) + kick (h1, h2) + averages, ping-pong buffers
   static void fused(clb_handle *h, double dtw, double h1, double h2, bool red)
   {
-    ScalarArgs a = h->sa;
-    a.dtw = dtw;
-    a.h1 = h1;
-    a.h2 = h2;
     const int nf = h->cf ^ 1, np = h->cp ^ 1;
     if (red)
-      CLB_LAUNCH(h, K_FUSED,
-                 k_scalar_sweep<R, NS, kBZ, kBY, true, true, 3><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, np), a, h->d_st, h->d_part));
+      sweep<R, NS, true, true, 3>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, h1, h2);
     else
-      CLB_LAUNCH(h, K_FUSED,
-                 k_scalar_sweep<R, NS, kBZ, kBY, true, true, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, np), a, h->d_st, h->d_part));
+      sweep<R, NS, true, true, 0>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, h1, h2);
     h->cf = nf;
     h->cp = np;
   }
   // drift (dtw) with optional field averages, writes the other field buffer
   static void drift_fields(clb_handle *h, double dtw, bool red)
   {
-    ScalarArgs a = h->sa;
-    a.dtw = dtw;
     const int nf = h->cf ^ 1;
     if (red)
-      CLB_LAUNCH(h, K_DRIFT_SWEEP,
-                 k_scalar_sweep<R, NS, kBZ, kBY, true, false, 2><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+      sweep<R, NS, true, false, 2>(h, K_DRIFT_SWEEP, h->cf, h->cp, nf, h->cp, dtw, 0.0, 0.0);
     else
-      CLB_LAUNCH(h, K_DRIFT_SWEEP,
-                 k_scalar_sweep<R, NS, kBZ, kBY, true, false, 0><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, nf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+      sweep<R, NS, true, false, 0>(h, K_DRIFT_SWEEP, h->cf, h->cp, nf, h->cp, dtw, 0.0, 0.0);
     h->cf = nf;
   }
-  // elementwise in-place drift (reference order)
+  // elementwise in-place drift over the whole padded arrays (ghosts stay periodic copies)
   static void drift(clb_handle *h, double dtw)
   {
     CLB_LAUNCH(h, K_DRIFT,
-               k_drift<R><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), (size_t)NS * h->n3,
-                                                               dtw, h->d_st));
+               k_drift<R><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp),
+                                                               (size_t)NS * (size_t)h->pd.comp, dtw, h->d_st));
   }
   // <pi^2> partials (elementwise grid)
   static int reduce_pi2(clb_handle *h)
   {
-    CLB_LAUNCH(h, K_RED_PI2, k_reduce_pi2<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(P<R>(h, h->cp), h->n3, h->d_part));
+    CLB_LAUNCH(h, K_RED_PI2, k_reduce_pi2_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(P<R>(h, h->cp), h->pd, h->d_part));
     return kElemBlocks;
   }
   // <grad^2>, <V> (and <pi^2> with all=true) partials (sweep grid)
   static int reduce_fields(clb_handle *h, bool all)
   {
-    ScalarArgs a = h->sa;
     if (all)
-      CLB_LAUNCH(h, K_RED_FIELDS,
-                 k_scalar_sweep<R, NS, kBZ, kBY, false, false, 3><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+      sweep<R, NS, false, false, 3>(h, K_RED_FIELDS, h->cf, h->cp, h->cf, h->cp, 0.0, 0.0, 0.0);
     else
-      CLB_LAUNCH(h, K_RED_FIELDS,
-                 k_scalar_sweep<R, NS, kBZ, kBY, false, false, 2><<<h->sweep_grid, dim3(kBZ, kBY), 0, h->stream>>>(
-                     F<R>(h, h->cf), P<R>(h, h->cp), F<R>(h, h->cf), P<R>(h, h->cp), a, h->d_st, h->d_part));
+      sweep<R, NS, false, false, 2>(h, K_RED_FIELDS, h->cf, h->cp, h->cf, h->cp, 0.0, 0.0, 0.0);
     return h->sweep_blocks;
   }
   static void measure(clb_handle *h, double am)
   {
     CLB_LAUNCH(h, K_MEASURE,
-               k_measure<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->sa, am,
-                                                                    h->d_part));
+               k_measure_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->pd,
+                                                                        h->sa.inv_dx2, h->sa.c0_quarter,
+                                                                        h->sa.q_half, am, h->d_part));
     CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeasSlots><<<1, 256, 0, h->stream>>>(h->d_part, kElemBlocks, h->d_sums));
   }
 };
+
+// Host arrays (plane after plane, N x N each) <-> padded device components, through the staging
+// buffer in whole planes, with FP32 conversion on the GPU and the periodic ghosts filled after upload.
+cudaError_t upload(clb_handle *h, const double *src, void *dst)
+{
+  const long long planes = (long long)h->NS * h->N, per = (long long)h->N * h->N;
+  const long long chunk = std::max<long long>(1, (long long)h->stage_n / per);
+  for (long long p0 = 0; p0 < planes; p0 += chunk) {
+    const long long np = std::min(chunk, planes - p0);
+    cudaError_t r = cudaMemcpyAsync(h->d_stage, src + p0 * per, (size_t)(np * per) * sizeof(double),
+                                    cudaMemcpyHostToDevice, h->stream);
+    if (r != cudaSuccess) return r;
+    if (h->fp32)
+      CLB_LAUNCH(h, K_CONVERT, k_scatter<double, float><<<kElemBlocks, 256, 0, h->stream>>>(
+                                   h->d_stage, static_cast<float *>(dst), h->pd, p0, np));
+    else
+      CLB_LAUNCH(h, K_CONVERT, k_scatter<double, double><<<kElemBlocks, 256, 0, h->stream>>>(
+                                   h->d_stage, static_cast<double *>(dst), h->pd, p0, np));
+  }
+  if (h->fp32)
+    CLB_LAUNCH(h, K_CONVERT, k_fill_ghosts<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<float *>(dst), h->pd, h->NS));
+  else
+    CLB_LAUNCH(h, K_CONVERT, k_fill_ghosts<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<double *>(dst), h->pd, h->NS));
+  return cudaGetLastError();
+}
+
+cudaError_t download(clb_handle *h, const void *src, double *dst)
+{
+  const long long planes = (long long)h->NS * h->N, per = (long long)h->N * h->N;
+  const long long chunk = std::max<long long>(1, (long long)h->stage_n / per);
+  for (long long p0 = 0; p0 < planes; p0 += chunk) {
+    const long long np = std::min(chunk, planes - p0);
+    if (h->fp32)
+      CLB_LAUNCH(h, K_CONVERT, k_gather<float, double><<<kElemBlocks, 256, 0, h->stream>>>(
+                                   static_cast<const float *>(src), h->d_stage, h->pd, p0, np));
+    else
+      CLB_LAUNCH(h, K_CONVERT, k_gather<double, double><<<kElemBlocks, 256, 0, h->stream>>>(
+                                   static_cast<const double *>(src), h->d_stage, h->pd, p0, np));
+    cudaError_t r = cudaMemcpyAsync(dst + p0 * per, h->d_stage, (size_t)(np * per) * sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->stream);
+    if (r != cudaSuccess) return r;
+  }
+  return cudaStreamSynchronize(h->stream);
+}
+
+// 3-D tensor map over the stacked padded components: dims {Zp, Yp, NS N}, box = one plane tile.
+bool encode_map(clb_handle *h, void *base, CUtensorMap *map, std::string &why)
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      why = "cuTensorMapEncodeTiled not available from the driver";
+      return false;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const Pad &pd = h->pd;
+  const cuuint64_t dims[3] = {(cuuint64_t)pd.Zp, (cuuint64_t)pd.Yp, (cuuint64_t)h->NS * (cuuint64_t)pd.N};
+  const cuuint64_t strides[2] = {(cuuint64_t)pd.Zp * h->esz, (cuuint64_t)pd.plane * h->esz};
+  const cuuint32_t boxz = h->fp32 ? (cuuint32_t)TileGeom<float>::BOXZ : (cuuint32_t)TileGeom<double>::BOXZ;
+  const cuuint32_t box[3] = {boxz, (cuuint32_t)(kTY + 2), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(map, h->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims,
+                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    why = "cuTensorMapEncodeTiled returned " + std::to_string((int)r);
+    return false;
+  }
+  return true;
+}
 
 void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1)
 {
@@ -419,6 +501,10 @@ int sync_and_check(clb_handle *h, const char *where)
   DevState s;
   e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return h->cuda_fail(e, where);
+  int terr = 0;
+  e = cudaMemcpy(&terr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  if (terr != 0) return h->fail(CLB_ETIMEOUT, std::string(where) + ": a sweep's bounded wait for its tile loads gave up");
   if (s.status != 0) return h->fail(CLB_ENONFINITE, std::string(where) + ": a volume average or a(t) is not finite");
   return CLB_OK;
 }
@@ -492,7 +578,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   h->fp32 = cfg->precision == CLB_PREC_FP32_SPLIT;
   h->esz = h->fp32 ? sizeof(float) : sizeof(double);
   h->ws = ws;
-  setup_geometry(h);
+  h->pd = make_pad(h->N, (int)h->esz);
   ScalarArgs &a = h->sa;
   a.N = h->N;
   a.inv_dx2 = 1.0 / (cfg->dx * cfg->dx);
@@ -500,10 +586,27 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   a.q = md->couplings[1];
   a.c0_quarter = 0.25 * md->couplings[0];
   a.q_half = 0.5 * md->couplings[1];
+  // ring depth: as many plane stages as fit in ~48 KiB, at least 3 (planes x, x+1 and one in flight)
+  const size_t slot = h->fp32 ? (size_t)TileGeom<float>::SLOT : (size_t)TileGeom<double>::SLOT;
+  const size_t stage_bytes = (size_t)h->NS * 2 * slot;
+  h->S = (int)std::max<size_t>(3, std::min<size_t>(8, (48 * 1024) / stage_bytes));
+  h->sweep_smem = (size_t)h->S * stage_bytes + (size_t)h->S * sizeof(uint64_t) + 8 * kRedSlots * sizeof(double);
+  const int bpsm = (int)std::max<size_t>(1, std::min<size_t>(8, (220 * 1024) / (h->sweep_smem + 1024)));
+  setup_geometry(h, bpsm);
+  SweepArgs &w = h->sw;
+  w.pd = h->pd;
+  w.LX = a.LX;
+  w.S = h->S;
+  w.tries = kWaitTries;
+  w.inv_dx2 = a.inv_dx2;
+  w.c0 = a.c0;
+  w.q = a.q;
+  w.c0_quarter = a.c0_quarter;
+  w.q_half = a.q_half;
   const double fm = md->fStar / md->MPl;
   h->sp = SFParams{md->alpha, fm * fm, cfg->dt, 1.0 / (double)h->n3};
   h->part_rows = (size_t)std::max(h->sweep_blocks, kElemBlocks);
-  const size_t bytes = (size_t)h->NS * h->n3 * h->esz;
+  const size_t bytes = (size_t)h->NS * (size_t)h->pd.comp * h->esz;
   const size_t nbuf = cfg->path == CLB_PATH_FUSED ? 2 : 1;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   for (size_t b = 0; ok && b < nbuf; ++b) {
@@ -513,15 +616,28 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   ok = ok && cudaMalloc(&h->d_st, sizeof(DevState)) == cudaSuccess;
   ok = ok && cudaMalloc(&h->d_part, h->part_rows * kMeasSlots * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&h->d_sums, kMeasSlots * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess && cudaMemset(h->d_err, 0, sizeof(int)) == cudaSuccess;
   ok = ok && cudaEventCreate(&h->ev_call[0]) == cudaSuccess && cudaEventCreate(&h->ev_call[1]) == cudaSuccess;
-  if (ok && h->fp32) {
-    h->stage_n = std::min<size_t>((size_t)h->NS * h->n3, (size_t)1 << 23); // <= 64 MiB of doubles
+  if (ok) {
+    h->stage_n = std::max<size_t>(kStageMin, (size_t)h->N * h->N);
     ok = cudaMalloc(&h->d_stage, h->stage_n * sizeof(double)) == cudaSuccess;
   }
   if (!ok) {
     g_err = std::string("clb_create: device allocation failed: ") + cudaGetErrorString(cudaGetLastError());
     clb_destroy(h);
     return CLB_ENOMEM;
+  }
+  for (size_t b = 0; b < nbuf; ++b) {
+    std::string why;
+    if (!encode_map(h, h->fld[b], &h->tm_f[b], why) || !encode_map(h, h->pi[b], &h->tm_p[b], why)) {
+      g_err = "clb_create: tensor map: " + why;
+      clb_destroy(h);
+      return CLB_ECUDA;
+    }
+  }
+  if (nbuf == 1) {
+    h->tm_f[1] = h->tm_f[0];
+    h->tm_p[1] = h->tm_p[0];
   }
   DevState s{};
   s.aI = s.aSI = s.aIM = 1.0;
@@ -542,6 +658,7 @@ void clb_destroy(clb_handle *h)
   if (h->d_st) cudaFree(h->d_st);
   if (h->d_part) cudaFree(h->d_part);
   if (h->d_sums) cudaFree(h->d_sums);
+  if (h->d_err) cudaFree(h->d_err);
   if (h->d_hist) cudaFree(h->d_hist);
   if (h->d_stage) cudaFree(h->d_stage);
   for (auto &p : h->pend) {
@@ -566,29 +683,12 @@ int clb_num_components(const clb_handle *h, int32_t *nf, int32_t *np)
 int clb_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
 {
   if (!h || !fields || !momenta) return h ? h->fail(CLB_EINVAL, "clb_set_state: null argument") : CLB_EINVAL;
-  const size_t n = (size_t)h->NS * h->n3;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->cf = h->cp = 0;
-  if (h->fp32) {
-    // FP64 host arrays through a device staging buffer, converted on the GPU
-    auto up = [&](const double *src, float *dst) -> cudaError_t {
-      for (size_t off = 0; off < n; off += h->stage_n) {
-        const size_t c = std::min(h->stage_n, n - off);
-        cudaError_t r = cudaMemcpyAsync(h->d_stage, src + off, c * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-        if (r != cudaSuccess) return r;
-        CLB_LAUNCH(h, K_CONVERT, k_convert<double, float><<<kElemBlocks, 256, 0, h->stream>>>(h->d_stage, dst + off, c));
-      }
-      return cudaGetLastError();
-    };
-    e = up(fields, static_cast<float *>(h->fld[0]));
-    if (e == cudaSuccess) e = up(momenta, static_cast<float *>(h->pi[0]));
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  } else {
-    e = cudaMemcpyAsync(h->fld[0], fields, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h->pi[0], momenta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  }
+  e = upload(h, fields, h->fld[0]);
+  if (e == cudaSuccess) e = upload(h, momenta, h->pi[0]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   DevState s{};
   s.aI = s.aSI = s.aIM = 1.0;
@@ -617,22 +717,7 @@ int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefacto
   if (!h) return CLB_EINVAL;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
-  const size_t n = (size_t)h->NS * h->n3;
-  auto fetch = [&](void *src, double *dst) -> cudaError_t {
-    if (!dst) return cudaSuccess;
-    if (h->fp32) {
-      const float *fs = static_cast<const float *>(src);
-      for (size_t off = 0; off < n; off += h->stage_n) {
-        const size_t c = std::min(h->stage_n, n - off);
-        CLB_LAUNCH(h, K_CONVERT, k_convert<float, double><<<kElemBlocks, 256, 0, h->stream>>>(fs + off, h->d_stage, c));
-        cudaError_t r = cudaMemcpyAsync(dst + off, h->d_stage, c * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-        if (r != cudaSuccess) return r;
-      }
-      return cudaStreamSynchronize(h->stream);
-    }
-    cudaError_t r = cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    return r == cudaSuccess ? cudaStreamSynchronize(h->stream) : r;
-  };
+  auto fetch = [&](void *src, double *dst) -> cudaError_t { return dst ? download(h, src, dst) : cudaSuccess; };
   e = fetch(h->fld[h->cf], fields);
   if (e == cudaSuccess) e = fetch(h->pi[h->cp], momenta);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
