@@ -129,6 +129,8 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_kernel_stats": (C.c_int, [H, C.POINTER(KernelStat), C.c_int32, C.POINTER(C.c_int32)]),
             "clb_last_evolve_ms": (C.c_int, [H, dp]),
             "clb_cuda_stream": (C.c_void_p, [H]),
+            "clb_spectrum": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                       C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
         }
         for name, (res, args) in more.items():
             fn = getattr(lib, name)
@@ -166,6 +168,7 @@ EXPORTED = [
     "clb_evolve",
     "clb_sync",
     "clb_measure",
+    "clb_spectrum",
     "clb_history",
     "clb_set_profiling",
     "clb_reset_stats",

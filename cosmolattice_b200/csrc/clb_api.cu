@@ -10,12 +10,15 @@
 #include "../../include/clb200.h"
 #include "clb_internal.cuh"
 #include "clb_scalar.cuh"
+#include "clb_spectrum.cuh"
 #include "clb_sweep.cuh"
 
 #include <cudaTypedefs.h>
+#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -52,6 +55,9 @@ std::vector<double> vv_coeffs(int ev)
 constexpr int kElemBlocks = 148 * 8; // elementwise grid: 8 resident 256-thread blocks per SM
 constexpr uint32_t kWaitTries = 1u << 24; // bound of each mbarrier wait in the sweeps
 constexpr size_t kStageMin = (size_t)1 << 23; // host-transfer staging: >= 64 MiB of doubles
+constexpr int kDefaultShapeFP64 = 0;          // ShapeW
+constexpr int kDefaultShapeFP32 = 2;          // ShapeH
+constexpr int kPlanesPerBlock = 32;           // x-run length of one sweep block
 
 } // namespace
 
@@ -74,6 +80,8 @@ struct clb_handle {
   Pad pd{};           // padded component layout (clb_sweep.cuh)
   CUtensorMap tm_f[2], tm_p[2];
   int S = 3;          // sweep ring stages
+  int shape = 0;      // sweep block shape: 0 ShapeW, 1 ShapeQ, 2 ShapeH (clb_sweep.cuh)
+  int bz = 64, by = 8; // sites per block tile in z and y
   size_t sweep_smem = 0;
   int *d_err = nullptr; // set by a sweep whose bounded wait gave up
   DevState *d_st = nullptr;
@@ -109,6 +117,15 @@ struct clb_handle {
   // staging buffer for FP32 <-> FP64 host transfers
   double *d_stage = nullptr;
   size_t stage_n = 0;
+  // spectra: in-place D2Z buffer, cuFFT plan and binning scratch (allocated on first use)
+  double *d_spec = nullptr;
+  bool plan_ok = false;
+  cufftHandle plan = 0;
+  double *d_spec_part = nullptr;
+  unsigned long long *d_spec_cnt = nullptr;
+  double *d_spec_out = nullptr;
+  unsigned long long *d_spec_outc = nullptr;
+  int spec_nbins_cap = 0;
 
   int fail(int code, const std::string &m)
   {
@@ -130,15 +147,18 @@ namespace {
     if (e_ != cudaSuccess) return (h)->cuda_fail(e_, where);                                                           \
   } while (0)
 
-// Sweep geometry: 64 x 8 (z, y) sites per block; the x direction is split so the grid holds about
+// Sweep geometry: bz x by (z, y) sites per block; the x direction is split so the grid holds about
 // two waves of resident blocks.
 void setup_geometry(clb_handle *h, int blocks_per_sm)
 {
   const int N = h->N;
-  const int gx = (N + kTileZ - 1) / kTileZ, gy = (N + kTY - 1) / kTY;
-  const int target = 148 * std::max(1, blocks_per_sm) * 2;
-  int xs = (target + gx * gy - 1) / (gx * gy);
+  const int gx = (N + h->bz - 1) / h->bz, gy = (N + h->by - 1) / h->by;
+  // Many short x-runs (about 32 planes) beat few long ones: a block's plane rate is bounded by its
+  // own pipeline, so throughput comes from many blocks cycling through the SMs.
+  (void)blocks_per_sm;
+  int xs = std::max(1, (N + kPlanesPerBlock - 1) / kPlanesPerBlock);
   xs = std::max(1, std::min(xs, std::max(1, N / 4)));
+  if (const char *env = std::getenv("CLB_SWEEP_XS")) xs = std::max(1, std::min(N, std::atoi(env)));
   int LX = (N + xs - 1) / xs;
   xs = (N + LX - 1) / LX;
   h->sa.LX = LX;
@@ -149,10 +169,11 @@ void setup_geometry(clb_handle *h, int blocks_per_sm)
 template <class R> R *F(clb_handle *h, int b) { return static_cast<R *>(h->fld[b]); }
 template <class R> R *P(clb_handle *h, int b) { return static_cast<R *>(h->pi[b]); }
 
-enum KKind { K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_NKINDS };
+enum KKind { K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_SPECTRUM, K_NKINDS };
 const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
                                           "scalar_drift",       "reduce_pi2",        "reduce_fields",
-                                          "tail",               "measure",           "convert"};
+                                          "tail",               "measure",           "convert",
+                                          "spectrum"};
 
 cudaEvent_t take_event(clb_handle *h)
 {
@@ -209,24 +230,33 @@ void collect_profile(clb_handle *h)
 }
 
 // ---- kernel launchers (templated on storage type and field count) ----------------------------
-template <class R, int NS, bool DRIFT, bool KICK, int RED> void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po,
-                                                                     double dtw, double h1, double h2)
+template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
+void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2)
 {
-  using TG = TileGeom<R>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_sweep<R, NS, DRIFT, KICK, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_sweep<R, NS, SH, DRIFT, KICK, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         160 * 1024);
     attr_set = true;
   }
-  (void)TG::SLOT;
   SweepArgs a = h->sw;
   a.dtw = dtw;
   a.h1 = h1;
   a.h2 = h2;
   CLB_LAUNCH(h, kind,
-             k_sweep<R, NS, DRIFT, KICK, RED><<<h->sweep_grid, dim3(kTZ, kTY), h->sweep_smem, h->stream>>>(
+             k_sweep<R, NS, SH, DRIFT, KICK, RED><<<h->sweep_grid, dim3(SH::TZ, SH::TY), h->sweep_smem, h->stream>>>(
                  h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]), a, h->d_st,
                  h->d_part, h->d_err));
+}
+
+template <class R, int NS, bool DRIFT, bool KICK, int RED>
+void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2)
+{
+  if constexpr (NS == 1) {
+    if (h->shape == 1) return sweep_sh<R, NS, ShapeQ, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
+    if (h->shape == 2) return sweep_sh<R, NS, ShapeH, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
+  }
+  sweep_sh<R, NS, ShapeW, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
 }
 
 template <class R, int NS> struct Launch {
@@ -349,8 +379,8 @@ bool encode_map(clb_handle *h, void *base, CUtensorMap *map, std::string &why)
   const Pad &pd = h->pd;
   const cuuint64_t dims[3] = {(cuuint64_t)pd.Zp, (cuuint64_t)pd.Yp, (cuuint64_t)h->NS * (cuuint64_t)pd.N};
   const cuuint64_t strides[2] = {(cuuint64_t)pd.Zp * h->esz, (cuuint64_t)pd.plane * h->esz};
-  const cuuint32_t boxz = h->fp32 ? (cuuint32_t)TileGeom<float>::BOXZ : (cuuint32_t)TileGeom<double>::BOXZ;
-  const cuuint32_t box[3] = {boxz, (cuuint32_t)(kTY + 2), 1};
+  const cuuint32_t boxz = (cuuint32_t)(h->bz + 2 * (16 / (int)h->esz));
+  const cuuint32_t box[3] = {boxz, (cuuint32_t)(h->by + 2), 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode(map, h->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims,
                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -587,9 +617,20 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   a.c0_quarter = 0.25 * md->couplings[0];
   a.q_half = 0.5 * md->couplings[1];
   // ring depth: as many plane stages as fit in ~48 KiB, at least 3 (planes x, x+1 and one in flight)
-  const size_t slot = h->fp32 ? (size_t)TileGeom<float>::SLOT : (size_t)TileGeom<double>::SLOT;
+  // sweep shape: default per storage type and field count, CLB_SWEEP_SHAPE=0/1/2 overrides (one field)
+  h->shape = (h->NS == 1) ? (h->fp32 ? kDefaultShapeFP32 : kDefaultShapeFP64) : 0;
+  if (const char *env = std::getenv("CLB_SWEEP_SHAPE")) {
+    const int v = std::atoi(env);
+    if (h->NS == 1 && v >= 0 && v <= 2) h->shape = v;
+  }
+  h->bz = 64;
+  h->by = h->shape == 1 ? 16 : 8;
+  const size_t box_bytes = (size_t)(h->bz + 2 * (16 / (int)h->esz)) * (size_t)(h->by + 2) * h->esz;
+  const size_t slot = ((box_bytes + 127) / 128) * 128;
   const size_t stage_bytes = (size_t)h->NS * 2 * slot;
-  h->S = (int)std::max<size_t>(3, std::min<size_t>(8, (48 * 1024) / stage_bytes));
+  size_t ring_budget = 32 * 1024;
+  if (const char *env = std::getenv("CLB_SWEEP_RING_KB")) ring_budget = (size_t)std::max(8, std::atoi(env)) * 1024;
+  h->S = (int)std::max<size_t>(3, std::min<size_t>(8, ring_budget / stage_bytes));
   h->sweep_smem = (size_t)h->S * stage_bytes + (size_t)h->S * sizeof(uint64_t) + 8 * kRedSlots * sizeof(double);
   const int bpsm = (int)std::max<size_t>(1, std::min<size_t>(8, (220 * 1024) / (h->sweep_smem + 1024)));
   setup_geometry(h, bpsm);
@@ -661,6 +702,12 @@ void clb_destroy(clb_handle *h)
   if (h->d_err) cudaFree(h->d_err);
   if (h->d_hist) cudaFree(h->d_hist);
   if (h->d_stage) cudaFree(h->d_stage);
+  if (h->plan_ok) cufftDestroy(h->plan);
+  if (h->d_spec) cudaFree(h->d_spec);
+  if (h->d_spec_part) cudaFree(h->d_spec_part);
+  if (h->d_spec_cnt) cudaFree(h->d_spec_cnt);
+  if (h->d_spec_out) cudaFree(h->d_spec_out);
+  if (h->d_spec_outc) cudaFree(h->d_spec_outc);
   for (auto &p : h->pend) {
     h->ev_pool.push_back(p.a);
     h->ev_pool.push_back(p.b);
@@ -923,6 +970,110 @@ int clb_measure(clb_handle *h, double e0, clb_measurement *m)
   m->aI = s.aI;
   m->aDotI = s.aDotI;
   m->hubble = s.aDotI / s.aI;
+  return CLB_OK;
+}
+
+constexpr int kSpecBlocks = 148 * 2;
+
+int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                 int32_t nbins, int32_t fold, double *k_out, double *value_out, int64_t *count_out)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_spectrum: call clb_initialize first");
+  if (which < 0 || which > 1 || comp < 0 || comp >= h->NS)
+    return h->fail(CLB_EINVAL, "clb_spectrum: which must be 0 (field) or 1 (momentum) and comp a scalar index");
+  if (ps_type < 1 || ps_type > 2) return h->fail(CLB_EINVAL, "powerSpectrumType " + std::to_string(ps_type) + " is not a valid powerSpectrumType.");
+  if (ps_version < 1 || ps_version > 2)
+    return h->fail(CLB_EINVAL, "clb_spectrum: PS_version 1 (bin mean |k|) and 2 (bin centre) are supported");
+  if (!(dk > 0) || nbins < 1) return h->fail(CLB_EINVAL, "clb_spectrum: dk must be positive and nbins >= 1");
+  if (!value_out) return h->fail(CLB_EINVAL, "clb_spectrum: null output");
+  const int N = h->N;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+  const size_t spec_n = (size_t)N * N * 2 * (N / 2 + 1);
+  if (!h->d_spec) {
+    if ((e = cudaMalloc(&h->d_spec, spec_n * sizeof(double))) != cudaSuccess)
+      return h->fail(CLB_ENOMEM, std::string("clb_spectrum: ") + cudaGetErrorString(e));
+  }
+  if (!h->plan_ok) {
+    if (cufftPlan3d(&h->plan, N, N, N, CUFFT_D2Z) != CUFFT_SUCCESS) return h->fail(CLB_ECUDA, "clb_spectrum: cufftPlan3d failed");
+    h->plan_ok = true;
+    if (cufftSetStream(h->plan, h->stream) != CUFFT_SUCCESS) return h->fail(CLB_ECUDA, "clb_spectrum: cufftSetStream failed");
+  }
+  if (nbins > h->spec_nbins_cap) {
+    if (h->d_spec_part) cudaFree(h->d_spec_part);
+    if (h->d_spec_cnt) cudaFree(h->d_spec_cnt);
+    if (h->d_spec_out) cudaFree(h->d_spec_out);
+    if (h->d_spec_outc) cudaFree(h->d_spec_outc);
+    h->d_spec_part = nullptr;
+    h->d_spec_cnt = nullptr;
+    h->d_spec_out = nullptr;
+    h->d_spec_outc = nullptr;
+    bool ok = cudaMalloc(&h->d_spec_part, (size_t)kSpecBlocks * nbins * 2 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&h->d_spec_cnt, (size_t)kSpecBlocks * nbins * sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMalloc(&h->d_spec_out, (size_t)nbins * 2 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&h->d_spec_outc, (size_t)nbins * sizeof(unsigned long long)) == cudaSuccess;
+    if (!ok) {
+      h->spec_nbins_cap = 0;
+      return h->fail(CLB_ENOMEM, "clb_spectrum: scratch allocation failed");
+    }
+    h->spec_nbins_cap = nbins;
+  }
+  void *src = which == 0 ? h->fld[h->cf] : h->pi[h->cp];
+  const size_t comp_off = (size_t)comp * (size_t)h->pd.comp;
+  if (h->fp32)
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + comp_off, h->d_spec, h->pd));
+  else
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(src) + comp_off, h->d_spec, h->pd));
+  if (cufftExecD2Z(h->plan, h->d_spec, reinterpret_cast<cufftDoubleComplex *>(h->d_spec)) != CUFFT_SUCCESS)
+    return h->fail(CLB_ECUDA, "clb_spectrum: cufftExecD2Z failed");
+  const size_t smem = (size_t)nbins * (2 * sizeof(double) + sizeof(unsigned long long));
+  static size_t smem_attr = 0;
+  if (smem > 48 * 1024 && smem > smem_attr) {
+    if ((e = cudaFuncSetAttribute(k_spec_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+      return h->fail(CLB_EINVAL, "clb_spectrum: too many bins for shared memory");
+    smem_attr = smem;
+  }
+  CLB_LAUNCH(h, K_SPECTRUM,
+             k_spec_bin<<<kSpecBlocks, 256, smem, h->stream>>>(reinterpret_cast<const double2 *>(h->d_spec), N, dk, nbins,
+                                                                 fold, h->d_spec_part, h->d_spec_cnt));
+  CLB_LAUNCH(h, K_SPECTRUM,
+             k_spec_sum<<<(nbins + 255) / 256, 256, 0, h->stream>>>(h->d_spec_part, h->d_spec_cnt, kSpecBlocks, nbins,
+                                                                    h->d_spec_out, h->d_spec_out + nbins, h->d_spec_outc));
+  std::vector<double> sums(2 * (size_t)nbins);
+  std::vector<unsigned long long> cnt(nbins);
+  e = cudaMemcpyAsync(sums.data(), h->d_spec_out, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(cnt.data(), h->d_spec_outc, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+  collect_profile(h);
+  DevState s;
+  if ((e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+  // PowerSpectrumMeasurer::powerSpectrum normalisation (powerspectrum.h:95-106)
+  const double pi = 3.14159265358979323846;
+  const double dx = h->cfg.dx;
+  const double kIR = 2 * pi / (N * dx);
+  double N5 = 1;
+  for (int i = 0; i < 5; ++i) N5 *= (double)N;
+  const double mom_factor = which == 1 ? std::pow(s.aI, 2 * h->md.alpha - 6) : 1.0; // scalarsingletmeasurer.h:80
+  for (int b = 0; b < nbins; ++b) {
+    const double sum = sums[b], nsum = sums[nbins + b];
+    const unsigned long long c = cnt[b];
+    const double ntil = (ps_version == 1 && c > 0) ? nsum / (double)c : (b + 0.5) * dk;
+    double v = 0;
+    if (c > 0) {
+      if (ps_type == 1) {
+        v = kIR * ntil * dx / dk / N5 / 2.0 / pi * sum;
+      } else {
+        const double t = kIR * ntil * dx / N;
+        v = t * t * t / dk / 2.0 / (pi * pi) * (sum / (double)c);
+      }
+    }
+    value_out[b] = mom_factor * v;
+    if (k_out) k_out[b] = ntil * kIR;
+    if (count_out) count_out[b] = (int64_t)c;
+  }
   return CLB_OK;
 }
 

@@ -44,14 +44,20 @@ inline Pad make_pad(int N, int esz)
   return p;
 }
 
-constexpr int kTZ = 32, kTY = 8, kVZ = 2;
-constexpr int kTileZ = kTZ * kVZ; // 64 z sites per block
-constexpr int kSweepThreads = kTZ * kTY;
+// Block shape: TZ x TY threads, each owning VZ consecutive z sites of one row, so a block covers a
+// (TZ VZ) x TY tile of (z, y) sites per plane.
+template <int TZ_, int TY_, int VZ_> struct Shape {
+  static constexpr int TZ = TZ_, TY = TY_, VZ = VZ_;
+  static constexpr int BZ = TZ * VZ, BY = TY, THREADS = TZ * TY;
+};
+using ShapeW = Shape<32, 8, 2>;  // 64 x 8 sites, 2 per thread
+using ShapeQ = Shape<16, 16, 4>; // 64 x 16 sites, 4 per thread
+using ShapeH = Shape<16, 8, 4>;  // 64 x 8 sites, 4 per thread, 128 threads
 
-template <class R> struct TileGeom {
+template <class R, class SH> struct TileGeom {
   static constexpr int G = 16 / (int)sizeof(R);
-  static constexpr int BOXZ = kTileZ + 2 * G; // 68 (FP64) / 72 (FP32): 16-byte multiple
-  static constexpr int BOXY = kTY + 2;
+  static constexpr int BOXZ = SH::BZ + 2 * G; // a 16-byte multiple
+  static constexpr int BOXY = SH::BY + 2;
   static constexpr int BYTES = BOXZ * BOXY * (int)sizeof(R);
   static constexpr int SLOT = ((BYTES + 127) / 128) * 128; // TMA smem destinations 128-byte aligned
 };
@@ -65,43 +71,86 @@ struct SweepArgs {
   double dtw, h1, h2;
 };
 
-template <class R> struct Vec2;
-template <> struct Vec2<double> { using T = double2; };
-template <> struct Vec2<float> { using T = float2; };
+// VZ consecutive values from 16-byte-aligned shared memory.
+template <class R, int VZ> __device__ __forceinline__ void ldv(const R *p, R (&v)[VZ])
+{
+  if constexpr (sizeof(R) == 8) {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 2) {
+      const double2 t = *reinterpret_cast<const double2 *>(p + k);
+      v[k] = t.x;
+      v[k + 1] = t.y;
+    }
+  } else if constexpr (VZ == 4) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 2) {
+      const float2 t = *reinterpret_cast<const float2 *>(p + k);
+      v[k] = t.x;
+      v[k + 1] = t.y;
+    }
+  }
+}
 
-template <class R, int NS> constexpr int sweep_boxes(bool loadp) { return NS * (loadp ? 2 : 1); }
+// VZ consecutive values to global memory at an address aligned to VZ elements (or 16 bytes).
+template <class R, int VZ> __device__ __forceinline__ void stv(R *p, const R (&v)[VZ])
+{
+  if constexpr (sizeof(R) == 8) {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 2) *reinterpret_cast<double2 *>(p + k) = double2{v[k], v[k + 1]};
+  } else if constexpr (VZ == 4) {
+    *reinterpret_cast<float4 *>(p) = float4{v[0], v[1], v[2], v[3]};
+  } else {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 2) *reinterpret_cast<float2 *>(p + k) = float2{v[k], v[k + 1]};
+  }
+}
 
 // DRIFT / KICK / RED as in k_scalar_sweep (clb_scalar.cuh); fout/pout are padded arrays.
-template <class R, int NS, bool DRIFT, bool KICK, int RED>
-__global__ void __launch_bounds__(kSweepThreads)
+template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
+__global__ void __launch_bounds__(SH::THREADS)
     k_sweep(const __grid_constant__ CUtensorMap tmf, const __grid_constant__ CUtensorMap tmp, R *fout, R *pout,
             SweepArgs a, const DevState *__restrict__ st, double *__restrict__ partials, int *__restrict__ err)
 {
   using A = Ar<R>;
   using Pot = Lphi4<R, NS>;
-  using TG = TileGeom<R>;
-  using V2 = typename Vec2<R>::T;
+  using TG = TileGeom<R, SH>;
+  constexpr int VZ = SH::VZ;
   constexpr bool LOADP = DRIFT || KICK || (RED & 1);
   constexpr int NB = LOADP ? 2 : 1;
+  constexpr int BOXZ = TG::BOXZ;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int S = a.S;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S * NS * NB * TG::SLOT);
+  const size_t stage_bytes = (size_t)NS * NB * TG::SLOT;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S * stage_bytes);
   double *red_smem = reinterpret_cast<double *>(bars + S);
   __shared__ int abort_flag;
 
   const Pad &pd = a.pd;
   const int N = pd.N;
-  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * kTZ + tz;
-  const int z0 = blockIdx.x * kTileZ, y0 = blockIdx.y * kTY;
+  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * SH::TZ + tz;
+  const int z0 = blockIdx.x * SH::BZ, y0 = blockIdx.y * SH::BY;
   const int x0 = blockIdx.z * a.LX, x1 = min(N, x0 + a.LX);
-  const int zl = kVZ * tz;
-  const int z = z0 + zl, y = y0 + ty;
+  const int z = z0 + VZ * tz, y = y0 + ty;
   const bool vy = y < N;
-  const bool v0 = vy && z < N, v1 = vy && z + 1 < N;
-  const int row = ty + 1, col = TG::G + zl;
-  const int nplanes = x1 - x0 + 2; // planes x0-1 .. x1
+  const int nvalid = vy ? max(0, min(VZ, N - z)) : 0; // sites of this thread inside the lattice
+  const int toff = (ty + 1) * BOXZ + TG::G + VZ * tz; // box offset of site 0
+  const int nplanes = x1 - x0 + 2;                     // planes x0-1 .. x1
   const uint32_t tx_bytes = (uint32_t)(NS * NB * TG::BYTES);
+
+  if (x0 >= x1) { // block-uniform: no planes, but its partial row must not hold stale sums
+    if (RED && tid == 0) {
+      const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+      for (int k = 0; k < kRedSlots; ++k) partials[bid * kRedSlots + k] = 0.0;
+    }
+    return;
+  }
 
   R pdr = R(0), dtw = R(0), KA = R(0), KB = R(0);
   if (DRIFT) {
@@ -116,8 +165,9 @@ __global__ void __launch_bounds__(kSweepThreads)
   const R c0 = (R)a.c0, q = (R)a.q, c0q = (R)a.c0_quarter, qh = (R)a.q_half;
   const R two = R(2);
 
+  // box (stage s, field f, k = 0 phi / 1 pi)
   auto box = [&](int s, int f, int k) -> R * {
-    return reinterpret_cast<R *>(smem_raw + ((size_t)(s * NS + f) * NB + k) * TG::SLOT);
+    return reinterpret_cast<R *>(smem_raw + (size_t)s * stage_bytes + (size_t)(f * NB + k) * TG::SLOT);
   };
   auto issue = [&](int j) { // plane ring index j -> lattice plane x0 - 1 + j (periodic)
     const int s = j % S;
@@ -130,19 +180,29 @@ __global__ void __launch_bounds__(kSweepThreads)
       if (LOADP) tma_load_3d(box(s, f, 1), &tmp, &bars[s], z0, y0, f * N + p);
     }
   };
-  auto dval = [&](int s, int f, int r, int c) -> R {
-    R v = box(s, f, 0)[r * TG::BOXZ + c];
-    if (DRIFT) v = drift_val<R>(v, box(s, f, 1)[r * TG::BOXZ + c], pdr, dtw);
-    return v;
+  auto drift1 = [&](R phi, R pi) -> R { return DRIFT ? drift_val<R>(phi, pi, pdr, dtw) : phi; };
+  // VZ drifted values at box offset o of stage s, field f (and the raw pi values if wanted)
+  auto dquad = [&](int s, int f, int o, R (&out)[VZ], R (*praw)[VZ]) {
+    R fv[VZ];
+    ldv<R, VZ>(box(s, f, 0) + o, fv);
+    if (LOADP) {
+      R pv[VZ];
+      ldv<R, VZ>(box(s, f, 1) + o, pv);
+#pragma unroll
+      for (int k = 0; k < VZ; ++k) out[k] = drift1(fv[k], pv[k]);
+      if (praw)
+#pragma unroll
+        for (int k = 0; k < VZ; ++k) (*praw)[k] = pv[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < VZ; ++k) out[k] = fv[k];
+    }
+  };
+  auto dscalar = [&](int s, int f, int o) -> R {
+    const R fv = box(s, f, 0)[o];
+    return LOADP ? drift1(fv, box(s, f, 1)[o]) : fv;
   };
 
-  if (x0 >= x1) { // block-uniform: no planes, but its partial row must not hold stale sums
-    if (RED && tid == 0) {
-      const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-      for (int k = 0; k < kRedSlots; ++k) partials[bid * kRedSlots + k] = 0.0;
-    }
-    return;
-  }
   if (tid == 0) {
     abort_flag = 0;
     prefetch_tensormap(&tmf);
@@ -160,20 +220,20 @@ __global__ void __launch_bounds__(kSweepThreads)
     if (tid == 0) waited = j + 1;
   };
 
-  R prev[NS][2], cur[NS][2], nxt[NS][2], piC[NS][2], piN[NS][2];
+  // periodic ghost copies this thread writes (they depend on y and z only): y row -1 / N, z column -1 / N
+  const long long ioff = (long long)(y + 1) * pd.Zp + (z + pd.G); // offset of site 0 inside a plane
+  const int ghost_y = (y == 0) ? N : (y == N - 1 ? -1 : -2);     // target row, -2: none
+  const int kz_first = z == 0 ? 0 : -1;                         // site writing the z = N ghost
+  const int kz_last = (N - 1 - z >= 0 && N - 1 - z < nvalid) ? N - 1 - z : -1; // site writing z = -1
+  const bool has_ghost = nvalid > 0 && (ghost_y != -2 || kz_first >= 0 || kz_last >= 0);
+
+  R prev[NS][VZ], cur[NS][VZ], nxt[NS][VZ], piC[NS][VZ], piN[NS][VZ];
   wait_plane(0);
 #pragma unroll
-  for (int f = 0; f < NS; ++f)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) prev[f][k] = dval(0, f, row, col + k);
+  for (int f = 0; f < NS; ++f) dquad(0, f, toff, prev[f], nullptr);
   wait_plane(1);
 #pragma unroll
-  for (int f = 0; f < NS; ++f)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      cur[f][k] = dval(1 % S, f, row, col + k);
-      if (LOADP) piC[f][k] = box(1 % S, f, 1)[row * TG::BOXZ + col + k];
-    }
+  for (int f = 0; f < NS; ++f) dquad(1 % S, f, toff, cur[f], LOADP ? &piC[f] : nullptr);
   __syncthreads();
   if (abort_flag) goto drain;
   if (tid == 0 && S < nplanes) {
@@ -183,33 +243,23 @@ __global__ void __launch_bounds__(kSweepThreads)
 
   {
     double acc_pi2 = 0, acc_g2 = 0, acc_v = 0;
-    for (int x = x0; x < x1; ++x) {
+    long long pbase = (long long)x0 * pd.plane;
+    for (int x = x0; x < x1; ++x, pbase += pd.plane) {
       const int j = x - x0 + 1;
       const int sb = j % S, sn = (j + 1) % S;
       wait_plane(j + 1);
-#pragma unroll
-      for (int f = 0; f < NS; ++f)
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          nxt[f][k] = dval(sn, f, row, col + k);
-          if (LOADP) piN[f][k] = box(sn, f, 1)[row * TG::BOXZ + col + k];
-        }
-      // in-plane neighbours of plane x (drifted), per field: y-1 and y+1 pairs, z-1 of site 0, z+1 of site 1
-      R ym[NS][2], yp[NS][2], zm0[NS], zp1[NS];
+      R ym[NS][VZ], yp[NS][VZ], zmv[NS], zpv[NS];
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
-        ym[f][0] = dval(sb, f, row - 1, col);
-        ym[f][1] = dval(sb, f, row - 1, col + 1);
-        yp[f][0] = dval(sb, f, row + 1, col);
-        yp[f][1] = dval(sb, f, row + 1, col + 1);
-        zm0[f] = dval(sb, f, row, col - 1);
-        zp1[f] = dval(sb, f, row, col + 2);
+        dquad(sn, f, toff, nxt[f], LOADP ? &piN[f] : nullptr);
+        dquad(sb, f, toff - BOXZ, ym[f], nullptr);
+        dquad(sb, f, toff + BOXZ, yp[f], nullptr);
+        zmv[f] = dscalar(sb, f, toff - 1);
+        zpv[f] = dscalar(sb, f, toff + VZ);
       }
-      const long long base = pd.at(x, y, z);
-      R outf[NS][2], outp[NS][2];
+      R outp[NS][VZ];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const bool vk = k == 0 ? v0 : v1;
+      for (int k = 0; k < VZ; ++k) {
         R cv[NS];
 #pragma unroll
         for (int f = 0; f < NS; ++f) cv[f] = cur[f][k];
@@ -217,13 +267,12 @@ __global__ void __launch_bounds__(kSweepThreads)
 #pragma unroll
         for (int f = 0; f < NS; ++f) {
           const R c = cur[f][k];
-          const R zn = k == 0 ? cur[f][1] : zp1[f];
-          const R zmv = k == 0 ? zm0[f] : cur[f][0];
-          outf[f][k] = c;
+          const R zn = k + 1 < VZ ? cur[f][k + 1 < VZ ? k + 1 : 0] : zpv[f];
+          const R zm = k > 0 ? cur[f][k > 0 ? k - 1 : 0] : zmv[f];
           if (KICK) {
             const R txv = A::sub(A::add(nxt[f][k], prev[f][k]), A::mul(two, c));
             const R tyv = A::sub(A::add(yp[f][k], ym[f][k]), A::mul(two, c));
-            const R tzv = A::sub(A::add(zn, zmv), A::mul(two, c));
+            const R tzv = A::sub(A::add(zn, zm), A::mul(two, c));
             const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
             const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cv, c0, q)));
             const KickOut<R> ko = kick_val<R>(piC[f][k], K, a.h1, a.h2);
@@ -233,46 +282,43 @@ __global__ void __launch_bounds__(kSweepThreads)
             const double pc = (double)piC[f][k];
             site_pi2 = f == 0 ? pc * pc : site_pi2 + pc * pc;
           }
-          if ((RED & 2) && vk) {
+          if ((RED & 2) && k < nvalid) {
             const R gx = A::sub(nxt[f][k], c), gy = A::sub(yp[f][k], c), gz = A::sub(zn, c);
             acc_g2 += (double)A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
           }
         }
-        if ((RED & 1) && vk) acc_pi2 += site_pi2;
-        if ((RED & 2) && vk) acc_v += (double)Pot::V(cv, c0q, qh);
+        if ((RED & 1) && k < nvalid) acc_pi2 += site_pi2;
+        if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, c0q, qh);
       }
-      // stores: interior pair, then the periodic ghost copies of boundary sites
+      // stores: the thread's VZ sites, then the periodic ghost copies of boundary sites
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
-        const long long o = (long long)f * pd.comp;
-        if (DRIFT) {
-          if (v0 && v1) {
-            *reinterpret_cast<V2 *>(fout + o + base) = V2{outf[f][0], outf[f][1]};
-          } else if (v0) {
-            fout[o + base] = outf[f][0];
-          }
-        }
-        if (KICK) {
-          if (v0 && v1) {
-            *reinterpret_cast<V2 *>(pout + o + base) = V2{outp[f][0], outp[f][1]};
-          } else if (v0) {
-            pout[o + base] = outp[f][0];
-          }
-        }
+        const long long o = (long long)f * pd.comp + pbase + ioff;
+        if (nvalid == VZ) {
+          if (DRIFT) stv<R, VZ>(fout + o, cur[f]);
+          if (KICK) stv<R, VZ>(pout + o, outp[f]);
+        } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const bool vk = k == 0 ? v0 : v1;
-          if (!vk) continue;
-          const int zk = z + k;
-          long long g[3];
-          int ng = 0;
-          if (y == 0) g[ng++] = pd.at(x, N, zk);
-          if (y == N - 1) g[ng++] = pd.at(x, -1, zk);
-          if (zk == 0) g[ng++] = pd.at(x, y, N);
-          if (zk == N - 1 && ng < 3) g[ng++] = pd.at(x, y, -1);
-          for (int i = 0; i < ng; ++i) {
-            if (DRIFT) fout[o + g[i]] = outf[f][k];
-            if (KICK) pout[o + g[i]] = outp[f][k];
+          for (int k = 0; k < VZ; ++k)
+            if (k < nvalid) {
+              if (DRIFT) fout[o + k] = cur[f][k];
+              if (KICK) pout[o + k] = outp[f][k];
+            }
+        }
+        if (has_ghost) {
+          const long long fp = (long long)f * pd.comp + pbase;
+#pragma unroll
+          for (int k = 0; k < VZ; ++k) {
+            if (k >= nvalid) continue;
+            long long g[3];
+            int ng = 0;
+            if (ghost_y != -2) g[ng++] = fp + pd.at(0, ghost_y, z + k);
+            if (k == kz_first) g[ng++] = fp + pd.at(0, y, N);
+            if (k == kz_last) g[ng++] = fp + pd.at(0, y, -1);
+            for (int i = 0; i < ng; ++i) {
+              if (DRIFT) fout[g[i]] = cur[f][k];
+              if (KICK) pout[g[i]] = outp[f][k];
+            }
           }
         }
       }
@@ -285,7 +331,7 @@ __global__ void __launch_bounds__(kSweepThreads)
 #pragma unroll
       for (int f = 0; f < NS; ++f)
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < VZ; ++k) {
           prev[f][k] = cur[f][k];
           cur[f][k] = nxt[f][k];
           if (LOADP) piC[f][k] = piN[f][k];
@@ -293,7 +339,7 @@ __global__ void __launch_bounds__(kSweepThreads)
     }
     if (RED) {
       double v[kRedSlots] = {acc_pi2, acc_g2, acc_v};
-      block_reduce<kRedSlots, kSweepThreads>(v, red_smem);
+      block_reduce<kRedSlots, SH::THREADS>(v, red_smem);
       if (tid == 0) {
         const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
 #pragma unroll

@@ -103,6 +103,18 @@ class Lattice:
         self._check(self.lib.clb_measure(self.h, float(e0), C.byref(m)))
         return measurement_to_dict(m)
 
+    def spectrum(self, which: int = 0, comp: int = 0, ps_type: int = 1, ps_version: int = 1, dk: float = 1.0,
+                 nbins: Optional[int] = None, fold: bool = True):
+        """(k, spectrum, mode counts) of scalar `comp`: which = 0 field, 1 momentum."""
+        if nbins is None:
+            nbins = int(np.floor(np.sqrt(3.0) / 2.0 * self.rp.N / dk))
+        k = np.empty(nbins)
+        v = np.empty(nbins)
+        c = np.empty(nbins, dtype=np.int64)
+        self._check(self.lib.clb_spectrum(self.h, which, comp, ps_type, ps_version, float(dk), nbins, 1 if fold else 0,
+                                          _dp(k), _dp(v), c.ctypes.data_as(C.POINTER(C.c_int64))))
+        return k, v, c
+
     def history(self) -> np.ndarray:
         """Per-step rows (a, aDot, <pi^2>, <grad^2>, <V>) of the last evolve call."""
         n = C.c_int64()

@@ -151,6 +151,21 @@ int clb_sync(clb_handle *h);
  * total energy used for energy_cons without expansion (ignored with expansion). */
 int clb_measure(clb_handle *h, double e0, clb_measurement *out);
 
+/* Radially binned power spectrum of scalar component `comp` at the current state
+ * (PowerSpectrumMeasurer::powerSpectrum, measurements/powerspectrum.h:84-134, as called from
+ * ScalarSingletMeasurer::measureSpectra, scalarsingletmeasurer.h:74-83).
+ *   which: 0 the field, 1 the momentum (times a^(2 alpha - 6), scalarsingletmeasurer.h:80).
+ *   ps_type: 1 (sum over the bin x kIR n dx / dk / N^5 / 2 pi) or 2 (bin average x (kIR n dx / N)^3
+ *            / dk / 2 pi^2), the reference's PS_type (runparameters.h:119).
+ *   ps_version: 1 n = the bin's mean |n| over its modes, 2 n = the bin centre (b + 1/2) dk.
+ *   Bins: b = floor(|n| / dk) over the full N^3 grid of integer wave vectors n; modes with b >= nbins
+ *   go to the last bin if fold != 0, else they are not counted.  The reference's default is
+ *   nbins = floor(sqrt(3)/2 N / dk) with every mode counted (fold = 1; runparameters.h:98).
+ * Outputs per bin: k_out = n kIR (may be NULL), value_out, count_out = number of modes (may be NULL).
+ * The transform is cuFFT D2Z in FP64 for either storage precision. */
+int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                 int32_t nbins, int32_t fold, double *k_out, double *value_out, int64_t *count_out);
+
 /* ---- per-step results and instrumentation (no reference counterpart: the reference writes these
  *      averages to text files at its output cadence, measurer.h:87-121) -------------------------- */
 
