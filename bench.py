@@ -207,8 +207,25 @@ def run_form(rp, model, fields, momenta, sf, precision, warmup, steps, device, w
     lat.sync()
     m1 = lat.measure(m0["energies"][-1])
     hist = lat.history()
+    # field spectra at the end of the run: the reference's default bins and N/2 bins
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    spec = lat.spectrum(which=0)
+    torch.cuda.synchronize(device)
+    spec_ms = (time.perf_counter() - t0) * 1e3
+    spec_half = lat.spectrum(which=0, nbins=rp.N // 2, fold=False)
     lat.close()
-    return {"ms": ms, "stats": stats, "clocks": clk.summary(), "m0": m0, "m1": m1, "hist_rows": len(hist)}
+    return {"ms": ms, "stats": stats, "clocks": clk.summary(), "m0": m0, "m1": m1, "hist_rows": len(hist),
+            "spec": spec, "spec_half": spec_half, "spec_ms": spec_ms}
+
+
+def spectrum_error(a, b):
+    """max relative difference of spectrum b to a over a's populated band (> 1e-6 of its peak)."""
+    import numpy as np
+
+    va, vb = a[1], b[1]
+    band = va > 1e-6 * va.max()
+    return float((np.abs(va - vb)[band] / np.abs(va)[band]).max())
 
 
 def run_e2e(rp, model, fields, momenta, sf, steps, device):
@@ -350,7 +367,12 @@ def main():
             "friedmann_abs_diff": abs(f32["friedmann"][0] - f64["friedmann"][0]),
             "energy_rel_diff": max(abs(a - b) / abs(b) for a, b in zip(f32["energies"], f64["energies"]) if b != 0),
             "a_rel_diff": abs(f32["aI"] - f64["aI"]) / f64["aI"],
+            "spectrum_rel_diff": spectrum_error(r64["spec"], r32["spec"]),
+            "spectrum_rel_diff_half_bins": spectrum_error(r64["spec_half"], r32["spec_half"]),
+            "spectrum_bins": [len(r64["spec"][1]), len(r64["spec_half"][1])],
+            "mode_counts_equal": bool((r64["spec"][2] == r32["spec"][2]).all()),
         },
+        "spectrum_ms": r64["spec_ms"],
         "e2e": {"value": 1.0 / e2e_val if world > 1 else e2e["value"], "unit": "site-updates/s",
                 "h2d_bytes_per_step": e2e["h2d_bytes_per_step"], "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
                 "seconds": e2e["seconds"], "timer": "host wall clock around the C-ABI calls"},
