@@ -80,6 +80,7 @@ struct clb_handle {
   Pad pd{};           // padded component layout (clb_sweep.cuh)
   CUtensorMap tm_f[2], tm_p[2];
   int S = 3;          // sweep ring stages
+  int rs = 0;         // FP32 split storage: current reference slot in DevState
   int shape = 0;      // sweep block shape: 0 ShapeW, 1 ShapeQ, 2 ShapeH (clb_sweep.cuh)
   int bz = 64, by = 8; // sites per block tile in z and y
   size_t sweep_smem = 0;
@@ -243,10 +244,12 @@ void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dt
   a.dtw = dtw;
   a.h1 = h1;
   a.h2 = h2;
+  a.rs = h->rs;
   CLB_LAUNCH(h, kind,
              k_sweep<R, NS, SH, DRIFT, KICK, RED><<<h->sweep_grid, dim3(SH::TZ, SH::TY), h->sweep_smem, h->stream>>>(
                  h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]), a, h->d_st,
                  h->d_part, h->d_err));
+  if (sizeof(R) == 4 && (DRIFT || KICK)) h->rs ^= 1; // the launch advanced the FP64 references
 }
 
 template <class R, int NS, bool DRIFT, bool KICK, int RED>
@@ -291,12 +294,14 @@ template <class R, int NS> struct Launch {
   {
     CLB_LAUNCH(h, K_DRIFT,
                k_drift<R><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp),
-                                                               (size_t)NS * (size_t)h->pd.comp, dtw, h->d_st));
+                                                               (size_t)NS * (size_t)h->pd.comp, dtw, h->d_st, h->rs,
+                                                               NS));
+    if (sizeof(R) == 4) h->rs ^= 1;
   }
   // <pi^2> partials (elementwise grid)
   static int reduce_pi2(clb_handle *h)
   {
-    CLB_LAUNCH(h, K_RED_PI2, k_reduce_pi2_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(P<R>(h, h->cp), h->pd, h->d_part));
+    CLB_LAUNCH(h, K_RED_PI2, k_reduce_pi2_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(P<R>(h, h->cp), h->pd, h->d_st, h->rs, h->d_part));
     return kElemBlocks;
   }
   // <grad^2>, <V> (and <pi^2> with all=true) partials (sweep grid)
@@ -313,14 +318,14 @@ template <class R, int NS> struct Launch {
     CLB_LAUNCH(h, K_MEASURE,
                k_measure_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->pd,
                                                                         h->sa.inv_dx2, h->sa.c0_quarter,
-                                                                        h->sa.q_half, am, h->d_part));
+                                                                        h->sa.q_half, am, h->d_st, h->rs, h->d_part));
     CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeasSlots><<<1, 256, 0, h->stream>>>(h->d_part, kElemBlocks, h->d_sums));
   }
 };
 
 // Host arrays (plane after plane, N x N each) <-> padded device components, through the staging
 // buffer in whole planes, with FP32 conversion on the GPU and the periodic ghosts filled after upload.
-cudaError_t upload(clb_handle *h, const double *src, void *dst)
+cudaError_t upload(clb_handle *h, const double *src, void *dst, CompOffsets off)
 {
   const long long planes = (long long)h->NS * h->N, per = (long long)h->N * h->N;
   const long long chunk = std::max<long long>(1, (long long)h->stage_n / per);
@@ -331,10 +336,10 @@ cudaError_t upload(clb_handle *h, const double *src, void *dst)
     if (r != cudaSuccess) return r;
     if (h->fp32)
       CLB_LAUNCH(h, K_CONVERT, k_scatter<double, float><<<kElemBlocks, 256, 0, h->stream>>>(
-                                   h->d_stage, static_cast<float *>(dst), h->pd, p0, np));
+                                   h->d_stage, static_cast<float *>(dst), h->pd, p0, np, off));
     else
       CLB_LAUNCH(h, K_CONVERT, k_scatter<double, double><<<kElemBlocks, 256, 0, h->stream>>>(
-                                   h->d_stage, static_cast<double *>(dst), h->pd, p0, np));
+                                   h->d_stage, static_cast<double *>(dst), h->pd, p0, np, off));
   }
   if (h->fp32)
     CLB_LAUNCH(h, K_CONVERT, k_fill_ghosts<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<float *>(dst), h->pd, h->NS));
@@ -343,7 +348,7 @@ cudaError_t upload(clb_handle *h, const double *src, void *dst)
   return cudaGetLastError();
 }
 
-cudaError_t download(clb_handle *h, const void *src, double *dst)
+cudaError_t download(clb_handle *h, const void *src, double *dst, CompOffsets off)
 {
   const long long planes = (long long)h->NS * h->N, per = (long long)h->N * h->N;
   const long long chunk = std::max<long long>(1, (long long)h->stage_n / per);
@@ -351,10 +356,10 @@ cudaError_t download(clb_handle *h, const void *src, double *dst)
     const long long np = std::min(chunk, planes - p0);
     if (h->fp32)
       CLB_LAUNCH(h, K_CONVERT, k_gather<float, double><<<kElemBlocks, 256, 0, h->stream>>>(
-                                   static_cast<const float *>(src), h->d_stage, h->pd, p0, np));
+                                   static_cast<const float *>(src), h->d_stage, h->pd, p0, np, off));
     else
       CLB_LAUNCH(h, K_CONVERT, k_gather<double, double><<<kElemBlocks, 256, 0, h->stream>>>(
-                                   static_cast<const double *>(src), h->d_stage, h->pd, p0, np));
+                                   static_cast<const double *>(src), h->d_stage, h->pd, p0, np, off));
     cudaError_t r = cudaMemcpyAsync(dst + p0 * per, h->d_stage, (size_t)(np * per) * sizeof(double),
                                     cudaMemcpyDeviceToHost, h->stream);
     if (r != cudaSuccess) return r;
@@ -733,8 +738,23 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->cf = h->cp = 0;
-  e = upload(h, fields, h->fld[0]);
-  if (e == cudaSuccess) e = upload(h, momenta, h->pi[0]);
+  h->rs = 0;
+  // FP32 split storage: each component is stored as its deviation from its FP64 volume mean
+  CompOffsets fo{{0.0, 0.0}}, po{{0.0, 0.0}};
+  if (h->fp32) {
+    for (int f = 0; f < h->NS; ++f) {
+      double sf_ = 0, sp_ = 0;
+      const double *fa = fields + (size_t)f * h->n3, *pa = momenta + (size_t)f * h->n3;
+      for (size_t i = 0; i < h->n3; ++i) {
+        sf_ += fa[i];
+        sp_ += pa[i];
+      }
+      fo.v[f] = sf_ / (double)h->n3;
+      po.v[f] = sp_ / (double)h->n3;
+    }
+  }
+  e = upload(h, fields, h->fld[0], fo);
+  if (e == cudaSuccess) e = upload(h, momenta, h->pi[0], po);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   DevState s{};
@@ -751,6 +771,10 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
   s.drift_p = std::pow(s.aSI, al - 3);
   s.kick_A = std::pow(s.aI, 1 + al);
   s.kick_B = std::pow(s.aI, 3 + al);
+  for (int f = 0; f < 2; ++f) {
+    s.ref_phi[0][f] = s.ref_phi[1][f] = fo.v[f];
+    s.ref_pi[0][f] = s.ref_pi[1][f] = po.v[f];
+  }
   e = cudaMemcpy(h->d_st, &s, sizeof(s), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->has_state = true;
@@ -764,9 +788,20 @@ int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefacto
   if (!h) return CLB_EINVAL;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
-  auto fetch = [&](void *src, double *dst) -> cudaError_t { return dst ? download(h, src, dst) : cudaSuccess; };
-  e = fetch(h->fld[h->cf], fields);
-  if (e == cudaSuccess) e = fetch(h->pi[h->cp], momenta);
+  DevState cur;
+  e = cudaMemcpy(&cur, h->d_st, sizeof(cur), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
+  CompOffsets fo{{0.0, 0.0}}, po{{0.0, 0.0}};
+  if (h->fp32)
+    for (int f = 0; f < h->NS; ++f) {
+      fo.v[f] = cur.ref_phi[h->rs][f];
+      po.v[f] = cur.ref_pi[h->rs][f];
+    }
+  auto fetch = [&](void *src, double *dst, CompOffsets off) -> cudaError_t {
+    return dst ? download(h, src, dst, off) : cudaSuccess;
+  };
+  e = fetch(h->fld[h->cf], fields, fo);
+  if (e == cudaSuccess) e = fetch(h->pi[h->cp], momenta, po);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
   if (sf) {
     DevState s;
@@ -1021,10 +1056,16 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
   }
   void *src = which == 0 ? h->fld[h->cf] : h->pi[h->cp];
   const size_t comp_off = (size_t)comp * (size_t)h->pd.comp;
+  double ref = 0.0;
+  if (h->fp32) {
+    DevState cur;
+    if ((e = cudaMemcpy(&cur, h->d_st, sizeof(cur), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+    ref = which == 0 ? cur.ref_phi[h->rs][comp] : cur.ref_pi[h->rs][comp];
+  }
   if (h->fp32)
-    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + comp_off, h->d_spec, h->pd));
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + comp_off, h->d_spec, h->pd, ref));
   else
-    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(src) + comp_off, h->d_spec, h->pd));
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(src) + comp_off, h->d_spec, h->pd, ref));
   if (cufftExecD2Z(h->plan, h->d_spec, reinterpret_cast<cufftDoubleComplex *>(h->d_spec)) != CUFFT_SUCCESS)
     return h->fail(CLB_ECUDA, "clb_spectrum: cufftExecD2Z failed");
   const size_t smem = (size_t)nbins * (2 * sizeof(double) + sizeof(unsigned long long));

@@ -24,6 +24,11 @@ struct DevState {
   double kick_B;  // pow(aI, 3 + alpha)
   int32_t status; // 0 ok, 1 non-finite average seen
   int32_t pad;
+  // FP32/FP64-split storage: phi = ref_phi + s, pi = ref_pi + p with s, p the FP32 arrays and the
+  // homogeneous references in FP64, advanced by the same VV map as a homogeneous site.  Two slots:
+  // a sweep reads slot rs and its first block writes the advanced values into slot rs ^ 1.
+  double ref_phi[2][2]; // [slot][field]
+  double ref_pi[2][2];
 };
 
 // Constants of the scale-factor equation (scalefactorkernels.h:73-77) and Friedmann constraint.

@@ -235,10 +235,20 @@ __global__ void __launch_bounds__(BZ *BY)
 
 // ---- elementwise kernels --------------------------------------------------------------------
 // Drift of every component in place: phi += p (dtw pi)  (velocityverlet.h:181-184).
+// With FP32 split storage (padded layout) the first thread also advances the FP64 references
+// from slot rs into slot rs ^ 1 (ns fields).
 template <class R>
-__global__ void __launch_bounds__(256) k_drift(R *fld, const R *pi, size_t n, double dtw, const DevState *__restrict__ st)
+__global__ void __launch_bounds__(256)
+    k_drift(R *fld, const R *pi, size_t n, double dtw, const DevState *__restrict__ st, int rs = 0, int ns = 0)
 {
   const R pd = (R)st->drift_p, w = (R)dtw;
+  if (sizeof(R) == 4 && ns > 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+    DevState *sw = const_cast<DevState *>(st); // slot rs ^ 1 is read by nobody during this launch
+    for (int f = 0; f < ns; ++f) {
+      sw->ref_phi[rs ^ 1][f] = __dadd_rn(st->ref_phi[rs][f], __dmul_rn(st->drift_p, __dmul_rn(dtw, st->ref_pi[rs][f])));
+      sw->ref_pi[rs ^ 1][f] = st->ref_pi[rs][f];
+    }
+  }
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     fld[i] = drift_val<R>(fld[i], pi[i], pd, w);
 }

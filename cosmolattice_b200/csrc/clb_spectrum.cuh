@@ -16,7 +16,7 @@ namespace clb {
 
 // Padded component -> real input of an in-place R2C transform (row pitch 2 (N/2 + 1) doubles).
 template <class R>
-__global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, double *__restrict__ dst, Pad pd)
+__global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, double *__restrict__ dst, Pad pd, double off)
 {
   const int N = pd.N;
   const long long pitch = 2LL * (N / 2 + 1);
@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, 
     const int x = (int)(r / N), y = (int)(r % N);
     const R *s = src + pd.at(x, y, 0);
     double *d = dst + r * pitch;
-    for (int z = threadIdx.x; z < N; z += blockDim.x) d[z] = (double)s[z];
+    for (int z = threadIdx.x; z < N; z += blockDim.x) d[z] = off + (double)s[z];
   }
 }
 

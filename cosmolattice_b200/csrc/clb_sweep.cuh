@@ -66,6 +66,7 @@ struct SweepArgs {
   Pad pd;
   int LX;          // planes per block
   int S;           // ring stages
+  int rs;          // FP32 split storage: reference slot read by this launch
   uint32_t tries;  // bound of each mbarrier wait
   double inv_dx2, c0, q, c0_quarter, q_half;
   double dtw, h1, h2;
@@ -111,7 +112,63 @@ template <class R, int VZ> __device__ __forceinline__ void stv(R *p, const R (&v
   }
 }
 
+// One VV sweep applied to the homogeneous FP64 references of the split storage: the same drift and
+// kicks as a site with zero fluctuation (the Laplacian of a constant vanishes).
+template <int NS> struct RefStep {
+  double phi[NS], pi_mid[NS], pi_next[NS], dV[NS];
+  double V; // potential at the reference point
+};
+
+// lphi4 with one field about a reference phi_r: exact polynomial differences in the fluctuation s,
+//   dV(phi_r + s) - dV(phi_r) = s (a1 + s (a2 + c0 s)),      a1 = 3 c0 phi_r^2, a2 = 3 c0 phi_r
+//   V(phi_r + s) - V(phi_r)   = s (b1 + s (b2 + s (b3 + c0/4 s))), b1 = c0 phi_r^3, b2 = 3/2 c0 phi_r^2,
+//                                                               b3 = c0 phi_r
+// evaluated in FP32 (relative precision of the fluctuation's own force and energy).
+struct Lphi4SplitCoef {
+  float a1, a2, c0, b1, b2, b3, c0q;
+  __host__ __device__ static Lphi4SplitCoef make(double phi_r, double c0)
+  {
+    Lphi4SplitCoef k;
+    k.a1 = (float)(3.0 * c0 * phi_r * phi_r);
+    k.a2 = (float)(3.0 * c0 * phi_r);
+    k.c0 = (float)c0;
+    k.b1 = (float)(c0 * phi_r * phi_r * phi_r);
+    k.b2 = (float)(1.5 * c0 * phi_r * phi_r);
+    k.b3 = (float)(c0 * phi_r);
+    k.c0q = (float)(0.25 * c0);
+    return k;
+  }
+  __device__ __forceinline__ float ddV(float s) const { return s * fmaf(s, fmaf(c0, s, a2), a1); }
+  __device__ __forceinline__ float dVpot(float s) const { return s * fmaf(s, fmaf(s, fmaf(c0q, s, b3), b2), b1); }
+};
+
+template <int NS>
+__device__ __forceinline__ RefStep<NS> ref_step(const DevState *st, int rs, bool drift, bool kick, double dtw, double h1,
+                                                double h2, double c0, double q)
+{
+  RefStep<NS> r;
+  double phi[NS];
+#pragma unroll
+  for (int f = 0; f < NS; ++f) {
+    phi[f] = st->ref_phi[rs][f];
+    if (drift) phi[f] = __dadd_rn(phi[f], __dmul_rn(st->drift_p, __dmul_rn(dtw, st->ref_pi[rs][f])));
+    r.phi[f] = phi[f];
+  }
+  r.V = Lphi4<double, NS>::V(phi, 0.25 * c0, 0.5 * q);
+#pragma unroll
+  for (int f = 0; f < NS; ++f) {
+    r.dV[f] = Lphi4<double, NS>::dV(f, phi, c0, q);
+    const double Kr = -__dmul_rn(st->kick_B, r.dV[f]);
+    const double p0 = st->ref_pi[rs][f];
+    r.pi_mid[f] = kick ? __dadd_rn(p0, __dmul_rn(h1, Kr)) : p0;
+    r.pi_next[f] = (kick && h2 != 0.0) ? __dadd_rn(r.pi_mid[f], __dmul_rn(h2, Kr)) : r.pi_mid[f];
+  }
+  return r;
+}
+
 // DRIFT / KICK / RED as in k_scalar_sweep (clb_scalar.cuh); fout/pout are padded arrays.
+// FP32 storage holds fluctuations around the FP64 references (DevState::ref_*): FP32 arithmetic on
+// the fluctuations, with the reference terms of the volume sums added in FP64.
 template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
 __global__ void __launch_bounds__(SH::THREADS)
     k_sweep(const __grid_constant__ CUtensorMap tmf, const __grid_constant__ CUtensorMap tmp, R *fout, R *pout,
@@ -124,6 +181,7 @@ __global__ void __launch_bounds__(SH::THREADS)
   constexpr bool LOADP = DRIFT || KICK || (RED & 1);
   constexpr int NB = LOADP ? 2 : 1;
   constexpr int BOXZ = TG::BOXZ;
+  constexpr bool SPLIT = sizeof(R) == 4;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int S = a.S;
@@ -164,6 +222,21 @@ __global__ void __launch_bounds__(SH::THREADS)
   const R inv_dx2 = (R)a.inv_dx2;
   const R c0 = (R)a.c0, q = (R)a.q, c0q = (R)a.c0_quarter, qh = (R)a.q_half;
   const R two = R(2);
+  RefStep<NS> rf{};
+  Lphi4SplitCoef spc{};
+  const float h1f = (float)a.h1, h2f = (float)a.h2;
+  if constexpr (SPLIT) {
+    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.c0, a.q);
+    spc = Lphi4SplitCoef::make(rf.phi[0], a.c0);
+    if ((DRIFT || KICK) && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
+      DevState *sw = const_cast<DevState *>(st); // slot rs ^ 1 is read by no block of this launch
+#pragma unroll
+      for (int f = 0; f < NS; ++f) {
+        sw->ref_phi[a.rs ^ 1][f] = rf.phi[f];
+        sw->ref_pi[a.rs ^ 1][f] = rf.pi_next[f];
+      }
+    }
+  }
 
   // box (stage s, field f, k = 0 phi / 1 pi)
   auto box = [&](int s, int f, int k) -> R * {
@@ -243,6 +316,10 @@ __global__ void __launch_bounds__(SH::THREADS)
 
   {
     double acc_pi2 = 0, acc_g2 = 0, acc_v = 0;
+    double acc_p[NS]; // FP32 split: sum of the momentum fluctuation per field
+#pragma unroll
+    for (int f = 0; f < NS; ++f) acc_p[f] = 0;
+    long long cnt = 0; // FP32 split: sites summed by this thread
     long long pbase = (long long)x0 * pd.plane;
     for (int x = x0; x < x1; ++x, pbase += pd.plane) {
       const int j = x - x0 + 1;
@@ -258,6 +335,67 @@ __global__ void __launch_bounds__(SH::THREADS)
         zpv[f] = dscalar(sb, f, toff + VZ);
       }
       R outp[NS][VZ];
+      if constexpr (SPLIT) {
+        // FP32 fluctuations about the FP64 references: FP32 arithmetic throughout, per-plane FP32
+        // partial sums folded into FP64 accumulators (the reference terms are added at the end)
+        float s_p[NS], s_p2 = 0.f, s_g2 = 0.f, s_dv = 0.f;
+#pragma unroll
+        for (int f = 0; f < NS; ++f) s_p[f] = 0.f;
+#pragma unroll
+        for (int k = 0; k < VZ; ++k) {
+          const bool vk = k < nvalid;
+          float cv[NS];
+          double cd[NS];
+#pragma unroll
+          for (int f = 0; f < NS; ++f) {
+            cv[f] = cur[f][k];
+            if constexpr (NS > 1) cd[f] = rf.phi[f] + (double)cur[f][k];
+          }
+#pragma unroll
+          for (int f = 0; f < NS; ++f) {
+            const float c = cur[f][k];
+            const float zn = k + 1 < VZ ? cur[f][k + 1 < VZ ? k + 1 : 0] : zpv[f];
+            const float zm = k > 0 ? cur[f][k > 0 ? k - 1 : 0] : zmv[f];
+            if (KICK) {
+              const float lap = inv_dx2 * ((((nxt[f][k] + prev[f][k]) - 2.f * c) + ((yp[f][k] + ym[f][k]) - 2.f * c)) +
+                                           ((zn + zm) - 2.f * c));
+              float ddv;
+              if constexpr (NS == 1)
+                ddv = spc.ddV(c);
+              else
+                ddv = (float)(Lphi4<double, NS>::dV(f, cd, a.c0, a.q) - rf.dV[f]);
+              const float K = KA * lap - KB * ddv;
+              const float pm = fmaf(h1f, K, piC[f][k]);
+              outp[f][k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
+              if ((RED & 1) && vk) {
+                s_p[f] += pm;
+                s_p2 = fmaf(pm, pm, s_p2);
+              }
+            } else if ((RED & 1) && vk) {
+              s_p[f] += piC[f][k];
+              s_p2 = fmaf(piC[f][k], piC[f][k], s_p2);
+            }
+            if ((RED & 2) && vk) {
+              const float gx = nxt[f][k] - c, gy = yp[f][k] - c, gz = zn - c;
+              s_g2 += (gx * gx + gy * gy + gz * gz) * inv_dx2;
+            }
+          }
+          if ((RED & 2) && vk) {
+            if constexpr (NS == 1)
+              s_dv += spc.dVpot(cv[0]);
+            else
+              s_dv += (float)(Lphi4<double, NS>::V(cd, a.c0_quarter, a.q_half) - rf.V);
+          }
+        }
+        if (RED) {
+#pragma unroll
+          for (int f = 0; f < NS; ++f) acc_p[f] += (double)s_p[f];
+          acc_pi2 += (double)s_p2;
+          acc_g2 += (double)s_g2;
+          acc_v += (double)s_dv;
+          cnt += nvalid;
+        }
+      } else {
 #pragma unroll
       for (int k = 0; k < VZ; ++k) {
         R cv[NS];
@@ -289,6 +427,7 @@ __global__ void __launch_bounds__(SH::THREADS)
         }
         if ((RED & 1) && k < nvalid) acc_pi2 += site_pi2;
         if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, c0q, qh);
+      }
       }
       // stores: the thread's VZ sites, then the periodic ghost copies of boundary sites
 #pragma unroll
@@ -338,6 +477,14 @@ __global__ void __launch_bounds__(SH::THREADS)
         }
     }
     if (RED) {
+      if constexpr (SPLIT) {
+        // sum (pi_r + p)^2 = n pi_r^2 + 2 pi_r sum p + sum p^2;  sum V = n V_r + sum (V - V_r)
+        double t = acc_pi2;
+#pragma unroll
+        for (int f = 0; f < NS; ++f) t += (double)cnt * rf.pi_mid[f] * rf.pi_mid[f] + 2.0 * rf.pi_mid[f] * acc_p[f];
+        acc_pi2 = t;
+        acc_v += (double)cnt * rf.V;
+      }
       double v[kRedSlots] = {acc_pi2, acc_g2, acc_v};
       block_reduce<kRedSlots, SH::THREADS>(v, red_smem);
       if (tid == 0) {
@@ -361,10 +508,14 @@ drain:
 // ---- padded elementwise / row kernels -------------------------------------------------------------
 // Sum over interior sites of sum_f pi_f^2 into slot 0 of each block's partial row.
 template <class R, int NS>
-__global__ void __launch_bounds__(256) k_reduce_pi2_pad(const R *pi, Pad pd, double *__restrict__ partials)
+__global__ void __launch_bounds__(256)
+    k_reduce_pi2_pad(const R *pi, Pad pd, const DevState *__restrict__ st, int rs, double *__restrict__ partials)
 {
   __shared__ double smem[(256 / 32) * kRedSlots];
   const int N = pd.N;
+  double pref[NS];
+#pragma unroll
+  for (int f = 0; f < NS; ++f) pref[f] = sizeof(R) == 4 ? st->ref_pi[rs][f] : 0.0;
   double acc = 0;
   for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
     const int x = (int)(r / N), y = (int)(r % N);
@@ -373,7 +524,7 @@ __global__ void __launch_bounds__(256) k_reduce_pi2_pad(const R *pi, Pad pd, dou
       double v = 0;
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
-        const double p = (double)pi[f * pd.comp + s];
+        const double p = sizeof(R) == 4 ? pref[f] + (double)pi[f * pd.comp + s] : (double)pi[f * pd.comp + s];
         v = f == 0 ? p * p : v + p * p;
       }
       acc += v;
@@ -389,8 +540,9 @@ __global__ void __launch_bounds__(256) k_reduce_pi2_pad(const R *pi, Pad pd, dou
 template <class R, int NS>
 __global__ void __launch_bounds__(256)
     k_measure_pad(const R *fld, const R *pi, Pad pd, double inv_dx2d, double c0qd, double qhd, double am,
-                  double *__restrict__ partials)
+                  const DevState *__restrict__ st, int rs, double *__restrict__ partials)
 {
+  constexpr bool SPLIT = sizeof(R) == 4;
   using A = Ar<R>;
   using Pot = Lphi4<R, NS>;
   __shared__ double smem[(256 / 32) * kMeasSlots];
@@ -406,24 +558,28 @@ __global__ void __launch_bounds__(256)
       const long long s = pd.at(x, y, z);
       const long long sx = pd.at(xp, y, z), sy = pd.at(x, y + 1, z), sz = pd.at(x, y, z + 1);
       R v[NS];
+      double vd[NS];
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
         const long long o = f * pd.comp;
         const R c = fld[o + s];
         v[f] = c;
+        const double cfull = SPLIT ? st->ref_phi[rs][f] + (double)c : (double)c;
+        vd[f] = cfull;
         const R gx = A::sub(fld[o + sx], c), gy = A::sub(fld[o + sy], c), gz = A::sub(fld[o + sz], c);
         const R g2 = A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
-        const double p = (double)pi[o + s];
+        const double p = SPLIT ? st->ref_pi[rs][f] + (double)pi[o + s] : (double)pi[o + s];
         const double m = p * am;
         acc[6 * f + 0] += p * p;
         acc[6 * f + 1] += (double)g2;
-        acc[6 * f + 2] += (double)c;
-        acc[6 * f + 3] += (double)c * (double)c;
+        acc[6 * f + 2] += cfull;
+        acc[6 * f + 3] += cfull * cfull;
         acc[6 * f + 4] += m;
         acc[6 * f + 5] += m * m;
       }
 #pragma unroll
-      for (int k = 0; k < NS; ++k) acc[6 * NS + k] += (double)Pot::Vterm(k, v, c0q, qh);
+      for (int k = 0; k < NS; ++k)
+        acc[6 * NS + k] += SPLIT ? Lphi4<double, NS>::Vterm(k, vd, c0qd, qhd) : (double)Pot::Vterm(k, v, c0q, qh);
     }
   }
   block_reduce<kMeasSlots, 256>(acc, smem);
@@ -432,8 +588,14 @@ __global__ void __launch_bounds__(256)
 }
 
 // Host-order planes (plane p = f N + x, N x N each) -> padded interior, with type conversion.
+// Per-component constant removed on upload and added back on download (FP32 split references).
+struct CompOffsets {
+  double v[2];
+};
+
 template <class S, class D>
-__global__ void __launch_bounds__(256) k_scatter(const S *__restrict__ src, D *__restrict__ dst, Pad pd, long long p0, long long np)
+__global__ void __launch_bounds__(256)
+    k_scatter(const S *__restrict__ src, D *__restrict__ dst, Pad pd, long long p0, long long np, CompOffsets off)
 {
   const int N = pd.N;
   for (long long r = blockIdx.x; r < np * N; r += gridDim.x) {
@@ -441,12 +603,14 @@ __global__ void __launch_bounds__(256) k_scatter(const S *__restrict__ src, D *_
     const int y = (int)(r % N);
     const int f = (int)(p / N), x = (int)(p % N);
     const long long o = (long long)f * pd.comp + pd.at(x, y, 0);
-    for (int z = threadIdx.x; z < N; z += blockDim.x) dst[o + z] = (D)src[r * N + z];
+    const double c = off.v[f];
+    for (int z = threadIdx.x; z < N; z += blockDim.x) dst[o + z] = (D)((double)src[r * N + z] - c);
   }
 }
 
 template <class S, class D>
-__global__ void __launch_bounds__(256) k_gather(const S *__restrict__ src, D *__restrict__ dst, Pad pd, long long p0, long long np)
+__global__ void __launch_bounds__(256)
+    k_gather(const S *__restrict__ src, D *__restrict__ dst, Pad pd, long long p0, long long np, CompOffsets off)
 {
   const int N = pd.N;
   for (long long r = blockIdx.x; r < np * N; r += gridDim.x) {
@@ -454,7 +618,8 @@ __global__ void __launch_bounds__(256) k_gather(const S *__restrict__ src, D *__
     const int y = (int)(r % N);
     const int f = (int)(p / N), x = (int)(p % N);
     const long long o = (long long)f * pd.comp + pd.at(x, y, 0);
-    for (int z = threadIdx.x; z < N; z += blockDim.x) dst[r * N + z] = (D)src[o + z];
+    const double c = off.v[f];
+    for (int z = threadIdx.x; z < N; z += blockDim.x) dst[r * N + z] = (D)(c + (double)src[o + z]);
   }
 }
 
