@@ -31,6 +31,7 @@ PATH_FUSED = 0
 PATH_REFERENCE = 1
 
 MODEL_LPHI4 = 1
+MODEL_LPHI4U1 = 2
 
 MAX_COUPLINGS = 8
 MAX_ENERGIES = 32
@@ -76,6 +77,7 @@ class Measurement(C.Structure):
         ("friedmann", C.c_double * 3),
         ("n_means", C.c_int32),
         ("means", (C.c_double * 6) * MAX_MEANS),
+        ("gauss_u1", C.c_double * 3),
     ]
 
 

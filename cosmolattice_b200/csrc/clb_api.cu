@@ -9,6 +9,7 @@
 
 #include "../../include/clb200.h"
 #include "clb_internal.cuh"
+#include "clb_handle.cuh"
 #include "clb_scalar.cuh"
 #include "clb_spectrum.cuh"
 #include "clb_sweep.cuh"
@@ -62,91 +63,23 @@ constexpr int kPlanesPerBlock = 32;           // x-run length of one sweep block
 } // namespace
 
 namespace clb {
+// complex scalar + U(1) sector (clb_u1.cu)
+int u1_create(clb_handle *h);
+void u1_destroy(clb_handle *h);
+int u1_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf);
+int u1_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
+int u1_initialize(clb_handle *h, int32_t correct_adot);
+int u1_evolve(clb_handle *h, int64_t n);
+int u1_sync(clb_handle *h);
+int u1_measure(clb_handle *h, double e0, clb_measurement *m);
+
 // Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
 __attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
 } // namespace clb
 
-struct clb_handle {
-  clb_config cfg;
-  clb_model_desc md;
-  int N = 0;
-  size_t n3 = 0;
-  int NS = 0;
-  bool fp32 = false;
-  size_t esz = 8;
-  void *fld[2] = {nullptr, nullptr};
-  void *pi[2] = {nullptr, nullptr};
-  int cf = 0, cp = 0; // current field / momentum buffer
-  Pad pd{};           // padded component layout (clb_sweep.cuh)
-  CUtensorMap tm_f[2], tm_p[2];
-  int S = 3;          // sweep ring stages
-  int rs = 0;         // FP32 split storage: current reference slot in DevState
-  int shape = 0;      // sweep block shape: 0 ShapeW, 1 ShapeQ, 2 ShapeH (clb_sweep.cuh)
-  int bz = 64, by = 8; // sites per block tile in z and y
-  size_t sweep_smem = 0;
-  int *d_err = nullptr; // set by a sweep whose bounded wait gave up
-  DevState *d_st = nullptr;
-  double *d_part = nullptr;
-  double *d_sums = nullptr;
-  size_t part_rows = 0;
-  cudaStream_t stream = nullptr;
-  std::vector<double> ws;
-  bool has_state = false, initialized = false, synced = true;
-  ScalarArgs sa{};
-  SweepArgs sw{};
-  SFParams sp{};
-  dim3 sweep_grid;
-  int sweep_blocks = 0;
-  std::string err;
-
-  // instrumentation: launch counts always; per-launch CUDA events on the stream when prof
-  bool prof = false;
-  struct Pend {
-    int kind;
-    cudaEvent_t a, b;
-  };
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<Pend> pend;
-  int64_t launches[16] = {};
-  int64_t timed[16] = {};
-  double kernel_ms[16] = {};
-  cudaEvent_t ev_call[2] = {nullptr, nullptr};
-  double last_evolve_ms = 0;
-  // per-step history rows of the last evolve call
-  double *d_hist = nullptr;
-  int64_t hist_cap = 0, hist_rows = 0;
-  // staging buffer for FP32 <-> FP64 host transfers
-  double *d_stage = nullptr;
-  size_t stage_n = 0;
-  // spectra: in-place D2Z buffer, cuFFT plan and binning scratch (allocated on first use)
-  double *d_spec = nullptr;
-  bool plan_ok = false;
-  cufftHandle plan = 0;
-  double *d_spec_part = nullptr;
-  unsigned long long *d_spec_cnt = nullptr;
-  double *d_spec_out = nullptr;
-  unsigned long long *d_spec_outc = nullptr;
-  int spec_nbins_cap = 0;
-
-  int fail(int code, const std::string &m)
-  {
-    err = m;
-    return code;
-  }
-  int cuda_fail(cudaError_t e, const char *where)
-  {
-    err = std::string(where) + ": " + cudaGetErrorString(e);
-    return CLB_ECUDA;
-  }
-};
 
 namespace {
 
-#define CLB_CHECK_LAUNCH(h, where)                                                                                     \
-  do {                                                                                                                 \
-    cudaError_t e_ = cudaGetLastError();                                                                               \
-    if (e_ != cudaSuccess) return (h)->cuda_fail(e_, where);                                                           \
-  } while (0)
 
 // Sweep geometry: bz x by (z, y) sites per block; the x direction is split so the grid holds about
 // two waves of resident blocks.
@@ -169,66 +102,6 @@ void setup_geometry(clb_handle *h, int blocks_per_sm)
 
 template <class R> R *F(clb_handle *h, int b) { return static_cast<R *>(h->fld[b]); }
 template <class R> R *P(clb_handle *h, int b) { return static_cast<R *>(h->pi[b]); }
-
-enum KKind { K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_SPECTRUM, K_NKINDS };
-const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
-                                          "scalar_drift",       "reduce_pi2",        "reduce_fields",
-                                          "tail",               "measure",           "convert",
-                                          "spectrum"};
-
-cudaEvent_t take_event(clb_handle *h)
-{
-  if (!h->ev_pool.empty()) {
-    cudaEvent_t e = h->ev_pool.back();
-    h->ev_pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e = nullptr;
-  cudaEventCreate(&e);
-  return e;
-}
-
-// Counts a launch and, when profiling, brackets it with events on the handle's stream.
-struct ProfScope {
-  clb_handle *h;
-  int kind;
-  cudaEvent_t a = nullptr;
-  ProfScope(clb_handle *hh, int k) : h(hh), kind(k)
-  {
-    ++h->launches[kind];
-    if (h->prof) {
-      a = take_event(h);
-      cudaEventRecord(a, h->stream);
-    }
-  }
-  ~ProfScope()
-  {
-    if (h->prof) {
-      cudaEvent_t b = take_event(h);
-      cudaEventRecord(b, h->stream);
-      h->pend.push_back({kind, a, b});
-    }
-  }
-};
-#define CLB_LAUNCH(h, kind, ...)                                                                                       \
-  do {                                                                                                                 \
-    ProfScope ps_((h), (kind));                                                                                        \
-    __VA_ARGS__;                                                                                                       \
-  } while (0)
-
-void collect_profile(clb_handle *h)
-{
-  for (auto &p : h->pend) {
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
-      h->kernel_ms[p.kind] += ms;
-      ++h->timed[p.kind];
-    }
-    h->ev_pool.push_back(p.a);
-    h->ev_pool.push_back(p.b);
-  }
-  h->pend.clear();
-}
 
 // ---- kernel launchers (templated on storage type and field count) ----------------------------
 template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
@@ -559,11 +432,16 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_EINVAL;
   }
   *out = nullptr;
-  if (md->kind != CLB_MODEL_LPHI4) {
+  const bool u1 = md->kind == CLB_MODEL_LPHI4U1;
+  if (md->kind != CLB_MODEL_LPHI4 && !u1) {
     g_err = "clb_create: unknown model kind";
     return CLB_EUNSUPPORTED;
   }
-  if (md->n_scalars < 1 || md->n_scalars > 2) {
+  if (u1 && cfg->precision != CLB_PREC_FP64) {
+    g_err = "clb_create: lphi4U1 runs in FP64 storage";
+    return CLB_EUNSUPPORTED;
+  }
+  if (!u1 && (md->n_scalars < 1 || md->n_scalars > 2)) {
     g_err = "clb_create: lphi4 supports 1 or 2 scalar singlets";
     return CLB_EUNSUPPORTED;
   }
@@ -609,6 +487,17 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   h->md = *md;
   h->N = cfg->N;
   h->n3 = (size_t)cfg->N * cfg->N * cfg->N;
+  if (u1) {
+    h->ws = ws;
+    const int r = u1_create(h);
+    if (r != CLB_OK) {
+      g_err = std::string("clb_create: device allocation failed: ") + cudaGetErrorString(cudaGetLastError());
+      clb_destroy(h);
+      return r;
+    }
+    *out = h;
+    return CLB_OK;
+  }
   h->NS = md->n_scalars;
   h->fp32 = cfg->precision == CLB_PREC_FP32_SPLIT;
   h->esz = h->fp32 ? sizeof(float) : sizeof(double);
@@ -697,6 +586,7 @@ void clb_destroy(clb_handle *h)
 {
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  u1_destroy(h);
   for (int b = 0; b < 2; ++b) {
     if (h->fld[b]) cudaFree(h->fld[b]);
     if (h->pi[b]) cudaFree(h->pi[b]);
@@ -735,6 +625,7 @@ int clb_num_components(const clb_handle *h, int32_t *nf, int32_t *np)
 int clb_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
 {
   if (!h || !fields || !momenta) return h ? h->fail(CLB_EINVAL, "clb_set_state: null argument") : CLB_EINVAL;
+  if (h->u1) return u1_set_state(h, fields, momenta, sf);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->cf = h->cp = 0;
@@ -786,6 +677,7 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
 int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
 {
   if (!h) return CLB_EINVAL;
+  if (h->u1) return u1_get_state(h, fields, momenta, sf);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
   DevState cur;
@@ -821,6 +713,11 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
 {
   if (!h) return CLB_EINVAL;
   if (!h->has_state) return h->fail(CLB_ESTATE, "clb_initialize: no state uploaded");
+  if (h->u1) {
+    const int r = u1_initialize(h, correct_adot);
+    if (r == CLB_OK) h->initialized = true;
+    return r;
+  }
   dispatch<Init>(h, (int)correct_adot);
   h->synced = true;
   int r = sync_and_check(h, "clb_initialize");
@@ -843,6 +740,11 @@ int clb_evolve(clb_handle *h, int64_t n)
     if (e == cudaSuccess) e = cudaMalloc(&h->d_hist, (size_t)n * kHistCols * sizeof(double));
     if (e != cudaSuccess) return h->fail(CLB_ENOMEM, std::string("clb_evolve: history buffer: ") + cudaGetErrorString(e));
     h->hist_cap = n;
+  }
+  if (h->u1) {
+    const int r = u1_evolve(h, n);
+    if (r == CLB_OK && h->cfg.expansion) h->hist_rows = n;
+    return r;
   }
   cudaEventRecord(h->ev_call[0], h->stream);
   if (h->cfg.evolver == CLB_LF)
@@ -922,6 +824,7 @@ int clb_sync(clb_handle *h)
 {
   if (!h) return CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_sync: call clb_initialize first");
+  if (h->u1) return u1_sync(h);
   if (h->cfg.evolver == CLB_LF) dispatch<SyncLF>(h);
   return sync_and_check(h, "clb_sync");
 }
@@ -930,6 +833,7 @@ int clb_measure(clb_handle *h, double e0, clb_measurement *m)
 {
   if (!h || !m) return h ? h->fail(CLB_EINVAL, "clb_measure: null argument") : CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_measure: call clb_initialize first");
+  if (h->u1) return u1_measure(h, e0, m);
   DevState s;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
@@ -1015,6 +919,7 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
 {
   if (!h) return CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_spectrum: call clb_initialize first");
+  if (h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_spectrum: scalar-singlet models only");
   if (which < 0 || which > 1 || comp < 0 || comp >= h->NS)
     return h->fail(CLB_EINVAL, "clb_spectrum: which must be 0 (field) or 1 (momentum) and comp a scalar index");
   if (ps_type < 1 || ps_type > 2) return h->fail(CLB_EINVAL, "powerSpectrumType " + std::to_string(ps_type) + " is not a valid powerSpectrumType.");

@@ -1,0 +1,448 @@
+// clb_u1.cuh - sm_100a kernels of the complex scalar + U(1) gauge sector (lphi4U1).
+//
+// Restates, in the reference's rounding order (every product and sum pinned with the _rn
+// intrinsics, so the FP64 path rounds where the reference's expression templates round):
+//   ComplexScalarKernels::get   evolvers/kernels/complexscalarkernels.h:28-35
+//   covLaplacianCS, U1 links    definitions/gaugederivatives.h:48-53, 92-102
+//   U1Kernels::get              evolvers/kernels/u1kernels.h:31-52
+//   U1Current, U1ChargeDensity  definitions/mattercurrents.h:27-76
+//   grad2CS, B2U1, pi2U1        definitions/fieldfunctionals.h:80-153
+//   GaussLaws::checkU1          definitions/gausslaws.h:34-53
+//   ScaleFactorKernels::get     evolvers/kernels/scalefactorkernels.h:27-80 (complex scalar and U(1) terms)
+//   Energies (CS, U(1))         definitions/energies.h:47-97, 217-239
+//   lphi4U1 potential           models/lphi4U1.h:117-129 (V = c4 |phi|^4, dV/d|phi| = 4 c4 |phi|^3)
+//
+// Layout: ten FP64 arrays of N^3 sites (x slowest, z fastest), fields then momenta, components
+// Re phi, Im phi, A_x, A_y, A_z.  Links U_i(x) = exp(-i dx gQ A_i(x)) are formed on the fly.
+
+#pragma once
+
+#include "clb_internal.cuh"
+
+namespace clb {
+
+constexpr int kU1Red = 7;   // kick-sweep partial slots (see k_u1_kick)
+constexpr int kU1Meas = 24; // measurement partial slots (see k_u1_measure)
+
+// Scale factor, cached volume averages (the reference's CSpi2AvI, U1pi2AvI, ... of abstractmodel.h)
+// and the per-sweep coefficients derived from them.
+struct U1State {
+  double aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
+  double csPi2I, csPi2SI, csPi2SIM, csGrad2I;
+  double u1Pi2I, u1Pi2SI, u1Pi2SIM, u1Mag2I;
+  double potI, potSI;
+  double cs_drift; // pow(aSI, alpha - 3)        (velocityverlet.h:195)
+  double u1_drift; // pow(aSI, alpha - 1)        (velocityverlet.h:207)
+  double kA;       // pow(aI, 1 + alpha)         (complexscalarkernels.h:33, u1kernels.h:45)
+  double kB2;      // pow(aI, 3 + alpha) / 2     (complexscalarkernels.h:34)
+  double kG;       // pow(aI, -1 + alpha)        (u1kernels.h:46)
+  int32_t status, pad;
+};
+
+struct U1Params {
+  int N;
+  size_t n3;
+  double dx, dx2, inv_dx2;
+  double ndxg;  // (-dx) gQ: link phase per unit A
+  double gQ, c4;
+  double J0;    // 2/dx (fStar/omegaStar)^2            (mattercurrents.h:29, 70)
+  double el0;   // 0.5 (omegaStar/fStar)^2             (energies.h:70, 80)
+  double alpha, fm2, dt, inv_n3;
+};
+
+// Kick factors of up to two successive kicks with the same kernel: complex scalar (dt/2 w, or
+// w dt on the leapfrog) and U(1) (dt w / 2) (velocityverlet.h:141-157, leapfrog.h:141-155).
+struct U1Kick {
+  double hc[2], hu[2];
+};
+
+__device__ __forceinline__ double u1_m(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double u1_a(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double u1_s(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double u1_d(double a, double b) { return __ddiv_rn(a, b); }
+
+// Periodic neighbour offsets of site s = (x N + y) N + z: op[d] to x + d, om[d] to x - d.
+__device__ __forceinline__ void u1_offsets(int N, size_t s, long long (&op)[3], long long (&om)[3])
+{
+  const int z = (int)(s % (size_t)N);
+  const size_t t = s / (size_t)N;
+  const int y = (int)(t % (size_t)N);
+  const int x = (int)(t / (size_t)N);
+  const int c[3] = {x, y, z};
+  const long long st[3] = {(long long)N * N, (long long)N, 1};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    op[d] = c[d] + 1 == N ? -(long long)(N - 1) * st[d] : st[d];
+    om[d] = c[d] == 0 ? (long long)(N - 1) * st[d] : -st[d];
+  }
+}
+
+// Per-site kernel values.  Fields f: [Re phi, Im phi, A_x, A_y, A_z] x n3.
+struct U1Site {
+  double fr, fi;            // phi(x)
+  double wr[3], wi[3];      // U_i(x) phi(x + i)
+  double g0[3][3];          // forwDiff(A_j, i)(x) = (A_j(x + i) - A_j(x)) / dx, [i][j]
+  double Kr, Ki;            // complex scalar kernel
+  double KA[3];             // U(1) kernel per direction
+  double nrm;               // |phi|
+};
+
+template <bool KERNEL>
+__device__ __forceinline__ void u1_site(const double *__restrict__ f, const U1Params &a, size_t s,
+                                        const long long (&op)[3], const long long (&om)[3], double kA, double kB2,
+                                        double kG, U1Site &o)
+{
+  const size_t n3 = a.n3;
+  const double *phr = f, *phi = f + n3;
+  const double *A[3] = {f + 2 * n3, f + 3 * n3, f + 4 * n3};
+  o.fr = phr[s];
+  o.fi = phi[s];
+  double pr = 0, pim = 0, mr = 0, mim = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const size_t sp = s + op[d];
+    double ur, ui;
+    sincos(u1_m(a.ndxg, A[d][s]), &ui, &ur);
+    const double gr = phr[sp], gi = phi[sp];
+    o.wr[d] = u1_s(u1_m(ur, gr), u1_m(ui, gi));
+    o.wi[d] = u1_a(u1_m(ur, gi), u1_m(ui, gr));
+    if (KERNEL) {
+      // conj(U_d(x - d)) phi(x - d)
+      const size_t sm = s + om[d];
+      double vr, vi;
+      sincos(u1_m(a.ndxg, A[d][sm]), &vi, &vr);
+      const double nvi = -vi, hr = phr[sm], hi = phi[sm];
+      const double cr = u1_s(u1_m(vr, hr), u1_m(nvi, hi));
+      const double ci = u1_a(u1_m(vr, hi), u1_m(nvi, hr));
+      if (d == 0) {
+        pr = o.wr[0];
+        pim = o.wi[0];
+        mr = cr;
+        mim = ci;
+      } else {
+        pr = u1_a(pr, o.wr[d]);
+        pim = u1_a(pim, o.wi[d]);
+        mr = u1_a(mr, cr);
+        mim = u1_a(mim, ci);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) o.g0[i][j] = u1_d(u1_s(A[j][s + op[i]], A[j][s]), a.dx);
+  o.nrm = sqrt(u1_a(u1_m(o.fr, o.fr), u1_m(o.fi, o.fi)));
+  if (!KERNEL) return;
+  // complex scalar: a^{1+alpha} covLap(phi) - a^{3+alpha}/2 (dV/d|phi|)/|phi| phi
+  const double clr = u1_d(u1_s(u1_a(pr, mr), u1_m(6.0, o.fr)), a.dx2);
+  const double cli = u1_d(u1_s(u1_a(pim, mim), u1_m(6.0, o.fi)), a.dx2);
+  const double nd = u1_m(a.c4, u1_m(4.0, u1_m(u1_m(o.nrm, o.nrm), o.nrm)));
+  const double q = u1_d(nd, o.nrm);
+  o.Kr = u1_s(u1_m(kA, clr), u1_m(kB2, u1_m(q, o.fr)));
+  o.Ki = u1_s(u1_m(kA, cli), u1_m(kB2, u1_m(q, o.fi)));
+  // U(1): a^{alpha-1} (lapl A_i - sum_j backDiff_j forwDiff_i A_j) - a^{1+alpha} J_i
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double c = A[i][s];
+    double t[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) t[d] = u1_s(u1_a(A[i][s + op[d]], A[i][s + om[d]]), u1_m(2.0, c));
+    const double lap = u1_m(a.inv_dx2, u1_a(u1_a(t[0], t[1]), t[2]));
+    double grad = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const size_t sj = s + om[j];
+      const size_t sij = i == j ? s : s + op[i] + om[j]; // x + i - j
+      const double g1 = u1_d(u1_s(A[j][sij], A[j][sj]), a.dx);
+      const double tj = u1_d(u1_s(o.g0[i][j], g1), a.dx);
+      grad = j == 0 ? tj : u1_a(grad, tj);
+    }
+    const double im = u1_s(u1_m(o.wr[i], o.fi), u1_m(o.wi[i], o.fr));
+    const double J = u1_m(a.J0, u1_m(a.gQ, im));
+    o.KA[i] = u1_s(u1_m(kG, u1_s(lap, grad)), u1_m(kA, J));
+  }
+}
+
+// sum_j |D+_j phi|^2 (fieldfunctionals.h:80-84) from the site's covariant neighbours
+__device__ __forceinline__ double u1_cs_grad2(const U1Site &o, double dx)
+{
+  double acc = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double dr = u1_d(u1_s(o.wr[j], o.fr), dx), di = u1_d(u1_s(o.wi[j], o.fi), dx);
+    const double n2 = u1_a(u1_m(dr, dr), u1_m(di, di));
+    acc = j == 0 ? n2 : u1_a(acc, n2);
+  }
+  return acc;
+}
+
+// F_21^2 + (F_31^2 + F_32^2), F_ij = forwDiff(A_j, i) - forwDiff(A_i, j) (fieldfunctionals.h:133-141)
+__device__ __forceinline__ double u1_b2(const U1Site &o)
+{
+  const double f21 = u1_s(o.g0[1][0], o.g0[0][1]);
+  const double f31 = u1_s(o.g0[2][0], o.g0[0][2]);
+  const double f32 = u1_s(o.g0[2][1], o.g0[1][2]);
+  return u1_a(u1_m(f21, f21), u1_a(u1_m(f31, f31), u1_m(f32, f32)));
+}
+
+__device__ __forceinline__ double u1_pot(const U1Site &o, double c4)
+{
+  return u1_m(c4, u1_m(u1_m(u1_m(o.nrm, o.nrm), o.nrm), o.nrm));
+}
+
+// Kick sweep: NK (0, 1 or 2) successive in-place kicks of all five momenta with the kernel at the
+// current fields.  Partials per block: [0,1] complex-scalar |pi|^2 and U(1) sum pi_i^2 after the
+// first kick (or of the momenta as they are, NK = 0), [2] sum |D phi|^2, [3] B^2, [4] V, [5,6] the
+// momentum sums after the second kick.  RF adds the field slots, RP the momentum slots.
+template <int NK, bool RF, bool RP>
+__global__ void __launch_bounds__(256)
+    k_u1_kick(const double *__restrict__ f, double *__restrict__ p, U1Params a, U1Kick kc,
+              const U1State *__restrict__ st, double *__restrict__ partials)
+{
+  __shared__ double smem[(256 / 32) * kU1Red];
+  const size_t n3 = a.n3;
+  const double kA = st->kA, kB2 = st->kB2, kG = st->kG;
+  double acc[kU1Red];
+#pragma unroll
+  for (int k = 0; k < kU1Red; ++k) acc[k] = 0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    long long op[3], om[3];
+    u1_offsets(a.N, s, op, om);
+    U1Site o;
+    u1_site<(NK > 0)>(f, a, s, op, om, kA, kB2, kG, o);
+    if (RF) {
+      acc[2] += u1_cs_grad2(o, a.dx);
+      acc[3] += u1_b2(o);
+      acc[4] += u1_pot(o, a.c4);
+    }
+    double q[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) q[c] = p[c * n3 + s];
+#pragma unroll
+    for (int k = 0; k < (NK > 0 ? NK : 1); ++k) {
+      if (NK > 0) {
+        q[0] = u1_a(q[0], u1_m(kc.hc[k], o.Kr));
+        q[1] = u1_a(q[1], u1_m(kc.hc[k], o.Ki));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) q[2 + i] = u1_a(q[2 + i], u1_m(kc.hu[k], o.KA[i]));
+      }
+      if (RP) {
+        acc[k == 0 ? 0 : 5] += u1_a(u1_m(q[0], q[0]), u1_m(q[1], q[1]));
+        acc[k == 0 ? 1 : 6] += u1_a(u1_a(u1_m(q[2], q[2]), u1_m(q[3], q[3])), u1_m(q[4], q[4]));
+      }
+    }
+    if (NK > 0) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) p[c * n3 + s] = q[c];
+    }
+  }
+  if (RF || RP) {
+    block_reduce<kU1Red, 256>(acc, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < kU1Red; ++k) partials[(size_t)blockIdx.x * kU1Red + k] = acc[k];
+    }
+  }
+}
+
+// Drifts phi += ((pow(aSI, alpha-3) dt) w) pi_phi and A += ((pow(aSI, alpha-1) w) dt) pi_A
+// (velocityverlet.h:193-210; the leapfrog's forms leapfrog.h:203-217 are w = 1).
+__global__ void __launch_bounds__(256)
+    k_u1_drift(double *__restrict__ f, const double *__restrict__ p, size_t n3, double w, double dt,
+               const U1State *__restrict__ st)
+{
+  const double cc = u1_m(u1_m(st->cs_drift, dt), w);
+  const double cu = u1_m(u1_m(st->u1_drift, w), dt);
+  const size_t n = 5 * n3, n2 = 2 * n3;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    f[i] = u1_a(f[i], u1_m(i < n2 ? cc : cu, p[i]));
+}
+
+// ScaleFactorKernels::get with complex-scalar and U(1) energies (scalefactorkernels.h:73-77,
+// energies.h:47-97).
+__device__ __forceinline__ double u1_sf_kernel(const U1State &s, const U1Params &p)
+{
+  const double al = p.alpha;
+  const double e4 = u1_m(p.el0, ipow_d(s.aI, -4));
+  const double Ekcs = u1_m(s.csPi2I, ipow_d(s.aI, -6));
+  const double Egcs = u1_m(s.csGrad2I, ipow_d(s.aI, -2));
+  const double Eel = u1_m(e4, s.u1Pi2I), Emag = u1_m(e4, s.u1Mag2I);
+  const double br = u1_a(u1_a(u1_a(u1_m(al - 2, Ekcs), u1_m(al, Egcs)), u1_m(al - 1, u1_a(Eel, Emag))),
+                         u1_m(al + 1, s.potI));
+  return u1_m(u1_m(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
+}
+
+// Second momentum slots of a two-kick sweep become the cached <pi^2> (after T_VV_KICK_HALF).
+constexpr uint32_t T_STORE_PI2_B = 1u << 13;
+
+// One-thread tail: fixed-order sum of the kick-sweep partials and the scale-factor update, in
+// the order of the VelocityVerlet and LeapFrog schedules (same flags as the scalar tail).
+__global__ void __launch_bounds__(256)
+    k_u1_tail(const double *__restrict__ partials, TailOp op, U1State *__restrict__ st, U1Params p)
+{
+  __shared__ double smem[(256 / 32) * kU1Red];
+  double v[kU1Red];
+#pragma unroll
+  for (int k = 0; k < kU1Red; ++k) v[k] = 0;
+  if (op.nblocks > 0) {
+    for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x) {
+#pragma unroll
+      for (int k = 0; k < kU1Red; ++k) v[k] += partials[(size_t)b * kU1Red + k];
+    }
+    block_reduce<kU1Red, 256>(v, smem);
+  }
+  if (threadIdx.x != 0) return;
+  U1State s = *st;
+  const double csP = v[0] * p.inv_n3, u1P = v[1] * p.inv_n3, csG = v[2] * p.inv_n3, u1B = v[3] * p.inv_n3;
+  const double pot = v[4] * p.inv_n3, csP2 = v[5] * p.inv_n3, u1P2 = v[6] * p.inv_n3;
+  const double dt = p.dt;
+  const uint32_t fl = op.flags;
+  if (fl & T_STORE_ALL) { // Averages::setAllAverages (averages.h:349-378)
+    s.potI = s.potSI = pot;
+    s.u1Pi2I = s.u1Pi2SI = u1P;
+    s.u1Mag2I = u1B;
+    s.csPi2I = s.csPi2SI = csP;
+    s.csGrad2I = csG;
+  }
+  auto write_hist = [&]() {
+    double *r = op.hist + op.hist_row * kHistCols;
+    r[0] = s.aI;
+    r[1] = s.aDotI;
+    r[2] = s.csPi2I;
+    r[3] = s.csGrad2I;
+    r[4] = s.potI;
+  };
+  const bool hist = op.hist != nullptr && op.hist_row >= 0;
+  if (fl & T_STORE_FIELDS) {
+    s.csGrad2I = csG;
+    s.u1Mag2I = u1B;
+    s.potI = pot;
+  }
+  if (hist && (fl & T_HIST_EARLY)) write_hist();
+  if (fl & T_STORE_PI2_I) {
+    s.csPi2I = csP;
+    s.u1Pi2I = u1P;
+  }
+  if (fl & T_STORE_PI2_LF) { // leapfrog.h:152-167
+    s.csPi2SIM = s.csPi2SI;
+    s.csPi2SI = csP;
+    s.csPi2I = 0.5 * (s.csPi2SIM + s.csPi2SI);
+    s.u1Pi2SIM = s.u1Pi2SI;
+    s.u1Pi2SI = u1P;
+    s.u1Pi2I = 0.5 * (s.u1Pi2SIM + s.u1Pi2SI);
+  }
+  if (fl & T_CORRECT_ADOT) { // HubbleConstraint::get RHS with Energies::rho (energies.h:217-239)
+    const double e4 = u1_m(p.el0, ipow_d(s.aI, -4));
+    const double rho = u1_a(u1_a(u1_a(u1_a(u1_m(s.csPi2I, ipow_d(s.aI, -6)), u1_m(s.csGrad2I, ipow_d(s.aI, -2))),
+                                      u1_m(e4, s.u1Pi2I)),
+                                 u1_m(e4, s.u1Mag2I)),
+                            s.potI);
+    s.aDotI = sqrt(u1_m(u1_m(pow(s.aI, 2 * p.alpha + 2) / 3., p.fm2), rho));
+  }
+  if (fl & T_VV_KICK_ONE) s.aDotI = u1_a(s.aDotSI, u1_m(u1_m(dt / 2, u1_sf_kernel(s, p)), op.w));
+  if (hist && !(fl & T_HIST_EARLY)) write_hist();
+  if (fl & T_LF_SYNC) s.aDotI = u1_a(s.aDotSI, u1_m(dt / 2.0, u1_sf_kernel(s, p)));
+  if (fl & T_LF_CTOR) s.aDotSI = u1_s(s.aDotI, u1_m(dt / 2.0, u1_sf_kernel(s, p)));
+  if (fl & T_LF_KICK) {
+    s.aDotSIM = s.aDotSI;
+    s.aDotSI = u1_a(s.aDotSI, u1_m(dt, u1_sf_kernel(s, p)));
+    s.aDotI = (s.aDotSIM + s.aDotSI) / 2.0;
+  }
+  if (fl & T_LF_DRIFT) {
+    s.aIM = s.aI;
+    s.aI = u1_a(s.aI, u1_m(dt, s.aDotSI));
+    s.aSI = (s.aIM + s.aI) / 2.0;
+  }
+  if (fl & T_VV_KICK_HALF) s.aDotSI = u1_a(s.aDotI, u1_m(u1_m(dt / 2, u1_sf_kernel(s, p)), op.w2));
+  if (fl & T_STORE_PI2_B) {
+    s.csPi2I = csP2;
+    s.u1Pi2I = u1P2;
+  }
+  if (fl & T_VV_DRIFT) {
+    s.aIM = s.aI;
+    s.aI = u1_a(s.aI, u1_m(u1_m(dt, s.aDotSI), op.w2));
+    s.aSI = (s.aIM + s.aI) / 2.0;
+  }
+  s.cs_drift = pow(s.aSI, p.alpha - 3);
+  s.u1_drift = pow(s.aSI, p.alpha - 1);
+  s.kA = pow(s.aI, 1 + p.alpha);
+  s.kB2 = pow(s.aI, 3 + p.alpha) / 2;
+  s.kG = pow(s.aI, -1 + p.alpha);
+  if (!isfinite(s.aI) || !isfinite(s.aDotI) || !isfinite(s.aDotSI) || !isfinite(s.csPi2I) || !isfinite(s.u1Pi2I) ||
+      !isfinite(s.csGrad2I) || !isfinite(s.u1Mag2I) || !isfinite(s.potI))
+    s.status = 1;
+  *st = s;
+}
+
+// Measurement sums (one sweep): [0] |pi_phi|^2, [1] sum |D phi|^2, [2] sum pi_A^2, [3] B^2, [4] V,
+// [5..10] Re phi, (Re phi)^2, Im phi, (Im phi)^2, |phi|, |phi|^2, [11..16] the same of pi_phi,
+// [17] |pi_A|, [18] |B|, [19..22] Gauss |LHS - RHS|, |sum of squares|, |RHS|, |LHS|
+// (gausslaws.h:34-53 with U1ChargeDensity, mattercurrents.h:27-48).
+__global__ void __launch_bounds__(256)
+    k_u1_measure(const double *__restrict__ f, const double *__restrict__ p, U1Params a, double *__restrict__ partials)
+{
+  __shared__ double smem[(256 / 32) * kU1Meas];
+  const size_t n3 = a.n3;
+  double acc[kU1Meas];
+#pragma unroll
+  for (int k = 0; k < kU1Meas; ++k) acc[k] = 0;
+  const double gnorm = u1_m(a.J0, a.gQ);
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    long long op[3], om[3];
+    u1_offsets(a.N, s, op, om);
+    U1Site o;
+    u1_site<false>(f, a, s, op, om, 0, 0, 0, o);
+    const double pr = p[s], pi = p[n3 + s];
+    double q[3], l[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      q[i] = p[(2 + i) * n3 + s];
+      l[i] = u1_s(q[i], p[(2 + i) * n3 + s + om[i]]);
+    }
+    const double cp2 = u1_a(u1_m(pr, pr), u1_m(pi, pi));
+    const double up2 = u1_a(u1_a(u1_m(q[0], q[0]), u1_m(q[1], q[1])), u1_m(q[2], q[2]));
+    const double b2 = u1_b2(o);
+    acc[0] += cp2;
+    acc[1] += u1_cs_grad2(o, a.dx);
+    acc[2] += up2;
+    acc[3] += b2;
+    acc[4] += u1_pot(o, a.c4);
+    acc[5] += o.fr;
+    acc[6] += u1_m(o.fr, o.fr);
+    acc[7] += o.fi;
+    acc[8] += u1_m(o.fi, o.fi);
+    acc[9] += o.nrm;
+    acc[10] += u1_m(o.nrm, o.nrm);
+    const double pn = sqrt(cp2);
+    acc[11] += pr;
+    acc[12] += u1_m(pr, pr);
+    acc[13] += pi;
+    acc[14] += u1_m(pi, pi);
+    acc[15] += pn;
+    acc[16] += u1_m(pn, pn);
+    acc[17] += sqrt(up2);
+    // |B| with B_1 = F_32, B_2 = F_13, B_3 = F_21
+    {
+      const double b1 = u1_s(o.g0[2][1], o.g0[1][2]), bb = u1_s(o.g0[0][2], o.g0[2][0]), b3 = u1_s(o.g0[1][0], o.g0[0][1]);
+      acc[18] += sqrt(u1_a(u1_a(u1_m(b1, b1), u1_m(bb, bb)), u1_m(b3, b3)));
+    }
+    // Gauss: LHS = sum_i (pi_i(x) - pi_i(x - i)) / dx, RHS = -dx rho, rho = (J0 gQ) Im(conj(pi_phi) phi)
+    const double LHS = u1_d(u1_a(u1_a(l[0], l[1]), l[2]), a.dx);
+    const double im = u1_s(u1_m(pr, o.fi), u1_m(pi, o.fr));
+    const double RHS = u1_m(-a.dx, u1_m(gnorm, im));
+    const double L1 = u1_d(l[0], a.dx), L2 = u1_d(l[1], a.dx), L3 = u1_d(l[2], a.dx);
+    const double diff = u1_s(LHS, RHS);
+    const double sum = u1_a(u1_a(u1_a(u1_m(L1, L1), u1_m(L2, L2)), u1_m(L3, L3)), u1_m(RHS, RHS));
+    acc[19] += fabs(diff);
+    acc[20] += fabs(sum);
+    acc[21] += fabs(RHS);
+    acc[22] += fabs(LHS);
+  }
+  block_reduce<kU1Meas, 256>(acc, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < kU1Meas; ++k) partials[(size_t)blockIdx.x * kU1Meas + k] = acc[k];
+  }
+}
+
+} // namespace clb

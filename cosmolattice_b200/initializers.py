@@ -49,6 +49,9 @@ def initial_scale_factor(model: Model, rp: RunParameters):
     for i in range(model.Ns):
         # Energies::kineticS with the default a = 1 in force at that point
         kin += 0.5 * (model.piS0[i] / model.fStar / model.omegaStar) ** 2
+    for c in getattr(model, "piCS0", []) if getattr(model, "NCs", 0) else []:
+        # Energies::kineticCS: |pi|^2 with no 1/2 (energies.h:47-50)
+        kin += (c / model.fStar / model.omegaStar) ** 2
     rho = kin + model.pot0
     return rp.a0, model.fStar / model.MPl * math.sqrt(rho / 3.0)
 
@@ -93,3 +96,91 @@ def scalar_initial_state(model: Model, rp: RunParameters):
         fields[f] = phi + model.fldS0[f] / model.fStar
         momenta[f] = pi + model.piS0[f] / model.fStar / model.omegaStar
     return fields, momenta, aI, aDot
+
+
+def _fluct_norm(model: Model, rp: RunParameters, k, m2):
+    """FluctuationsGenerator::getFluctuationsNorm in 3-D (fluctuationsgenerator.h:39-65)."""
+    omega = np.sqrt(k * k + (m2 if m2 > 0 else 0.0))
+    amp = model.omegaStar / model.fStar if model.fluct_amplitude is None else model.fluct_amplitude
+    with np.errstate(divide="ignore", invalid="ignore"):
+        norm = np.where(k <= rp.kCutoff, amp * (rp.lSide / rp.dx ** 2) ** 1.5 * (2 * omega) ** -0.5 / math.sqrt(2.0), 0.0)
+    norm[0, 0, 0] = 0.0
+    return norm, omega
+
+
+def complex_scalar_fluctuations(model: Model, rp: RunParameters, aDot: float):
+    """U1Initializer::addFluctuationsCScalarFromPhases (u1initializer.h:157-230): per component
+    Rayleigh amplitudes a_c, three uniform phases and the fourth fixed by
+    e11 = e01 e10 conj(e00) so the initial charge density follows from the amplitudes; modes
+    phi_c = a_c (e_c0 + e_c1)/2, pi_c = -i omega a_c (e_c0 - e_c1)/2 - aDot phi_c, zero modes 0."""
+    N = rp.N
+    nx, ny, nz = wave_numbers(N)
+    k = np.sqrt(nx * nx + ny * ny + nz * nz) * rp.kIR
+    out_f, out_p = [], []
+    norms = [_fluct_norm(model, rp, k, model.masses2CS[c]) for c in range(2)]
+    omega0 = norms[0][1]
+    shape = norms[0][0].shape
+
+    def rayleigh(label):
+        g = _rng(rp.baseSeed, label)
+        return np.sqrt(-2.0 * np.log1p(-g.random(shape)))
+
+    def phase(label):
+        g = _rng(rp.baseSeed, label)
+        return np.exp(2j * np.pi * g.random(shape))
+
+    e00, e01, e10 = phase("phase00cmplx_0_0"), phase("phase01cmplx_0_0"), phase("phase10cmplx_0_1")
+    e11 = e01 * e10 * np.conj(e00)
+    for c, (ea, eb) in enumerate(((e00, e01), (e10, e11))):
+        a = norms[c][0] * rayleigh(f"norm{c}cmplx_0_{c}")
+        fk = a * (ea + eb) / 2.0
+        fk[0, 0, 0] = 0.0
+        pk = -1j * omega0 * a * (ea - eb) / 2.0 - aDot * fk
+        pk[0, 0, 0] = 0.0
+        out_f.append(sfft.irfftn(fk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
+        out_p.append(sfft.irfftn(pk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
+    return out_f, out_p
+
+
+def gauss_momenta_u1(model: Model, rp: RunParameters, phi, pi):
+    """pi_A from the Gauss constraint in momentum space with A = 0 (u1initializer.h:90-114):
+    j0 = -dx^2 rho, pi_i(k) = conj(1 - e^{-2 pi i n_i/N}) / sum_j |1 - e^{-2 pi i n_j/N}|^2 j0(k),
+    zero mode 0; rho = 2/dx (fStar/omegaStar)^2 gQ Im(conj(pi_phi) phi) (mattercurrents.h:27-48)."""
+    N = rp.N
+    rho = 2.0 / rp.dx * (model.fStar / model.omegaStar) ** 2 * model.gQ * (pi[0] * phi[1] - pi[1] * phi[0])
+    j0 = sfft.rfftn(-rp.dx ** 2 * rho, axes=(0, 1, 2), workers=-1)
+    nx, ny, nz = wave_numbers(N)
+    keff = [1.0 - np.exp(-2j * np.pi * n / N) for n in (nx, ny, nz)]
+    k2 = sum(np.abs(q) ** 2 for q in keff)
+    k2 = np.broadcast_to(k2, j0.shape).copy()
+    k2[0, 0, 0] = 1.0
+    out = []
+    for q in keff:
+        pk = np.conj(q) / k2 * j0
+        pk[0, 0, 0] = 0.0
+        out.append(sfft.irfftn(pk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
+    return out
+
+
+def u1_initial_state(model: Model, rp: RunParameters):
+    """lphi4U1 state (5 x N^3 fields and momenta: Re phi, Im phi, A_x, A_y, A_z) by the
+    RandomWithMatter recipe (u1initializer.h:77-117) and the initial (aI, aDotI)."""
+    aI, aDot = initial_scale_factor(model, rp)
+    N = rp.N
+    fields = np.zeros((5, N, N, N), dtype=np.float64)
+    momenta = np.zeros_like(fields)
+    fl, pl = complex_scalar_fluctuations(model, rp, aDot)
+    for c in range(2):
+        fields[c] = fl[c] + model.fldCS0[c] / model.fStar
+        momenta[c] = pl[c] + model.piCS0[c] / model.fStar / model.omegaStar
+    pa = gauss_momenta_u1(model, rp, fields[:2], momenta[:2])
+    for i in range(3):
+        momenta[2 + i] = pa[i]
+    return fields, momenta, aI, aDot
+
+
+def initial_state(model: Model, rp: RunParameters):
+    """Initial state of any supported model (ModelInitializer::initialize, modelinitializer.h:47-81)."""
+    if getattr(model, "NU1", 0):
+        return u1_initial_state(model, rp)
+    return scalar_initial_state(model, rp)

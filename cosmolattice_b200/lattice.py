@@ -14,7 +14,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _capi
-from .initializers import scalar_initial_state
+from .initializers import initial_state
 from .models import Model
 from .params import RunParameters
 
@@ -154,6 +154,7 @@ def measurement_to_dict(m: _capi.Measurement) -> Dict[str, object]:
         "energies": [m.energies[i] for i in range(m.n_energies)],
         "friedmann": [m.friedmann[i] for i in range(3)],
         "means": [[m.means[f][j] for j in range(6)] for f in range(m.n_means)],
+        "gauss_u1": [m.gauss_u1[i] for i in range(3)],
     }
 
 
@@ -164,7 +165,7 @@ class ModelInitializer:
         self.model = model
 
     def initialize(self, model: Model, rp: RunParameters, lattice: Lattice) -> None:
-        fields, momenta, aI, aDot = scalar_initial_state(model, rp)
+        fields, momenta, aI, aDot = initial_state(model, rp)
         lattice.set_state(fields, momenta, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aDot, "aDotSI": aDot})
         lattice.initialize(correct_adot=True)
 
@@ -202,19 +203,36 @@ class Measurer:
         if self.outdir:
             os.makedirs(self.outdir, exist_ok=True)
 
+    def _mean_files(self):
+        """Names of the per-field means files, in the order of the measurement's means rows
+        (scalarsingletmeasurer.h, complexscalarmeasurer.h:40-52, u1measurer.h:45-55)."""
+        m = self.model
+        if getattr(m, "NU1", 0):
+            return ["cmplx_scalar_0_0", "cmplx_scalar_0_1", "norm_cmplx_scalar_0", "norm_U1_0"]
+        return [f"scalar_{i}" for i in range(m.Ns)]
+
     def _headers(self):
         m = self.model
         en = ["t"]
         for i in range(m.Ns):
             en += [f"E^kin_scal{i}", f"E^grad_scal{i}"]
+        for i in range(getattr(m, "NCs", 0)):
+            en += [f"E^kin_cmplxscal{i}", f"E^grad_cmplxscal{i}"]
+        for i in range(getattr(m, "NU1", 0)):
+            en += [f"E^kin_U1{i}", f"E^grad_U1{i}"]
         en += [f"Vpot_term_{k}" for k in range(m.NPotTerms)] + ["E_tot"]
         cons = ["t"] + (["rel_diff_friedmann", "LHS_friedmann", "RHS_friedmann"] if self.rp.expansion else ["energy_cons"])
-        return {
+        means = ["t", "<phi>", "<pi>", "<phi^2>", "<pi^2>", "rms(phi)", "rms(pi)"]
+        means_eb = ["t", "<|E|>", "<|B|>", "<|E|^2>", "<|B|^2>", "rms(|E|)", "rms(|B|)"]
+        h = {
             "energies": en,
             "energy_conservation": cons,
             "scale_factor": ["t", "a", "aDot", "H"],
-            **{f"scalar_{i}": ["t", "<phi>", "<pi>", "<phi^2>", "<pi^2>", "rms(phi)", "rms(pi)"] for i in range(m.Ns)},
+            **{name: (means_eb if name.startswith("norm_U1") else means) for name in self._mean_files()},
         }
+        if getattr(m, "NU1", 0):
+            h["gauss_U1_0"] = ["t", "av|LHS-RHS|_over_av|LHS+RHS|", "av|LHS|", "av|RHS|"]
+        return h
 
     def _write(self, name: str, values: List[float]) -> None:
         if not self.outdir:
@@ -249,8 +267,10 @@ class Measurer:
         self._write("energy_conservation", [t] + (m["friedmann"] if self.rp.expansion else m["friedmann"][:1]))
         if self.rp.expansion:
             self._write("scale_factor", [t, m["aI"], m["aDotI"], m["hubble"]])
-        for i, row in enumerate(m["means"]):
-            self._write(f"scalar_{i}", [t] + row)
+        for name, row in zip(self._mean_files(), m["means"]):
+            self._write(name, [t] + row)
+        if getattr(self.model, "NU1", 0):
+            self._write("gauss_U1_0", [t] + m["gauss_u1"])
         return m
 
     def close(self) -> None:

@@ -187,4 +187,67 @@ class lphi4_1f(lphi4):
     NPotTerms = 1
 
 
-MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f}
+class lphi4U1(Model):
+    """models/lphi4U1.h: one complex scalar charged under one U(1), V = |phi|^4 in program variables.
+
+    Keys: lambda, cmplx_field_initial_norm (GeV), cmplx_momentum_initial_norm (GeV^2, default 0),
+    gU1s (default 1) and CSU1_charges (default 1) (complexscalarbase.h:71-72), lambda_prog (default
+    1, multiplies the quartic term in program units).  Rescaling (lphi4U1.h:95-97): alpha = 1,
+    fStar = |phi_0|, omegaStar = sqrt(lambda) |phi_0|.  The homogeneous norm is split equally over
+    the two components (lphi4U1.h:75-76).  Components on the device: Re phi, Im phi, A_x, A_y, A_z.
+    """
+
+    name = "lphi4U1"
+    kind = _capi.MODEL_LPHI4U1
+    Ns = 0
+    NCs = 1
+    NU1 = 1
+    NPotTerms = 1
+    n_components = 5
+
+    def __init__(self, par: ParameterParser, rp: RunParameters):
+        super().__init__(par, rp)
+        self.lam = par.get_float("lambda")
+        self.c4 = par.get_float("lambda_prog", 1.0)
+        n0 = par.get_float("cmplx_field_initial_norm")
+        np0 = par.get_float("cmplx_momentum_initial_norm", 0.0)
+        self.fldCS0 = [n0 / math.sqrt(2.0), n0 / math.sqrt(2.0)]
+        self.piCS0 = [np0 / math.sqrt(2.0), np0 / math.sqrt(2.0)]
+        self.cm = CouplingsManager([[True]])
+        g = par.get_floats("gU1s", 1, [1.0])
+        q = par.get_floats("CSU1_charges", 1, [1.0])
+        self.cm.set_effective_charges(q, g)
+        self.gQ = self.cm(0, 0)
+        self.alpha = 1.0
+        self.fStar = n0
+        self.omegaStar = math.sqrt(self.lam) * n0
+        if par.has("fluct_amplitude"):
+            self.fluct_amplitude = par.get_float("fluct_amplitude")
+        self.set_initial_potential_and_masses_from_potential()
+
+    def potential_terms(self, k, phi):
+        return self.c4 * (phi[0] ** 2 + phi[1] ** 2) ** 2
+
+    def pot_deriv_norm(self, nrm):
+        return self.c4 * 4 * nrm ** 3
+
+    def pot_deriv2_norm(self, nrm):
+        return self.c4 * 12 * nrm ** 2
+
+    def set_initial_potential_and_masses_from_potential(self) -> None:
+        """abstractmodel.h:220-248 with deriv2ComponentFromNorm (potential.h:36-42); a zero
+        condensate is evaluated at |phi| = 1e-14 (abstractmodel.h:282)."""
+        phi = [v / self.fStar for v in self.fldCS0]
+        if phi[0] == 0 and phi[1] == 0:
+            phi = [1e-14 * 0.70710678118654752] * 2
+        n2 = phi[0] ** 2 + phi[1] ** 2
+        n = math.sqrt(n2)
+        nd, nd2 = self.pot_deriv_norm(n), self.pot_deriv2_norm(n)
+        self.pot0 = self.potential_terms(0, [v / self.fStar for v in self.fldCS0])
+        self.masses2CS = [1.0 / n2 * nd2 * c ** 2 + nd / n * (1 - c ** 2 / n2) for c in phi]
+
+    def couplings(self):
+        return [self.c4, self.gQ]
+
+
+MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f, "lphi4U1": lphi4U1}

@@ -57,6 +57,11 @@ extern "C" {
  *                       with c[0] = 1 and c[1] = q reproducing the reference header exactly).
  */
 #define CLB_MODEL_LPHI4 1
+/*   CLB_MODEL_LPHI4U1 : one complex scalar charged under one U(1) gauge field (models/lphi4U1.h),
+ *                       V = c[0] |phi|^4 (c[0] = 1 is the reference header), c[1] = g Q, the effective
+ *                       charge (CouplingsManager, couplingsmanager.h:167-218).  Components, fields and
+ *                       momenta alike: Re phi, Im phi, A_1, A_2, A_3 (program units; n_scalars = 0). */
+#define CLB_MODEL_LPHI4U1 2
 
 #define CLB_MAX_COUPLINGS 8
 
@@ -97,7 +102,11 @@ typedef struct clb_scalefactor {
  *  friedmann[] holds (LHS-RHS)/(LHS+RHS), LHS, RHS with expansion (hubbleconstraint.h:27-36), or
  *  energy_cons = |1 - E/E0| in friedmann[0] without expansion (energiesmeasurer.h:116-118).
  *  means[f][] per scalar singlet: <phi>, <dphi/dt>, <phi^2>, <(dphi/dt)^2>, rms(phi), rms(dphi/dt)
- *  with dphi/dt = a^(alpha-3) pi (meansmeasurer.h:28-48, scalarsingletmeasurer.h:61-66). */
+ *  with dphi/dt = a^(alpha-3) pi (meansmeasurer.h:28-48, scalarsingletmeasurer.h:61-66).
+ *  For CLB_MODEL_LPHI4U1 the rows are: sqrt2 Re phi, sqrt2 Im phi, |phi| (with their momenta
+ *  a^(alpha-3) pi), then |E| = |a^(alpha-1) pi_A| and |B| (complexscalarmeasurer.h:61-72,
+ *  u1measurer.h:78-87); energies: E^kin_cmplxscal0, E^grad_cmplxscal0, E^kin_U10, E^grad_U10, <V>,
+ *  E_tot (energiesmeasurer.h:62-90). */
 typedef struct clb_measurement {
   double aI, aDotI, hubble;            /* scalefactormeasurer.h:37-48 */
   int32_t n_energies;
@@ -105,6 +114,8 @@ typedef struct clb_measurement {
   double friedmann[3];
   int32_t n_means;
   double means[CLB_MAX_MEANS][6];
+  /* GaussLaws::checkU1 (gausslaws.h:34-53): av|LHS-RHS| / av|LHS^2 sum + RHS^2|, av|LHS|, av|RHS| */
+  double gauss_u1[3];
 } clb_measurement;
 
 typedef struct clb_handle clb_handle;

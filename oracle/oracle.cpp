@@ -23,6 +23,7 @@
 // are added in x order, independent of the OpenMP thread count.
 
 #include "../include/clb200.h"
+#include "oracle_models.h"
 
 #include <cmath>
 #include <cstdio>
@@ -320,6 +321,15 @@ struct Oracle {
 
 thread_local std::string g_err;
 
+// Every orc_handle is a Handle: the scalar oracle above or a gauge-sector oracle (oracle_models.h).
+struct Handle {
+  int kind;
+  void *impl;
+};
+inline Handle *H(void *h) { return reinterpret_cast<Handle *>(h); }
+inline bool isU1(void *h) { return H(h)->kind == CLB_MODEL_LPHI4U1; }
+inline Oracle *S(void *h) { return reinterpret_cast<Oracle *>(H(h)->impl); }
+
 } // namespace
 
 extern "C" {
@@ -328,12 +338,19 @@ typedef struct orc_handle orc_handle;
 
 const char *orc_last_error(orc_handle *h)
 {
-  return h ? reinterpret_cast<Oracle *>(h)->err.c_str() : g_err.c_str();
+  if (!h) return g_err.c_str();
+  return isU1(h) ? oracle_models::u1_err(H(h)->impl).c_str() : S(h)->err.c_str();
 }
 
 int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out)
 {
   if (!cfg || !md || !out) { g_err = "null argument"; return CLB_EINVAL; }
+  if (md->kind == CLB_MODEL_LPHI4U1) {
+    void *u = oracle_models::u1_create(cfg, md, g_err);
+    if (!u) return CLB_EINVAL;
+    *out = reinterpret_cast<orc_handle *>(new Handle{CLB_MODEL_LPHI4U1, u});
+    return CLB_OK;
+  }
   if (md->kind != CLB_MODEL_LPHI4 || md->n_scalars < 1 || md->n_scalars > 2) {
     g_err = "oracle: only lphi4 with 1 or 2 scalar singlets";
     return CLB_EUNSUPPORTED;
@@ -351,15 +368,24 @@ int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out
     o->ws = vvCoeffs(cfg->evolver);
     if (o->ws.empty()) { delete o; g_err = "unsupported evolver"; return CLB_EUNSUPPORTED; }
   }
-  *out = reinterpret_cast<orc_handle *>(o);
+  *out = reinterpret_cast<orc_handle *>(new Handle{CLB_MODEL_LPHI4, o});
   return CLB_OK;
 }
 
-void orc_destroy(orc_handle *h) { delete reinterpret_cast<Oracle *>(h); }
+void orc_destroy(orc_handle *h)
+{
+  if (!h) return;
+  if (isU1(h))
+    oracle_models::u1_destroy(H(h)->impl);
+  else
+    delete S(h);
+  delete H(h);
+}
 
 int orc_set_state(orc_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_set_state(H(h)->impl, fields, momenta, sf);
+  Oracle *o = S(h);
   std::memcpy(o->fld.data(), fields, o->fld.size() * sizeof(double));
   std::memcpy(o->pi.data(), momenta, o->pi.size() * sizeof(double));
   if (sf) {
@@ -372,7 +398,8 @@ int orc_set_state(orc_handle *h, const double *fields, const double *momenta, co
 
 int orc_get_state(orc_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_get_state(H(h)->impl, fields, momenta, sf);
+  Oracle *o = S(h);
   if (fields) std::memcpy(fields, o->fld.data(), o->fld.size() * sizeof(double));
   if (momenta) std::memcpy(momenta, o->pi.data(), o->pi.size() * sizeof(double));
   if (sf) {
@@ -385,7 +412,8 @@ int orc_get_state(orc_handle *h, double *fields, double *momenta, clb_scalefacto
 // ModelInitializer tail (modelinitializer.h:74-80) then the evolver constructor (leapfrog.h:35).
 int orc_initialize(orc_handle *h, int32_t correct_adot)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_initialize(H(h)->impl, correct_adot);
+  Oracle *o = S(h);
   o->setAllAverages();
   if (o->cfg.expansion && correct_adot) {
     double hl[3];
@@ -400,7 +428,8 @@ int orc_initialize(orc_handle *h, int32_t correct_adot)
 
 int orc_evolve(orc_handle *h, int64_t n)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_evolve(H(h)->impl, n);
+  Oracle *o = S(h);
   if (!o->initialized) { o->err = "evolve before initialize"; return CLB_ESTATE; }
   for (int64_t s = 0; s < n; ++s) {
     if (o->cfg.evolver == CLB_LF)
@@ -413,7 +442,8 @@ int orc_evolve(orc_handle *h, int64_t n)
 
 int orc_sync(orc_handle *h)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_sync(H(h)->impl);
+  Oracle *o = S(h);
   if (o->cfg.evolver == CLB_LF) o->syncLF();
   return CLB_OK;
 }
@@ -422,7 +452,8 @@ int orc_sync(orc_handle *h)
 // (meansmeasurer.h:28-48), ScaleFactorMeasurer (scalefactormeasurer.h:37-48).
 int orc_measure(orc_handle *h, double e0, clb_measurement *m)
 {
-  Oracle *o = reinterpret_cast<Oracle *>(h);
+  if (isU1(h)) return oracle_models::u1_measure(H(h)->impl, e0, m);
+  Oracle *o = S(h);
   std::memset(m, 0, sizeof(*m));
   if (!o->cfg.expansion) o->potAvI = o->avPot();               // measurer.h:274-276
   const double am6 = ipow(o->aI, -6), am2 = ipow(o->aI, -2);

@@ -79,7 +79,7 @@ class OracleLattice:
         if rc != 0:
             raise RuntimeError(self.lib.orc_last_error(None).decode())
         self.h = h
-        self.n_components = model.Ns
+        self.n_components = getattr(model, "n_components", model.Ns)
 
     def close(self):
         if getattr(self, "h", None):

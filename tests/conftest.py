@@ -37,6 +37,28 @@ def make_scalar_case(N=16, evolver="VV2", expansion=True, model="lphi4_1f", dt=0
     return par, rp, m, f, p, sf
 
 
+def make_u1_case(N=12, evolver="VV2", expansion=True, dt=0.01, seed="u", amp=1e-2, gU1=0.5, kcut=None,
+                 extra=None):
+    """Parameter set, run parameters, lphi4U1 model and RandomWithMatter initial state."""
+    from cosmolattice_b200 import MODELS, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import u1_initial_state
+
+    params = {
+        "N": N, "kIR": 1.0, "dt": dt, "evolver": evolver, "expansion": "true" if expansion else "false",
+        "lambda": 1.0, "cmplx_field_initial_norm": "5.6964e18", "cmplx_momentum_initial_norm": "0",
+        "gU1s": gU1, "CSU1_charges": 1, "fluct_amplitude": amp,
+        "kCutOff": kcut if kcut is not None else N / 4.0, "baseSeed": seed,
+    }
+    if extra:
+        params.update(extra)
+    par = ParameterParser(params=params)
+    rp = RunParameters(par)
+    m = MODELS["lphi4U1"](par, rp)
+    f, p, aI, aD = u1_initial_state(m, rp)
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+    return par, rp, m, f, p, sf
+
+
 @pytest.fixture(scope="session")
 def gpu_available():
     try:

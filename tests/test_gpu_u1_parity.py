@@ -1,0 +1,166 @@
+"""Parity of the CUDA complex scalar + U(1) path (lphi4U1) with the FP64 CPU oracle (B200).
+
+Tolerances as for the scalar path: started from identical arrays, per-site fields and momenta
+within 1e-12 relative (to each component's max |value|) after 100 steps; a(t), aDot, energies,
+means and the Gauss-law averages within 1e-10 relative.  The Gauss ratio av|LHS-RHS|/av|..| is a
+difference of two nearly equal averages, so it is compared on the scale of av|LHS|: the two
+residuals agree within 1e-11 av|LHS|.
+"""
+import numpy as np
+import pytest
+
+from conftest import make_u1_case
+
+pytestmark = pytest.mark.gpu
+
+SITE_TOL = 1e-12
+AVG_TOL = 1e-10
+
+
+def rel_comp(a, b, N):
+    a = np.asarray(a).reshape(5, -1)
+    b = np.asarray(b).reshape(5, -1)
+    out = []
+    for c in range(5):
+        sc = np.abs(b[c]).max()
+        out.append(np.abs(a[c] - b[c]).max() / sc if sc > 0 else np.abs(a[c]).max())
+    return max(out)
+
+
+def run_pair(N, evolver, expansion, nsteps, measure_every=None, dt=0.01, amp=2e-2, links=0.0):
+    from cosmolattice_b200 import Lattice
+    from oracle.oracle import OracleLattice
+
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver=evolver, expansion=expansion, dt=dt, amp=amp)
+    if links:
+        rng = np.random.default_rng(11)
+        f = f.copy()
+        f[2:] = rng.normal(0.0, links, f[2:].shape)
+    gpu = Lattice(m, rp)
+    cpu = OracleLattice(m, rp)
+    meas = {"gpu": [], "cpu": []}
+    for key, lat in (("gpu", gpu), ("cpu", cpu)):
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.sync()
+        m0 = lat.measure(1.0)
+        e0 = m0["energies"][-1]
+        meas[key].append(m0)
+        done = 0
+        while done < nsteps:
+            k = nsteps - done if measure_every is None else min(measure_every, nsteps - done)
+            lat.evolve(k)
+            done += k
+            if measure_every is not None:
+                lat.sync()
+                meas[key].append(lat.measure(e0))
+        lat.sync()
+        meas[key].append(lat.measure(e0))
+    out = (gpu.get_state(), cpu.get_state(), meas)
+    gpu.close()
+    cpu.close()
+    return out
+
+
+def check_state(g, c, N):
+    (fg, pg, sg), (fc, pc, sc) = g, c
+    assert rel_comp(fg, fc, N) < SITE_TOL, rel_comp(fg, fc, N)
+    assert rel_comp(pg, pc, N) < SITE_TOL, rel_comp(pg, pc, N)
+    for k in ("aI", "aDotI"):
+        assert abs(sg[k] - sc[k]) <= AVG_TOL * max(abs(sc[k]), 1e-300), (k, sg[k], sc[k])
+
+
+def check_meas(mg, mc):
+    for a, b in zip(mg, mc):
+        for ea, eb in zip(a["energies"], b["energies"]):
+            assert abs(ea - eb) <= AVG_TOL * abs(eb) + 1e-300, (a["energies"], b["energies"])
+        for k in (1, 2):
+            assert abs(a["friedmann"][k] - b["friedmann"][k]) <= AVG_TOL * abs(b["friedmann"][k]) + 1e-300
+        assert len(a["means"]) == len(b["means"]) == 4
+        for ra, rb in zip(a["means"], b["means"]):
+            scales = [max(abs(rb[0]), rb[4]), max(abs(rb[1]), rb[5]), abs(rb[2]), abs(rb[3])]
+            for x, y, sc in zip(ra[:4], rb[:4], scales):
+                assert abs(x - y) <= AVG_TOL * max(sc, 1e-300), (ra, rb)
+        ga, gb = a["gauss_u1"], b["gauss_u1"]
+        for k in (1, 2):
+            assert abs(ga[k] - gb[k]) <= AVG_TOL * abs(gb[k]) + 1e-300, (ga, gb)
+        if gb[1] > 0:
+            # ratio = avDiff / avSum; compare the residuals avDiff on the scale of av|LHS|
+            avsum_b = gb[1] / max(gb[0], 1e-300) if gb[0] > 0 else None
+            if avsum_b:
+                assert abs(ga[0] - gb[0]) * avsum_b <= 1e-11 * gb[1] + AVG_TOL * abs(gb[0]) * avsum_b
+
+
+@pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV2", False), ("VV4", True), ("LF", True),
+                                               ("LF", False), ("VV6", True)])
+def test_lphi4u1_100_steps(evolver, expansion):
+    N = 16
+    g, c, meas = run_pair(N, evolver, expansion, 100)
+    check_state(g, c, N)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("evolver", ["VV2", "LF"])
+def test_lphi4u1_measure_cadence_and_links(evolver):
+    # measurements between evolve calls (the LF sync/measure side effects), random initial links
+    N = 12
+    g, c, meas = run_pair(N, evolver, True, 60, measure_every=7, links=0.05)
+    check_state(g, c, N)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_lphi4u1_ragged_size_and_history():
+    # N not a multiple of any tile; per-step history rows of a(t)
+    from cosmolattice_b200 import Lattice
+
+    N = 13
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver="VV2", expansion=True)
+    g, c, meas = run_pair(N, "VV2", True, 30)
+    check_state(g, c, N)
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(10)
+    h = lat.history()
+    _, _, s = lat.get_state()
+    assert h.shape == (10, 5)
+    assert h[-1, 0] == s["aI"] and h[-1, 1] == s["aDotI"]
+    assert np.all(np.diff(h[:, 0]) > 0)
+    lat.close()
+
+
+def test_gauss_law_preserved_on_gpu():
+    from cosmolattice_b200 import Lattice
+
+    from test_oracle_u1 import gauss_field
+
+    N = 24
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver="VV4", expansion=True, amp=5e-2, dt=0.005)
+    G0, r0 = gauss_field(rp, m, f.ravel(), p.ravel())
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(200)
+    f1, p1, _ = lat.get_state()
+    lat.close()
+    G1, r1 = gauss_field(rp, m, f1, p1)
+    assert np.abs(r1 - r0).max() > 1e-6 * np.abs(r0).max()
+    assert np.abs(G1 - G0).max() < 1e-12 * np.abs(r0).max()
+
+
+def test_u1_rejects_unsupported_requests():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_u1_case(N=8)
+    with pytest.raises(_capi.ClbError) as e:
+        Lattice(m, rp, precision="fp32")
+    assert e.value.code == _capi.CLB_EUNSUPPORTED
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    with pytest.raises(_capi.ClbError) as e:
+        lat.spectrum(which=0)
+    assert e.value.code == _capi.CLB_EUNSUPPORTED
+    with pytest.raises(ValueError):
+        lat.set_state(f[:2], p[:2], sf)
+    lat.close()
