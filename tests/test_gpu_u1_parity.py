@@ -2,9 +2,9 @@
 
 Tolerances as for the scalar path: started from identical arrays, per-site fields and momenta
 within 1e-12 relative (to each component's max |value|) after 100 steps; a(t), aDot, energies,
-means and the Gauss-law averages within 1e-10 relative.  The Gauss ratio av|LHS-RHS|/av|..| is a
-difference of two nearly equal averages, so it is compared on the scale of av|LHS|: the two
-residuals agree within 1e-11 av|LHS|.
+means and the Gauss-law averages av|LHS|, av|RHS| within 1e-10 relative.  The Gauss ratio
+av|LHS-RHS|/av|sum of squares| is formed from the difference of two nearly equal per-site terms
+(cancellation of about 1e3 here), so it is compared within 1e-8 relative.
 """
 import numpy as np
 import pytest
@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 
 SITE_TOL = 1e-12
 AVG_TOL = 1e-10
+GAUSS_RATIO_TOL = 1e-8
 
 
 def rel_comp(a, b, N):
@@ -84,11 +85,7 @@ def check_meas(mg, mc):
         ga, gb = a["gauss_u1"], b["gauss_u1"]
         for k in (1, 2):
             assert abs(ga[k] - gb[k]) <= AVG_TOL * abs(gb[k]) + 1e-300, (ga, gb)
-        if gb[1] > 0:
-            # ratio = avDiff / avSum; compare the residuals avDiff on the scale of av|LHS|
-            avsum_b = gb[1] / max(gb[0], 1e-300) if gb[0] > 0 else None
-            if avsum_b:
-                assert abs(ga[0] - gb[0]) * avsum_b <= 1e-11 * gb[1] + AVG_TOL * abs(gb[0]) * avsum_b
+        assert abs(ga[0] - gb[0]) <= GAUSS_RATIO_TOL * abs(gb[0]) + 1e-300, (ga, gb)
 
 
 @pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV2", False), ("VV4", True), ("LF", True),
