@@ -101,6 +101,16 @@ class ClbError(RuntimeError):
         self.code = code
 
 
+class AdjointGrad(C.Structure):
+    """clb_adjoint_grad."""
+
+    _fields_ = [
+        ("observable", C.c_double),
+        ("dO_dcouplings", C.c_double * 8),
+        ("dO_dscalefactor", C.c_double * 2),
+    ]
+
+
 def _declare(lib: C.CDLL, prefix: str) -> None:
     H = C.c_void_p
     dp = C.POINTER(C.c_double)
@@ -133,6 +143,8 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_cuda_stream": (C.c_void_p, [H]),
             "clb_spectrum": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
+            "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
+            "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
         }
         for name, (res, args) in more.items():
             fn = getattr(lib, name)
@@ -177,5 +189,7 @@ EXPORTED = [
     "clb_kernel_stats",
     "clb_last_evolve_ms",
     "clb_cuda_stream",
+    "clb_forward",
+    "clb_backward",
     "clb_scalar_averages_noalloc",
 ]

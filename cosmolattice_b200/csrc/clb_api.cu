@@ -72,6 +72,8 @@ int u1_initialize(clb_handle *h, int32_t correct_adot);
 int u1_evolve(clb_handle *h, int64_t n);
 int u1_sync(clb_handle *h);
 int u1_measure(clb_handle *h, double e0, clb_measurement *m);
+int u1_forward(clb_handle *h, int64_t nsteps, int32_t K, const double *w, int32_t nw, double *obs);
+int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *out);
 
 // Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
 __attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
@@ -910,6 +912,22 @@ int clb_measure(clb_handle *h, double e0, clb_measurement *m)
   m->aDotI = s.aDotI;
   m->hubble = s.aDotI / s.aI;
   return CLB_OK;
+}
+
+int clb_forward(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, const double *weights, int32_t n_weights,
+                double *observable)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_forward: call clb_initialize first");
+  if (!h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint pair covers lphi4U1");
+  return u1_forward(h, nsteps, checkpoint_every, weights, n_weights, observable);
+}
+
+int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *grad)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_backward: the adjoint pair covers lphi4U1");
+  return u1_backward(h, through_init, fields_bar, momenta_bar, grad);
 }
 
 constexpr int kSpecBlocks = 148 * 2;

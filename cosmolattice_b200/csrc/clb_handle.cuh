@@ -103,13 +103,13 @@ namespace {
 
 enum KKind {
   K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_SPECTRUM,
-  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_NKINDS
+  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_U1_ADJ, K_NKINDS
 };
 const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
                                           "scalar_drift",       "reduce_pi2",        "reduce_fields",
                                           "tail",               "measure",           "convert",
                                           "spectrum",           "u1_kick_sweep",     "u1_drift",
-                                          "u1_reduce"};
+                                          "u1_reduce",          "u1_adjoint_sweep"};
 
 cudaEvent_t take_event(clb_handle *h)
 {

@@ -7,6 +7,7 @@
 // both kicks in sequence and reduces the momenta after each; on the leapfrog the field averages of
 // a step are reduced by the next step's kick sweep, which reads the same fields.
 
+#include "clb_adjoint.cuh"
 #include "clb_handle.cuh"
 #include "clb_u1.cuh"
 
@@ -28,6 +29,21 @@ struct U1Sector {
   double *d_part = nullptr; // kU1Blocks x kU1Meas
   double *d_sums = nullptr; // kU1Meas
   U1Params prm{};
+  // adjoint: checkpoints every K steps, one segment of stage-boundary states, cotangents
+  struct Ckpt {
+    double *f = nullptr, *p = nullptr;
+    U1State st{};
+  };
+  std::vector<Ckpt> ckpt;
+  double *seg = nullptr; // (K S + 1) boundary states of 10 N^3
+  int64_t seg_cap = 0;   // boundary states the segment buffer holds
+  U1State *d_rec = nullptr;
+  double *qbar = nullptr, *pbar[2] = {nullptr, nullptr};
+  double *d_apart = nullptr, *d_asums = nullptr;
+  int64_t fwd_steps = -1, fwd_K = 0;
+  double fwd_w[5] = {0, 0, 0, 0, 0};
+  double fwd_avg[5] = {0, 0, 0, 0, 0}; // final <|pi_phi|^2>, <|D phi|^2>, <pi_A^2>, <B^2>, <V>
+  double fwd_a = 1, fwd_obs = 0;
 };
 
 namespace {
@@ -147,10 +163,30 @@ __attribute__((visibility("hidden"))) int u1_create(clb_handle *h)
   return cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice) == cudaSuccess ? CLB_OK : CLB_ECUDA;
 }
 
+static void free_adjoint(U1Sector *u)
+{
+  for (auto &c : u->ckpt) {
+    if (c.f) cudaFree(c.f);
+    if (c.p) cudaFree(c.p);
+  }
+  u->ckpt.clear();
+  if (u->seg) cudaFree(u->seg);
+  if (u->d_rec) cudaFree(u->d_rec);
+  u->seg = nullptr;
+  u->d_rec = nullptr;
+  u->seg_cap = 0;
+  for (double **b : {&u->qbar, &u->pbar[0], &u->pbar[1], &u->d_apart, &u->d_asums}) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  u->fwd_steps = -1;
+}
+
 __attribute__((visibility("hidden"))) void u1_destroy(clb_handle *h)
 {
   U1Sector *u = h->u1;
   if (!u) return;
+  free_adjoint(u);
   if (u->f) cudaFree(u->f);
   if (u->p) cudaFree(u->p);
   if (u->d_st) cudaFree(u->d_st);
@@ -360,6 +396,367 @@ __attribute__((visibility("hidden"))) int u1_measure(clb_handle *h, double e0, c
   m->aDotI = s.aDotI;
   m->hubble = s.aDotI / s.aI;
   return CLB_OK;
+}
+
+// ---- adjoint: forward with checkpoints, backward by segment recompute -------------------------
+namespace {
+
+constexpr int kAvgN = 5; // <|pi_phi|^2>, <|D phi|^2>, <pi_A^2>, <B^2>, <V>
+
+// Scale-factor equation F(a, <.>) (scalefactorkernels.h:73-77) and its partial derivatives.
+struct SFGrad {
+  double dA[kAvgN];
+  double da;
+};
+SFGrad sf_grad(const U1Params &p, double a, const double (&A)[kAvgN])
+{
+  const double al = p.alpha, e = p.el0;
+  const double c = std::pow(a, 2 * al + 1) / 3.0 * p.fm2, dc = (2 * al + 1) * std::pow(a, 2 * al) / 3.0 * p.fm2;
+  const double br = (al - 2) * A[0] * std::pow(a, -6) + al * A[1] * std::pow(a, -2) +
+                    (al - 1) * e * std::pow(a, -4) * (A[2] + A[3]) + (al + 1) * A[4];
+  const double dbr = (al - 2) * A[0] * -6 * std::pow(a, -7) + al * A[1] * -2 * std::pow(a, -3) +
+                     (al - 1) * e * -4 * std::pow(a, -5) * (A[2] + A[3]);
+  SFGrad g;
+  g.dA[0] = c * (al - 2) * std::pow(a, -6);
+  g.dA[1] = c * al * std::pow(a, -2);
+  g.dA[2] = g.dA[3] = c * (al - 1) * e * std::pow(a, -4);
+  g.dA[4] = c * (al + 1);
+  g.da = dc * br + c * dbr;
+  return g;
+}
+
+void averages_of(const U1State &s, double (&A)[kAvgN])
+{
+  A[0] = s.csPi2I;
+  A[1] = s.csGrad2I;
+  A[2] = s.u1Pi2I;
+  A[3] = s.u1Mag2I;
+  A[4] = s.potI;
+}
+
+// One VV stage as the reference orders it (velocityverlet.h:61-114); with the same arithmetic as
+// the merged sweeps of u1_evolve.
+void vv_stage(clb_handle *h, double w)
+{
+  const double dt = h->cfg.dt;
+  const bool ex = h->cfg.expansion != 0;
+  if (ex) tail(h, T_VV_KICK_HALF, false, 0, w);
+  kick_sweep(h, 1, false, ex, vv_kick(dt, w, 0.0));
+  if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w);
+  drift(h, w);
+  kick_sweep(h, 1, ex, ex, vv_kick(dt, w, 0.0));
+  if (ex) tail(h, T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, true, w, 0);
+}
+
+cudaError_t copy_state(clb_handle *h, double *f, double *p, bool to_live)
+{
+  U1Sector *u = h->u1;
+  const size_t bytes = 5 * h->n3 * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(to_live ? u->f : f, to_live ? f : u->f, bytes, cudaMemcpyDeviceToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(to_live ? u->p : p, to_live ? p : u->p, bytes, cudaMemcpyDeviceToDevice, h->stream);
+  return e;
+}
+
+// Energies (energiesmeasurer.h:45-122) from the five averages at scale factor a.
+void energies_of(const U1Params &p, double a, const double (&A)[kAvgN], double (&E)[kAvgN])
+{
+  E[0] = A[0] * std::pow(a, -6);
+  E[1] = A[1] * std::pow(a, -2);
+  E[2] = p.el0 * std::pow(a, -4) * A[2];
+  E[3] = p.el0 * std::pow(a, -4) * A[3];
+  E[4] = A[4];
+}
+
+int adj_sweep(clb_handle *h, int pre, const double *f, const double *p, const double *pin, double *pout,
+              const U1AdjArgs &g, double (&S)[kAdjSlots])
+{
+  U1Sector *u = h->u1;
+  if (pre)
+    k_u1_adj<1><<<kU1Blocks, 256, 0, h->stream>>>(f, p, pin, u->qbar, pout, u->prm, g, u->d_apart);
+  else
+    k_u1_adj<0><<<kU1Blocks, 256, 0, h->stream>>>(f, p, pin, u->qbar, pout, u->prm, g, u->d_apart);
+  ++h->launches[K_U1_ADJ];
+  k_sum_partials<kAdjSlots><<<1, 256, 0, h->stream>>>(u->d_apart, kU1Blocks, u->d_asums);
+  cudaError_t e = cudaMemcpyAsync(S, u->d_asums, sizeof(S), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? CLB_OK : h->cuda_fail(e, "clb_backward");
+}
+
+U1AdjArgs adj_args(const U1Params &p, double a, const double (&Abar)[kAvgN], double hc, double hu)
+{
+  const double al = p.alpha;
+  U1AdjArgs g{};
+  g.Api = Abar[0];
+  g.AD = Abar[1];
+  g.AE = Abar[2];
+  g.AB = Abar[3];
+  g.AV = Abar[4];
+  g.kA = std::pow(a, 1 + al);
+  g.kB2 = std::pow(a, 3 + al) / 2;
+  g.kG = std::pow(a, al - 1);
+  g.dkA = (1 + al) * std::pow(a, al);
+  g.dkB2 = (3 + al) * std::pow(a, 2 + al) / 2;
+  g.dkG = (al - 1) * std::pow(a, al - 2);
+  g.hc = hc;
+  g.hu = hu;
+  g.J0 = p.J0;
+  g.r2 = p.J0 * p.dx; // 2 (fStar/omegaStar)^2
+  g.inv_n3 = p.inv_n3;
+  return g;
+}
+
+} // namespace
+
+// Forward pass of the adjoint pair: nsteps VV steps from the current (initialized) state with a
+// checkpoint every K steps, then the observable O = sum_k w_k E_k / E_tot over the energy
+// components (E_kin, E_grad of the complex scalar, E_el, E_mag, V).
+__attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nsteps, int32_t K, const double *w,
+                                                     int32_t nw, double *obs)
+{
+  U1Sector *u = h->u1;
+  if (h->cfg.evolver == CLB_LF) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers");
+  if (nsteps < 1 || K < 1) return h->fail(CLB_EINVAL, "clb_forward: nsteps and checkpoint_every must be >= 1");
+  if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward");
+  free_adjoint(u);
+  const size_t bytes = 5 * h->n3 * sizeof(double);
+  const int64_t nck = (nsteps + K - 1) / K;
+  const int64_t S = 2 * (int64_t)h->ws.size() - 1;
+  const int64_t seg_states = std::min<int64_t>(K, nsteps) * S + 1;
+  bool ok = true;
+  u->ckpt.resize((size_t)nck + 1); // + the end state, restored after the backward pass
+  for (auto &c : u->ckpt) ok = ok && cudaMalloc(&c.f, bytes) == cudaSuccess && cudaMalloc(&c.p, bytes) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->seg, (size_t)seg_states * 2 * bytes) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_rec, (size_t)seg_states * sizeof(U1State)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->qbar, bytes) == cudaSuccess && cudaMalloc(&u->pbar[0], bytes) == cudaSuccess &&
+       cudaMalloc(&u->pbar[1], bytes) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_apart, (size_t)kU1Blocks * kAdjSlots * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_asums, kAdjSlots * sizeof(double)) == cudaSuccess;
+  if (!ok) {
+    free_adjoint(u);
+    return h->fail(CLB_ENOMEM, "clb_forward: checkpoint or segment storage does not fit; use a smaller checkpoint_every");
+  }
+  u->seg_cap = seg_states;
+  const std::vector<double> &ws = h->ws;
+  const size_t P = ws.size();
+  cudaEventRecord(h->ev_call[0], h->stream);
+  for (int64_t st = 0; st < nsteps; ++st) {
+    if (st % K == 0) {
+      U1Sector::Ckpt &c = u->ckpt[(size_t)(st / K)];
+      if ((e = copy_state(h, c.f, c.p, false)) != cudaSuccess) return h->cuda_fail(e, "clb_forward");
+      if ((e = cudaMemcpyAsync(&c.st, u->d_st, sizeof(U1State), cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
+        return h->cuda_fail(e, "clb_forward");
+    }
+    for (int64_t i = 0; i < S; ++i) vv_stage(h, ws[(size_t)i < P ? (size_t)i : (size_t)(S - i - 1)]);
+  }
+  cudaEventRecord(h->ev_call[1], h->stream);
+  {
+    U1Sector::Ckpt &c = u->ckpt.back();
+    if ((e = copy_state(h, c.f, c.p, false)) != cudaSuccess) return h->cuda_fail(e, "clb_forward");
+    if ((e = cudaMemcpyAsync(&c.st, u->d_st, sizeof(U1State), cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_forward");
+  }
+  int r = check(h, "clb_forward");
+  if (r != CLB_OK) return r;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, h->ev_call[0], h->ev_call[1]) == cudaSuccess) h->last_evolve_ms = ms;
+  // final averages (one measurement sweep) and the observable
+  CLB_LAUNCH(h, K_MEASURE, k_u1_measure<<<kU1Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, u->d_part));
+  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kU1Meas><<<1, 256, 0, h->stream>>>(u->d_part, kU1Blocks, u->d_sums));
+  double v[kU1Meas];
+  U1State s;
+  e = cudaMemcpyAsync(v, u->d_sums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward");
+  const double inv = u->prm.inv_n3;
+  u->fwd_avg[0] = v[0] * inv;
+  u->fwd_avg[1] = v[1] * inv;
+  u->fwd_avg[2] = v[2] * inv;
+  u->fwd_avg[3] = v[3] * inv;
+  u->fwd_avg[4] = v[4] * inv;
+  u->fwd_a = s.aI;
+  for (int k = 0; k < kAvgN; ++k) u->fwd_w[k] = k < nw ? w[k] : 0.0;
+  double E[kAvgN], Et = 0, Ew = 0;
+  energies_of(u->prm, s.aI, u->fwd_avg, E);
+  for (int k = 0; k < kAvgN; ++k) {
+    Et += E[k];
+    Ew += u->fwd_w[k] * E[k];
+  }
+  u->fwd_obs = Ew / Et;
+  u->fwd_steps = nsteps;
+  u->fwd_K = K;
+  h->synced = true;
+  if (obs) *obs = u->fwd_obs;
+  return CLB_OK;
+}
+
+// Backward pass: cotangents of the forward start state and of the couplings for the observable
+// of the last u1_forward.  Segments are recomputed from their checkpoints (bitwise the forward
+// states) and each stage is reversed by the two adjoint sweeps.  With through_init the start state
+// is taken as produced by clb_initialize(correct_adot = 1), whose aDot = sqrt(Friedmann RHS)
+// (modelinitializer.h:77-78) is differentiated too.
+__attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar,
+                                                      double *momenta_bar, clb_adjoint_grad *out)
+{
+  U1Sector *u = h->u1;
+  if (u->fwd_steps < 0) return h->fail(CLB_ESTATE, "clb_backward: call clb_forward first");
+  const U1Params &prm = u->prm;
+  const bool ex = h->cfg.expansion != 0;
+  const double dt = h->cfg.dt, al = prm.alpha;
+  const size_t bytes = 5 * h->n3 * sizeof(double);
+  const std::vector<double> &ws = h->ws;
+  const size_t P = ws.size();
+  const int64_t S = 2 * (int64_t)P - 1;
+  auto wof = [&](int64_t i) { return ws[(size_t)i < P ? (size_t)i : (size_t)(S - i - 1)]; };
+  cudaError_t e = cudaSuccess;
+  double thg = 0, thc = 0;       // explicit d/dgQ, d/dc4
+  double S9[kAdjSlots];
+  int cur = 0;
+  // seed: O = sum_k w_k E_k / E_tot at the final state
+  double E[kAvgN], Et = 0, Ew = 0;
+  energies_of(prm, u->fwd_a, u->fwd_avg, E);
+  for (int k = 0; k < kAvgN; ++k) {
+    Et += E[k];
+    Ew += u->fwd_w[k] * E[k];
+  }
+  double Ebar[kAvgN], Abar[kAvgN];
+  for (int k = 0; k < kAvgN; ++k) Ebar[k] = (u->fwd_w[k] - Ew / Et) / Et;
+  const double a = u->fwd_a, el = prm.el0;
+  Abar[0] = Ebar[0] * std::pow(a, -6);
+  Abar[1] = Ebar[1] * std::pow(a, -2);
+  Abar[2] = Ebar[2] * el * std::pow(a, -4);
+  Abar[3] = Ebar[3] * el * std::pow(a, -4);
+  Abar[4] = Ebar[4];
+  double abar = Ebar[0] * u->fwd_avg[0] * -6 * std::pow(a, -7) + Ebar[1] * u->fwd_avg[1] * -2 * std::pow(a, -3) +
+                (Ebar[2] * u->fwd_avg[2] + Ebar[3] * u->fwd_avg[3]) * el * -4 * std::pow(a, -5);
+  double adbar = 0;
+  if (!ex) abar = 0;
+  if ((e = cudaMemsetAsync(u->qbar, 0, bytes, h->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(u->pbar[cur], 0, bytes, h->stream)) != cudaSuccess)
+    return h->cuda_fail(e, "clb_backward");
+  int r = adj_sweep(h, 0, u->f, u->p, u->pbar[cur], u->pbar[cur ^ 1], adj_args(prm, a, Abar, 0, 0), S9);
+  if (r != CLB_OK) return r;
+  cur ^= 1;
+  thg += Abar[1] * prm.inv_n3 * S9[5];
+  thc += Abar[4] * prm.inv_n3 * S9[8];
+  std::vector<U1State> rec((size_t)u->seg_cap);
+  const int64_t nck = (int64_t)u->ckpt.size() - 1; // the last entry holds the forward's end state
+  double *seg = u->seg;
+  auto segf = [&](int64_t b) { return seg + (size_t)b * 10 * h->n3; };
+  auto segp = [&](int64_t b) { return seg + (size_t)b * 10 * h->n3 + 5 * h->n3; };
+  for (int64_t c = nck - 1; c >= 0; --c) {
+    const int64_t s0 = c * u->fwd_K, s1 = std::min(u->fwd_steps, s0 + u->fwd_K);
+    const int64_t nb = (s1 - s0) * S; // stages in this segment
+    // recompute the segment, keeping every stage-boundary state and scalar record
+    U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
+    if ((e = copy_state(h, ck.f, ck.p, true)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(u->d_st, &ck.st, sizeof(U1State), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+    for (int64_t b = 0; b <= nb; ++b) {
+      if (b > 0) vv_stage(h, wof((b - 1) % S));
+      if ((e = copy_state(h, segf(b), segp(b), false)) != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+      k_u1_record<<<1, 1, 0, h->stream>>>(u->d_st, u->d_rec, b);
+    }
+    e = cudaMemcpyAsync(rec.data(), u->d_rec, (size_t)(nb + 1) * sizeof(U1State), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+    for (int64_t b = nb - 1; b >= 0; --b) {
+      const double w = wof(b % S), hc = dt / 2 * w, hu = dt * w / 2, dtw = dt * w;
+      const U1State &R0 = rec[(size_t)b], &R1 = rec[(size_t)b + 1];
+      double A0[kAvgN], A1[kAvgN], A1bar[kAvgN] = {0, 0, 0, 0, 0}, A0bar[kAvgN] = {0, 0, 0, 0, 0};
+      averages_of(R0, A0);
+      averages_of(R1, A1);
+      // without expansion a stays at its set value: R0.aI = R1.aI, aS = the set aSI
+      const double a0 = R0.aI, a1 = R1.aI, aS = R1.aSI;
+      // step 6: aDot1 = aDotS + dt/2 w F(a1, <.>1)
+      double adS = 0, abar1 = 0;
+      if (ex) {
+        const SFGrad g1 = sf_grad(prm, a1, A1);
+        const double F6 = dt / 2 * w * adbar;
+        adS = adbar;
+        abar1 = abar + F6 * g1.da;
+        for (int k = 0; k < kAvgN; ++k) A1bar[k] = F6 * g1.dA[k];
+      }
+      // steps 5 and 4 at the stage output
+      U1AdjArgs g = adj_args(prm, a1, A1bar, hc, hu);
+      g.cdf = dtw * std::pow(aS, al - 3);
+      g.cda = dtw * std::pow(aS, al - 1);
+      if ((r = adj_sweep(h, 1, segf(b + 1), segp(b + 1), u->pbar[cur], u->pbar[cur ^ 1], g, S9)) != CLB_OK) return r;
+      cur ^= 1;
+      thg += hc * S9[2] + hu * S9[3] + A1bar[1] * prm.inv_n3 * S9[5];
+      thc += hc * S9[4] + A1bar[4] * prm.inv_n3 * S9[8];
+      double abar0 = 0, adbar0 = 0;
+      if (ex) {
+        abar1 += hc * S9[0] + hu * S9[1];
+        const double aSbar = dtw * ((al - 3) * std::pow(aS, al - 4) * S9[6] + (al - 1) * std::pow(aS, al - 2) * S9[7]);
+        // step 3: a1 = a0 + dt w aDotS, aS = (a0 + a1)/2
+        abar1 += aSbar / 2;
+        abar0 = aSbar / 2 + abar1;
+        adS += dtw * abar1;
+        // step 1: aDotS = aDot0 + dt/2 w F(a0, <.>0)
+        const SFGrad g0 = sf_grad(prm, a0, A0);
+        const double F1 = dt / 2 * w * adS;
+        adbar0 = adS;
+        abar0 += F1 * g0.da;
+        for (int k = 0; k < kAvgN; ++k) A0bar[k] = F1 * g0.dA[k];
+      }
+      // steps 2 and 1 at the stage input
+      g = adj_args(prm, a0, A0bar, hc, hu);
+      if ((r = adj_sweep(h, 0, segf(b), segp(b), u->pbar[cur], u->pbar[cur ^ 1], g, S9)) != CLB_OK) return r;
+      cur ^= 1;
+      thg += hc * S9[2] + hu * S9[3] + A0bar[1] * prm.inv_n3 * S9[5];
+      thc += hc * S9[4] + A0bar[4] * prm.inv_n3 * S9[8];
+      if (ex) abar0 += hc * S9[0] + hu * S9[1];
+      abar = abar0;
+      adbar = adbar0;
+    }
+  }
+  // the start state is the first checkpoint, now at segment boundary 0 of the last recompute
+  if (through_init && ex) {
+    // aDot0 = sqrt(RHS), RHS = a^{2 alpha + 2}/3 fm2 rho(<.>)  (hubbleconstraint.h:27-36)
+    const U1State &R = rec[0];
+    double A0[kAvgN], Ib[kAvgN];
+    averages_of(R, A0);
+    const double a0 = R.aI;
+    const double C = std::pow(a0, 2 * al + 2) / 3.0 * prm.fm2, dC = (2 * al + 2) * std::pow(a0, 2 * al + 1) / 3.0 * prm.fm2;
+    const double rho = A0[0] * std::pow(a0, -6) + A0[1] * std::pow(a0, -2) + el * std::pow(a0, -4) * (A0[2] + A0[3]) + A0[4];
+    const double drho = A0[0] * -6 * std::pow(a0, -7) + A0[1] * -2 * std::pow(a0, -3) + el * -4 * std::pow(a0, -5) * (A0[2] + A0[3]);
+    const double RHSbar = adbar / (2 * R.aDotI);
+    Ib[0] = RHSbar * C * std::pow(a0, -6);
+    Ib[1] = RHSbar * C * std::pow(a0, -2);
+    Ib[2] = Ib[3] = RHSbar * C * el * std::pow(a0, -4);
+    Ib[4] = RHSbar * C;
+    abar += RHSbar * (dC * rho + C * drho);
+    adbar = 0;
+    if ((r = adj_sweep(h, 0, segf(0), segp(0), u->pbar[cur], u->pbar[cur ^ 1], adj_args(prm, a0, Ib, 0, 0), S9)) != CLB_OK)
+      return r;
+    cur ^= 1;
+    thg += Ib[1] * prm.inv_n3 * S9[5];
+    thc += Ib[4] * prm.inv_n3 * S9[8];
+  }
+  // leave the live state at the forward's end again
+  {
+    const U1Sector::Ckpt &end = u->ckpt.back();
+    if ((e = copy_state(h, end.f, end.p, true)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(u->d_st, &end.st, sizeof(U1State), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+  }
+  if (fields_bar) e = cudaMemcpyAsync(fields_bar, u->qbar, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && momenta_bar) e = cudaMemcpyAsync(momenta_bar, u->pbar[cur], bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->dO_dcouplings[0] = thc;
+    out->dO_dcouplings[1] = thg;
+    out->dO_dscalefactor[0] = ex ? abar : 0.0;
+    out->dO_dscalefactor[1] = ex ? adbar : 0.0;
+    out->observable = u->fwd_obs;
+  }
+  return check(h, "clb_backward");
 }
 
 } // namespace clb

@@ -108,11 +108,26 @@ def _fluct_norm(model: Model, rp: RunParameters, k, m2):
     return norm, omega
 
 
-def complex_scalar_fluctuations(model: Model, rp: RunParameters, aDot: float):
+def _homogeneous_adot_tangent(model: Model, rp: RunParameters, param: str) -> float:
+    """d aDot / d param of initial_scale_factor (only pot0 = c4 |phi_0/f*|^4 depends on c4)."""
+    if not rp.expansion or param != "c4":
+        return 0.0
+    aI, aDot = initial_scale_factor(model, rp)
+    if aDot == 0.0:
+        return 0.0
+    rho3 = (aDot * model.MPl / model.fStar) ** 2  # rho / 3
+    return model.fStar / model.MPl * 0.5 / math.sqrt(rho3) * (model.pot0 / model.c4) / 3.0
+
+
+def complex_scalar_fluctuations(model: Model, rp: RunParameters, aDot: float, tangent: str = None,
+                                daDot: float = 0.0):
     """U1Initializer::addFluctuationsCScalarFromPhases (u1initializer.h:157-230): per component
     Rayleigh amplitudes a_c, three uniform phases and the fourth fixed by
     e11 = e01 e10 conj(e00) so the initial charge density follows from the amplitudes; modes
-    phi_c = a_c (e_c0 + e_c1)/2, pi_c = -i omega a_c (e_c0 - e_c1)/2 - aDot phi_c, zero modes 0."""
+    phi_c = a_c (e_c0 + e_c1)/2, pi_c = -i omega a_c (e_c0 - e_c1)/2 - aDot phi_c, zero modes 0.
+
+    With ``tangent`` ("amp" or "c4") the same draws give d phi_c, d pi_c with respect to the
+    fluctuation amplitude or the quartic coupling (through m^2 = masses2CS and aDot)."""
     N = rp.N
     nx, ny, nz = wave_numbers(N)
     k = np.sqrt(nx * nx + ny * ny + nz * nz) * rp.kIR
@@ -129,25 +144,44 @@ def complex_scalar_fluctuations(model: Model, rp: RunParameters, aDot: float):
         g = _rng(rp.baseSeed, label)
         return np.exp(2j * np.pi * g.random(shape))
 
+    amp = model.omegaStar / model.fStar if model.fluct_amplitude is None else model.fluct_amplitude
+    m2 = model.masses2CS[0]
+    domega0 = np.zeros_like(omega0)
+    if tangent == "c4" and m2 > 0:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            domega0 = np.where(omega0 > 0, (m2 / model.c4) / (2 * omega0), 0.0)
     e00, e01, e10 = phase("phase00cmplx_0_0"), phase("phase01cmplx_0_0"), phase("phase10cmplx_0_1")
     e11 = e01 * e10 * np.conj(e00)
     for c, (ea, eb) in enumerate(((e00, e01), (e10, e11))):
-        a = norms[c][0] * rayleigh(f"norm{c}cmplx_0_{c}")
+        norm, om = norms[c]
+        a = norm * rayleigh(f"norm{c}cmplx_0_{c}")
         fk = a * (ea + eb) / 2.0
         fk[0, 0, 0] = 0.0
-        pk = -1j * omega0 * a * (ea - eb) / 2.0 - aDot * fk
+        if tangent is None:
+            pk = -1j * omega0 * a * (ea - eb) / 2.0 - aDot * fk
+        else:
+            if tangent == "amp":
+                da = a / amp
+            elif tangent == "c4" and model.masses2CS[c] > 0:
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    dom = np.where(om > 0, (model.masses2CS[c] / model.c4) / (2 * om), 0.0)
+                    da = np.where(om > 0, -0.5 * a * dom / om, 0.0)
+            else:
+                da = np.zeros_like(a)
+            dfk = da * (ea + eb) / 2.0
+            dfk[0, 0, 0] = 0.0
+            pk = -1j * (domega0 * a + omega0 * da) * (ea - eb) / 2.0 - daDot * fk - aDot * dfk
+            fk = dfk
         pk[0, 0, 0] = 0.0
         out_f.append(sfft.irfftn(fk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
         out_p.append(sfft.irfftn(pk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
     return out_f, out_p
 
 
-def gauss_momenta_u1(model: Model, rp: RunParameters, phi, pi):
-    """pi_A from the Gauss constraint in momentum space with A = 0 (u1initializer.h:90-114):
-    j0 = -dx^2 rho, pi_i(k) = conj(1 - e^{-2 pi i n_i/N}) / sum_j |1 - e^{-2 pi i n_j/N}|^2 j0(k),
-    zero mode 0; rho = 2/dx (fStar/omegaStar)^2 gQ Im(conj(pi_phi) phi) (mattercurrents.h:27-48)."""
+def gauss_solve_u1(rp: RunParameters, rho):
+    """pi_i(k) = conj(1 - e^{-2 pi i n_i/N}) / sum_j |1 - e^{-2 pi i n_j/N}|^2 j0(k), j0 = -dx^2 rho,
+    zero mode 0 (u1initializer.h:90-114)."""
     N = rp.N
-    rho = 2.0 / rp.dx * (model.fStar / model.omegaStar) ** 2 * model.gQ * (pi[0] * phi[1] - pi[1] * phi[0])
     j0 = sfft.rfftn(-rp.dx ** 2 * rho, axes=(0, 1, 2), workers=-1)
     nx, ny, nz = wave_numbers(N)
     keff = [1.0 - np.exp(-2j * np.pi * n / N) for n in (nx, ny, nz)]
@@ -160,6 +194,17 @@ def gauss_momenta_u1(model: Model, rp: RunParameters, phi, pi):
         pk[0, 0, 0] = 0.0
         out.append(sfft.irfftn(pk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
     return out
+
+
+def charge_density_u1(model: Model, rp: RunParameters, phi, pi, gQ=None):
+    """rho = 2/dx (fStar/omegaStar)^2 gQ Im(conj(pi_phi) phi) (mattercurrents.h:27-48)."""
+    g = model.gQ if gQ is None else gQ
+    return 2.0 / rp.dx * (model.fStar / model.omegaStar) ** 2 * g * (pi[0] * phi[1] - pi[1] * phi[0])
+
+
+def gauss_momenta_u1(model: Model, rp: RunParameters, phi, pi):
+    """pi_A from the Gauss constraint in momentum space with A = 0 (u1initializer.h:90-114)."""
+    return gauss_solve_u1(rp, charge_density_u1(model, rp, phi, pi))
 
 
 def u1_initial_state(model: Model, rp: RunParameters):
@@ -184,3 +229,28 @@ def initial_state(model: Model, rp: RunParameters):
     if getattr(model, "NU1", 0):
         return u1_initial_state(model, rp)
     return scalar_initial_state(model, rp)
+
+
+def u1_initial_state_tangent(model: Model, rp: RunParameters, param: str):
+    """d(fields, momenta)/d param of u1_initial_state for param in ("amp", "c4", "gQ"): the
+    fluctuation amplitude, the quartic coupling (lambda_prog) and the gauge coupling g Q."""
+    fields, momenta, aI, aDot = u1_initial_state(model, rp)
+    N = rp.N
+    df = np.zeros_like(fields)
+    dp = np.zeros_like(momenta)
+    if param in ("amp", "c4"):
+        fl, pl = complex_scalar_fluctuations(model, rp, aDot, tangent=param,
+                                             daDot=_homogeneous_adot_tangent(model, rp, param))
+        for c in range(2):
+            df[c] = fl[c]
+            dp[c] = pl[c]
+        drho = 2.0 / rp.dx * (model.fStar / model.omegaStar) ** 2 * model.gQ * (
+            dp[0] * fields[1] + momenta[0] * df[1] - dp[1] * fields[0] - momenta[1] * df[0])
+        pa = gauss_solve_u1(rp, drho)
+    elif param == "gQ":
+        pa = gauss_solve_u1(rp, charge_density_u1(model, rp, fields[:2], momenta[:2], gQ=1.0))
+    else:
+        raise ValueError(f"unknown parameter {param!r}")
+    for i in range(3):
+        dp[2 + i] = pa[i]
+    return df, dp

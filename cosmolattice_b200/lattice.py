@@ -115,6 +115,26 @@ class Lattice:
                                           _dp(k), _dp(v), c.ctypes.data_as(C.POINTER(C.c_int64))))
         return k, v, c
 
+    def forward(self, n_steps: int, checkpoint_every: int, weights) -> float:
+        """clb_forward: n_steps VV steps with checkpoints; returns O = sum_k w_k E_k / E_tot."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        o = C.c_double()
+        self._check(self.lib.clb_forward(self.h, int(n_steps), int(checkpoint_every), _dp(w), int(w.size), C.byref(o)))
+        return o.value
+
+    def backward(self, through_init: bool = True):
+        """clb_backward: (fields_bar, momenta_bar, grad dict) of the last forward's observable."""
+        n = self.n_field_components * self.rp.N ** 3
+        fb, pb = np.empty(n), np.empty(n)
+        g = _capi.AdjointGrad()
+        self._check(self.lib.clb_backward(self.h, 1 if through_init else 0, _dp(fb), _dp(pb), C.byref(g)))
+        return fb, pb, {
+            "observable": g.observable,
+            "dO_dcouplings": [g.dO_dcouplings[i] for i in range(8)],
+            "dO_daI": g.dO_dscalefactor[0],
+            "dO_daDotI": g.dO_dscalefactor[1],
+        }
+
     def history(self) -> np.ndarray:
         """Per-step rows (a, aDot, <pi^2>, <grad^2>, <V>) of the last evolve call."""
         n = C.c_int64()

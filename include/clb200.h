@@ -205,6 +205,34 @@ int clb_last_evolve_ms(clb_handle *h, double *ms);
 /* The cudaStream_t the handle launches on (for callers that order their own work after it). */
 void *clb_cuda_stream(clb_handle *h);
 
+/* ---- adjoint (reverse-mode) pair ----------------------------------------------------------------
+ * No counterpart in the reference, which has no differentiation.  Replaces, for gradient studies,
+ * a caller's finite-difference loop around Evolver::evolve (evolvers/evolver.h:102-127) and
+ * EnergiesMeasurer::measure (measurements/energiesmeasurer.h:45-122).
+ *
+ * clb_forward runs nsteps VV steps from the current (initialized) state, storing the full state
+ * every checkpoint_every steps, and returns the observable
+ *     O = sum_k w_k E_k / E_tot
+ * over the energy components E_k in clb_measurement order without E_tot (lphi4U1: E_kin and
+ * E_grad of the complex scalar, E_el, E_mag, V; n_weights <= 5).  clb_backward then returns dO
+ * with respect to the state at the forward's start (fields_bar, momenta_bar: same layout as
+ * clb_set_state; either may be NULL), to the scale factor there, and to the couplings through
+ * their explicit appearance in the evolution.  With through_init = 1 the start state is taken as
+ * made by clb_initialize(h, 1), whose aDot = sqrt(Friedmann RHS) is differentiated as well (the
+ * aDot cotangent is then 0).  The backward pass recomputes each segment from its checkpoint;
+ * device memory: (nsteps/checkpoint_every + 1) states plus checkpoint_every x stages + 1 states.
+ * lphi4U1 with the VV evolvers; other models and the leapfrog return CLB_EUNSUPPORTED.  After
+ * clb_backward the handle holds the forward's end state again. */
+typedef struct clb_adjoint_grad {
+  double observable;         /* O of the forward pass                                       */
+  double dO_dcouplings[8];   /* clb_model_desc.couplings order (lphi4U1: [0] c4, [1] gQ)     */
+  double dO_dscalefactor[2]; /* aI, aDotI at the forward's start (0 without expansion)      */
+} clb_adjoint_grad;
+
+int clb_forward(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, const double *weights, int32_t n_weights,
+                double *observable);
+int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *grad);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
  * For callers that cannot call cudaMalloc: a runtime that owns the whole device memory pool, code
  * issued while a CUDA graph is being captured, or an embedding that forbids allocation after
