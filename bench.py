@@ -48,6 +48,10 @@ def parse_args():
     ap.add_argument("--N", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--config", default="lphi4", choices=["lphi4", "lphi4U1-adjoint"],
+                    help="lphi4: the headline 512^3 scalar workload; lphi4U1-adjoint: 128^3 VV4 gauge "
+                         "run with the adjoint gradient and its finite-difference check")
+    ap.add_argument("--checkpoint-every", type=int, default=50)
     return ap.parse_args()
 
 
@@ -308,8 +312,87 @@ def roofline(stats, N, precision, peak, peak_kind):
     }
 
 
+def main_u1_adjoint(args):
+    """128^3 lphi4U1, VV4, dt = 0.005, g = 0.5, lambda = 1, amplitude 1e-3, self-consistent
+    expansion: forward + backward time of the adjoint pair, gradients of the final gauge-energy
+    fraction against central differences (relative h = 1e-4) of the plain GPU path."""
+    import torch
+
+    from cosmolattice_b200 import MODELS, Lattice, ParameterParser, RunParameters
+    from cosmolattice_b200.adjoint import GAUGE_FRACTION, observable_from_measurement, u1_gradients
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    N = args.N if args.N != 512 else 128
+    steps = args.steps if args.steps != 2000 else 1000
+    base = {"amp": 1e-3, "c4": 1.0, "gQ": 0.5}
+
+    def setup(over=None):
+        v = dict(base)
+        v.update(over or {})
+        par = ParameterParser(params={
+            "N": N, "kIR": 1.0, "dt": 0.005, "evolver": "VV4", "expansion": "true", "lambda": 1.0,
+            "lambda_prog": v["c4"], "cmplx_field_initial_norm": "5.6964e18", "cmplx_momentum_initial_norm": "0",
+            "gU1s": v["gQ"], "CSU1_charges": 1, "fluct_amplitude": v["amp"], "kCutOff": N / 4.0, "baseSeed": "cfg3"})
+        rp = RunParameters(par)
+        return rp, MODELS["lphi4U1"](par, rp)
+
+    def plain(over):
+        from cosmolattice_b200.initializers import u1_initial_state
+
+        rp, m = setup(over)
+        f, p, aI, aD = u1_initial_state(m, rp)
+        lat = Lattice(m, rp)
+        lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
+        lat.initialize()
+        lat.evolve(steps)
+        ms = lat.last_evolve_ms()
+        o = observable_from_measurement(lat.measure(1.0))
+        lat.close()
+        return o, ms
+
+    rp, m = setup()
+    lat = Lattice(m, rp)
+    lat.set_profiling(False)
+    t0 = time.perf_counter()
+    O, grads, rec = u1_gradients(m, rp, steps, args.checkpoint_every, GAUGE_FRACTION, lattice=lat)
+    t_total = time.perf_counter() - t0
+    fwd_ms = lat.last_evolve_ms()
+    lat.close()
+    fdv, plain_ms = {}, []
+    for prm in ("amp", "c4", "gQ"):
+        h = 1e-4 * base[prm]
+        up, ms1 = plain({prm: base[prm] + h})
+        dn, ms2 = plain({prm: base[prm] - h})
+        plain_ms += [ms1, ms2]
+        fdv[prm] = (up - dn) / (2 * h)
+    sites = N ** 3
+    line = {
+        "metric": "adjoint gradient of the final gauge-energy fraction (forward + backward wall time)",
+        "value": t_total, "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": steps,
+        "dtype": "f64", "data": "synthetic (seeded RandomWithMatter initial state)",
+        "config": {"workload": f"lphi4U1 {N}^3 VV4 dt=0.005 g=0.5 lambda=1 amplitude=1e-3, expansion, "
+                               f"{steps} steps, checkpoint every {args.checkpoint_every}"},
+        "observable": O,
+        "gradient": grads,
+        "finite_difference": fdv,
+        "rel_diff": {k: abs(grads[k] - fdv[k]) / abs(fdv[k]) for k in grads},
+        "forward_ms": fwd_ms,
+        "forward_site_updates_per_s": sites * steps / (fwd_ms * 1e-3),
+        "plain_evolve_ms": statistics.median(plain_ms),
+        "backward_over_forward": (t_total * 1e3 - fwd_ms) / fwd_ms,
+        "fp32_split": "not built for lphi4U1 (FP64 storage only)",
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse_args()
+    if args.config == "lphi4U1-adjoint":
+        return main_u1_adjoint(args)
     if args.impl == "reference":
         return main_reference(args)
     world, rank, local = dist_setup(args)
