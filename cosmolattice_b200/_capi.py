@@ -145,6 +145,16 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
             "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
             "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
+            "clb_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(ModelDesc), C.c_int32, C.POINTER(H)]),
+            "clb_batch_destroy": (None, [H]),
+            "clb_batch_last_error": (C.c_char_p, [H]),
+            "clb_batch_set_state": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(ScaleFactor)]),
+            "clb_batch_get_state": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(ScaleFactor)]),
+            "clb_batch_initialize": (C.c_int, [H, C.c_int32]),
+            "clb_batch_evolve": (C.c_int, [H, C.c_int64]),
+            "clb_batch_measure": (C.c_int, [H, C.c_int32, C.c_double, C.POINTER(Measurement)]),
+            "clb_batch_last_evolve_ms": (C.c_int, [H, dp]),
+            "clb_batch_kernel_launches": (C.c_int, [H, C.POINTER(C.c_int64)]),
         }
         for name, (res, args) in more.items():
             fn = getattr(lib, name)
@@ -191,5 +201,15 @@ EXPORTED = [
     "clb_cuda_stream",
     "clb_forward",
     "clb_backward",
+    "clb_batch_create",
+    "clb_batch_destroy",
+    "clb_batch_last_error",
+    "clb_batch_set_state",
+    "clb_batch_get_state",
+    "clb_batch_initialize",
+    "clb_batch_evolve",
+    "clb_batch_measure",
+    "clb_batch_last_evolve_ms",
+    "clb_batch_kernel_launches",
     "clb_scalar_averages_noalloc",
 ]

@@ -11,8 +11,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libclb200.so")
 
-SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_noalloc.cu"]
-DEPS = ["clb_api.cu", "clb_u1.cu", "clb_noalloc.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
+SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_noalloc.cu"]
+DEPS = ["clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_batch.cuh", "clb_vv.h", "clb_adjoint.cuh", "clb_noalloc.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1,0 +1,262 @@
+// clb_batch.cuh - sm_100a kernels of the batched lphi4 ensemble (many independent lattices).
+//
+// Every member is one real scalar with V = c0/4 phi^4 (models/lphi4.h:154-206 with the daughter
+// field removed) on its own N^3 periodic lattice; the members share dt, evolver and expansion
+// mode and differ in N, dx, c0, initial state and scale factor.  One launch of k_batch_sweep
+// advances all members by one fused VV stage (the same drift + two-kick sweep as the single
+// lattice path: velocityverlet.h:51-114, 129-196); k_batch_tail then updates each member's scale
+// factor from its own fixed-order volume sums (scalefactorkernels.h:27-80).
+//
+// Storage: the members' N^3 arrays are concatenated (each starting on a 128-byte boundary).  FP64
+// stores the fields themselves; FP32 stores each member's deviation from its FP64 homogeneous
+// reference (DevState::ref_phi/ref_pi), as the single-lattice FP32/FP64-split form does.
+#pragma once
+
+#include "clb_internal.cuh"
+#include "clb_scalar.cuh"
+#include "clb_sweep.cuh"
+
+namespace clb {
+
+struct BatchLat {
+  int N, gx, gy, gz, LX; // sweep grid of this member: (z, y) tiles of 32 x 8, x runs of LX planes
+  int first_block, nblocks;
+  long long off;         // element offset of the member's arrays
+  double inv_dx2, c0, c0q;
+  SFParams sp;
+};
+
+constexpr int kBZ = 32, kBY = 8;
+
+// DRIFT / KICK / RED as in k_sweep; one block = one (z, y) tile of one member, marching over LX
+// x-planes.  fin/pin are never written; fout/pout alias them only without DRIFT.
+template <class R, bool DRIFT, bool KICK, int RED>
+__global__ void __launch_bounds__(kBZ *kBY)
+    k_batch_sweep(const R *fin, const R *pin, R *fout, R *pout, const BatchLat *__restrict__ lats,
+                  const int *__restrict__ blk_lat, DevState *__restrict__ sts, int rs, double dtw_d, double h1,
+                  double h2, double *__restrict__ partials)
+{
+  using A = Ar<R>;
+  constexpr bool SPLIT = sizeof(R) == 4;
+  __shared__ R tile[3][kBY + 2][kBZ + 2];
+  __shared__ double red_smem[(kBZ * kBY / 32) * kRedSlots];
+  const int L = blk_lat[blockIdx.x];
+  const BatchLat lt = lats[L];
+  DevState *st = sts + L;
+  const int local = blockIdx.x - lt.first_block;
+  const int bx = local % lt.gx, by = (local / lt.gx) % lt.gy, bz = local / (lt.gx * lt.gy);
+  const int N = lt.N;
+  fin += lt.off;
+  pin += lt.off;
+  fout += lt.off;
+  pout += lt.off;
+  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * kBZ + tz;
+  const int z0 = bx * kBZ, y0 = by * kBY;
+  const int hz = min(kBZ, N - z0), hy = min(kBY, N - y0);
+  const int x0 = bz * lt.LX, x1 = min(N, x0 + lt.LX);
+  const bool valid = tz < hz && ty < hy;
+  const int y = y0 + ty, z = z0 + tz;
+  const int ym = y0 == 0 ? N - 1 : y0 - 1, yp = y0 + hy == N ? 0 : y0 + hy;
+  const int zm = z0 == 0 ? N - 1 : z0 - 1, zp = z0 + hz == N ? 0 : z0 + hz;
+
+  // the member's reference step (split form) and its coefficients
+  RefStep<1> rf{};
+  Lphi4SplitCoef spc{};
+  if constexpr (SPLIT) {
+    rf = ref_step<1>(st, rs, DRIFT, KICK, dtw_d, h1, h2, lt.c0, 0.0);
+    spc = Lphi4SplitCoef::make(rf.phi[0], lt.c0);
+    if ((DRIFT || KICK) && local == 0 && tid == 0) {
+      st->ref_phi[rs ^ 1][0] = rf.phi[0];
+      st->ref_pi[rs ^ 1][0] = rf.pi_next[0];
+    }
+  }
+  const R pd = DRIFT ? (R)st->drift_p : R(0), dtw = DRIFT ? (R)dtw_d : R(0);
+  const R KA = KICK ? (R)st->kick_A : R(0), KB = KICK ? (R)st->kick_B : R(0);
+  const R inv_dx2 = (R)lt.inv_dx2, c0 = (R)lt.c0, c0q = (R)lt.c0q, two = R(2);
+  const float h1f = (float)h1, h2f = (float)h2;
+
+  auto sidx = [&](int x, int yy, int zz) -> size_t { return ((size_t)x * N + yy) * N + zz; };
+  auto ld = [&](size_t s) -> R {
+    R v = fin[s];
+    if (DRIFT) v = drift_val<R>(v, pin[s], pd, dtw);
+    return v;
+  };
+
+  double acc_pi2 = 0, acc_g2 = 0, acc_v = 0, acc_p = 0;
+  long long cnt = 0;
+  R prev = R(0), cur = R(0), nxt = R(0), piC = R(0), piN = R(0);
+  constexpr bool LOADP = KICK || (RED & 1);
+  if (x0 < x1) {
+    const int xm = x0 == 0 ? N - 1 : x0 - 1;
+    if (valid) {
+      prev = ld(sidx(xm, y, z));
+      cur = ld(sidx(x0, y, z));
+      tile[0][ty + 1][tz + 1] = cur;
+      if (ty == 0) tile[0][0][tz + 1] = ld(sidx(x0, ym, z));
+      if (ty == hy - 1) tile[0][hy + 1][tz + 1] = ld(sidx(x0, yp, z));
+      if (tz == 0) tile[0][ty + 1][0] = ld(sidx(x0, y, zm));
+      if (tz == hz - 1) tile[0][ty + 1][hz + 1] = ld(sidx(x0, y, zp));
+      if (LOADP) piC = pin[sidx(x0, y, z)];
+    }
+    int b = 0;
+    for (int x = x0; x < x1; ++x) {
+      const int bn = b == 2 ? 0 : b + 1;
+      const int xn = x + 1 == N ? 0 : x + 1;
+      const bool last = x + 1 == x1;
+      if (valid) {
+        nxt = ld(sidx(xn, y, z));
+        if (!last) {
+          tile[bn][ty + 1][tz + 1] = nxt;
+          if (ty == 0) tile[bn][0][tz + 1] = ld(sidx(xn, ym, z));
+          if (ty == hy - 1) tile[bn][hy + 1][tz + 1] = ld(sidx(xn, yp, z));
+          if (tz == 0) tile[bn][ty + 1][0] = ld(sidx(xn, y, zm));
+          if (tz == hz - 1) tile[bn][ty + 1][hz + 1] = ld(sidx(xn, y, zp));
+          if (LOADP) piN = pin[sidx(xn, y, z)];
+        }
+      }
+      __syncthreads();
+      if (valid) {
+        const size_t s = sidx(x, y, z);
+        const R c = cur;
+        const R ynb = tile[b][ty + 2][tz + 1], ymb = tile[b][ty][tz + 1];
+        const R znb = tile[b][ty + 1][tz + 2], zmb = tile[b][ty + 1][tz];
+        if (DRIFT) fout[s] = c;
+        if constexpr (SPLIT) {
+          if (KICK) {
+            const float lap = inv_dx2 * ((((nxt + prev) - 2.f * c) + ((ynb + ymb) - 2.f * c)) + ((znb + zmb) - 2.f * c));
+            const float K = KA * lap - KB * spc.ddV(c);
+            const float pm = fmaf(h1f, K, piC);
+            pout[s] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
+            if (RED & 1) {
+              acc_p += (double)pm;
+              acc_pi2 += (double)(pm * pm);
+            }
+          } else if (RED & 1) {
+            acc_p += (double)piC;
+            acc_pi2 += (double)(piC * piC);
+          }
+          if (RED & 2) {
+            const float gx = nxt - c, gy = ynb - c, gz = znb - c;
+            acc_g2 += (double)((gx * gx + gy * gy + gz * gz) * inv_dx2);
+            acc_v += (double)spc.dVpot(c);
+          }
+          ++cnt;
+        } else {
+          if (KICK) {
+            const R txv = A::sub(A::add(nxt, prev), A::mul(two, c));
+            const R tyv = A::sub(A::add(ynb, ymb), A::mul(two, c));
+            const R tzv = A::sub(A::add(znb, zmb), A::mul(two, c));
+            const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
+            const R cv[1] = {c};
+            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Lphi4<R, 1>::dV(0, cv, c0, R(0))));
+            const KickOut<R> ko = kick_val<R>(piC, K, h1, h2);
+            pout[s] = ko.next;
+            if (RED & 1) acc_pi2 += ko.mid * ko.mid;
+          } else if (RED & 1) {
+            acc_pi2 += (double)piC * (double)piC;
+          }
+          if (RED & 2) {
+            const R gx = A::sub(nxt, c), gy = A::sub(ynb, c), gz = A::sub(znb, c);
+            acc_g2 += (double)A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
+            const R cv[1] = {c};
+            acc_v += (double)Lphi4<R, 1>::V(cv, c0q, R(0));
+          }
+        }
+      }
+      prev = cur;
+      cur = nxt;
+      if (LOADP) piC = piN;
+      b = bn;
+    }
+  }
+  if (RED) {
+    if constexpr (SPLIT) {
+      // sum (pi_r + p)^2 = n pi_r^2 + 2 pi_r sum p + sum p^2;  sum V = n V_r + sum (V - V_r)
+      acc_pi2 += (double)cnt * rf.pi_mid[0] * rf.pi_mid[0] + 2.0 * rf.pi_mid[0] * acc_p;
+      acc_v += (double)cnt * rf.V;
+    }
+    double v[kRedSlots] = {acc_pi2, acc_g2, acc_v};
+    block_reduce<kRedSlots, kBZ * kBY>(v, red_smem);
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) partials[(size_t)blockIdx.x * kRedSlots + k] = v[k];
+    }
+  }
+}
+
+// One block per member: fixed-order sum of the member's block partials, then the tail's
+// scale-factor bookkeeping (tail_apply) on the member's DevState.
+__global__ void __launch_bounds__(256)
+    k_batch_tail(const double *__restrict__ partials, const BatchLat *__restrict__ lats, DevState *__restrict__ sts,
+                 TailOp op, int reduced)
+{
+  __shared__ double smem[(256 / 32) * kRedSlots];
+  const BatchLat lt = lats[blockIdx.x];
+  double v[kRedSlots] = {0, 0, 0};
+  if (reduced) {
+    for (int b = threadIdx.x; b < lt.nblocks; b += blockDim.x) {
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) v[k] += partials[(size_t)(lt.first_block + b) * kRedSlots + k];
+    }
+    block_reduce<kRedSlots, 256>(v, smem);
+  }
+  if (threadIdx.x != 0) return;
+  DevState s = sts[blockIdx.x];
+  TailOp o = op;
+  o.hist = nullptr;
+  tail_apply(s, o, lt.sp, v[0], v[1], v[2]);
+  sts[blockIdx.x] = s;
+}
+
+// Host FP64 arrays <-> member storage: dst = (R)(src - off) and back (FP32: off = the member's
+// reference value; FP64: off = 0).
+template <class R>
+__global__ void __launch_bounds__(256) k_batch_pack(const double *__restrict__ src, R *__restrict__ dst, size_t n, double off)
+{
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (R)(src[i] - off);
+}
+template <class R>
+__global__ void __launch_bounds__(256) k_batch_unpack(const R *__restrict__ src, double *__restrict__ dst, size_t n, double off)
+{
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = off + (double)src[i];
+}
+
+// Measurement sums of one member (slots of k_measure: pi^2, grad^2, phi, phi^2, mom, mom^2, V),
+// in FP64 from the stored values plus the member's references.
+template <class R>
+__global__ void __launch_bounds__(256)
+    k_batch_measure(const R *__restrict__ f, const R *__restrict__ p, BatchLat lt, const DevState *__restrict__ st,
+                    int rs, double am, double *__restrict__ partials)
+{
+  __shared__ double smem[(256 / 32) * 7];
+  constexpr bool SPLIT = sizeof(R) == 4;
+  const int N = lt.N;
+  const size_t n3 = (size_t)N * N * N;
+  f += lt.off;
+  p += lt.off;
+  const double fr = SPLIT ? st->ref_phi[rs][0] : 0.0, pr = SPLIT ? st->ref_pi[rs][0] : 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(s % N), y = (int)((s / N) % N), x = (int)(s / ((size_t)N * N));
+    const size_t sx = ((size_t)(x + 1 == N ? 0 : x + 1) * N + y) * N + z;
+    const size_t sy = ((size_t)x * N + (y + 1 == N ? 0 : y + 1)) * N + z;
+    const size_t sz = ((size_t)x * N + y) * N + (z + 1 == N ? 0 : z + 1);
+    const double c = fr + (double)f[s], pi = pr + (double)p[s];
+    const double gx = (double)f[sx] - (double)f[s], gy = (double)f[sy] - (double)f[s], gz = (double)f[sz] - (double)f[s];
+    const double m = pi * am;
+    acc[0] += pi * pi;
+    acc[1] += (gx * gx + gy * gy + gz * gz) * lt.inv_dx2;
+    acc[2] += c;
+    acc[3] += c * c;
+    acc[4] += m;
+    acc[5] += m * m;
+    acc[6] += lt.c0q * c * c * c * c;
+  }
+  block_reduce<7, 256>(acc, smem);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 7; ++k) partials[(size_t)blockIdx.x * 7 + k] = acc[k];
+}
+
+} // namespace clb

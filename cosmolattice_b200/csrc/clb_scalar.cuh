@@ -333,21 +333,12 @@ __device__ __forceinline__ double sf_kernel(const DevState &s, const SFParams &p
   return __dmul_rn(__dmul_rn(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
 }
 
-static __global__ void __launch_bounds__(256)
-    k_tail(const double *__restrict__ partials, TailOp op, DevState *__restrict__ st, SFParams p)
+// Scale-factor bookkeeping of one tail (the flags of TailOp, in schedule order) given the volume
+// sums of <pi^2>, <grad^2> and <V>; shared by the single-lattice and the batched tails.
+__device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const SFParams &p, double pi2s, double g2s,
+                                           double pots)
 {
-  __shared__ double smem[(256 / 32) * kRedSlots];
-  double v[kRedSlots] = {0, 0, 0};
-  if (op.nblocks > 0) {
-    for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x) {
-#pragma unroll
-      for (int k = 0; k < kRedSlots; ++k) v[k] += partials[(size_t)b * kRedSlots + k];
-    }
-    block_reduce<kRedSlots, 256>(v, smem);
-  }
-  if (threadIdx.x != 0) return;
-  DevState s = *st;
-  const double pi2 = v[0] * p.inv_n3, g2 = v[1] * p.inv_n3, pot = v[2] * p.inv_n3;
+  const double pi2 = pi2s * p.inv_n3, g2 = g2s * p.inv_n3, pot = pots * p.inv_n3;
   const double dt = p.dt;
   const uint32_t fl = op.flags;
   if (fl & T_STORE_ALL) {
@@ -411,6 +402,23 @@ static __global__ void __launch_bounds__(256)
   if (!isfinite(s.aI) || !isfinite(s.aDotI) || !isfinite(s.aDotSI) || !isfinite(s.pi2AvI) ||
       !isfinite(s.grad2AvI) || !isfinite(s.potAvI))
     s.status = 1;
+}
+
+static __global__ void __launch_bounds__(256)
+    k_tail(const double *__restrict__ partials, TailOp op, DevState *__restrict__ st, SFParams p)
+{
+  __shared__ double smem[(256 / 32) * kRedSlots];
+  double v[kRedSlots] = {0, 0, 0};
+  if (op.nblocks > 0) {
+    for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x) {
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) v[k] += partials[(size_t)b * kRedSlots + k];
+    }
+    block_reduce<kRedSlots, 256>(v, smem);
+  }
+  if (threadIdx.x != 0) return;
+  DevState s = *st;
+  tail_apply(s, op, p, v[0], v[1], v[2]);
   *st = s;
 }
 

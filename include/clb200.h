@@ -233,6 +233,26 @@ int clb_forward(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, const d
                 double *observable);
 int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *grad);
 
+/* ---- batched ensemble ----------------------------------------------------------------------------
+ * No counterpart in the reference (one lattice per process, source/cosmolattice.cpp:134-201).  Many
+ * independent one-field lphi4 lattices (model kind CLB_MODEL_LPHI4, n_scalars 1) advance together:
+ * one sweep launch per VV stage covers every member, each member keeps its own scale factor and
+ * volume averages, and clb_batch_evolve runs as one CUDA graph.  Members share dt, evolver (VV
+ * family), expansion mode, precision and device, and differ in N (2..1024), dx, couplings[0] and
+ * state.  Member arrays are N^3 doubles as in clb_set_state; measurements as clb_measure. */
+typedef struct clb_batch clb_batch;
+
+int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t n, clb_batch **out);
+void clb_batch_destroy(clb_batch *b);
+const char *clb_batch_last_error(const clb_batch *b);
+int clb_batch_set_state(clb_batch *b, int32_t i, const double *fields, const double *momenta, const clb_scalefactor *sf);
+int clb_batch_get_state(clb_batch *b, int32_t i, double *fields, double *momenta, clb_scalefactor *sf);
+int clb_batch_initialize(clb_batch *b, int32_t correct_adot);
+int clb_batch_evolve(clb_batch *b, int64_t nsteps);
+int clb_batch_measure(clb_batch *b, int32_t i, double e0, clb_measurement *m);
+int clb_batch_last_evolve_ms(clb_batch *b, double *ms);
+int clb_batch_kernel_launches(clb_batch *b, int64_t *n);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
  * For callers that cannot call cudaMalloc: a runtime that owns the whole device memory pool, code
  * issued while a CUDA graph is being captured, or an embedding that forbids allocation after

@@ -1,0 +1,129 @@
+"""Batched lphi4 ensemble (clb_batch_*) against single-lattice runs (B200).
+
+FP64 batch: every member matches the CPU oracle run on its own, per site within 1e-12 after the
+run (same kernels' rounding as the single path; only the volume-sum order differs), a(t) and
+energies within 1e-10.  FP32/FP64-split batch: each member within the bounds of the
+single-lattice FP32 split test (fields 1e-6 of max |phi|, fluctuations 1e-3, a(t) 1e-7,
+Friedmann 1e-6 absolute) of its FP64 run.  Sizes are ragged and differ per member.
+"""
+import numpy as np
+import pytest
+
+from conftest import make_scalar_case
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [(8, 1.0, 1e-3, "a"), (12, 0.5, 1e-2, "b"), (16, 2.0, 3e-3, "c"), (13, 1.3, 1e-4, "d"), (33, 0.8, 5e-3, "e")]
+
+
+def members(evolver="VV2", expansion=True, dt=0.01):
+    out = []
+    for N, lam, amp, seed in MEMBERS:
+        out.append(make_scalar_case(N=N, evolver=evolver, expansion=expansion, dt=dt, seed=seed, amp=amp,
+                                    extra={"lambda_prog": lam}))
+    return out
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+def run_batch(cases, precision, steps, chunks=1):
+    from cosmolattice_b200.batch import LatticeBatch
+
+    bt = LatticeBatch([(c[2], c[1]) for c in cases], precision=precision)
+    for i, c in enumerate(cases):
+        bt.set_state(i, c[3], c[4], c[5])
+    bt.initialize()
+    m0 = [bt.measure(i) for i in range(len(cases))]
+    for _ in range(chunks):
+        bt.evolve(steps // chunks)
+    out = [bt.get_state(i) for i in range(len(cases))]
+    m1 = [bt.measure(i, m0[i]["energies"][-1]) for i in range(len(cases))]
+    bt.close()
+    return out, m0, m1
+
+
+def run_oracle(c, steps):
+    from oracle.oracle import OracleLattice
+
+    o = OracleLattice(c[2], c[1])
+    o.set_state(c[3], c[4], c[5])
+    o.initialize()
+    m0 = o.measure(1.0)
+    o.evolve(steps)
+    st = o.get_state()
+    m1 = o.measure(m0["energies"][-1])
+    o.close()
+    return st, m0, m1
+
+
+@pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV4", True), ("VV2", False)])
+def test_fp64_batch_matches_oracle_per_member(evolver, expansion):
+    cases = members(evolver, expansion)
+    out, m0, m1 = run_batch(cases, "fp64", 40, chunks=2)
+    for i, c in enumerate(cases):
+        (fo, po, so), mo0, mo1 = run_oracle(c, 40)
+        fg, pg, sg = out[i]
+        assert rel(fg, fo) < 1e-12 and rel(pg, po) < 1e-12, (i, rel(fg, fo), rel(pg, po))
+        assert abs(sg["aI"] - so["aI"]) <= 1e-10 * so["aI"]
+        for a, b in zip(m1[i]["energies"], mo1["energies"]):
+            assert abs(a - b) <= 1e-10 * abs(b) + 1e-300
+
+
+def test_fp32_batch_tracks_fp64():
+    cases = members("VV2", True)
+    g32, _, m32 = run_batch(cases, "fp32", 100)
+    g64, _, m64 = run_batch(cases, "fp64", 100)
+    for i in range(len(cases)):
+        (fa, pa, sa), (fb, pb, sb) = g32[i], g64[i]
+        assert rel(fa, fb) < 1e-6
+        assert rel(fa - fa.mean(), fb - fb.mean()) < 1e-3, (i, rel(fa - fa.mean(), fb - fb.mean()))
+        assert abs(sa["aI"] - sb["aI"]) / sb["aI"] < 1e-7
+        assert abs(m32[i]["friedmann"][0] - m64[i]["friedmann"][0]) < 1e-6
+
+
+def test_batch_equals_single_lattice_fp64_and_graph_replay():
+    # the batch member and the single-lattice handle run the same arithmetic; replaying a cached
+    # graph (same step count twice) continues the run correctly
+    from cosmolattice_b200 import Lattice
+    from cosmolattice_b200.batch import LatticeBatch
+
+    cases = members("VV2", True)[:3]
+    bt = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp64")
+    singles = []
+    for i, c in enumerate(cases):
+        bt.set_state(i, c[3], c[4], c[5])
+        s = Lattice(c[2], c[1], precision="fp64")
+        s.set_state(c[3], c[4], c[5])
+        s.initialize()
+        singles.append(s)
+    bt.initialize()
+    for _ in range(3):
+        bt.evolve(7)
+        for s in singles:
+            s.evolve(7)
+    n_launch = bt.kernel_launches()
+    assert n_launch > 0
+    for i, s in enumerate(singles):
+        fb, pb, sb = bt.get_state(i)
+        fs, ps, ss = s.get_state()
+        assert rel(fb, fs) < 1e-12 and rel(pb, ps) < 1e-12
+        assert abs(sb["aI"] - ss["aI"]) <= 1e-12 * ss["aI"]
+        s.close()
+    bt.close()
+
+
+def test_batch_rejects_mixed_members():
+    from cosmolattice_b200 import _capi
+    from cosmolattice_b200.batch import LatticeBatch
+
+    a = make_scalar_case(N=8, dt=0.01)
+    b = make_scalar_case(N=8, dt=0.02)
+    with pytest.raises(_capi.ClbError) as e:
+        LatticeBatch([(a[2], a[1]), (b[2], b[1])])
+    assert e.value.code == _capi.CLB_EINVAL
+    c = make_scalar_case(N=8, model="lphi4")
+    with pytest.raises(_capi.ClbError) as e:
+        LatticeBatch([(c[2], c[1])])
+    assert e.value.code == _capi.CLB_EUNSUPPORTED
