@@ -84,37 +84,52 @@ __global__ void __launch_bounds__(kBZ *kBY)
 
   double acc_pi2 = 0, acc_g2 = 0, acc_v = 0, acc_p = 0;
   long long cnt = 0;
-  R prev = R(0), cur = R(0), nxt = R(0), piC = R(0), piN = R(0);
   constexpr bool LOADP = KICK || (RED & 1);
-  if (x0 < x1) {
-    const int xm = x0 == 0 ? N - 1 : x0 - 1;
-    if (valid) {
-      prev = ld(sidx(xm, y, z));
-      cur = ld(sidx(x0, y, z));
-      tile[0][ty + 1][tz + 1] = cur;
-      if (ty == 0) tile[0][0][tz + 1] = ld(sidx(x0, ym, z));
-      if (ty == hy - 1) tile[0][hy + 1][tz + 1] = ld(sidx(x0, yp, z));
-      if (tz == 0) tile[0][ty + 1][0] = ld(sidx(x0, y, zm));
-      if (tz == hz - 1) tile[0][ty + 1][hz + 1] = ld(sidx(x0, y, zp));
-      if (LOADP) piC = pin[sidx(x0, y, z)];
+  // One plane's values for this thread: centre, in-plane halo values it owns, momentum.
+  struct Plane {
+    R c, h[4], pi;
+  };
+  const bool hym = ty == 0, hyp = ty == hy - 1, hzm = tz == 0, hzp = tz == hz - 1;
+  auto load = [&](int xp, bool tile_too, Plane &q) {
+    q.c = ld(sidx(xp, y, z));
+    if (tile_too) {
+      if (hym) q.h[0] = ld(sidx(xp, ym, z));
+      if (hyp) q.h[1] = ld(sidx(xp, yp, z));
+      if (hzm) q.h[2] = ld(sidx(xp, y, zm));
+      if (hzp) q.h[3] = ld(sidx(xp, y, zp));
+      if (LOADP) q.pi = pin[sidx(xp, y, z)];
     }
+  };
+  auto store = [&](int tb, const Plane &q) {
+    tile[tb][ty + 1][tz + 1] = q.c;
+    if (hym) tile[tb][0][tz + 1] = q.h[0];
+    if (hyp) tile[tb][hy + 1][tz + 1] = q.h[1];
+    if (hzm) tile[tb][ty + 1][0] = q.h[2];
+    if (hzp) tile[tb][ty + 1][hz + 1] = q.h[3];
+  };
+  auto wrapx = [&](int xx) { return xx >= N ? xx - N : xx; };
+  R prev = R(0), cur = R(0), nxt = R(0), piC = R(0), piN = R(0);
+  if (x0 < x1) {
+    // prologue: planes x0 - 1 (centre), x0 and x0 + 1; loads run two planes ahead of the compute
+    Plane q0{}, q1{};
+    if (valid) {
+      prev = ld(sidx(x0 == 0 ? N - 1 : x0 - 1, y, z));
+      load(x0, true, q0);
+      load(wrapx(x0 + 1), x0 + 1 < x1, q1);
+      store(0, q0);
+      if (x0 + 1 < x1) store(1, q1);
+      cur = q0.c;
+      piC = q0.pi;
+      nxt = q1.c;
+      piN = q1.pi;
+    }
+    __syncthreads();
     int b = 0;
     for (int x = x0; x < x1; ++x) {
-      const int bn = b == 2 ? 0 : b + 1;
-      const int xn = x + 1 == N ? 0 : x + 1;
-      const bool last = x + 1 == x1;
-      if (valid) {
-        nxt = ld(sidx(xn, y, z));
-        if (!last) {
-          tile[bn][ty + 1][tz + 1] = nxt;
-          if (ty == 0) tile[bn][0][tz + 1] = ld(sidx(xn, ym, z));
-          if (ty == hy - 1) tile[bn][hy + 1][tz + 1] = ld(sidx(xn, yp, z));
-          if (tz == 0) tile[bn][ty + 1][0] = ld(sidx(xn, y, zm));
-          if (tz == hz - 1) tile[bn][ty + 1][hz + 1] = ld(sidx(xn, y, zp));
-          if (LOADP) piN = pin[sidx(xn, y, z)];
-        }
-      }
-      __syncthreads();
+      const int b2 = b == 0 ? 2 : b - 1; // buffer of plane x + 2 (held plane x - 1)
+      const bool has2 = x + 2 <= x1, tile2 = x + 2 < x1;
+      Plane q2{};
+      if (valid && has2) load(wrapx(x + 2), tile2, q2);
       if (valid) {
         const size_t s = sidx(x, y, z);
         const R c = cur;
@@ -162,11 +177,15 @@ __global__ void __launch_bounds__(kBZ *kBY)
             acc_v += (double)Lphi4<R, 1>::V(cv, c0q, R(0));
           }
         }
+        prev = cur;
+        cur = nxt;
+        piC = piN;
+        nxt = q2.c;
+        piN = q2.pi;
+        if (tile2) store(b2, q2);
       }
-      prev = cur;
-      cur = nxt;
-      if (LOADP) piC = piN;
-      b = bn;
+      __syncthreads();
+      b = b == 2 ? 0 : b + 1;
     }
   }
   if (RED) {
