@@ -32,6 +32,7 @@ PATH_REFERENCE = 1
 
 MODEL_LPHI4 = 1
 MODEL_LPHI4U1 = 2
+MODEL_LPHI4SU2U1 = 3
 
 MAX_COUPLINGS = 8
 MAX_ENERGIES = 32
@@ -78,6 +79,7 @@ class Measurement(C.Structure):
         ("n_means", C.c_int32),
         ("means", (C.c_double * 6) * MAX_MEANS),
         ("gauss_u1", C.c_double * 3),
+        ("gauss_su2", C.c_double * 3),
     ]
 
 

@@ -52,6 +52,9 @@ def initial_scale_factor(model: Model, rp: RunParameters):
     for c in getattr(model, "piCS0", []) if getattr(model, "NCs", 0) else []:
         # Energies::kineticCS: |pi|^2 with no 1/2 (energies.h:47-50)
         kin += (c / model.fStar / model.omegaStar) ** 2
+    for c in getattr(model, "piD0", []):
+        # Energies::kineticSU2Doublet: |pi|^2 with no 1/2 (energies.h:57-60)
+        kin += (c / model.fStar / model.omegaStar) ** 2
     rho = kin + model.pot0
     return rp.a0, model.fStar / model.MPl * math.sqrt(rho / 3.0)
 
@@ -224,8 +227,88 @@ def u1_initial_state(model: Model, rp: RunParameters):
     return fields, momenta, aI, aDot
 
 
+def doublet_fluctuations(model: Model, rp: RunParameters, aDot: float):
+    """SU2Initializer::addFluctuationsSU2DoubletFromPhases (su2initializer.h:115-186): per component
+    Rayleigh amplitudes a_c and left phases l_c, one right phase r_0 and r_c = r_0 l_c conj(l_0);
+    Phi_c = a_c (l_c + r_c)/2, pi_c = -i omega_0 a_c (l_c - r_c)/2 - aDot Phi_c / sqrt(2) (the
+    reference's extra 1/sqrt(2) on the aDot term is kept), zero modes 0."""
+    N = rp.N
+    nx, ny, nz = wave_numbers(N)
+    k = np.sqrt(nx * nx + ny * ny + nz * nz) * rp.kIR
+    norms = [_fluct_norm(model, rp, k, model.masses2D[c]) for c in range(4)]
+    omega0 = norms[0][1]
+    shape = norms[0][0].shape
+
+    def rayleigh(label):
+        g = _rng(rp.baseSeed, label)
+        return np.sqrt(-2.0 * np.log1p(-g.random(shape)))
+
+    def phase(label):
+        g = _rng(rp.baseSeed, label)
+        return np.exp(2j * np.pi * g.random(shape))
+
+    amps = [norms[c][0] * rayleigh(f"normSU2Doublet_0_{c}") for c in range(4)]
+    left = [phase(f"phaseLeftSU2Doublet_0_{c}") for c in range(4)]
+    r0 = phase("phaseRightSU2Doublet_0_0")
+    right = [r0 * left[c] * np.conj(left[0]) for c in range(4)]
+    out_f, out_p = [], []
+    for c in range(4):
+        fk = amps[c] * (left[c] + right[c]) / 2.0
+        fk[0, 0, 0] = 0.0
+        pk = -1j * omega0 * amps[c] * (left[c] - right[c]) / 2.0 - aDot * fk / math.sqrt(2.0)
+        pk[0, 0, 0] = 0.0
+        out_f.append(sfft.irfftn(fk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
+        out_p.append(sfft.irfftn(pk, s=(N, N, N), axes=(0, 1, 2), workers=-1))
+    return out_f, out_p
+
+
+def su2u1_initial_state(model: Model, rp: RunParameters):
+    """lphi4SU2U1 state: ModelInitializer order (modelinitializer.h:51-66) - scale factor, scalar
+    singlet, SU(2) doublet with pi_SU2 from the SU(2) Gauss law and unit links
+    (su2initializer.h:39-88), complex scalar with pi_A from the U(1) Gauss law whose charge
+    includes the doublet (u1initializer.h:77-117, mattercurrents.h:27-48)."""
+    aI, aDot = initial_scale_factor(model, rp)
+    N = rp.N
+    fields = np.zeros((22, N, N, N))
+    momenta = np.zeros((19, N, N, N))
+    phi, pi = scalar_fluctuations(model, rp, 0, aDot)
+    fields[0] = phi + model.fldS0[0] / model.fStar
+    momenta[0] = pi + model.piS0[0] / model.fStar / model.omegaStar
+    fl, pl = doublet_fluctuations(model, rp, aDot)
+    for c in range(4):
+        fields[3 + c] = fl[c] + model.fldD0[c] / model.fStar
+        momenta[3 + c] = pl[c] + model.piD0[c] / model.fStar / model.omegaStar
+    # SU(2) charge density rho_b = (fStar/omegaStar)^2 / 2 g Re((i s_b Phi)^+ pi_Phi)
+    u = fields[3] + 1j * fields[4]
+    v = fields[5] + 1j * fields[6]
+    pu = momenta[3] + 1j * momenta[4]
+    pv = momenta[5] + 1j * momenta[6]
+    isig = [(1j * v, 1j * u), (v, -u), (1j * u, -1j * v)]
+    r2 = (model.fStar / model.omegaStar) ** 2
+    for b in range(3):
+        a, c = isig[b]
+        rho = r2 / 2 * (model.gQ_S * np.real(np.conj(a) * pu + np.conj(c) * pv))
+        pa = gauss_solve_u1(rp, rho / rp.dx)  # j0 = -dx rho (gauss_solve_u1 applies -dx^2)
+        for i in range(3):
+            momenta[10 + 3 * i + b] = pa[i]
+    for i in range(3):
+        fields[10 + 4 * i] = 1.0
+    fl, pl = complex_scalar_fluctuations(model, rp, aDot)
+    for c in range(2):
+        fields[1 + c] = fl[c] + model.fldCS0[c] / model.fStar
+        momenta[1 + c] = pl[c] + model.piCS0[c] / model.fStar / model.omegaStar
+    rho = 2.0 / rp.dx * r2 * (model.gQ_C * (momenta[1] * fields[2] - momenta[2] * fields[1])
+                              + model.gQ_D * np.imag(np.conj(pu) * u + np.conj(pv) * v))
+    pa = gauss_solve_u1(rp, rho)
+    for i in range(3):
+        momenta[7 + i] = pa[i]
+    return fields, momenta, aI, aDot
+
+
 def initial_state(model: Model, rp: RunParameters):
     """Initial state of any supported model (ModelInitializer::initialize, modelinitializer.h:47-81)."""
+    if getattr(model, "NSU2", 0):
+        return su2u1_initial_state(model, rp)
     if getattr(model, "NU1", 0):
         return u1_initial_state(model, rp)
     return scalar_initial_state(model, rp)

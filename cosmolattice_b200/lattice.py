@@ -81,9 +81,9 @@ class Lattice:
         self._check(self.lib.clb_set_state(self.h, _dp(f), _dp(p), C.byref(s) if s is not None else None))
 
     def get_state(self, fields: bool = True, momenta: bool = True):
-        n = self.n_field_components * self.rp.N ** 3
-        f = np.empty(n) if fields else None
-        p = np.empty(n) if momenta else None
+        n3 = self.rp.N ** 3
+        f = np.empty(self.n_field_components * n3) if fields else None
+        p = np.empty(self.n_momentum_components * n3) if momenta else None
         sf = _capi.ScaleFactor()
         self._check(self.lib.clb_get_state(self.h, _dp(f) if fields else None, _dp(p) if momenta else None, C.byref(sf)))
         sfd = {k: getattr(sf, k) for k, _ in _capi.ScaleFactor._fields_}
@@ -124,8 +124,8 @@ class Lattice:
 
     def backward(self, through_init: bool = True):
         """clb_backward: (fields_bar, momenta_bar, grad dict) of the last forward's observable."""
-        n = self.n_field_components * self.rp.N ** 3
-        fb, pb = np.empty(n), np.empty(n)
+        n3 = self.rp.N ** 3
+        fb, pb = np.empty(self.n_field_components * n3), np.empty(self.n_momentum_components * n3)
         g = _capi.AdjointGrad()
         self._check(self.lib.clb_backward(self.h, 1 if through_init else 0, _dp(fb), _dp(pb), C.byref(g)))
         return fb, pb, {
@@ -175,6 +175,7 @@ def measurement_to_dict(m: _capi.Measurement) -> Dict[str, object]:
         "friedmann": [m.friedmann[i] for i in range(3)],
         "means": [[m.means[f][j] for j in range(6)] for f in range(m.n_means)],
         "gauss_u1": [m.gauss_u1[i] for i in range(3)],
+        "gauss_su2": [m.gauss_su2[i] for i in range(3)],
     }
 
 

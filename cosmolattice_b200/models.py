@@ -250,4 +250,93 @@ class lphi4U1(Model):
         return [self.c4, self.gQ]
 
 
-MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f, "lphi4U1": lphi4U1}
+def _deriv2_component(nd, nd2, comps, c):
+    """deriv2ComponentFromNorm (potential.h:36-42) at a homogeneous point."""
+    n2 = sum(v * v for v in comps)
+    n = math.sqrt(n2)
+    return 1.0 / n2 * nd2 * comps[c] ** 2 + nd / n * (1 - comps[c] ** 2 / n2)
+
+
+class lphi4SU2U1(Model):
+    """models/lphi4SU2U1.h: real scalar S, complex scalar phi (U(1) charge), SU(2) doublet Phi
+    (U(1) and SU(2) charges), one U(1) and one SU(2) gauge field.
+
+    V = c4 |Phi|^4 + qG (|Phi| S)^2 + 2 qH (|Phi| |phi|)^2 in program units (lphi4SU2U1.h:147-160;
+    c4 = lambda_prog, 1 in the header).  Keys: lambda, qG, qH, initial_amplitudes,
+    initial_momenta, cmplx_field_initial_norm, cmplx_momentum_initial_norm,
+    SU2Doublet_initial_norm, SU2Doublet_initial_momenta_norm, gU1s, gSU2s, CSU1_charges,
+    SU2DoubletU1_charges, SU2DoubletSU2_charges (defaults 1; complexscalarbase.h:71-72,
+    su2doubletbase.h:74-80).  Rescaling (lphi4SU2U1.h:118-121): alpha = 1, fStar = |Phi_0|,
+    omegaStar = sqrt(lambda) |Phi_0|.  Device components: fields S, phi (2), Phi (4), A (3), SU(2)
+    links (3 x 4 quaternion components); momenta S, phi (2), Phi (4), A (3), SU(2) (3 x 3).
+    """
+
+    name = "lphi4SU2U1"
+    kind = _capi.MODEL_LPHI4SU2U1
+    Ns = 1
+    NCs = 1
+    NU1 = 1
+    NSU2Doublet = 1
+    NSU2 = 1
+    NPotTerms = 3
+    n_components = 22
+    n_momentum_components = 19
+
+    def __init__(self, par: ParameterParser, rp: RunParameters):
+        super().__init__(par, rp)
+        self.lam = par.get_float("lambda")
+        self.c4 = par.get_float("lambda_prog", 1.0)
+        self.qG = par.get_float("qG")
+        self.qH = par.get_float("qH")
+        self.fldS0 = [par.get_float("initial_amplitudes", 0.0)]
+        self.piS0 = [par.get_float("initial_momenta", 0.0)]
+        nC = par.get_float("cmplx_field_initial_norm", 0.0)
+        npC = par.get_float("cmplx_momentum_initial_norm", 0.0)
+        self.fldCS0 = [nC / math.sqrt(2.0)] * 2
+        self.piCS0 = [npC / math.sqrt(2.0)] * 2
+        nD = par.get_float("SU2Doublet_initial_norm")
+        npD = par.get_float("SU2Doublet_initial_momenta_norm", 0.0)
+        self.fldD0 = [nD / 2] * 4
+        self.piD0 = [npD / 2] * 4
+        gU1 = par.get_floats("gU1s", 1, [1.0])
+        gSU2 = par.get_floats("gSU2s", 1, [1.0])
+        cs_u1 = CouplingsManager([[True]])
+        cs_u1.set_effective_charges(par.get_floats("CSU1_charges", 1, [1.0]), gU1)
+        d_u1 = CouplingsManager([[True]])
+        d_u1.set_effective_charges(par.get_floats("SU2DoubletU1_charges", 1, [1.0]), gU1)
+        d_su2 = CouplingsManager([[True]])
+        d_su2.set_effective_charges(par.get_floats("SU2DoubletSU2_charges", 1, [1.0]), gSU2)
+        self.gQ_C, self.gQ_D, self.gQ_S = cs_u1(0, 0), d_u1(0, 0), d_su2(0, 0)
+        self.alpha = 1.0
+        self.fStar = nD
+        self.omegaStar = math.sqrt(self.lam) * nD
+        if par.has("fluct_amplitude"):
+            self.fluct_amplitude = par.get_float("fluct_amplitude")
+        self.set_initial_potential_and_masses_from_potential()
+
+    def _norms(self, S, C, D):
+        return math.sqrt(sum(v * v for v in D)), math.sqrt(sum(v * v for v in C)), S
+
+    def set_initial_potential_and_masses_from_potential(self) -> None:
+        """abstractmodel.h:220-248 with the zero-condensate floor 1e-14 (abstractmodel.h:282)."""
+        S = self.fldS0[0] / self.fStar
+        C = [v / self.fStar for v in self.fldCS0]
+        D = [v / self.fStar for v in self.fldD0]
+        if C[0] == 0 and C[1] == 0:
+            C = [1e-14 * 0.70710678118654752] * 2
+        if all(v == 0 for v in D):
+            D = [1e-14 / 2] * 4
+        nD, nC, _ = self._norms(S, C, D)
+        self.pot0 = self.c4 * nD ** 4 + self.qG * (nD * S) ** 2 + 2 * self.qH * (nD * nC) ** 2
+        self.masses2S = [2 * self.qG * nD ** 2]
+        ndC, nd2C = 4 * self.qH * nD ** 2 * nC, 4 * self.qH
+        self.masses2CS = [_deriv2_component(ndC, nd2C, C, c) for c in range(2)]
+        ndD = 4 * self.c4 * nD ** 3 + nD * (2 * self.qG * S ** 2 + 4 * self.qH * nC ** 2)
+        nd2D = 12 * self.c4 * nD ** 2 + 2 * self.qG * S ** 2 + 4 * self.qH * nC ** 2
+        self.masses2D = [_deriv2_component(ndD, nd2D, D, c) for c in range(4)]
+
+    def couplings(self):
+        return [self.qG, self.qH, self.gQ_C, self.gQ_D, self.gQ_S, self.c4]
+
+
+MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f, "lphi4U1": lphi4U1, "lphi4SU2U1": lphi4SU2U1}

@@ -62,6 +62,7 @@ extern "C" {
  *                       charge (CouplingsManager, couplingsmanager.h:167-218).  Components, fields and
  *                       momenta alike: Re phi, Im phi, A_1, A_2, A_3 (program units; n_scalars = 0). */
 #define CLB_MODEL_LPHI4U1 2
+#define CLB_MODEL_LPHI4SU2U1 3
 
 #define CLB_MAX_COUPLINGS 8
 
@@ -116,6 +117,7 @@ typedef struct clb_measurement {
   double means[CLB_MAX_MEANS][6];
   /* GaussLaws::checkU1 (gausslaws.h:34-53): av|LHS-RHS| / av|LHS^2 sum + RHS^2|, av|LHS|, av|RHS| */
   double gauss_u1[3];
+  double gauss_su2[3];  /* lphi4SU2U1: checkSU2 (gausslaws.h:56-80), same three numbers as gauss_u1 */
 } clb_measurement;
 
 typedef struct clb_handle clb_handle;

@@ -328,6 +328,7 @@ struct Handle {
 };
 inline Handle *H(void *h) { return reinterpret_cast<Handle *>(h); }
 inline bool isU1(void *h) { return H(h)->kind == CLB_MODEL_LPHI4U1; }
+inline bool isSU2(void *h) { return H(h)->kind == CLB_MODEL_LPHI4SU2U1; }
 inline Oracle *S(void *h) { return reinterpret_cast<Oracle *>(H(h)->impl); }
 
 } // namespace
@@ -339,12 +340,19 @@ typedef struct orc_handle orc_handle;
 const char *orc_last_error(orc_handle *h)
 {
   if (!h) return g_err.c_str();
+  if (isSU2(h)) return oracle_models::su2_err(H(h)->impl).c_str();
   return isU1(h) ? oracle_models::u1_err(H(h)->impl).c_str() : S(h)->err.c_str();
 }
 
 int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out)
 {
   if (!cfg || !md || !out) { g_err = "null argument"; return CLB_EINVAL; }
+  if (md->kind == CLB_MODEL_LPHI4SU2U1) {
+    void *u = oracle_models::su2_create(cfg, md, g_err);
+    if (!u) return CLB_EINVAL;
+    *out = reinterpret_cast<orc_handle *>(new Handle{CLB_MODEL_LPHI4SU2U1, u});
+    return CLB_OK;
+  }
   if (md->kind == CLB_MODEL_LPHI4U1) {
     void *u = oracle_models::u1_create(cfg, md, g_err);
     if (!u) return CLB_EINVAL;
@@ -375,7 +383,9 @@ int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out
 void orc_destroy(orc_handle *h)
 {
   if (!h) return;
-  if (isU1(h))
+  if (isSU2(h))
+    oracle_models::su2_destroy(H(h)->impl);
+  else if (isU1(h))
     oracle_models::u1_destroy(H(h)->impl);
   else
     delete S(h);
@@ -384,6 +394,7 @@ void orc_destroy(orc_handle *h)
 
 int orc_set_state(orc_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
 {
+  if (isSU2(h)) return oracle_models::su2_set_state(H(h)->impl, fields, momenta, sf);
   if (isU1(h)) return oracle_models::u1_set_state(H(h)->impl, fields, momenta, sf);
   Oracle *o = S(h);
   std::memcpy(o->fld.data(), fields, o->fld.size() * sizeof(double));
@@ -398,6 +409,7 @@ int orc_set_state(orc_handle *h, const double *fields, const double *momenta, co
 
 int orc_get_state(orc_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
 {
+  if (isSU2(h)) return oracle_models::su2_get_state(H(h)->impl, fields, momenta, sf);
   if (isU1(h)) return oracle_models::u1_get_state(H(h)->impl, fields, momenta, sf);
   Oracle *o = S(h);
   if (fields) std::memcpy(fields, o->fld.data(), o->fld.size() * sizeof(double));
@@ -412,6 +424,7 @@ int orc_get_state(orc_handle *h, double *fields, double *momenta, clb_scalefacto
 // ModelInitializer tail (modelinitializer.h:74-80) then the evolver constructor (leapfrog.h:35).
 int orc_initialize(orc_handle *h, int32_t correct_adot)
 {
+  if (isSU2(h)) return oracle_models::su2_initialize(H(h)->impl, correct_adot);
   if (isU1(h)) return oracle_models::u1_initialize(H(h)->impl, correct_adot);
   Oracle *o = S(h);
   o->setAllAverages();
@@ -428,6 +441,7 @@ int orc_initialize(orc_handle *h, int32_t correct_adot)
 
 int orc_evolve(orc_handle *h, int64_t n)
 {
+  if (isSU2(h)) return oracle_models::su2_evolve(H(h)->impl, n);
   if (isU1(h)) return oracle_models::u1_evolve(H(h)->impl, n);
   Oracle *o = S(h);
   if (!o->initialized) { o->err = "evolve before initialize"; return CLB_ESTATE; }
@@ -442,6 +456,7 @@ int orc_evolve(orc_handle *h, int64_t n)
 
 int orc_sync(orc_handle *h)
 {
+  if (isSU2(h)) return oracle_models::su2_sync(H(h)->impl);
   if (isU1(h)) return oracle_models::u1_sync(H(h)->impl);
   Oracle *o = S(h);
   if (o->cfg.evolver == CLB_LF) o->syncLF();
@@ -452,6 +467,7 @@ int orc_sync(orc_handle *h)
 // (meansmeasurer.h:28-48), ScaleFactorMeasurer (scalefactormeasurer.h:37-48).
 int orc_measure(orc_handle *h, double e0, clb_measurement *m)
 {
+  if (isSU2(h)) return oracle_models::su2_measure(H(h)->impl, e0, m);
   if (isU1(h)) return oracle_models::u1_measure(H(h)->impl, e0, m);
   Oracle *o = S(h);
   std::memset(m, 0, sizeof(*m));

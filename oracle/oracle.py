@@ -80,6 +80,7 @@ class OracleLattice:
             raise RuntimeError(self.lib.orc_last_error(None).decode())
         self.h = h
         self.n_components = getattr(model, "n_components", model.Ns)
+        self.n_momentum_components = getattr(model, "n_momentum_components", self.n_components)
 
     def close(self):
         if getattr(self, "h", None):
@@ -105,9 +106,9 @@ class OracleLattice:
         self._check(self.lib.orc_set_state(self.h, _dp(f), _dp(p), C.byref(s) if s is not None else None))
 
     def get_state(self, fields=True, momenta=True):
-        n = self.n_components * self.rp.N ** 3
-        f = np.empty(n)
-        p = np.empty(n)
+        n3 = self.rp.N ** 3
+        f = np.empty(self.n_components * n3)
+        p = np.empty(self.n_momentum_components * n3)
         sf = self.capi.ScaleFactor()
         self._check(self.lib.orc_get_state(self.h, _dp(f), _dp(p), C.byref(sf)))
         return f, p, {k: getattr(sf, k) for k, _ in self.capi.ScaleFactor._fields_}

@@ -59,6 +59,31 @@ def make_u1_case(N=12, evolver="VV2", expansion=True, dt=0.01, seed="u", amp=1e-
     return par, rp, m, f, p, sf
 
 
+def make_su2_case(N=8, evolver="VV2", expansion=True, dt=0.005, seed="s", amp=1e-2, gU1=0.35, gSU2=0.6,
+                  qG=50.0, qH=50.0, kcut=None, extra=None):
+    """lphi4SU2U1 parameter set, run parameters, model and initial state (lphi4SU2U1.in values for
+    the homogeneous doublet, qG and qH; the gauge couplings of the 384^3 case)."""
+    from cosmolattice_b200 import MODELS, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import su2u1_initial_state
+
+    params = {
+        "N": N, "kIR": 1.0, "dt": dt, "evolver": evolver, "expansion": "true" if expansion else "false",
+        "lambda": 1.0, "qG": qG, "qH": qH, "initial_amplitudes": 0.0, "initial_momenta": 0.0,
+        "cmplx_field_initial_norm": 0.0, "cmplx_momentum_initial_norm": 0.0,
+        "SU2Doublet_initial_norm": "5.25151e18", "SU2Doublet_initial_momenta_norm": 0.0,
+        "gU1s": gU1, "gSU2s": gSU2, "fluct_amplitude": amp,
+        "kCutOff": kcut if kcut is not None else N / 4.0, "baseSeed": seed,
+    }
+    if extra:
+        params.update(extra)
+    par = ParameterParser(params=params)
+    rp = RunParameters(par)
+    m = MODELS["lphi4SU2U1"](par, rp)
+    f, p, aI, aD = su2u1_initial_state(m, rp)
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+    return par, rp, m, f, p, sf
+
+
 @pytest.fixture(scope="session")
 def gpu_available():
     try:
