@@ -11,13 +11,15 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libclb200.so")
 
-SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_noalloc.cu"]
-DEPS = ["clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_batch.cuh", "clb_vv.h", "clb_adjoint.cuh", "clb_noalloc.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
+SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_su2.cu", "clb_batch.cu", "clb_noalloc.cu"]
+# per-unit flags: the lphi4SU2U1 unit writes the reference's rounding order as plain expressions
+UNIT_FLAGS = {"clb_su2.cu": ["-fmad=false"]}
+DEPS = ["clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_batch.cuh", "clb_vv.h", "clb_adjoint.cuh", "clb_su2.cu", "clb_su2.cuh", "clb_noalloc.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -34,10 +36,25 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB, "-lcufft"]
+    objs = []
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(src):
+        obj = os.path.join(LIB_DIR, src.replace(".cu", ".o"))
+        cmd = [nvcc, *NVCC_FLAGS, *UNIT_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(one, SOURCES))
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB, "-lcufft"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    for o in objs:
+        os.remove(o)
     return LIB
 
 

@@ -54,6 +54,16 @@ int u1_measure(clb_handle *h, double e0, clb_measurement *m);
 int u1_forward(clb_handle *h, int64_t nsteps, int32_t K, const double *w, int32_t nw, double *obs);
 int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *out);
 
+// lphi4SU2U1 (clb_su2.cu)
+int su2_create(clb_handle *h);
+void su2_destroy(clb_handle *h);
+int su2_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf);
+int su2_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
+int su2_initialize(clb_handle *h, int32_t correct_adot);
+int su2_evolve(clb_handle *h, int64_t n);
+int su2_sync(clb_handle *h);
+int su2_measure(clb_handle *h, double e0, clb_measurement *m);
+
 // Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
 __attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
 } // namespace clb
@@ -414,7 +424,12 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   }
   *out = nullptr;
   const bool u1 = md->kind == CLB_MODEL_LPHI4U1;
-  if (md->kind != CLB_MODEL_LPHI4 && !u1) {
+  const bool su2 = md->kind == CLB_MODEL_LPHI4SU2U1;
+  if (su2 && cfg->precision != CLB_PREC_FP64) {
+    g_err = "clb_create: lphi4SU2U1 runs in FP64 storage";
+    return CLB_EUNSUPPORTED;
+  }
+  if (md->kind != CLB_MODEL_LPHI4 && !u1 && !su2) {
     g_err = "clb_create: unknown model kind";
     return CLB_EUNSUPPORTED;
   }
@@ -422,7 +437,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     g_err = "clb_create: lphi4U1 runs in FP64 storage";
     return CLB_EUNSUPPORTED;
   }
-  if (!u1 && (md->n_scalars < 1 || md->n_scalars > 2)) {
+  if (!u1 && !su2 && (md->n_scalars < 1 || md->n_scalars > 2)) {
     g_err = "clb_create: lphi4 supports 1 or 2 scalar singlets";
     return CLB_EUNSUPPORTED;
   }
@@ -468,9 +483,9 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   h->md = *md;
   h->N = cfg->N;
   h->n3 = (size_t)cfg->N * cfg->N * cfg->N;
-  if (u1) {
+  if (u1 || su2) {
     h->ws = ws;
-    const int r = u1_create(h);
+    const int r = u1 ? u1_create(h) : su2_create(h);
     if (r != CLB_OK) {
       g_err = std::string("clb_create: device allocation failed: ") + cudaGetErrorString(cudaGetLastError());
       clb_destroy(h);
@@ -568,6 +583,7 @@ void clb_destroy(clb_handle *h)
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
   u1_destroy(h);
+  su2_destroy(h);
   for (int b = 0; b < 2; ++b) {
     if (h->fld[b]) cudaFree(h->fld[b]);
     if (h->pi[b]) cudaFree(h->pi[b]);
@@ -599,7 +615,7 @@ int clb_num_components(const clb_handle *h, int32_t *nf, int32_t *np)
 {
   if (!h) return CLB_EINVAL;
   if (nf) *nf = h->NS;
-  if (np) *np = h->NS;
+  if (np) *np = h->su2 ? 19 : h->NS;
   return CLB_OK;
 }
 
@@ -607,6 +623,7 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
 {
   if (!h || !fields || !momenta) return h ? h->fail(CLB_EINVAL, "clb_set_state: null argument") : CLB_EINVAL;
   if (h->u1) return u1_set_state(h, fields, momenta, sf);
+  if (h->su2) return su2_set_state(h, fields, momenta, sf);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->cf = h->cp = 0;
@@ -659,6 +676,7 @@ int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefacto
 {
   if (!h) return CLB_EINVAL;
   if (h->u1) return u1_get_state(h, fields, momenta, sf);
+  if (h->su2) return su2_get_state(h, fields, momenta, sf);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
   DevState cur;
@@ -694,8 +712,8 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
 {
   if (!h) return CLB_EINVAL;
   if (!h->has_state) return h->fail(CLB_ESTATE, "clb_initialize: no state uploaded");
-  if (h->u1) {
-    const int r = u1_initialize(h, correct_adot);
+  if (h->u1 || h->su2) {
+    const int r = h->u1 ? u1_initialize(h, correct_adot) : su2_initialize(h, correct_adot);
     if (r == CLB_OK) h->initialized = true;
     return r;
   }
@@ -722,8 +740,8 @@ int clb_evolve(clb_handle *h, int64_t n)
     if (e != cudaSuccess) return h->fail(CLB_ENOMEM, std::string("clb_evolve: history buffer: ") + cudaGetErrorString(e));
     h->hist_cap = n;
   }
-  if (h->u1) {
-    const int r = u1_evolve(h, n);
+  if (h->u1 || h->su2) {
+    const int r = h->u1 ? u1_evolve(h, n) : su2_evolve(h, n);
     if (r == CLB_OK && h->cfg.expansion) h->hist_rows = n;
     return r;
   }
@@ -806,6 +824,7 @@ int clb_sync(clb_handle *h)
   if (!h) return CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_sync: call clb_initialize first");
   if (h->u1) return u1_sync(h);
+  if (h->su2) return su2_sync(h);
   if (h->cfg.evolver == CLB_LF) dispatch<SyncLF>(h);
   return sync_and_check(h, "clb_sync");
 }
@@ -815,6 +834,7 @@ int clb_measure(clb_handle *h, double e0, clb_measurement *m)
   if (!h || !m) return h ? h->fail(CLB_EINVAL, "clb_measure: null argument") : CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_measure: call clb_initialize first");
   if (h->u1) return u1_measure(h, e0, m);
+  if (h->su2) return su2_measure(h, e0, m);
   DevState s;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost);
@@ -916,7 +936,7 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
 {
   if (!h) return CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_spectrum: call clb_initialize first");
-  if (h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_spectrum: scalar-singlet models only");
+  if (h->u1 || h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_spectrum: scalar-singlet models only");
   if (which < 0 || which > 1 || comp < 0 || comp >= h->NS)
     return h->fail(CLB_EINVAL, "clb_spectrum: which must be 0 (field) or 1 (momentum) and comp a scalar index");
   if (ps_type < 1 || ps_type > 2) return h->fail(CLB_EINVAL, "powerSpectrumType " + std::to_string(ps_type) + " is not a valid powerSpectrumType.");

@@ -14,8 +14,10 @@
 
 namespace clb {
 struct U1Sector;
+struct SU2Sector;
 }
 using clb::U1Sector;
+using clb::SU2Sector;
 using namespace clb;
 
 struct clb_handle {
@@ -50,7 +52,8 @@ struct clb_handle {
   dim3 sweep_grid;
   int sweep_blocks = 0;
   std::string err;
-  U1Sector *u1 = nullptr; // complex scalar + U(1) sector state (clb_u1.cu), null for scalar models
+  U1Sector *u1 = nullptr;   // complex scalar + U(1) sector state (clb_u1.cu), null for other models
+  SU2Sector *su2 = nullptr; // lphi4SU2U1 state (clb_su2.cu), null for other models
 
   // instrumentation: launch counts always; per-launch CUDA events on the stream when prof
   bool prof = false;

@@ -53,7 +53,9 @@ enum TailFlags : uint32_t {
   T_LF_SYNC = 1u << 9,      // aDotI = aDotSI + dt/2 F                 (leapfrog.h:111)
   T_LF_CTOR = 1u << 10,     // aDotSI = aDotI - dt/2 F                 (leapfrog.h:35)
   T_CORRECT_ADOT = 1u << 11,// aDotI = sqrt(Friedmann RHS)             (modelinitializer.h:77-78)
-  T_HIST_EARLY = 1u << 12   // history row right after the field averages (LF step end)
+  T_HIST_EARLY = 1u << 12,  // history row right after the field averages (LF step end)
+  T_STORE_PI2_B = 1u << 13  // a two-kick sweep's second momentum sums become the cached <pi^2>
+                            // (after T_VV_KICK_HALF; the gauge sectors' tails)
 };
 
 struct TailOp {
@@ -130,6 +132,22 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *smem /* [N
       for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
       v[k] = s;
     }
+  }
+}
+
+// Periodic neighbour offsets of site s = (x N + y) N + z: op[d] to x + d, om[d] to x - d.
+__device__ __forceinline__ void u1_offsets(int N, size_t s, long long (&op)[3], long long (&om)[3])
+{
+  const int z = (int)(s % (size_t)N);
+  const size_t t = s / (size_t)N;
+  const int y = (int)(t % (size_t)N);
+  const int x = (int)(t / (size_t)N);
+  const int c[3] = {x, y, z};
+  const long long st[3] = {(long long)N * N, (long long)N, 1};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    op[d] = c[d] + 1 == N ? -(long long)(N - 1) * st[d] : st[d];
+    om[d] = c[d] == 0 ? (long long)(N - 1) * st[d] : -st[d];
   }
 }
 

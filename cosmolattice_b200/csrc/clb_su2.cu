@@ -1,0 +1,381 @@
+// clb_su2.cu - lphi4SU2U1 (real scalar, complex scalar, SU(2) doublet, U(1) and SU(2) fields)
+// behind the libclb200 C ABI.  Compiled without FMA contraction (see build.py): the kernels'
+// plain expressions then round in the reference's order.
+//
+// Schedules restate VelocityVerlet::evolve (velocityverlet.h:51-114) and LeapFrog::evolve / sync
+// (leapfrog.h:42-116) with every sector of the model; the second kick of a VV stage and the first
+// of the next share one sweep (no field or a(t) change in between), as in the other sectors.
+
+#include "clb_handle.cuh"
+#include "clb_su2.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace clb {
+
+using namespace su2d;
+
+namespace {
+constexpr int kSU2Blocks = 148 * 8; // 128-thread grid-stride sweeps
+}
+
+struct SU2Sector {
+  double *f = nullptr, *p = nullptr; // 22 and 19 x N^3
+  State *d_st = nullptr;
+  double *d_part = nullptr, *d_sums = nullptr;
+  Params prm{};
+};
+
+namespace {
+
+Params su2_params(const clb_handle *h)
+{
+  Params a{};
+  const clb_config &c = h->cfg;
+  const clb_model_desc &m = h->md;
+  a.N = c.N;
+  a.n3 = h->n3;
+  a.dx = c.dx;
+  a.dx2 = c.dx * c.dx;
+  a.inv_dx2 = 1.0 / (c.dx * c.dx);
+  a.inv_dx = 1.0 / c.dx;
+  a.qG = m.couplings[0];
+  a.qH = m.couplings[1];
+  a.gC = m.couplings[2];
+  a.gD = m.couplings[3];
+  a.gS = m.couplings[4];
+  a.c4 = m.couplings[5];
+  const double rfo = m.fStar / m.omegaStar, rof = m.omegaStar / m.fStar;
+  a.rfo2 = rfo * rfo;
+  a.rof2 = rof * rof;
+  const double fm = m.fStar / m.MPl;
+  a.alpha = m.alpha;
+  a.fm2 = fm * fm;
+  a.dt = c.dt;
+  a.inv_n3 = 1.0 / (double)h->n3;
+  return a;
+}
+
+void coefs(State &s, double al)
+{
+  s.kA = std::pow(s.aI, 1 + al);
+  s.kB = std::pow(s.aI, 3 + al);
+  s.kB2 = std::pow(s.aI, 3 + al) / 2;
+  s.kG = std::pow(s.aI, -1 + al);
+  s.p3 = std::pow(s.aSI, al - 3);
+  s.p1 = std::pow(s.aSI, al - 1);
+}
+
+// Kick factors (velocityverlet.h:129-162; leapfrog.h:131-170): S (w dt)/2, phi, Phi and SU(2)
+// (dt/2) w, U(1) (dt w)/2 on the VV; (w dt) for all on the leapfrog.
+Kick vv_kick(double dt, double wa, double wb)
+{
+  Kick k{};
+  const double w[2] = {wa, wb};
+  for (int i = 0; i < 2; ++i) {
+    k.h[i][0] = w[i] * dt / 2;
+    k.h[i][1] = k.h[i][2] = k.h[i][4] = dt / 2 * w[i];
+    k.h[i][3] = dt * w[i] / 2;
+  }
+  return k;
+}
+Kick lf_kick(double dt, double w)
+{
+  Kick k{};
+  for (int g = 0; g < 5; ++g) k.h[0][g] = w * dt;
+  return k;
+}
+
+void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
+{
+  SU2Sector *u = h->su2;
+  const int kind = nk == 0 ? K_U1_REDUCE : K_U1_KICK;
+#define CLB_SU2K(NK, RF, RP)                                                                                            \
+  CLB_LAUNCH(h, kind, k_kick<NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(u->f, u->p, u->prm, kc, u->d_st, u->d_part))
+  if (nk == 0) {
+    if (rf && rp)
+      CLB_SU2K(0, true, true);
+    else if (rf)
+      CLB_SU2K(0, true, false);
+    else
+      CLB_SU2K(0, false, true);
+  } else if (nk == 1) {
+    if (rf && rp)
+      CLB_SU2K(1, true, true);
+    else if (rp)
+      CLB_SU2K(1, false, true);
+    else
+      CLB_SU2K(1, false, false);
+  } else {
+    if (rf && rp)
+      CLB_SU2K(2, true, true);
+    else
+      CLB_SU2K(2, false, false);
+  }
+#undef CLB_SU2K
+}
+
+void drift(clb_handle *h, double w, bool lf)
+{
+  SU2Sector *u = h->su2;
+  CLB_LAUNCH(h, K_U1_DRIFT, k_drift<<<kSU2Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, w, lf ? 1 : 0, u->d_st));
+}
+
+void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
+{
+  SU2Sector *u = h->su2;
+  TailOp op{flags, reduced ? kSU2Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
+  CLB_LAUNCH(h, K_TAIL, su2d::k_tail<<<1, 256, 0, h->stream>>>(u->d_part, op, u->d_st, u->prm));
+}
+
+int check(clb_handle *h, const char *where)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  collect_profile(h);
+  State s;
+  e = cudaMemcpy(&s, h->su2->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  if (s.status != 0) return h->fail(CLB_ENONFINITE, std::string(where) + ": a volume average or a(t) is not finite");
+  return CLB_OK;
+}
+
+} // namespace
+
+__attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
+{
+  SU2Sector *u = new SU2Sector();
+  h->su2 = u;
+  h->NS = NF;
+  u->prm = su2_params(h);
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->f, NF * h->n3 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->p, NP * h->n3 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMemset(u->f, 0, NF * h->n3 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMemset(u->p, 0, NP * h->n3 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_st, sizeof(State)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_part, (size_t)kSU2Blocks * kMeas * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_sums, kMeas * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaEventCreate(&h->ev_call[0]) == cudaSuccess && cudaEventCreate(&h->ev_call[1]) == cudaSuccess;
+  if (!ok) return CLB_ENOMEM;
+  State s{};
+  s.aI = s.aSI = s.aIM = 1.0;
+  coefs(s, h->md.alpha);
+  return cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice) == cudaSuccess ? CLB_OK : CLB_ECUDA;
+}
+
+__attribute__((visibility("hidden"))) void su2_destroy(clb_handle *h)
+{
+  SU2Sector *u = h->su2;
+  if (!u) return;
+  for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums})
+    if (q) cudaFree(q);
+  delete u;
+  h->su2 = nullptr;
+}
+
+__attribute__((visibility("hidden"))) int su2_set_state(clb_handle *h, const double *fields, const double *momenta,
+                                                        const clb_scalefactor *sf)
+{
+  SU2Sector *u = h->su2;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  State s{};
+  s.aI = s.aSI = s.aIM = 1.0;
+  if (sf) {
+    s.aI = sf->aI;
+    s.aSI = sf->aSI;
+    s.aIM = sf->aIM;
+    s.aDotI = sf->aDotI;
+    s.aDotSI = sf->aDotSI;
+    s.aDotSIM = sf->aDotSIM;
+  }
+  coefs(s, h->md.alpha);
+  if ((e = cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice)) != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  h->has_state = true;
+  h->initialized = false;
+  h->synced = true;
+  return CLB_OK;
+}
+
+__attribute__((visibility("hidden"))) int su2_get_state(clb_handle *h, double *fields, double *momenta,
+                                                        clb_scalefactor *sf)
+{
+  SU2Sector *u = h->su2;
+  State s;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess && fields) e = cudaMemcpyAsync(fields, u->f, NF * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && momenta) e = cudaMemcpyAsync(momenta, u->p, NP * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
+  if (sf) {
+    sf->aI = s.aI;
+    sf->aSI = s.aSI;
+    sf->aIM = s.aIM;
+    sf->aDotI = s.aDotI;
+    sf->aDotSI = s.aDotSI;
+    sf->aDotSIM = s.aDotSIM;
+  }
+  return CLB_OK;
+}
+
+__attribute__((visibility("hidden"))) int su2_initialize(clb_handle *h, int32_t correct_adot)
+{
+  sweep(h, 0, true, true, Kick{});
+  uint32_t fl = T_STORE_ALL;
+  if (h->cfg.expansion && correct_adot) fl |= T_CORRECT_ADOT;
+  if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
+  tail(h, fl, true);
+  h->synced = true;
+  return check(h, "clb_initialize");
+}
+
+__attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nsteps)
+{
+  const double dt = h->cfg.dt;
+  const bool ex = h->cfg.expansion != 0;
+  cudaEventRecord(h->ev_call[0], h->stream);
+  if (h->cfg.evolver == CLB_LF) {
+    sweep(h, 1, false, ex, lf_kick(dt, h->synced ? 0.5 : 1.0));
+    if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
+    for (int64_t s = 0; s < nsteps; ++s) {
+      drift(h, 1.0, true);
+      if (s + 1 < nsteps) {
+        sweep(h, 1, ex, ex, lf_kick(dt, 1.0));
+        if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true, 0, 0, s);
+      } else if (ex) {
+        sweep(h, 0, true, false, Kick{});
+        tail(h, T_STORE_FIELDS | T_HIST_EARLY, true, 0, 0, s);
+      }
+    }
+    h->synced = false;
+  } else {
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    const int64_t total = nsteps * (int64_t)S;
+    const double w0 = wof(0);
+    if (ex) tail(h, T_VV_KICK_HALF, false, 0, w0);
+    sweep(h, 1, false, ex, vv_kick(dt, w0, 0.0));
+    if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w0);
+    for (int64_t k = 0; k < total; ++k) {
+      const size_t i = (size_t)(k % (int64_t)S);
+      const double w = wof(i);
+      const bool more = k + 1 < total;
+      const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+      drift(h, w, false);
+      sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
+      if (ex) {
+        uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
+        if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
+        tail(h, fl, true, w, wn, i + 1 == S ? k / (int64_t)S : -1);
+      }
+    }
+  }
+  cudaEventRecord(h->ev_call[1], h->stream);
+  const int r = check(h, "clb_evolve");
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, h->ev_call[0], h->ev_call[1]) == cudaSuccess) h->last_evolve_ms = ms;
+  return r;
+}
+
+__attribute__((visibility("hidden"))) int su2_sync(clb_handle *h)
+{
+  if (h->cfg.evolver == CLB_LF && !h->synced) {
+    sweep(h, 1, false, h->cfg.expansion != 0, lf_kick(h->cfg.dt, 0.5));
+    if (h->cfg.expansion) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
+  }
+  h->synced = true;
+  return check(h, "clb_sync");
+}
+
+// Measurement (energiesmeasurer.h:45-122 and the sector measurers): energies E_kin, E_grad of S,
+// phi, Phi; E_el, E_mag of U(1) and SU(2); the three potential terms; E_tot.  Means rows: S,
+// sqrt2 Re phi, sqrt2 Im phi, |phi|, |Phi|, U(1) |E| |B|, SU(2) |E| |B|.  Both Gauss checks.
+// Energies::rho's setAllAverages side effect (energies.h:219) is applied to the cached averages.
+__attribute__((visibility("hidden"))) int su2_measure(clb_handle *h, double e0, clb_measurement *m)
+{
+  SU2Sector *u = h->su2;
+  State s;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  const double al = h->md.alpha;
+  const double am = std::pow(s.aI, al - 3), ag = std::pow(s.aI, al - 1);
+  CLB_LAUNCH(h, K_MEASURE, su2d::k_measure<<<kSU2Blocks, 128, 0, h->stream>>>(u->f, u->p, u->prm, am, ag, u->d_part));
+  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeas><<<1, 256, 0, h->stream>>>(u->d_part, kSU2Blocks, u->d_sums));
+  double v[kMeas];
+  e = cudaMemcpyAsync(v, u->d_sums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  collect_profile(h);
+  const double inv = u->prm.inv_n3;
+  for (double &x : v) x *= inv;
+  // setAllAverages
+  for (int g = 0; g < 5; ++g) s.pi2[g] = s.pi2SI[g] = v[g];
+  s.g2S = v[5];
+  s.g2C = v[6];
+  s.g2D = v[7];
+  s.b2A = v[8];
+  s.b2G = v[9];
+  s.potI = v[10];
+  std::memset(m, 0, sizeof(*m));
+  const En E = energies_of(s, u->prm);
+  const double en[10] = {E.ks, E.gs, E.kc, E.gc, E.kd, E.gd, E.ea, E.ba, E.eg, E.bg};
+  double Etot = 0;
+  int k = 0;
+  for (int i = 0; i < 10; ++i) {
+    m->energies[k++] = en[i];
+    Etot += en[i];
+  }
+  for (int i = 0; i < 3; ++i) {
+    m->energies[k++] = v[11 + i];
+    Etot += v[11 + i];
+  }
+  m->energies[k++] = Etot;
+  m->n_energies = k;
+  if (h->cfg.expansion) {
+    const double LHS = s.aDotI * s.aDotI;
+    const double RHS = std::pow(s.aI, 2 * al + 2) / 3. * u->prm.fm2 * rho_of(s, u->prm);
+    m->friedmann[0] = (LHS - RHS) / (LHS + RHS);
+    m->friedmann[1] = LHS;
+    m->friedmann[2] = RHS;
+  } else {
+    m->friedmann[0] = std::fabs(1.0 - Etot / e0);
+  }
+  if ((e = cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice)) != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  for (int r = 0; r < 7; ++r) {
+    const double a1 = v[14 + 4 * r], a2 = v[15 + 4 * r], b1 = v[16 + 4 * r], b2 = v[17 + 4 * r];
+    const double r1 = a2 - a1 * a1, rr = b2 - b1 * b1;
+    m->means[r][0] = a1;
+    m->means[r][1] = b1;
+    m->means[r][2] = a2;
+    m->means[r][3] = b2;
+    m->means[r][4] = r1 > 0 ? std::sqrt(r1) : 0;
+    m->means[r][5] = rr > 0 ? std::sqrt(rr) : 0;
+  }
+  m->n_means = 7;
+  m->gauss_u1[0] = v[42] / v[43];
+  m->gauss_u1[1] = v[45];
+  m->gauss_u1[2] = v[44];
+  double gs[4] = {0, 0, 0, 0};
+  for (int b = 0; b < 3; ++b)
+    for (int q = 0; q < 4; ++q) gs[q] = b == 0 ? v[46 + 4 * b + q] : gs[q] + v[46 + 4 * b + q];
+  m->gauss_su2[0] = gs[0] / gs[1];
+  m->gauss_su2[1] = gs[3];
+  m->gauss_su2[2] = gs[2];
+  m->aI = s.aI;
+  m->aDotI = s.aDotI;
+  m->hubble = s.aDotI / s.aI;
+  return CLB_OK;
+}
+
+} // namespace clb

@@ -61,22 +61,6 @@ __device__ __forceinline__ double u1_a(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double u1_s(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double u1_d(double a, double b) { return __ddiv_rn(a, b); }
 
-// Periodic neighbour offsets of site s = (x N + y) N + z: op[d] to x + d, om[d] to x - d.
-__device__ __forceinline__ void u1_offsets(int N, size_t s, long long (&op)[3], long long (&om)[3])
-{
-  const int z = (int)(s % (size_t)N);
-  const size_t t = s / (size_t)N;
-  const int y = (int)(t % (size_t)N);
-  const int x = (int)(t / (size_t)N);
-  const int c[3] = {x, y, z};
-  const long long st[3] = {(long long)N * N, (long long)N, 1};
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    op[d] = c[d] + 1 == N ? -(long long)(N - 1) * st[d] : st[d];
-    om[d] = c[d] == 0 ? (long long)(N - 1) * st[d] : -st[d];
-  }
-}
-
 // Per-site kernel values.  Fields f: [Re phi, Im phi, A_x, A_y, A_z] x n3.
 struct U1Site {
   double fr, fi;            // phi(x)
@@ -247,7 +231,7 @@ __global__ void __launch_bounds__(256)
 
 // Drifts phi += ((pow(aSI, alpha-3) dt) w) pi_phi and A += ((pow(aSI, alpha-1) w) dt) pi_A
 // (velocityverlet.h:193-210; the leapfrog's forms leapfrog.h:203-217 are w = 1).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_u1_drift(double *__restrict__ f, const double *__restrict__ p, size_t n3, double w, double dt,
                const U1State *__restrict__ st)
 {
@@ -272,12 +256,10 @@ __device__ __forceinline__ double u1_sf_kernel(const U1State &s, const U1Params 
   return u1_m(u1_m(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
 }
 
-// Second momentum slots of a two-kick sweep become the cached <pi^2> (after T_VV_KICK_HALF).
-constexpr uint32_t T_STORE_PI2_B = 1u << 13;
 
 // One-thread tail: fixed-order sum of the kick-sweep partials and the scale-factor update, in
 // the order of the VelocityVerlet and LeapFrog schedules (same flags as the scalar tail).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_u1_tail(const double *__restrict__ partials, TailOp op, U1State *__restrict__ st, U1Params p)
 {
   __shared__ double smem[(256 / 32) * kU1Red];
@@ -378,7 +360,7 @@ __global__ void __launch_bounds__(256)
 // [5..10] Re phi, (Re phi)^2, Im phi, (Im phi)^2, |phi|, |phi|^2, [11..16] the same of pi_phi,
 // [17] |pi_A|, [18] |B|, [19..22] Gauss |LHS - RHS|, |sum of squares|, |RHS|, |LHS|
 // (gausslaws.h:34-53 with U1ChargeDensity, mattercurrents.h:27-48).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_u1_measure(const double *__restrict__ f, const double *__restrict__ p, U1Params a, double *__restrict__ partials)
 {
   __shared__ double smem[(256 / 32) * kU1Meas];

@@ -1,0 +1,144 @@
+"""Parity of the CUDA lphi4SU2U1 path with the FP64 CPU oracle (B200).
+
+Same bars as the other sectors: per-site fields and momenta within 1e-12 relative (to each
+component's max |value|) after 100 steps; a(t), aDot, energies, means and the Gauss averages
+within 1e-10 relative, the Gauss ratios within 1e-8 relative (difference of nearly equal
+terms).  Both Gauss laws are preserved per site on the GPU too.
+"""
+import numpy as np
+import pytest
+
+from conftest import make_su2_case
+
+pytestmark = pytest.mark.gpu
+
+SITE_TOL = 1e-12
+AVG_TOL = 1e-10
+RATIO_TOL = 1e-8
+
+
+def rel_comp(a, b, nc):
+    a = np.asarray(a).reshape(nc, -1)
+    b = np.asarray(b).reshape(nc, -1)
+    out = []
+    for c in range(nc):
+        sc = np.abs(b[c]).max()
+        out.append(np.abs(a[c] - b[c]).max() / sc if sc > 0 else np.abs(a[c]).max())
+    return max(out)
+
+
+def random_links(f, rng, s=0.1):
+    f = f.copy()
+    N = f.shape[1]
+    for i in range(3):
+        q = rng.normal(0, s, (4, N, N, N))
+        q[0] += 1
+        f[10 + 4 * i:14 + 4 * i] = q / np.sqrt((q * q).sum(axis=0))
+    f[7:10] = rng.normal(0, 0.2, (3, N, N, N))
+    return f
+
+
+def run_pair(N, evolver, expansion, nsteps, measure_every=None, links=False):
+    from cosmolattice_b200 import Lattice
+    from oracle.oracle import OracleLattice
+
+    par, rp, m, f, p, sf = make_su2_case(N=N, evolver=evolver, expansion=expansion, amp=3e-2)
+    if links:
+        f = random_links(f, np.random.default_rng(4))
+    gpu = Lattice(m, rp)
+    cpu = OracleLattice(m, rp)
+    meas = {"gpu": [], "cpu": []}
+    for key, lat in (("gpu", gpu), ("cpu", cpu)):
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.sync()
+        m0 = lat.measure(1.0)
+        e0 = m0["energies"][-1]
+        meas[key].append(m0)
+        done = 0
+        while done < nsteps:
+            k = nsteps - done if measure_every is None else min(measure_every, nsteps - done)
+            lat.evolve(k)
+            done += k
+            if measure_every is not None:
+                lat.sync()
+                meas[key].append(lat.measure(e0))
+        lat.sync()
+        meas[key].append(lat.measure(e0))
+    out = (gpu.get_state(), cpu.get_state(), meas)
+    gpu.close()
+    cpu.close()
+    return out
+
+
+def check(g, c, meas):
+    (fg, pg, sg), (fc, pc, sc) = g, c
+    assert rel_comp(fg, fc, 22) < SITE_TOL, rel_comp(fg, fc, 22)
+    assert rel_comp(pg, pc, 19) < SITE_TOL, rel_comp(pg, pc, 19)
+    for k in ("aI", "aDotI"):
+        assert abs(sg[k] - sc[k]) <= AVG_TOL * max(abs(sc[k]), 1e-300), (k, sg[k], sc[k])
+    for a, b in zip(meas["gpu"], meas["cpu"]):
+        assert len(a["energies"]) == len(b["energies"]) == 14
+        for ea, eb in zip(a["energies"], b["energies"]):
+            assert abs(ea - eb) <= AVG_TOL * abs(eb) + 1e-30, (a["energies"], b["energies"])
+        for k in (1, 2):
+            assert abs(a["friedmann"][k] - b["friedmann"][k]) <= AVG_TOL * abs(b["friedmann"][k]) + 1e-300
+        assert len(a["means"]) == len(b["means"]) == 7
+        for ra, rb in zip(a["means"], b["means"]):
+            scales = [max(abs(rb[0]), rb[4]), max(abs(rb[1]), rb[5]), abs(rb[2]), abs(rb[3])]
+            for x, y, s in zip(ra[:4], rb[:4], scales):
+                assert abs(x - y) <= AVG_TOL * max(s, 1e-300) + 1e-30, (ra, rb)
+        for key in ("gauss_u1", "gauss_su2"):
+            ga, gb = a[key], b[key]
+            for k in (1, 2):
+                assert abs(ga[k] - gb[k]) <= AVG_TOL * abs(gb[k]) + 1e-300, (key, ga, gb)
+            assert abs(ga[0] - gb[0]) <= RATIO_TOL * abs(gb[0]) + 1e-300, (key, ga, gb)
+
+
+@pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV2", False), ("VV4", True), ("LF", True)])
+def test_lphi4su2u1_100_steps(evolver, expansion):
+    g, c, meas = run_pair(8, evolver, expansion, 100)
+    check(g, c, meas)
+
+
+@pytest.mark.parametrize("evolver", ["VV2", "LF"])
+def test_lphi4su2u1_links_and_measure_cadence(evolver):
+    g, c, meas = run_pair(7, evolver, True, 40, measure_every=9, links=True)
+    check(g, c, meas)
+
+
+def test_gauss_laws_preserved_on_gpu():
+    from cosmolattice_b200 import Lattice
+
+    from test_oracle_su2 import gauss_fields
+
+    par, rp, m, f, p, sf = make_su2_case(N=12, evolver="VV2", expansion=True, amp=5e-2)
+    f = random_links(f, np.random.default_rng(9), 0.05)
+    g1a, g2a, rho = gauss_fields(rp, m, f.ravel(), p.ravel())
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(100)
+    f1, p1, _ = lat.get_state()
+    lat.close()
+    g1b, g2b, _ = gauss_fields(rp, m, f1, p1)
+    assert np.abs(g1b - g1a).max() < 1e-12 * np.abs(rho).max() * rp.dx
+    assert np.abs(g2b - g2a).max() < 1e-11 * np.abs(g2a).max() + 1e-14
+    U = f1.reshape(22, -1)[10:].reshape(3, 4, -1)
+    assert np.abs((U * U).sum(axis=1) - 1).max() < 1e-13
+
+
+def test_su2_rejects_unsupported():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_su2_case(N=6)
+    with pytest.raises(_capi.ClbError) as e:
+        Lattice(m, rp, precision="fp32")
+    assert e.value.code == _capi.CLB_EUNSUPPORTED
+    lat = Lattice(m, rp)
+    assert (lat.n_field_components, lat.n_momentum_components) == (22, 19)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    with pytest.raises(_capi.ClbError):
+        lat.spectrum(which=0)
+    lat.close()
