@@ -48,7 +48,7 @@ def parse_args():
     ap.add_argument("--N", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--config", default="lphi4", choices=["lphi4", "lphi4U1-adjoint", "batched"],
+    ap.add_argument("--config", default="lphi4", choices=["lphi4", "lphi4U1-adjoint", "batched", "lphi4SU2U1"],
                     help="lphi4: the headline 512^3 scalar workload; lphi4U1-adjoint: 128^3 VV4 gauge "
                          "run with the adjoint gradient and its finite-difference check; batched: 384 "
                          "lphi4 lattices of 32^3-96^3 in one graph-captured ensemble")
@@ -482,8 +482,84 @@ def main_batched(args):
     print(json.dumps(line))
 
 
+def main_su2(args):
+    """lphi4SU2U1, N^3 (default 384), dt = 0.005, VV2, self-consistent expansion, lambda = 1,
+    g_SU2 = 0.6, g_U1 = 0.35, qG = qH = 50 and the homogeneous doublet of lphi4SU2U1.in, unit links,
+    fluctuations of relative amplitude 1e-3 cut at N kIR / 4: FP64 site-updates/s with both Gauss
+    checks, energies and a doublet spectrum at the start and the end."""
+    import torch
+
+    from cosmolattice_b200 import MODELS, Lattice, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import su2u1_initial_state
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    N = args.N if args.N != 512 else 384
+    steps = args.steps if args.steps != 2000 else 1000
+    par = ParameterParser(params={
+        "N": N, "kIR": 1.0, "dt": 0.005, "evolver": "VV2", "expansion": "true", "lambda": 1.0, "qG": 50, "qH": 50,
+        "initial_amplitudes": 0.0, "initial_momenta": 0.0, "cmplx_field_initial_norm": 0.0,
+        "cmplx_momentum_initial_norm": 0.0, "SU2Doublet_initial_norm": "5.25151e18",
+        "SU2Doublet_initial_momenta_norm": 0.0, "gU1s": 0.35, "gSU2s": 0.6, "fluct_amplitude": 1e-3,
+        "kCutOff": N / 4.0, "baseSeed": f"cfg4-{rank}"})
+    rp = RunParameters(par)
+    m = MODELS["lphi4SU2U1"](par, rp)
+    t0 = time.perf_counter()
+    f, p, aI, aD = su2u1_initial_state(m, rp)
+    ic_s = time.perf_counter() - t0
+    lat = Lattice(m, rp, device=local)
+    lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
+    del f, p
+    lat.initialize()
+    lat.sync()
+    m0 = lat.measure(1.0)
+    k0, s0, _ = lat.spectrum(which=0, comp=3)
+    lat.evolve(args.warmup)
+    lat.set_profiling(True)
+    lat.reset_stats()
+    with ClockSampler(local) as clk:
+        lat.evolve(steps)
+    ms = lat.last_evolve_ms()
+    stats = lat.kernel_stats()
+    lat.set_profiling(False)
+    lat.sync()
+    m1 = lat.measure(m0["energies"][-1])
+    k1, s1, _ = lat.spectrum(which=0, comp=3)
+    lat.close()
+    if rank != 0:
+        return
+    sites = N ** 3
+    peak, peak_kind = measured_peaks()
+    kick = stats.get("gauge_kick_sweep", {})
+    kick_ms = kick["total_ms"] / kick["timed_launches"] if kick.get("timed_launches") else None
+    line = {
+        "metric": "site-updates/s (lphi4SU2U1, FP64)", "value": sites * steps / (ms * 1e-3), "unit": "site-updates/s",
+        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic (seeded doublet, complex-scalar and scalar fluctuations; unit links)",
+        "config": {"workload": f"lphi4SU2U1 {N}^3 VV2 dt=0.005 gSU2=0.6 gU1=0.35 lambda=1 qG=qH=50, expansion, {steps} steps"},
+        "roofline": {"bound": "hbm", "kernel": "kick sweep (all five sectors)", "launch_ms": kick_ms,
+                     "algorithmic_bytes_per_launch": sites * 8 * (22 + 2 * 19),
+                     "achieved": (sites * 8 * (22 + 2 * 19) / (kick_ms * 1e-3) / 1e9) if kick_ms else None,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"},
+        "gauss_su2": {"start": m0["gauss_su2"], "end": m1["gauss_su2"]},
+        "gauss_u1": {"start": m0["gauss_u1"], "end": m1["gauss_u1"]},
+        "energies_start": m0["energies"], "energies_end": m1["energies"],
+        "friedmann_end": m1["friedmann"], "a_end": m1["aI"],
+        "doublet_spectrum_bins": len(s1), "doublet_spectrum_end_head": [float(x) for x in s1[:8]],
+        "initial_state_s": ic_s,
+        "kernel_launches": {k: v["launches"] for k, v in stats.items() if v["launches"]},
+        "fp32_form": "not built for lphi4SU2U1 (FP64 storage only)",
+        "adjoint": "not built for lphi4SU2U1",
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse_args()
+    if args.config == "lphi4SU2U1":
+        return main_su2(args)
     if args.config == "batched":
         return main_batched(args)
     if args.config == "lphi4U1-adjoint":

@@ -64,6 +64,9 @@ int su2_evolve(clb_handle *h, int64_t n);
 int su2_sync(clb_handle *h);
 int su2_measure(clb_handle *h, double e0, clb_measurement *m);
 
+const double *u1_component(clb_handle *h, int which, int comp, bool *gauge);
+const double *su2_component(clb_handle *h, int which, int comp, bool *gauge);
+
 // Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
 __attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
 } // namespace clb
@@ -936,8 +939,15 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
 {
   if (!h) return CLB_EINVAL;
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_spectrum: call clb_initialize first");
-  if (h->u1 || h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_spectrum: scalar-singlet models only");
-  if (which < 0 || which > 1 || comp < 0 || comp >= h->NS)
+  const bool gauge_model = h->u1 || h->su2;
+  bool gauge_comp = false;
+  const double *plain = nullptr;
+  if (gauge_model) {
+    if (which < 0 || which > 1) return h->fail(CLB_EINVAL, "clb_spectrum: which must be 0 (field) or 1 (momentum)");
+    plain = h->u1 ? u1_component(h, which, comp, &gauge_comp) : su2_component(h, which, comp, &gauge_comp);
+    if (!plain) return h->fail(CLB_EINVAL, "clb_spectrum: component index out of range");
+  }
+  if (!gauge_model && (which < 0 || which > 1 || comp < 0 || comp >= h->NS))
     return h->fail(CLB_EINVAL, "clb_spectrum: which must be 0 (field) or 1 (momentum) and comp a scalar index");
   if (ps_type < 1 || ps_type > 2) return h->fail(CLB_EINVAL, "powerSpectrumType " + std::to_string(ps_type) + " is not a valid powerSpectrumType.");
   if (ps_version < 1 || ps_version > 2)
@@ -976,18 +986,21 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
     }
     h->spec_nbins_cap = nbins;
   }
-  void *src = which == 0 ? h->fld[h->cf] : h->pi[h->cp];
-  const size_t comp_off = (size_t)comp * (size_t)h->pd.comp;
-  double ref = 0.0;
-  if (h->fp32) {
-    DevState cur;
-    if ((e = cudaMemcpy(&cur, h->d_st, sizeof(cur), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
-    ref = which == 0 ? cur.ref_phi[h->rs][comp] : cur.ref_pi[h->rs][comp];
+  if (plain) {
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather_plain<<<kElemBlocks, 256, 0, h->stream>>>(plain, h->d_spec, N));
+  } else {
+    void *src = which == 0 ? h->fld[h->cf] : h->pi[h->cp];
+    const size_t comp_off = (size_t)comp * (size_t)h->pd.comp;
+    double ref = 0.0;
+    if (h->fp32) {
+      DevState cur;
+      if ((e = cudaMemcpy(&cur, h->d_st, sizeof(cur), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+      ref = which == 0 ? cur.ref_phi[h->rs][comp] : cur.ref_pi[h->rs][comp];
+      CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + comp_off, h->d_spec, h->pd, ref));
+    } else {
+      CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(src) + comp_off, h->d_spec, h->pd, ref));
+    }
   }
-  if (h->fp32)
-    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + comp_off, h->d_spec, h->pd, ref));
-  else
-    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(src) + comp_off, h->d_spec, h->pd, ref));
   if (cufftExecD2Z(h->plan, h->d_spec, reinterpret_cast<cufftDoubleComplex *>(h->d_spec)) != CUFFT_SUCCESS)
     return h->fail(CLB_ECUDA, "clb_spectrum: cufftExecD2Z failed");
   const size_t smem = (size_t)nbins * (2 * sizeof(double) + sizeof(unsigned long long));
@@ -1011,15 +1024,26 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
   collect_profile(h);
-  DevState s;
-  if ((e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+  double aI = 1.0;
+  if (gauge_model) {
+    clb_scalefactor sf;
+    const int r = h->u1 ? u1_get_state(h, nullptr, nullptr, &sf) : su2_get_state(h, nullptr, nullptr, &sf);
+    if (r != CLB_OK) return r;
+    aI = sf.aI;
+  } else {
+    DevState s;
+    if ((e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
+    aI = s.aI;
+  }
   // PowerSpectrumMeasurer::powerSpectrum normalisation (powerspectrum.h:95-106)
   const double pi = 3.14159265358979323846;
   const double dx = h->cfg.dx;
   const double kIR = 2 * pi / (N * dx);
   double N5 = 1;
   for (int i = 0; i < 5; ++i) N5 *= (double)N;
-  const double mom_factor = which == 1 ? std::pow(s.aI, 2 * h->md.alpha - 6) : 1.0; // scalarsingletmeasurer.h:80
+  // momenta: a^{2 alpha - 6} for matter (scalarsingletmeasurer.h:80), a^{2 alpha - 2} for gauge
+  // components (u1measurer.h:102-103)
+  const double mom_factor = which == 1 ? std::pow(aI, 2 * h->md.alpha - (gauge_comp ? 2 : 6)) : 1.0;
   for (int b = 0; b < nbins; ++b) {
     const double sum = sums[b], nsum = sums[nbins + b];
     const unsigned long long c = cnt[b];

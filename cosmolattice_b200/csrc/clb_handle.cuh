@@ -111,8 +111,8 @@ enum KKind {
 const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
                                           "scalar_drift",       "reduce_pi2",        "reduce_fields",
                                           "tail",               "measure",           "convert",
-                                          "spectrum",           "u1_kick_sweep",     "u1_drift",
-                                          "u1_reduce",          "u1_adjoint_sweep"};
+                                          "spectrum",           "gauge_kick_sweep",  "gauge_drift",
+                                          "gauge_reduce",       "u1_adjoint_sweep"};
 
 cudaEvent_t take_event(clb_handle *h)
 {

@@ -28,6 +28,17 @@ __global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, 
   }
 }
 
+// Unpadded N^3 component (x slowest) -> real input of an in-place R2C transform.
+__global__ void __launch_bounds__(256) k_spec_gather_plain(const double *__restrict__ src, double *__restrict__ dst, int N)
+{
+  const long long pitch = 2LL * (N / 2 + 1);
+  for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
+    const double *s = src + r * N;
+    double *d = dst + r * pitch;
+    for (int z = threadIdx.x; z < N; z += blockDim.x) d[z] = s[z];
+  }
+}
+
 // One block per group of (kx, ky) rows; shared-memory histograms of sum w |f|^2, sum w |n| and the
 // integer mode count, written as one partial row per block.
 __global__ void __launch_bounds__(256)

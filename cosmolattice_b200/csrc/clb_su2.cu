@@ -378,4 +378,13 @@ __attribute__((visibility("hidden"))) int su2_measure(clb_handle *h, double e0, 
   return CLB_OK;
 }
 
+// Device array of one state component (clb_spectrum): which 0 fields (22), 1 momenta (19); gauge
+// tells whether the component belongs to the U(1) or SU(2) field.
+__attribute__((visibility("hidden"))) const double *su2_component(clb_handle *h, int which, int comp, bool *gauge)
+{
+  if (comp < 0 || comp >= (which == 0 ? NF : NP)) return nullptr;
+  *gauge = comp >= 7;
+  return (which == 0 ? h->su2->f : h->su2->p) + (size_t)comp * h->n3;
+}
+
 } // namespace clb

@@ -759,4 +759,13 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
   return check(h, "clb_backward");
 }
 
+// Device array of one state component (clb_spectrum): which 0 fields, 1 momenta; gauge tells
+// whether the component belongs to the U(1) field.
+__attribute__((visibility("hidden"))) const double *u1_component(clb_handle *h, int which, int comp, bool *gauge)
+{
+  if (comp < 0 || comp >= 5) return nullptr;
+  *gauge = comp >= 2;
+  return (which == 0 ? h->u1->f : h->u1->p) + (size_t)comp * h->n3;
+}
+
 } // namespace clb

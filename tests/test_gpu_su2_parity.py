@@ -140,5 +140,11 @@ def test_su2_rejects_unsupported():
     lat.set_state(f, p, sf)
     lat.initialize()
     with pytest.raises(_capi.ClbError):
-        lat.spectrum(which=0)
+        lat.spectrum(which=1, comp=19)
+    from oracle.spectrum import spectrum
+
+    fg, _, _ = lat.get_state()
+    k, v, c = lat.spectrum(which=0, comp=3)
+    ko, vo, co = spectrum(fg.reshape(22, 6, 6, 6)[3], rp.dx)
+    assert c.tolist() == co.tolist() and np.abs(v - vo).max() <= 1e-10 * np.abs(vo).max()
     lat.close()

@@ -156,8 +156,31 @@ def test_u1_rejects_unsupported_requests():
     lat.set_state(f, p, sf)
     lat.initialize()
     with pytest.raises(_capi.ClbError) as e:
-        lat.spectrum(which=0)
-    assert e.value.code == _capi.CLB_EUNSUPPORTED
+        lat.spectrum(which=0, comp=5)
+    assert e.value.code == _capi.CLB_EINVAL
     with pytest.raises(ValueError):
         lat.set_state(f[:2], p[:2], sf)
+    lat.close()
+
+
+def test_u1_spectra_match_numpy():
+    # field and momentum spectra of matter (a^{2 alpha - 6}) and gauge (a^{2 alpha - 2}) components
+    from cosmolattice_b200 import Lattice
+    from oracle.spectrum import spectrum
+
+    N = 16
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver="VV2", expansion=True)
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(20)
+    fg, pg, s = lat.get_state()
+    fg, pg = fg.reshape(5, N, N, N), pg.reshape(5, N, N, N)
+    for which, arr in ((0, fg), (1, pg)):
+        for comp in (0, 1, 3):
+            fac = 1.0 if which == 0 else s["aI"] ** (2 * m.alpha - (2 if comp >= 2 else 6))
+            k, v, c = lat.spectrum(which=which, comp=comp)
+            ko, vo, co = spectrum(arr[comp], rp.dx, factor=fac)
+            assert c.tolist() == co.tolist()
+            assert np.abs(v - vo).max() <= 1e-10 * np.abs(vo).max()
     lat.close()
