@@ -508,50 +508,68 @@ def main_su2(args):
     t0 = time.perf_counter()
     f, p, aI, aD = su2u1_initial_state(m, rp)
     ic_s = time.perf_counter() - t0
-    lat = Lattice(m, rp, device=local)
-    lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
+    sf = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+
+    def run(precision):
+        lat = Lattice(m, rp, precision=precision, device=local)
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.sync()
+        m0 = lat.measure(1.0)
+        lat.evolve(args.warmup)
+        lat.set_profiling(True)
+        lat.reset_stats()
+        with ClockSampler(local) as clk:
+            lat.evolve(steps)
+        ms = lat.last_evolve_ms()
+        stats = lat.kernel_stats()
+        lat.set_profiling(False)
+        lat.sync()
+        m1 = lat.measure(m0["energies"][-1])
+        k1, s1, _ = lat.spectrum(which=0, comp=3)
+        lat.close()
+        return {"ms": ms, "stats": stats, "m0": m0, "m1": m1, "spec": s1, "clocks": clk.summary()}
+
+    r64 = run("fp64")
+    r32 = run("fp32")
     del f, p
-    lat.initialize()
-    lat.sync()
-    m0 = lat.measure(1.0)
-    k0, s0, _ = lat.spectrum(which=0, comp=3)
-    lat.evolve(args.warmup)
-    lat.set_profiling(True)
-    lat.reset_stats()
-    with ClockSampler(local) as clk:
-        lat.evolve(steps)
-    ms = lat.last_evolve_ms()
-    stats = lat.kernel_stats()
-    lat.set_profiling(False)
-    lat.sync()
-    m1 = lat.measure(m0["energies"][-1])
-    k1, s1, _ = lat.spectrum(which=0, comp=3)
-    lat.close()
     if rank != 0:
         return
     sites = N ** 3
     peak, peak_kind = measured_peaks()
-    kick = stats.get("gauge_kick_sweep", {})
-    kick_ms = kick["total_ms"] / kick["timed_launches"] if kick.get("timed_launches") else None
+
+    def roof(r, esz):
+        kick = r["stats"].get("gauge_kick_sweep", {})
+        kms = kick["total_ms"] / kick["timed_launches"] if kick.get("timed_launches") else None
+        byts = sites * esz * (22 + 2 * 19)
+        return {"bound": "hbm", "kernel": "kick sweep (all five sectors)", "launch_ms": kms,
+                "algorithmic_bytes_per_launch": byts, "achieved": byts / (kms * 1e-3) / 1e9 if kms else None,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": (byts / (kms * 1e-3) / 1e9) / peak if kms else None}
+
+    m64, m32 = r64["m1"], r32["m1"]
     line = {
-        "metric": "site-updates/s (lphi4SU2U1, FP64)", "value": sites * steps / (ms * 1e-3), "unit": "site-updates/s",
-        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "metric": "site-updates/s (lphi4SU2U1)", "value": sites * steps / (r64["ms"] * 1e-3), "unit": "site-updates/s",
+        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": r64["ms"] / steps, "higher_is_better": True,
         "dtype": "f64", "data": "synthetic (seeded doublet, complex-scalar and scalar fluctuations; unit links)",
         "config": {"workload": f"lphi4SU2U1 {N}^3 VV2 dt=0.005 gSU2=0.6 gU1=0.35 lambda=1 qG=qH=50, expansion, {steps} steps"},
-        "roofline": {"bound": "hbm", "kernel": "kick sweep (all five sectors)", "launch_ms": kick_ms,
-                     "algorithmic_bytes_per_launch": sites * 8 * (22 + 2 * 19),
-                     "achieved": (sites * 8 * (22 + 2 * 19) / (kick_ms * 1e-3) / 1e9) if kick_ms else None,
-                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"},
-        "gauss_su2": {"start": m0["gauss_su2"], "end": m1["gauss_su2"]},
-        "gauss_u1": {"start": m0["gauss_u1"], "end": m1["gauss_u1"]},
-        "energies_start": m0["energies"], "energies_end": m1["energies"],
-        "friedmann_end": m1["friedmann"], "a_end": m1["aI"],
-        "doublet_spectrum_bins": len(s1), "doublet_spectrum_end_head": [float(x) for x in s1[:8]],
+        "roofline": roof(r64, 8),
+        "fp32": {"value": sites * steps / (r32["ms"] * 1e-3), "ms_per_step": r32["ms"] / steps,
+                 "speedup_vs_fp64": r64["ms"] / r32["ms"], "roofline": roof(r32, 4),
+                 "unitarize_every": 10,
+                 "a_rel_diff": abs(m32["aI"] - m64["aI"]) / m64["aI"],
+                 "energy_rel_diff": max(abs(x - y) / abs(y) for x, y in zip(m32["energies"], m64["energies"]) if y != 0),
+                 "gauss_su2_end": m32["gauss_su2"], "gauss_u1_end": m32["gauss_u1"],
+                 "spectrum_rel_diff": float(abs(r32["spec"] - r64["spec"]).max() / abs(r64["spec"]).max())},
+        "gauss_su2": {"start": r64["m0"]["gauss_su2"], "end": m64["gauss_su2"]},
+        "gauss_u1": {"start": r64["m0"]["gauss_u1"], "end": m64["gauss_u1"]},
+        "energies_start": r64["m0"]["energies"], "energies_end": m64["energies"],
+        "friedmann_end": m64["friedmann"], "a_end": m64["aI"],
+        "doublet_spectrum_bins": len(r64["spec"]), "doublet_spectrum_end_head": [float(x) for x in r64["spec"][:8]],
         "initial_state_s": ic_s,
-        "kernel_launches": {k: v["launches"] for k, v in stats.items() if v["launches"]},
-        "fp32_form": "not built for lphi4SU2U1 (FP64 storage only)",
+        "kernel_launches": {k: v["launches"] for k, v in r64["stats"].items() if v["launches"]},
         "adjoint": "not built for lphi4SU2U1",
-        "clocks": clk.summary(),
+        "clocks": r64["clocks"], "clocks_fp32": r32["clocks"],
     }
     print(json.dumps(line))
 

@@ -428,10 +428,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   *out = nullptr;
   const bool u1 = md->kind == CLB_MODEL_LPHI4U1;
   const bool su2 = md->kind == CLB_MODEL_LPHI4SU2U1;
-  if (su2 && cfg->precision != CLB_PREC_FP64) {
-    g_err = "clb_create: lphi4SU2U1 runs in FP64 storage";
-    return CLB_EUNSUPPORTED;
-  }
+
   if (md->kind != CLB_MODEL_LPHI4 && !u1 && !su2) {
     g_err = "clb_create: unknown model kind";
     return CLB_EUNSUPPORTED;

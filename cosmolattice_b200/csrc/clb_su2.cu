@@ -23,11 +23,18 @@ constexpr int kSU2Blocks = 148 * 8; // 128-thread grid-stride sweeps
 }
 
 struct SU2Sector {
-  double *f = nullptr, *p = nullptr; // 22 and 19 x N^3
+  void *f = nullptr, *p = nullptr; // 22 and 19 x N^3 of double (FP64) or float (FP32 form)
+  bool fp32 = false;
+  size_t esz = 8;
   State *d_st = nullptr;
   double *d_part = nullptr, *d_sums = nullptr;
+  double *d_stage = nullptr; // one FP64 component, for FP32 conversions
+  int64_t steps_since_unitarize = 0;
   Params prm{};
 };
+
+// FP32 form: links re-unitarised every this many steps
+constexpr int64_t kUnitarizeEvery = 10;
 
 namespace {
 
@@ -89,12 +96,14 @@ Kick lf_kick(double dt, double w)
   return k;
 }
 
-void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
+template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
 {
   SU2Sector *u = h->su2;
   const int kind = nk == 0 ? K_U1_REDUCE : K_U1_KICK;
+  const S *f = static_cast<const S *>(u->f);
+  S *p = static_cast<S *>(u->p);
 #define CLB_SU2K(NK, RF, RP)                                                                                            \
-  CLB_LAUNCH(h, kind, k_kick<NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(u->f, u->p, u->prm, kc, u->d_st, u->d_part))
+  CLB_LAUNCH(h, kind, k_kick<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, p, u->prm, kc, u->d_st, u->d_part))
   if (nk == 0) {
     if (rf && rp)
       CLB_SU2K(0, true, true);
@@ -118,10 +127,36 @@ void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
 #undef CLB_SU2K
 }
 
+void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
+{
+  if (h->su2->fp32)
+    sweep_t<float>(h, nk, rf, rp, kc);
+  else
+    sweep_t<double>(h, nk, rf, rp, kc);
+}
+
 void drift(clb_handle *h, double w, bool lf)
 {
   SU2Sector *u = h->su2;
-  CLB_LAUNCH(h, K_U1_DRIFT, k_drift<<<kSU2Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, w, lf ? 1 : 0, u->d_st));
+  if (u->fp32)
+    CLB_LAUNCH(h, K_U1_DRIFT, k_drift<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f),
+                                                                                 static_cast<const float *>(u->p),
+                                                                                 u->prm, w, lf ? 1 : 0, u->d_st));
+  else
+    CLB_LAUNCH(h, K_U1_DRIFT, k_drift<double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<double *>(u->f),
+                                                                                  static_cast<const double *>(u->p),
+                                                                                  u->prm, w, lf ? 1 : 0, u->d_st));
+}
+
+// FP32 form: after the drift of every kUnitarizeEvery-th step the links are projected back to
+// unit quaternions.
+void step_done(clb_handle *h)
+{
+  SU2Sector *u = h->su2;
+  if (!u->fp32) return;
+  if (++u->steps_since_unitarize < kUnitarizeEvery) return;
+  u->steps_since_unitarize = 0;
+  CLB_LAUNCH(h, K_U1_DRIFT, k_unitarize<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f), h->n3));
 }
 
 void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
@@ -152,11 +187,14 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   h->su2 = u;
   h->NS = NF;
   u->prm = su2_params(h);
+  u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
+  u->esz = u->fp32 ? sizeof(float) : sizeof(double);
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->f, NF * h->n3 * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->p, NP * h->n3 * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMemset(u->f, 0, NF * h->n3 * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMemset(u->p, 0, NP * h->n3 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->p, NP * h->n3 * u->esz) == cudaSuccess;
+  ok = ok && cudaMemset(u->f, 0, NF * h->n3 * u->esz) == cudaSuccess;
+  ok = ok && cudaMemset(u->p, 0, NP * h->n3 * u->esz) == cudaSuccess;
+  if (u->fp32) ok = ok && cudaMalloc(&u->d_stage, h->n3 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_st, sizeof(State)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_part, (size_t)kSU2Blocks * kMeas * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_sums, kMeas * sizeof(double)) == cudaSuccess;
@@ -172,7 +210,7 @@ __attribute__((visibility("hidden"))) void su2_destroy(clb_handle *h)
 {
   SU2Sector *u = h->su2;
   if (!u) return;
-  for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums})
+  for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums, (void *)u->d_stage})
     if (q) cudaFree(q);
   delete u;
   h->su2 = nullptr;
@@ -183,10 +221,22 @@ __attribute__((visibility("hidden"))) int su2_set_state(clb_handle *h, const dou
 {
   SU2Sector *u = h->su2;
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (!u->fp32) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  } else {
+    // one component at a time through the FP64 staging buffer
+    for (int c = 0; c < NF + NP && e == cudaSuccess; ++c) {
+      const double *src = c < NF ? fields + (size_t)c * h->n3 : momenta + (size_t)(c - NF) * h->n3;
+      float *dst = static_cast<float *>(c < NF ? u->f : u->p) + (size_t)(c < NF ? c : c - NF) * h->n3;
+      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+      if (e == cudaSuccess) k_convert<double, float><<<kSU2Blocks, 256, 0, h->stream>>>(u->d_stage, dst, h->n3);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
+  u->steps_since_unitarize = 0;
   State s{};
   s.aI = s.aSI = s.aIM = 1.0;
   if (sf) {
@@ -211,8 +261,19 @@ __attribute__((visibility("hidden"))) int su2_get_state(clb_handle *h, double *f
   SU2Sector *u = h->su2;
   State s;
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess && fields) e = cudaMemcpyAsync(fields, u->f, NF * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess && momenta) e = cudaMemcpyAsync(momenta, u->p, NP * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (!u->fp32) {
+    if (e == cudaSuccess && fields) e = cudaMemcpyAsync(fields, u->f, NF * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && momenta) e = cudaMemcpyAsync(momenta, u->p, NP * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  } else {
+    for (int c = 0; c < NF + NP && e == cudaSuccess; ++c) {
+      double *dst = c < NF ? (fields ? fields + (size_t)c * h->n3 : nullptr) : (momenta ? momenta + (size_t)(c - NF) * h->n3 : nullptr);
+      if (!dst) continue;
+      const float *src = static_cast<const float *>(c < NF ? u->f : u->p) + (size_t)(c < NF ? c : c - NF) * h->n3;
+      k_convert<float, double><<<kSU2Blocks, 256, 0, h->stream>>>(src, u->d_stage, h->n3);
+      e = cudaMemcpyAsync(dst, u->d_stage, h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_get_state");
@@ -248,6 +309,7 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
     if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
     for (int64_t s = 0; s < nsteps; ++s) {
       drift(h, 1.0, true);
+      step_done(h);
       if (s + 1 < nsteps) {
         sweep(h, 1, ex, ex, lf_kick(dt, 1.0));
         if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true, 0, 0, s);
@@ -272,6 +334,7 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
       const bool more = k + 1 < total;
       const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
       drift(h, w, false);
+      if (i + 1 == S) step_done(h);
       sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
       if (ex) {
         uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
@@ -310,7 +373,12 @@ __attribute__((visibility("hidden"))) int su2_measure(clb_handle *h, double e0, 
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
   const double al = h->md.alpha;
   const double am = std::pow(s.aI, al - 3), ag = std::pow(s.aI, al - 1);
-  CLB_LAUNCH(h, K_MEASURE, su2d::k_measure<<<kSU2Blocks, 128, 0, h->stream>>>(u->f, u->p, u->prm, am, ag, u->d_part));
+  if (u->fp32)
+    CLB_LAUNCH(h, K_MEASURE, su2d::k_measure<float><<<kSU2Blocks, 128, 0, h->stream>>>(
+                                 static_cast<const float *>(u->f), static_cast<const float *>(u->p), u->prm, am, ag, u->d_part));
+  else
+    CLB_LAUNCH(h, K_MEASURE, su2d::k_measure<double><<<kSU2Blocks, 128, 0, h->stream>>>(
+                                 static_cast<const double *>(u->f), static_cast<const double *>(u->p), u->prm, am, ag, u->d_part));
   CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeas><<<1, 256, 0, h->stream>>>(u->d_part, kSU2Blocks, u->d_sums));
   double v[kMeas];
   e = cudaMemcpyAsync(v, u->d_sums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
@@ -382,9 +450,14 @@ __attribute__((visibility("hidden"))) int su2_measure(clb_handle *h, double e0, 
 // tells whether the component belongs to the U(1) or SU(2) field.
 __attribute__((visibility("hidden"))) const double *su2_component(clb_handle *h, int which, int comp, bool *gauge)
 {
+  SU2Sector *u = h->su2;
   if (comp < 0 || comp >= (which == 0 ? NF : NP)) return nullptr;
   *gauge = comp >= 7;
-  return (which == 0 ? h->su2->f : h->su2->p) + (size_t)comp * h->n3;
+  if (!u->fp32) return static_cast<const double *>(which == 0 ? u->f : u->p) + (size_t)comp * h->n3;
+  // FP32 form: the component in FP64 in the staging buffer (ordered on the handle's stream)
+  const float *src = static_cast<const float *>(which == 0 ? u->f : u->p) + (size_t)comp * h->n3;
+  k_convert<float, double><<<kSU2Blocks, 256, 0, h->stream>>>(src, u->d_stage, h->n3);
+  return u->d_stage;
 }
 
 } // namespace clb

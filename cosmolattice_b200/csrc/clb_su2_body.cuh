@@ -1,0 +1,509 @@
+// clb_su2_body.cuh - lphi4SU2U1 site arithmetic, kick, drift and measurement kernels, templated on
+// the storage type S (double or float) and the arithmetic type T of the site kernels.  The FP64
+// form uses S = T = double and rounds in the reference's order (the unit is compiled without FMA
+// contraction); the FP32 form stores and stencils in float (S = T = float) with every kick and
+// drift increment added in FP64 and rounded once, and measures in FP64 (T = double over float
+// storage).  Included by clb_su2.cuh.
+#pragma once
+
+#include "clb_su2.cuh"
+
+namespace clb {
+namespace su2d {
+
+template <class T> struct C2 {
+  T re, im;
+};
+template <class T> __device__ __forceinline__ C2<T> cmul(C2<T> a, C2<T> b)
+{
+  return C2<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <class T> __device__ __forceinline__ C2<T> cadd(C2<T> a, C2<T> b) { return C2<T>{a.re + b.re, a.im + b.im}; }
+template <class T> __device__ __forceinline__ C2<T> csub(C2<T> a, C2<T> b) { return C2<T>{a.re - b.re, a.im - b.im}; }
+template <class T> __device__ __forceinline__ C2<T> conj_(C2<T> a) { return C2<T>{a.re, -a.im}; }
+template <class T> struct Q4 {
+  T w, x, y, z;
+};
+template <class T> __device__ __forceinline__ Q4<T> qmul(const Q4<T> &a, const Q4<T> &b)
+{
+  return Q4<T>{a.w * b.w - (a.x * b.x + a.y * b.y + a.z * b.z), a.w * b.x + b.w * a.x - (a.y * b.z - a.z * b.y),
+               a.w * b.y + b.w * a.y - (a.z * b.x - a.x * b.z), a.w * b.z + b.w * a.z - (a.x * b.y - a.y * b.x)};
+}
+template <class T> __device__ __forceinline__ Q4<T> qdag(const Q4<T> &a) { return Q4<T>{a.w, -a.x, -a.y, -a.z}; }
+template <class T> struct D2 {
+  C2<T> u, v;
+};
+// U (u, v) with U = [[q0 + i q3, q2 + i q1], [-q2 + i q1, q0 - i q3]]
+template <class T> __device__ __forceinline__ D2<T> qapply(const Q4<T> &q, const D2<T> &d)
+{
+  return D2<T>{cadd(cmul(C2<T>{q.w, q.z}, d.u), cmul(C2<T>{q.y, q.x}, d.v)),
+               cadd(cmul(C2<T>{-q.y, q.x}, d.u), cmul(C2<T>{q.w, -q.z}, d.v))};
+}
+template <class T> __device__ __forceinline__ D2<T> dscale(C2<T> c, const D2<T> &d) { return D2<T>{cmul(c, d.u), cmul(c, d.v)}; }
+template <class T> __device__ __forceinline__ C2<T> sprod(const D2<T> &a, const D2<T> &b)
+{
+  return cadd(cmul(conj_(a.u), b.u), cmul(conj_(a.v), b.v));
+}
+// i sigma_b applied to a doublet
+template <class T> __device__ __forceinline__ D2<T> isig(int b, const D2<T> &d)
+{
+  const C2<T> I{0, 1};
+  if (b == 0) return D2<T>{cmul(I, d.v), cmul(I, d.u)};
+  if (b == 1) return D2<T>{d.v, C2<T>{-d.u.re, -d.u.im}};
+  return D2<T>{cmul(I, d.u), cmul(C2<T>{0, -1}, d.v)};
+}
+template <class T> __device__ __forceinline__ T ipw(T x, int n)
+{
+  if (n < 0) return T(1) / ipw(x, -n);
+  T r = x;
+  for (int i = 1; i < n; ++i) r = r * x;
+  return n == 0 ? T(1) : r;
+}
+
+// Read-only view of one state at one site (storage S, arithmetic T), with the oracle's names.
+template <class S, class T> struct Site {
+  const S *f;
+  const Params *a;
+  size_t s;
+  long long op[3], om[3];
+  T dx, gC, gD, gS;
+  __device__ __forceinline__ T F(int c, size_t t) const { return (T)f[(size_t)c * a->n3 + t]; }
+  __device__ __forceinline__ Q4<T> link(int i, size_t t) const
+  {
+    const int b = 10 + 4 * i;
+    return Q4<T>{F(b, t), F(b + 1, t), F(b + 2, t), F(b + 3, t)};
+  }
+  __device__ __forceinline__ D2<T> dbl(size_t t) const { return D2<T>{C2<T>{F(3, t), F(4, t)}, C2<T>{F(5, t), F(6, t)}}; }
+  __device__ __forceinline__ C2<T> cs(size_t t) const { return C2<T>{F(1, t), F(2, t)}; }
+  __device__ __forceinline__ C2<T> phase(T g, int i, size_t t) const
+  {
+    const T th = (-dx * g) * F(7 + i, t);
+    return C2<T>{cos(th), sin(th)};
+  }
+  __device__ __forceinline__ T normD(size_t t) const
+  {
+    T q = 0;
+    for (int c = 0; c < 4; ++c) q = c == 0 ? F(3, t) * F(3, t) : q + F(3 + c, t) * F(3 + c, t);
+    return sqrt(q);
+  }
+  __device__ __forceinline__ T normC(size_t t) const { return sqrt(F(1, t) * F(1, t) + F(2, t) * F(2, t)); }
+  __device__ __forceinline__ T potTerm(int k) const
+  {
+    const T nD = normD(s);
+    if (k == 0) return (T)a->c4 * ipw(nD, 4);
+    if (k == 1) return (T)a->qG * ipw(nD * F(0, s), 2);
+    return 2 * (T)a->qH * ipw(nD * normC(s), 2);
+  }
+  __device__ __forceinline__ T pot() const { return (potTerm(0) + potTerm(1)) + potTerm(2); }
+  __device__ __forceinline__ size_t pl(int i) const { return s + op[i]; }
+  __device__ __forceinline__ size_t mi(int i) const { return s + om[i]; }
+  __device__ __forceinline__ size_t plmi(int i, int j) const { return i == j ? s : s + op[i] + om[j]; }
+  __device__ __forceinline__ D2<T> wD(int i) const { return dscale(phase(gD, i, s), qapply(link(i, s), dbl(pl(i)))); }
+  __device__ __forceinline__ C2<T> wC(int i) const { return cmul(phase(gC, i, s), cs(pl(i))); }
+  __device__ __forceinline__ T lapl(int comp) const
+  {
+    const T c = F(comp, s);
+    T t[3];
+    for (int d = 0; d < 3; ++d) t[d] = (F(comp, pl(d)) + F(comp, mi(d))) - 2 * c;
+    return (T(1) / (dx * dx)) * ((t[0] + t[1]) + t[2]);
+  }
+  __device__ __forceinline__ T fd(int comp, size_t t0, size_t t1) const { return (F(comp, t1) - F(comp, t0)) / dx; }
+  __device__ __forceinline__ Q4<T> plaq(int i, int j) const
+  {
+    return qmul(qmul(qmul(link(i, s), link(j, pl(i))), qdag(link(i, pl(j)))), qdag(link(j, s)));
+  }
+  __device__ __forceinline__ Q4<T> plaqBack(int i, int j) const
+  {
+    const size_t sm = mi(j);
+    return qdag(qmul(qmul(qmul(link(i, s), qdag(link(j, plmi(i, j)))), qdag(link(i, sm))), link(j, sm)));
+  }
+};
+
+template <class S, class T> __device__ __forceinline__ Site<S, T> make_site(const S *f, const Params &a, size_t s)
+{
+  Site<S, T> v;
+  v.f = f;
+  v.a = &a;
+  v.s = s;
+  v.dx = (T)a.dx;
+  v.gC = (T)a.gC;
+  v.gD = (T)a.gD;
+  v.gS = (T)a.gS;
+  u1_offsets(a.N, s, v.op, v.om);
+  return v;
+}
+
+// ---- momentum kernels at one site (momentum-component order) ----------------------------------
+template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<S, T> &v)
+{
+  C2<T> plus{0, 0}, minus{0, 0};
+  for (int d = 0; d < 3; ++d) {
+    const C2<T> w = cmul(v.phase(v.gC, d, v.s), v.cs(v.pl(d)));
+    const C2<T> m = cmul(conj_(v.phase(v.gC, d, v.mi(d))), v.cs(v.mi(d)));
+    plus = d == 0 ? w : cadd(plus, w);
+    minus = d == 0 ? m : cadd(minus, m);
+  }
+  const T dx2 = v.dx * v.dx;
+  const C2<T> c = v.cs(v.s);
+  return C2<T>{((plus.re + minus.re) - 6 * c.re) / dx2, ((plus.im + minus.im) - 6 * c.im) / dx2};
+}
+
+template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S, T> &v, T out[4])
+{
+  D2<T> plus{}, minus{};
+  for (int d = 0; d < 3; ++d) {
+    const D2<T> w = qapply(v.link(d, v.s), dscale(v.phase(v.gD, d, v.s), v.dbl(v.pl(d))));
+    const size_t sm = v.mi(d);
+    const D2<T> m = qapply(qdag(v.link(d, sm)), dscale(conj_(v.phase(v.gD, d, sm)), v.dbl(sm)));
+    if (d == 0) {
+      plus = w;
+      minus = m;
+    } else {
+      plus = D2<T>{cadd(plus.u, w.u), cadd(plus.v, w.v)};
+      minus = D2<T>{cadd(minus.u, m.u), cadd(minus.v, m.v)};
+    }
+  }
+  const T dx2 = v.dx * v.dx;
+  const D2<T> c = v.dbl(v.s);
+  out[0] = ((plus.u.re + minus.u.re) - 6 * c.u.re) / dx2;
+  out[1] = ((plus.u.im + minus.u.im) - 6 * c.u.im) / dx2;
+  out[2] = ((plus.v.re + minus.v.re) - 6 * c.v.re) / dx2;
+  out[3] = ((plus.v.im + minus.v.im) - 6 * c.v.im) / dx2;
+}
+
+template <class S, class T> __device__ __forceinline__ void kernels(const Site<S, T> &v, const State &st, T K[NP])
+{
+  const Params &a = *v.a;
+  const size_t s = v.s;
+  const T A = (T)st.kA, B = (T)st.kB, B2 = (T)st.kB2, G = (T)st.kG;
+  const T qG = (T)a.qG, qH = (T)a.qH, c4 = (T)a.c4, rfo2 = (T)a.rfo2;
+  const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
+  K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
+  const C2<T> cl = covLapC(v);
+  const T ndC = 4 * qH * ipw(nD, 2) * nC;
+  K[1] = A * cl.re - B2 * (ndC / nC * v.F(1, s));
+  K[2] = A * cl.im - B2 * (ndC / nC * v.F(2, s));
+  T dl[4];
+  covLapD(v, dl);
+  const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
+  for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (ndD / nD * v.F(3 + c, s));
+  const D2<T> D0 = v.dbl(s);
+  const C2<T> C0 = v.cs(s);
+  for (int i = 0; i < 3; ++i) {
+    const T lap = v.lapl(7 + i);
+    T grad = 0;
+    for (int j = 0; j < 3; ++j) {
+      const T g0 = v.fd(7 + j, s, v.pl(i));
+      const T g1 = v.fd(7 + j, v.mi(j), v.plmi(i, j));
+      const T t = (g0 - g1) / v.dx;
+      grad = j == 0 ? t : grad + t;
+    }
+    const T Jc = v.gC * cmul(conj_(v.wC(i)), C0).im;
+    const T Jd = v.gD * sprod(v.wD(i), D0).im;
+    const T J = T(2.0) / v.dx * rfo2 * (Jc + Jd);
+    K[7 + i] = G * (lap - grad) - A * J;
+  }
+  const T normGrad = ipw(T(1) / v.dx, 3) / v.gS * G;
+  const T normSrc = (T(1) / v.dx) * A;
+  for (int i = 0; i < 3; ++i) {
+    T gr[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
+    bool first = true;
+    for (int j = 0; j < 3; ++j) {
+      if (j == i) continue;
+      const Q4<T> P = v.plaq(i, j), Pb = v.plaqBack(i, j);
+      const T pv[3] = {P.x, P.y, P.z}, bv[3] = {Pb.x, Pb.y, Pb.z};
+      for (int c = 0; c < 3; ++c) {
+        gr[c] = first ? pv[c] : gr[c] + pv[c];
+        gb[c] = first ? bv[c] : gb[c] + bv[c];
+      }
+      first = false;
+    }
+    const D2<T> W = v.wD(i);
+    for (int c = 0; c < 3; ++c) {
+      const T J = rfo2 / 2 * (v.gS * sprod(W, isig(c, D0)).re);
+      K[10 + 3 * i + c] = -normGrad * (gr[c] - gb[c]) - normSrc * J;
+    }
+  }
+}
+
+// ---- per-site averages (fieldfunctionals.h) -------------------------------------------------------
+template <class S, class T> __device__ __forceinline__ T sGrad2(const Site<S, T> &v)
+{
+  T acc = 0;
+  for (int j = 0; j < 3; ++j) {
+    const T g = v.fd(0, v.s, v.pl(j));
+    acc = j == 0 ? g * g : acc + g * g;
+  }
+  return acc;
+}
+template <class S, class T> __device__ __forceinline__ T cGrad2(const Site<S, T> &v)
+{
+  const C2<T> c = v.cs(v.s);
+  T acc = 0;
+  for (int j = 0; j < 3; ++j) {
+    const C2<T> d0 = csub(v.wC(j), c);
+    const C2<T> d{d0.re / v.dx, d0.im / v.dx};
+    const T n2 = d.re * d.re + d.im * d.im;
+    acc = j == 0 ? n2 : acc + n2;
+  }
+  return acc;
+}
+template <class S, class T> __device__ __forceinline__ T dGrad2(const Site<S, T> &v)
+{
+  const D2<T> c = v.dbl(v.s);
+  T acc = 0;
+  for (int j = 0; j < 3; ++j) {
+    const D2<T> w = qapply(v.link(j, v.s), dscale(v.phase(v.gD, j, v.s), v.dbl(v.pl(j))));
+    const C2<T> du0 = csub(w.u, c.u), dv0 = csub(w.v, c.v);
+    const C2<T> du{du0.re / v.dx, du0.im / v.dx}, dv{dv0.re / v.dx, dv0.im / v.dx};
+    const T n2 = (du.re * du.re + du.im * du.im) + (dv.re * dv.re + dv.im * dv.im);
+    acc = j == 0 ? n2 : acc + n2;
+  }
+  return acc;
+}
+template <class S, class T> __device__ __forceinline__ T Fij(const Site<S, T> &v, int i, int j)
+{
+  return v.fd(7 + j, v.s, v.pl(i)) - v.fd(7 + i, v.s, v.pl(j));
+}
+template <class S, class T> __device__ __forceinline__ T aB2(const Site<S, T> &v)
+{
+  const T f21 = Fij(v, 1, 0), f31 = Fij(v, 2, 0), f32 = Fij(v, 2, 1);
+  return f21 * f21 + (f31 * f31 + f32 * f32);
+}
+template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v)
+{
+  const T c = T(4.0) / (ipw(v.dx, 4) * ipw(v.gS, 2));
+  const T t10 = 2 - 2 * v.plaq(1, 0).w, t20 = 2 - 2 * v.plaq(2, 0).w, t21 = 2 - 2 * v.plaq(2, 1).w;
+  return c * (t10 + (t20 + t21));
+}
+// momentum sums of the five sectors (FP64) from momentum values q[19]
+template <class R> __device__ __forceinline__ void pi2s(const R *qs, double out[5])
+{
+  double q[NP];
+  for (int c = 0; c < NP; ++c) q[c] = (double)qs[c];
+  out[0] = q[0] * q[0];
+  out[1] = q[1] * q[1] + q[2] * q[2];
+  out[2] = ((q[3] * q[3] + q[4] * q[4]) + q[5] * q[5]) + q[6] * q[6];
+  out[3] = (q[7] * q[7] + q[8] * q[8]) + q[9] * q[9];
+  double acc = 0;
+  for (int i = 0; i < 3; ++i) {
+    double ai = 0;
+    for (int b = 0; b < 3; ++b) {
+      const double e = q[10 + 3 * i + b];
+      ai = b == 0 ? 4 * (e * e) : ai + 4 * (e * e);
+    }
+    acc = i == 0 ? ai : acc + ai;
+  }
+  out[4] = acc;
+}
+
+__device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c < 7 ? 2 : c < 10 ? 3 : 4; }
+
+// Kick sweep: NK (0..2) in-place kicks with the kernel at the current fields, each increment added
+// in FP64 and rounded to the storage type once.  Partials: [0..4] momentum sums after the first kick
+// (or as they are, NK = 0), [5..10] <grad^2> S, phi, Phi, <B^2> U(1), SU(2), <V>; [11..15] the
+// momentum sums after the second kick.
+template <class S, int NK, bool RF, bool RP>
+__global__ void __launch_bounds__(128)
+    k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
+           double *__restrict__ partials)
+{
+  __shared__ double smem[(128 / 32) * kRed];
+  const State st = *stp;
+  double acc[kRed];
+  for (int k = 0; k < kRed; ++k) acc[k] = 0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
+    const Site<S, S> v = make_site<S, S>(f, a, s);
+    S q[NP];
+    for (int c = 0; c < NP; ++c) q[c] = p[(size_t)c * a.n3 + s];
+    if (NK > 0) {
+      S K[NP];
+      kernels(v, st, K);
+      for (int k = 0; k < NK; ++k) {
+        for (int c = 0; c < NP; ++c) q[c] = (S)((double)q[c] + kc.h[k][sector(c)] * (double)K[c]);
+        if (RP) {
+          double t[5];
+          pi2s(q, t);
+          for (int g = 0; g < 5; ++g) acc[(k == 0 ? 0 : 11) + g] += t[g];
+        }
+      }
+      for (int c = 0; c < NP; ++c) p[(size_t)c * a.n3 + s] = q[c];
+    } else if (RP) {
+      double t[5];
+      pi2s(q, t);
+      for (int g = 0; g < 5; ++g) acc[g] += t[g];
+    }
+    if (RF) {
+      acc[5] += (double)sGrad2(v);
+      acc[6] += (double)cGrad2(v);
+      acc[7] += (double)dGrad2(v);
+      acc[8] += (double)aB2(v);
+      acc[9] += (double)gB2(v);
+      acc[10] += (double)v.pot();
+    }
+  }
+  if (RF || RP) {
+    block_reduce<kRed, 128>(acc, smem);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < kRed; ++k) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
+  }
+}
+
+// Drifts (velocityverlet.h:181-222; the leapfrog's forms leapfrog.h:203-236 have lf = 1), in FP64
+// and rounded to the storage type once.
+__device__ __forceinline__ Q4<double> qexp(double p1, double p2, double p3)
+{
+  const double n = sqrt(p1 * p1 + p2 * p2 + p3 * p3);
+  if (n == 0) return Q4<double>{1, 0, 0, 0};
+  const double sn = sin(n) / n;
+  return Q4<double>{cos(n), sn * p1, sn * p2, sn * p3};
+}
+template <class S>
+__global__ void __launch_bounds__(256)
+    k_drift(S *__restrict__ f, const S *__restrict__ p, Params a, double w, int lf, const State *__restrict__ stp)
+{
+  const double dt = a.dt, p3 = stp->p3, p1 = stp->p1;
+  const double cC = lf ? p3 * dt : p3 * dt * w;
+  const double cA = lf ? p1 * dt : p1 * w * dt;
+  const double cG = lf ? p1 * a.dx * dt * a.gS : w * p1 * a.dx * dt * a.gS;
+  const double dtw = lf ? dt : dt * w;
+  const size_t n3 = a.n3;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    f[s] = (S)((double)f[s] + p3 * (dtw * (double)p[s]));
+    for (int c = 1; c < 7; ++c) f[c * n3 + s] = (S)((double)f[c * n3 + s] + cC * (double)p[c * n3 + s]);
+    for (int i = 0; i < 3; ++i)
+      f[(7 + i) * n3 + s] = (S)((double)f[(7 + i) * n3 + s] + cA * (double)p[(7 + i) * n3 + s] * 1.0);
+    for (int i = 0; i < 3; ++i) {
+      const size_t pb = (size_t)(10 + 3 * i) * n3 + s, fb = (size_t)(10 + 4 * i) * n3 + s;
+      const Q4<double> E = qexp(cG * (double)p[pb], cG * (double)p[pb + n3], cG * (double)p[pb + 2 * n3]);
+      const Q4<double> U = qmul(E, Q4<double>{(double)f[fb], (double)f[fb + n3], (double)f[fb + 2 * n3], (double)f[fb + 3 * n3]});
+      f[fb] = (S)U.w;
+      f[fb + n3] = (S)U.x;
+      f[fb + 2 * n3] = (S)U.y;
+      f[fb + 3 * n3] = (S)U.z;
+    }
+  }
+}
+
+// Re-unitarisation of the stored links (FP32 form): U <- U / |U| in FP64.
+template <class S> __global__ void __launch_bounds__(256) k_unitarize(S *__restrict__ f, size_t n3)
+{
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < 3 * n3; s += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = s / n3, t = s - i * n3, fb = (size_t)(10 + 4 * i) * n3 + t;
+    const double w = f[fb], x = f[fb + n3], y = f[fb + 2 * n3], z = f[fb + 3 * n3];
+    const double r = 1.0 / sqrt(((w * w + x * x) + y * y) + z * z);
+    f[fb] = (S)(w * r);
+    f[fb + n3] = (S)(x * r);
+    f[fb + 2 * n3] = (S)(y * r);
+    f[fb + 3 * n3] = (S)(z * r);
+  }
+}
+
+// ---- measurement sums (one sweep) ----------------------------------------------------------------
+// [0..4] momentum sums of the five sectors, [5..10] field sums as in the kick sweep, [11..13] the
+// three potential terms, means [14..41] (seven rows of f, f^2, m, m^2 with raw values), Gauss
+// U(1) [42..45] (|LHS-RHS|, |sum|, |RHS|, |LHS|), Gauss SU(2) [46..57] (same per algebra index).
+template <class S>
+__global__ void __launch_bounds__(128)
+    k_measure(const S *__restrict__ f, const S *__restrict__ p, Params a, double am, double ag,
+              double *__restrict__ partials)
+{
+  __shared__ double smem[(128 / 32) * kMeas];
+  double acc[kMeas];
+  for (int k = 0; k < kMeas; ++k) acc[k] = 0;
+  const size_t n3 = a.n3;
+  const double dx = a.dx;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    const Site<S, double> v = make_site<S, double>(f, a, s);
+    double q[NP];
+    for (int c = 0; c < NP; ++c) q[c] = (double)p[(size_t)c * n3 + s];
+    double t[5];
+    pi2s(q, t);
+    for (int g = 0; g < 5; ++g) acc[g] += t[g];
+    acc[5] += sGrad2(v);
+    acc[6] += cGrad2(v);
+    acc[7] += dGrad2(v);
+    acc[8] += aB2(v);
+    acc[9] += gB2(v);
+    acc[10] += v.pot();
+    for (int k = 0; k < 3; ++k) acc[11 + k] += v.potTerm(k);
+    auto row = [&](int r, double fv, double mv) {
+      acc[14 + 4 * r] += fv;
+      acc[15 + 4 * r] += fv * fv;
+      acc[16 + 4 * r] += mv;
+      acc[17 + 4 * r] += mv * mv;
+    };
+    const double r2 = sqrt(2.0);
+    row(0, v.F(0, s), q[0] * am);
+    row(1, r2 * v.F(1, s), r2 * q[1] * am);
+    row(2, r2 * v.F(2, s), r2 * q[2] * am);
+    {
+      const double pa = q[1] * am, pb = q[2] * am;
+      row(3, v.normC(s), sqrt(pa * pa + pb * pb));
+    }
+    {
+      double pd = 0;
+      for (int c = 0; c < 4; ++c) pd += q[3 + c] * q[3 + c];
+      row(4, v.normD(s), sqrt(pd) * am);
+    }
+    {
+      const double e1 = q[7] * ag, e2 = q[8] * ag, e3 = q[9] * ag;
+      const double b1 = Fij(v, 2, 1), b2 = Fij(v, 0, 2), b3 = Fij(v, 1, 0);
+      row(5, sqrt(e1 * e1 + e2 * e2 + e3 * e3), sqrt(b1 * b1 + b2 * b2 + b3 * b3));
+    }
+    {
+      double e = 0;
+      for (int c = 0; c < 9; ++c) e += 4 * q[10 + c] * q[10 + c];
+      row(6, ag * sqrt(e), sqrt(gB2(v)));
+    }
+    // Gauss U(1)
+    {
+      double l[3];
+      for (int i = 0; i < 3; ++i) l[i] = q[7 + i] - (double)p[(size_t)(7 + i) * n3 + v.mi(i)];
+      const double LHS = ((l[0] + l[1]) + l[2]) / dx;
+      const double nrm = 2 / dx * a.rfo2;
+      const double imc = cmul(conj_(C2<double>{q[1], q[2]}), v.cs(s)).im;
+      const double imd = sprod(D2<double>{C2<double>{q[3], q[4]}, C2<double>{q[5], q[6]}}, v.dbl(s)).im;
+      const double rho = nrm * a.gC * imc + nrm * a.gD * imd;
+      const double RHS = -dx * rho;
+      const double L1 = l[0] / dx, L2 = l[1] / dx, L3 = l[2] / dx;
+      const double diff = LHS - (RHS + 0.0), sum = L1 * L1 + L2 * L2 + L3 * L3 + (RHS + 0.0) * (RHS + 0.0);
+      acc[42] += sqrt(diff * diff);
+      acc[43] += sqrt(sum * sum);
+      acc[44] += sqrt(RHS * RHS);
+      acc[45] += sqrt(LHS * LHS);
+    }
+    // Gauss SU(2)
+    {
+      double L[3];
+      for (int i = 0; i < 3; ++i) {
+        const size_t sm = v.mi(i);
+        const Q4<double> Ui = v.link(i, sm);
+        const size_t pb = (size_t)(10 + 3 * i) * n3 + sm;
+        const Q4<double> r =
+            qmul(qmul(qdag(Ui), Q4<double>{0, (double)p[pb], (double)p[pb + n3], (double)p[pb + 2 * n3]}), Ui);
+        const double rv[3] = {r.x, r.y, r.z};
+        for (int b = 0; b < 3; ++b) {
+          const double tt = (1 / dx) * (q[10 + 3 * i + b] - rv[b]);
+          L[b] = i == 0 ? tt : L[b] + tt;
+        }
+      }
+      const D2<double> D0 = v.dbl(s);
+      const D2<double> pd{C2<double>{q[3], q[4]}, C2<double>{q[5], q[6]}};
+      for (int b = 0; b < 3; ++b) {
+        const double R = (-1.0) * (a.rfo2 / 2 * (a.gS * sprod(isig(b, D0), pd).re));
+        const double df = L[b] - R, sm = L[b] + R;
+        acc[46 + 4 * b] += sqrt(df * df);
+        acc[47 + 4 * b] += sqrt(sm * sm);
+        acc[48 + 4 * b] += sqrt(R * R);
+        acc[49 + 4 * b] += sqrt(L[b] * L[b]);
+      }
+    }
+  }
+  block_reduce<kMeas, 128>(acc, smem);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kMeas; ++k) partials[(size_t)blockIdx.x * kMeas + k] = acc[k];
+}
+
+} // namespace su2d
+} // namespace clb
