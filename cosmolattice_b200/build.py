@@ -31,17 +31,20 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, out: str = None, defines=()) -> str:
+    """Compile every unit for sm_100a and link ``out`` (default: the package library)."""
+    lib = out or LIB
+    if not force and out is None and not _stale():
         return LIB
-    os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
     objs = []
     from concurrent.futures import ThreadPoolExecutor
 
     def one(src):
-        obj = os.path.join(LIB_DIR, src.replace(".cu", ".o"))
-        cmd = [nvcc, *NVCC_FLAGS, *UNIT_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
+        obj = os.path.join(os.path.dirname(lib), src.replace(".cu", ".o"))
+        cmd = [nvcc, *NVCC_FLAGS, *UNIT_FLAGS.get(src, []), *[f"-D{d}" for d in defines], "-c",
+               os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
@@ -49,13 +52,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(one, SOURCES))
-    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB, "-lcufft"]
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", lib, "-lcufft"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
