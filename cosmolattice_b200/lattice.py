@@ -218,6 +218,7 @@ class Measurer:
         self.rp = rp
         self.outdir = outdir if outdir is not None else rp.outFn
         self.outputFreq = max(1, int(round(rp.tOutFreq / rp.dt)))
+        self.spectraFreq = max(1, int(round(rp.tOutInfreq / rp.dt)))  # measurer.h:48-53
         self.e0 = None
         self.files: Dict[str, object] = {}
         self.history: List[Dict[str, object]] = []
@@ -274,6 +275,60 @@ class Measurer:
     def are_we_measuring(self, n: int) -> bool:
         return n % self.outputFreq == 0
 
+    def are_we_measuring_spectra(self, n: int) -> bool:
+        return n % self.spectraFreq == 0
+
+    def _spectra_sets(self):
+        """(file name, [(which, comp, gauge-electric)...] summed into column 1, same for column 2) per
+        measured field (scalarsingletmeasurer.h:74-83, complexscalarmeasurer.h:75-90,
+        su2doubletmeasurer.h, u1measurer.h:91-104)."""
+        m = self.model
+        if getattr(m, "NSU2", 0):
+            return [("scalar_0", [(0, 0)], [(1, 0)]),
+                    ("norm_cmplx_scalar_0", [(0, 1), (0, 2)], [(1, 1), (1, 2)]),
+                    ("norm_SU2Doublet_0", [(0, c) for c in range(3, 7)], [(1, c) for c in range(3, 7)]),
+                    ("norm_U1_0", [(1, 7), (1, 8), (1, 9)], None)]
+        if getattr(m, "NU1", 0):
+            return [("norm_cmplx_scalar_0", [(0, 0), (0, 1)], [(1, 0), (1, 1)]),
+                    ("norm_U1_0", [(1, 2), (1, 3), (1, 4)], None)]
+        return [(f"scalar_{i}", [(0, i)], [(1, i)]) for i in range(m.Ns)]
+
+    def measure_spectra(self, t: float, lattice: Lattice) -> None:
+        """SpectrumSaverStd::save (spectrumsaverstd.h:54-96), verbosity 0: one line per bin with the
+        bin centre times kIR and the spectra of the measured quantity, a blank line per time."""
+        if not self.outdir:
+            return
+        rp = self.rp
+        for name, cols1, cols2 in self._spectra_sets():
+            cols = []
+            k = None
+            for group in (cols1, cols2):
+                if group is None:
+                    continue
+                acc = None
+                for which, comp in group:
+                    kk, v, _ = lattice.spectrum(which=which, comp=comp, ps_type=rp.powerSpectrumType,
+                                                ps_version=rp.powerSpectrumVersion, dk=rp.deltaKBin,
+                                                nbins=rp.nBinsSpectra)
+                    acc = v if acc is None else acc + v
+                    k = kk
+                cols.append(acc)
+            key = "spectra_" + name
+            if key not in self.files:
+                path = os.path.join(self.outdir, key + ".txt")
+                if os.path.exists(path) and not rp.appendMode and not rp.overwriteMode:
+                    raise FileExistsError(f'Refusing to overwrite existing output file "{path}".')
+                fh = open(path, "a" if rp.appendMode else "w")
+                if rp.printHeaders and not rp.appendMode:
+                    fh.write("1:binCentralValue " + " ".join(f"{i + 2}:PS" for i in range(len(cols))) + "\n")
+                self.files[key] = fh
+            fh = self.files[key]
+            centres = (np.arange(rp.nBinsSpectra) + 0.5) * rp.deltaKBin * rp.kIR
+            for b in range(rp.nBinsSpectra):
+                fh.write(" ".join(f"{x:.15g}" for x in [centres[b]] + [c[b] for c in cols]) + "\n")
+            fh.write("\n")
+            fh.flush()
+
     def measure(self, n: int, t: float, lattice: Lattice) -> Dict[str, object]:
         first = self.e0 is None
         m = lattice.measure(self.e0 if self.e0 is not None else 1.0)
@@ -314,11 +369,16 @@ def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fu
     t = rp.t0
     i = 0
     while t < rp.tMax - rp.dt / 2.0:
-        if measurer.are_we_measuring(i):
+        freq = measurer.are_we_measuring(i)
+        infreq = measurer.are_we_measuring_spectra(i)
+        if freq or infreq:
             evolver.sync(model, t - rp.t0)
+        if freq:
             measurer.measure(i, t, lattice)
+        if infreq:
+            measurer.measure_spectra(t, lattice)
         # advance to the next measurement in one device call
-        n = measurer.outputFreq - (i % measurer.outputFreq)
+        n = min(measurer.outputFreq - (i % measurer.outputFreq), measurer.spectraFreq - (i % measurer.spectraFreq))
         n_left = int(round((rp.tMax - t) / rp.dt))
         n = max(1, min(n, n_left))
         evolver.evolve_n(n)
