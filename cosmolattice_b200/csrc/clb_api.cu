@@ -267,7 +267,7 @@ bool encode_map(clb_handle *h, void *base, CUtensorMap *map, std::string &why)
 void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1)
 {
   TailOp op{flags, nblocks, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
-  CLB_LAUNCH(h, K_TAIL, k_tail<<<1, 256, 0, h->stream>>>(h->d_part, op, h->d_st, h->sp));
+  CLB_LAUNCH(h, K_TAIL, k_tail<<<1, kTailThreads, 0, h->stream>>>(h->d_part, op, h->d_st, h->sp));
 }
 
 // Dispatch on (storage, field count).

@@ -404,17 +404,32 @@ __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const 
     s.status = 1;
 }
 
-static __global__ void __launch_bounds__(256)
+// The tail reduces one partial row per sweep block (8192 rows at 512^3): 1024 threads, each with
+// four independent accumulators, so the loads overlap instead of waiting out the latency one by one.
+constexpr int kTailThreads = 1024;
+
+static __global__ void __launch_bounds__(kTailThreads)
     k_tail(const double *__restrict__ partials, TailOp op, DevState *__restrict__ st, SFParams p)
 {
-  __shared__ double smem[(256 / 32) * kRedSlots];
+  __shared__ double smem[(kTailThreads / 32) * kRedSlots];
   double v[kRedSlots] = {0, 0, 0};
   if (op.nblocks > 0) {
-    for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x) {
+    double w[4][kRedSlots] = {};
+    const int T = blockDim.x;
+    int b = threadIdx.x;
+    for (; b + 3 * T < op.nblocks; b += 4 * T) {
 #pragma unroll
-      for (int k = 0; k < kRedSlots; ++k) v[k] += partials[(size_t)b * kRedSlots + k];
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int k = 0; k < kRedSlots; ++k) w[u][k] += partials[(size_t)(b + u * T) * kRedSlots + k];
     }
-    block_reduce<kRedSlots, 256>(v, smem);
+    for (; b < op.nblocks; b += T) {
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) w[0][k] += partials[(size_t)b * kRedSlots + k];
+    }
+#pragma unroll
+    for (int k = 0; k < kRedSlots; ++k) v[k] = (w[0][k] + w[1][k]) + (w[2][k] + w[3][k]);
+    block_reduce<kRedSlots, kTailThreads>(v, smem);
   }
   if (threadIdx.x != 0) return;
   DevState s = *st;
