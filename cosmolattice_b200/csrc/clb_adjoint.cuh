@@ -136,9 +136,10 @@ constexpr int kAdjSlots = 9;
 // PRE = 0: sweep at the stage input (q0, p0): transposed kick of pbar_in = pbar1, then the
 // average gradients; writes qbar and pbar_out = pbar0.  With hc = hu = 0 it applies only the
 // average gradients (observable seed, initial aDot correction).
-template <int PRE>
+// S is the storage type of the forward state (f, p); the cotangents are FP64 in either form.
+template <int PRE, class S>
 __global__ void __launch_bounds__(256)
-    k_u1_adj(const double *__restrict__ f, const double *__restrict__ p, const double *__restrict__ pbar_in,
+    k_u1_adj(const S *__restrict__ f, const S *__restrict__ p, const double *__restrict__ pbar_in,
              double *__restrict__ qbar, double *__restrict__ pbar_out, U1Params a, U1AdjArgs g,
              double *__restrict__ partials)
 {
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(256)
   // cotangent of the kick output at a site (PRE adds the momentum-average gradients)
   auto lam = [&](int c, size_t y) -> double {
     double l = pbar_in[c * n3 + y];
-    if (PRE) l += (c < 2 ? g.Api : g.AE) * two_n3 * p[c * n3 + y];
+    if (PRE) l += (c < 2 ? g.Api : g.AE) * two_n3 * (double)p[c * n3 + y];
     return l;
   };
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(256)
     U1Pieces o;
     auto ld = [&](int c, size_t y) -> Dual2 {
       const double mu = c < 2 ? lam(c, y) : g.r2 * lam(c, y);
-      return Dual2{f[c * n3 + y], mu, 0.0};
+      return Dual2{(double)f[c * n3 + y], mu, 0.0};
     };
     u1_pieces(ld, a, s, op, om, o);
     // kernel values and derivatives (complexscalarkernels.h:33-34, u1kernels.h:50)
@@ -207,13 +208,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int c = 0; c < 5; ++c) {
         const bool phi = c < 2;
-        const double p1 = p[c * n3 + s] - (phi ? g.hc : g.hu) * K[c].v;
+        const double p1 = (double)p[c * n3 + s] - (phi ? g.hc : g.hu) * K[c].v;
         pb[c] = l[c] + (phi ? g.cdf : g.cda) * qb[c];
         acc[phi ? 6 : 7] += p1 * qb[c];
       }
     } else {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) pb[c] = l[c] + (c < 2 ? g.Api : g.AE) * two_n3 * p[c * n3 + s];
+      for (int c = 0; c < 5; ++c) pb[c] = l[c] + (c < 2 ? g.Api : g.AE) * two_n3 * (double)p[c * n3 + s];
     }
 #pragma unroll
     for (int c = 0; c < 5; ++c) {

@@ -433,10 +433,6 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     g_err = "clb_create: unknown model kind";
     return CLB_EUNSUPPORTED;
   }
-  if (u1 && cfg->precision != CLB_PREC_FP64) {
-    g_err = "clb_create: lphi4U1 runs in FP64 storage";
-    return CLB_EUNSUPPORTED;
-  }
   if (!u1 && !su2 && (md->n_scalars < 1 || md->n_scalars > 2)) {
     g_err = "clb_create: lphi4 supports 1 or 2 scalar singlets";
     return CLB_EUNSUPPORTED;

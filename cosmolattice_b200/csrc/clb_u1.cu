@@ -24,18 +24,21 @@ constexpr int kU1Blocks = 148 * 8; // grid-stride sweeps: 8 resident 256-thread 
 }
 
 struct U1Sector {
-  double *f = nullptr, *p = nullptr; // 5 x N^3 each
+  void *f = nullptr, *p = nullptr; // 5 x N^3 each, FP64 or FP32 (esz bytes per value)
+  bool fp32 = false;
+  size_t esz = 8;
+  double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   U1State *d_st = nullptr;
   double *d_part = nullptr; // kU1Blocks x kU1Meas
   double *d_sums = nullptr; // kU1Meas
   U1Params prm{};
   // adjoint: checkpoints every K steps, one segment of stage-boundary states, cotangents
   struct Ckpt {
-    double *f = nullptr, *p = nullptr;
+    void *f = nullptr, *p = nullptr;
     U1State st{};
   };
   std::vector<Ckpt> ckpt;
-  double *seg = nullptr; // (K S + 1) boundary states of 10 N^3
+  char *seg = nullptr;   // (K S + 1) boundary states of 10 N^3 values
   int64_t seg_cap = 0;   // boundary states the segment buffer holds
   U1State *d_rec = nullptr;
   double *qbar = nullptr, *pbar[2] = {nullptr, nullptr};
@@ -88,18 +91,44 @@ U1Kick vv_kick(double dt, double wa, double wb)
 }
 U1Kick lf_kick(double dt, double w) { return U1Kick{{w * dt, 0.0}, {w * dt, 0.0}}; }
 
-template <int NK, bool RF, bool RP> void kick(clb_handle *h, int kind, const U1Kick &kc)
+template <int NK, bool RF, bool RP, class S> void kick_t(clb_handle *h, int kind, const U1Kick &kc)
 {
   U1Sector *u = h->u1;
   CLB_LAUNCH(h, kind,
-             k_u1_kick<NK, RF, RP><<<kU1Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, kc, u->d_st, u->d_part));
+             k_u1_kick<NK, RF, RP, S><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<const S *>(u->f),
+                                                                         static_cast<S *>(u->p), u->prm, kc, u->d_st,
+                                                                         u->d_part));
+}
+template <int NK, bool RF, bool RP> void kick(clb_handle *h, int kind, const U1Kick &kc)
+{
+  if (h->u1->fp32) return kick_t<NK, RF, RP, float>(h, kind, kc);
+  kick_t<NK, RF, RP, double>(h, kind, kc);
 }
 
-void drift(clb_handle *h, double w)
+template <class S> void drift_t(clb_handle *h, double w)
 {
   U1Sector *u = h->u1;
   CLB_LAUNCH(h, K_U1_DRIFT,
-             k_u1_drift<<<kU1Blocks, 256, 0, h->stream>>>(u->f, u->p, h->n3, w, h->cfg.dt, u->d_st));
+             k_u1_drift<S><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<S *>(u->f), static_cast<const S *>(u->p),
+                                                              h->n3, w, h->cfg.dt, u->d_st));
+}
+void drift(clb_handle *h, double w)
+{
+  if (h->u1->fp32) return drift_t<float>(h, w);
+  drift_t<double>(h, w);
+}
+
+// One measurement sweep of the live state into d_sums (unnormalised sums, kU1Meas slots).
+void measure_sums(clb_handle *h)
+{
+  U1Sector *u = h->u1;
+  if (u->fp32)
+    CLB_LAUNCH(h, K_MEASURE, k_u1_measure<float><<<kU1Blocks, 256, 0, h->stream>>>(
+                                 static_cast<const float *>(u->f), static_cast<const float *>(u->p), u->prm, u->d_part));
+  else
+    CLB_LAUNCH(h, K_MEASURE, k_u1_measure<double><<<kU1Blocks, 256, 0, h->stream>>>(
+                                 static_cast<const double *>(u->f), static_cast<const double *>(u->p), u->prm, u->d_part));
+  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kU1Meas><<<1, 256, 0, h->stream>>>(u->d_part, kU1Blocks, u->d_sums));
 }
 
 void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
@@ -148,10 +177,13 @@ __attribute__((visibility("hidden"))) int u1_create(clb_handle *h)
   h->u1 = u;
   h->NS = 5;
   u->prm = make_params(h);
-  const size_t bytes = 5 * h->n3 * sizeof(double);
+  u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
+  u->esz = u->fp32 ? sizeof(float) : sizeof(double);
+  const size_t bytes = 5 * h->n3 * u->esz;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, bytes) == cudaSuccess && cudaMalloc(&u->p, bytes) == cudaSuccess;
   ok = ok && cudaMemset(u->f, 0, bytes) == cudaSuccess && cudaMemset(u->p, 0, bytes) == cudaSuccess;
+  if (u->fp32) ok = ok && cudaMalloc(&u->d_stage, h->n3 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_st, sizeof(U1State)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_part, (size_t)kU1Blocks * kU1Meas * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_sums, kU1Meas * sizeof(double)) == cudaSuccess;
@@ -192,6 +224,7 @@ __attribute__((visibility("hidden"))) void u1_destroy(clb_handle *h)
   if (u->d_st) cudaFree(u->d_st);
   if (u->d_part) cudaFree(u->d_part);
   if (u->d_sums) cudaFree(u->d_sums);
+  if (u->d_stage) cudaFree(u->d_stage);
   delete u;
   h->u1 = nullptr;
 }
@@ -202,8 +235,19 @@ __attribute__((visibility("hidden"))) int u1_set_state(clb_handle *h, const doub
   U1Sector *u = h->u1;
   const size_t bytes = 5 * h->n3 * sizeof(double);
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, bytes, cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, bytes, cudaMemcpyHostToDevice, h->stream);
+  if (!u->fp32) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, bytes, cudaMemcpyHostToDevice, h->stream);
+  } else {
+    // one component at a time through the FP64 staging buffer, rounded once to FP32
+    for (int c = 0; c < 10 && e == cudaSuccess; ++c) {
+      const double *src = (c < 5 ? fields : momenta) + (size_t)(c % 5) * h->n3;
+      float *dst = static_cast<float *>(c < 5 ? u->f : u->p) + (size_t)(c % 5) * h->n3;
+      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+      if (e == cudaSuccess) k_convert<double, float><<<kU1Blocks, 256, 0, h->stream>>>(u->d_stage, dst, h->n3);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   U1State s{};
@@ -231,8 +275,20 @@ __attribute__((visibility("hidden"))) int u1_get_state(clb_handle *h, double *fi
   U1Sector *u = h->u1;
   const size_t bytes = 5 * h->n3 * sizeof(double);
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess && fields) e = cudaMemcpyAsync(fields, u->f, bytes, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess && momenta) e = cudaMemcpyAsync(momenta, u->p, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (!u->fp32) {
+    if (e == cudaSuccess && fields) e = cudaMemcpyAsync(fields, u->f, bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && momenta) e = cudaMemcpyAsync(momenta, u->p, bytes, cudaMemcpyDeviceToHost, h->stream);
+  } else {
+    for (int c = 0; c < 10 && e == cudaSuccess; ++c) {
+      double *dst = c < 5 ? fields : momenta;
+      if (!dst) continue;
+      dst += (size_t)(c % 5) * h->n3;
+      const float *src = static_cast<const float *>(c < 5 ? u->f : u->p) + (size_t)(c % 5) * h->n3;
+      k_convert<float, double><<<kU1Blocks, 256, 0, h->stream>>>(src, u->d_stage, h->n3);
+      e = cudaMemcpyAsync(dst, u->d_stage, h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+  }
   U1State s;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -333,8 +389,7 @@ __attribute__((visibility("hidden"))) int u1_measure(clb_handle *h, double e0, c
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaMemcpy(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
-  CLB_LAUNCH(h, K_MEASURE, k_u1_measure<<<kU1Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, u->d_part));
-  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kU1Meas><<<1, 256, 0, h->stream>>>(u->d_part, kU1Blocks, u->d_sums));
+  measure_sums(h);
   double v[kU1Meas];
   e = cudaMemcpyAsync(v, u->d_sums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -448,10 +503,10 @@ void vv_stage(clb_handle *h, double w)
   if (ex) tail(h, T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, true, w, 0);
 }
 
-cudaError_t copy_state(clb_handle *h, double *f, double *p, bool to_live)
+cudaError_t copy_state(clb_handle *h, void *f, void *p, bool to_live)
 {
   U1Sector *u = h->u1;
-  const size_t bytes = 5 * h->n3 * sizeof(double);
+  const size_t bytes = 5 * h->n3 * u->esz;
   cudaError_t e = cudaMemcpyAsync(to_live ? u->f : f, to_live ? f : u->f, bytes, cudaMemcpyDeviceToDevice, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(to_live ? u->p : p, to_live ? p : u->p, bytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -468,14 +523,22 @@ void energies_of(const U1Params &p, double a, const double (&A)[kAvgN], double (
   E[4] = A[4];
 }
 
-int adj_sweep(clb_handle *h, int pre, const double *f, const double *p, const double *pin, double *pout,
+template <int PRE, class T>
+void adj_launch(clb_handle *h, const void *f, const void *p, const double *pin, double *pout, const U1AdjArgs &g)
+{
+  U1Sector *u = h->u1;
+  k_u1_adj<PRE, T><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<const T *>(f), static_cast<const T *>(p), pin,
+                                                      u->qbar, pout, u->prm, g, u->d_apart);
+}
+
+int adj_sweep(clb_handle *h, int pre, const void *f, const void *p, const double *pin, double *pout,
               const U1AdjArgs &g, double (&S)[kAdjSlots])
 {
   U1Sector *u = h->u1;
-  if (pre)
-    k_u1_adj<1><<<kU1Blocks, 256, 0, h->stream>>>(f, p, pin, u->qbar, pout, u->prm, g, u->d_apart);
+  if (u->fp32)
+    pre ? adj_launch<1, float>(h, f, p, pin, pout, g) : adj_launch<0, float>(h, f, p, pin, pout, g);
   else
-    k_u1_adj<0><<<kU1Blocks, 256, 0, h->stream>>>(f, p, pin, u->qbar, pout, u->prm, g, u->d_apart);
+    pre ? adj_launch<1, double>(h, f, p, pin, pout, g) : adj_launch<0, double>(h, f, p, pin, pout, g);
   ++h->launches[K_U1_ADJ];
   k_sum_partials<kAdjSlots><<<1, 256, 0, h->stream>>>(u->d_apart, kU1Blocks, u->d_asums);
   cudaError_t e = cudaMemcpyAsync(S, u->d_asums, sizeof(S), cudaMemcpyDeviceToHost, h->stream);
@@ -521,7 +584,7 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward");
   free_adjoint(u);
-  const size_t bytes = 5 * h->n3 * sizeof(double);
+  const size_t bytes = 5 * h->n3 * u->esz, dbytes = 5 * h->n3 * sizeof(double);
   const int64_t nck = (nsteps + K - 1) / K;
   const int64_t S = 2 * (int64_t)h->ws.size() - 1;
   const int64_t seg_states = std::min<int64_t>(K, nsteps) * S + 1;
@@ -530,8 +593,8 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   for (auto &c : u->ckpt) ok = ok && cudaMalloc(&c.f, bytes) == cudaSuccess && cudaMalloc(&c.p, bytes) == cudaSuccess;
   ok = ok && cudaMalloc(&u->seg, (size_t)seg_states * 2 * bytes) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_rec, (size_t)seg_states * sizeof(U1State)) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->qbar, bytes) == cudaSuccess && cudaMalloc(&u->pbar[0], bytes) == cudaSuccess &&
-       cudaMalloc(&u->pbar[1], bytes) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->qbar, dbytes) == cudaSuccess && cudaMalloc(&u->pbar[0], dbytes) == cudaSuccess &&
+       cudaMalloc(&u->pbar[1], dbytes) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_apart, (size_t)kU1Blocks * kAdjSlots * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_asums, kAdjSlots * sizeof(double)) == cudaSuccess;
   if (!ok) {
@@ -563,8 +626,7 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   float ms = 0;
   if (cudaEventElapsedTime(&ms, h->ev_call[0], h->ev_call[1]) == cudaSuccess) h->last_evolve_ms = ms;
   // final averages (one measurement sweep) and the observable
-  CLB_LAUNCH(h, K_MEASURE, k_u1_measure<<<kU1Blocks, 256, 0, h->stream>>>(u->f, u->p, u->prm, u->d_part));
-  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kU1Meas><<<1, 256, 0, h->stream>>>(u->d_part, kU1Blocks, u->d_sums));
+  measure_sums(h);
   double v[kU1Meas];
   U1State s;
   e = cudaMemcpyAsync(v, u->d_sums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
@@ -606,7 +668,7 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
   const U1Params &prm = u->prm;
   const bool ex = h->cfg.expansion != 0;
   const double dt = h->cfg.dt, al = prm.alpha;
-  const size_t bytes = 5 * h->n3 * sizeof(double);
+  const size_t bytes = 5 * h->n3 * sizeof(double); // cotangents are FP64 in either form
   const std::vector<double> &ws = h->ws;
   const size_t P = ws.size();
   const int64_t S = 2 * (int64_t)P - 1;
@@ -644,9 +706,10 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
   thc += Abar[4] * prm.inv_n3 * S9[8];
   std::vector<U1State> rec((size_t)u->seg_cap);
   const int64_t nck = (int64_t)u->ckpt.size() - 1; // the last entry holds the forward's end state
-  double *seg = u->seg;
-  auto segf = [&](int64_t b) { return seg + (size_t)b * 10 * h->n3; };
-  auto segp = [&](int64_t b) { return seg + (size_t)b * 10 * h->n3 + 5 * h->n3; };
+  char *seg = u->seg;
+  const size_t half = 5 * h->n3 * u->esz;
+  auto segf = [&](int64_t b) -> void * { return seg + (size_t)b * 2 * half; };
+  auto segp = [&](int64_t b) -> void * { return seg + (size_t)b * 2 * half + half; };
   for (int64_t c = nck - 1; c >= 0; --c) {
     const int64_t s0 = c * u->fwd_K, s1 = std::min(u->fwd_steps, s0 + u->fwd_K);
     const int64_t nb = (s1 - s0) * S; // stages in this segment
@@ -763,9 +826,14 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
 // whether the component belongs to the U(1) field.
 __attribute__((visibility("hidden"))) const double *u1_component(clb_handle *h, int which, int comp, bool *gauge)
 {
+  U1Sector *u = h->u1;
   if (comp < 0 || comp >= 5) return nullptr;
   *gauge = comp >= 2;
-  return (which == 0 ? h->u1->f : h->u1->p) + (size_t)comp * h->n3;
+  if (!u->fp32) return static_cast<const double *>(which == 0 ? u->f : u->p) + (size_t)comp * h->n3;
+  // FP32 form: the component in FP64 in the staging buffer (ordered on the handle's stream)
+  const float *src = static_cast<const float *>(which == 0 ? u->f : u->p) + (size_t)comp * h->n3;
+  k_convert<float, double><<<kU1Blocks, 256, 0, h->stream>>>(src, u->d_stage, h->n3);
+  return u->d_stage;
 }
 
 } // namespace clb

@@ -60,44 +60,54 @@ __device__ __forceinline__ double u1_m(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double u1_a(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double u1_s(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double u1_d(double a, double b) { return __ddiv_rn(a, b); }
+// FP32 form: plain single-precision arithmetic (contraction allowed)
+__device__ __forceinline__ float u1_m(float a, float b) { return a * b; }
+__device__ __forceinline__ float u1_a(float a, float b) { return a + b; }
+__device__ __forceinline__ float u1_s(float a, float b) { return a - b; }
+__device__ __forceinline__ float u1_d(float a, float b) { return a / b; }
+__device__ __forceinline__ void u1_sincos(double x, double *sn, double *cs) { sincos(x, sn, cs); }
+__device__ __forceinline__ void u1_sincos(float x, float *sn, float *cs) { sincosf(x, sn, cs); }
 
-// Per-site kernel values.  Fields f: [Re phi, Im phi, A_x, A_y, A_z] x n3.
-struct U1Site {
-  double fr, fi;            // phi(x)
-  double wr[3], wi[3];      // U_i(x) phi(x + i)
-  double g0[3][3];          // forwDiff(A_j, i)(x) = (A_j(x + i) - A_j(x)) / dx, [i][j]
-  double Kr, Ki;            // complex scalar kernel
-  double KA[3];             // U(1) kernel per direction
-  double nrm;               // |phi|
+// Per-site kernel values in arithmetic type T.  Fields f (storage S): [Re phi, Im phi, A_x, A_y,
+// A_z] x n3.  The FP64 form (S = T = double) pins every rounding; the FP32 form computes in float.
+template <class T> struct U1Site {
+  T fr, fi;            // phi(x)
+  T wr[3], wi[3];      // U_i(x) phi(x + i)
+  T g0[3][3];          // forwDiff(A_j, i)(x) = (A_j(x + i) - A_j(x)) / dx, [i][j]
+  T Kr, Ki;            // complex scalar kernel
+  T KA[3];             // U(1) kernel per direction
+  T nrm;               // |phi|
 };
 
-template <bool KERNEL>
-__device__ __forceinline__ void u1_site(const double *__restrict__ f, const U1Params &a, size_t s,
-                                        const long long (&op)[3], const long long (&om)[3], double kA, double kB2,
-                                        double kG, U1Site &o)
+template <bool KERNEL, class S, class T>
+__device__ __forceinline__ void u1_site(const S *__restrict__ f, const U1Params &a, size_t s,
+                                        const long long (&op)[3], const long long (&om)[3], T kA, T kB2, T kG,
+                                        U1Site<T> &o)
 {
   const size_t n3 = a.n3;
-  const double *phr = f, *phi = f + n3;
-  const double *A[3] = {f + 2 * n3, f + 3 * n3, f + 4 * n3};
-  o.fr = phr[s];
-  o.fi = phi[s];
-  double pr = 0, pim = 0, mr = 0, mim = 0;
+  const S *phr = f, *phi = f + n3;
+  const S *A[3] = {f + 2 * n3, f + 3 * n3, f + 4 * n3};
+  const T ndxg = (T)a.ndxg, dx = (T)a.dx, dx2 = (T)a.dx2, inv_dx2 = (T)a.inv_dx2, c4 = (T)a.c4;
+  const T J0 = (T)a.J0, gQ = (T)a.gQ;
+  o.fr = (T)phr[s];
+  o.fi = (T)phi[s];
+  T pr = 0, pim = 0, mr = 0, mim = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const size_t sp = s + op[d];
-    double ur, ui;
-    sincos(u1_m(a.ndxg, A[d][s]), &ui, &ur);
-    const double gr = phr[sp], gi = phi[sp];
+    T ur, ui;
+    u1_sincos(u1_m(ndxg, (T)A[d][s]), &ui, &ur);
+    const T gr = (T)phr[sp], gi = (T)phi[sp];
     o.wr[d] = u1_s(u1_m(ur, gr), u1_m(ui, gi));
     o.wi[d] = u1_a(u1_m(ur, gi), u1_m(ui, gr));
     if (KERNEL) {
       // conj(U_d(x - d)) phi(x - d)
       const size_t sm = s + om[d];
-      double vr, vi;
-      sincos(u1_m(a.ndxg, A[d][sm]), &vi, &vr);
-      const double nvi = -vi, hr = phr[sm], hi = phi[sm];
-      const double cr = u1_s(u1_m(vr, hr), u1_m(nvi, hi));
-      const double ci = u1_a(u1_m(vr, hi), u1_m(nvi, hr));
+      T vr, vi;
+      u1_sincos(u1_m(ndxg, (T)A[d][sm]), &vi, &vr);
+      const T nvi = -vi, hr = (T)phr[sm], hi = (T)phi[sm];
+      const T cr = u1_s(u1_m(vr, hr), u1_m(nvi, hi));
+      const T ci = u1_a(u1_m(vr, hi), u1_m(nvi, hr));
       if (d == 0) {
         pr = o.wr[0];
         pim = o.wi[0];
@@ -114,62 +124,62 @@ __device__ __forceinline__ void u1_site(const double *__restrict__ f, const U1Pa
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) o.g0[i][j] = u1_d(u1_s(A[j][s + op[i]], A[j][s]), a.dx);
+    for (int j = 0; j < 3; ++j) o.g0[i][j] = u1_d(u1_s((T)A[j][s + op[i]], (T)A[j][s]), dx);
   o.nrm = sqrt(u1_a(u1_m(o.fr, o.fr), u1_m(o.fi, o.fi)));
   if (!KERNEL) return;
   // complex scalar: a^{1+alpha} covLap(phi) - a^{3+alpha}/2 (dV/d|phi|)/|phi| phi
-  const double clr = u1_d(u1_s(u1_a(pr, mr), u1_m(6.0, o.fr)), a.dx2);
-  const double cli = u1_d(u1_s(u1_a(pim, mim), u1_m(6.0, o.fi)), a.dx2);
-  const double nd = u1_m(a.c4, u1_m(4.0, u1_m(u1_m(o.nrm, o.nrm), o.nrm)));
-  const double q = u1_d(nd, o.nrm);
+  const T clr = u1_d(u1_s(u1_a(pr, mr), u1_m(T(6.0), o.fr)), dx2);
+  const T cli = u1_d(u1_s(u1_a(pim, mim), u1_m(T(6.0), o.fi)), dx2);
+  const T nd = u1_m(c4, u1_m(T(4.0), u1_m(u1_m(o.nrm, o.nrm), o.nrm)));
+  const T q = u1_d(nd, o.nrm);
   o.Kr = u1_s(u1_m(kA, clr), u1_m(kB2, u1_m(q, o.fr)));
   o.Ki = u1_s(u1_m(kA, cli), u1_m(kB2, u1_m(q, o.fi)));
   // U(1): a^{alpha-1} (lapl A_i - sum_j backDiff_j forwDiff_i A_j) - a^{1+alpha} J_i
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    const double c = A[i][s];
-    double t[3];
+    const T c = (T)A[i][s];
+    T t[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) t[d] = u1_s(u1_a(A[i][s + op[d]], A[i][s + om[d]]), u1_m(2.0, c));
-    const double lap = u1_m(a.inv_dx2, u1_a(u1_a(t[0], t[1]), t[2]));
-    double grad = 0;
+    for (int d = 0; d < 3; ++d) t[d] = u1_s(u1_a((T)A[i][s + op[d]], (T)A[i][s + om[d]]), u1_m(T(2.0), c));
+    const T lap = u1_m(inv_dx2, u1_a(u1_a(t[0], t[1]), t[2]));
+    T grad = 0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const size_t sj = s + om[j];
       const size_t sij = i == j ? s : s + op[i] + om[j]; // x + i - j
-      const double g1 = u1_d(u1_s(A[j][sij], A[j][sj]), a.dx);
-      const double tj = u1_d(u1_s(o.g0[i][j], g1), a.dx);
+      const T g1 = u1_d(u1_s((T)A[j][sij], (T)A[j][sj]), dx);
+      const T tj = u1_d(u1_s(o.g0[i][j], g1), dx);
       grad = j == 0 ? tj : u1_a(grad, tj);
     }
-    const double im = u1_s(u1_m(o.wr[i], o.fi), u1_m(o.wi[i], o.fr));
-    const double J = u1_m(a.J0, u1_m(a.gQ, im));
+    const T im = u1_s(u1_m(o.wr[i], o.fi), u1_m(o.wi[i], o.fr));
+    const T J = u1_m(J0, u1_m(gQ, im));
     o.KA[i] = u1_s(u1_m(kG, u1_s(lap, grad)), u1_m(kA, J));
   }
 }
 
 // sum_j |D+_j phi|^2 (fieldfunctionals.h:80-84) from the site's covariant neighbours
-__device__ __forceinline__ double u1_cs_grad2(const U1Site &o, double dx)
+template <class T> __device__ __forceinline__ T u1_cs_grad2(const U1Site<T> &o, T dx)
 {
-  double acc = 0;
+  T acc = 0;
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    const double dr = u1_d(u1_s(o.wr[j], o.fr), dx), di = u1_d(u1_s(o.wi[j], o.fi), dx);
-    const double n2 = u1_a(u1_m(dr, dr), u1_m(di, di));
+    const T dr = u1_d(u1_s(o.wr[j], o.fr), dx), di = u1_d(u1_s(o.wi[j], o.fi), dx);
+    const T n2 = u1_a(u1_m(dr, dr), u1_m(di, di));
     acc = j == 0 ? n2 : u1_a(acc, n2);
   }
   return acc;
 }
 
 // F_21^2 + (F_31^2 + F_32^2), F_ij = forwDiff(A_j, i) - forwDiff(A_i, j) (fieldfunctionals.h:133-141)
-__device__ __forceinline__ double u1_b2(const U1Site &o)
+template <class T> __device__ __forceinline__ T u1_b2(const U1Site<T> &o)
 {
-  const double f21 = u1_s(o.g0[1][0], o.g0[0][1]);
-  const double f31 = u1_s(o.g0[2][0], o.g0[0][2]);
-  const double f32 = u1_s(o.g0[2][1], o.g0[1][2]);
+  const T f21 = u1_s(o.g0[1][0], o.g0[0][1]);
+  const T f31 = u1_s(o.g0[2][0], o.g0[0][2]);
+  const T f32 = u1_s(o.g0[2][1], o.g0[1][2]);
   return u1_a(u1_m(f21, f21), u1_a(u1_m(f31, f31), u1_m(f32, f32)));
 }
 
-__device__ __forceinline__ double u1_pot(const U1Site &o, double c4)
+template <class T> __device__ __forceinline__ T u1_pot(const U1Site<T> &o, T c4)
 {
   return u1_m(c4, u1_m(u1_m(u1_m(o.nrm, o.nrm), o.nrm), o.nrm));
 }
@@ -183,37 +193,42 @@ __device__ __forceinline__ double u1_pot(const U1Site &o, double c4)
 #ifndef CLB_U1_KICK_MINB
 #define CLB_U1_KICK_MINB 2
 #endif
-template <int NK, bool RF, bool RP>
+template <int NK, bool RF, bool RP, class S>
 __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
-    k_u1_kick(const double *__restrict__ f, double *__restrict__ p, U1Params a, U1Kick kc,
-              const U1State *__restrict__ st, double *__restrict__ partials)
+    k_u1_kick(const S *__restrict__ f, S *__restrict__ p, U1Params a, U1Kick kc, const U1State *__restrict__ st,
+              double *__restrict__ partials)
 {
   __shared__ double smem[(256 / 32) * kU1Red];
   const size_t n3 = a.n3;
-  const double kA = st->kA, kB2 = st->kB2, kG = st->kG;
+  const S kA = (S)st->kA, kB2 = (S)st->kB2, kG = (S)st->kG;
   double acc[kU1Red];
 #pragma unroll
   for (int k = 0; k < kU1Red; ++k) acc[k] = 0;
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
-    U1Site o;
+    U1Site<S> o;
     u1_site<(NK > 0)>(f, a, s, op, om, kA, kB2, kG, o);
     if (RF) {
-      acc[2] += u1_cs_grad2(o, a.dx);
-      acc[3] += u1_b2(o);
-      acc[4] += u1_pot(o, a.c4);
+      acc[2] += (double)u1_cs_grad2(o, (S)a.dx);
+      acc[3] += (double)u1_b2(o);
+      acc[4] += (double)u1_pot(o, (S)a.c4);
     }
+    // momenta and their increments in FP64 (FP32 storage: rounded once per kick)
     double q[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) q[c] = p[c * n3 + s];
+    for (int c = 0; c < 5; ++c) q[c] = (double)p[c * n3 + s];
 #pragma unroll
     for (int k = 0; k < (NK > 0 ? NK : 1); ++k) {
       if (NK > 0) {
-        q[0] = u1_a(q[0], u1_m(kc.hc[k], o.Kr));
-        q[1] = u1_a(q[1], u1_m(kc.hc[k], o.Ki));
+        q[0] = u1_a(q[0], u1_m(kc.hc[k], (double)o.Kr));
+        q[1] = u1_a(q[1], u1_m(kc.hc[k], (double)o.Ki));
 #pragma unroll
-        for (int i = 0; i < 3; ++i) q[2 + i] = u1_a(q[2 + i], u1_m(kc.hu[k], o.KA[i]));
+        for (int i = 0; i < 3; ++i) q[2 + i] = u1_a(q[2 + i], u1_m(kc.hu[k], (double)o.KA[i]));
+        if (sizeof(S) == 4) {
+#pragma unroll
+          for (int c = 0; c < 5; ++c) q[c] = (double)(S)q[c]; // the stored value after this kick
+        }
       }
       if (RP) {
         acc[k == 0 ? 0 : 5] += u1_a(u1_m(q[0], q[0]), u1_m(q[1], q[1]));
@@ -222,7 +237,7 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
     }
     if (NK > 0) {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) p[c * n3 + s] = q[c];
+      for (int c = 0; c < 5; ++c) p[c * n3 + s] = (S)q[c];
     }
   }
   if (RF || RP) {
@@ -236,15 +251,16 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
 
 // Drifts phi += ((pow(aSI, alpha-3) dt) w) pi_phi and A += ((pow(aSI, alpha-1) w) dt) pi_A
 // (velocityverlet.h:193-210; the leapfrog's forms leapfrog.h:203-217 are w = 1).
-static __global__ void __launch_bounds__(256)
-    k_u1_drift(double *__restrict__ f, const double *__restrict__ p, size_t n3, double w, double dt,
+template <class S>
+__global__ void __launch_bounds__(256)
+    k_u1_drift(S *__restrict__ f, const S *__restrict__ p, size_t n3, double w, double dt,
                const U1State *__restrict__ st)
 {
   const double cc = u1_m(u1_m(st->cs_drift, dt), w);
   const double cu = u1_m(u1_m(st->u1_drift, w), dt);
   const size_t n = 5 * n3, n2 = 2 * n3;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    f[i] = u1_a(f[i], u1_m(i < n2 ? cc : cu, p[i]));
+    f[i] = (S)u1_a((double)f[i], u1_m(i < n2 ? cc : cu, (double)p[i]));
 }
 
 // ScaleFactorKernels::get with complex-scalar and U(1) energies (scalefactorkernels.h:73-77,
@@ -365,8 +381,10 @@ static __global__ void __launch_bounds__(256)
 // [5..10] Re phi, (Re phi)^2, Im phi, (Im phi)^2, |phi|, |phi|^2, [11..16] the same of pi_phi,
 // [17] |pi_A|, [18] |B|, [19..22] Gauss |LHS - RHS|, |sum of squares|, |RHS|, |LHS|
 // (gausslaws.h:34-53 with U1ChargeDensity, mattercurrents.h:27-48).
-static __global__ void __launch_bounds__(256)
-    k_u1_measure(const double *__restrict__ f, const double *__restrict__ p, U1Params a, double *__restrict__ partials)
+// FP32 storage is measured in FP64 arithmetic on the stored values.
+template <class S>
+__global__ void __launch_bounds__(256)
+    k_u1_measure(const S *__restrict__ f, const S *__restrict__ p, U1Params a, double *__restrict__ partials)
 {
   __shared__ double smem[(256 / 32) * kU1Meas];
   const size_t n3 = a.n3;
@@ -377,14 +395,14 @@ static __global__ void __launch_bounds__(256)
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
-    U1Site o;
-    u1_site<false>(f, a, s, op, om, 0, 0, 0, o);
-    const double pr = p[s], pi = p[n3 + s];
+    U1Site<double> o;
+    u1_site<false>(f, a, s, op, om, 0.0, 0.0, 0.0, o);
+    const double pr = (double)p[s], pi = (double)p[n3 + s];
     double q[3], l[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      q[i] = p[(2 + i) * n3 + s];
-      l[i] = u1_s(q[i], p[(2 + i) * n3 + s + om[i]]);
+      q[i] = (double)p[(2 + i) * n3 + s];
+      l[i] = u1_s(q[i], (double)p[(2 + i) * n3 + s + om[i]]);
     }
     const double cp2 = u1_a(u1_m(pr, pr), u1_m(pi, pi));
     const double up2 = u1_a(u1_a(u1_m(q[0], q[0]), u1_m(q[1], q[1])), u1_m(q[2], q[2]));

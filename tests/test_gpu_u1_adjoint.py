@@ -151,3 +151,24 @@ def test_adjoint_rejects_unsupported():
         lat.backward()
     assert e.value.code == _capi.CLB_ESTATE
     lat.close()
+
+
+def test_fp32_form_gradients_track_fp64():
+    # FP32 storage forward (FP64 increments and sums), FP64 cotangents: the observable and its
+    # gradients follow the FP64 pair to the FP32 trajectory error (bounds: 1e-5 on O, 1e-3 on
+    # each gradient relative to the largest one).
+    from cosmolattice_b200 import Lattice
+    from cosmolattice_b200.adjoint import u1_gradients
+
+    N, dt, n, K = 12, 0.01, 30, 5
+    par, rp, m, f, p, sf = case(N, "VV4", True, dt)
+    O64, g64, _ = u1_gradients(m, rp, n, K)
+    lat = Lattice(m, rp, precision="fp32")
+    O32, g32, _ = u1_gradients(m, rp, n, K, lattice=lat)
+    lat.close()
+    scale = max(abs(v) for v in g64.values())
+    print("fp32 adjoint: O", abs(O32 - O64) / abs(O64),
+          {k: abs(g32[k] - g64[k]) / scale for k in g64})
+    assert abs(O32 - O64) <= 1e-5 * abs(O64)
+    for k in g64:
+        assert abs(g32[k] - g64[k]) <= 1e-3 * scale, (k, g32[k], g64[k])
