@@ -548,7 +548,58 @@ def main_su2(args):
 
     r64 = run("fp64")
     r32 = run("fp32")
-    del f, p
+
+    # d(gauge-energy fraction)/d g_SU2 by the tangent-linear form, FP64 and FP32 storage
+    from cosmolattice_b200.adjoint import SU2_GAUGE_FRACTION
+
+    from cosmolattice_b200.initializers import su2u1_initial_state_tangent
+
+    dfs, dps, cds = su2u1_initial_state_tangent(m, rp, "gSU2", (f, p))
+    sfs = {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+
+    def grad_run(precision):
+        lat = Lattice(m, rp, precision=precision, device=local)
+        t0 = time.perf_counter()
+        lat.set_state(f, p, sfs)
+        lat.tangent_begin(cds, dfs, dps)
+        lat.initialize()
+        lat.evolve(steps)
+        lat.sync()
+        O, dO = lat.tangent_observable(SU2_GAUGE_FRACTION)
+        E, dE = lat.tangent_energies()
+        wall = time.perf_counter() - t0
+        ms = lat.last_evolve_ms()
+        lat.close()
+        return {"observable": O, "gradient": dO, "energies": E.tolist(), "d_energies": dE.tolist(),
+                "evolve_ms": ms, "wall_s": wall}
+
+    g64 = grad_run("fp64")
+    g32 = grad_run("fp32")
+    # central difference of the plain FP64 path at h = 1e-2 g_SU2: the start state is linear in
+    # g_SU2 (only the Gauss-solved SU(2) momenta depend on it), so it is p + (g - g0) dp.  Smaller
+    # steps are dominated by rounding in the SU(2) magnetic energy, 4/(dx^4 g^2) sum(2 - tr P),
+    # which is 1e-11 of E_tot here.
+    fdE = []
+    h = 1e-2 * 0.6
+    for g in (0.6 + h, 0.6 - h):
+        par_g = ParameterParser(params=dict(par.params, gSU2s=g))
+        rp_g = RunParameters(par_g)
+        m_g = MODELS["lphi4SU2U1"](par_g, rp_g)
+        lat = Lattice(m_g, rp_g, device=local)
+        lat.set_state(f, p + (g - 0.6) * dps.reshape(p.shape), sfs)
+        lat.initialize()
+        lat.evolve(steps)
+        lat.sync()
+        e = lat.measure(1.0)["energies"]
+        fdE.append(list(e[:10]) + [sum(e[10:13])])
+        lat.close()
+    del f, p, dfs, dps
+    fd_comp = [(a - b) / (2 * h) for a, b in zip(fdE[0], fdE[1])]
+    Ow = [sum(w * x for w, x in zip(SU2_GAUGE_FRACTION, E)) / sum(E) for E in fdE]
+    fd = (Ow[0] - Ow[1]) / (2 * h)
+    names = ["Ekin_S", "Egrad_S", "Ekin_phi", "Egrad_phi", "Ekin_Phi", "Egrad_Phi", "Eel_U1", "Emag_U1",
+             "Eel_SU2", "Emag_SU2", "V"]
+    comp_diff = {nm: abs(t - d) / abs(d) if d else None for nm, t, d in zip(names, g64["d_energies"], fd_comp)}
     if rank != 0:
         return
     sites = N ** 3
@@ -585,7 +636,17 @@ def main_su2(args):
         "doublet_spectrum_bins": len(r64["spec"]), "doublet_spectrum_end_head": [float(x) for x in r64["spec"][:8]],
         "initial_state_s": ic_s,
         "kernel_launches": {k: v["launches"] for k, v in r64["stats"].items() if v["launches"]},
-        "adjoint": "not built for lphi4SU2U1",
+        "gradient_gSU2": {
+            "observable": "(E_el + E_mag of U(1) and SU(2)) / E_tot at the end",
+            "method": "tangent-linear (forward-mode) evolution, one pass, no checkpoints",
+            "fp64": g64, "fp32": g32,
+            "finite_difference": fd, "fd_step": "h = 1e-2 g_SU2 (central)",
+            "rel_diff_fp64_vs_fd": abs(g64["gradient"] - fd) / abs(fd),
+            "rel_diff_fp32_vs_fd": abs(g32["gradient"] - fd) / abs(fd),
+            "rel_diff_fp32_vs_fp64": abs(g32["gradient"] - g64["gradient"]) / abs(g64["gradient"]),
+            "d_energies_fd": fd_comp, "d_energies_rel_diff_fp64_vs_fd": comp_diff,
+            "cost_vs_plain_fp64": g64["evolve_ms"] / r64["ms"], "cost_fp32_vs_plain_fp32": g32["evolve_ms"] / r32["ms"],
+        },
         "clocks": r64["clocks"], "clocks_fp32": r32["clocks"],
     }
     print(json.dumps(line))

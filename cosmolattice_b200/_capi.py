@@ -147,6 +147,11 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
             "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
             "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
+            "clb_tangent_begin": (C.c_int, [H, dp, C.c_int32, dp, dp, C.POINTER(ScaleFactor)]),
+            "clb_tangent_get_state": (C.c_int, [H, dp, dp, C.POINTER(ScaleFactor)]),
+            "clb_tangent_observable": (C.c_int, [H, dp, C.c_int32, dp, dp]),
+            "clb_tangent_energies": (C.c_int, [H, dp, dp]),
+            "clb_tangent_end": (C.c_int, [H]),
             "clb_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(ModelDesc), C.c_int32, C.POINTER(H)]),
             "clb_batch_destroy": (None, [H]),
             "clb_batch_last_error": (C.c_char_p, [H]),
@@ -203,6 +208,11 @@ EXPORTED = [
     "clb_cuda_stream",
     "clb_forward",
     "clb_backward",
+    "clb_tangent_begin",
+    "clb_tangent_get_state",
+    "clb_tangent_observable",
+    "clb_tangent_energies",
+    "clb_tangent_end",
     "clb_batch_create",
     "clb_batch_destroy",
     "clb_batch_last_error",

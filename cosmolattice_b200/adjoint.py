@@ -1,4 +1,5 @@
-"""Gradients of final energy fractions of lphi4U1 through the adjoint pair of the C ABI.
+"""Gradients of final energy fractions: lphi4U1 through the adjoint pair of the C ABI, lphi4SU2U1
+through its tangent-linear form.
 
 dO/dtheta = (explicit dependence of the evolution on theta, from clb_backward)
           + <fields_bar, d fields_0 / d theta> + <momenta_bar, d momenta_0 / d theta>,
@@ -41,6 +42,43 @@ def u1_gradients(model: Model, rp: RunParameters, n_steps: int, checkpoint_every
         lat.close()
     g["fields_bar"], g["momenta_bar"] = fb, pb
     return O, out, g
+
+
+SU2_GAUGE_FRACTION = (0.0,) * 6 + (1.0, 1.0, 1.0, 1.0, 0.0)  # (E_el + E_mag of U(1) and SU(2)) / E_tot
+
+
+def su2_gradient(model: Model, rp: RunParameters, n_steps: int, param: str = "gSU2",
+                 weights: Sequence[float] = SU2_GAUGE_FRACTION, lattice: Lattice = None,
+                 state=None) -> Tuple[float, float]:
+    """(O, dO/dparam) for O = sum_k w_k E_k / E_tot of lphi4SU2U1 after n_steps, param "gSU2" or
+    "gU1", by the tangent-linear form (clb_tangent_*): the start state of su2u1_initial_state with
+    its tangent, clb_initialize(correct_adot=1) and the evolution differentiated in one pass.
+    E_k: E_kin and E_grad of S, phi, Phi; E_el, E_mag of U(1) and SU(2); V."""
+    from .initializers import su2u1_initial_state, su2u1_initial_state_tangent
+
+    lat = lattice if lattice is not None else Lattice(model, rp)
+    if state is None:
+        state = su2u1_initial_state(model, rp)
+    f, p, aI, aD = state
+    lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
+    df, dp, cd = su2u1_initial_state_tangent(model, rp, param, (f, p))
+    lat.tangent_begin(cd, df, dp)
+    lat.initialize(correct_adot=True)
+    lat.evolve(n_steps)
+    lat.sync()
+    O, dO = lat.tangent_observable(weights)
+    lat.tangent_end()
+    if lattice is None:
+        lat.close()
+    return O, dO
+
+
+def su2_observable_from_measurement(m: Dict[str, object], weights: Sequence[float] = SU2_GAUGE_FRACTION) -> float:
+    """O = sum_k w_k E_k / E_tot from an lphi4SU2U1 measurement dict (10 sector energies, the three
+    potential terms, E_tot): V is the sum of the potential terms."""
+    e = list(m["energies"])
+    comps = e[:10] + [sum(e[10:13])]
+    return float(sum(w * x for w, x in zip(weights, comps)) / sum(comps))
 
 
 def observable_from_measurement(m: Dict[str, object], weights: Sequence[float] = GAUGE_FRACTION) -> float:

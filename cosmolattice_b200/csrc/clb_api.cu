@@ -63,6 +63,12 @@ int su2_initialize(clb_handle *h, int32_t correct_adot);
 int su2_evolve(clb_handle *h, int64_t n);
 int su2_sync(clb_handle *h);
 int su2_measure(clb_handle *h, double e0, clb_measurement *m);
+int su2_tangent_begin(clb_handle *h, const double *couplings_dot, int32_t n, const double *fields_dot,
+                      const double *momenta_dot, const clb_scalefactor *sf_dot);
+int su2_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot, clb_scalefactor *sf_dot);
+int su2_tangent_observable(clb_handle *h, const double *w, int32_t nw, double *obs, double *dobs);
+int su2_tangent_end(clb_handle *h);
+int su2_tangent_energies(clb_handle *h, double *E, double *dE);
 
 const double *u1_component(clb_handle *h, int which, int comp, bool *gauge);
 const double *su2_component(clb_handle *h, int which, int comp, bool *gauge);
@@ -923,6 +929,46 @@ int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double
   if (!h) return CLB_EINVAL;
   if (!h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_backward: the adjoint pair covers lphi4U1");
   return u1_backward(h, through_init, fields_bar, momenta_bar, grad);
+}
+
+int clb_tangent_begin(clb_handle *h, const double *couplings_dot, int32_t n_couplings, const double *fields_dot,
+                      const double *momenta_dot, const clb_scalefactor *sf_dot)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers lphi4SU2U1");
+  if (!h->has_state) return h->fail(CLB_ESTATE, "clb_tangent_begin: call clb_set_state first");
+  return su2_tangent_begin(h, couplings_dot, n_couplings, fields_dot, momenta_dot, sf_dot);
+}
+
+int clb_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot, clb_scalefactor *sf_dot)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_get_state: the tangent-linear form covers lphi4SU2U1");
+  return su2_tangent_get_state(h, fields_dot, momenta_dot, sf_dot);
+}
+
+int clb_tangent_observable(clb_handle *h, const double *weights, int32_t n_weights, double *observable,
+                           double *d_observable)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_observable: the tangent-linear form covers lphi4SU2U1");
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_tangent_observable: call clb_initialize first");
+  return su2_tangent_observable(h, weights, n_weights, observable, d_observable);
+}
+
+int clb_tangent_energies(clb_handle *h, double *energies, double *d_energies)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_energies: the tangent-linear form covers lphi4SU2U1");
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_tangent_energies: call clb_initialize first");
+  return su2_tangent_energies(h, energies, d_energies);
+}
+
+int clb_tangent_end(clb_handle *h)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_end: the tangent-linear form covers lphi4SU2U1");
+  return su2_tangent_end(h);
 }
 
 constexpr int kSpecBlocks = 148 * 2;

@@ -31,6 +31,12 @@ struct SU2Sector {
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   int64_t steps_since_unitarize = 0;
   Params prm{};
+  // tangent-linear form: d(state) along the coupling direction tan_cd, active while tangent
+  bool tangent = false;
+  CoupDot tan_cd{};
+  void *df = nullptr, *dp = nullptr;
+  TState *d_tst = nullptr;
+  double *d_tpart = nullptr, *d_tsums = nullptr;
 };
 
 // FP32 form: links re-unitarised every this many steps
@@ -66,14 +72,14 @@ Params su2_params(const clb_handle *h)
   return a;
 }
 
-void coefs(State &s, double al)
+template <class T> void coefs(StateT<T> &s, double al)
 {
-  s.kA = std::pow(s.aI, 1 + al);
-  s.kB = std::pow(s.aI, 3 + al);
-  s.kB2 = std::pow(s.aI, 3 + al) / 2;
-  s.kG = std::pow(s.aI, -1 + al);
-  s.p3 = std::pow(s.aSI, al - 3);
-  s.p1 = std::pow(s.aSI, al - 1);
+  s.kA = pow(s.aI, 1 + al);
+  s.kB = pow(s.aI, 3 + al);
+  s.kB2 = pow(s.aI, 3 + al) / 2;
+  s.kG = pow(s.aI, -1 + al);
+  s.p3 = pow(s.aSI, al - 3);
+  s.p1 = pow(s.aSI, al - 1);
 }
 
 // Kick factors (velocityverlet.h:129-162; leapfrog.h:131-170): S (w dt)/2, phi, Phi and SU(2)
@@ -127,17 +133,73 @@ template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const K
 #undef CLB_SU2K
 }
 
+template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
+{
+  SU2Sector *u = h->su2;
+  const int kind = nk == 0 ? K_U1_REDUCE : K_U1_KICK;
+  const S *f = static_cast<const S *>(u->f), *df = static_cast<const S *>(u->df);
+  S *p = static_cast<S *>(u->p), *dp = static_cast<S *>(u->dp);
+#define CLB_SU2T(NK, RF, RP)                                                                                            \
+  CLB_LAUNCH(h, kind,                                                                                                   \
+             k_kick_tan<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, df, p, dp, u->prm, kc, u->d_tst,          \
+                                                                            u->tan_cd, u->d_tpart))
+  if (nk == 0) {
+    if (rf && rp)
+      CLB_SU2T(0, true, true);
+    else if (rf)
+      CLB_SU2T(0, true, false);
+    else
+      CLB_SU2T(0, false, true);
+  } else if (nk == 1) {
+    if (rf && rp)
+      CLB_SU2T(1, true, true);
+    else if (rp)
+      CLB_SU2T(1, false, true);
+    else
+      CLB_SU2T(1, false, false);
+  } else {
+    if (rf && rp)
+      CLB_SU2T(2, true, true);
+    else
+      CLB_SU2T(2, false, false);
+  }
+#undef CLB_SU2T
+}
+
 void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
 {
-  if (h->su2->fp32)
+  SU2Sector *u = h->su2;
+  if (u->tangent) {
+    if (u->fp32)
+      sweep_tan_t<float>(h, nk, rf, rp, kc);
+    else
+      sweep_tan_t<double>(h, nk, rf, rp, kc);
+  } else if (u->fp32) {
     sweep_t<float>(h, nk, rf, rp, kc);
-  else
+  } else {
     sweep_t<double>(h, nk, rf, rp, kc);
+  }
+}
+
+template <class S> void drift_tan_t(clb_handle *h, double w, bool lf)
+{
+  SU2Sector *u = h->su2;
+  CLB_LAUNCH(h, K_U1_DRIFT,
+             k_drift_tan<S><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<S *>(u->f), static_cast<S *>(u->df),
+                                                               static_cast<const S *>(u->p), static_cast<const S *>(u->dp),
+                                                               u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd));
 }
 
 void drift(clb_handle *h, double w, bool lf)
 {
   SU2Sector *u = h->su2;
+  if (u->tangent) {
+    if (u->fp32)
+      drift_tan_t<float>(h, w, lf);
+    else
+      drift_tan_t<double>(h, w, lf);
+    return;
+  }
   if (u->fp32)
     CLB_LAUNCH(h, K_U1_DRIFT, k_drift<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f),
                                                                                  static_cast<const float *>(u->p),
@@ -156,14 +218,30 @@ void step_done(clb_handle *h)
   if (!u->fp32) return;
   if (++u->steps_since_unitarize < kUnitarizeEvery) return;
   u->steps_since_unitarize = 0;
-  CLB_LAUNCH(h, K_U1_DRIFT, k_unitarize<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f), h->n3));
+  if (u->tangent)
+    CLB_LAUNCH(h, K_U1_DRIFT, k_unitarize_tan<float><<<kSU2Blocks, 256, 0, h->stream>>>(
+                                  static_cast<float *>(u->f), static_cast<float *>(u->df), h->n3));
+  else
+    CLB_LAUNCH(h, K_U1_DRIFT, k_unitarize<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f), h->n3));
 }
 
 void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
 {
   SU2Sector *u = h->su2;
   TailOp op{flags, reduced ? kSU2Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
-  CLB_LAUNCH(h, K_TAIL, su2d::k_tail<<<1, 256, 0, h->stream>>>(u->d_part, op, u->d_st, u->prm));
+  if (u->tangent)
+    CLB_LAUNCH(h, K_TAIL, su2d::k_tail<Tan<double>><<<1, 256, 0, h->stream>>>(u->d_tpart, op, u->d_tst, u->prm));
+  else
+    CLB_LAUNCH(h, K_TAIL, su2d::k_tail<double><<<1, 256, 0, h->stream>>>(u->d_part, op, u->d_st, u->prm));
+}
+
+// Value part of the tangent-form scalar state.
+State values_of(const TState &t)
+{
+  State s{};
+  zip_state(s, t, [](double &x, const Tan<double> &y) { x = y.v; });
+  s.status = t.status;
+  return s;
 }
 
 int check(clb_handle *h, const char *where)
@@ -172,8 +250,19 @@ int check(clb_handle *h, const char *where)
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, where);
   collect_profile(h);
+  SU2Sector *u = h->su2;
   State s;
-  e = cudaMemcpy(&s, h->su2->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  if (u->tangent) {
+    // the tangent form advances d_tst; its value part is the state the plain calls read
+    TState t;
+    e = cudaMemcpy(&t, u->d_tst, sizeof(t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+      s = values_of(t);
+      e = cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice);
+    }
+  } else {
+    e = cudaMemcpy(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost);
+  }
   if (e != cudaSuccess) return h->cuda_fail(e, where);
   if (s.status != 0) return h->fail(CLB_ENONFINITE, std::string(where) + ": a volume average or a(t) is not finite");
   return CLB_OK;
@@ -206,10 +295,23 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   return cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice) == cudaSuccess ? CLB_OK : CLB_ECUDA;
 }
 
+namespace {
+void free_tangent(SU2Sector *u)
+{
+  for (void *q : {u->df, u->dp, (void *)u->d_tst, (void *)u->d_tpart, (void *)u->d_tsums})
+    if (q) cudaFree(q);
+  u->df = u->dp = nullptr;
+  u->d_tst = nullptr;
+  u->d_tpart = u->d_tsums = nullptr;
+  u->tangent = false;
+}
+} // namespace
+
 __attribute__((visibility("hidden"))) void su2_destroy(clb_handle *h)
 {
   SU2Sector *u = h->su2;
   if (!u) return;
+  free_tangent(u);
   for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums, (void *)u->d_stage})
     if (q) cudaFree(q);
   delete u;
@@ -221,6 +323,7 @@ __attribute__((visibility("hidden"))) int su2_set_state(clb_handle *h, const dou
 {
   SU2Sector *u = h->su2;
   cudaError_t e = cudaStreamSynchronize(h->stream);
+  free_tangent(u); // a new state ends the tangent-linear form
   if (!u->fp32) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
@@ -420,6 +523,17 @@ __attribute__((visibility("hidden"))) int su2_measure(clb_handle *h, double e0, 
     m->friedmann[0] = std::fabs(1.0 - Etot / e0);
   }
   if ((e = cudaMemcpy(u->d_st, &s, sizeof(s), cudaMemcpyHostToDevice)) != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  if (u->tangent) {
+    // the same refresh of the cached values in the tangent form (tangents kept: the refreshed
+    // averages differ from the cached ones by the reduction order only)
+    TState t;
+    e = cudaMemcpy(&t, u->d_tst, sizeof(t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+      zip_state(t, s, [](Tan<double> &x, const double &y) { x.v = y; });
+      e = cudaMemcpy(u->d_tst, &t, sizeof(t), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_measure");
+  }
   for (int r = 0; r < 7; ++r) {
     const double a1 = v[14 + 4 * r], a2 = v[15 + 4 * r], b1 = v[16 + 4 * r], b2 = v[17 + 4 * r];
     const double r1 = a2 - a1 * a1, rr = b2 - b1 * b1;
@@ -458,6 +572,187 @@ __attribute__((visibility("hidden"))) const double *su2_component(clb_handle *h,
   const float *src = static_cast<const float *>(which == 0 ? u->f : u->p) + (size_t)comp * h->n3;
   k_convert<float, double><<<kSU2Blocks, 256, 0, h->stream>>>(src, u->d_stage, h->n3);
   return u->d_stage;
+}
+
+// ---- tangent-linear form -------------------------------------------------------------------------
+namespace {
+// n components of N^3 FP64 host values into device storage of either form (and back).
+cudaError_t upload_comps(clb_handle *h, void *dst, const double *src, int n)
+{
+  SU2Sector *u = h->su2;
+  cudaError_t e = cudaSuccess;
+  if (!u->fp32) {
+    if (src) return cudaMemcpyAsync(dst, src, n * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    return cudaMemsetAsync(dst, 0, n * h->n3 * sizeof(double), h->stream);
+  }
+  if (!src) return cudaMemsetAsync(dst, 0, n * h->n3 * sizeof(float), h->stream);
+  for (int c = 0; c < n && e == cudaSuccess; ++c) {
+    e = cudaMemcpyAsync(u->d_stage, src + (size_t)c * h->n3, h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      k_convert<double, float><<<kSU2Blocks, 256, 0, h->stream>>>(u->d_stage, static_cast<float *>(dst) + (size_t)c * h->n3, h->n3);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  }
+  return e;
+}
+cudaError_t download_comps(clb_handle *h, double *dst, const void *src, int n)
+{
+  SU2Sector *u = h->su2;
+  cudaError_t e = cudaSuccess;
+  if (!dst) return e;
+  if (!u->fp32) return cudaMemcpyAsync(dst, src, n * h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  for (int c = 0; c < n && e == cudaSuccess; ++c) {
+    k_convert<float, double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<const float *>(src) + (size_t)c * h->n3,
+                                                                 u->d_stage, h->n3);
+    e = cudaMemcpyAsync(dst + (size_t)c * h->n3, u->d_stage, h->n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  }
+  return e;
+}
+} // namespace
+
+// Starts the tangent-linear form: from here clb_initialize, clb_evolve and clb_sync also advance
+// the derivative of the state along couplings_dot (the six couplings' derivatives), starting from
+// the given start-state tangent (null: zero).
+__attribute__((visibility("hidden"))) int su2_tangent_begin(clb_handle *h, const double *couplings_dot, int32_t n,
+                                                            const double *fields_dot, const double *momenta_dot,
+                                                            const clb_scalefactor *sf_dot)
+{
+  SU2Sector *u = h->su2;
+  if (n < 0 || n > 6 || (n > 0 && !couplings_dot))
+    return h->fail(CLB_EINVAL, "clb_tangent_begin: up to 6 coupling derivatives");
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_tangent_begin");
+  free_tangent(u);
+  bool ok = cudaMalloc(&u->df, NF * h->n3 * u->esz) == cudaSuccess && cudaMalloc(&u->dp, NP * h->n3 * u->esz) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_tst, sizeof(TState)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_tpart, (size_t)kSU2Blocks * 2 * kRed * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->d_tsums, 2 * kRed * sizeof(double)) == cudaSuccess;
+  if (!ok) {
+    free_tangent(u);
+    return h->fail(CLB_ENOMEM, "clb_tangent_begin: tangent storage does not fit");
+  }
+  if ((e = upload_comps(h, u->df, fields_dot, NF)) != cudaSuccess || (e = upload_comps(h, u->dp, momenta_dot, NP)) != cudaSuccess) {
+    free_tangent(u);
+    return h->cuda_fail(e, "clb_tangent_begin");
+  }
+  State s;
+  if ((e = cudaMemcpy(&s, u->d_st, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+    free_tangent(u);
+    return h->cuda_fail(e, "clb_tangent_begin");
+  }
+  TState t{};
+  zip_state(t, s, [](Tan<double> &x, const double &y) { x = Tan<double>(y, 0.0); });
+  if (sf_dot) {
+    t.aI.d = sf_dot->aI;
+    t.aSI.d = sf_dot->aSI;
+    t.aIM.d = sf_dot->aIM;
+    t.aDotI.d = sf_dot->aDotI;
+    t.aDotSI.d = sf_dot->aDotSI;
+    t.aDotSIM.d = sf_dot->aDotSIM;
+  }
+  coefs(t, h->md.alpha);
+  t.status = s.status;
+  if ((e = cudaMemcpy(u->d_tst, &t, sizeof(t), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    free_tangent(u);
+    return h->cuda_fail(e, "clb_tangent_begin");
+  }
+  for (int k = 0; k < 6; ++k) u->tan_cd.v[k] = k < n ? couplings_dot[k] : 0.0;
+  u->tangent = true;
+  return CLB_OK;
+}
+
+__attribute__((visibility("hidden"))) int su2_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot,
+                                                                clb_scalefactor *sf_dot)
+{
+  SU2Sector *u = h->su2;
+  if (!u->tangent) return h->fail(CLB_ESTATE, "clb_tangent_get_state: call clb_tangent_begin first");
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = download_comps(h, fields_dot, u->df, NF);
+  if (e == cudaSuccess) e = download_comps(h, momenta_dot, u->dp, NP);
+  TState t;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&t, u->d_tst, sizeof(t), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_tangent_get_state");
+  if (sf_dot) {
+    sf_dot->aI = t.aI.d;
+    sf_dot->aSI = t.aSI.d;
+    sf_dot->aIM = t.aIM.d;
+    sf_dot->aDotI = t.aDotI.d;
+    sf_dot->aDotSI = t.aDotSI.d;
+    sf_dot->aDotSIM = t.aDotSIM.d;
+  }
+  return CLB_OK;
+}
+
+// The 11 energies (E_kin, E_grad of S, phi, Phi; E_el, E_mag of U(1), SU(2); V) at the current
+// state with their tangents, from one tangent reduction sweep.
+static int tangent_energies(clb_handle *h, const char *where, Tan<double> (&en)[11])
+{
+  SU2Sector *u = h->su2;
+  if (!u->tangent) return h->fail(CLB_ESTATE, std::string(where) + ": call clb_tangent_begin first");
+  if (h->cfg.evolver == CLB_LF && !h->synced) return h->fail(CLB_ESTATE, std::string(where) + ": call clb_sync first");
+  sweep(h, 0, true, true, Kick{});
+  CLB_LAUNCH(h, K_MEASURE, k_sum_partials<2 * kRed><<<1, 256, 0, h->stream>>>(u->d_tpart, kSU2Blocks, u->d_tsums));
+  double v[2 * kRed];
+  TState t;
+  cudaError_t e = cudaMemcpyAsync(v, u->d_tsums, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&t, u->d_tst, sizeof(t), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, where);
+  collect_profile(h);
+  using T = Tan<double>;
+  const double inv = u->prm.inv_n3;
+  auto av = [&](int k) { return T(v[k] * inv, v[kRed + k] * inv); };
+  for (int g = 0; g < 5; ++g) t.pi2[g] = av(g);
+  t.g2S = av(5);
+  t.g2C = av(6);
+  t.g2D = av(7);
+  t.b2A = av(8);
+  t.b2G = av(9);
+  t.potI = av(10);
+  const EnT<T> E = energies_of(t, u->prm);
+  const T all[11] = {E.ks, E.gs, E.kc, E.gc, E.kd, E.gd, E.ea, E.ba, E.eg, E.bg, t.potI};
+  for (int k = 0; k < 11; ++k) en[k] = all[k];
+  return CLB_OK;
+}
+
+__attribute__((visibility("hidden"))) int su2_tangent_energies(clb_handle *h, double *E, double *dE)
+{
+  Tan<double> en[11];
+  const int r = tangent_energies(h, "clb_tangent_energies", en);
+  if (r != CLB_OK) return r;
+  for (int k = 0; k < 11; ++k) {
+    if (E) E[k] = en[k].v;
+    if (dE) dE[k] = en[k].d;
+  }
+  return CLB_OK;
+}
+
+// O = sum_k w_k E_k / E_tot over the 11 energies and its derivative along the tangent.
+__attribute__((visibility("hidden"))) int su2_tangent_observable(clb_handle *h, const double *w, int32_t nw, double *obs,
+                                                                 double *dobs)
+{
+  if (nw < 0 || nw > 11 || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_tangent_observable: up to 11 energy weights");
+  using T = Tan<double>;
+  T en[11];
+  const int r = tangent_energies(h, "clb_tangent_observable", en);
+  if (r != CLB_OK) return r;
+  T Et(0.0), Ew(0.0);
+  for (int k = 0; k < 11; ++k) {
+    Et = Et + en[k];
+    if (k < nw) Ew = Ew + w[k] * en[k];
+  }
+  const T O = Ew / Et;
+  if (obs) *obs = O.v;
+  if (dobs) *dobs = O.d;
+  return CLB_OK;
+}
+
+__attribute__((visibility("hidden"))) int su2_tangent_end(clb_handle *h)
+{
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  free_tangent(h->su2);
+  return e == cudaSuccess ? CLB_OK : h->cuda_fail(e, "clb_tangent_end");
 }
 
 } // namespace clb

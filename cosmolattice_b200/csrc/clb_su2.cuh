@@ -28,6 +28,7 @@
 
 #include "clb_internal.cuh"
 #include "clb_scalar.cuh"
+#include "clb_tangent.cuh"
 
 namespace clb {
 namespace su2d {
@@ -46,67 +47,109 @@ struct Params {
 };
 
 // Scale factor, the cached averages of the five sectors (S, phi, Phi, A, SU(2)) and the sweep
-// coefficients derived from a and aS.
-struct State {
-  double aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
-  double pi2[5], pi2SI[5], pi2SIM[5];
-  double g2S, g2C, g2D, b2A, b2G, potI;
-  double kA, kB, kB2, kG; // pow(aI, 1+alpha), pow(aI, 3+alpha), /2, pow(aI, -1+alpha)
-  double p3, p1;          // pow(aSI, alpha-3), pow(aSI, alpha-1)
+// coefficients derived from a and aS; T = double, or Tan<double> in the tangent-linear form.
+template <class T> struct StateT {
+  T aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
+  T pi2[5], pi2SI[5], pi2SIM[5];
+  T g2S, g2C, g2D, b2A, b2G, potI;
+  T kA, kB, kB2, kG; // pow(aI, 1+alpha), pow(aI, 3+alpha), /2, pow(aI, -1+alpha)
+  T p3, p1;          // pow(aSI, alpha-3), pow(aSI, alpha-1)
   int32_t status, pad;
 };
+using State = StateT<double>;
+using TState = StateT<Tan<double>>;
+
+// Applies fn(x.m, y.m) to every floating member m of two scalar states.
+template <class A, class B, class Fn> inline void zip_state(StateT<A> &x, const StateT<B> &y, Fn fn)
+{
+  fn(x.aI, y.aI);
+  fn(x.aSI, y.aSI);
+  fn(x.aIM, y.aIM);
+  fn(x.aDotI, y.aDotI);
+  fn(x.aDotSI, y.aDotSI);
+  fn(x.aDotSIM, y.aDotSIM);
+  for (int g = 0; g < 5; ++g) {
+    fn(x.pi2[g], y.pi2[g]);
+    fn(x.pi2SI[g], y.pi2SI[g]);
+    fn(x.pi2SIM[g], y.pi2SIM[g]);
+  }
+  fn(x.g2S, y.g2S);
+  fn(x.g2C, y.g2C);
+  fn(x.g2D, y.g2D);
+  fn(x.b2A, y.b2A);
+  fn(x.b2G, y.b2G);
+  fn(x.potI, y.potI);
+  fn(x.kA, y.kA);
+  fn(x.kB, y.kB);
+  fn(x.kB2, y.kB2);
+  fn(x.kG, y.kG);
+  fn(x.p3, y.p3);
+  fn(x.p1, y.p1);
+}
 
 struct Kick {
   double h[2][5]; // kick factors of up to two kicks: S, phi, Phi, A, SU(2)
 };
 
-__device__ __host__ inline double ipw_h(double x, int n)
+template <class T> __device__ __host__ inline T ipw_h(T x, int n)
 {
   if (n < 0) return 1.0 / ipw_h(x, -n);
-  double r = x;
+  T r = x;
   for (int i = 1; i < n; ++i) r = r * x;
-  return n == 0 ? 1.0 : r;
+  return n == 0 ? T(1.0) : r;
 }
 
 // ---- tail: volume sums and the scale-factor update --------------------------------------------
-struct En {
-  double ks, gs, kc, gc, kd, gd, ea, ba, eg, bg;
+template <class T> struct EnT {
+  T ks, gs, kc, gc, kd, gd, ea, ba, eg, bg;
 };
-__device__ __host__ inline En energies_of(const State &s, const Params &p)
+using En = EnT<double>;
+template <class T> __device__ __host__ inline EnT<T> energies_of(const StateT<T> &s, const Params &p)
 {
-  const double a6 = ipw_h(s.aI, -6), a2 = ipw_h(s.aI, -2), e4 = 0.5 * p.rof2 * ipw_h(s.aI, -4);
-  return En{0.5 * s.pi2[0] * a6, 0.5 * s.g2S * a2, s.pi2[1] * a6, s.g2C * a2, s.pi2[2] * a6, s.g2D * a2,
-            e4 * s.pi2[3] * 1.0, e4 * s.b2A / 1.0, e4 * s.pi2[4], e4 * s.b2G};
+  const T a6 = ipw_h(s.aI, -6), a2 = ipw_h(s.aI, -2), e4 = 0.5 * p.rof2 * ipw_h(s.aI, -4);
+  return EnT<T>{0.5 * s.pi2[0] * a6, 0.5 * s.g2S * a2, s.pi2[1] * a6, s.g2C * a2, s.pi2[2] * a6, s.g2D * a2,
+                e4 * s.pi2[3] * 1.0, e4 * s.b2A / 1.0, e4 * s.pi2[4], e4 * s.b2G};
 }
-__device__ __forceinline__ double sf_kernel(const State &s, const Params &p)
+template <class T> __device__ __forceinline__ T sf_kernel(const StateT<T> &s, const Params &p)
 {
   const double al = p.alpha;
-  const En E = energies_of(s, p);
+  const EnT<T> E = energies_of(s, p);
   return pow(s.aI, 2 * al + 1) / 3.0 * p.fm2 *
          ((((al - 2) * ((E.ks + E.kc) + E.kd) + al * ((E.gs + E.gc) + E.gd)) +
            (al - 1) * ((1.0 * (E.ea + E.ba) + E.eg) + E.bg)) +
           (al + 1) * s.potI);
 }
-__device__ __host__ inline double rho_of(const State &s, const Params &p)
+template <class T> __device__ __host__ inline T rho_of(const StateT<T> &s, const Params &p)
 {
-  const En E = energies_of(s, p);
+  const EnT<T> E = energies_of(s, p);
   return ((((((((((E.ks + E.kc) + E.kd) + E.gs) + E.gc) + E.gd) + E.ea) + E.ba) + E.eg) + E.bg) + 0.0) + s.potI;
 }
 
-static __global__ void __launch_bounds__(256)
-    k_tail(const double *__restrict__ partials, TailOp op, State *__restrict__ stp, Params p)
+// One-thread tail.  T = double: partials [block][kRed]; T = Tan<double>: [block][2 kRed], the
+// values then their tangents.
+template <class T>
+__global__ void __launch_bounds__(256)
+    k_tail(const double *__restrict__ partials, TailOp op, StateT<T> *__restrict__ stp, Params p)
 {
-  __shared__ double smem[(256 / 32) * kRed];
-  double v[kRed];
-  for (int k = 0; k < kRed; ++k) v[k] = 0;
+  constexpr int W = TanTraits<T>::is ? 2 : 1;
+  __shared__ double smem[(256 / 32) * kRed * W];
+  double r[kRed * W];
+  for (int k = 0; k < kRed * W; ++k) r[k] = 0;
   if (op.nblocks > 0) {
     for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x)
-      for (int k = 0; k < kRed; ++k) v[k] += partials[(size_t)b * kRed + k];
-    block_reduce<kRed, 256>(v, smem);
+      for (int k = 0; k < kRed * W; ++k) r[k] += partials[(size_t)b * kRed * W + k];
+    block_reduce<kRed * W, 256>(r, smem);
   }
   if (threadIdx.x != 0) return;
-  State s = *stp;
-  for (int k = 0; k < kRed; ++k) v[k] *= p.inv_n3;
+  StateT<T> s = *stp;
+  T v[kRed];
+  for (int k = 0; k < kRed; ++k) {
+    if constexpr (TanTraits<T>::is)
+      v[k] = T(r[k], r[kRed + k]);
+    else
+      v[k] = r[k];
+    v[k] = v[k] * p.inv_n3;
+  }
   const double dt = p.dt;
   const uint32_t fl = op.flags;
   auto store_fields = [&]() {
@@ -122,12 +165,12 @@ static __global__ void __launch_bounds__(256)
     for (int g = 0; g < 5; ++g) s.pi2[g] = s.pi2SI[g] = v[g];
   }
   auto write_hist = [&]() {
-    double *r = op.hist + op.hist_row * kHistCols;
-    r[0] = s.aI;
-    r[1] = s.aDotI;
-    r[2] = s.pi2[2];
-    r[3] = s.g2D;
-    r[4] = s.potI;
+    double *h = op.hist + op.hist_row * kHistCols;
+    h[0] = val(s.aI);
+    h[1] = val(s.aDotI);
+    h[2] = val(s.pi2[2]);
+    h[3] = val(s.g2D);
+    h[4] = val(s.potI);
   };
   const bool hist = op.hist != nullptr && op.hist_row >= 0;
   if (fl & T_STORE_FIELDS) store_fields();
@@ -169,8 +212,8 @@ static __global__ void __launch_bounds__(256)
   s.kG = pow(s.aI, -1 + p.alpha);
   s.p3 = pow(s.aSI, p.alpha - 3);
   s.p1 = pow(s.aSI, p.alpha - 1);
-  bool ok = isfinite(s.aI) && isfinite(s.aDotI) && isfinite(s.aDotSI) && isfinite(s.potI);
-  for (int g = 0; g < 5; ++g) ok = ok && isfinite(s.pi2[g]);
+  bool ok = finite_(s.aI) && finite_(s.aDotI) && finite_(s.aDotSI) && finite_(s.potI);
+  for (int g = 0; g < 5; ++g) ok = ok && finite_(s.pi2[g]);
   if (!ok) s.status = 1;
   *stp = s;
 }

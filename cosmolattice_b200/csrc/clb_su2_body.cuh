@@ -61,13 +61,22 @@ template <class T> __device__ __forceinline__ T ipw(T x, int n)
 }
 
 // Read-only view of one state at one site (storage S, arithmetic T), with the oracle's names.
+// With T = Tan<S> a value reads as (f, df): the state and its tangent.
 template <class S, class T> struct Site {
   const S *f;
+  const S *df;
   const Params *a;
   size_t s;
   long long op[3], om[3];
-  T dx, gC, gD, gS;
-  __device__ __forceinline__ T F(int c, size_t t) const { return (T)f[(size_t)c * a->n3 + t]; }
+  T dx, gC, gD, gS, qG, qH, c4;
+  __device__ __forceinline__ T F(int c, size_t t) const
+  {
+    const size_t i = (size_t)c * a->n3 + t;
+    if constexpr (TanTraits<T>::is)
+      return T((typename TanTraits<T>::base)f[i], (typename TanTraits<T>::base)df[i]);
+    else
+      return (T)f[i];
+  }
   __device__ __forceinline__ Q4<T> link(int i, size_t t) const
   {
     const int b = 10 + 4 * i;
@@ -90,9 +99,9 @@ template <class S, class T> struct Site {
   __device__ __forceinline__ T potTerm(int k) const
   {
     const T nD = normD(s);
-    if (k == 0) return (T)a->c4 * ipw(nD, 4);
-    if (k == 1) return (T)a->qG * ipw(nD * F(0, s), 2);
-    return 2 * (T)a->qH * ipw(nD * normC(s), 2);
+    if (k == 0) return c4 * ipw(nD, 4);
+    if (k == 1) return qG * ipw(nD * F(0, s), 2);
+    return 2 * qH * ipw(nD * normC(s), 2);
   }
   __device__ __forceinline__ T pot() const { return (potTerm(0) + potTerm(1)) + potTerm(2); }
   __device__ __forceinline__ size_t pl(int i) const { return s + op[i]; }
@@ -123,12 +132,45 @@ template <class S, class T> __device__ __forceinline__ Site<S, T> make_site(cons
 {
   Site<S, T> v;
   v.f = f;
+  v.df = nullptr;
   v.a = &a;
   v.s = s;
   v.dx = (T)a.dx;
   v.gC = (T)a.gC;
   v.gD = (T)a.gD;
   v.gS = (T)a.gS;
+  v.qG = (T)a.qG;
+  v.qH = (T)a.qH;
+  v.c4 = (T)a.c4;
+  u1_offsets(a.N, s, v.op, v.om);
+  return v;
+}
+
+// Derivatives of the couplings along the tangent direction, in the model's order: qG, qH, gQ of
+// phi, gQ of Phi under U(1), gQ of Phi under SU(2), c4.
+struct CoupDot {
+  double v[6];
+};
+
+// Tangent-linear view: the state f with its tangent df, and the couplings with their tangents.
+template <class S>
+__device__ __forceinline__ Site<S, Tan<S>> make_site_tan(const S *f, const S *df, const Params &a, size_t s,
+                                                        const CoupDot &cd)
+{
+  using T = Tan<S>;
+  Site<S, T> v;
+  v.f = f;
+  v.df = df;
+  v.a = &a;
+  v.s = s;
+  v.dx = T(a.dx);
+  auto cp = [&](double x, int k) { return T((S)x, (S)cd.v[k]); };
+  v.qG = cp(a.qG, 0);
+  v.qH = cp(a.qH, 1);
+  v.gC = cp(a.gC, 2);
+  v.gD = cp(a.gD, 3);
+  v.gS = cp(a.gS, 4);
+  v.c4 = cp(a.c4, 5);
   u1_offsets(a.N, s, v.op, v.om);
   return v;
 }
@@ -171,12 +213,17 @@ template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S
   out[3] = ((plus.v.im + minus.v.im) - 6 * c.v.im) / dx2;
 }
 
-template <class S, class T> __device__ __forceinline__ void kernels(const Site<S, T> &v, const State &st, T K[NP])
+// Kick coefficients pow(aI, 1+alpha), pow(aI, 3+alpha), its half and pow(aI, -1+alpha).
+template <class T> struct Coef {
+  T A, B, B2, G;
+};
+
+template <class S, class T> __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP])
 {
   const Params &a = *v.a;
   const size_t s = v.s;
-  const T A = (T)st.kA, B = (T)st.kB, B2 = (T)st.kB2, G = (T)st.kG;
-  const T qG = (T)a.qG, qH = (T)a.qH, c4 = (T)a.c4, rfo2 = (T)a.rfo2;
+  const T A = C.A, B = C.B, B2 = C.B2, G = C.G;
+  const T qG = v.qG, qH = v.qH, c4 = v.c4, rfo2 = (T)a.rfo2;
   const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
   K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
   const C2<T> cl = covLapC(v);
@@ -326,7 +373,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : 
     for (int c = 0; c < NP; ++c) q[c] = p[(size_t)c * a.n3 + s];
     if (NK > 0) {
       S K[NP];
-      kernels(v, st, K);
+      kernels(v, Coef<S>{(S)st.kA, (S)st.kB, (S)st.kB2, (S)st.kG}, K);
       for (int k = 0; k < NK; ++k) {
         for (int c = 0; c < NP; ++c) q[c] = (S)((double)q[c] + kc.h[k][sector(c)] * (double)K[c]);
         if (RP) {
@@ -511,6 +558,166 @@ __global__ void __launch_bounds__(128)
   block_reduce<kMeas, 128>(acc, smem);
   if (threadIdx.x == 0)
     for (int k = 0; k < kMeas; ++k) partials[(size_t)blockIdx.x * kMeas + k] = acc[k];
+}
+
+// ---- tangent-linear form ---------------------------------------------------------------------------
+// The kernels below evolve (state, tangent) pairs: every expression is the plain kernel's, in
+// Tan arithmetic, so the state follows the plain evolution bitwise and the tangent is its exact
+// derivative along the coupling direction (and the tangent of the start state).
+
+// derivative of pi2s along the momentum tangent dq
+template <class R> __device__ __forceinline__ void pi2s_tan(const R *qs, const R *dqs, double out[5])
+{
+  double q[NP], d[NP];
+  for (int c = 0; c < NP; ++c) {
+    q[c] = (double)qs[c];
+    d[c] = (double)dqs[c];
+  }
+  out[0] = 2 * (q[0] * d[0]);
+  out[1] = 2 * (q[1] * d[1] + q[2] * d[2]);
+  out[2] = 2 * (((q[3] * d[3] + q[4] * d[4]) + q[5] * d[5]) + q[6] * d[6]);
+  out[3] = 2 * ((q[7] * d[7] + q[8] * d[8]) + q[9] * d[9]);
+  double acc = 0;
+  for (int c = 10; c < NP; ++c) acc += 8 * (q[c] * d[c]);
+  out[4] = acc;
+}
+
+// Tangent kick sweep: k_kick on (p, dp) with kernels and field sums in Tan<S>; partials
+// [block][2 kRed]: the kRed sums of k_kick, then their tangents.
+template <class S, int NK, bool RF, bool RP>
+__global__ void __launch_bounds__(128)
+    k_kick_tan(const S *__restrict__ f, const S *__restrict__ df, S *__restrict__ p, S *__restrict__ dp, Params a,
+               Kick kc, const TState *__restrict__ stp, CoupDot cd, double *__restrict__ partials)
+{
+  using T = Tan<S>;
+  __shared__ double smem[(128 / 32) * 2 * kRed];
+  const Coef<T> C{T(stp->kA), T(stp->kB), T(stp->kB2), T(stp->kG)};
+  double acc[2 * kRed];
+  for (int k = 0; k < 2 * kRed; ++k) acc[k] = 0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
+    const Site<S, T> v = make_site_tan<S>(f, df, a, s, cd);
+    S q[NP], dq[NP];
+    for (int c = 0; c < NP; ++c) {
+      q[c] = p[(size_t)c * a.n3 + s];
+      dq[c] = dp[(size_t)c * a.n3 + s];
+    }
+    auto add_pi = [&](int base) {
+      double t[5], td[5];
+      pi2s(q, t);
+      pi2s_tan(q, dq, td);
+      for (int g = 0; g < 5; ++g) {
+        acc[base + g] += t[g];
+        acc[kRed + base + g] += td[g];
+      }
+    };
+    if (NK > 0) {
+      T K[NP];
+      kernels(v, C, K);
+      for (int k = 0; k < NK; ++k) {
+        for (int c = 0; c < NP; ++c) {
+          const double h = kc.h[k][sector(c)];
+          q[c] = (S)((double)q[c] + h * (double)K[c].v);
+          dq[c] = (S)((double)dq[c] + h * (double)K[c].d);
+        }
+        if (RP) add_pi(k == 0 ? 0 : 11);
+      }
+      for (int c = 0; c < NP; ++c) {
+        p[(size_t)c * a.n3 + s] = q[c];
+        dp[(size_t)c * a.n3 + s] = dq[c];
+      }
+    } else if (RP) {
+      add_pi(0);
+    }
+    if (RF) {
+      const T r[6] = {sGrad2(v), cGrad2(v), dGrad2(v), aB2(v), gB2(v), v.pot()};
+      for (int k = 0; k < 6; ++k) {
+        acc[5 + k] += (double)r[k].v;
+        acc[kRed + 5 + k] += (double)r[k].d;
+      }
+    }
+  }
+  if (RF || RP) {
+    block_reduce<2 * kRed, 128>(acc, smem);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 2 * kRed; ++k) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
+  }
+}
+
+// exp of an algebra element with its tangent; the value is qexp's.  d(sin n / n)/dn =
+// (n cos n - sin n) / n^2 is taken from its Taylor series below n = 0.1, where the closed form
+// cancels.
+__device__ __forceinline__ Q4<Tan<double>> qexp_tan(Tan<double> p1, Tan<double> p2, Tan<double> p3)
+{
+  using T = Tan<double>;
+  const double n = sqrt(p1.v * p1.v + p2.v * p2.v + p3.v * p3.v);
+  if (n == 0) return Q4<T>{T(1.0), T(0.0, p1.d), T(0.0, p2.d), T(0.0, p3.d)};
+  const double sn = sin(n) / n, cn = cos(n);
+  const double dn = ((p1.v * p1.d + p2.v * p2.d) + p3.v * p3.d) / n;
+  double ds;
+  if (n < 0.1) {
+    const double x = n * n;
+    ds = -n * (1.0 / 3 - x * (1.0 / 30 - x * (1.0 / 840 - x / 45360)));
+  } else {
+    ds = (n * cn - sin(n)) / (n * n);
+  }
+  const double sd = ds * dn;
+  return Q4<T>{T(cn, -sin(n) * dn), T(sn * p1.v, sd * p1.v + sn * p1.d), T(sn * p2.v, sd * p2.v + sn * p2.d),
+               T(sn * p3.v, sd * p3.v + sn * p3.d)};
+}
+
+// Tangent drift: k_drift on (f, df) with the drift coefficients' tangents (through aS, and g_SU2 in
+// the link step).
+template <class S>
+__global__ void __launch_bounds__(256)
+    k_drift_tan(S *__restrict__ f, S *__restrict__ df, const S *__restrict__ p, const S *__restrict__ dp, Params a,
+                double w, int lf, const TState *__restrict__ stp, CoupDot cd)
+{
+  using T = Tan<double>;
+  const double dt = a.dt;
+  const T p3 = stp->p3, p1 = stp->p1;
+  const T gS(a.gS, cd.v[4]);
+  const T cC = lf ? p3 * dt : p3 * dt * w;
+  const T cA = lf ? p1 * dt : p1 * w * dt;
+  const T cG = lf ? p1 * a.dx * dt * gS : w * p1 * a.dx * dt * gS;
+  const double dtw = lf ? dt : dt * w;
+  const size_t n3 = a.n3;
+  auto ld = [](const S *x, const S *dx, size_t i) { return T((double)x[i], (double)dx[i]); };
+  auto put = [](S *x, S *dx, size_t i, T r) {
+    x[i] = (S)r.v;
+    dx[i] = (S)r.d;
+  };
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+    put(f, df, s, ld(f, df, s) + p3 * (dtw * ld(p, dp, s)));
+    for (int c = 1; c < 7; ++c) put(f, df, c * n3 + s, ld(f, df, c * n3 + s) + cC * ld(p, dp, c * n3 + s));
+    for (int i = 0; i < 3; ++i)
+      put(f, df, (7 + i) * n3 + s, ld(f, df, (7 + i) * n3 + s) + cA * ld(p, dp, (7 + i) * n3 + s) * 1.0);
+    for (int i = 0; i < 3; ++i) {
+      const size_t pb = (size_t)(10 + 3 * i) * n3 + s, fb = (size_t)(10 + 4 * i) * n3 + s;
+      const Q4<T> E = qexp_tan(cG * ld(p, dp, pb), cG * ld(p, dp, pb + n3), cG * ld(p, dp, pb + 2 * n3));
+      const Q4<T> U = qmul(E, Q4<T>{ld(f, df, fb), ld(f, df, fb + n3), ld(f, df, fb + 2 * n3), ld(f, df, fb + 3 * n3)});
+      put(f, df, fb, U.w);
+      put(f, df, fb + n3, U.x);
+      put(f, df, fb + 2 * n3, U.y);
+      put(f, df, fb + 3 * n3, U.z);
+    }
+  }
+}
+
+// Tangent re-unitarisation (FP32 form): U <- U / |U| on (f, df).
+template <class S> __global__ void __launch_bounds__(256) k_unitarize_tan(S *__restrict__ f, S *__restrict__ df, size_t n3)
+{
+  using T = Tan<double>;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < 3 * n3; s += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = s / n3, t = s - i * n3, fb = (size_t)(10 + 4 * i) * n3 + t;
+    T q[4];
+    for (int c = 0; c < 4; ++c) q[c] = T((double)f[fb + c * n3], (double)df[fb + c * n3]);
+    const T r = 1.0 / sqrt(((q[0] * q[0] + q[1] * q[1]) + q[2] * q[2]) + q[3] * q[3]);
+    for (int c = 0; c < 4; ++c) {
+      const T u = q[c] * r;
+      f[fb + c * n3] = (S)u.v;
+      df[fb + c * n3] = (S)u.d;
+    }
+  }
 }
 
 } // namespace su2d

@@ -305,6 +305,41 @@ def su2u1_initial_state(model: Model, rp: RunParameters):
     return fields, momenta, aI, aDot
 
 
+def su2u1_initial_state_tangent(model: Model, rp: RunParameters, param: str, state=None):
+    """(fields_dot, momenta_dot, couplings_dot) of su2u1_initial_state along param: "gSU2" (the
+    SU(2) coupling: only the SU(2) momenta, solved from the doublet charge, depend on it) or "gU1"
+    (the U(1) coupling: only the U(1) momenta).  Both enter linearly through the Gauss solves.
+    state: (fields, momenta) of su2u1_initial_state, if already made."""
+    fields, momenta = state if state is not None else su2u1_initial_state(model, rp)[:2]
+    df = np.zeros_like(fields)
+    dp = np.zeros_like(momenta)
+    cd = np.zeros(6)
+    r2 = (model.fStar / model.omegaStar) ** 2
+    u = fields[3] + 1j * fields[4]
+    v = fields[5] + 1j * fields[6]
+    pu = momenta[3] + 1j * momenta[4]
+    pv = momenta[5] + 1j * momenta[6]
+    if param == "gSU2":
+        cd[4] = model.Q_S
+        isig = [(1j * v, 1j * u), (v, -u), (1j * u, -1j * v)]
+        for b in range(3):
+            a, c = isig[b]
+            rho = r2 / 2 * (model.Q_S * np.real(np.conj(a) * pu + np.conj(c) * pv))
+            pa = gauss_solve_u1(rp, rho / rp.dx)
+            for i in range(3):
+                dp[10 + 3 * i + b] = pa[i]
+    elif param == "gU1":
+        cd[2], cd[3] = model.Q_C, model.Q_D
+        rho = 2.0 / rp.dx * r2 * (model.Q_C * (momenta[1] * fields[2] - momenta[2] * fields[1])
+                                  + model.Q_D * np.imag(np.conj(pu) * u + np.conj(pv) * v))
+        pa = gauss_solve_u1(rp, rho)
+        for i in range(3):
+            dp[7 + i] = pa[i]
+    else:
+        raise ValueError(f"unknown parameter {param!r}")
+    return df, dp, cd
+
+
 def initial_state(model: Model, rp: RunParameters):
     """Initial state of any supported model (ModelInitializer::initialize, modelinitializer.h:47-81)."""
     if getattr(model, "NSU2", 0):

@@ -135,6 +135,52 @@ class Lattice:
             "dO_daDotI": g.dO_dscalefactor[1],
         }
 
+    def tangent_begin(self, couplings_dot, fields_dot=None, momenta_dot=None,
+                      sf_dot: Optional[Dict[str, float]] = None) -> None:
+        """clb_tangent_begin: from now on evolve the derivative of the state along the coupling
+        direction couplings_dot (model.couplings() order) alongside the state."""
+        n3 = self.rp.N ** 3
+        cd = np.ascontiguousarray(couplings_dot, dtype=np.float64)
+        f = p = None
+        if fields_dot is not None:
+            f = np.ascontiguousarray(fields_dot, dtype=np.float64)
+            if f.size != self.n_field_components * n3:
+                raise ValueError("fields_dot does not match the model's component count")
+        if momenta_dot is not None:
+            p = np.ascontiguousarray(momenta_dot, dtype=np.float64)
+            if p.size != self.n_momentum_components * n3:
+                raise ValueError("momenta_dot does not match the model's component count")
+        s = None
+        if sf_dot is not None:
+            s = _capi.ScaleFactor(**{k: float(sf_dot.get(k, 0.0)) for k in ("aI", "aSI", "aIM", "aDotI", "aDotSI", "aDotSIM")})
+        self._check(self.lib.clb_tangent_begin(self.h, _dp(cd), int(cd.size), _dp(f) if f is not None else None,
+                                               _dp(p) if p is not None else None, C.byref(s) if s is not None else None))
+
+    def tangent_get_state(self):
+        """(fields_dot, momenta_dot, scale-factor tangents) of the tangent-linear form."""
+        n3 = self.rp.N ** 3
+        f = np.empty(self.n_field_components * n3)
+        p = np.empty(self.n_momentum_components * n3)
+        sf = _capi.ScaleFactor()
+        self._check(self.lib.clb_tangent_get_state(self.h, _dp(f), _dp(p), C.byref(sf)))
+        return f, p, {k: getattr(sf, k) for k, _ in _capi.ScaleFactor._fields_}
+
+    def tangent_observable(self, weights):
+        """(O, dO/dcoupling) for O = sum_k w_k E_k / E_tot at the current state."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        o, do = C.c_double(), C.c_double()
+        self._check(self.lib.clb_tangent_observable(self.h, _dp(w), int(w.size), C.byref(o), C.byref(do)))
+        return o.value, do.value
+
+    def tangent_energies(self):
+        """(E, dE): the 11 energies of tangent_observable and their derivatives."""
+        e, de = np.empty(11), np.empty(11)
+        self._check(self.lib.clb_tangent_energies(self.h, _dp(e), _dp(de)))
+        return e, de
+
+    def tangent_end(self) -> None:
+        self._check(self.lib.clb_tangent_end(self.h))
+
     def history(self) -> np.ndarray:
         """Per-step rows (a, aDot, <pi^2>, <grad^2>, <V>) of the last evolve call."""
         n = C.c_int64()

@@ -307,6 +307,10 @@ class lphi4SU2U1(Model):
         d_su2 = CouplingsManager([[True]])
         d_su2.set_effective_charges(par.get_floats("SU2DoubletSU2_charges", 1, [1.0]), gSU2)
         self.gQ_C, self.gQ_D, self.gQ_S = cs_u1(0, 0), d_u1(0, 0), d_su2(0, 0)
+        # charges: d(gQ)/d(g) of the three effective couplings
+        self.Q_C = par.get_floats("CSU1_charges", 1, [1.0])[0]
+        self.Q_D = par.get_floats("SU2DoubletU1_charges", 1, [1.0])[0]
+        self.Q_S = par.get_floats("SU2DoubletSU2_charges", 1, [1.0])[0]
         self.alpha = 1.0
         self.fStar = nD
         self.omegaStar = math.sqrt(self.lam) * nD

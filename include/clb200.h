@@ -235,6 +235,31 @@ int clb_forward(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, const d
                 double *observable);
 int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *grad);
 
+/* ---- tangent-linear (forward-mode) form ---------------------------------------------------------
+ * No counterpart in the reference.  Replaces a caller's central-difference pair of runs around
+ * Evolver::evolve (evolvers/evolver.h:102-127) and EnergiesMeasurer::measure
+ * (measurements/energiesmeasurer.h:45-122) for the derivative with respect to one coupling.
+ *
+ * clb_tangent_begin sets the direction: the derivatives of the couplings (clb_model_desc order;
+ * lphi4SU2U1: qG, qH, gQ of phi, gQ of Phi under U(1), gQ of Phi under SU(2), c4; missing ones
+ * 0), and the tangent of the current state along it (same layouts as clb_set_state; NULL: zero).
+ * d/d g_SU2 is couplings_dot = {0, 0, 0, 0, Q_SU2}; d/d g_U1 is {0, 0, Q_phi, Q_Phi}.  From then on
+ * clb_initialize, clb_evolve and clb_sync advance the state exactly as without it and its tangent
+ * alongside (the scale factor's too, through the self-consistent expansion), in one pass with no
+ * checkpoints; clb_measure refreshes the cached averages of both.  clb_tangent_observable returns
+ *     O = sum_k w_k E_k / E_tot,  E_k = E_kin, E_grad of S, phi, Phi; E_el, E_mag of U(1) and SU(2); V
+ * (n_weights <= 11) and its derivative along the direction at the current state.  clb_set_state or clb_tangent_end
+ * ends the form.  lphi4SU2U1 only (other models: CLB_EUNSUPPORTED); device memory: one more
+ * state. */
+int clb_tangent_begin(clb_handle *h, const double *couplings_dot, int32_t n_couplings, const double *fields_dot,
+                      const double *momenta_dot, const clb_scalefactor *sf_dot);
+int clb_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot, clb_scalefactor *sf_dot);
+int clb_tangent_observable(clb_handle *h, const double *weights, int32_t n_weights, double *observable,
+                           double *d_observable);
+/* The 11 energies E_k of clb_tangent_observable and their derivatives (either array may be NULL). */
+int clb_tangent_energies(clb_handle *h, double *energies, double *d_energies);
+int clb_tangent_end(clb_handle *h);
+
 /* ---- batched ensemble ----------------------------------------------------------------------------
  * No counterpart in the reference (one lattice per process, source/cosmolattice.cpp:134-201).  Many
  * independent one-field lphi4 lattices (model kind CLB_MODEL_LPHI4, n_scalars 1) advance together:
