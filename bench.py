@@ -453,9 +453,11 @@ def main_batched(args):
         ms = bt.last_evolve_ms()
         launches = bt.kernel_launches() - l0
         meas = [bt.measure(i) for i in range(len(cases))]
+        tuning[precision] = bt.tuning()
         bt.close()
         return ms, launches, meas, clk.summary()
 
+    tuning = {}
     ms32, launches, m32, clocks = batch_run("fp32", steps)
     ms64, _, m64, _ = batch_run("fp64", steps)
     # one at a time through the single-lattice handle (FP32 split), seq_steps each
@@ -489,6 +491,7 @@ def main_batched(args):
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes_per_step": sites * 16},
         "fp64_batch": {"value": sites * steps / (ms64 * 1e-3), "ms_per_step": ms64 / steps},
+        "sweep_autotuner": tuning,
         "one_at_a_time": {"value": seq_value, "steps": args.seq_steps, "path": "single-lattice handle, FP32 split",
                           "batched_speedup": value / seq_value},
         "fp32_vs_fp64": {"friedmann_abs_diff_max": max(fr), "a_rel_diff_max": max(ar), "energy_rel_diff_max": max(er)},

@@ -103,6 +103,19 @@ class ClbError(RuntimeError):
         self.code = code
 
 
+class BatchTuning(C.Structure):
+    """clb_batch_tuning."""
+
+    _fields_ = [
+        ("tile_z", C.c_int32),
+        ("tile_y", C.c_int32),
+        ("planes_x", C.c_int32),
+        ("candidates", C.c_int32),
+        ("ms_per_sweep", C.c_double),
+        ("ms_default", C.c_double),
+    ]
+
+
 class AdjointGrad(C.Structure):
     """clb_adjoint_grad."""
 
@@ -162,6 +175,9 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_batch_measure": (C.c_int, [H, C.c_int32, C.c_double, C.POINTER(Measurement)]),
             "clb_batch_last_evolve_ms": (C.c_int, [H, dp]),
             "clb_batch_kernel_launches": (C.c_int, [H, C.POINTER(C.c_int64)]),
+            "clb_batch_autotune": (C.c_int, [H, C.c_int32, C.POINTER(BatchTuning)]),
+            "clb_batch_set_tuning": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32]),
+            "clb_batch_get_tuning": (C.c_int, [H, C.POINTER(BatchTuning)]),
         }
         for name, (res, args) in more.items():
             fn = getattr(lib, name)
@@ -223,5 +239,8 @@ EXPORTED = [
     "clb_batch_measure",
     "clb_batch_last_evolve_ms",
     "clb_batch_kernel_launches",
+    "clb_batch_autotune",
+    "clb_batch_set_tuning",
+    "clb_batch_get_tuning",
     "clb_scalar_averages_noalloc",
 ]

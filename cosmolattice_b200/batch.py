@@ -93,3 +93,21 @@ class LatticeBatch:
         v = C.c_int64()
         self._check(self.lib.clb_batch_kernel_launches(self.h, C.byref(v)))
         return v.value
+
+    @staticmethod
+    def _tuning_dict(t) -> Dict[str, object]:
+        return {k: getattr(t, k) for k, _ in _capi.BatchTuning._fields_}
+
+    def autotune(self, reps: int = 5) -> Dict[str, object]:
+        """clb_batch_autotune: time every sweep configuration on this ensemble and keep the fastest."""
+        t = _capi.BatchTuning()
+        self._check(self.lib.clb_batch_autotune(self.h, int(reps), C.byref(t)))
+        return self._tuning_dict(t)
+
+    def set_tuning(self, tile_z: int, tile_y: int, planes_x: int) -> None:
+        self._check(self.lib.clb_batch_set_tuning(self.h, int(tile_z), int(tile_y), int(planes_x)))
+
+    def tuning(self) -> Dict[str, object]:
+        t = _capi.BatchTuning()
+        self._check(self.lib.clb_batch_get_tuning(self.h, C.byref(t)))
+        return self._tuning_dict(t)

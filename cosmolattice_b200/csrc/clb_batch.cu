@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -24,7 +25,19 @@ namespace {
 thread_local std::string g_berr;
 constexpr int kPackBlocks = 148 * 8;
 constexpr int kMeasBlocks = 148 * 4;
-constexpr int kLX = 32; // x planes per sweep block
+
+// Sweep configurations the autotuner chooses from: (z, y) tile shapes compiled for, and the
+// x-run lengths (planes per block, capped at the member's N).
+struct TileShape {
+  int bz, by;
+};
+constexpr TileShape kTiles[] = {{32, 4}, {32, 8}, {32, 16}, {64, 4}};
+constexpr int kNTiles = sizeof(kTiles) / sizeof(kTiles[0]);
+constexpr int kRuns[] = {8, 16, 32, 64, 1024};
+constexpr int kDefaultTile = 1, kDefaultRun = 32; // 32 x 8 tiles, 32-plane runs
+
+// Tuned configurations by ensemble (precision, device and sorted member sizes), for the process.
+std::map<std::string, std::pair<int, int>> g_tuned;
 
 } // namespace
 
@@ -35,6 +48,10 @@ struct clb_batch {
   std::vector<BatchLat> lat;       // host copy of the member descriptors
   std::vector<int> blk_lat;
   int total_blocks = 0;
+  int tile = kDefaultTile, run = kDefaultRun; // sweep configuration (kTiles index, x-run)
+  bool tuned = false;                         // set by the autotuner or the caller
+  clb_batch_tuning tuning{};
+  size_t blk_cap = 0, part_cap = 0;           // d_blk, d_part capacities (elements)
   long long total_elems = 0;
   bool fp32 = false;
   size_t esz = 8;
@@ -72,14 +89,15 @@ struct clb_batch {
 
 namespace {
 
-template <class R> void sweep_launch(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2)
+template <int BZ, int BY, class R>
+void sweep_tile(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2)
 {
   const R *fin = static_cast<const R *>(b->f[b->cf]), *pin = static_cast<const R *>(b->p[b->cf]);
   R *fout = static_cast<R *>(b->f[drift ? b->cf ^ 1 : b->cf]), *pout = static_cast<R *>(b->p[drift ? b->cf ^ 1 : b->cf]);
-  const dim3 grid(b->total_blocks), block(kBZ, kBY);
+  const dim3 grid(b->total_blocks), block(BZ, BY);
 #define CLB_BS(D, K, RD)                                                                                               \
-  k_batch_sweep<R, D, K, RD><<<grid, block, 0, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk, b->d_st, b->rs, \
-                                                              dtw, h1, h2, b->d_part)
+  k_batch_sweep<BZ, BY, R, D, K, RD><<<grid, block, 0, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk, b->d_st, \
+                                                                      b->rs, dtw, h1, h2, b->d_part)
   if (drift && kick && red)
     CLB_BS(true, true, 3);
   else if (drift && kick)
@@ -89,17 +107,137 @@ template <class R> void sweep_launch(clb_batch *b, bool drift, bool kick, int re
   else
     CLB_BS(false, false, 3);
 #undef CLB_BS
+}
+
+// One sweep with the current configuration; advance = false leaves the buffer parity and the
+// reference slot as they are (the autotuner's timing sweeps write only the idle buffers).
+template <class R>
+void sweep_launch(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2, bool advance = true)
+{
+  switch (b->tile) {
+  case 0: sweep_tile<32, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 1: sweep_tile<32, 8, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 2: sweep_tile<32, 16, R>(b, drift, kick, red, dtw, h1, h2); break;
+  default: sweep_tile<64, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  }
   ++b->launches;
+  if (!advance) return;
   if (drift) b->cf ^= 1;
   if (sizeof(R) == 4 && (drift || kick)) b->rs ^= 1;
 }
 
-void sweep(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2)
+// Member sweep grids for (tile, run): per-member tile counts, block ranges and the block ->
+// member table, uploaded to the device (buffers grown when needed).
+cudaError_t layout(clb_batch *b, int tile, int run)
+{
+  const TileShape t = kTiles[tile];
+  int blocks = 0;
+  b->blk_lat.clear();
+  for (int i = 0; i < b->n; ++i) {
+    BatchLat &L = b->lat[(size_t)i];
+    L.gx = (L.N + t.bz - 1) / t.bz;
+    L.gy = (L.N + t.by - 1) / t.by;
+    L.LX = std::min(L.N, run);
+    L.gz = (L.N + L.LX - 1) / L.LX;
+    L.first_block = blocks;
+    L.nblocks = L.gx * L.gy * L.gz;
+    blocks += L.nblocks;
+    for (int k = 0; k < L.nblocks; ++k) b->blk_lat.push_back(i);
+  }
+  cudaError_t e = cudaSuccess;
+  if ((size_t)blocks > b->blk_cap) {
+    if (b->d_blk) cudaFree(b->d_blk);
+    b->d_blk = nullptr;
+    e = cudaMalloc(&b->d_blk, (size_t)blocks * sizeof(int));
+    if (e != cudaSuccess) return e;
+    b->blk_cap = (size_t)blocks;
+  }
+  const size_t part = (size_t)std::max(blocks * kRedSlots, kMeasBlocks * 7);
+  if (part > b->part_cap) {
+    if (b->d_part) cudaFree(b->d_part);
+    b->d_part = nullptr;
+    e = cudaMalloc(&b->d_part, part * sizeof(double));
+    if (e != cudaSuccess) return e;
+    b->part_cap = part;
+  }
+  e = cudaMemcpyAsync(b->d_lat, b->lat.data(), (size_t)b->n * sizeof(BatchLat), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_blk, b->blk_lat.data(), (size_t)blocks * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return e;
+  b->total_blocks = blocks;
+  b->tile = tile;
+  b->run = run;
+  return cudaSuccess;
+}
+
+// Drops the captured graphs (they hold the old grid).
+void drop_graphs(clb_batch *b)
+{
+  for (auto &g : b->graphs) cudaGraphExecDestroy(g.second.exec);
+  b->graphs.clear();
+}
+
+std::string tune_key(const clb_batch *b)
+{
+  std::vector<int> ns;
+  for (const BatchLat &L : b->lat) ns.push_back(L.N);
+  std::sort(ns.begin(), ns.end());
+  std::string k = std::to_string(b->cfg.device) + (b->fp32 ? "/fp32/" : "/fp64/");
+  for (int n : ns) k += std::to_string(n) + ",";
+  return k;
+}
+
+void sweep(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2, bool advance = true)
 {
   if (b->fp32)
-    sweep_launch<float>(b, drift, kick, red, dtw, h1, h2);
+    sweep_launch<float>(b, drift, kick, red, dtw, h1, h2, advance);
   else
-    sweep_launch<double>(b, drift, kick, red, dtw, h1, h2);
+    sweep_launch<double>(b, drift, kick, red, dtw, h1, h2, advance);
+}
+
+// Autotuner: times the fused drift + two-kick + reduction sweep (the one every stage runs) of the
+// whole ensemble for every (tile, run) candidate, `reps` launches each after a warm-up launch, on
+// the handle's stream with CUDA events, and keeps the fastest.  The timing sweeps read the current
+// state and write only the idle state buffers, the next reference slot and the partials, so the
+// state is unchanged.
+int autotune(clb_batch *b, int reps)
+{
+  const double dt = b->cfg.dt, w = b->ws[0];
+  cudaError_t e = cudaSuccess;
+  double best = 1e300, def = 0;
+  int bt = kDefaultTile, br = kDefaultRun, count = 0;
+  int maxN = 0;
+  for (const BatchLat &L : b->lat) maxN = std::max(maxN, L.N);
+  for (int t = 0; t < kNTiles && e == cudaSuccess; ++t) {
+    for (int run : kRuns) {
+      if (run != kRuns[0] && run / 2 >= maxN) continue; // the same grids as run / 2
+      if ((e = layout(b, t, run)) != cudaSuccess) break;
+      sweep(b, true, true, 3, dt * w, w * dt / 2, w * dt / 2, false);
+      cudaEventRecord(b->ev[0], b->stream);
+      for (int r = 0; r < reps; ++r) sweep(b, true, true, 3, dt * w, w * dt / 2, w * dt / 2, false);
+      cudaEventRecord(b->ev[1], b->stream);
+      if ((e = cudaEventSynchronize(b->ev[1])) != cudaSuccess) break;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+      const double per = ms / reps;
+      ++count;
+      if (t == kDefaultTile && run == kDefaultRun) def = per;
+      if (per < best) {
+        best = per;
+        bt = t;
+        br = run;
+      }
+    }
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = layout(b, bt, br);
+  if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_autotune");
+  drop_graphs(b);
+  b->tuned = true;
+  b->tuning = clb_batch_tuning{kTiles[bt].bz, kTiles[bt].by, br, count, best, def};
+  g_tuned[tune_key(b)] = {bt, br};
+  return CLB_OK;
 }
 
 void btail(clb_batch *b, uint32_t flags, bool reduced, double w = 0, double w2 = 0)
@@ -226,17 +364,10 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
   b->esz = b->fp32 ? 4 : 8;
   b->has_state.assign((size_t)n, 0);
   long long off = 0;
-  int blocks = 0;
   for (int i = 0; i < n; ++i) {
     BatchLat L{};
     const int N = cfgs[i].N;
     L.N = N;
-    L.gx = (N + kBZ - 1) / kBZ;
-    L.gy = (N + kBY - 1) / kBY;
-    L.LX = std::min(N, kLX);
-    L.gz = (N + L.LX - 1) / L.LX;
-    L.first_block = blocks;
-    L.nblocks = L.gx * L.gy * L.gz;
     L.off = off;
     L.inv_dx2 = 1.0 / (cfgs[i].dx * cfgs[i].dx);
     L.c0 = mds[i].couplings[0];
@@ -245,11 +376,8 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
     L.sp = SFParams{mds[i].alpha, fm * fm, c0.dt, 1.0 / ((double)N * N * N)};
     const long long n3 = (long long)N * N * N;
     off += (n3 + 31) / 32 * 32; // 128-byte aligned members
-    blocks += L.nblocks;
     b->lat.push_back(L);
-    for (int k = 0; k < L.nblocks; ++k) b->blk_lat.push_back(i);
   }
-  b->total_blocks = blocks;
   b->total_elems = off;
   long long max_n3 = 0;
   for (auto &L : b->lat) max_n3 = std::max(max_n3, (long long)L.N * L.N * L.N);
@@ -260,14 +388,20 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
     ok = cudaMalloc(&b->f[i], bytes) == cudaSuccess && cudaMalloc(&b->p[i], bytes) == cudaSuccess &&
          cudaMemset(b->f[i], 0, bytes) == cudaSuccess && cudaMemset(b->p[i], 0, bytes) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_lat, (size_t)n * sizeof(BatchLat)) == cudaSuccess;
-  ok = ok && cudaMalloc(&b->d_blk, (size_t)blocks * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_st, (size_t)n * sizeof(DevState)) == cudaSuccess;
-  ok = ok && cudaMalloc(&b->d_part, (size_t)std::max(blocks * kRedSlots, kMeasBlocks * 7) * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_sums, 8 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_stage, b->stage_n * sizeof(double)) == cudaSuccess;
   ok = ok && cudaEventCreate(&b->ev[0]) == cudaSuccess && cudaEventCreate(&b->ev[1]) == cudaSuccess;
-  ok = ok && cudaMemcpy(b->d_lat, b->lat.data(), (size_t)n * sizeof(BatchLat), cudaMemcpyHostToDevice) == cudaSuccess;
-  ok = ok && cudaMemcpy(b->d_blk, b->blk_lat.data(), (size_t)blocks * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) {
+    // a configuration tuned earlier in this process for the same ensemble, else the default
+    auto it = g_tuned.find(tune_key(b));
+    const bool cached = it != g_tuned.end();
+    ok = layout(b, cached ? it->second.first : kDefaultTile, cached ? it->second.second : kDefaultRun) == cudaSuccess;
+    if (cached) {
+      b->tuned = true;
+      b->tuning = clb_batch_tuning{kTiles[b->tile].bz, kTiles[b->tile].by, b->run, 0, 0.0, 0.0};
+    }
+  }
   if (ok) {
     std::vector<DevState> s((size_t)n);
     for (auto &x : s) {
@@ -393,6 +527,17 @@ int clb_batch_evolve(clb_batch *b, int64_t nsteps)
   if (!b->initialized) return b->fail(CLB_ESTATE, "clb_batch_evolve: call clb_batch_initialize first");
   if (nsteps < 0) return b->fail(CLB_EINVAL, "clb_batch_evolve: negative step count");
   if (nsteps == 0) return CLB_OK;
+  if (!b->tuned) {
+    // first evolve: choose the sweep configuration (CLB_BATCH_AUTOTUNE=0 keeps the default)
+    const char *env = std::getenv("CLB_BATCH_AUTOTUNE");
+    if (!(env && env[0] == '0')) {
+      const int r = autotune(b, 5);
+      if (r != CLB_OK) return r;
+    } else {
+      b->tuned = true;
+      b->tuning = clb_batch_tuning{kTiles[b->tile].bz, kTiles[b->tile].by, b->run, 0, 0.0, 0.0};
+    }
+  }
   const auto key = std::make_tuple(nsteps, b->cf, b->rs);
   auto it = b->graphs.find(key);
   const int cf0 = b->cf, rs0 = b->rs;
@@ -513,6 +658,47 @@ int clb_batch_measure(clb_batch *b, int32_t i, double e0, clb_measurement *m)
   m->aI = s.aI;
   m->aDotI = s.aDotI;
   m->hubble = s.aDotI / s.aI;
+  return CLB_OK;
+}
+
+
+int clb_batch_autotune(clb_batch *b, int32_t reps, clb_batch_tuning *out)
+{
+  if (!b) return CLB_EINVAL;
+  if (reps < 1 || reps > 1000) return b->fail(CLB_EINVAL, "clb_batch_autotune: reps in [1, 1000]");
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_autotune");
+  const int r = autotune(b, reps);
+  if (r == CLB_OK && out) *out = b->tuning;
+  return r;
+}
+
+int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t planes_x)
+{
+  if (!b) return CLB_EINVAL;
+  int t = -1;
+  for (int k = 0; k < kNTiles; ++k)
+    if (kTiles[k].bz == tile_z && kTiles[k].by == tile_y) t = k;
+  if (t < 0) return b->fail(CLB_EINVAL, "clb_batch_set_tuning: tile must be 32x4, 32x8, 32x16 or 64x4");
+  if (planes_x < 1) return b->fail(CLB_EINVAL, "clb_batch_set_tuning: planes_x must be >= 1");
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = layout(b, t, planes_x);
+  if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_set_tuning");
+  drop_graphs(b);
+  b->tuned = true;
+  b->tuning = clb_batch_tuning{tile_z, tile_y, planes_x, 0, 0.0, 0.0};
+  return CLB_OK;
+}
+
+int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out)
+{
+  if (!b || !out) return CLB_EINVAL;
+  *out = b->tuning;
+  if (!b->tuned) {
+    out->tile_z = kTiles[b->tile].bz;
+    out->tile_y = kTiles[b->tile].by;
+    out->planes_x = b->run;
+  }
   return CLB_OK;
 }
 

@@ -19,31 +19,31 @@
 namespace clb {
 
 struct BatchLat {
-  int N, gx, gy, gz, LX; // sweep grid of this member: (z, y) tiles of 32 x 8, x runs of LX planes
+  int N, gx, gy, gz, LX; // sweep grid of this member: (z, y) tiles of BZ x BY, x runs of LX planes
   int first_block, nblocks;
   long long off;         // element offset of the member's arrays
   double inv_dx2, c0, c0q;
   SFParams sp;
 };
 
-constexpr int kBZ = 32, kBY = 8;
-
-// DRIFT / KICK / RED as in k_sweep; one block = one (z, y) tile of one member, marching over LX
-// x-planes.  fin/pin are never written; fout/pout alias them only without DRIFT.
-// Four resident 256-thread blocks per SM (64 registers): 1.43x over the unbounded build.
+// DRIFT / KICK / RED as in k_sweep; one block = one BZ x BY (z, y) tile of one member, marching
+// over LX x-planes (tile shape and LX are chosen by the batch autotuner).  fin/pin are never
+// written; fout/pout alias them only without DRIFT.
+// Register budget: that of four resident 256-thread blocks per SM (64 registers), whatever the
+// tile: 1.43x over the unbounded build at 32 x 8.
 #ifndef CLB_BATCH_MINB
 #define CLB_BATCH_MINB 4
 #endif
-template <class R, bool DRIFT, bool KICK, int RED>
-__global__ void __launch_bounds__(kBZ *kBY, CLB_BATCH_MINB)
+template <int BZ, int BY, class R, bool DRIFT, bool KICK, int RED>
+__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY))
     k_batch_sweep(const R *fin, const R *pin, R *fout, R *pout, const BatchLat *__restrict__ lats,
                   const int *__restrict__ blk_lat, DevState *__restrict__ sts, int rs, double dtw_d, double h1,
                   double h2, double *__restrict__ partials)
 {
   using A = Ar<R>;
   constexpr bool SPLIT = sizeof(R) == 4;
-  __shared__ R tile[3][kBY + 2][kBZ + 2];
-  __shared__ double red_smem[(kBZ * kBY / 32) * kRedSlots];
+  __shared__ R tile[3][BY + 2][BZ + 2];
+  __shared__ double red_smem[(BZ * BY / 32) * kRedSlots];
   const int L = blk_lat[blockIdx.x];
   const BatchLat lt = lats[L];
   DevState *st = sts + L;
@@ -54,9 +54,9 @@ __global__ void __launch_bounds__(kBZ *kBY, CLB_BATCH_MINB)
   pin += lt.off;
   fout += lt.off;
   pout += lt.off;
-  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * kBZ + tz;
-  const int z0 = bx * kBZ, y0 = by * kBY;
-  const int hz = min(kBZ, N - z0), hy = min(kBY, N - y0);
+  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * BZ + tz;
+  const int z0 = bx * BZ, y0 = by * BY;
+  const int hz = min(BZ, N - z0), hy = min(BY, N - y0);
   const int x0 = bz * lt.LX, x1 = min(N, x0 + lt.LX);
   const bool valid = tz < hz && ty < hy;
   const int y = y0 + ty, z = z0 + tz;
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kBZ *kBY, CLB_BATCH_MINB)
       acc_v += (double)cnt * rf.V;
     }
     double v[kRedSlots] = {acc_pi2, acc_g2, acc_v};
-    block_reduce<kRedSlots, kBZ * kBY>(v, red_smem);
+    block_reduce<kRedSlots, BZ * BY>(v, red_smem);
     if (tid == 0) {
 #pragma unroll
       for (int k = 0; k < kRedSlots; ++k) partials[(size_t)blockIdx.x * kRedSlots + k] = v[k];

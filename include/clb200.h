@@ -248,9 +248,9 @@ int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double
  * alongside (the scale factor's too, through the self-consistent expansion), in one pass with no
  * checkpoints; clb_measure refreshes the cached averages of both.  clb_tangent_observable returns
  *     O = sum_k w_k E_k / E_tot,  E_k = E_kin, E_grad of S, phi, Phi; E_el, E_mag of U(1) and SU(2); V
- * (n_weights <= 11) and its derivative along the direction at the current state.  clb_set_state or clb_tangent_end
- * ends the form.  lphi4SU2U1 only (other models: CLB_EUNSUPPORTED); device memory: one more
- * state. */
+ * (n_weights <= 11) and its derivative along the direction at the current state.  clb_set_state
+ * or clb_tangent_end ends the form.  lphi4SU2U1 only (other models: CLB_EUNSUPPORTED); device
+ * memory: one more state. */
 int clb_tangent_begin(clb_handle *h, const double *couplings_dot, int32_t n_couplings, const double *fields_dot,
                       const double *momenta_dot, const clb_scalefactor *sf_dot);
 int clb_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot, clb_scalefactor *sf_dot);
@@ -279,6 +279,24 @@ int clb_batch_evolve(clb_batch *b, int64_t nsteps);
 int clb_batch_measure(clb_batch *b, int32_t i, double e0, clb_measurement *m);
 int clb_batch_last_evolve_ms(clb_batch *b, double *ms);
 int clb_batch_kernel_launches(clb_batch *b, int64_t *n);
+
+/* Sweep configuration of the ensemble: the (z, y) tile of one sweep block and the x-planes each
+ * block marches over.  The first clb_batch_evolve of a handle times every compiled tile (32x4,
+ * 32x8, 32x16, 64x4) with x-runs of 8, 16, 32, 64 and N planes on the ensemble itself and keeps
+ * the fastest (environment CLB_BATCH_AUTOTUNE=0: keep 32x8, 32 planes); later handles of the same
+ * ensemble shape in the process reuse it.  clb_batch_autotune reruns it (reps timed sweeps per
+ * candidate); clb_batch_set_tuning fixes a configuration.  The fields do not depend on it; the
+ * volume sums are summed in a tile-dependent order. */
+typedef struct clb_batch_tuning {
+  int32_t tile_z, tile_y, planes_x; /* the configuration in use                                  */
+  int32_t candidates;               /* configurations timed (0: set, cached or default)          */
+  double ms_per_sweep;              /* its time for one fused stage sweep of all members         */
+  double ms_default;                /* the same for 32x8 tiles with 32-plane runs                */
+} clb_batch_tuning;
+
+int clb_batch_autotune(clb_batch *b, int32_t reps, clb_batch_tuning *out);
+int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t planes_x);
+int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
  * For callers that cannot call cudaMalloc: a runtime that owns the whole device memory pool, code

@@ -28,10 +28,12 @@ def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
 
 
-def run_batch(cases, precision, steps, chunks=1):
+def run_batch(cases, precision, steps, chunks=1, tuning=None):
     from cosmolattice_b200.batch import LatticeBatch
 
     bt = LatticeBatch([(c[2], c[1]) for c in cases], precision=precision)
+    if tuning is not None:
+        bt.set_tuning(*tuning)
     for i, c in enumerate(cases):
         bt.set_state(i, c[3], c[4], c[5])
     bt.initialize()
@@ -127,3 +129,48 @@ def test_batch_rejects_mixed_members():
     with pytest.raises(_capi.ClbError) as e:
         LatticeBatch([(c[2], c[1])])
     assert e.value.code == _capi.CLB_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("tile", [(32, 4, 8), (32, 8, 32), (32, 16, 5), (64, 4, 1024), (32, 4, 1)])
+def test_every_sweep_configuration_matches_oracle(tile):
+    # every compiled tile shape, with x-runs shorter than, equal to and longer than the members
+    cases = members("VV4", True)
+    out, m0, m1 = run_batch(cases, "fp64", 20, tuning=tile)
+    for i, c in enumerate(cases):
+        st, o0, o1 = run_oracle(c, 20)
+        assert rel(out[i][0], st[0]) < 1e-12 and rel(out[i][1], st[1]) < 1e-12, (tile, i)
+        assert abs(m1[i]["aI"] - o1["aI"]) <= 1e-10 * abs(o1["aI"])
+
+
+def test_autotuner_picks_a_timed_configuration():
+    from cosmolattice_b200.batch import LatticeBatch
+
+    cases = members()
+    bt = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp32")
+    for i, c in enumerate(cases):
+        bt.set_state(i, c[3], c[4], c[5])
+    bt.initialize()
+    assert bt.tuning()["candidates"] == 0
+    t = bt.autotune(3)
+    print("autotune", t)
+    assert t["candidates"] >= 8 and t["ms_per_sweep"] > 0 and t["ms_default"] > 0
+    assert t["ms_per_sweep"] <= t["ms_default"]
+    assert (t["tile_z"], t["tile_y"]) in {(32, 4), (32, 8), (32, 16), (64, 4)} and t["planes_x"] >= 8
+    assert bt.tuning() == t
+    f0 = [bt.get_state(i) for i in range(len(cases))]
+    bt.evolve(10)
+    # the timing sweeps left the state alone: a second handle without tuning runs the same steps
+    bt2 = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp32")
+    bt2.set_tuning(t["tile_z"], t["tile_y"], t["planes_x"])
+    for i, c in enumerate(cases):
+        bt2.set_state(i, c[3], c[4], c[5])
+    bt2.initialize()
+    assert all(np.array_equal(a[0], b[0]) for a, b in zip(f0, [bt2.get_state(i) for i in range(len(cases))]))
+    bt2.evolve(10)
+    for i in range(len(cases)):
+        a, b = bt.get_state(i), bt2.get_state(i)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    with pytest.raises(Exception):
+        bt.set_tuning(16, 16, 8)
+    bt.close()
+    bt2.close()
