@@ -24,17 +24,28 @@ GAUGE_FRACTION = (0.0, 0.0, 1.0, 1.0, 0.0)  # (E_el + E_mag) / E_tot
 
 def u1_gradients(model: Model, rp: RunParameters, n_steps: int, checkpoint_every: int,
                  weights: Sequence[float] = GAUGE_FRACTION, params: Iterable[str] = ("amp", "c4", "gQ"),
-                 lattice: Lattice = None) -> Tuple[float, Dict[str, float], Dict[str, object]]:
-    """(O, {param: dO/dparam}, backward record) for O = sum_k w_k E_k / E_tot after n_steps."""
+                 lattice: Lattice = None, state=None, tangents=None
+                 ) -> Tuple[float, Dict[str, float], Dict[str, object]]:
+    """(O, {param: dO/dparam}, backward record) for O = sum_k w_k E_k / E_tot after n_steps.
+    state: u1_initial_state(model, rp) if already made; tangents: {param: (df, dp)} likewise.
+    The record holds the wall times of the forward and backward calls."""
+    import time
+
     lat = lattice if lattice is not None else Lattice(model, rp)
-    f, p, aI, aD = u1_initial_state(model, rp)
+    if state is None:
+        state = u1_initial_state(model, rp)
+    f, p, aI, aD = state
     lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
     lat.initialize(correct_adot=True)
+    t0 = time.perf_counter()
     O = lat.forward(n_steps, checkpoint_every, weights)
+    t1 = time.perf_counter()
     fb, pb, g = lat.backward(through_init=True)
+    t2 = time.perf_counter()
+    g["forward_s"], g["backward_s"] = t1 - t0, t2 - t1
     out = {}
     for prm in params:
-        df, dp = u1_initial_state_tangent(model, rp, prm)
+        df, dp = tangents[prm] if tangents is not None else u1_initial_state_tangent(model, rp, prm, state)
         ic = float(fb @ df.ravel() + pb @ dp.ravel())
         explicit = {"amp": 0.0, "c4": g["dO_dcouplings"][0], "gQ": g["dO_dcouplings"][1]}[prm]
         out[prm] = ic + explicit

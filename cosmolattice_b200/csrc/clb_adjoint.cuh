@@ -21,89 +21,85 @@
 // d<|D phi|^2>/dA_i = 1/N^3 (2 gQ/dx) Im(conj(U_i phi(x+i)) phi), d<B^2>/dA = -2/N^3 curl curl A,
 // d<V>/dphi = 1/N^3 dV/dphi.
 //
-// Two sweeps per stage run backwards: k_u1_adj<1> at the stage output (steps 6, 5 and 4) and
-// k_u1_adj<0> at the stage input (steps 2 and 1); the scalar steps (F, a, aDot) are formed on the
-// host between them from the per-site dot products these sweeps reduce.
+// The coupling gQ enters U only through U_D(phi, gQ A), so dU/dgQ = (1/gQ) sum_x,i A_i dU_D'/dA_i
+// (U_D' = a^{1+alpha} U_D), and for any cotangent lt of the momenta
+//   lt . dK/dgQ = (m_A/gQ) sum_x,i [A_i (J^D w)_i + w_i K^D_i],   w = M^{-1} lt,
+// with K^D_i = -kA J0 gQ Im(conj(U_i phi(x+i)) phi) the U_D part of the U(1) kernel and J^D w its
+// derivative along w: the one dual lane of the state direction also gives the coupling
+// derivative.  Likewise d(sum |D phi|^2)/dgQ = (2/dx) sum A_i Im(conj(U_i phi(x+i)) phi).
+//
+// One sweep per stage boundary runs backwards.  It fuses the two transposed kicks that act on the
+// fields there: part A, the first kick of the stage that starts at the boundary (maps 2 and 1 of
+// that stage), and part B, the second kick of the stage that ends there (maps 6, 5 and 4).  Both
+// kicks use the kernel at the same fields and scale factor, J^T is linear, and the momentum-average
+// gradients between them are local to each site, so one JVP along
+//   w = M^{-1} (hA . lambda_A + hB . lambda_B),  lambda_A = pbar,  lambda_B = pbar + (momentum-average terms)
+// gives both.  The scalar steps (F, a, aDot) are formed on the host between sweeps from the per-site
+// dot products the sweeps reduce.
 
 #pragma once
 
 #include "clb_internal.cuh"
+#include "clb_tangent.cuh"
 #include "clb_u1.cuh"
 
 namespace clb {
 
-// Value plus two derivative directions: [0] the state direction mu, [1] d/dgQ.
-struct Dual2 {
-  double v, d0, d1;
-};
-__device__ __forceinline__ Dual2 dl(double v) { return Dual2{v, 0.0, 0.0}; }
-__device__ __forceinline__ Dual2 operator+(Dual2 a, Dual2 b) { return Dual2{a.v + b.v, a.d0 + b.d0, a.d1 + b.d1}; }
-__device__ __forceinline__ Dual2 operator-(Dual2 a, Dual2 b) { return Dual2{a.v - b.v, a.d0 - b.d0, a.d1 - b.d1}; }
-__device__ __forceinline__ Dual2 operator*(Dual2 a, Dual2 b)
-{
-  return Dual2{a.v * b.v, a.d0 * b.v + a.v * b.d0, a.d1 * b.v + a.v * b.d1};
-}
-__device__ __forceinline__ Dual2 operator*(double s, Dual2 a) { return Dual2{s * a.v, s * a.d0, s * a.d1}; }
-__device__ __forceinline__ Dual2 operator*(Dual2 a, double s) { return Dual2{s * a.v, s * a.d0, s * a.d1}; }
-__device__ __forceinline__ Dual2 operator/(Dual2 a, double s) { return Dual2{a.v / s, a.d0 / s, a.d1 / s}; }
-__device__ __forceinline__ void sincos_d(Dual2 t, Dual2 &s, Dual2 &c)
+using TD = Tan<double>;
+
+__device__ __forceinline__ void sincos_t(TD t, TD &s, TD &c)
 {
   double sv, cv;
   sincos(t.v, &sv, &cv);
-  s = Dual2{sv, cv * t.d0, cv * t.d1};
-  c = Dual2{cv, -sv * t.d0, -sv * t.d1};
+  s = TD(sv, cv * t.d);
+  c = TD(cv, -sv * t.d);
 }
 
-// Stencil pieces of the lphi4U1 kernel at one site, in dual numbers.
+// Stencil pieces of the lphi4U1 kernel at one site, as values with their derivative along w.
 struct U1Pieces {
-  Dual2 cl[2];  // covariant Laplacian of phi
-  Dual2 dv[2];  // dV/dphi_c = 4 c4 |phi|^2 phi_c
-  Dual2 cc[3];  // lapl A_i - sum_j backDiff_j forwDiff_i A_j
-  Dual2 im[3];  // Im(conj(U_i phi(x+i)) phi(x))
-  Dual2 d2;     // sum_i |D_i phi|^2
+  TD cl[2];     // covariant Laplacian of phi
+  TD dv[2];     // dV/dphi_c = 4 c4 |phi|^2 phi_c
+  TD cc[3];     // lapl A_i - sum_j backDiff_j forwDiff_i A_j
+  TD im[3];     // Im(conj(U_i phi(x+i)) phi(x))
   double vn[2]; // |phi|^2 phi_c (d dV/dphi_c / d c4 / 4)
   double n4;    // |phi|^4 (dV / d c4)
 };
 
-// ld(c, site) returns component c at a site as a dual number (value, direction, 0).
+// ld(c, site) returns component c at a site as (value, derivative along w).
 template <class LD>
 __device__ __forceinline__ void u1_pieces(LD ld, const U1Params &a, size_t s, const long long (&op)[3],
                                           const long long (&om)[3], U1Pieces &o)
 {
-  const Dual2 g = Dual2{a.gQ, 0.0, 1.0};
-  const double ndx = -a.dx;
-  const Dual2 fr = ld(0, s), fi = ld(1, s);
-  Dual2 pr = dl(0), pim = dl(0), mr = dl(0), mim = dl(0), d2 = dl(0);
+  const double ndxg = -a.dx * a.gQ;
+  const TD fr = ld(0, s), fi = ld(1, s);
+  TD pr(0.0), pim(0.0), mr(0.0), mim(0.0);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const size_t sp = s + op[d], sm = s + om[d];
-    Dual2 ur, ui, vr, vi;
-    sincos_d(ndx * (g * ld(2 + d, s)), ui, ur);
-    const Dual2 gr = ld(0, sp), gi = ld(1, sp);
-    const Dual2 wr = ur * gr - ui * gi, wi = ur * gi + ui * gr;
-    sincos_d(ndx * (g * ld(2 + d, sm)), vi, vr);
-    const Dual2 hr = ld(0, sm), hi = ld(1, sm);
+    TD ur, ui, vr, vi;
+    sincos_t(ndxg * ld(2 + d, s), ui, ur);
+    const TD gr = ld(0, sp), gi = ld(1, sp);
+    const TD wr = ur * gr - ui * gi, wi = ur * gi + ui * gr;
+    sincos_t(ndxg * ld(2 + d, sm), vi, vr);
+    const TD hr = ld(0, sm), hi = ld(1, sm);
     pr = pr + wr;
     pim = pim + wi;
     mr = mr + (vr * hr + vi * hi);
     mim = mim + (vr * hi - vi * hr);
     o.im[d] = wr * fi - wi * fr;
-    const Dual2 er = wr - fr, ei = wi - fi;
-    d2 = d2 + (er * er + ei * ei);
   }
   o.cl[0] = (pr + mr - 6.0 * fr) / a.dx2;
   o.cl[1] = (pim + mim - 6.0 * fi) / a.dx2;
-  const Dual2 n2 = fr * fr + fi * fi;
+  const TD n2 = fr * fr + fi * fi;
   o.dv[0] = (4.0 * a.c4) * (n2 * fr);
   o.dv[1] = (4.0 * a.c4) * (n2 * fi);
   o.vn[0] = n2.v * fr.v;
   o.vn[1] = n2.v * fi.v;
   o.n4 = n2.v * n2.v;
-  o.d2 = d2 / a.dx2;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    const Dual2 c = ld(2 + i, s);
-    Dual2 acc = dl(0);
+    const TD c = ld(2 + i, s);
+    TD acc(0.0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) acc = acc + (ld(2 + i, s + op[d]) + ld(2 + i, s + om[d]) - 2.0 * c);
 #pragma unroll
@@ -116,29 +112,30 @@ __device__ __forceinline__ void u1_pieces(LD ld, const U1Params &a, size_t s, co
 }
 
 struct U1AdjArgs {
-  // cotangents of the five averages at this sweep's state: <|pi_phi|^2>, <sum pi_A^2> act on the
-  // momenta, <|D phi|^2>, <B^2>, <V> on the fields
-  double Api, AE, AD, AB, AV;
-  double kA, kB2, kG;    // kick coefficients at this sweep's a
-  double dkA, dkB2, dkG; // their a-derivatives
-  double hc, hu;         // kick factors of the transposed kick (0: none)
-  double cdf, cda;       // dt w D(aS) per group: transposed drift (stage-output sweep only)
-  double J0;             // 2/dx (fStar/omegaStar)^2
-  double r2;             // 2 (fStar/omegaStar)^2 = 1/m_A
+  double hA[2], hB[2];         // kick factors (phi, A) of part A and part B; 0: no such kick
+  double ApiA, AEA, ApiB, AEB; // cotangents of <|pi_phi|^2>, <sum pi_A^2> at part A's and part B's map
+  double AD, AB, AV;           // cotangents of <|D phi|^2>, <B^2>, <V>, both parts
+  double cdf, cda;             // transposed drift of part B: dt w D(aS) per group (0: none)
+  double kA, kB2, kG;          // kick coefficients at the boundary's a
+  double dkA, dkB2, dkG;       // their a-derivatives
+  double J0;                   // 2/dx (fStar/omegaStar)^2
+  double r2;                   // 2 (fStar/omegaStar)^2 = 1/m_A
   double inv_n3;
 };
 
-// d/da (phi, A), d/dgQ (phi, A), d/dc4, d<|D phi|^2>/dgQ, drift (phi, A), d<V>/dc4
-constexpr int kAdjSlots = 9;
+// [0] a-derivative dot of part A, [1] of part B, [2] d/dgQ and [3] d/dc4 of both kicks, [4]
+// d(sum |D phi|^2)/dgQ, [5] sum |phi|^4, [6] [7] part B's drift dots (phi, A)
+constexpr int kAdjSlots = 8;
 
-// PRE = 1: sweep at the stage output (q1, p2): momentum-average gradients enter before the
-// transposed kick, and the transposed drift follows; writes qbar = qbar0 and pbar_out = pbar1.
-// PRE = 0: sweep at the stage input (q0, p0): transposed kick of pbar_in = pbar1, then the
-// average gradients; writes qbar and pbar_out = pbar0.  With hc = hu = 0 it applies only the
-// average gradients (observable seed, initial aDot correction).
 // S is the storage type of the forward state (f, p); the cotangents are FP64 in either form.
-template <int PRE, class S>
-__global__ void __launch_bounds__(256)
+// Reads qbar and pbar_in (lambda_A); writes qbar and pbar_out = lambda_B + (transposed drift).
+// Two resident 256-thread blocks per SM (128 registers): 1.30x over one block at 254 registers;
+// three are slower (spills).
+#ifndef CLB_U1_ADJ_MINB
+#define CLB_U1_ADJ_MINB 2
+#endif
+template <class S>
+__global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
     k_u1_adj(const S *__restrict__ f, const S *__restrict__ p, const double *__restrict__ pbar_in,
              double *__restrict__ qbar, double *__restrict__ pbar_out, U1Params a, U1AdjArgs g,
              double *__restrict__ partials)
@@ -149,72 +146,73 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int k = 0; k < kAdjSlots; ++k) acc[k] = 0;
   const double two_n3 = 2.0 * g.inv_n3;
-  // cotangent of the kick output at a site (PRE adds the momentum-average gradients)
-  auto lam = [&](int c, size_t y) -> double {
-    double l = pbar_in[c * n3 + y];
-    if (PRE) l += (c < 2 ? g.Api : g.AE) * two_n3 * (double)p[c * n3 + y];
-    return l;
-  };
+  const double cP = (g.ApiA + g.ApiB) * two_n3, cE = (g.AEA + g.AEB) * two_n3;
+  const double kJ = g.kA * g.J0 * a.gQ;
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
-    U1Pieces o;
-    auto ld = [&](int c, size_t y) -> Dual2 {
-      const double mu = c < 2 ? lam(c, y) : g.r2 * lam(c, y);
-      return Dual2{(double)f[c * n3 + y], mu, 0.0};
+    // the JVP direction at a site: M^{-1} (hA lambda_A + hB lambda_B)
+    auto ld = [&](int c, size_t y) -> TD {
+      const double lA = pbar_in[c * n3 + y];
+      const int sec = c < 2 ? 0 : 1;
+      const double lB = lA + (sec == 0 ? cP : cE) * (double)p[c * n3 + y];
+      const double w = g.hA[sec] * lA + g.hB[sec] * lB;
+      return TD((double)f[c * n3 + y], sec == 0 ? w : g.r2 * w);
     };
+    U1Pieces o;
     u1_pieces(ld, a, s, op, om, o);
     // kernel values and derivatives (complexscalarkernels.h:33-34, u1kernels.h:50)
-    Dual2 K[5];
+    TD K[5];
     K[0] = g.kA * o.cl[0] - g.kB2 * o.dv[0];
     K[1] = g.kA * o.cl[1] - g.kB2 * o.dv[1];
-    const Dual2 gq = Dual2{a.gQ, 0.0, 1.0};
 #pragma unroll
-    for (int i = 0; i < 3; ++i) K[2 + i] = g.kG * o.cc[i] - (g.kA * g.J0) * (gq * o.im[i]);
-    double l[5], qb[5];
+    for (int i = 0; i < 3; ++i) K[2 + i] = g.kG * o.cc[i] - kJ * o.im[i];
+    double lA[5], lB[5], qb[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-      l[c] = lam(c, s);
+      lA[c] = pbar_in[c * n3 + s];
+      lB[c] = lA[c] + (c < 2 ? cP : cE) * (double)p[c * n3 + s];
       qb[c] = qbar[c * n3 + s];
     }
-    // transposed kick: qbar += h M J (M^{-1} lambda)
-    qb[0] += g.hc * K[0].d0;
-    qb[1] += g.hc * K[1].d0;
+    // both transposed kicks: qbar += M J w
+    qb[0] += K[0].d;
+    qb[1] += K[1].d;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) qb[2 + i] += g.hu * K[2 + i].d0 / g.r2;
+    for (int i = 0; i < 3; ++i) qb[2 + i] += K[2 + i].d / g.r2;
     // gradients of the field averages
 #pragma unroll
     for (int c = 0; c < 2; ++c) qb[c] += g.AD * (-two_n3) * o.cl[c].v + g.AV * g.inv_n3 * o.dv[c].v;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
       qb[2 + i] += g.AD * g.inv_n3 * (2.0 * a.gQ / a.dx) * o.im[i].v + g.AB * (-two_n3) * o.cc[i].v;
-    // parameter and scale-factor dot products of the transposed kick
+    // scale-factor and coupling dot products
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      acc[0] += l[c] * (g.dkA * o.cl[c].v - g.dkB2 * o.dv[c].v);
-      acc[2] += l[c] * K[c].d1;
-      acc[4] += l[c] * (-g.kB2 * 4.0 * o.vn[c]);
+      const double da = g.dkA * o.cl[c].v - g.dkB2 * o.dv[c].v;
+      acc[0] += g.hA[0] * lA[c] * da;
+      acc[1] += g.hB[0] * lB[c] * da;
+      acc[3] += (g.hA[0] * lA[c] + g.hB[0] * lB[c]) * (-g.kB2 * 4.0 * o.vn[c]);
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      acc[1] += l[2 + i] * (g.dkG * o.cc[i].v - g.dkA * g.J0 * a.gQ * o.im[i].v);
-      acc[3] += l[2 + i] * K[2 + i].d1;
+      const double da = g.dkG * o.cc[i].v - g.dkA * g.J0 * a.gQ * o.im[i].v;
+      acc[0] += g.hA[1] * lA[2 + i] * da;
+      acc[1] += g.hB[1] * lB[2 + i] * da;
+      const double Ai = (double)f[(2 + i) * n3 + s];
+      const double wi = g.r2 * (g.hA[1] * lA[2 + i] + g.hB[1] * lB[2 + i]);
+      acc[2] += -(g.kA * g.J0 / g.r2) * (Ai * o.im[i].d + wi * o.im[i].v);
+      acc[4] += (2.0 / a.dx) * Ai * o.im[i].v;
     }
-    acc[5] += o.d2.d1;
-    acc[8] += o.n4;
+    acc[5] += o.n4;
+    // part B's transposed drift: pbar = lambda_B + dt w D qbar; its aS dot uses the momentum
+    // before part B's kick, p - hB K
     double pb[5];
-    if (PRE) {
-      // transposed drift: pbar1 = lambda + dt w D qbar1; the drift's aS dot uses p1 = p2 - h K(q1)
 #pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        const bool phi = c < 2;
-        const double p1 = (double)p[c * n3 + s] - (phi ? g.hc : g.hu) * K[c].v;
-        pb[c] = l[c] + (phi ? g.cdf : g.cda) * qb[c];
-        acc[phi ? 6 : 7] += p1 * qb[c];
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) pb[c] = l[c] + (c < 2 ? g.Api : g.AE) * two_n3 * (double)p[c * n3 + s];
+    for (int c = 0; c < 5; ++c) {
+      const bool phi = c < 2;
+      const double p1 = (double)p[c * n3 + s] - g.hB[phi ? 0 : 1] * K[c].v;
+      pb[c] = lB[c] + (phi ? g.cdf : g.cda) * qb[c];
+      acc[phi ? 6 : 7] += p1 * qb[c];
     }
 #pragma unroll
     for (int c = 0; c < 5; ++c) {

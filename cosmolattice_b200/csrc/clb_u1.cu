@@ -156,6 +156,84 @@ void kick_sweep(clb_handle *h, int nk, bool rf, bool rp, const U1Kick &kc)
   return kick<2, false, false>(h, kind, kc);
 }
 
+cudaError_t copy_state(clb_handle *h, void *f, void *p, bool to_live)
+{
+  U1Sector *u = h->u1;
+  const size_t bytes = 5 * h->n3 * u->esz;
+  cudaError_t e = cudaMemcpyAsync(to_live ? u->f : f, to_live ? f : u->f, bytes, cudaMemcpyDeviceToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(to_live ? u->p : p, to_live ? p : u->p, bytes, cudaMemcpyDeviceToDevice, h->stream);
+  return e;
+}
+
+// Boundary states and scalar records of a recomputed segment (adjoint).
+struct SegSave {
+  char *seg;     // boundary b at seg + 2 b half: fields, then momenta
+  size_t half;   // bytes of 5 N^3 values
+  U1State *rec;  // row b: the scalar state at boundary b
+};
+
+template <int NK, bool RED, class S> void kick_save_t(clb_handle *h, const U1Kick &kc, char *slot, size_t half)
+{
+  U1Sector *u = h->u1;
+  CLB_LAUNCH(h, K_U1_KICK,
+             k_u1_kick<NK, RED, RED, S, true><<<kU1Blocks, 256, 0, h->stream>>>(
+                 static_cast<const S *>(u->f), static_cast<S *>(u->p), u->prm, kc, u->d_st, u->d_part,
+                 reinterpret_cast<S *>(slot), reinterpret_cast<S *>(slot + half)));
+}
+template <class S> void kick_save_s(clb_handle *h, int nk, bool red, const U1Kick &kc, char *slot, size_t half)
+{
+  if (nk == 2)
+    red ? kick_save_t<2, true, S>(h, kc, slot, half) : kick_save_t<2, false, S>(h, kc, slot, half);
+  else
+    red ? kick_save_t<1, true, S>(h, kc, slot, half) : kick_save_t<1, false, S>(h, kc, slot, half);
+}
+
+// VelocityVerlet::evolve over nsteps with merged kicks (as u1_evolve).  With sv, the state and the
+// scalar record at every stage boundary are kept: the merged sweep writes the state between its
+// two kicks, and its tail is split at the boundary so the record can be taken there.
+void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
+{
+  const double dt = h->cfg.dt;
+  const bool ex = h->cfg.expansion != 0;
+  const std::vector<double> &ws = h->ws;
+  const size_t P = ws.size(), S = 2 * P - 1;
+  auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+  const int64_t total = nsteps * (int64_t)S;
+  const double w0 = wof(0);
+  if (sv) {
+    copy_state(h, sv->seg, sv->seg + sv->half, false);
+    k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, 0);
+  }
+  if (ex) tail(h, T_VV_KICK_HALF, false, 0, w0); // kickScaleFactorHalf
+  kick_sweep(h, 1, false, ex, vv_kick(dt, w0, 0.0));
+  if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w0); // <pi^2>, driftScaleFactor
+  for (int64_t k = 0; k < total; ++k) {
+    const size_t i = (size_t)(k % (int64_t)S);
+    const double w = wof(i);
+    const bool more = k + 1 < total;
+    const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+    drift(h, w);
+    if (!sv) {
+      kick_sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
+      if (ex) {
+        uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
+        if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
+        tail(h, fl, true, w, wn, i + 1 == S ? k / (int64_t)S : -1);
+      }
+    } else {
+      char *slot = sv->seg + (size_t)(k + 1) * 2 * sv->half;
+      if (h->u1->fp32)
+        kick_save_s<float>(h, more ? 2 : 1, ex, vv_kick(dt, w, wn), slot, sv->half);
+      else
+        kick_save_s<double>(h, more ? 2 : 1, ex, vv_kick(dt, w, wn), slot, sv->half);
+      if (ex) tail(h, T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, true, w, 0);
+      k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, k + 1);
+      if (ex && more) tail(h, T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT, true, w, wn);
+    }
+  }
+}
+
 int check(clb_handle *h, const char *where)
 {
   cudaError_t e = cudaGetLastError();
@@ -340,27 +418,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
     }
     h->synced = false;
   } else {
-    const std::vector<double> &ws = h->ws;
-    const size_t P = ws.size(), S = 2 * P - 1;
-    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
-    const int64_t total = nsteps * (int64_t)S;
-    const double w0 = wof(0);
-    if (ex) tail(h, T_VV_KICK_HALF, false, 0, w0); // kickScaleFactorHalf
-    kick_sweep(h, 1, false, ex, vv_kick(dt, w0, 0.0));
-    if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w0); // <pi^2>, driftScaleFactor
-    for (int64_t k = 0; k < total; ++k) {
-      const size_t i = (size_t)(k % (int64_t)S);
-      const double w = wof(i);
-      const bool more = k + 1 < total;
-      const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
-      drift(h, w);
-      kick_sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
-      if (ex) {
-        uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
-        if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
-        tail(h, fl, true, w, wn, i + 1 == S ? k / (int64_t)S : -1);
-      }
-    }
+    vv_run(h, nsteps, nullptr);
   }
   cudaEventRecord(h->ev_call[1], h->stream);
   const int r = check(h, "clb_evolve");
@@ -489,30 +547,6 @@ void averages_of(const U1State &s, double (&A)[kAvgN])
   A[4] = s.potI;
 }
 
-// One VV stage as the reference orders it (velocityverlet.h:61-114); with the same arithmetic as
-// the merged sweeps of u1_evolve.
-void vv_stage(clb_handle *h, double w)
-{
-  const double dt = h->cfg.dt;
-  const bool ex = h->cfg.expansion != 0;
-  if (ex) tail(h, T_VV_KICK_HALF, false, 0, w);
-  kick_sweep(h, 1, false, ex, vv_kick(dt, w, 0.0));
-  if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w);
-  drift(h, w);
-  kick_sweep(h, 1, ex, ex, vv_kick(dt, w, 0.0));
-  if (ex) tail(h, T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, true, w, 0);
-}
-
-cudaError_t copy_state(clb_handle *h, void *f, void *p, bool to_live)
-{
-  U1Sector *u = h->u1;
-  const size_t bytes = 5 * h->n3 * u->esz;
-  cudaError_t e = cudaMemcpyAsync(to_live ? u->f : f, to_live ? f : u->f, bytes, cudaMemcpyDeviceToDevice, h->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(to_live ? u->p : p, to_live ? p : u->p, bytes, cudaMemcpyDeviceToDevice, h->stream);
-  return e;
-}
-
 // Energies (energiesmeasurer.h:45-122) from the five averages at scale factor a.
 void energies_of(const U1Params &p, double a, const double (&A)[kAvgN], double (&E)[kAvgN])
 {
@@ -523,46 +557,40 @@ void energies_of(const U1Params &p, double a, const double (&A)[kAvgN], double (
   E[4] = A[4];
 }
 
-template <int PRE, class T>
+template <class T>
 void adj_launch(clb_handle *h, const void *f, const void *p, const double *pin, double *pout, const U1AdjArgs &g)
 {
   U1Sector *u = h->u1;
-  k_u1_adj<PRE, T><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<const T *>(f), static_cast<const T *>(p), pin,
-                                                      u->qbar, pout, u->prm, g, u->d_apart);
+  k_u1_adj<T><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<const T *>(f), static_cast<const T *>(p), pin, u->qbar,
+                                                 pout, u->prm, g, u->d_apart);
 }
 
-int adj_sweep(clb_handle *h, int pre, const void *f, const void *p, const double *pin, double *pout,
-              const U1AdjArgs &g, double (&S)[kAdjSlots])
+// One fused adjoint sweep at a boundary state and its dot products S.
+int adj_sweep(clb_handle *h, const void *f, const void *p, const double *pin, double *pout, const U1AdjArgs &g,
+              double (&S)[kAdjSlots])
 {
   U1Sector *u = h->u1;
   if (u->fp32)
-    pre ? adj_launch<1, float>(h, f, p, pin, pout, g) : adj_launch<0, float>(h, f, p, pin, pout, g);
+    CLB_LAUNCH(h, K_U1_ADJ, adj_launch<float>(h, f, p, pin, pout, g));
   else
-    pre ? adj_launch<1, double>(h, f, p, pin, pout, g) : adj_launch<0, double>(h, f, p, pin, pout, g);
-  ++h->launches[K_U1_ADJ];
-  k_sum_partials<kAdjSlots><<<1, 256, 0, h->stream>>>(u->d_apart, kU1Blocks, u->d_asums);
+    CLB_LAUNCH(h, K_U1_ADJ, adj_launch<double>(h, f, p, pin, pout, g));
+  CLB_LAUNCH(h, K_TAIL, k_sum_partials<kAdjSlots><<<1, 256, 0, h->stream>>>(u->d_apart, kU1Blocks, u->d_asums));
   cudaError_t e = cudaMemcpyAsync(S, u->d_asums, sizeof(S), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   return e == cudaSuccess ? CLB_OK : h->cuda_fail(e, "clb_backward");
 }
 
-U1AdjArgs adj_args(const U1Params &p, double a, const double (&Abar)[kAvgN], double hc, double hu)
+// Sweep arguments at scale factor a with both parts empty: kick coefficients and their a-derivatives.
+U1AdjArgs adj_base(const U1Params &p, double a)
 {
   const double al = p.alpha;
   U1AdjArgs g{};
-  g.Api = Abar[0];
-  g.AD = Abar[1];
-  g.AE = Abar[2];
-  g.AB = Abar[3];
-  g.AV = Abar[4];
   g.kA = std::pow(a, 1 + al);
   g.kB2 = std::pow(a, 3 + al) / 2;
   g.kG = std::pow(a, al - 1);
   g.dkA = (1 + al) * std::pow(a, al);
   g.dkB2 = (3 + al) * std::pow(a, 2 + al) / 2;
   g.dkG = (al - 1) * std::pow(a, al - 2);
-  g.hc = hc;
-  g.hu = hu;
   g.J0 = p.J0;
   g.r2 = p.J0 * p.dx; // 2 (fStar/omegaStar)^2
   g.inv_n3 = p.inv_n3;
@@ -602,17 +630,13 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
     return h->fail(CLB_ENOMEM, "clb_forward: checkpoint or segment storage does not fit; use a smaller checkpoint_every");
   }
   u->seg_cap = seg_states;
-  const std::vector<double> &ws = h->ws;
-  const size_t P = ws.size();
   cudaEventRecord(h->ev_call[0], h->stream);
-  for (int64_t st = 0; st < nsteps; ++st) {
-    if (st % K == 0) {
-      U1Sector::Ckpt &c = u->ckpt[(size_t)(st / K)];
-      if ((e = copy_state(h, c.f, c.p, false)) != cudaSuccess) return h->cuda_fail(e, "clb_forward");
-      if ((e = cudaMemcpyAsync(&c.st, u->d_st, sizeof(U1State), cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
-        return h->cuda_fail(e, "clb_forward");
-    }
-    for (int64_t i = 0; i < S; ++i) vv_stage(h, ws[(size_t)i < P ? (size_t)i : (size_t)(S - i - 1)]);
+  for (int64_t c = 0; c < nck; ++c) {
+    U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
+    if ((e = copy_state(h, ck.f, ck.p, false)) != cudaSuccess) return h->cuda_fail(e, "clb_forward");
+    if ((e = cudaMemcpyAsync(&ck.st, u->d_st, sizeof(U1State), cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_forward");
+    vv_run(h, std::min<int64_t>(K, nsteps - c * K), nullptr); // the merged schedule of clb_evolve
   }
   cudaEventRecord(h->ev_call[1], h->stream);
   {
@@ -656,10 +680,12 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
 }
 
 // Backward pass: cotangents of the forward start state and of the couplings for the observable
-// of the last u1_forward.  Segments are recomputed from their checkpoints (bitwise the forward
-// states) and each stage is reversed by the two adjoint sweeps.  With through_init the start state
-// is taken as produced by clb_initialize(correct_adot = 1), whose aDot = sqrt(Friedmann RHS)
-// (modelinitializer.h:77-78) is differentiated too.
+// of the last u1_forward.  Segments are recomputed from their checkpoints with the forward's
+// merged schedule (bitwise the forward states), keeping every stage-boundary state and scalar
+// record; then one fused adjoint sweep per boundary walks the segment backwards (part A: the
+// first kick of the stage starting there, part B: the second kick of the stage ending there).
+// With through_init the start state is taken as produced by clb_initialize(correct_adot = 1),
+// whose aDot = sqrt(Friedmann RHS) (modelinitializer.h:77-78) is differentiated too.
 __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar,
                                                       double *momenta_bar, clb_adjoint_grad *out)
 {
@@ -667,16 +693,17 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
   if (u->fwd_steps < 0) return h->fail(CLB_ESTATE, "clb_backward: call clb_forward first");
   const U1Params &prm = u->prm;
   const bool ex = h->cfg.expansion != 0;
-  const double dt = h->cfg.dt, al = prm.alpha;
+  const double dt = h->cfg.dt, al = prm.alpha, el = prm.el0;
   const size_t bytes = 5 * h->n3 * sizeof(double); // cotangents are FP64 in either form
   const std::vector<double> &ws = h->ws;
   const size_t P = ws.size();
   const int64_t S = 2 * (int64_t)P - 1;
   auto wof = [&](int64_t i) { return ws[(size_t)i < P ? (size_t)i : (size_t)(S - i - 1)]; };
   cudaError_t e = cudaSuccess;
-  double thg = 0, thc = 0;       // explicit d/dgQ, d/dc4
-  double S9[kAdjSlots];
+  double thg = 0, thc = 0; // explicit d/dgQ, d/dc4
+  double Sd[kAdjSlots];
   int cur = 0;
+  int r = CLB_OK;
   // seed: O = sum_k w_k E_k / E_tot at the final state
   double E[kAvgN], Et = 0, Ew = 0;
   energies_of(prm, u->fwd_a, u->fwd_avg, E);
@@ -684,121 +711,151 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
     Et += E[k];
     Ew += u->fwd_w[k] * E[k];
   }
-  double Ebar[kAvgN], Abar[kAvgN];
+  double Ebar[kAvgN];
   for (int k = 0; k < kAvgN; ++k) Ebar[k] = (u->fwd_w[k] - Ew / Et) / Et;
-  const double a = u->fwd_a, el = prm.el0;
-  Abar[0] = Ebar[0] * std::pow(a, -6);
-  Abar[1] = Ebar[1] * std::pow(a, -2);
-  Abar[2] = Ebar[2] * el * std::pow(a, -4);
-  Abar[3] = Ebar[3] * el * std::pow(a, -4);
-  Abar[4] = Ebar[4];
-  double abar = Ebar[0] * u->fwd_avg[0] * -6 * std::pow(a, -7) + Ebar[1] * u->fwd_avg[1] * -2 * std::pow(a, -3) +
-                (Ebar[2] * u->fwd_avg[2] + Ebar[3] * u->fwd_avg[3]) * el * -4 * std::pow(a, -5);
-  double adbar = 0;
-  if (!ex) abar = 0;
+  // part A pending at the next boundary to process: the transposed first kick of the stage that
+  // starts there (or the observable's seed, with no kick), its average cotangents, and the
+  // cotangents of a and aDot there before its a-dot products are added
+  struct PendA {
+    bool on;
+    double h[2];
+    double Abar[kAvgN];
+    double abar, adbar;
+  } pend{};
+  {
+    const double a = u->fwd_a;
+    pend.on = true;
+    pend.Abar[0] = Ebar[0] * std::pow(a, -6);
+    pend.Abar[1] = Ebar[1] * std::pow(a, -2);
+    pend.Abar[2] = Ebar[2] * el * std::pow(a, -4);
+    pend.Abar[3] = Ebar[3] * el * std::pow(a, -4);
+    pend.Abar[4] = Ebar[4];
+    pend.abar = ex ? Ebar[0] * u->fwd_avg[0] * -6 * std::pow(a, -7) + Ebar[1] * u->fwd_avg[1] * -2 * std::pow(a, -3) +
+                         (Ebar[2] * u->fwd_avg[2] + Ebar[3] * u->fwd_avg[3]) * el * -4 * std::pow(a, -5)
+                   : 0.0;
+    pend.adbar = 0;
+  }
+  double abar = 0, adbar = 0; // cotangents of a, aDot at the boundary just processed
   if ((e = cudaMemsetAsync(u->qbar, 0, bytes, h->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(u->pbar[cur], 0, bytes, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "clb_backward");
-  int r = adj_sweep(h, 0, u->f, u->p, u->pbar[cur], u->pbar[cur ^ 1], adj_args(prm, a, Abar, 0, 0), S9);
-  if (r != CLB_OK) return r;
-  cur ^= 1;
-  thg += Abar[1] * prm.inv_n3 * S9[5];
-  thc += Abar[4] * prm.inv_n3 * S9[8];
   std::vector<U1State> rec((size_t)u->seg_cap);
   const int64_t nck = (int64_t)u->ckpt.size() - 1; // the last entry holds the forward's end state
-  char *seg = u->seg;
   const size_t half = 5 * h->n3 * u->esz;
-  auto segf = [&](int64_t b) -> void * { return seg + (size_t)b * 2 * half; };
-  auto segp = [&](int64_t b) -> void * { return seg + (size_t)b * 2 * half + half; };
+  SegSave sv{u->seg, half, u->d_rec};
+  auto segf = [&](int64_t b) -> void * { return u->seg + (size_t)b * 2 * half; };
+  auto segp = [&](int64_t b) -> void * { return u->seg + (size_t)b * 2 * half + half; };
   for (int64_t c = nck - 1; c >= 0; --c) {
     const int64_t s0 = c * u->fwd_K, s1 = std::min(u->fwd_steps, s0 + u->fwd_K);
     const int64_t nb = (s1 - s0) * S; // stages in this segment
-    // recompute the segment, keeping every stage-boundary state and scalar record
+    // recompute the segment from its checkpoint, keeping every boundary state and record
     U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
     if ((e = copy_state(h, ck.f, ck.p, true)) != cudaSuccess ||
         (e = cudaMemcpyAsync(u->d_st, &ck.st, sizeof(U1State), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
       return h->cuda_fail(e, "clb_backward");
-    for (int64_t b = 0; b <= nb; ++b) {
-      if (b > 0) vv_stage(h, wof((b - 1) % S));
-      if ((e = copy_state(h, segf(b), segp(b), false)) != cudaSuccess) return h->cuda_fail(e, "clb_backward");
-      k_u1_record<<<1, 1, 0, h->stream>>>(u->d_st, u->d_rec, b);
-    }
+    vv_run(h, s1 - s0, &sv);
     e = cudaMemcpyAsync(rec.data(), u->d_rec, (size_t)(nb + 1) * sizeof(U1State), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "clb_backward");
-    for (int64_t b = nb - 1; b >= 0; --b) {
-      const double w = wof(b % S), hc = dt / 2 * w, hu = dt * w / 2, dtw = dt * w;
-      const U1State &R0 = rec[(size_t)b], &R1 = rec[(size_t)b + 1];
-      double A0[kAvgN], A1[kAvgN], A1bar[kAvgN] = {0, 0, 0, 0, 0}, A0bar[kAvgN] = {0, 0, 0, 0, 0};
-      averages_of(R0, A0);
-      averages_of(R1, A1);
-      // without expansion a stays at its set value: R0.aI = R1.aI, aS = the set aSI
-      const double a0 = R0.aI, a1 = R1.aI, aS = R1.aSI;
-      // step 6: aDot1 = aDotS + dt/2 w F(a1, <.>1)
-      double adS = 0, abar1 = 0;
-      if (ex) {
-        const SFGrad g1 = sf_grad(prm, a1, A1);
-        const double F6 = dt / 2 * w * adbar;
-        adS = adbar;
-        abar1 = abar + F6 * g1.da;
-        for (int k = 0; k < kAvgN; ++k) A1bar[k] = F6 * g1.dA[k];
+    for (int64_t b = nb; b >= 0; --b) {
+      const U1State &Rb = rec[(size_t)b];
+      double Ab[kAvgN];
+      averages_of(Rb, Ab);
+      const double ab = Rb.aI; // without expansion a stays at its set value
+      U1AdjArgs g = adj_base(prm, ab);
+      double AD = 0, AB = 0, AV = 0;
+      const bool partA = pend.on, partB = b >= 1;
+      const bool init = partA && c == 0 && b == 0 && through_init && ex;
+      double Ib[kAvgN] = {0, 0, 0, 0, 0}, RHSbar = 0;
+      if (init) {
+        // aDot0 = sqrt(RHS), RHS = a^{2 alpha + 2}/3 fm2 rho(<.>)  (hubbleconstraint.h:27-36): its
+        // average cotangents join part A's at the start state
+        const double C = std::pow(ab, 2 * al + 2) / 3.0 * prm.fm2;
+        RHSbar = pend.adbar / (2 * Rb.aDotI);
+        Ib[0] = RHSbar * C * std::pow(ab, -6);
+        Ib[1] = RHSbar * C * std::pow(ab, -2);
+        Ib[2] = Ib[3] = RHSbar * C * el * std::pow(ab, -4);
+        Ib[4] = RHSbar * C;
       }
-      // steps 5 and 4 at the stage output
-      U1AdjArgs g = adj_args(prm, a1, A1bar, hc, hu);
-      g.cdf = dtw * std::pow(aS, al - 3);
-      g.cda = dtw * std::pow(aS, al - 1);
-      if ((r = adj_sweep(h, 1, segf(b + 1), segp(b + 1), u->pbar[cur], u->pbar[cur ^ 1], g, S9)) != CLB_OK) return r;
-      cur ^= 1;
-      thg += hc * S9[2] + hu * S9[3] + A1bar[1] * prm.inv_n3 * S9[5];
-      thc += hc * S9[4] + A1bar[4] * prm.inv_n3 * S9[8];
-      double abar0 = 0, adbar0 = 0;
-      if (ex) {
-        abar1 += hc * S9[0] + hu * S9[1];
-        const double aSbar = dtw * ((al - 3) * std::pow(aS, al - 4) * S9[6] + (al - 1) * std::pow(aS, al - 2) * S9[7]);
-        // step 3: a1 = a0 + dt w aDotS, aS = (a0 + a1)/2
-        abar1 += aSbar / 2;
-        abar0 = aSbar / 2 + abar1;
-        adS += dtw * abar1;
-        // step 1: aDotS = aDot0 + dt/2 w F(a0, <.>0)
-        const SFGrad g0 = sf_grad(prm, a0, A0);
-        const double F1 = dt / 2 * w * adS;
-        adbar0 = adS;
-        abar0 += F1 * g0.da;
-        for (int k = 0; k < kAvgN; ++k) A0bar[k] = F1 * g0.dA[k];
+      if (partA) {
+        g.hA[0] = pend.h[0];
+        g.hA[1] = pend.h[1];
+        g.ApiA = pend.Abar[0] + Ib[0];
+        g.AEA = pend.Abar[2] + Ib[2];
+        AD += pend.Abar[1] + Ib[1];
+        AB += pend.Abar[3] + Ib[3];
+        AV += pend.Abar[4] + Ib[4];
       }
-      // steps 2 and 1 at the stage input
-      g = adj_args(prm, a0, A0bar, hc, hu);
-      if ((r = adj_sweep(h, 0, segf(b), segp(b), u->pbar[cur], u->pbar[cur ^ 1], g, S9)) != CLB_OK) return r;
+      // part B: the stage b - 1 ending here, maps 6 (aDot1 = aDotS + dt/2 w F(a1, <.>1)), 5 and 4
+      const int64_t sb = b - 1;
+      const double wB = partB ? wof(sb % S) : 0.0, dtwB = dt * wB;
+      const double adbar_b = partA ? pend.adbar : adbar; // aDot cotangent at this boundary
+      double F6 = 0, A1bar[kAvgN] = {0, 0, 0, 0, 0};
+      SFGrad g1{};
+      const double aS = Rb.aSI; // the stage ending here set aSI
+      if (partB) {
+        g.hB[0] = dt / 2 * wB;
+        g.hB[1] = dt * wB / 2;
+        if (ex) {
+          g1 = sf_grad(prm, ab, Ab);
+          F6 = dt / 2 * wB * adbar_b;
+          for (int k = 0; k < kAvgN; ++k) A1bar[k] = F6 * g1.dA[k];
+        }
+        g.ApiB = A1bar[0];
+        g.AEB = A1bar[2];
+        AD += A1bar[1];
+        AB += A1bar[3];
+        AV += A1bar[4];
+        g.cdf = dtwB * std::pow(aS, al - 3);
+        g.cda = dtwB * std::pow(aS, al - 1);
+      }
+      g.AD = AD;
+      g.AB = AB;
+      g.AV = AV;
+      if ((r = adj_sweep(h, segf(b), segp(b), u->pbar[cur], u->pbar[cur ^ 1], g, Sd)) != CLB_OK) return r;
       cur ^= 1;
-      thg += hc * S9[2] + hu * S9[3] + A0bar[1] * prm.inv_n3 * S9[5];
-      thc += hc * S9[4] + A0bar[4] * prm.inv_n3 * S9[8];
-      if (ex) abar0 += hc * S9[0] + hu * S9[1];
-      abar = abar0;
-      adbar = adbar0;
+      thg += Sd[2] + AD * prm.inv_n3 * Sd[4];
+      thc += Sd[3] + AV * prm.inv_n3 * Sd[5];
+      if (partA) {
+        abar = ex ? pend.abar + Sd[0] : 0.0;
+        adbar = pend.adbar;
+        pend.on = false;
+      }
+      if (init) {
+        const double C = std::pow(ab, 2 * al + 2) / 3.0 * prm.fm2, dC = (2 * al + 2) * std::pow(ab, 2 * al + 1) / 3.0 * prm.fm2;
+        const double rho = Ab[0] * std::pow(ab, -6) + Ab[1] * std::pow(ab, -2) + el * std::pow(ab, -4) * (Ab[2] + Ab[3]) + Ab[4];
+        const double drho = Ab[0] * -6 * std::pow(ab, -7) + Ab[1] * -2 * std::pow(ab, -3) + el * -4 * std::pow(ab, -5) * (Ab[2] + Ab[3]);
+        abar += RHSbar * (dC * rho + C * drho);
+        adbar = 0;
+      }
+      if (partB) {
+        // the rest of stage b - 1: maps 6, 4, 3 and 1; its part A is pending at boundary b - 1
+        pend.on = true;
+        pend.h[0] = dt / 2 * wB;
+        pend.h[1] = dt * wB / 2;
+        for (int k = 0; k < kAvgN; ++k) pend.Abar[k] = 0;
+        pend.abar = pend.adbar = 0;
+        if (ex) {
+          double abar1 = abar + F6 * g1.da + Sd[1];
+          double adS = adbar_b;
+          const double aSbar = dtwB * ((al - 3) * std::pow(aS, al - 4) * Sd[6] + (al - 1) * std::pow(aS, al - 2) * Sd[7]);
+          // map 3: a1 = a0 + dt w aDotS, aS = (a0 + a1)/2
+          abar1 += aSbar / 2;
+          double abar0 = aSbar / 2 + abar1;
+          adS += dtwB * abar1;
+          // map 1: aDotS = aDot0 + dt/2 w F(a0, <.>0)
+          const U1State &R0 = rec[(size_t)sb];
+          double A0[kAvgN];
+          averages_of(R0, A0);
+          const SFGrad g0 = sf_grad(prm, R0.aI, A0);
+          const double F1 = dt / 2 * wB * adS;
+          abar0 += F1 * g0.da;
+          for (int k = 0; k < kAvgN; ++k) pend.Abar[k] = F1 * g0.dA[k];
+          pend.abar = abar0;
+          pend.adbar = adS;
+        }
+      }
     }
-  }
-  // the start state is the first checkpoint, now at segment boundary 0 of the last recompute
-  if (through_init && ex) {
-    // aDot0 = sqrt(RHS), RHS = a^{2 alpha + 2}/3 fm2 rho(<.>)  (hubbleconstraint.h:27-36)
-    const U1State &R = rec[0];
-    double A0[kAvgN], Ib[kAvgN];
-    averages_of(R, A0);
-    const double a0 = R.aI;
-    const double C = std::pow(a0, 2 * al + 2) / 3.0 * prm.fm2, dC = (2 * al + 2) * std::pow(a0, 2 * al + 1) / 3.0 * prm.fm2;
-    const double rho = A0[0] * std::pow(a0, -6) + A0[1] * std::pow(a0, -2) + el * std::pow(a0, -4) * (A0[2] + A0[3]) + A0[4];
-    const double drho = A0[0] * -6 * std::pow(a0, -7) + A0[1] * -2 * std::pow(a0, -3) + el * -4 * std::pow(a0, -5) * (A0[2] + A0[3]);
-    const double RHSbar = adbar / (2 * R.aDotI);
-    Ib[0] = RHSbar * C * std::pow(a0, -6);
-    Ib[1] = RHSbar * C * std::pow(a0, -2);
-    Ib[2] = Ib[3] = RHSbar * C * el * std::pow(a0, -4);
-    Ib[4] = RHSbar * C;
-    abar += RHSbar * (dC * rho + C * drho);
-    adbar = 0;
-    if ((r = adj_sweep(h, 0, segf(0), segp(0), u->pbar[cur], u->pbar[cur ^ 1], adj_args(prm, a0, Ib, 0, 0), S9)) != CLB_OK)
-      return r;
-    cur ^= 1;
-    thg += Ib[1] * prm.inv_n3 * S9[5];
-    thc += Ib[4] * prm.inv_n3 * S9[8];
   }
   // leave the live state at the forward's end again
   {

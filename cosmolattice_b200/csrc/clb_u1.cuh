@@ -193,10 +193,12 @@ template <class T> __device__ __forceinline__ T u1_pot(const U1Site<T> &o, T c4)
 #ifndef CLB_U1_KICK_MINB
 #define CLB_U1_KICK_MINB 2
 #endif
-template <int NK, bool RF, bool RP, class S>
+// SAVE (adjoint recompute): also writes the fields and the momenta after the first kick, the state
+// at the stage boundary between the two kicks, to save_f / save_p.
+template <int NK, bool RF, bool RP, class S, bool SAVE = false>
 __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
     k_u1_kick(const S *__restrict__ f, S *__restrict__ p, U1Params a, U1Kick kc, const U1State *__restrict__ st,
-              double *__restrict__ partials)
+              double *__restrict__ partials, S *__restrict__ save_f = nullptr, S *__restrict__ save_p = nullptr)
 {
   __shared__ double smem[(256 / 32) * kU1Red];
   const size_t n3 = a.n3;
@@ -228,6 +230,13 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
         if (sizeof(S) == 4) {
 #pragma unroll
           for (int c = 0; c < 5; ++c) q[c] = (double)(S)q[c]; // the stored value after this kick
+        }
+        if (SAVE && k == 0) {
+#pragma unroll
+          for (int c = 0; c < 5; ++c) {
+            save_p[c * n3 + s] = (S)q[c];
+            save_f[c * n3 + s] = f[c * n3 + s];
+          }
         }
       }
       if (RP) {

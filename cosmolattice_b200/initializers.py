@@ -349,10 +349,11 @@ def initial_state(model: Model, rp: RunParameters):
     return scalar_initial_state(model, rp)
 
 
-def u1_initial_state_tangent(model: Model, rp: RunParameters, param: str):
+def u1_initial_state_tangent(model: Model, rp: RunParameters, param: str, state=None):
     """d(fields, momenta)/d param of u1_initial_state for param in ("amp", "c4", "gQ"): the
-    fluctuation amplitude, the quartic coupling (lambda_prog) and the gauge coupling g Q."""
-    fields, momenta, aI, aDot = u1_initial_state(model, rp)
+    fluctuation amplitude, the quartic coupling (lambda_prog) and the gauge coupling g Q.
+    state: (fields, momenta, aI, aDot) of u1_initial_state, if already made."""
+    fields, momenta, aI, aDot = state if state is not None else u1_initial_state(model, rp)
     N = rp.N
     df = np.zeros_like(fields)
     dp = np.zeros_like(momenta)
