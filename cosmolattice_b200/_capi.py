@@ -164,6 +164,8 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_tangent_get_state": (C.c_int, [H, dp, dp, C.POINTER(ScaleFactor)]),
             "clb_tangent_observable": (C.c_int, [H, dp, C.c_int32, dp, dp]),
             "clb_tangent_energies": (C.c_int, [H, dp, dp]),
+            "clb_tangent_spectrum": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                               C.c_int32, dp, dp, dp, C.POINTER(C.c_int64)]),
             "clb_tangent_end": (C.c_int, [H]),
             "clb_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(ModelDesc), C.c_int32, C.POINTER(H)]),
             "clb_batch_destroy": (None, [H]),
@@ -228,6 +230,7 @@ EXPORTED = [
     "clb_tangent_get_state",
     "clb_tangent_observable",
     "clb_tangent_energies",
+    "clb_tangent_spectrum",
     "clb_tangent_end",
     "clb_batch_create",
     "clb_batch_destroy",

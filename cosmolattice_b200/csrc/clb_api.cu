@@ -69,6 +69,7 @@ int su2_tangent_get_state(clb_handle *h, double *fields_dot, double *momenta_dot
 int su2_tangent_observable(clb_handle *h, const double *w, int32_t nw, double *obs, double *dobs);
 int su2_tangent_end(clb_handle *h);
 int su2_tangent_energies(clb_handle *h, double *E, double *dE);
+const void *su2_tangent_component(clb_handle *h, int which, int comp, bool *f32, double *aI, double *daI);
 
 const double *u1_component(clb_handle *h, int which, int comp, bool *gauge);
 const double *su2_component(clb_handle *h, int which, int comp, bool *gauge);
@@ -598,6 +599,7 @@ void clb_destroy(clb_handle *h)
   if (h->d_stage) cudaFree(h->d_stage);
   if (h->plan_ok) cufftDestroy(h->plan);
   if (h->d_spec) cudaFree(h->d_spec);
+  if (h->d_spec2) cudaFree(h->d_spec2);
   if (h->d_spec_part) cudaFree(h->d_spec_part);
   if (h->d_spec_cnt) cudaFree(h->d_spec_cnt);
   if (h->d_spec_out) cudaFree(h->d_spec_out);
@@ -973,10 +975,35 @@ int clb_tangent_end(clb_handle *h)
 
 constexpr int kSpecBlocks = 148 * 2;
 
-int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
-                 int32_t nbins, int32_t fold, double *k_out, double *value_out, int64_t *count_out)
+} // extern "C"
+
+namespace {
+
+// PowerSpectrumMeasurer::powerSpectrum normalisation (powerspectrum.h:95-106) of a bin's sum of
+// |f_k|^2 (linear in sum), and the bin's wave number ntil (in units of kIR).
+double spec_value(const clb_handle *h, int ps_type, int ps_version, double dk, int b, unsigned long long c,
+                  double nsum, double sum, double *ntil_out)
 {
-  if (!h) return CLB_EINVAL;
+  const double pi = 3.14159265358979323846;
+  const int N = h->N;
+  const double dx = h->cfg.dx;
+  const double kIR = 2 * pi / (N * dx);
+  double N5 = 1;
+  for (int i = 0; i < 5; ++i) N5 *= (double)N;
+  const double ntil = (ps_version == 1 && c > 0) ? nsum / (double)c : (b + 0.5) * dk;
+  *ntil_out = ntil;
+  if (c == 0) return 0.0;
+  if (ps_type == 1) return kIR * ntil * dx / dk / N5 / 2.0 / pi * sum;
+  const double t = kIR * ntil * dx / N;
+  return t * t * t / dk / 2.0 / (pi * pi) * (sum / (double)c);
+}
+
+// clb_spectrum, also returning the raw bin sums [sum |f|^2 | sum |n|] and counts, and whether the
+// component belongs to a gauge field.
+int spectrum_impl(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                  int32_t nbins, int32_t fold, double *k_out, double *value_out, int64_t *count_out,
+                  std::vector<double> &sums, std::vector<unsigned long long> &cnt, bool &gauge_comp_out)
+{
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_spectrum: call clb_initialize first");
   const bool gauge_model = h->u1 || h->su2;
   bool gauge_comp = false;
@@ -1055,8 +1082,9 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
   CLB_LAUNCH(h, K_SPECTRUM,
              k_spec_sum<<<(nbins + 255) / 256, 256, 0, h->stream>>>(h->d_spec_part, h->d_spec_cnt, kSpecBlocks, nbins,
                                                                     h->d_spec_out, h->d_spec_out + nbins, h->d_spec_outc));
-  std::vector<double> sums(2 * (size_t)nbins);
-  std::vector<unsigned long long> cnt(nbins);
+  sums.assign(2 * (size_t)nbins, 0.0);
+  cnt.assign(nbins, 0ull);
+  gauge_comp_out = gauge_comp;
   e = cudaMemcpyAsync(sums.data(), h->d_spec_out, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(cnt.data(), h->d_spec_outc, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream);
@@ -1074,31 +1102,92 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
     if ((e = cudaMemcpy(&s, h->d_st, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess) return h->cuda_fail(e, "clb_spectrum");
     aI = s.aI;
   }
-  // PowerSpectrumMeasurer::powerSpectrum normalisation (powerspectrum.h:95-106)
-  const double pi = 3.14159265358979323846;
-  const double dx = h->cfg.dx;
-  const double kIR = 2 * pi / (N * dx);
-  double N5 = 1;
-  for (int i = 0; i < 5; ++i) N5 *= (double)N;
+  const double kIR = 2 * 3.14159265358979323846 / (N * h->cfg.dx);
   // momenta: a^{2 alpha - 6} for matter (scalarsingletmeasurer.h:80), a^{2 alpha - 2} for gauge
   // components (u1measurer.h:102-103)
   const double mom_factor = which == 1 ? std::pow(aI, 2 * h->md.alpha - (gauge_comp ? 2 : 6)) : 1.0;
   for (int b = 0; b < nbins; ++b) {
-    const double sum = sums[b], nsum = sums[nbins + b];
     const unsigned long long c = cnt[b];
-    const double ntil = (ps_version == 1 && c > 0) ? nsum / (double)c : (b + 0.5) * dk;
-    double v = 0;
-    if (c > 0) {
-      if (ps_type == 1) {
-        v = kIR * ntil * dx / dk / N5 / 2.0 / pi * sum;
-      } else {
-        const double t = kIR * ntil * dx / N;
-        v = t * t * t / dk / 2.0 / (pi * pi) * (sum / (double)c);
-      }
-    }
-    value_out[b] = mom_factor * v;
+    double ntil;
+    value_out[b] = mom_factor * spec_value(h, ps_type, ps_version, dk, b, c, sums[nbins + b], sums[b], &ntil);
     if (k_out) k_out[b] = ntil * kIR;
     if (count_out) count_out[b] = (int64_t)c;
+  }
+  return CLB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                 int32_t nbins, int32_t fold, double *k_out, double *value_out, int64_t *count_out)
+{
+  if (!h) return CLB_EINVAL;
+  std::vector<double> sums;
+  std::vector<unsigned long long> cnt;
+  bool gauge_comp = false;
+  return spectrum_impl(h, which, comp, ps_type, ps_version, dk, nbins, fold, k_out, value_out, count_out, sums, cnt,
+                       gauge_comp);
+}
+
+// clb_spectrum of a component and its derivative along the tangent-linear form's direction.
+int clb_tangent_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                         int32_t nbins, int32_t fold, double *k_out, double *value_out, double *d_value_out,
+                         int64_t *count_out)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_spectrum: the tangent-linear form covers lphi4SU2U1");
+  if (!d_value_out) return h->fail(CLB_EINVAL, "clb_tangent_spectrum: null output");
+  bool f32 = false;
+  double aI = 1, daI = 0;
+  const void *tsrc = nullptr;
+  if (which == 0 || which == 1) tsrc = su2_tangent_component(h, which, comp, &f32, &aI, &daI);
+  if (!tsrc && (which == 0 || which == 1) && comp >= 0 && comp < (which == 0 ? 22 : 19))
+    return h->fail(CLB_ESTATE, "clb_tangent_spectrum: call clb_tangent_begin first");
+  std::vector<double> sums;
+  std::vector<unsigned long long> cnt;
+  bool gauge_comp = false;
+  int r = spectrum_impl(h, which, comp, ps_type, ps_version, dk, nbins, fold, k_out, value_out, count_out, sums, cnt,
+                        gauge_comp);
+  if (r != CLB_OK) return r;
+  // the component's transform is in d_spec; transform its tangent into d_spec2
+  const int N = h->N;
+  const size_t spec_n = (size_t)N * N * 2 * (N / 2 + 1);
+  cudaError_t e = cudaSuccess;
+  if (!h->d_spec2 && (e = cudaMalloc(&h->d_spec2, spec_n * sizeof(double))) != cudaSuccess)
+    return h->fail(CLB_ENOMEM, std::string("clb_tangent_spectrum: ") + cudaGetErrorString(e));
+  if (f32)
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather_raw<float><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const float *>(tsrc), h->d_spec2, N));
+  else
+    CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather_raw<double><<<kElemBlocks, 256, 0, h->stream>>>(static_cast<const double *>(tsrc), h->d_spec2, N));
+  if (cufftExecD2Z(h->plan, h->d_spec2, reinterpret_cast<cufftDoubleComplex *>(h->d_spec2)) != CUFFT_SUCCESS)
+    return h->fail(CLB_ECUDA, "clb_tangent_spectrum: cufftExecD2Z failed");
+  const size_t smem = (size_t)nbins * sizeof(double);
+  if (smem > 48 * 1024 && (e = cudaFuncSetAttribute(k_spec_bin_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    return h->fail(CLB_EINVAL, "clb_tangent_spectrum: too many bins for shared memory");
+  CLB_LAUNCH(h, K_SPECTRUM,
+             k_spec_bin_cross<<<kSpecBlocks, 256, smem, h->stream>>>(reinterpret_cast<const double2 *>(h->d_spec),
+                                                                     reinterpret_cast<const double2 *>(h->d_spec2), N,
+                                                                     dk, nbins, fold, h->d_spec_part, h->d_spec_cnt));
+  CLB_LAUNCH(h, K_SPECTRUM,
+             k_spec_sum<<<(nbins + 255) / 256, 256, 0, h->stream>>>(h->d_spec_part, h->d_spec_cnt, kSpecBlocks, nbins,
+                                                                    h->d_spec_out, h->d_spec_out + nbins, h->d_spec_outc));
+  std::vector<double> dsum((size_t)nbins);
+  e = cudaMemcpyAsync(dsum.data(), h->d_spec_out, dsum.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_tangent_spectrum");
+  collect_profile(h);
+  // value = m(a) S(sum): d value = m dS(dsum) + m' da S(sum), m = a^{2 alpha - 6} (matter momenta),
+  // a^{2 alpha - 2} (gauge momenta), 1 (fields)
+  const double ex = 2 * h->md.alpha - (gauge_comp ? 2 : 6);
+  const double m = which == 1 ? std::pow(aI, ex) : 1.0;
+  const double dm = which == 1 ? ex * std::pow(aI, ex - 1) * daI : 0.0;
+  for (int b = 0; b < nbins; ++b) {
+    double ntil;
+    const double v = spec_value(h, ps_type, ps_version, dk, b, cnt[b], sums[nbins + b], sums[b], &ntil);
+    const double dv = spec_value(h, ps_type, ps_version, dk, b, cnt[b], sums[nbins + b], dsum[b], &ntil);
+    d_value_out[b] = m * dv + dm * v;
   }
   return CLB_OK;
 }

@@ -76,6 +76,7 @@ struct clb_handle {
   size_t stage_n = 0;
   // spectra: in-place D2Z buffer, cuFFT plan and binning scratch (allocated on first use)
   double *d_spec = nullptr;
+  double *d_spec2 = nullptr; // the tangent's transform (clb_tangent_spectrum)
   bool plan_ok = false;
   cufftHandle plan = 0;
   double *d_spec_part = nullptr;

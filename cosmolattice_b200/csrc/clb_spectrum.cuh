@@ -39,6 +39,56 @@ __global__ void __launch_bounds__(256) k_spec_gather_plain(const double *__restr
   }
 }
 
+// Unpadded N^3 component of storage type R -> real input of an in-place R2C transform.
+template <class R>
+__global__ void __launch_bounds__(256) k_spec_gather_raw(const R *__restrict__ src, double *__restrict__ dst, int N)
+{
+  const long long pitch = 2LL * (N / 2 + 1);
+  for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
+    const R *s = src + r * N;
+    double *d = dst + r * pitch;
+    for (int z = threadIdx.x; z < N; z += blockDim.x) d[z] = (double)s[z];
+  }
+}
+
+// Tangent of the binned sum of |f_k|^2: per bin sum w 2 Re(conj(f_k) t_k) of the transforms of
+// a component (fk) and of its tangent (tk), with k_spec_bin's bins and weights; partial rows in
+// k_spec_bin's layout (the |n| and count slots left 0).
+__global__ void __launch_bounds__(256)
+    k_spec_bin_cross(const double2 *__restrict__ fk, const double2 *__restrict__ tk, int N, double dk, int nbins,
+                     int fold, double *__restrict__ part_val, unsigned long long *__restrict__ part_cnt)
+{
+  extern __shared__ unsigned char smem_raw[];
+  double *h_val = reinterpret_cast<double *>(smem_raw);
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) h_val[b] = 0.0;
+  __syncthreads();
+  const int nzh = N / 2 + 1;
+  for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
+    const int kx = (int)(r / N), ky = (int)(r % N);
+    const long long nx = kx <= N / 2 ? kx : kx - N;
+    const long long ny = ky <= N / 2 ? ky : ky - N;
+    const double2 *row = fk + r * nzh, *trow = tk + r * nzh;
+    for (int kz = threadIdx.x; kz < nzh; kz += blockDim.x) {
+      const long long n2 = nx * nx + ny * ny + (long long)kz * kz;
+      const double nn = sqrt((double)n2);
+      int b = (int)floor(nn / dk);
+      if (b >= nbins) {
+        if (!fold) continue;
+        b = nbins - 1;
+      }
+      const int w = (kz == 0 || (2 * kz == N)) ? 1 : 2;
+      const double2 v = row[kz], t = trow[kz];
+      atomicAdd(&h_val[b], w * (2.0 * (v.x * t.x + v.y * t.y)));
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+    part_val[((size_t)blockIdx.x * nbins + b) * 2 + 0] = h_val[b];
+    part_val[((size_t)blockIdx.x * nbins + b) * 2 + 1] = 0.0;
+    part_cnt[(size_t)blockIdx.x * nbins + b] = 0ull;
+  }
+}
+
 // One block per group of (kx, ky) rows; shared-memory histograms of sum w |f|^2, sum w |n| and the
 // integer mode count, written as one partial row per block.
 __global__ void __launch_bounds__(256)

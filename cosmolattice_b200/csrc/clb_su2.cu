@@ -755,4 +755,20 @@ __attribute__((visibility("hidden"))) int su2_tangent_end(clb_handle *h)
   return e == cudaSuccess ? CLB_OK : h->cuda_fail(e, "clb_tangent_end");
 }
 
+// Tangent of one state component (clb_tangent_spectrum): raw storage (float in the FP32 form) and
+// the scale factor with its tangent.
+__attribute__((visibility("hidden"))) const void *su2_tangent_component(clb_handle *h, int which, int comp, bool *f32,
+                                                                        double *aI, double *daI)
+{
+  SU2Sector *u = h->su2;
+  if (!u->tangent || comp < 0 || comp >= (which == 0 ? NF : NP)) return nullptr;
+  TState t;
+  if (cudaMemcpy(&t, u->d_tst, sizeof(t), cudaMemcpyDeviceToHost) != cudaSuccess) return nullptr;
+  *aI = t.aI.v;
+  *daI = t.aI.d;
+  *f32 = u->fp32;
+  const char *base = static_cast<const char *>(which == 0 ? u->df : u->dp);
+  return base + (size_t)comp * h->n3 * u->esz;
+}
+
 } // namespace clb

@@ -178,6 +178,18 @@ class Lattice:
         self._check(self.lib.clb_tangent_energies(self.h, _dp(e), _dp(de)))
         return e, de
 
+    def tangent_spectrum(self, which: int = 0, comp: int = 0, ps_type: int = 1, ps_version: int = 1, dk: float = 1.0,
+                         nbins: Optional[int] = None, fold: bool = True):
+        """(k, spectrum, d spectrum, mode counts): spectrum() and its derivative along the tangent."""
+        if nbins is None:
+            nbins = int(np.floor(np.sqrt(3.0) / 2.0 * self.rp.N / dk))
+        k, v, dv = np.empty(nbins), np.empty(nbins), np.empty(nbins)
+        c = np.empty(nbins, dtype=np.int64)
+        self._check(self.lib.clb_tangent_spectrum(self.h, which, comp, ps_type, ps_version, float(dk), nbins,
+                                                  1 if fold else 0, _dp(k), _dp(v), _dp(dv),
+                                                  c.ctypes.data_as(C.POINTER(C.c_int64))))
+        return k, v, dv, c
+
     def tangent_end(self) -> None:
         self._check(self.lib.clb_tangent_end(self.h))
 

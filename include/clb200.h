@@ -258,6 +258,11 @@ int clb_tangent_observable(clb_handle *h, const double *weights, int32_t n_weigh
                            double *d_observable);
 /* The 11 energies E_k of clb_tangent_observable and their derivatives (either array may be NULL). */
 int clb_tangent_energies(clb_handle *h, double *energies, double *d_energies);
+/* clb_spectrum of one component and, in d_value_out, its derivative along the direction (the
+ * momentum spectra's a-factor included). */
+int clb_tangent_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, int32_t ps_version, double dk,
+                         int32_t nbins, int32_t fold, double *k_out, double *value_out, double *d_value_out,
+                         int64_t *count_out);
 int clb_tangent_end(clb_handle *h);
 
 /* ---- batched ensemble ----------------------------------------------------------------------------

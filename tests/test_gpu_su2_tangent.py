@@ -183,3 +183,38 @@ def test_tangent_api_errors():
         lat.tangent_get_state()
     assert e.value.code == _capi.CLB_ESTATE
     lat.close()
+
+
+@pytest.mark.parametrize("which,comp", [(0, 3), (0, 11), (1, 10), (1, 7)])
+def test_spectrum_tangent_matches_gpu_finite_differences(which, comp):
+    # d/dg_SU2 of the binned spectrum (doublet field, an SU(2) link component, SU(2) and U(1)
+    # momenta with their a-factors) against central differences of clb_spectrum on the plain path
+    from cosmolattice_b200 import Lattice
+    from cosmolattice_b200.initializers import su2u1_initial_state_tangent
+
+    N, n = 8, 20
+    par, rp, m, f, p, sf = case(N, "VV2", True)
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    df, dp, cd = su2u1_initial_state_tangent(m, rp, "gSU2", (f, p))
+    lat.tangent_begin(cd, df, dp)
+    lat.initialize()
+    lat.evolve(n)
+    k, v, dv, c = lat.tangent_spectrum(which=which, comp=comp)
+    k0, v0, c0 = lat.spectrum(which=which, comp=comp)
+    lat.close()
+    assert np.array_equal(c, c0) and np.allclose(v, v0, rtol=1e-12, atol=0)  # bins summed by shared atomics
+    h = 1e-4 * BASE["gSU2"]
+    res = []
+    for g in (BASE["gSU2"] + h, BASE["gSU2"] - h):
+        _, rp2, m2, f2, p2, sf2 = case(N, "VV2", True, {"gSU2": g})
+        l2 = Lattice(m2, rp2)
+        l2.set_state(f2, p2, sf2)
+        l2.initialize()
+        l2.evolve(n)
+        res.append(l2.spectrum(which=which, comp=comp)[1])
+        l2.close()
+    ref = (res[0] - res[1]) / (2 * h)
+    sc = np.abs(ref).max()
+    print("spectrum tangent", which, comp, np.abs(dv - ref).max() / sc)
+    assert sc > 0 and np.abs(dv - ref).max() <= 1e-5 * sc
