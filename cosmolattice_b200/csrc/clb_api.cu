@@ -82,6 +82,24 @@ __attribute__((visibility("hidden"))) void set_global_error(const std::string &m
 namespace {
 
 
+// Launch with the programmatic-stream-serialization attribute: the kernel may start while the
+// previous kernel in the stream drains; it waits (griddep_wait) before touching dependent data.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 // Sweep geometry: bz x by (z, y) sites per block; the x direction is split so the grid holds about
 // two waves of resident blocks.
 void setup_geometry(clb_handle *h, int blocks_per_sm)
@@ -119,10 +137,16 @@ void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dt
   a.h1 = h1;
   a.h2 = h2;
   a.rs = h->rs;
-  CLB_LAUNCH(h, kind,
-             k_sweep<R, NS, SH, DRIFT, KICK, RED><<<h->sweep_grid, dim3(SH::TZ, SH::TY), h->sweep_smem, h->stream>>>(
-                 h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]), a, h->d_st,
-                 h->d_part, h->d_err));
+  if (h->pdl_now)
+    CLB_LAUNCH(h, kind,
+               launch_pdl(k_sweep<R, NS, SH, DRIFT, KICK, RED>, h->sweep_grid, dim3(SH::TZ, SH::TY), h->sweep_smem,
+                          h->stream, h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]),
+                          a, (const DevState *)h->d_st, h->d_part, h->d_err));
+  else
+    CLB_LAUNCH(h, kind,
+               k_sweep<R, NS, SH, DRIFT, KICK, RED><<<h->sweep_grid, dim3(SH::TZ, SH::TY), h->sweep_smem, h->stream>>>(
+                   h->tm_f[fb], h->tm_p[pb], static_cast<R *>(h->fld[fo]), static_cast<R *>(h->pi[po]), a, h->d_st,
+                   h->d_part, h->d_err));
   if (sizeof(R) == 4 && (DRIFT || KICK)) h->rs ^= 1; // the launch advanced the FP64 references
 }
 
@@ -274,7 +298,11 @@ bool encode_map(clb_handle *h, void *base, CUtensorMap *map, std::string &why)
 void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1)
 {
   TailOp op{flags, nblocks, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
-  CLB_LAUNCH(h, K_TAIL, k_tail<<<1, kTailThreads, 0, h->stream>>>(h->d_part, op, h->d_st, h->sp));
+  if (h->pdl_now)
+    CLB_LAUNCH(h, K_TAIL, launch_pdl(k_tail, dim3(1), dim3(kTailThreads), 0, h->stream, (const double *)h->d_part, op,
+                                     h->d_st, h->sp));
+  else
+    CLB_LAUNCH(h, K_TAIL, k_tail<<<1, kTailThreads, 0, h->stream>>>(h->d_part, op, h->d_st, h->sp));
 }
 
 // Dispatch on (storage, field count).
@@ -323,6 +351,7 @@ template <class R, int NS> struct EvolveVV {
     if (ex) tail(h, T_VV_KICK_HALF, 0, 0, w0); // kickScaleFactorHalf
     L::kick(h, w0 * dt / 2);                  // kickScalar with a(t) before the drift
     if (ex) tail(h, T_VV_DRIFT, 0, 0, w0);     // driftScaleFactor
+    h->pdl_now = h->pdl; // the fused sweeps and their tails overlap their launches
     for (int64_t k = 0; k < total; ++k) {
       const size_t i = (size_t)(k % (int64_t)S);
       const double w = wof(i);
@@ -335,6 +364,7 @@ template <class R, int NS> struct EvolveVV {
         tail(h, fl, h->sweep_blocks, w, wn, i + 1 == S ? k / (int64_t)S : -1);
       }
     }
+    h->pdl_now = false;
   }
 };
 
@@ -518,6 +548,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   }
   h->bz = 64;
   h->by = h->shape == 1 ? 16 : 8;
+  if (const char *env = std::getenv("CLB_PDL")) h->pdl = std::atoi(env) != 0;
   const size_t box_bytes = (size_t)(h->bz + 2 * (16 / (int)h->esz)) * (size_t)(h->by + 2) * h->esz;
   const size_t slot = ((box_bytes + 127) / 128) * 128;
   const size_t stage_bytes = (size_t)h->NS * 2 * slot;

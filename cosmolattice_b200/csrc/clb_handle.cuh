@@ -36,6 +36,8 @@ struct clb_handle {
   int S = 3;          // sweep ring stages
   int rs = 0;         // FP32 split storage: current reference slot in DevState
   int shape = 0;      // sweep block shape: 0 ShapeW, 1 ShapeQ, 2 ShapeH (clb_sweep.cuh)
+  bool pdl = true;     // programmatic dependent launch in the fused VV loop (CLB_PDL=0: off)
+  bool pdl_now = false; // set while the fused loop issues its sweeps and tails
   int bz = 64, by = 8; // sites per block tile in z and y
   size_t sweep_smem = 0;
   int *d_err = nullptr; // set by a sweep whose bounded wait gave up

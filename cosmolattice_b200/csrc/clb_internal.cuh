@@ -102,6 +102,13 @@ __device__ __forceinline__ double ipow_d(double x, int n)
   return r;
 }
 
+// Programmatic dependent launch (sm_90+): griddep_wait blocks until the preceding kernel in the
+// stream has completed and its writes are visible (a no-op when the launch has no programmatic
+// dependency); griddep_launch lets the next kernel, if launched with the attribute, start its
+// independent prologue once every block of this one has signalled or exited.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Deterministic block reduction of NV per-thread values; thread 0 of the block gets the sums.
 template <int NV, int NT>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], double *smem /* [NT/32][NV] */)

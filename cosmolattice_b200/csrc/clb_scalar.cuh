@@ -321,6 +321,18 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---- tail: fixed-order reduction of the block partials and the scale-factor update --------------
+// x^e of the scale-factor bookkeeping.  The exponents are alpha + k; alpha is an integer in every
+// model here (lphi4.h:125), and an integer power is a short multiply chain where pow() is a long
+// serial one on the single tail thread (both within an ulp of x^e).
+#ifndef CLB_TAIL_IPOW
+#define CLB_TAIL_IPOW 1
+#endif
+__device__ __forceinline__ double apow(double x, double e)
+{
+  if (CLB_TAIL_IPOW && e == rint(e) && fabs(e) <= 8.0) return ipow_d(x, (int)e);
+  return pow(x, e);
+}
+
 __device__ __forceinline__ double sf_kernel(const DevState &s, const SFParams &p)
 {
   // ScaleFactorKernels::get (scalefactorkernels.h:73-77), scalar singlets:
@@ -330,7 +342,7 @@ __device__ __forceinline__ double sf_kernel(const DevState &s, const SFParams &p
   const double Egs = __dmul_rn(0.5 * s.grad2AvI, ipow_d(s.aI, -2));
   const double br = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(al - 2, Eks), __dmul_rn(al, Egs)), __dmul_rn(al - 1, 0.0)),
                               __dmul_rn(al + 1, s.potAvI));
-  return __dmul_rn(__dmul_rn(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
+  return __dmul_rn(__dmul_rn(apow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
 }
 
 // Scale-factor bookkeeping of one tail (the flags of TailOp, in schedule order) given the volume
@@ -373,7 +385,7 @@ __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const 
     const double rho = __dadd_rn(__dadd_rn(__dmul_rn(0.5 * s.pi2AvI, ipow_d(s.aI, -6)),
                                            __dmul_rn(0.5 * s.grad2AvI, ipow_d(s.aI, -2))),
                                  s.potAvI);
-    const double RHS = __dmul_rn(__dmul_rn(pow(s.aI, 2 * p.alpha + 2) / 3., p.fm2), rho);
+    const double RHS = __dmul_rn(__dmul_rn(apow(s.aI, 2 * p.alpha + 2) / 3., p.fm2), rho);
     s.aDotI = sqrt(RHS);
   }
   if (fl & T_VV_KICK_ONE) s.aDotI = __dadd_rn(s.aDotSI, __dmul_rn(__dmul_rn(dt / 2, sf_kernel(s, p)), op.w));
@@ -396,9 +408,9 @@ __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const 
     s.aI = __dadd_rn(s.aI, __dmul_rn(__dmul_rn(dt, s.aDotSI), op.w2));
     s.aSI = (s.aIM + s.aI) / 2.0;
   }
-  s.drift_p = pow(s.aSI, p.alpha - 3);
-  s.kick_A = pow(s.aI, 1 + p.alpha);
-  s.kick_B = pow(s.aI, 3 + p.alpha);
+  s.drift_p = apow(s.aSI, p.alpha - 3);
+  s.kick_A = apow(s.aI, 1 + p.alpha);
+  s.kick_B = apow(s.aI, 3 + p.alpha);
   if (!isfinite(s.aI) || !isfinite(s.aDotI) || !isfinite(s.aDotSI) || !isfinite(s.pi2AvI) ||
       !isfinite(s.grad2AvI) || !isfinite(s.potAvI))
     s.status = 1;
@@ -412,6 +424,9 @@ static __global__ void __launch_bounds__(kTailThreads)
     k_tail(const double *__restrict__ partials, TailOp op, DevState *__restrict__ st, SFParams p)
 {
   __shared__ double smem[(kTailThreads / 32) * kRedSlots];
+  griddep_wait();   // the sweep's partials and state are complete
+  griddep_launch(); // the next sweep may set up its barriers meanwhile
+
   double v[kRedSlots] = {0, 0, 0};
   if (op.nblocks > 0) {
     double w[4][kRedSlots] = {};

@@ -202,6 +202,18 @@ __global__ void __launch_bounds__(SH::THREADS)
   const int nplanes = x1 - x0 + 2;                     // planes x0-1 .. x1
   const uint32_t tx_bytes = (uint32_t)(NS * NB * TG::BYTES);
 
+  // Independent of the preceding kernels: barrier set-up and tensor-map prefetch.  Everything after
+  // griddep_wait may read what they wrote (state arrays, DevState) or overwrite what they read
+  // (partials, the DevState reference slot).
+  if (tid == 0) {
+    abort_flag = 0;
+    prefetch_tensormap(&tmf);
+    if (LOADP) prefetch_tensormap(&tmp);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  griddep_wait();
+
   if (x0 >= x1) { // block-uniform: no planes, but its partial row must not hold stale sums
     if (RED && tid == 0) {
       const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
@@ -276,13 +288,6 @@ __global__ void __launch_bounds__(SH::THREADS)
     return LOADP ? drift1(fv, box(s, f, 1)[o]) : fv;
   };
 
-  if (tid == 0) {
-    abort_flag = 0;
-    prefetch_tensormap(&tmf);
-    if (LOADP) prefetch_tensormap(&tmp);
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
-    fence_mbar_init();
-  }
   __syncthreads();
   if (tid == 0)
     for (int j = 0; j < min(S, nplanes); ++j) issue(j);
@@ -476,6 +481,7 @@ __global__ void __launch_bounds__(SH::THREADS)
           if (LOADP) piC[f][k] = piN[f][k];
         }
     }
+    griddep_launch(); // planes done: the tail may be scheduled
     if (RED) {
       if constexpr (SPLIT) {
         // sum (pi_r + p)^2 = n pi_r^2 + 2 pi_r sum p + sum p^2;  sum V = n V_r + sum (V - V_r)
