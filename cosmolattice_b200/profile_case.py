@@ -4,6 +4,8 @@
     python -m cosmolattice_b200.profile_case --model lphi4U1 --N 128 --steps 5
     python -m cosmolattice_b200.profile_case --model lphi4SU2U1 --N 96 --steps 3 [--precision fp32]
     python -m cosmolattice_b200.profile_case --model batch --members 64 --steps 5 --precision fp32
+    python -m cosmolattice_b200.profile_case --model lphi4U1 --N 96 --steps 4 --mode adjoint
+    python -m cosmolattice_b200.profile_case --model lphi4SU2U1 --N 64 --steps 2 --mode tangent
 
 Gauge models and the batch run on seeded synthetic states (no FFT initial conditions): small
 Gaussian noise about the homogeneous point, links near unity.
@@ -85,6 +87,9 @@ def main(argv=None):
     ap.add_argument("--evolver", default="VV2")
     ap.add_argument("--model", default="lphi4", choices=["lphi4", "lphi4U1", "lphi4SU2U1", "batch"])
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--mode", default="evolve", choices=["evolve", "adjoint", "tangent"],
+                    help="adjoint: clb_forward + clb_backward (lphi4U1); tangent: the tangent-linear "
+                         "form along g_SU2 (lphi4SU2U1)")
     args = ap.parse_args(argv)
     if args.model == "batch":
         return _batch(args)
@@ -92,12 +97,21 @@ def main(argv=None):
         m, rp, f, p = _gauge_case(args)
         lat = Lattice(m, rp, precision=args.precision)
         lat.set_state(f, p, {"aI": 1.0, "aSI": 1.0, "aIM": 1.0, "aDotI": 0.5, "aDotSI": 0.5})
+        if args.mode == "tangent":
+            lat.tangent_begin([0, 0, 0, 0, 1, 0])
         lat.initialize()
         t0 = time.perf_counter()
-        lat.evolve(args.steps)
+        if args.mode == "adjoint":
+            lat.forward(args.steps, max(1, args.steps // 2), [0, 0, 1, 1, 0])
+            lat.backward(True)
+        else:
+            lat.evolve(args.steps)
+            if args.mode == "tangent":
+                lat.tangent_observable([0] * 6 + [1] * 4)
         dt = time.perf_counter() - t0
         lat.close()
-        print(f"{args.model} N={args.N} steps={args.steps} {args.precision}: {dt * 1e3 / args.steps:.3f} ms/step")
+        print(f"{args.model} {args.mode} N={args.N} steps={args.steps} {args.precision}: "
+              f"{dt * 1e3 / args.steps:.3f} ms/step")
         return
     N = args.N
     par = ParameterParser(params={"N": N, "kIR": 64.0 / N, "dt": 0.01, "evolver": args.evolver, "expansion": "true",
