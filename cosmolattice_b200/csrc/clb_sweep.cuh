@@ -342,8 +342,12 @@ __global__ void __launch_bounds__(SH::THREADS)
       R outp[NS][VZ];
       if constexpr (SPLIT) {
         // FP32 fluctuations about the FP64 references: FP32 arithmetic throughout, per-plane FP32
-        // partial sums folded into FP64 accumulators (the reference terms are added at the end)
+        // partial sums folded into FP64 accumulators (the reference terms are added at the end).
+        // Not bound to the reference's operation order: the Laplacian is (sum of the six
+        // neighbours) - 6 c with 1/dx^2 folded into the kick coefficient, and the gradient sum is
+        // scaled once per plane.
         float s_p[NS], s_p2 = 0.f, s_g2 = 0.f, s_dv = 0.f;
+        const float KAd = KA * inv_dx2;
 #pragma unroll
         for (int f = 0; f < NS; ++f) s_p[f] = 0.f;
 #pragma unroll
@@ -362,14 +366,14 @@ __global__ void __launch_bounds__(SH::THREADS)
             const float zn = k + 1 < VZ ? cur[f][k + 1 < VZ ? k + 1 : 0] : zpv[f];
             const float zm = k > 0 ? cur[f][k > 0 ? k - 1 : 0] : zmv[f];
             if (KICK) {
-              const float lap = inv_dx2 * ((((nxt[f][k] + prev[f][k]) - 2.f * c) + ((yp[f][k] + ym[f][k]) - 2.f * c)) +
-                                           ((zn + zm) - 2.f * c));
+              const float nsum = ((nxt[f][k] + prev[f][k]) + (yp[f][k] + ym[f][k])) + (zn + zm);
+              const float lap = fmaf(-6.f, c, nsum); // times 1/dx^2 in KAd
               float ddv;
               if constexpr (NS == 1)
                 ddv = spc.ddV(c);
               else
                 ddv = (float)(Lphi4<double, NS>::dV(f, cd, a.c0, a.q) - rf.dV[f]);
-              const float K = KA * lap - KB * ddv;
+              const float K = KAd * lap - KB * ddv;
               const float pm = fmaf(h1f, K, piC[f][k]);
               outp[f][k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
               if ((RED & 1) && vk) {
@@ -382,7 +386,7 @@ __global__ void __launch_bounds__(SH::THREADS)
             }
             if ((RED & 2) && vk) {
               const float gx = nxt[f][k] - c, gy = yp[f][k] - c, gz = zn - c;
-              s_g2 += (gx * gx + gy * gy + gz * gz) * inv_dx2;
+              s_g2 += gx * gx + gy * gy + gz * gz; // times 1/dx^2 per plane
             }
           }
           if ((RED & 2) && vk) {
@@ -396,7 +400,7 @@ __global__ void __launch_bounds__(SH::THREADS)
 #pragma unroll
           for (int f = 0; f < NS; ++f) acc_p[f] += (double)s_p[f];
           acc_pi2 += (double)s_p2;
-          acc_g2 += (double)s_g2;
+          acc_g2 += (double)s_g2 * a.inv_dx2;
           acc_v += (double)s_dv;
           cnt += nvalid;
         }
