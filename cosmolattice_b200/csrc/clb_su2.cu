@@ -29,6 +29,7 @@ struct SU2Sector {
   State *d_st = nullptr;
   double *d_part = nullptr, *d_sums = nullptr;
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
+  void *ph = nullptr;        // U(1) link phases (12 x N^3, storage type), kept by the drifts
   int64_t steps_since_unitarize = 0;
   Params prm{};
   // tangent-linear form: d(state) along the coupling direction tan_cd, active while tangent
@@ -109,7 +110,8 @@ template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const K
   const S *f = static_cast<const S *>(u->f);
   S *p = static_cast<S *>(u->p);
 #define CLB_SU2K(NK, RF, RP)                                                                                            \
-  CLB_LAUNCH(h, kind, k_kick<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, p, u->prm, kc, u->d_st, u->d_part))
+  CLB_LAUNCH(h, kind, k_kick<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, p, u->prm, kc, u->d_st, u->d_part, \
+                                                                               static_cast<const S *>(u->ph)))
   if (nk == 0) {
     if (rf && rp)
       CLB_SU2K(0, true, true);
@@ -187,7 +189,8 @@ template <class S> void drift_tan_t(clb_handle *h, double w, bool lf)
   CLB_LAUNCH(h, K_U1_DRIFT,
              k_drift_tan<S><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<S *>(u->f), static_cast<S *>(u->df),
                                                                static_cast<const S *>(u->p), static_cast<const S *>(u->dp),
-                                                               u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd));
+                                                               u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd,
+                                                               static_cast<S *>(u->ph)));
 }
 
 void drift(clb_handle *h, double w, bool lf)
@@ -203,11 +206,13 @@ void drift(clb_handle *h, double w, bool lf)
   if (u->fp32)
     CLB_LAUNCH(h, K_U1_DRIFT, k_drift<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f),
                                                                                  static_cast<const float *>(u->p),
-                                                                                 u->prm, w, lf ? 1 : 0, u->d_st));
+                                                                                 u->prm, w, lf ? 1 : 0, u->d_st,
+                                                                                 static_cast<float *>(u->ph)));
   else
     CLB_LAUNCH(h, K_U1_DRIFT, k_drift<double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<double *>(u->f),
                                                                                   static_cast<const double *>(u->p),
-                                                                                  u->prm, w, lf ? 1 : 0, u->d_st));
+                                                                                  u->prm, w, lf ? 1 : 0, u->d_st,
+                                                                                  static_cast<double *>(u->ph)));
 }
 
 // FP32 form: after the drift of every kUnitarizeEvery-th step the links are projected back to
@@ -283,6 +288,7 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   ok = ok && cudaMalloc(&u->p, NP * h->n3 * u->esz) == cudaSuccess;
   ok = ok && cudaMemset(u->f, 0, NF * h->n3 * u->esz) == cudaSuccess;
   ok = ok && cudaMemset(u->p, 0, NP * h->n3 * u->esz) == cudaSuccess;
+  ok = ok && cudaMalloc(&u->ph, 12 * h->n3 * u->esz) == cudaSuccess;
   if (u->fp32) ok = ok && cudaMalloc(&u->d_stage, h->n3 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_st, sizeof(State)) == cudaSuccess;
   ok = ok && cudaMalloc(&u->d_part, (size_t)kSU2Blocks * kMeas * sizeof(double)) == cudaSuccess;
@@ -312,7 +318,8 @@ __attribute__((visibility("hidden"))) void su2_destroy(clb_handle *h)
   SU2Sector *u = h->su2;
   if (!u) return;
   free_tangent(u);
-  for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums, (void *)u->d_stage})
+  for (void *q : {(void *)u->f, (void *)u->p, (void *)u->d_st, (void *)u->d_part, (void *)u->d_sums, (void *)u->d_stage,
+                  u->ph})
     if (q) cudaFree(q);
   delete u;
   h->su2 = nullptr;
@@ -336,6 +343,14 @@ __attribute__((visibility("hidden"))) int su2_set_state(clb_handle *h, const dou
       if (e == cudaSuccess) k_convert<double, float><<<kSU2Blocks, 256, 0, h->stream>>>(u->d_stage, dst, h->n3);
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }
+  }
+  if (e == cudaSuccess) {
+    // the link phases of the new A
+    if (u->fp32)
+      k_phases<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<const float *>(u->f), static_cast<float *>(u->ph), u->prm);
+    else
+      k_phases<double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<const double *>(u->f), static_cast<double *>(u->ph), u->prm);
+    e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");

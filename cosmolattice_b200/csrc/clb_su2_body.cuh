@@ -8,6 +8,8 @@
 
 #include "clb_su2.cuh"
 
+#include <type_traits>
+
 namespace clb {
 namespace su2d {
 
@@ -65,6 +67,9 @@ template <class T> __device__ __forceinline__ T ipw(T x, int n)
 template <class S, class T> struct Site {
   const S *f;
   const S *df;
+  // U(1) link phases exp(-i dx g A_i) for g = gQ of phi (C) and of Phi (D), kept by the drift:
+  // [4 i + 2 (0 C, 1 D) + (0 cos, 1 sin)] x n3; null: formed from A here
+  const S *ph;
   const Params *a;
   size_t s;
   long long op[3], om[3];
@@ -84,6 +89,20 @@ template <class S, class T> struct Site {
   }
   __device__ __forceinline__ D2<T> dbl(size_t t) const { return D2<T>{C2<T>{F(3, t), F(4, t)}, C2<T>{F(5, t), F(6, t)}}; }
   __device__ __forceinline__ C2<T> cs(size_t t) const { return C2<T>{F(1, t), F(2, t)}; }
+  // the stored phases when the arithmetic type is the storage type (the same cos and sin of the
+  // same argument, formed by the drift), else formed here
+  __device__ __forceinline__ C2<T> phaseCD(int which, int i, size_t t) const
+  {
+    if constexpr (std::is_same<S, T>::value) {
+      if (ph) {
+        const size_t b = (size_t)(4 * i + 2 * which) * a->n3 + t;
+        return C2<T>{ph[b], ph[b + a->n3]};
+      }
+    }
+    return phase(which == 0 ? gC : gD, i, t);
+  }
+  __device__ __forceinline__ C2<T> phaseC(int i, size_t t) const { return phaseCD(0, i, t); }
+  __device__ __forceinline__ C2<T> phaseD(int i, size_t t) const { return phaseCD(1, i, t); }
   __device__ __forceinline__ C2<T> phase(T g, int i, size_t t) const
   {
     const T th = (-dx * g) * F(7 + i, t);
@@ -107,8 +126,8 @@ template <class S, class T> struct Site {
   __device__ __forceinline__ size_t pl(int i) const { return s + op[i]; }
   __device__ __forceinline__ size_t mi(int i) const { return s + om[i]; }
   __device__ __forceinline__ size_t plmi(int i, int j) const { return i == j ? s : s + op[i] + om[j]; }
-  __device__ __forceinline__ D2<T> wD(int i) const { return dscale(phase(gD, i, s), qapply(link(i, s), dbl(pl(i)))); }
-  __device__ __forceinline__ C2<T> wC(int i) const { return cmul(phase(gC, i, s), cs(pl(i))); }
+  __device__ __forceinline__ D2<T> wD(int i) const { return dscale(phaseD(i, s), qapply(link(i, s), dbl(pl(i)))); }
+  __device__ __forceinline__ C2<T> wC(int i) const { return cmul(phaseC(i, s), cs(pl(i))); }
   __device__ __forceinline__ T lapl(int comp) const
   {
     const T c = F(comp, s);
@@ -133,6 +152,7 @@ template <class S, class T> __device__ __forceinline__ Site<S, T> make_site(cons
   Site<S, T> v;
   v.f = f;
   v.df = nullptr;
+  v.ph = nullptr;
   v.a = &a;
   v.s = s;
   v.dx = (T)a.dx;
@@ -161,6 +181,7 @@ __device__ __forceinline__ Site<S, Tan<S>> make_site_tan(const S *f, const S *df
   Site<S, T> v;
   v.f = f;
   v.df = df;
+  v.ph = nullptr;
   v.a = &a;
   v.s = s;
   v.dx = T(a.dx);
@@ -180,8 +201,8 @@ template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<
 {
   C2<T> plus{0, 0}, minus{0, 0};
   for (int d = 0; d < 3; ++d) {
-    const C2<T> w = cmul(v.phase(v.gC, d, v.s), v.cs(v.pl(d)));
-    const C2<T> m = cmul(conj_(v.phase(v.gC, d, v.mi(d))), v.cs(v.mi(d)));
+    const C2<T> w = cmul(v.phaseC(d, v.s), v.cs(v.pl(d)));
+    const C2<T> m = cmul(conj_(v.phaseC(d, v.mi(d))), v.cs(v.mi(d)));
     plus = d == 0 ? w : cadd(plus, w);
     minus = d == 0 ? m : cadd(minus, m);
   }
@@ -194,9 +215,9 @@ template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S
 {
   D2<T> plus{}, minus{};
   for (int d = 0; d < 3; ++d) {
-    const D2<T> w = qapply(v.link(d, v.s), dscale(v.phase(v.gD, d, v.s), v.dbl(v.pl(d))));
+    const D2<T> w = qapply(v.link(d, v.s), dscale(v.phaseD(d, v.s), v.dbl(v.pl(d))));
     const size_t sm = v.mi(d);
-    const D2<T> m = qapply(qdag(v.link(d, sm)), dscale(conj_(v.phase(v.gD, d, sm)), v.dbl(sm)));
+    const D2<T> m = qapply(qdag(v.link(d, sm)), dscale(conj_(v.phaseD(d, sm)), v.dbl(sm)));
     if (d == 0) {
       plus = w;
       minus = m;
@@ -300,7 +321,7 @@ template <class S, class T> __device__ __forceinline__ T dGrad2(const Site<S, T>
   const D2<T> c = v.dbl(v.s);
   T acc = 0;
   for (int j = 0; j < 3; ++j) {
-    const D2<T> w = qapply(v.link(j, v.s), dscale(v.phase(v.gD, j, v.s), v.dbl(v.pl(j))));
+    const D2<T> w = qapply(v.link(j, v.s), dscale(v.phaseD(j, v.s), v.dbl(v.pl(j))));
     const C2<T> du0 = csub(w.u, c.u), dv0 = csub(w.v, c.v);
     const C2<T> du{du0.re / v.dx, du0.im / v.dx}, dv{dv0.re / v.dx, dv0.im / v.dx};
     const T n2 = (du.re * du.re + du.im * du.im) + (dv.re * dv.re + dv.im * dv.im);
@@ -361,14 +382,15 @@ __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c
 template <class S, int NK, bool RF, bool RP>
 __global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
-           double *__restrict__ partials)
+           double *__restrict__ partials, const S *__restrict__ ph)
 {
   __shared__ double smem[(128 / 32) * kRed];
   const State st = *stp;
   double acc[kRed];
   for (int k = 0; k < kRed; ++k) acc[k] = 0;
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
-    const Site<S, S> v = make_site<S, S>(f, a, s);
+    Site<S, S> v = make_site<S, S>(f, a, s);
+    v.ph = ph;
     S q[NP];
     for (int c = 0; c < NP; ++c) q[c] = p[(size_t)c * a.n3 + s];
     if (NK > 0) {
@@ -413,9 +435,29 @@ __device__ __forceinline__ Q4<double> qexp(double p1, double p2, double p3)
   const double sn = sin(n) / n;
   return Q4<double>{cos(n), sn * p1, sn * p2, sn * p3};
 }
+// The U(1) link phases of A_i(x) for both couplings, exactly as Site::phase forms them, into the
+// phase arrays the kick reads.
+template <class S> __device__ __forceinline__ void put_phases(S *__restrict__ ph, const Params &a, int i, size_t s, S A)
+{
+  const size_t n3 = a.n3;
+#pragma unroll
+  for (int which = 0; which < 2; ++which) {
+    const S th = (-(S)a.dx * (S)(which == 0 ? a.gC : a.gD)) * A;
+    const size_t b = (size_t)(4 * i + 2 * which) * n3 + s;
+    ph[b] = cos(th);
+    ph[b + n3] = sin(th);
+  }
+}
+template <class S> __global__ void __launch_bounds__(256) k_phases(const S *__restrict__ f, S *__restrict__ ph, Params a)
+{
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x)
+    for (int i = 0; i < 3; ++i) put_phases(ph, a, i, s, f[(size_t)(7 + i) * a.n3 + s]);
+}
+
 template <class S>
 __global__ void __launch_bounds__(256)
-    k_drift(S *__restrict__ f, const S *__restrict__ p, Params a, double w, int lf, const State *__restrict__ stp)
+    k_drift(S *__restrict__ f, const S *__restrict__ p, Params a, double w, int lf, const State *__restrict__ stp,
+            S *__restrict__ ph)
 {
   const double dt = a.dt, p3 = stp->p3, p1 = stp->p1;
   const double cC = lf ? p3 * dt : p3 * dt * w;
@@ -426,8 +468,11 @@ __global__ void __launch_bounds__(256)
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     f[s] = (S)((double)f[s] + p3 * (dtw * (double)p[s]));
     for (int c = 1; c < 7; ++c) f[c * n3 + s] = (S)((double)f[c * n3 + s] + cC * (double)p[c * n3 + s]);
-    for (int i = 0; i < 3; ++i)
-      f[(7 + i) * n3 + s] = (S)((double)f[(7 + i) * n3 + s] + cA * (double)p[(7 + i) * n3 + s] * 1.0);
+    for (int i = 0; i < 3; ++i) {
+      const S A = (S)((double)f[(7 + i) * n3 + s] + cA * (double)p[(7 + i) * n3 + s] * 1.0);
+      f[(7 + i) * n3 + s] = A;
+      put_phases(ph, a, i, s, A);
+    }
     for (int i = 0; i < 3; ++i) {
       const size_t pb = (size_t)(10 + 3 * i) * n3 + s, fb = (size_t)(10 + 4 * i) * n3 + s;
       const Q4<double> E = qexp(cG * (double)p[pb], cG * (double)p[pb + n3], cG * (double)p[pb + 2 * n3]);
@@ -670,7 +715,7 @@ __device__ __forceinline__ Q4<Tan<double>> qexp_tan(Tan<double> p1, Tan<double> 
 template <class S>
 __global__ void __launch_bounds__(256)
     k_drift_tan(S *__restrict__ f, S *__restrict__ df, const S *__restrict__ p, const S *__restrict__ dp, Params a,
-                double w, int lf, const TState *__restrict__ stp, CoupDot cd)
+                double w, int lf, const TState *__restrict__ stp, CoupDot cd, S *__restrict__ ph)
 {
   using T = Tan<double>;
   const double dt = a.dt;
@@ -689,8 +734,10 @@ __global__ void __launch_bounds__(256)
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     put(f, df, s, ld(f, df, s) + p3 * (dtw * ld(p, dp, s)));
     for (int c = 1; c < 7; ++c) put(f, df, c * n3 + s, ld(f, df, c * n3 + s) + cC * ld(p, dp, c * n3 + s));
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) {
       put(f, df, (7 + i) * n3 + s, ld(f, df, (7 + i) * n3 + s) + cA * ld(p, dp, (7 + i) * n3 + s) * 1.0);
+      put_phases(ph, a, i, s, f[(7 + i) * n3 + s]); // the plain kicks after the tangent form read them
+    }
     for (int i = 0; i < 3; ++i) {
       const size_t pb = (size_t)(10 + 3 * i) * n3 + s, fb = (size_t)(10 + 4 * i) * n3 + s;
       const Q4<T> E = qexp_tan(cG * ld(p, dp, pb), cG * ld(p, dp, pb + n3), cG * ld(p, dp, pb + 2 * n3));
