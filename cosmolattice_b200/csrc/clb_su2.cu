@@ -10,6 +10,7 @@
 #include "clb_su2.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -30,6 +31,7 @@ struct SU2Sector {
   double *d_part = nullptr, *d_sums = nullptr;
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   void *ph = nullptr;        // U(1) link phases (12 x N^3, storage type), kept by the drifts
+  bool split = true;         // kick sweeps in two halves (CLB_SU2_SPLIT=0: one sweep)
   int64_t steps_since_unitarize = 0;
   Params prm{};
   // tangent-linear form: d(state) along the coupling direction tan_cd, active while tangent
@@ -109,9 +111,20 @@ template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const K
   const int kind = nk == 0 ? K_U1_REDUCE : K_U1_KICK;
   const S *f = static_cast<const S *>(u->f);
   S *p = static_cast<S *>(u->p);
+  // kick sweeps run as two halves (sectors S, phi, Phi, A; then SU(2)), which hold fewer registers
+  // than one sweep over every sector; reduction-only sweeps run whole
+#define CLB_SU2K1(NK, RF, RP, SECT)                                                                                     \
+  CLB_LAUNCH(h, kind, k_kick<S, NK, RF, RP, SECT><<<kSU2Blocks, 128, 0, h->stream>>>(                                  \
+                          f, p, u->prm, kc, u->d_st, u->d_part, static_cast<const S *>(u->ph)))
 #define CLB_SU2K(NK, RF, RP)                                                                                            \
-  CLB_LAUNCH(h, kind, k_kick<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, p, u->prm, kc, u->d_st, u->d_part, \
-                                                                               static_cast<const S *>(u->ph)))
+  do {                                                                                                                 \
+    if (NK > 0 && u->split) {                                                                                          \
+      CLB_SU2K1(NK, RF, RP, 1);                                                                                        \
+      CLB_SU2K1(NK, RF, RP, 2);                                                                                        \
+    } else {                                                                                                           \
+      CLB_SU2K1(NK, RF, RP, 0);                                                                                        \
+    }                                                                                                                  \
+  } while (0)
   if (nk == 0) {
     if (rf && rp)
       CLB_SU2K(0, true, true);
@@ -133,6 +146,7 @@ template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const K
       CLB_SU2K(2, false, false);
   }
 #undef CLB_SU2K
+#undef CLB_SU2K1
 }
 
 template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)
@@ -189,8 +203,7 @@ template <class S> void drift_tan_t(clb_handle *h, double w, bool lf)
   CLB_LAUNCH(h, K_U1_DRIFT,
              k_drift_tan<S><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<S *>(u->f), static_cast<S *>(u->df),
                                                                static_cast<const S *>(u->p), static_cast<const S *>(u->dp),
-                                                               u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd,
-                                                               static_cast<S *>(u->ph)));
+                                                               u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd));
 }
 
 void drift(clb_handle *h, double w, bool lf)
@@ -283,6 +296,7 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   u->prm = su2_params(h);
   u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
   u->esz = u->fp32 ? sizeof(float) : sizeof(double);
+  if (const char *env = std::getenv("CLB_SU2_SPLIT")) u->split = std::atoi(env) != 0;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;
   ok = ok && cudaMalloc(&u->p, NP * h->n3 * u->esz) == cudaSuccess;
@@ -765,8 +779,15 @@ __attribute__((visibility("hidden"))) int su2_tangent_observable(clb_handle *h, 
 
 __attribute__((visibility("hidden"))) int su2_tangent_end(clb_handle *h)
 {
-  cudaError_t e = cudaStreamSynchronize(h->stream);
-  free_tangent(h->su2);
+  SU2Sector *u = h->su2;
+  // the tangent form's kicks form the link phases themselves; the plain kicks read them again
+  if (u->fp32)
+    k_phases<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<const float *>(u->f), static_cast<float *>(u->ph), u->prm);
+  else
+    k_phases<double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<const double *>(u->f), static_cast<double *>(u->ph), u->prm);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  free_tangent(u);
   return e == cudaSuccess ? CLB_OK : h->cuda_fail(e, "clb_tangent_end");
 }
 

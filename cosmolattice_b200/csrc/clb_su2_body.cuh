@@ -239,57 +239,64 @@ template <class T> struct Coef {
   T A, B, B2, G;
 };
 
-template <class S, class T> __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP])
+// SECT: 0 all components, 1 S, phi, Phi and A (K[0..9]), 2 the SU(2) field (K[10..18]).
+template <int SECT = 0, class S, class T>
+__device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP])
 {
   const Params &a = *v.a;
   const size_t s = v.s;
   const T A = C.A, B = C.B, B2 = C.B2, G = C.G;
   const T qG = v.qG, qH = v.qH, c4 = v.c4, rfo2 = (T)a.rfo2;
-  const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
-  K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
-  const C2<T> cl = covLapC(v);
-  const T ndC = 4 * qH * ipw(nD, 2) * nC;
-  K[1] = A * cl.re - B2 * (ndC / nC * v.F(1, s));
-  K[2] = A * cl.im - B2 * (ndC / nC * v.F(2, s));
-  T dl[4];
-  covLapD(v, dl);
-  const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
-  for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (ndD / nD * v.F(3 + c, s));
-  const D2<T> D0 = v.dbl(s);
-  const C2<T> C0 = v.cs(s);
-  for (int i = 0; i < 3; ++i) {
-    const T lap = v.lapl(7 + i);
-    T grad = 0;
-    for (int j = 0; j < 3; ++j) {
-      const T g0 = v.fd(7 + j, s, v.pl(i));
-      const T g1 = v.fd(7 + j, v.mi(j), v.plmi(i, j));
-      const T t = (g0 - g1) / v.dx;
-      grad = j == 0 ? t : grad + t;
-    }
-    const T Jc = v.gC * cmul(conj_(v.wC(i)), C0).im;
-    const T Jd = v.gD * sprod(v.wD(i), D0).im;
-    const T J = T(2.0) / v.dx * rfo2 * (Jc + Jd);
-    K[7 + i] = G * (lap - grad) - A * J;
-  }
-  const T normGrad = ipw(T(1) / v.dx, 3) / v.gS * G;
-  const T normSrc = (T(1) / v.dx) * A;
-  for (int i = 0; i < 3; ++i) {
-    T gr[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
-    bool first = true;
-    for (int j = 0; j < 3; ++j) {
-      if (j == i) continue;
-      const Q4<T> P = v.plaq(i, j), Pb = v.plaqBack(i, j);
-      const T pv[3] = {P.x, P.y, P.z}, bv[3] = {Pb.x, Pb.y, Pb.z};
-      for (int c = 0; c < 3; ++c) {
-        gr[c] = first ? pv[c] : gr[c] + pv[c];
-        gb[c] = first ? bv[c] : gb[c] + bv[c];
+  if constexpr (SECT != 2) {
+    const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
+    K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
+    const C2<T> cl = covLapC(v);
+    const T ndC = 4 * qH * ipw(nD, 2) * nC;
+    K[1] = A * cl.re - B2 * (ndC / nC * v.F(1, s));
+    K[2] = A * cl.im - B2 * (ndC / nC * v.F(2, s));
+    T dl[4];
+    covLapD(v, dl);
+    const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
+    for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (ndD / nD * v.F(3 + c, s));
+    const D2<T> D0 = v.dbl(s);
+    const C2<T> C0 = v.cs(s);
+    for (int i = 0; i < 3; ++i) {
+      const T lap = v.lapl(7 + i);
+      T grad = 0;
+      for (int j = 0; j < 3; ++j) {
+        const T g0 = v.fd(7 + j, s, v.pl(i));
+        const T g1 = v.fd(7 + j, v.mi(j), v.plmi(i, j));
+        const T t = (g0 - g1) / v.dx;
+        grad = j == 0 ? t : grad + t;
       }
-      first = false;
+      const T Jc = v.gC * cmul(conj_(v.wC(i)), C0).im;
+      const T Jd = v.gD * sprod(v.wD(i), D0).im;
+      const T J = T(2.0) / v.dx * rfo2 * (Jc + Jd);
+      K[7 + i] = G * (lap - grad) - A * J;
     }
-    const D2<T> W = v.wD(i);
-    for (int c = 0; c < 3; ++c) {
-      const T J = rfo2 / 2 * (v.gS * sprod(W, isig(c, D0)).re);
-      K[10 + 3 * i + c] = -normGrad * (gr[c] - gb[c]) - normSrc * J;
+  }
+  if constexpr (SECT != 1) {
+    const D2<T> Dg = v.dbl(s);
+    const T normGrad = ipw(T(1) / v.dx, 3) / v.gS * G;
+    const T normSrc = (T(1) / v.dx) * A;
+    for (int i = 0; i < 3; ++i) {
+      T gr[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
+      bool first = true;
+      for (int j = 0; j < 3; ++j) {
+        if (j == i) continue;
+        const Q4<T> P = v.plaq(i, j), Pb = v.plaqBack(i, j);
+        const T pv[3] = {P.x, P.y, P.z}, bv[3] = {Pb.x, Pb.y, Pb.z};
+        for (int c = 0; c < 3; ++c) {
+          gr[c] = first ? pv[c] : gr[c] + pv[c];
+          gb[c] = first ? bv[c] : gb[c] + bv[c];
+        }
+        first = false;
+      }
+      const D2<T> W = v.wD(i);
+      for (int c = 0; c < 3; ++c) {
+        const T J = rfo2 / 2 * (v.gS * sprod(W, isig(c, Dg)).re);
+        K[10 + 3 * i + c] = -normGrad * (gr[c] - gb[c]) - normSrc * J;
+      }
     }
   }
 }
@@ -344,25 +351,30 @@ template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v
   const T t10 = 2 - 2 * v.plaq(1, 0).w, t20 = 2 - 2 * v.plaq(2, 0).w, t21 = 2 - 2 * v.plaq(2, 1).w;
   return c * (t10 + (t20 + t21));
 }
-// momentum sums of the five sectors (FP64) from momentum values q[19]
-template <class R> __device__ __forceinline__ void pi2s(const R *qs, double out[5])
+// momentum sums of the five sectors (FP64) from momentum values q[19]; G1 = 4: the first four
+// sectors only (q[0..9] read), G0 = 4: the SU(2) sector only (q[10..18] read)
+template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s(const R *qs, double out[5])
 {
   double q[NP];
-  for (int c = 0; c < NP; ++c) q[c] = (double)qs[c];
-  out[0] = q[0] * q[0];
-  out[1] = q[1] * q[1] + q[2] * q[2];
-  out[2] = ((q[3] * q[3] + q[4] * q[4]) + q[5] * q[5]) + q[6] * q[6];
-  out[3] = (q[7] * q[7] + q[8] * q[8]) + q[9] * q[9];
-  double acc = 0;
-  for (int i = 0; i < 3; ++i) {
-    double ai = 0;
-    for (int b = 0; b < 3; ++b) {
-      const double e = q[10 + 3 * i + b];
-      ai = b == 0 ? 4 * (e * e) : ai + 4 * (e * e);
-    }
-    acc = i == 0 ? ai : acc + ai;
+  for (int c = (G0 == 4 ? 10 : 0); c < (G1 == 4 ? 10 : NP); ++c) q[c] = (double)qs[c];
+  if (G0 == 0) {
+    out[0] = q[0] * q[0];
+    out[1] = q[1] * q[1] + q[2] * q[2];
+    out[2] = ((q[3] * q[3] + q[4] * q[4]) + q[5] * q[5]) + q[6] * q[6];
+    out[3] = (q[7] * q[7] + q[8] * q[8]) + q[9] * q[9];
   }
-  out[4] = acc;
+  if (G1 == 5) {
+    double acc = 0;
+    for (int i = 0; i < 3; ++i) {
+      double ai = 0;
+      for (int b = 0; b < 3; ++b) {
+        const double e = q[10 + 3 * i + b];
+        ai = b == 0 ? 4 * (e * e) : ai + 4 * (e * e);
+      }
+      acc = i == 0 ? ai : acc + ai;
+    }
+    out[4] = acc;
+  }
 }
 
 __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c < 7 ? 2 : c < 10 ? 3 : 4; }
@@ -379,11 +391,26 @@ __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c
 #ifndef CLB_SU2_KICK_MINB_F64
 #define CLB_SU2_KICK_MINB_F64 3
 #endif
-template <class S, int NK, bool RF, bool RP>
-__global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
+// SECT (as kernels()): 0 every sector in one sweep; 1 and 2 the two halves of a split sweep, run
+// one after the other over the same grid.  Each half updates, reduces and writes only its own
+// components and partial slots (1: sectors S, phi, Phi, A, the field sums but <B^2> of SU(2);
+// 2: the SU(2) sector and its <B^2>), so the halves hold fewer registers than the whole.
+// The halves of a split sweep (192^3, ms per step, same call): FP64 8.17 whole, 6.23 halves at
+// three blocks, 5.73 at four; FP32 4.66 whole, 3.31 halves at four blocks, 3.64 at five.
+#ifndef CLB_SU2_HALF_MINB_F32
+#define CLB_SU2_HALF_MINB_F32 4
+#endif
+#ifndef CLB_SU2_HALF_MINB_F64
+#define CLB_SU2_HALF_MINB_F64 4
+#endif
+template <class S, int NK, bool RF, bool RP, int SECT = 0>
+__global__ void __launch_bounds__(128, SECT == 0 ? (sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
+                                                  : (sizeof(S) == 4 ? CLB_SU2_HALF_MINB_F32 : CLB_SU2_HALF_MINB_F64))
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
            double *__restrict__ partials, const S *__restrict__ ph)
 {
+  constexpr int C0 = SECT == 2 ? 10 : 0, C1 = SECT == 1 ? 10 : NP; // momentum components [C0, C1)
+  constexpr int G0 = SECT == 2 ? 4 : 0, G1 = SECT == 1 ? 4 : 5;    // sectors [G0, G1)
   __shared__ double smem[(128 / 32) * kRed];
   const State st = *stp;
   double acc[kRed];
@@ -392,37 +419,43 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : 
     Site<S, S> v = make_site<S, S>(f, a, s);
     v.ph = ph;
     S q[NP];
-    for (int c = 0; c < NP; ++c) q[c] = p[(size_t)c * a.n3 + s];
+    for (int c = C0; c < C1; ++c) q[c] = p[(size_t)c * a.n3 + s];
     if (NK > 0) {
       S K[NP];
-      kernels(v, Coef<S>{(S)st.kA, (S)st.kB, (S)st.kB2, (S)st.kG}, K);
+      kernels<SECT>(v, Coef<S>{(S)st.kA, (S)st.kB, (S)st.kB2, (S)st.kG}, K);
       for (int k = 0; k < NK; ++k) {
-        for (int c = 0; c < NP; ++c) q[c] = (S)((double)q[c] + kc.h[k][sector(c)] * (double)K[c]);
+        for (int c = C0; c < C1; ++c) q[c] = (S)((double)q[c] + kc.h[k][sector(c)] * (double)K[c]);
         if (RP) {
           double t[5];
-          pi2s(q, t);
-          for (int g = 0; g < 5; ++g) acc[(k == 0 ? 0 : 11) + g] += t[g];
+          pi2s<G0, G1>(q, t);
+          for (int g = G0; g < G1; ++g) acc[(k == 0 ? 0 : 11) + g] += t[g];
         }
       }
-      for (int c = 0; c < NP; ++c) p[(size_t)c * a.n3 + s] = q[c];
+      for (int c = C0; c < C1; ++c) p[(size_t)c * a.n3 + s] = q[c];
     } else if (RP) {
       double t[5];
-      pi2s(q, t);
-      for (int g = 0; g < 5; ++g) acc[g] += t[g];
+      pi2s<G0, G1>(q, t);
+      for (int g = G0; g < G1; ++g) acc[g] += t[g];
     }
     if (RF) {
-      acc[5] += (double)sGrad2(v);
-      acc[6] += (double)cGrad2(v);
-      acc[7] += (double)dGrad2(v);
-      acc[8] += (double)aB2(v);
-      acc[9] += (double)gB2(v);
-      acc[10] += (double)v.pot();
+      if (SECT != 2) {
+        acc[5] += (double)sGrad2(v);
+        acc[6] += (double)cGrad2(v);
+        acc[7] += (double)dGrad2(v);
+        acc[8] += (double)aB2(v);
+      }
+      if (SECT != 1) acc[9] += (double)gB2(v);
+      if (SECT != 2) acc[10] += (double)v.pot();
     }
   }
   if (RF || RP) {
     block_reduce<kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
-      for (int k = 0; k < kRed; ++k) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
+      for (int k = 0; k < kRed; ++k) {
+        const bool mine = k < 5 || k >= 11 ? ((k < 5 ? k : k - 11) >= G0 && (k < 5 ? k : k - 11) < G1)
+                                           : (k == 9 ? SECT != 1 : SECT != 2);
+        if (mine) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
+      }
   }
 }
 
@@ -715,7 +748,7 @@ __device__ __forceinline__ Q4<Tan<double>> qexp_tan(Tan<double> p1, Tan<double> 
 template <class S>
 __global__ void __launch_bounds__(256)
     k_drift_tan(S *__restrict__ f, S *__restrict__ df, const S *__restrict__ p, const S *__restrict__ dp, Params a,
-                double w, int lf, const TState *__restrict__ stp, CoupDot cd, S *__restrict__ ph)
+                double w, int lf, const TState *__restrict__ stp, CoupDot cd)
 {
   using T = Tan<double>;
   const double dt = a.dt;
@@ -734,10 +767,8 @@ __global__ void __launch_bounds__(256)
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     put(f, df, s, ld(f, df, s) + p3 * (dtw * ld(p, dp, s)));
     for (int c = 1; c < 7; ++c) put(f, df, c * n3 + s, ld(f, df, c * n3 + s) + cC * ld(p, dp, c * n3 + s));
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 3; ++i)
       put(f, df, (7 + i) * n3 + s, ld(f, df, (7 + i) * n3 + s) + cA * ld(p, dp, (7 + i) * n3 + s) * 1.0);
-      put_phases(ph, a, i, s, f[(7 + i) * n3 + s]); // the plain kicks after the tangent form read them
-    }
     for (int i = 0; i < 3; ++i) {
       const size_t pb = (size_t)(10 + 3 * i) * n3 + s, fb = (size_t)(10 + 4 * i) * n3 + s;
       const Q4<T> E = qexp_tan(cG * ld(p, dp, pb), cG * ld(p, dp, pb + n3), cG * ld(p, dp, pb + 2 * n3));

@@ -218,3 +218,26 @@ def test_spectrum_tangent_matches_gpu_finite_differences(which, comp):
     sc = np.abs(ref).max()
     print("spectrum tangent", which, comp, np.abs(dv - ref).max() / sc)
     assert sc > 0 and np.abs(dv - ref).max() <= 1e-5 * sc
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_plain_evolution_after_tangent_end_is_bitwise(precision):
+    # the tangent form's kicks form the U(1) link phases themselves; after clb_tangent_end the plain
+    # kicks read the phase arrays again, which must hold the phases of the current A
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = case(8, "VV2", True)
+    out = []
+    for tangent in (False, True):
+        lat = Lattice(m, rp, precision=precision)
+        lat.set_state(f, p, sf)
+        if tangent:
+            lat.tangent_begin([0, 0, 0, 0, 1, 0])
+        lat.initialize()
+        lat.evolve(7)
+        if tangent:
+            lat.tangent_end()
+        lat.evolve(6)
+        out.append(lat.get_state())
+        lat.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
