@@ -155,10 +155,19 @@ template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, con
   const int kind = nk == 0 ? K_U1_REDUCE : K_U1_KICK;
   const S *f = static_cast<const S *>(u->f), *df = static_cast<const S *>(u->df);
   S *p = static_cast<S *>(u->p), *dp = static_cast<S *>(u->dp);
-#define CLB_SU2T(NK, RF, RP)                                                                                            \
+#define CLB_SU2T1(NK, RF, RP, SECT)                                                                                     \
   CLB_LAUNCH(h, kind,                                                                                                   \
-             k_kick_tan<S, NK, RF, RP><<<kSU2Blocks, 128, 0, h->stream>>>(f, df, p, dp, u->prm, kc, u->d_tst,          \
-                                                                            u->tan_cd, u->d_tpart))
+             k_kick_tan<S, NK, RF, RP, SECT><<<kSU2Blocks, 128, 0, h->stream>>>(f, df, p, dp, u->prm, kc, u->d_tst,    \
+                                                                                  u->tan_cd, u->d_tpart))
+#define CLB_SU2T(NK, RF, RP)                                                                                            \
+  do {                                                                                                                 \
+    if (NK > 0 && u->split) {                                                                                          \
+      CLB_SU2T1(NK, RF, RP, 1);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 2);                                                                                        \
+    } else {                                                                                                           \
+      CLB_SU2T1(NK, RF, RP, 0);                                                                                        \
+    }                                                                                                                  \
+  } while (0)
   if (nk == 0) {
     if (rf && rp)
       CLB_SU2T(0, true, true);
@@ -180,6 +189,7 @@ template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, con
       CLB_SU2T(2, false, false);
   }
 #undef CLB_SU2T
+#undef CLB_SU2T1
 }
 
 void sweep(clb_handle *h, int nk, bool rf, bool rp, const Kick &kc)

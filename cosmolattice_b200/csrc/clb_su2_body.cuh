@@ -643,31 +643,38 @@ __global__ void __launch_bounds__(128)
 // Tan arithmetic, so the state follows the plain evolution bitwise and the tangent is its exact
 // derivative along the coupling direction (and the tangent of the start state).
 
-// derivative of pi2s along the momentum tangent dq
-template <class R> __device__ __forceinline__ void pi2s_tan(const R *qs, const R *dqs, double out[5])
+// derivative of pi2s along the momentum tangent dq (sectors [G0, G1) as pi2s)
+template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s_tan(const R *qs, const R *dqs, double out[5])
 {
   double q[NP], d[NP];
-  for (int c = 0; c < NP; ++c) {
+  for (int c = (G0 == 4 ? 10 : 0); c < (G1 == 4 ? 10 : NP); ++c) {
     q[c] = (double)qs[c];
     d[c] = (double)dqs[c];
   }
-  out[0] = 2 * (q[0] * d[0]);
-  out[1] = 2 * (q[1] * d[1] + q[2] * d[2]);
-  out[2] = 2 * (((q[3] * d[3] + q[4] * d[4]) + q[5] * d[5]) + q[6] * d[6]);
-  out[3] = 2 * ((q[7] * d[7] + q[8] * d[8]) + q[9] * d[9]);
-  double acc = 0;
-  for (int c = 10; c < NP; ++c) acc += 8 * (q[c] * d[c]);
-  out[4] = acc;
+  if (G0 == 0) {
+    out[0] = 2 * (q[0] * d[0]);
+    out[1] = 2 * (q[1] * d[1] + q[2] * d[2]);
+    out[2] = 2 * (((q[3] * d[3] + q[4] * d[4]) + q[5] * d[5]) + q[6] * d[6]);
+    out[3] = 2 * ((q[7] * d[7] + q[8] * d[8]) + q[9] * d[9]);
+  }
+  if (G1 == 5) {
+    double acc = 0;
+    for (int c = 10; c < NP; ++c) acc += 8 * (q[c] * d[c]);
+    out[4] = acc;
+  }
 }
 
 // Tangent kick sweep: k_kick on (p, dp) with kernels and field sums in Tan<S>; partials
 // [block][2 kRed]: the kRed sums of k_kick, then their tangents.
-template <class S, int NK, bool RF, bool RP>
+// SECT as k_kick: 0 whole, 1 and 2 the halves of a split sweep.
+template <class S, int NK, bool RF, bool RP, int SECT = 0>
 __global__ void __launch_bounds__(128)
     k_kick_tan(const S *__restrict__ f, const S *__restrict__ df, S *__restrict__ p, S *__restrict__ dp, Params a,
                Kick kc, const TState *__restrict__ stp, CoupDot cd, double *__restrict__ partials)
 {
   using T = Tan<S>;
+  constexpr int C0 = SECT == 2 ? 10 : 0, C1 = SECT == 1 ? 10 : NP;
+  constexpr int G0 = SECT == 2 ? 4 : 0, G1 = SECT == 1 ? 4 : 5;
   __shared__ double smem[(128 / 32) * 2 * kRed];
   const Coef<T> C{T(stp->kA), T(stp->kB), T(stp->kB2), T(stp->kG)};
   double acc[2 * kRed];
@@ -675,31 +682,31 @@ __global__ void __launch_bounds__(128)
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
     const Site<S, T> v = make_site_tan<S>(f, df, a, s, cd);
     S q[NP], dq[NP];
-    for (int c = 0; c < NP; ++c) {
+    for (int c = C0; c < C1; ++c) {
       q[c] = p[(size_t)c * a.n3 + s];
       dq[c] = dp[(size_t)c * a.n3 + s];
     }
     auto add_pi = [&](int base) {
       double t[5], td[5];
-      pi2s(q, t);
-      pi2s_tan(q, dq, td);
-      for (int g = 0; g < 5; ++g) {
+      pi2s<G0, G1>(q, t);
+      pi2s_tan<G0, G1>(q, dq, td);
+      for (int g = G0; g < G1; ++g) {
         acc[base + g] += t[g];
         acc[kRed + base + g] += td[g];
       }
     };
     if (NK > 0) {
       T K[NP];
-      kernels(v, C, K);
+      kernels<SECT>(v, C, K);
       for (int k = 0; k < NK; ++k) {
-        for (int c = 0; c < NP; ++c) {
+        for (int c = C0; c < C1; ++c) {
           const double h = kc.h[k][sector(c)];
           q[c] = (S)((double)q[c] + h * (double)K[c].v);
           dq[c] = (S)((double)dq[c] + h * (double)K[c].d);
         }
         if (RP) add_pi(k == 0 ? 0 : 11);
       }
-      for (int c = 0; c < NP; ++c) {
+      for (int c = C0; c < C1; ++c) {
         p[(size_t)c * a.n3 + s] = q[c];
         dp[(size_t)c * a.n3 + s] = dq[c];
       }
@@ -707,17 +714,29 @@ __global__ void __launch_bounds__(128)
       add_pi(0);
     }
     if (RF) {
-      const T r[6] = {sGrad2(v), cGrad2(v), dGrad2(v), aB2(v), gB2(v), v.pot()};
-      for (int k = 0; k < 6; ++k) {
-        acc[5 + k] += (double)r[k].v;
-        acc[kRed + 5 + k] += (double)r[k].d;
+      auto addf = [&](int k, T r) {
+        acc[5 + k] += (double)r.v;
+        acc[kRed + 5 + k] += (double)r.d;
+      };
+      if (SECT != 2) {
+        addf(0, sGrad2(v));
+        addf(1, cGrad2(v));
+        addf(2, dGrad2(v));
+        addf(3, aB2(v));
       }
+      if (SECT != 1) addf(4, gB2(v));
+      if (SECT != 2) addf(5, v.pot());
     }
   }
   if (RF || RP) {
     block_reduce<2 * kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
-      for (int k = 0; k < 2 * kRed; ++k) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
+      for (int k = 0; k < 2 * kRed; ++k) {
+        const int j = k % kRed; // value and tangent slots alike
+        const bool mine = j < 5 || j >= 11 ? ((j < 5 ? j : j - 11) >= G0 && (j < 5 ? j : j - 11) < G1)
+                                           : (j == 9 ? SECT != 1 : SECT != 2);
+        if (mine) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
+      }
   }
 }
 
