@@ -109,6 +109,7 @@ class BatchTuning(C.Structure):
     _fields_ = [
         ("tile_z", C.c_int32),
         ("tile_y", C.c_int32),
+        ("sites_per_thread", C.c_int32),
         ("planes_x", C.c_int32),
         ("candidates", C.c_int32),
         ("ms_per_sweep", C.c_double),
@@ -178,7 +179,7 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_batch_last_evolve_ms": (C.c_int, [H, dp]),
             "clb_batch_kernel_launches": (C.c_int, [H, C.POINTER(C.c_int64)]),
             "clb_batch_autotune": (C.c_int, [H, C.c_int32, C.POINTER(BatchTuning)]),
-            "clb_batch_set_tuning": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32]),
+            "clb_batch_set_tuning": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "clb_batch_get_tuning": (C.c_int, [H, C.POINTER(BatchTuning)]),
         }
         for name, (res, args) in more.items():

@@ -104,8 +104,10 @@ class LatticeBatch:
         self._check(self.lib.clb_batch_autotune(self.h, int(reps), C.byref(t)))
         return self._tuning_dict(t)
 
-    def set_tuning(self, tile_z: int, tile_y: int, planes_x: int) -> None:
-        self._check(self.lib.clb_batch_set_tuning(self.h, int(tile_z), int(tile_y), int(planes_x)))
+    def set_tuning(self, tile_z: int, tile_y: int, planes_x: int, sites_per_thread: int = 1) -> None:
+        """Fix the sweep configuration: tile sites along z and y, x-planes per block, z sites per thread."""
+        self._check(self.lib.clb_batch_set_tuning(self.h, int(tile_z), int(tile_y), int(sites_per_thread),
+                                                  int(planes_x)))
 
     def tuning(self) -> Dict[str, object]:
         t = _capi.BatchTuning()

@@ -26,12 +26,13 @@ thread_local std::string g_berr;
 constexpr int kPackBlocks = 148 * 8;
 constexpr int kMeasBlocks = 148 * 4;
 
-// Sweep configurations the autotuner chooses from: (z, y) tile shapes compiled for, and the
-// x-run lengths (planes per block, capped at the member's N).
+// Sweep configurations the autotuner chooses from: block shapes compiled for (threads along z and
+// y, z sites per thread), and the x-run lengths (planes per block, capped at the member's N).
 struct TileShape {
-  int bz, by;
+  int bz, by, vz;
 };
-constexpr TileShape kTiles[] = {{32, 4}, {32, 8}, {32, 16}, {64, 4}};
+constexpr TileShape kTiles[] = {{32, 4, 1}, {32, 8, 1},  {32, 16, 1}, {64, 4, 1}, {16, 8, 2}, {16, 16, 2},
+                                {32, 8, 2}, {8, 16, 4},  {8, 32, 4},  {16, 8, 4}, {16, 16, 4}};
 constexpr int kNTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 constexpr int kRuns[] = {8, 16, 32, 64, 1024};
 constexpr int kDefaultTile = 1, kDefaultRun = 32; // 32 x 8 tiles, 32-plane runs
@@ -89,15 +90,15 @@ struct clb_batch {
 
 namespace {
 
-template <int BZ, int BY, class R>
+template <int BZ, int BY, int VZ, class R>
 void sweep_tile(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2)
 {
   const R *fin = static_cast<const R *>(b->f[b->cf]), *pin = static_cast<const R *>(b->p[b->cf]);
   R *fout = static_cast<R *>(b->f[drift ? b->cf ^ 1 : b->cf]), *pout = static_cast<R *>(b->p[drift ? b->cf ^ 1 : b->cf]);
   const dim3 grid(b->total_blocks), block(BZ, BY);
 #define CLB_BS(D, K, RD)                                                                                               \
-  k_batch_sweep<BZ, BY, R, D, K, RD><<<grid, block, 0, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk, b->d_st, \
-                                                                      b->rs, dtw, h1, h2, b->d_part)
+  k_batch_sweep<BZ, BY, VZ, R, D, K, RD><<<grid, block, 0, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk,    \
+                                                                          b->d_st, b->rs, dtw, h1, h2, b->d_part)
   if (drift && kick && red)
     CLB_BS(true, true, 3);
   else if (drift && kick)
@@ -115,10 +116,17 @@ template <class R>
 void sweep_launch(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, double h2, bool advance = true)
 {
   switch (b->tile) {
-  case 0: sweep_tile<32, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
-  case 1: sweep_tile<32, 8, R>(b, drift, kick, red, dtw, h1, h2); break;
-  case 2: sweep_tile<32, 16, R>(b, drift, kick, red, dtw, h1, h2); break;
-  default: sweep_tile<64, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 0: sweep_tile<32, 4, 1, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 1: sweep_tile<32, 8, 1, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 2: sweep_tile<32, 16, 1, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 3: sweep_tile<64, 4, 1, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 4: sweep_tile<16, 8, 2, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 5: sweep_tile<16, 16, 2, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 6: sweep_tile<32, 8, 2, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 7: sweep_tile<8, 16, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 8: sweep_tile<8, 32, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  case 9: sweep_tile<16, 8, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
+  default: sweep_tile<16, 16, 4, R>(b, drift, kick, red, dtw, h1, h2); break;
   }
   ++b->launches;
   if (!advance) return;
@@ -135,7 +143,7 @@ cudaError_t layout(clb_batch *b, int tile, int run)
   b->blk_lat.clear();
   for (int i = 0; i < b->n; ++i) {
     BatchLat &L = b->lat[(size_t)i];
-    L.gx = (L.N + t.bz - 1) / t.bz;
+    L.gx = (L.N + t.bz * t.vz - 1) / (t.bz * t.vz);
     L.gy = (L.N + t.by - 1) / t.by;
     L.LX = std::min(L.N, run);
     L.gz = (L.N + L.LX - 1) / L.LX;
@@ -178,6 +186,19 @@ void drop_graphs(clb_batch *b)
   b->graphs.clear();
 }
 
+// VZ sites per thread need every member's N to be a multiple of VZ (aligned vector loads).
+bool tile_fits(const clb_batch *b, int t)
+{
+  for (const BatchLat &L : b->lat)
+    if (L.N % kTiles[t].vz) return false;
+  return true;
+}
+
+clb_batch_tuning tuning_of(int t, int run, int candidates, double ms, double ms_def)
+{
+  return clb_batch_tuning{kTiles[t].bz * kTiles[t].vz, kTiles[t].by, kTiles[t].vz, run, candidates, ms, ms_def};
+}
+
 std::string tune_key(const clb_batch *b)
 {
   std::vector<int> ns;
@@ -210,6 +231,7 @@ int autotune(clb_batch *b, int reps)
   int maxN = 0;
   for (const BatchLat &L : b->lat) maxN = std::max(maxN, L.N);
   for (int t = 0; t < kNTiles && e == cudaSuccess; ++t) {
+    if (!tile_fits(b, t)) continue;
     for (int run : kRuns) {
       if (run != kRuns[0] && run / 2 >= maxN) continue; // the same grids as run / 2
       if ((e = layout(b, t, run)) != cudaSuccess) break;
@@ -235,7 +257,7 @@ int autotune(clb_batch *b, int reps)
   if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_autotune");
   drop_graphs(b);
   b->tuned = true;
-  b->tuning = clb_batch_tuning{kTiles[bt].bz, kTiles[bt].by, br, count, best, def};
+  b->tuning = tuning_of(bt, br, count, best, def);
   g_tuned[tune_key(b)] = {bt, br};
   return CLB_OK;
 }
@@ -399,7 +421,7 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
     ok = layout(b, cached ? it->second.first : kDefaultTile, cached ? it->second.second : kDefaultRun) == cudaSuccess;
     if (cached) {
       b->tuned = true;
-      b->tuning = clb_batch_tuning{kTiles[b->tile].bz, kTiles[b->tile].by, b->run, 0, 0.0, 0.0};
+      b->tuning = tuning_of(b->tile, b->run, 0, 0.0, 0.0);
     }
   }
   if (ok) {
@@ -535,7 +557,7 @@ int clb_batch_evolve(clb_batch *b, int64_t nsteps)
       if (r != CLB_OK) return r;
     } else {
       b->tuned = true;
-      b->tuning = clb_batch_tuning{kTiles[b->tile].bz, kTiles[b->tile].by, b->run, 0, 0.0, 0.0};
+      b->tuning = tuning_of(b->tile, b->run, 0, 0.0, 0.0);
     }
   }
   const auto key = std::make_tuple(nsteps, b->cf, b->rs);
@@ -673,32 +695,29 @@ int clb_batch_autotune(clb_batch *b, int32_t reps, clb_batch_tuning *out)
   return r;
 }
 
-int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t planes_x)
+int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x)
 {
   if (!b) return CLB_EINVAL;
   int t = -1;
   for (int k = 0; k < kNTiles; ++k)
-    if (kTiles[k].bz == tile_z && kTiles[k].by == tile_y) t = k;
-  if (t < 0) return b->fail(CLB_EINVAL, "clb_batch_set_tuning: tile must be 32x4, 32x8, 32x16 or 64x4");
+    if (kTiles[k].bz * kTiles[k].vz == tile_z && kTiles[k].by == tile_y && kTiles[k].vz == sites_per_thread) t = k;
+  if (t < 0) return b->fail(CLB_EINVAL, "clb_batch_set_tuning: not a compiled tile (see clb_batch_tuning)");
+  if (!tile_fits(b, t))
+    return b->fail(CLB_EINVAL, "clb_batch_set_tuning: every member's N must be a multiple of sites_per_thread");
   if (planes_x < 1) return b->fail(CLB_EINVAL, "clb_batch_set_tuning: planes_x must be >= 1");
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e == cudaSuccess) e = layout(b, t, planes_x);
   if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_set_tuning");
   drop_graphs(b);
   b->tuned = true;
-  b->tuning = clb_batch_tuning{tile_z, tile_y, planes_x, 0, 0.0, 0.0};
+  b->tuning = tuning_of(t, planes_x, 0, 0.0, 0.0);
   return CLB_OK;
 }
 
 int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out)
 {
   if (!b || !out) return CLB_EINVAL;
-  *out = b->tuning;
-  if (!b->tuned) {
-    out->tile_z = kTiles[b->tile].bz;
-    out->tile_y = kTiles[b->tile].by;
-    out->planes_x = b->run;
-  }
+  *out = b->tuned ? b->tuning : tuning_of(b->tile, b->run, 0, 0.0, 0.0);
   return CLB_OK;
 }
 

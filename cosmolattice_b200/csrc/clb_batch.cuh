@@ -26,23 +26,41 @@ struct BatchLat {
   SFParams sp;
 };
 
-// DRIFT / KICK / RED as in k_sweep; one block = one BZ x BY (z, y) tile of one member, marching
-// over LX x-planes (tile shape and LX are chosen by the batch autotuner).  fin/pin are never
-// written; fout/pout alias them only without DRIFT.
-// Register budget: that of four resident 256-thread blocks per SM (64 registers), whatever the
-// tile: 1.43x over the unbounded build at 32 x 8.
+// DRIFT / KICK / RED as in k_sweep; one block = one (BZ VZ) x BY (z, y) tile of one member, each
+// thread owning VZ consecutive z sites (vector loads and stores; every member's N a multiple of
+// VZ), marching over LX x-planes.  Tile shape, VZ and LX are chosen by the batch autotuner.
+// fin/pin are never written; fout/pout alias them only without DRIFT.
+// Register budget: that of four resident 256-thread blocks per SM (64 registers) for one site per
+// thread (1.43x over the unbounded build at 32 x 8), twice that for vector sites (their VZ-wide
+// planes spill at 64).
 #ifndef CLB_BATCH_MINB
 #define CLB_BATCH_MINB 4
 #endif
-template <int BZ, int BY, class R, bool DRIFT, bool KICK, int RED>
-__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY))
+template <class R, int VZ> __device__ __forceinline__ void ldg_v(const R *p, R (&v)[VZ])
+{
+  if constexpr (VZ == 1)
+    v[0] = p[0];
+  else
+    ldv<R, VZ>(p, v);
+}
+template <class R, int VZ> __device__ __forceinline__ void stg_v(R *p, const R (&v)[VZ])
+{
+  if constexpr (VZ == 1)
+    p[0] = v[0];
+  else
+    stv<R, VZ>(p, v);
+}
+
+template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
+__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ == 1 ? 1 : 2))
     k_batch_sweep(const R *fin, const R *pin, R *fout, R *pout, const BatchLat *__restrict__ lats,
                   const int *__restrict__ blk_lat, DevState *__restrict__ sts, int rs, double dtw_d, double h1,
                   double h2, double *__restrict__ partials)
 {
   using A = Ar<R>;
   constexpr bool SPLIT = sizeof(R) == 4;
-  __shared__ R tile[3][BY + 2][BZ + 2];
+  constexpr int TZ = BZ * VZ; // z sites per tile
+  __shared__ R tile[3][BY + 2][TZ + 2];
   __shared__ double red_smem[(BZ * BY / 32) * kRedSlots];
   const int L = blk_lat[blockIdx.x];
   const BatchLat lt = lats[L];
@@ -55,11 +73,12 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY))
   fout += lt.off;
   pout += lt.off;
   const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * BZ + tz;
-  const int z0 = bx * BZ, y0 = by * BY;
-  const int hz = min(BZ, N - z0), hy = min(BY, N - y0);
+  const int z0 = bx * TZ, y0 = by * BY;
+  const int hz = min(TZ, N - z0), hy = min(BY, N - y0);
   const int x0 = bz * lt.LX, x1 = min(N, x0 + lt.LX);
-  const bool valid = tz < hz && ty < hy;
-  const int y = y0 + ty, z = z0 + tz;
+  const int zt = VZ * tz;                     // the thread's first z inside the tile
+  const bool valid = zt < hz && ty < hy;      // then all VZ sites are inside (N % VZ == 0)
+  const int y = y0 + ty, z = z0 + zt;
   const int ym = y0 == 0 ? N - 1 : y0 - 1, yp = y0 + hy == N ? 0 : y0 + hy;
   const int zm = z0 == 0 ? N - 1 : z0 - 1, zp = z0 + hz == N ? 0 : z0 + hz;
 
@@ -80,52 +99,74 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY))
   const float h1f = (float)h1, h2f = (float)h2;
 
   auto sidx = [&](int x, int yy, int zz) -> size_t { return ((size_t)x * N + yy) * N + zz; };
-  auto ld = [&](size_t s) -> R {
+  auto ld1 = [&](size_t s) -> R {
     R v = fin[s];
     if (DRIFT) v = drift_val<R>(v, pin[s], pd, dtw);
     return v;
   };
+  auto ldq = [&](size_t s, R (&out)[VZ]) { // VZ drifted values
+    ldg_v<R, VZ>(fin + s, out);
+    if (DRIFT) {
+      R pv[VZ];
+      ldg_v<R, VZ>(pin + s, pv);
+#pragma unroll
+      for (int k = 0; k < VZ; ++k) out[k] = drift_val<R>(out[k], pv[k], pd, dtw);
+    }
+  };
 
   double acc_pi2 = 0, acc_g2 = 0, acc_v = 0, acc_p = 0;
   long long cnt = 0;
-  constexpr bool LOADP = KICK || (RED & 1);
-  // One plane's values for this thread: centre, in-plane halo values it owns, momentum.
+  constexpr bool LOADP = DRIFT || KICK || (RED & 1);
+  // One plane's values for this thread: its VZ sites, the in-plane halo values it owns, momenta.
   struct Plane {
-    R c, h[4], pi;
+    R c[VZ], pi[VZ], hm[VZ], hp[VZ], zl, zr;
   };
-  const bool hym = ty == 0, hyp = ty == hy - 1, hzm = tz == 0, hzp = tz == hz - 1;
+  const bool hym = ty == 0, hyp = ty == hy - 1, hzm = tz == 0, hzp = zt + VZ == hz;
   auto load = [&](int xp, bool tile_too, Plane &q) {
-    q.c = ld(sidx(xp, y, z));
+    const size_t s = sidx(xp, y, z);
+    ldg_v<R, VZ>(fin + s, q.c);
+    if (LOADP) ldg_v<R, VZ>(pin + s, q.pi);
+    if (DRIFT) {
+#pragma unroll
+      for (int k = 0; k < VZ; ++k) q.c[k] = drift_val<R>(q.c[k], q.pi[k], pd, dtw);
+    }
     if (tile_too) {
-      if (hym) q.h[0] = ld(sidx(xp, ym, z));
-      if (hyp) q.h[1] = ld(sidx(xp, yp, z));
-      if (hzm) q.h[2] = ld(sidx(xp, y, zm));
-      if (hzp) q.h[3] = ld(sidx(xp, y, zp));
-      if (LOADP) q.pi = pin[sidx(xp, y, z)];
+      if (hym) ldq(sidx(xp, ym, z), q.hm);
+      if (hyp) ldq(sidx(xp, yp, z), q.hp);
+      if (hzm) q.zl = ld1(sidx(xp, y, zm));
+      if (hzp) q.zr = ld1(sidx(xp, y, zp));
     }
   };
   auto store = [&](int tb, const Plane &q) {
-    tile[tb][ty + 1][tz + 1] = q.c;
-    if (hym) tile[tb][0][tz + 1] = q.h[0];
-    if (hyp) tile[tb][hy + 1][tz + 1] = q.h[1];
-    if (hzm) tile[tb][ty + 1][0] = q.h[2];
-    if (hzp) tile[tb][ty + 1][hz + 1] = q.h[3];
+#pragma unroll
+    for (int k = 0; k < VZ; ++k) {
+      tile[tb][ty + 1][1 + zt + k] = q.c[k];
+      if (hym) tile[tb][0][1 + zt + k] = q.hm[k];
+      if (hyp) tile[tb][hy + 1][1 + zt + k] = q.hp[k];
+    }
+    if (hzm) tile[tb][ty + 1][0] = q.zl;
+    if (hzp) tile[tb][ty + 1][hz + 1] = q.zr;
   };
   auto wrapx = [&](int xx) { return xx >= N ? xx - N : xx; };
-  R prev = R(0), cur = R(0), nxt = R(0), piC = R(0), piN = R(0);
+  R prev[VZ], cur[VZ], nxt[VZ], piC[VZ], piN[VZ];
+#pragma unroll
+  for (int k = 0; k < VZ; ++k) prev[k] = cur[k] = nxt[k] = piC[k] = piN[k] = R(0);
   if (x0 < x1) {
     // prologue: planes x0 - 1 (centre), x0 and x0 + 1; loads run two planes ahead of the compute
     Plane q0{}, q1{};
     if (valid) {
-      prev = ld(sidx(x0 == 0 ? N - 1 : x0 - 1, y, z));
+      ldq(sidx(x0 == 0 ? N - 1 : x0 - 1, y, z), prev);
       load(x0, true, q0);
       load(wrapx(x0 + 1), x0 + 1 < x1, q1);
       store(0, q0);
       if (x0 + 1 < x1) store(1, q1);
-      cur = q0.c;
-      piC = q0.pi;
-      nxt = q1.c;
-      piN = q1.pi;
+#pragma unroll
+      for (int k = 0; k < VZ; ++k) {
+        cur[k] = q0.c[k];
+        piC[k] = q0.pi[k];
+        nxt[k] = q1.c[k];
+        piN[k] = q1.pi[k];
+      }
     }
     __syncthreads();
     int b = 0;
@@ -136,56 +177,77 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY))
       if (valid && has2) load(wrapx(x + 2), tile2, q2);
       if (valid) {
         const size_t s = sidx(x, y, z);
-        const R c = cur;
-        const R ynb = tile[b][ty + 2][tz + 1], ymb = tile[b][ty][tz + 1];
-        const R znb = tile[b][ty + 1][tz + 2], zmb = tile[b][ty + 1][tz];
-        if (DRIFT) fout[s] = c;
+        R outp[VZ];
+        if (DRIFT) stg_v<R, VZ>(fout + s, cur);
         if constexpr (SPLIT) {
-          if (KICK) {
-            const float lap = inv_dx2 * ((((nxt + prev) - 2.f * c) + ((ynb + ymb) - 2.f * c)) + ((znb + zmb) - 2.f * c));
-            const float K = KA * lap - KB * spc.ddV(c);
-            const float pm = fmaf(h1f, K, piC);
-            pout[s] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
-            if (RED & 1) {
-              acc_p += (double)pm;
-              acc_pi2 += (double)(pm * pm);
+          float s_p = 0.f, s_p2 = 0.f, s_g2 = 0.f, s_dv = 0.f;
+#pragma unroll
+          for (int k = 0; k < VZ; ++k) {
+            const float c = cur[k];
+            const float ynb = tile[b][ty + 2][1 + zt + k], ymb = tile[b][ty][1 + zt + k];
+            const float znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : tile[b][ty + 1][1 + zt + VZ];
+            const float zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : tile[b][ty + 1][zt];
+            if (KICK) {
+              const float lap = inv_dx2 * ((((nxt[k] + prev[k]) - 2.f * c) + ((ynb + ymb) - 2.f * c)) + ((znb + zmb) - 2.f * c));
+              const float K = KA * lap - KB * spc.ddV(c);
+              const float pm = fmaf(h1f, K, piC[k]);
+              outp[k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
+              if (RED & 1) {
+                s_p += pm;
+                s_p2 = fmaf(pm, pm, s_p2);
+              }
+            } else if (RED & 1) {
+              s_p += piC[k];
+              s_p2 = fmaf(piC[k], piC[k], s_p2);
             }
-          } else if (RED & 1) {
-            acc_p += (double)piC;
-            acc_pi2 += (double)(piC * piC);
+            if (RED & 2) {
+              const float gx = nxt[k] - c, gy = ynb - c, gz = znb - c;
+              s_g2 += (gx * gx + gy * gy + gz * gz) * inv_dx2;
+              s_dv += spc.dVpot(c);
+            }
           }
-          if (RED & 2) {
-            const float gx = nxt - c, gy = ynb - c, gz = znb - c;
-            acc_g2 += (double)((gx * gx + gy * gy + gz * gz) * inv_dx2);
-            acc_v += (double)spc.dVpot(c);
-          }
-          ++cnt;
+          acc_p += (double)s_p;
+          acc_pi2 += (double)s_p2;
+          acc_g2 += (double)s_g2;
+          acc_v += (double)s_dv;
+          cnt += VZ;
         } else {
-          if (KICK) {
-            const R txv = A::sub(A::add(nxt, prev), A::mul(two, c));
-            const R tyv = A::sub(A::add(ynb, ymb), A::mul(two, c));
-            const R tzv = A::sub(A::add(znb, zmb), A::mul(two, c));
-            const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
-            const R cv[1] = {c};
-            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Lphi4<R, 1>::dV(0, cv, c0, R(0))));
-            const KickOut<R> ko = kick_val<R>(piC, K, h1, h2);
-            pout[s] = ko.next;
-            if (RED & 1) acc_pi2 += ko.mid * ko.mid;
-          } else if (RED & 1) {
-            acc_pi2 += (double)piC * (double)piC;
-          }
-          if (RED & 2) {
-            const R gx = A::sub(nxt, c), gy = A::sub(ynb, c), gz = A::sub(znb, c);
-            acc_g2 += (double)A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
-            const R cv[1] = {c};
-            acc_v += (double)Lphi4<R, 1>::V(cv, c0q, R(0));
+#pragma unroll
+          for (int k = 0; k < VZ; ++k) {
+            const R c = cur[k];
+            const R ynb = tile[b][ty + 2][1 + zt + k], ymb = tile[b][ty][1 + zt + k];
+            const R znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : tile[b][ty + 1][1 + zt + VZ];
+            const R zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : tile[b][ty + 1][zt];
+            if (KICK) {
+              const R txv = A::sub(A::add(nxt[k], prev[k]), A::mul(two, c));
+              const R tyv = A::sub(A::add(ynb, ymb), A::mul(two, c));
+              const R tzv = A::sub(A::add(znb, zmb), A::mul(two, c));
+              const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
+              const R cv[1] = {c};
+              const R K = A::sub(A::mul(KA, lap), A::mul(KB, Lphi4<R, 1>::dV(0, cv, c0, R(0))));
+              const KickOut<R> ko = kick_val<R>(piC[k], K, h1, h2);
+              outp[k] = ko.next;
+              if (RED & 1) acc_pi2 += ko.mid * ko.mid;
+            } else if (RED & 1) {
+              acc_pi2 += (double)piC[k] * (double)piC[k];
+            }
+            if (RED & 2) {
+              const R gx = A::sub(nxt[k], c), gy = A::sub(ynb, c), gz = A::sub(znb, c);
+              acc_g2 += (double)A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
+              const R cv[1] = {c};
+              acc_v += (double)Lphi4<R, 1>::V(cv, c0q, R(0));
+            }
           }
         }
-        prev = cur;
-        cur = nxt;
-        piC = piN;
-        nxt = q2.c;
-        piN = q2.pi;
+        if (KICK) stg_v<R, VZ>(pout + s, outp);
+#pragma unroll
+        for (int k = 0; k < VZ; ++k) {
+          prev[k] = cur[k];
+          cur[k] = nxt[k];
+          piC[k] = piN[k];
+          nxt[k] = q2.c[k];
+          piN[k] = q2.pi[k];
+        }
         if (tile2) store(b2, q2);
       }
       __syncthreads();

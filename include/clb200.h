@@ -285,22 +285,26 @@ int clb_batch_measure(clb_batch *b, int32_t i, double e0, clb_measurement *m);
 int clb_batch_last_evolve_ms(clb_batch *b, double *ms);
 int clb_batch_kernel_launches(clb_batch *b, int64_t *n);
 
-/* Sweep configuration of the ensemble: the (z, y) tile of one sweep block and the x-planes each
- * block marches over.  The first clb_batch_evolve of a handle times every compiled tile (32x4,
- * 32x8, 32x16, 64x4) with x-runs of 8, 16, 32, 64 and N planes on the ensemble itself and keeps
- * the fastest (environment CLB_BATCH_AUTOTUNE=0: keep 32x8, 32 planes); later handles of the same
+/* Sweep configuration of the ensemble: the (z, y) tile of one sweep block, the z sites each
+ * thread owns (vector loads; every member's N a multiple of it) and the x-planes each block
+ * marches over.  The first clb_batch_evolve of a handle times every compiled block shape (tile z x
+ * y x sites per thread: 32x4x1, 32x8x1, 32x16x1, 64x4x1, 32x8x2, 32x16x2, 64x8x2, 32x16x4, 32x32x4,
+ * 64x8x4, 64x16x4) with x-runs of 8, 16, 32, 64 and N planes on the ensemble itself and keeps the
+ * fastest (environment CLB_BATCH_AUTOTUNE=0: keep 32x8x1, 32 planes); later handles of the same
  * ensemble shape in the process reuse it.  clb_batch_autotune reruns it (reps timed sweeps per
  * candidate); clb_batch_set_tuning fixes a configuration.  The fields do not depend on it; the
- * volume sums are summed in a tile-dependent order. */
+ * volume sums are summed in a configuration-dependent order. */
 typedef struct clb_batch_tuning {
-  int32_t tile_z, tile_y, planes_x; /* the configuration in use                                  */
-  int32_t candidates;               /* configurations timed (0: set, cached or default)          */
-  double ms_per_sweep;              /* its time for one fused stage sweep of all members         */
-  double ms_default;                /* the same for 32x8 tiles with 32-plane runs                */
+  int32_t tile_z, tile_y;    /* sites of one sweep block's tile along z and y                 */
+  int32_t sites_per_thread;  /* consecutive z sites per thread                                */
+  int32_t planes_x;          /* x-planes per block                                            */
+  int32_t candidates;        /* configurations timed (0: set, cached or default)              */
+  double ms_per_sweep;       /* its time for one fused stage sweep of all members             */
+  double ms_default;         /* the same for 32x8x1 tiles with 32-plane runs                  */
 } clb_batch_tuning;
 
 int clb_batch_autotune(clb_batch *b, int32_t reps, clb_batch_tuning *out);
-int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t planes_x);
+int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x);
 int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------

@@ -131,10 +131,21 @@ def test_batch_rejects_mixed_members():
     assert e.value.code == _capi.CLB_EUNSUPPORTED
 
 
-@pytest.mark.parametrize("tile", [(32, 4, 8), (32, 8, 32), (32, 16, 5), (64, 4, 1024), (32, 4, 1)])
+# members whose N are multiples of 4, so that the vector-site tiles apply too
+MEMBERS4 = [(8, 1.0, 1e-3, "a"), (12, 0.5, 1e-2, "b"), (16, 2.0, 3e-3, "c"), (20, 1.3, 1e-4, "d"), (32, 0.8, 5e-3, "e")]
+
+
+def members4(evolver="VV4", expansion=True, dt=0.01):
+    return [make_scalar_case(N=N, evolver=evolver, expansion=expansion, dt=dt, seed=seed, amp=amp,
+                             extra={"lambda_prog": lam}) for N, lam, amp, seed in MEMBERS4]
+
+
+# (tile z sites, tile y, x-planes, z sites per thread)
+@pytest.mark.parametrize("tile", [(32, 4, 8, 1), (32, 8, 32, 1), (32, 16, 5, 1), (64, 4, 1024, 1), (32, 4, 1, 1),
+                                  (32, 8, 7, 2), (64, 8, 16, 2), (32, 16, 3, 4), (64, 16, 64, 4), (32, 32, 1024, 4)])
 def test_every_sweep_configuration_matches_oracle(tile):
-    # every compiled tile shape, with x-runs shorter than, equal to and longer than the members
-    cases = members("VV4", True)
+    # every block shape kind, with x-runs shorter than, equal to and longer than the members
+    cases = members("VV4", True) if tile[3] == 1 else members4()
     out, m0, m1 = run_batch(cases, "fp64", 20, tuning=tile)
     for i, c in enumerate(cases):
         st, o0, o1 = run_oracle(c, 20)
@@ -155,13 +166,14 @@ def test_autotuner_picks_a_timed_configuration():
     print("autotune", t)
     assert t["candidates"] >= 8 and t["ms_per_sweep"] > 0 and t["ms_default"] > 0
     assert t["ms_per_sweep"] <= t["ms_default"]
-    assert (t["tile_z"], t["tile_y"]) in {(32, 4), (32, 8), (32, 16), (64, 4)} and t["planes_x"] >= 8
+    assert (t["tile_z"], t["tile_y"], t["sites_per_thread"]) in {(32, 4, 1), (32, 8, 1), (32, 16, 1), (64, 4, 1)}
+    assert t["planes_x"] >= 8  # the members' odd N allow one site per thread only
     assert bt.tuning() == t
     f0 = [bt.get_state(i) for i in range(len(cases))]
     bt.evolve(10)
     # the timing sweeps left the state alone: a second handle without tuning runs the same steps
     bt2 = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp32")
-    bt2.set_tuning(t["tile_z"], t["tile_y"], t["planes_x"])
+    bt2.set_tuning(t["tile_z"], t["tile_y"], t["planes_x"], t["sites_per_thread"])
     for i, c in enumerate(cases):
         bt2.set_state(i, c[3], c[4], c[5])
     bt2.initialize()
@@ -172,5 +184,19 @@ def test_autotuner_picks_a_timed_configuration():
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     with pytest.raises(Exception):
         bt.set_tuning(16, 16, 8)
+    with pytest.raises(Exception):
+        bt.set_tuning(32, 8, 8, 2)  # N = 13 and 33 are not multiples of 2
     bt.close()
     bt2.close()
+
+
+def test_fp32_vector_tiles_track_fp64():
+    # the FP32 split form with vector sites: every member within the FP32 bounds of its FP64 run
+    cases = members4("VV2")
+    g32, _, m32 = run_batch(cases, "fp32", 60, tuning=(64, 16, 16, 4))
+    g64, _, m64 = run_batch(cases, "fp64", 60, tuning=(32, 8, 32, 1))
+    for i in range(len(cases)):
+        (fa, pa, sa), (fb, pb, sb) = g32[i], g64[i]
+        assert rel(fa, fb) < 1e-6
+        assert abs(sa["aI"] - sb["aI"]) / sb["aI"] < 1e-7
+        assert abs(m32[i]["friedmann"][0] - m64[i]["friedmann"][0]) < 1e-6
