@@ -161,6 +161,8 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
             "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
             "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
+            "clb_forward_spectrum": (C.c_int, [H, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                               C.c_double, C.c_int32, C.c_int32, dp, dp]),
             "clb_tangent_begin": (C.c_int, [H, dp, C.c_int32, dp, dp, C.POINTER(ScaleFactor)]),
             "clb_tangent_get_state": (C.c_int, [H, dp, dp, C.POINTER(ScaleFactor)]),
             "clb_tangent_observable": (C.c_int, [H, dp, C.c_int32, dp, dp]),
@@ -227,6 +229,7 @@ EXPORTED = [
     "clb_cuda_stream",
     "clb_forward",
     "clb_backward",
+    "clb_forward_spectrum",
     "clb_tangent_begin",
     "clb_tangent_get_state",
     "clb_tangent_observable",

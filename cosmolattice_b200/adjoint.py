@@ -24,11 +24,13 @@ GAUGE_FRACTION = (0.0, 0.0, 1.0, 1.0, 0.0)  # (E_el + E_mag) / E_tot
 
 def u1_gradients(model: Model, rp: RunParameters, n_steps: int, checkpoint_every: int,
                  weights: Sequence[float] = GAUGE_FRACTION, params: Iterable[str] = ("amp", "c4", "gQ"),
-                 lattice: Lattice = None, state=None, tangents=None
+                 lattice: Lattice = None, state=None, tangents=None, spectrum: Dict[str, object] = None
                  ) -> Tuple[float, Dict[str, float], Dict[str, object]]:
     """(O, {param: dO/dparam}, backward record) for O = sum_k w_k E_k / E_tot after n_steps.
-    state: u1_initial_state(model, rp) if already made; tangents: {param: (df, dp)} likewise.
-    The record holds the wall times of the forward and backward calls."""
+    spectrum: instead O = sum_b w_b P_b, P the binned spectrum of one component at the end state,
+    given as {"which", "comp", "bin_weights"} plus Lattice.spectrum's optional ps_type,
+    ps_version, dk, fold.  state: u1_initial_state(model, rp) if already made; tangents:
+    {param: (df, dp)} likewise.  The record holds the wall times of the forward and backward calls."""
     import time
 
     lat = lattice if lattice is not None else Lattice(model, rp)
@@ -38,7 +40,11 @@ def u1_gradients(model: Model, rp: RunParameters, n_steps: int, checkpoint_every
     lat.set_state(f, p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
     lat.initialize(correct_adot=True)
     t0 = time.perf_counter()
-    O = lat.forward(n_steps, checkpoint_every, weights)
+    if spectrum is not None:
+        sp = dict(spectrum)
+        O = lat.forward_spectrum(n_steps, checkpoint_every, sp.pop("which"), sp.pop("comp"), sp.pop("bin_weights"), **sp)
+    else:
+        O = lat.forward(n_steps, checkpoint_every, weights)
     t1 = time.perf_counter()
     fb, pb, g = lat.backward(through_init=True)
     t2 = time.perf_counter()

@@ -52,6 +52,7 @@ int u1_evolve(clb_handle *h, int64_t n);
 int u1_sync(clb_handle *h);
 int u1_measure(clb_handle *h, double e0, clb_measurement *m);
 int u1_forward(clb_handle *h, int64_t nsteps, int32_t K, const double *w, int32_t nw, double *obs);
+int u1_set_spectrum_seed(clb_handle *h, int which, int comp, const double *d_grad, double O, double abar);
 int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *out);
 
 // lphi4SU2U1 (clb_su2.cu)
@@ -631,6 +632,7 @@ void clb_destroy(clb_handle *h)
   if (h->plan_ok) cufftDestroy(h->plan);
   if (h->d_spec) cudaFree(h->d_spec);
   if (h->d_spec2) cudaFree(h->d_spec2);
+  if (h->plan_inv_ok) cufftDestroy(h->plan_inv);
   if (h->d_spec_part) cudaFree(h->d_spec_part);
   if (h->d_spec_cnt) cudaFree(h->d_spec_cnt);
   if (h->d_spec_out) cudaFree(h->d_spec_out);
@@ -1160,6 +1162,61 @@ int clb_spectrum(clb_handle *h, int32_t which, int32_t comp, int32_t ps_type, in
   bool gauge_comp = false;
   return spectrum_impl(h, which, comp, ps_type, ps_version, dk, nbins, fold, k_out, value_out, count_out, sums, cnt,
                        gauge_comp);
+}
+
+// clb_forward with the observable O = sum_b w_b P_b, P the clb_spectrum of one component at the
+// end state; the following clb_backward returns dO.
+int clb_forward_spectrum(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, int32_t which, int32_t comp,
+                         int32_t ps_type, int32_t ps_version, double dk, int32_t nbins, int32_t fold,
+                         const double *bin_weights, double *observable)
+{
+  if (!h) return CLB_EINVAL;
+  if (!h->initialized) return h->fail(CLB_ESTATE, "clb_forward_spectrum: call clb_initialize first");
+  if (!h->u1) return h->fail(CLB_EUNSUPPORTED, "clb_forward_spectrum: the adjoint pair covers lphi4U1");
+  if (!bin_weights || nbins < 1) return h->fail(CLB_EINVAL, "clb_forward_spectrum: one weight per bin");
+  int r = u1_forward(h, nsteps, checkpoint_every, nullptr, 0, nullptr);
+  if (r != CLB_OK) return r;
+  // the end state's spectrum: its bin sums and counts, and the component's transform in d_spec
+  std::vector<double> sums, vals((size_t)nbins);
+  std::vector<unsigned long long> cnt;
+  bool gauge = false;
+  r = spectrum_impl(h, which, comp, ps_type, ps_version, dk, nbins, fold, nullptr, vals.data(), nullptr, sums, cnt, gauge);
+  if (r != CLB_OK) return r;
+  clb_scalefactor sf;
+  if ((r = u1_get_state(h, nullptr, nullptr, &sf)) != CLB_OK) return r;
+  const double ex = 2 * h->md.alpha - (gauge ? 2 : 6);
+  const double m = which == 1 ? std::pow(sf.aI, ex) : 1.0;
+  double O = 0;
+  std::vector<double> g((size_t)nbins);
+  for (int b = 0; b < nbins; ++b) {
+    O += bin_weights[b] * vals[(size_t)b];
+    double ntil;
+    g[(size_t)b] = bin_weights[b] * m * spec_value(h, ps_type, ps_version, dk, b, cnt[(size_t)b], sums[(size_t)nbins + b], 1.0, &ntil);
+  }
+  const double abar = which == 1 ? ex * O / sf.aI : 0.0; // dO/da through the momentum spectra's a-factor
+  // dO/d(component) = 2 C2R(g f_k)
+  const int N = h->N;
+  const size_t spec_n = (size_t)N * N * 2 * (N / 2 + 1);
+  cudaError_t e = cudaSuccess;
+  if (!h->d_spec2 && (e = cudaMalloc(&h->d_spec2, spec_n * sizeof(double))) != cudaSuccess)
+    return h->fail(CLB_ENOMEM, std::string("clb_forward_spectrum: ") + cudaGetErrorString(e));
+  if (!h->plan_inv_ok) {
+    if (cufftPlan3d(&h->plan_inv, N, N, N, CUFFT_Z2D) != CUFFT_SUCCESS) return h->fail(CLB_ECUDA, "clb_forward_spectrum: cufftPlan3d failed");
+    h->plan_inv_ok = true;
+    if (cufftSetStream(h->plan_inv, h->stream) != CUFFT_SUCCESS) return h->fail(CLB_ECUDA, "clb_forward_spectrum: cufftSetStream failed");
+  }
+  double *d_g = h->d_spec_out; // nbins x 2 doubles of scratch (the bin sums are on the host by now)
+  if ((e = cudaMemcpyAsync(d_g, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+    return h->cuda_fail(e, "clb_forward_spectrum");
+  CLB_LAUNCH(h, K_SPECTRUM, k_spec_weight<<<kSpecBlocks, 256, 0, h->stream>>>(reinterpret_cast<double2 *>(h->d_spec), N, dk,
+                                                                             nbins, fold, d_g));
+  if (cufftExecZ2D(h->plan_inv, reinterpret_cast<cufftDoubleComplex *>(h->d_spec), h->d_spec) != CUFFT_SUCCESS)
+    return h->fail(CLB_ECUDA, "clb_forward_spectrum: cufftExecZ2D failed");
+  CLB_LAUNCH(h, K_SPECTRUM, k_spec_extract<<<kElemBlocks, 256, 0, h->stream>>>(h->d_spec, h->d_spec2, N, 2.0));
+  if ((e = cudaGetLastError()) != cudaSuccess) return h->cuda_fail(e, "clb_forward_spectrum");
+  if ((r = u1_set_spectrum_seed(h, which, comp, h->d_spec2, O, abar)) != CLB_OK) return r;
+  if (observable) *observable = O;
+  return CLB_OK;
 }
 
 // clb_spectrum of a component and its derivative along the tangent-linear form's direction.

@@ -81,6 +81,8 @@ struct clb_handle {
   double *d_spec2 = nullptr; // the tangent's transform (clb_tangent_spectrum)
   bool plan_ok = false;
   cufftHandle plan = 0;
+  bool plan_inv_ok = false; // Z2D, for spectrum-observable gradients
+  cufftHandle plan_inv = 0;
   double *d_spec_part = nullptr;
   unsigned long long *d_spec_cnt = nullptr;
   double *d_spec_out = nullptr;

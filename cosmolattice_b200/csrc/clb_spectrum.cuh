@@ -89,6 +89,39 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Gradient of sum_b g_b (sum over bin b of |f_k|^2), step 1: each mode of the half spectrum times
+// the weight g of its bin (k_spec_bin's bin rule; modes outside the bins: 0).  A C2R transform of
+// the result, times 2, is the gradient with respect to the real component.
+__global__ void __launch_bounds__(256)
+    k_spec_weight(double2 *__restrict__ fk, int N, double dk, int nbins, int fold, const double *__restrict__ gbin)
+{
+  const int nzh = N / 2 + 1;
+  for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
+    const int kx = (int)(r / N), ky = (int)(r % N);
+    const long long nx = kx <= N / 2 ? kx : kx - N;
+    const long long ny = ky <= N / 2 ? ky : ky - N;
+    double2 *row = fk + r * nzh;
+    for (int kz = threadIdx.x; kz < nzh; kz += blockDim.x) {
+      const long long n2 = nx * nx + ny * ny + (long long)kz * kz;
+      int b = (int)floor(sqrt((double)n2) / dk);
+      double g = 0.0;
+      if (b < nbins || fold) g = gbin[b < nbins ? b : nbins - 1];
+      row[kz] = double2{row[kz].x * g, row[kz].y * g};
+    }
+  }
+}
+
+// Real output of an in-place C2R transform (row pitch 2 (N/2 + 1)) times scale -> N^3 array.
+__global__ void __launch_bounds__(256) k_spec_extract(const double *__restrict__ src, double *__restrict__ dst, int N, double scale)
+{
+  const long long pitch = 2LL * (N / 2 + 1);
+  for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
+    const double *s = src + r * pitch;
+    double *d = dst + r * N;
+    for (int z = threadIdx.x; z < N; z += blockDim.x) d[z] = scale * s[z];
+  }
+}
+
 // One block per group of (kx, ky) rows; shared-memory histograms of sum w |f|^2, sum w |n| and the
 // integer mode count, written as one partial row per block.
 __global__ void __launch_bounds__(256)

@@ -47,6 +47,10 @@ struct U1Sector {
   double fwd_w[5] = {0, 0, 0, 0, 0};
   double fwd_avg[5] = {0, 0, 0, 0, 0}; // final <|pi_phi|^2>, <|D phi|^2>, <pi_A^2>, <B^2>, <V>
   double fwd_a = 1, fwd_obs = 0;
+  // spectrum observable (clb_forward_spectrum): the cotangent of one component at the end state
+  int seed_which = -1, seed_comp = 0; // -1: the energy observable of u1_forward
+  double seed_abar = 0;
+  double *seed = nullptr; // N^3
 };
 
 namespace {
@@ -285,11 +289,12 @@ static void free_adjoint(U1Sector *u)
   u->seg = nullptr;
   u->d_rec = nullptr;
   u->seg_cap = 0;
-  for (double **b : {&u->qbar, &u->pbar[0], &u->pbar[1], &u->d_apart, &u->d_asums}) {
+  for (double **b : {&u->qbar, &u->pbar[0], &u->pbar[1], &u->d_apart, &u->d_asums, &u->seed}) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
   u->fwd_steps = -1;
+  u->seed_which = -1;
 }
 
 __attribute__((visibility("hidden"))) void u1_destroy(clb_handle *h)
@@ -712,7 +717,7 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
     Ew += u->fwd_w[k] * E[k];
   }
   double Ebar[kAvgN];
-  for (int k = 0; k < kAvgN; ++k) Ebar[k] = (u->fwd_w[k] - Ew / Et) / Et;
+  for (int k = 0; k < kAvgN; ++k) Ebar[k] = u->seed_which >= 0 ? 0.0 : (u->fwd_w[k] - Ew / Et) / Et;
   // part A pending at the next boundary to process: the transposed first kick of the stage that
   // starts there (or the observable's seed, with no kick), its average cotangents, and the
   // cotangents of a and aDot there before its a-dot products are added
@@ -733,12 +738,19 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
     pend.abar = ex ? Ebar[0] * u->fwd_avg[0] * -6 * std::pow(a, -7) + Ebar[1] * u->fwd_avg[1] * -2 * std::pow(a, -3) +
                          (Ebar[2] * u->fwd_avg[2] + Ebar[3] * u->fwd_avg[3]) * el * -4 * std::pow(a, -5)
                    : 0.0;
+    if (u->seed_which >= 0) pend.abar = ex ? u->seed_abar : 0.0;
     pend.adbar = 0;
   }
   double abar = 0, adbar = 0; // cotangents of a, aDot at the boundary just processed
   if ((e = cudaMemsetAsync(u->qbar, 0, bytes, h->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(u->pbar[cur], 0, bytes, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "clb_backward");
+  if (u->seed_which >= 0) {
+    // a spectrum observable: its gradient with respect to one component at the end state
+    double *dst = (u->seed_which == 0 ? u->qbar : u->pbar[cur]) + (size_t)u->seed_comp * h->n3;
+    if ((e = cudaMemcpyAsync(dst, u->seed, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+  }
   std::vector<U1State> rec((size_t)u->seg_cap);
   const int64_t nck = (int64_t)u->ckpt.size() - 1; // the last entry holds the forward's end state
   const size_t half = 5 * h->n3 * u->esz;
@@ -877,6 +889,26 @@ __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t thr
     out->observable = u->fwd_obs;
   }
   return check(h, "clb_backward");
+}
+
+// The observable of the last u1_forward becomes a spectrum observable O with the given cotangent
+// of component comp of the fields (which 0) or momenta (which 1) at the end state (N^3, device)
+// and of a there (clb_forward_spectrum).
+__attribute__((visibility("hidden"))) int u1_set_spectrum_seed(clb_handle *h, int which, int comp, const double *d_grad,
+                                                               double O, double abar)
+{
+  U1Sector *u = h->u1;
+  if (u->fwd_steps < 0) return h->fail(CLB_ESTATE, "clb_forward_spectrum: no forward pass");
+  cudaError_t e = cudaSuccess;
+  if (!u->seed) e = cudaMalloc(&u->seed, h->n3 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(u->seed, d_grad, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward_spectrum");
+  u->seed_which = which;
+  u->seed_comp = comp;
+  u->seed_abar = abar;
+  u->fwd_obs = O;
+  return CLB_OK;
 }
 
 // Device array of one state component (clb_spectrum): which 0 fields, 1 momenta; gauge tells

@@ -122,6 +122,17 @@ class Lattice:
         self._check(self.lib.clb_forward(self.h, int(n_steps), int(checkpoint_every), _dp(w), int(w.size), C.byref(o)))
         return o.value
 
+    def forward_spectrum(self, n_steps: int, checkpoint_every: int, which: int, comp: int, bin_weights,
+                         ps_type: int = 1, ps_version: int = 1, dk: float = 1.0, fold: bool = False) -> float:
+        """clb_forward_spectrum: the forward pass with O = sum_b w_b P_b, P the spectrum() of one
+        component at the end state (same arguments); backward() then returns dO."""
+        w = np.ascontiguousarray(bin_weights, dtype=np.float64)
+        o = C.c_double()
+        self._check(self.lib.clb_forward_spectrum(self.h, int(n_steps), int(checkpoint_every), int(which), int(comp),
+                                                  int(ps_type), int(ps_version), float(dk), int(w.size),
+                                                  1 if fold else 0, _dp(w), C.byref(o)))
+        return o.value
+
     def backward(self, through_init: bool = True):
         """clb_backward: (fields_bar, momenta_bar, grad dict) of the last forward's observable."""
         n3 = self.rp.N ** 3

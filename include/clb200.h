@@ -234,6 +234,12 @@ typedef struct clb_adjoint_grad {
 int clb_forward(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, const double *weights, int32_t n_weights,
                 double *observable);
 int clb_backward(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar, clb_adjoint_grad *grad);
+/* clb_forward with the observable O = sum_b w_b P_b, P the binned spectrum of clb_spectrum (same
+ * arguments) of one component at the end state, w one weight per bin; clb_backward then returns
+ * dO (the momentum spectra's a-factor differentiated too).  lphi4U1. */
+int clb_forward_spectrum(clb_handle *h, int64_t nsteps, int32_t checkpoint_every, int32_t which, int32_t comp,
+                         int32_t ps_type, int32_t ps_version, double dk, int32_t nbins, int32_t fold,
+                         const double *bin_weights, double *observable);
 
 /* ---- tangent-linear (forward-mode) form ---------------------------------------------------------
  * No counterpart in the reference.  Replaces a caller's central-difference pair of runs around

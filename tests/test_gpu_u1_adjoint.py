@@ -172,3 +172,68 @@ def test_fp32_form_gradients_track_fp64():
     assert abs(O32 - O64) <= 1e-5 * abs(O64)
     for k in g64:
         assert abs(g32[k] - g64[k]) <= 1e-3 * scale, (k, g32[k], g64[k])
+
+
+SPEC_CASES = [
+    # (evolver, which, comp, spectrum options): a scalar field, a gauge momentum (a^(2 alpha - 2)
+    # factor), a scalar momentum over fewer bins than modes without folding
+    ("VV2", 0, 0, {"ps_type": 1, "ps_version": 1, "dk": 1.0, "fold": True, "nbins": 10}),
+    ("VV4", 1, 3, {"ps_type": 2, "ps_version": 2, "dk": 1.0, "fold": True, "nbins": 10}),
+    ("VV2", 1, 1, {"ps_type": 1, "ps_version": 2, "dk": 1.5, "fold": False, "nbins": 4}),
+]
+
+
+def spectrum_weights(nbins):
+    return np.linspace(0.5, 1.5, nbins) * np.where(np.arange(nbins) % 2 == 0, 1.0, -0.5)
+
+
+def plain_spectrum_observable(N, evolver, dt, n, which, comp, opts, over=None):
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = case(N, evolver, True, dt, over)
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(n)
+    lat.sync()
+    o = dict(opts)
+    _, v, _ = lat.spectrum(which, comp, **o)
+    lat.close()
+    return float(spectrum_weights(opts["nbins"]) @ v)
+
+
+@pytest.mark.parametrize("evolver,which,comp,opts", SPEC_CASES)
+def test_spectrum_observable_gradients_match_finite_differences(evolver, which, comp, opts):
+    # O = sum_b w_b P_b of one component at the end state (clb_forward_spectrum)
+    from cosmolattice_b200.adjoint import u1_gradients
+
+    N, dt, n = 12, 0.01, 30
+    par, rp, m, f, p, sf = case(N, evolver, True, dt)
+    spec = {k: v for k, v in opts.items() if k != "nbins"}
+    spec.update(which=which, comp=comp, bin_weights=spectrum_weights(opts["nbins"]))
+    O, grads, _ = u1_gradients(m, rp, n, 7, spectrum=spec)
+    assert abs(O - plain_spectrum_observable(N, evolver, dt, n, which, comp, opts)) <= 1e-12 * abs(O)
+    for prm in ("amp", "c4", "gQ"):
+        h = 1e-4 * BASE[prm]
+        up = plain_spectrum_observable(N, evolver, dt, n, which, comp, opts, {prm: BASE[prm] + h})
+        dn = plain_spectrum_observable(N, evolver, dt, n, which, comp, opts, {prm: BASE[prm] - h})
+        ref = (up - dn) / (2 * h)
+        assert abs(grads[prm] - ref) <= REL * abs(ref), (prm, grads[prm], ref)
+
+
+def test_energy_observable_after_spectrum_observable():
+    # a plain clb_forward after clb_forward_spectrum is the energy observable again
+    from cosmolattice_b200.adjoint import u1_gradients
+
+    from cosmolattice_b200 import Lattice
+
+    N, dt, n = 10, 0.01, 12
+    par, rp, m, f, p, sf = case(N, "VV2", True, dt)
+    lat = Lattice(m, rp)
+    O0, g0, _ = u1_gradients(m, rp, n, 5, lattice=lat)
+    u1_gradients(m, rp, n, 5, lattice=lat, spectrum={"which": 0, "comp": 2, "bin_weights": np.ones(6)})
+    O1, g1, _ = u1_gradients(m, rp, n, 5, lattice=lat)
+    lat.close()
+    assert O1 == O0
+    for prm in g0:
+        assert g1[prm] == g0[prm]
