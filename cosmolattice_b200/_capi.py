@@ -68,6 +68,23 @@ class ScaleFactor(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("aI", "aSI", "aIM", "aDotI", "aDotSI", "aDotSIM")]
 
 
+IC_MAX = 8
+
+
+class ICParams(C.Structure):
+    """clb_ic_params."""
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("amplitude", C.c_double),
+        ("k_cutoff", C.c_double),
+        ("adot", C.c_double),
+        ("mass2", C.c_double * IC_MAX),
+        ("fld0", C.c_double * IC_MAX),
+        ("pi0", C.c_double * IC_MAX),
+        ("charge", C.c_double * 4),
+    ]
+
+
 class Measurement(C.Structure):
     _fields_ = [
         ("aI", C.c_double),
@@ -161,6 +178,7 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
             "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
             "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
+            "clb_generate_state": (C.c_int, [H, C.POINTER(ICParams), C.POINTER(ScaleFactor)]),
             "clb_forward_spectrum": (C.c_int, [H, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                C.c_double, C.c_int32, C.c_int32, dp, dp]),
             "clb_tangent_begin": (C.c_int, [H, dp, C.c_int32, dp, dp, C.POINTER(ScaleFactor)]),
@@ -230,6 +248,7 @@ EXPORTED = [
     "clb_forward",
     "clb_backward",
     "clb_forward_spectrum",
+    "clb_generate_state",
     "clb_tangent_begin",
     "clb_tangent_get_state",
     "clb_tangent_observable",

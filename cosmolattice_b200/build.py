@@ -11,10 +11,10 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libclb200.so")
 
-SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_su2.cu", "clb_batch.cu", "clb_noalloc.cu"]
+SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_su2.cu", "clb_batch.cu", "clb_noalloc.cu", "clb_ic.cu"]
 # per-unit flags: the lphi4SU2U1 unit writes the reference's rounding order as plain expressions
 UNIT_FLAGS = {"clb_su2.cu": ["-fmad=false"]}
-DEPS = ["clb_tangent.cuh", "clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_batch.cuh", "clb_vv.h", "clb_adjoint.cuh", "clb_su2.cu", "clb_su2.cuh", "clb_noalloc.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
+DEPS = ["clb_tangent.cuh", "clb_api.cu", "clb_u1.cu", "clb_batch.cu", "clb_batch.cuh", "clb_vv.h", "clb_adjoint.cuh", "clb_su2.cu", "clb_su2.cuh", "clb_noalloc.cu", "clb_ic.cu", "clb_internal.cuh", "clb_handle.cuh", "clb_u1.cuh", "clb_scalar.cuh", "clb_sweep.cuh", "clb_tma.cuh", "clb_spectrum.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -59,6 +59,8 @@ int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar, double 
 int su2_create(clb_handle *h);
 void su2_destroy(clb_handle *h);
 int su2_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf);
+int scalar_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf,
+                     const double *means);
 int su2_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
 int su2_initialize(clb_handle *h, int32_t correct_adot);
 int su2_evolve(clb_handle *h, int64_t n);
@@ -231,7 +233,7 @@ cudaError_t upload(clb_handle *h, const double *src, void *dst, CompOffsets off)
   for (long long p0 = 0; p0 < planes; p0 += chunk) {
     const long long np = std::min(chunk, planes - p0);
     cudaError_t r = cudaMemcpyAsync(h->d_stage, src + p0 * per, (size_t)(np * per) * sizeof(double),
-                                    cudaMemcpyHostToDevice, h->stream);
+                                    cudaMemcpyDefault, h->stream);
     if (r != cudaSuccess) return r;
     if (h->fp32)
       CLB_LAUNCH(h, K_CONVERT, k_scatter<double, float><<<kElemBlocks, 256, 0, h->stream>>>(
@@ -661,13 +663,28 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
   if (!h || !fields || !momenta) return h ? h->fail(CLB_EINVAL, "clb_set_state: null argument") : CLB_EINVAL;
   if (h->u1) return u1_set_state(h, fields, momenta, sf);
   if (h->su2) return su2_set_state(h, fields, momenta, sf);
+  return scalar_set_state(h, fields, momenta, sf, nullptr);
+}
+
+} // extern "C"
+
+// lphi4 clb_set_state from host or device arrays; means (fields then momenta, one per scalar) are
+// the FP32 split form's references, computed here from host arrays when null.
+__attribute__((visibility("hidden"))) int clb::scalar_set_state(clb_handle *h, const double *fields, const double *momenta,
+                                                                const clb_scalefactor *sf, const double *means)
+{
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_set_state");
   h->cf = h->cp = 0;
   h->rs = 0;
   // FP32 split storage: each component is stored as its deviation from its FP64 volume mean
   CompOffsets fo{{0.0, 0.0}}, po{{0.0, 0.0}};
-  if (h->fp32) {
+  if (h->fp32 && means) {
+    for (int f = 0; f < h->NS; ++f) {
+      fo.v[f] = means[f];
+      po.v[f] = means[2 + f];
+    }
+  } else if (h->fp32) {
     for (int f = 0; f < h->NS; ++f) {
       double sf_ = 0, sp_ = 0;
       const double *fa = fields + (size_t)f * h->n3, *pa = momenta + (size_t)f * h->n3;
@@ -708,6 +725,8 @@ int clb_set_state(clb_handle *h, const double *fields, const double *momenta, co
   h->synced = true;
   return CLB_OK;
 }
+
+extern "C" {
 
 int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf)
 {

@@ -111,13 +111,13 @@ namespace {
 
 enum KKind {
   K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_SPECTRUM,
-  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_U1_ADJ, K_NKINDS
+  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_U1_ADJ, K_INIT, K_NKINDS
 };
 const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
                                           "scalar_drift",       "reduce_pi2",        "reduce_fields",
                                           "tail",               "measure",           "convert",
                                           "spectrum",           "gauge_kick_sweep",  "gauge_drift",
-                                          "gauge_reduce",       "u1_adjoint_sweep"};
+                                          "gauge_reduce",       "u1_adjoint_sweep",  "initial_conditions"};
 
 cudaEvent_t take_event(clb_handle *h)
 {

@@ -356,14 +356,14 @@ __attribute__((visibility("hidden"))) int su2_set_state(clb_handle *h, const dou
   cudaError_t e = cudaStreamSynchronize(h->stream);
   free_tangent(u); // a new state ends the tangent-linear form
   if (!u->fp32) {
-    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, NF * h->n3 * sizeof(double), cudaMemcpyDefault, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, NP * h->n3 * sizeof(double), cudaMemcpyDefault, h->stream);
   } else {
     // one component at a time through the FP64 staging buffer
     for (int c = 0; c < NF + NP && e == cudaSuccess; ++c) {
       const double *src = c < NF ? fields + (size_t)c * h->n3 : momenta + (size_t)(c - NF) * h->n3;
       float *dst = static_cast<float *>(c < NF ? u->f : u->p) + (size_t)(c < NF ? c : c - NF) * h->n3;
-      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyDefault, h->stream);
       if (e == cudaSuccess) k_convert<double, float><<<kSU2Blocks, 256, 0, h->stream>>>(u->d_stage, dst, h->n3);
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }

@@ -319,14 +319,14 @@ __attribute__((visibility("hidden"))) int u1_set_state(clb_handle *h, const doub
   const size_t bytes = 5 * h->n3 * sizeof(double);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (!u->fp32) {
-    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, bytes, cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->f, fields, bytes, cudaMemcpyDefault, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u->p, momenta, bytes, cudaMemcpyDefault, h->stream);
   } else {
     // one component at a time through the FP64 staging buffer, rounded once to FP32
     for (int c = 0; c < 10 && e == cudaSuccess; ++c) {
       const double *src = (c < 5 ? fields : momenta) + (size_t)(c % 5) * h->n3;
       float *dst = static_cast<float *>(c < 5 ? u->f : u->p) + (size_t)(c % 5) * h->n3;
-      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+      e = cudaMemcpyAsync(u->d_stage, src, h->n3 * sizeof(double), cudaMemcpyDefault, h->stream);
       if (e == cudaSuccess) k_convert<double, float><<<kU1Blocks, 256, 0, h->stream>>>(u->d_stage, dst, h->n3);
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }

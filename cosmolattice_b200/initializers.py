@@ -373,3 +373,40 @@ def u1_initial_state_tangent(model: Model, rp: RunParameters, param: str, state=
     for i in range(3):
         dp[2 + i] = pa[i]
     return df, dp
+
+
+def device_ic_params(model: Model, rp: RunParameters, seed: int = None) -> dict:
+    """clb_ic_params for model (matter components in the model's field order) and the initial
+    (aI, aDotI) of initial_scale_factor, as ({...}, aI, aDot).  seed defaults to 64 bits of
+    sha256(baseSeed)."""
+    aI, aDot = initial_scale_factor(model, rp)
+    if seed is None:
+        seed = int.from_bytes(hashlib.sha256(f"{rp.baseSeed}|device".encode()).digest()[:8], "little")
+    fs, ws = model.fStar, model.omegaStar
+    amp = ws / fs if model.fluct_amplitude is None else model.fluct_amplitude
+    if getattr(model, "NSU2", 0):
+        m2 = [model.masses2S[0]] + list(model.masses2CS[:2]) + list(model.masses2D[:4])
+        f0 = [model.fldS0[0] / fs] + [c / fs for c in model.fldCS0[:2]] + [c / fs for c in model.fldD0[:4]]
+        p0 = [model.piS0[0] / fs / ws] + [c / fs / ws for c in model.piCS0[:2]] + [c / fs / ws for c in model.piD0[:4]]
+        charge = [model.gQ_S, model.gQ_C, model.gQ_D, 0.0]
+    elif getattr(model, "NU1", 0):
+        m2 = list(model.masses2CS[:2])
+        f0 = [c / fs for c in model.fldCS0[:2]]
+        p0 = [c / fs / ws for c in model.piCS0[:2]]
+        charge = [model.gQ, 0.0, 0.0, 0.0]
+    else:
+        m2 = list(model.masses2S)
+        f0 = [v / fs for v in model.fldS0]
+        p0 = [v / fs / ws for v in model.piS0]
+        charge = [0.0] * 4
+    return ({"seed": int(seed), "amplitude": amp, "k_cutoff": rp.kCutoff, "adot": aDot,
+             "mass2": m2, "fld0": f0, "pi0": p0, "charge": charge}, aI, aDot)
+
+
+def device_initial_state(lattice, model: Model, rp: RunParameters, seed: int = None) -> dict:
+    """Generate the initial state on the device (clb_generate_state) into lattice; returns the
+    parameters used (device_ic_params) with aI and aDotI added."""
+    p, aI, aDot = device_ic_params(model, rp, seed)
+    lattice.generate_state(p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aDot, "aDotSI": aDot})
+    p.update(aI=aI, aDotI=aDot)
+    return p

@@ -80,6 +80,23 @@ class Lattice:
             s = _capi.ScaleFactor(**{k: float(sf.get(k, 0.0)) for k in ("aI", "aSI", "aIM", "aDotI", "aDotSI", "aDotSIM")})
         self._check(self.lib.clb_set_state(self.h, _dp(f), _dp(p), C.byref(s) if s is not None else None))
 
+    def generate_state(self, params: Dict[str, object], sf: Optional[Dict[str, float]] = None) -> None:
+        """clb_generate_state: the initial state drawn and transformed on the device.  params: seed,
+        amplitude, k_cutoff, adot, and per matter component mass2, fld0, pi0; charge."""
+        p = _capi.ICParams()
+        p.seed = int(params["seed"]) & ((1 << 64) - 1)
+        for k in ("amplitude", "k_cutoff", "adot"):
+            setattr(p, k, float(params[k]))
+        for k, n in (("mass2", _capi.IC_MAX), ("fld0", _capi.IC_MAX), ("pi0", _capi.IC_MAX), ("charge", 4)):
+            v = list(params.get(k, ()))
+            if len(v) > n:
+                raise ValueError(f"{k}: at most {n} values")
+            getattr(p, k)[:] = [float(x) for x in v] + [0.0] * (n - len(v))
+        s = None
+        if sf is not None:
+            s = _capi.ScaleFactor(**{k: float(sf.get(k, 0.0)) for k in ("aI", "aSI", "aIM", "aDotI", "aDotSI", "aDotSIM")})
+        self._check(self.lib.clb_generate_state(self.h, C.byref(p), C.byref(s) if s is not None else None))
+
     def get_state(self, fields: bool = True, momenta: bool = True):
         n3 = self.rp.N ** 3
         f = np.empty(self.n_field_components * n3) if fields else None

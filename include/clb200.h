@@ -144,6 +144,30 @@ int clb_num_components(const clb_handle *h, int32_t *n_field_components, int32_t
  * of ModelInitializer::initialize (modelinitializer.h:54-69). */
 int clb_set_state(clb_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf);
 
+/* Initial state generated on the device (replaces the host generator; the reference's
+ * ModelInitializer::initialize field part, modelinitializer.h:51-69): fluctuations by
+ * FluctuationsGenerator::conjugateGaussianFluctuations for singlets (fluctuationsgenerator.h:39-71,
+ * 130-150), U1Initializer::addFluctuationsCScalarFromPhases for the complex scalar
+ * (u1initializer.h:157-230), SU2Initializer::addFluctuationsSU2DoubletFromPhases for the doublet
+ * (su2initializer.h:115-186); gauge momenta from the Gauss laws with A = 0 and unit links
+ * (u1initializer.h:90-114, su2initializer.h:65-85); then the homogeneous parts.  Random numbers:
+ * Philox4x64-10 with key (seed, stream) and counter (mode index, 0, 0, 0); the kz = 0 and N/2
+ * planes are Hermitian.  Matter components in the model's field order: lphi4 singlets 0..Ns-1;
+ * lphi4U1 Re phi, Im phi; lphi4SU2U1 S, Re phi, Im phi, Phi_1..Phi_4.  sf as in clb_set_state. */
+#define CLB_IC_MAX 8
+typedef struct clb_ic_params {
+  uint64_t seed;
+  double amplitude;          /* omega_* / f_* in the reference (fluctuationsgenerator.h:91-98)      */
+  double k_cutoff;           /* modes with |k| > k_cutoff (program units) are 0                     */
+  double adot;               /* aDot of the homogeneous background, in pi_k = ... - aDot phi_k       */
+  double mass2[CLB_IC_MAX];  /* m^2 per matter component (program units); omega_k = sqrt(k^2 + max(m^2, 0)) */
+  double fld0[CLB_IC_MAX];   /* homogeneous field values (program units)                             */
+  double pi0[CLB_IC_MAX];    /* homogeneous momenta (program units)                                  */
+  double charge[4];          /* lphi4U1: g Q; lphi4SU2U1: g Q of the doublet under SU(2), g Q of the
+                                complex scalar and of the doublet under U(1)                         */
+} clb_ic_params;
+int clb_generate_state(clb_handle *h, const clb_ic_params *p, const clb_scalefactor *sf);
+
 /* Download the state (fields, momenta may be NULL to skip). */
 int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
 
