@@ -88,8 +88,8 @@ __device__ __forceinline__ void u1_pieces(LD ld, const U1Params &a, size_t s, co
     mim = mim + (vr * hi - vi * hr);
     o.im[d] = wr * fi - wi * fr;
   }
-  o.cl[0] = (pr + mr - 6.0 * fr) / a.dx2;
-  o.cl[1] = (pim + mim - 6.0 * fi) / a.dx2;
+  o.cl[0] = (pr + mr - 6.0 * fr) * a.inv_dx2;
+  o.cl[1] = (pim + mim - 6.0 * fi) * a.inv_dx2;
   const TD n2 = fr * fr + fi * fi;
   o.dv[0] = (4.0 * a.c4) * (n2 * fr);
   o.dv[1] = (4.0 * a.c4) * (n2 * fi);
@@ -107,7 +107,7 @@ __device__ __forceinline__ void u1_pieces(LD ld, const U1Params &a, size_t s, co
       const size_t sij = i == j ? s : s + op[i] + om[j];
       acc = acc - ((ld(2 + j, s + op[i]) - ld(2 + j, s)) - (ld(2 + j, sij) - ld(2 + j, s + om[j])));
     }
-    o.cc[i] = acc / a.dx2;
+    o.cc[i] = acc * a.inv_dx2;
   }
 }
 
@@ -148,6 +148,10 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
   const double two_n3 = 2.0 * g.inv_n3;
   const double cP = (g.ApiA + g.ApiB) * two_n3, cE = (g.AEA + g.AEB) * two_n3;
   const double kJ = g.kA * g.J0 * a.gQ;
+  // loop invariants; the adjoint is not bound to the forward's rounding order, so its divides
+  // by dx^2 and by m_A^-1 are multiplies by reciprocals
+  const double inv_r2 = 1.0 / g.r2, cJ = g.kA * g.J0 * inv_r2, cD = g.AD * g.inv_n3 * (2.0 * a.gQ / a.dx);
+  const double two_dx = 2.0 / a.dx, dJ = g.dkA * g.J0 * a.gQ;
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
@@ -178,13 +182,13 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
     qb[0] += K[0].d;
     qb[1] += K[1].d;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) qb[2 + i] += K[2 + i].d / g.r2;
+    for (int i = 0; i < 3; ++i) qb[2 + i] += K[2 + i].d * inv_r2;
     // gradients of the field averages
 #pragma unroll
     for (int c = 0; c < 2; ++c) qb[c] += g.AD * (-two_n3) * o.cl[c].v + g.AV * g.inv_n3 * o.dv[c].v;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-      qb[2 + i] += g.AD * g.inv_n3 * (2.0 * a.gQ / a.dx) * o.im[i].v + g.AB * (-two_n3) * o.cc[i].v;
+      qb[2 + i] += cD * o.im[i].v + g.AB * (-two_n3) * o.cc[i].v;
     // scale-factor and coupling dot products
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -195,13 +199,13 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const double da = g.dkG * o.cc[i].v - g.dkA * g.J0 * a.gQ * o.im[i].v;
+      const double da = g.dkG * o.cc[i].v - dJ * o.im[i].v;
       acc[0] += g.hA[1] * lA[2 + i] * da;
       acc[1] += g.hB[1] * lB[2 + i] * da;
       const double Ai = (double)f[(2 + i) * n3 + s];
       const double wi = g.r2 * (g.hA[1] * lA[2 + i] + g.hB[1] * lB[2 + i]);
-      acc[2] += -(g.kA * g.J0 / g.r2) * (Ai * o.im[i].d + wi * o.im[i].v);
-      acc[4] += (2.0 / a.dx) * Ai * o.im[i].v;
+      acc[2] += -cJ * (Ai * o.im[i].d + wi * o.im[i].v);
+      acc[4] += two_dx * Ai * o.im[i].v;
     }
     acc[5] += o.n4;
     // part B's transposed drift: pbar = lambda_B + dt w D qbar; its aS dot uses the momentum

@@ -468,6 +468,7 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__
   double v[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) v[k] = 0;
+#pragma unroll 5
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
     for (int k = 0; k < NV; ++k) v[k] += partials[(size_t)b * NV + k];

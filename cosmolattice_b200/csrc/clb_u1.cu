@@ -181,7 +181,7 @@ template <int NK, bool RED, class S> void kick_save_t(clb_handle *h, const U1Kic
 {
   U1Sector *u = h->u1;
   CLB_LAUNCH(h, K_U1_KICK,
-             k_u1_kick<NK, RED, RED, S, true><<<kU1Blocks, 256, 0, h->stream>>>(
+             k_u1_kick<NK, RED, RED, S, true, true><<<kU1Blocks, 256, 0, h->stream>>>(
                  static_cast<const S *>(u->f), static_cast<S *>(u->p), u->prm, kc, u->d_st, u->d_part,
                  reinterpret_cast<S *>(slot), reinterpret_cast<S *>(slot + half)));
 }
@@ -231,9 +231,15 @@ void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
         kick_save_s<float>(h, more ? 2 : 1, ex, vv_kick(dt, w, wn), slot, sv->half);
       else
         kick_save_s<double>(h, more ? 2 : 1, ex, vv_kick(dt, w, wn), slot, sv->half);
-      if (ex) tail(h, T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, true, w, 0);
-      k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, k + 1);
-      if (ex && more) tail(h, T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT, true, w, wn);
+      if (ex) {
+        // first kick's tail, the boundary record, second kick's tail: one launch
+        U1Sector *u = h->u1;
+        const TailOp a{T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE, kU1Blocks, w, 0.0, nullptr, -1};
+        const TailOp b{more ? (uint32_t)(T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT) : 0u, kU1Blocks, w, wn, nullptr, -1};
+        CLB_LAUNCH(h, K_TAIL, k_u1_tail_split<<<1, 256, 0, h->stream>>>(u->d_part, a, b, u->d_st, u->prm, sv->rec, k + 1));
+      } else {
+        k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, k + 1);
+      }
     }
   }
 }
@@ -685,9 +691,11 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
 }
 
 // Backward pass: cotangents of the forward start state and of the couplings for the observable
-// of the last u1_forward.  Segments are recomputed from their checkpoints with the forward's
-// merged schedule (bitwise the forward states), keeping every stage-boundary state and scalar
-// record; then one fused adjoint sweep per boundary walks the segment backwards (part A: the
+// of the last u1_forward.  Segments are recomputed from their (bitwise) checkpoints with the
+// forward's merged schedule, keeping every stage-boundary state and scalar record; the FP64
+// recompute evaluates the kernel in FD arithmetic (contracted, divisions as reciprocal multiplies),
+// which moves the linearisation point by rounding only.  Then one fused adjoint sweep per
+// boundary walks the segment backwards (part A: the
 // first kick of the stage starting there, part B: the second kick of the stage ending there).
 // With through_init the start state is taken as produced by clb_initialize(correct_adot = 1),
 // whose aDot = sqrt(Friedmann RHS) (modelinitializer.h:77-78) is differentiated too.

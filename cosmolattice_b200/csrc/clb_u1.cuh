@@ -19,6 +19,8 @@
 
 #include "clb_internal.cuh"
 
+#include <type_traits>
+
 namespace clb {
 
 constexpr int kU1Red = 7;   // kick-sweep partial slots (see k_u1_kick)
@@ -67,6 +69,23 @@ __device__ __forceinline__ float u1_s(float a, float b) { return a - b; }
 __device__ __forceinline__ float u1_d(float a, float b) { return a / b; }
 __device__ __forceinline__ void u1_sincos(double x, double *sn, double *cs) { sincos(x, sn, cs); }
 __device__ __forceinline__ void u1_sincos(float x, float *sn, float *cs) { sincosf(x, sn, cs); }
+
+// FP64 arithmetic of the adjoint's segment recompute, which is not bound to the reference's
+// rounding order: products and sums may contract into FMAs, and a division becomes a multiply by
+// the divisor's reciprocal (formed once per site for the lattice spacing).
+struct FD {
+  double v;
+  FD() = default;
+  __host__ __device__ constexpr FD(double x) : v(x) {}
+  __host__ __device__ explicit constexpr operator double() const { return v; }
+};
+__device__ __forceinline__ FD u1_m(FD a, FD b) { return FD(a.v * b.v); }
+__device__ __forceinline__ FD u1_a(FD a, FD b) { return FD(a.v + b.v); }
+__device__ __forceinline__ FD u1_s(FD a, FD b) { return FD(a.v - b.v); }
+__device__ __forceinline__ FD u1_d(FD a, FD b) { return FD(a.v * (1.0 / b.v)); }
+__device__ __forceinline__ FD operator-(FD a) { return FD(-a.v); }
+__device__ __forceinline__ FD sqrt(FD a) { return FD(::sqrt(a.v)); }
+__device__ __forceinline__ void u1_sincos(FD x, FD *sn, FD *cs) { sincos(x.v, &sn->v, &cs->v); }
 
 // Per-site kernel values in arithmetic type T.  Fields f (storage S): [Re phi, Im phi, A_x, A_y,
 // A_z] x n3.  The FP64 form (S = T = double) pins every rounding; the FP32 form computes in float.
@@ -194,27 +213,29 @@ template <class T> __device__ __forceinline__ T u1_pot(const U1Site<T> &o, T c4)
 #define CLB_U1_KICK_MINB 2
 #endif
 // SAVE (adjoint recompute): also writes the fields and the momenta after the first kick, the state
-// at the stage boundary between the two kicks, to save_f / save_p.
-template <int NK, bool RF, bool RP, class S, bool SAVE = false>
+// at the stage boundary between the two kicks, to save_f / save_p.  FAST (FP64 storage only):
+// the kernel values in FD arithmetic.
+template <int NK, bool RF, bool RP, class S, bool SAVE = false, bool FAST = false>
 __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
     k_u1_kick(const S *__restrict__ f, S *__restrict__ p, U1Params a, U1Kick kc, const U1State *__restrict__ st,
               double *__restrict__ partials, S *__restrict__ save_f = nullptr, S *__restrict__ save_p = nullptr)
 {
   __shared__ double smem[(256 / 32) * kU1Red];
+  using T = typename std::conditional<FAST && sizeof(S) == 8, FD, S>::type;
   const size_t n3 = a.n3;
-  const S kA = (S)st->kA, kB2 = (S)st->kB2, kG = (S)st->kG;
+  const T kA = (T)st->kA, kB2 = (T)st->kB2, kG = (T)st->kG;
   double acc[kU1Red];
 #pragma unroll
   for (int k = 0; k < kU1Red; ++k) acc[k] = 0;
   for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
-    U1Site<S> o;
+    U1Site<T> o;
     u1_site<(NK > 0)>(f, a, s, op, om, kA, kB2, kG, o);
     if (RF) {
-      acc[2] += (double)u1_cs_grad2(o, (S)a.dx);
+      acc[2] += (double)u1_cs_grad2(o, (T)a.dx);
       acc[3] += (double)u1_b2(o);
-      acc[4] += (double)u1_pot(o, (S)a.c4);
+      acc[4] += (double)u1_pot(o, (T)a.c4);
     }
     // momenta and their increments in FP64 (FP32 storage: rounded once per kick)
     double q[5];
@@ -289,22 +310,25 @@ __device__ __forceinline__ double u1_sf_kernel(const U1State &s, const U1Params 
 
 // One-thread tail: fixed-order sum of the kick-sweep partials and the scale-factor update, in
 // the order of the VelocityVerlet and LeapFrog schedules (same flags as the scalar tail).
-static __global__ void __launch_bounds__(256)
-    k_u1_tail(const double *__restrict__ partials, TailOp op, U1State *__restrict__ st, U1Params p)
+// Fixed-order sum of the kick-sweep partial rows (all threads of one 256-thread block; the
+// totals are valid in thread 0).
+__device__ __forceinline__ void u1_reduce_partials(const double *__restrict__ partials, int nblocks,
+                                                   double (&v)[kU1Red], double *smem)
 {
-  __shared__ double smem[(256 / 32) * kU1Red];
-  double v[kU1Red];
 #pragma unroll
   for (int k = 0; k < kU1Red; ++k) v[k] = 0;
-  if (op.nblocks > 0) {
-    for (int b = threadIdx.x; b < op.nblocks; b += blockDim.x) {
+  if (nblocks <= 0) return;
+#pragma unroll 5
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
-      for (int k = 0; k < kU1Red; ++k) v[k] += partials[(size_t)b * kU1Red + k];
-    }
-    block_reduce<kU1Red, 256>(v, smem);
+    for (int k = 0; k < kU1Red; ++k) v[k] += partials[(size_t)b * kU1Red + k];
   }
-  if (threadIdx.x != 0) return;
-  U1State s = *st;
+  block_reduce<kU1Red, 256>(v, smem);
+}
+
+// The scale-factor update of one tail on the state s from the reduced sums v.
+__device__ __forceinline__ void u1_tail_apply(U1State &s, const double (&v)[kU1Red], const TailOp &op, const U1Params &p)
+{
   const double csP = v[0] * p.inv_n3, u1P = v[1] * p.inv_n3, csG = v[2] * p.inv_n3, u1B = v[3] * p.inv_n3;
   const double pot = v[4] * p.inv_n3, csP2 = v[5] * p.inv_n3, u1P2 = v[6] * p.inv_n3;
   const double dt = p.dt;
@@ -383,6 +407,36 @@ static __global__ void __launch_bounds__(256)
   if (!isfinite(s.aI) || !isfinite(s.aDotI) || !isfinite(s.aDotSI) || !isfinite(s.csPi2I) || !isfinite(s.u1Pi2I) ||
       !isfinite(s.csGrad2I) || !isfinite(s.u1Mag2I) || !isfinite(s.potI))
     s.status = 1;
+}
+
+static __global__ void __launch_bounds__(256)
+    k_u1_tail(const double *__restrict__ partials, TailOp op, U1State *__restrict__ st, U1Params p)
+{
+  __shared__ double smem[(256 / 32) * kU1Red];
+  double v[kU1Red];
+  u1_reduce_partials(partials, op.nblocks, v, smem);
+  if (threadIdx.x != 0) return;
+  U1State s = *st;
+  u1_tail_apply(s, v, op, p);
+  *st = s;
+}
+
+// A stage boundary of the adjoint's segment recompute in one launch: the tail of the merged
+// sweep's first kick (a), the boundary's record row, then the tail of its second kick (b, if
+// b.flags), both from one reduction of the partials; the same values as k_u1_tail(a),
+// k_u1_record, k_u1_tail(b).
+static __global__ void __launch_bounds__(256)
+    k_u1_tail_split(const double *__restrict__ partials, TailOp a, TailOp b, U1State *__restrict__ st, U1Params p,
+                    U1State *__restrict__ rec, int64_t row)
+{
+  __shared__ double smem[(256 / 32) * kU1Red];
+  double v[kU1Red];
+  u1_reduce_partials(partials, a.nblocks, v, smem);
+  if (threadIdx.x != 0) return;
+  U1State s = *st;
+  u1_tail_apply(s, v, a, p);
+  rec[row] = s;
+  if (b.flags) u1_tail_apply(s, v, b, p);
   *st = s;
 }
 
