@@ -381,8 +381,10 @@ def main_u1_adjoint(args):
     state = u1_initial_state(m, rp)
     tangents = {prm: u1_initial_state_tangent(m, rp, prm, state) for prm in ("amp", "c4", "gQ")}
     setup_s = time.perf_counter() - t0
+    # one untimed gradient first (module loading, checkpoint and segment allocation), then the timed one
     lat = Lattice(m, rp)
     lat.set_profiling(False)
+    u1_gradients(m, rp, steps, args.checkpoint_every, GAUGE_FRACTION, lattice=lat, state=state, tangents=tangents)
     O, grads, rec = u1_gradients(m, rp, steps, args.checkpoint_every, GAUGE_FRACTION, lattice=lat, state=state,
                                  tangents=tangents)
     t_total = rec["forward_s"] + rec["backward_s"]
@@ -391,6 +393,7 @@ def main_u1_adjoint(args):
     # FP32/FP64 split: FP32 state storage and stencils, FP64 increments, sums and cotangents
     lat = Lattice(m, rp, precision="fp32")
     lat.set_profiling(False)
+    u1_gradients(m, rp, steps, args.checkpoint_every, GAUGE_FRACTION, lattice=lat, state=state, tangents=tangents)
     O32, grads32, rec32 = u1_gradients(m, rp, steps, args.checkpoint_every, GAUGE_FRACTION, lattice=lat,
                                        state=state, tangents=tangents)
     t_total32 = rec32["forward_s"] + rec32["backward_s"]

@@ -622,25 +622,31 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward");
-  free_adjoint(u);
   const size_t bytes = 5 * h->n3 * u->esz, dbytes = 5 * h->n3 * sizeof(double);
   const int64_t nck = (nsteps + K - 1) / K;
   const int64_t S = 2 * (int64_t)h->ws.size() - 1;
   const int64_t seg_states = std::min<int64_t>(K, nsteps) * S + 1;
-  bool ok = true;
-  u->ckpt.resize((size_t)nck + 1); // + the end state, restored after the backward pass
-  for (auto &c : u->ckpt) ok = ok && cudaMalloc(&c.f, bytes) == cudaSuccess && cudaMalloc(&c.p, bytes) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->seg, (size_t)seg_states * 2 * bytes) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->d_rec, (size_t)seg_states * sizeof(U1State)) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->qbar, dbytes) == cudaSuccess && cudaMalloc(&u->pbar[0], dbytes) == cudaSuccess &&
-       cudaMalloc(&u->pbar[1], dbytes) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->d_apart, (size_t)kU1Blocks * kAdjSlots * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc(&u->d_asums, kAdjSlots * sizeof(double)) == cudaSuccess;
-  if (!ok) {
+  // the storage of the previous pair is kept when its layout fits (same checkpoint count and
+  // segment length); the observable is reset either way
+  u->fwd_steps = -1;
+  u->seed_which = -1;
+  if (!(u->ckpt.size() == (size_t)nck + 1 && u->seg_cap == seg_states && u->qbar)) {
     free_adjoint(u);
-    return h->fail(CLB_ENOMEM, "clb_forward: checkpoint or segment storage does not fit; use a smaller checkpoint_every");
+    bool ok = true;
+    u->ckpt.resize((size_t)nck + 1); // + the end state, restored after the backward pass
+    for (auto &c : u->ckpt) ok = ok && cudaMalloc(&c.f, bytes) == cudaSuccess && cudaMalloc(&c.p, bytes) == cudaSuccess;
+    ok = ok && cudaMalloc(&u->seg, (size_t)seg_states * 2 * bytes) == cudaSuccess;
+    ok = ok && cudaMalloc(&u->d_rec, (size_t)seg_states * sizeof(U1State)) == cudaSuccess;
+    ok = ok && cudaMalloc(&u->qbar, dbytes) == cudaSuccess && cudaMalloc(&u->pbar[0], dbytes) == cudaSuccess &&
+         cudaMalloc(&u->pbar[1], dbytes) == cudaSuccess;
+    ok = ok && cudaMalloc(&u->d_apart, (size_t)kU1Blocks * kAdjSlots * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&u->d_asums, kAdjSlots * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+      free_adjoint(u);
+      return h->fail(CLB_ENOMEM, "clb_forward: checkpoint or segment storage does not fit; use a smaller checkpoint_every");
+    }
+    u->seg_cap = seg_states;
   }
-  u->seg_cap = seg_states;
   cudaEventRecord(h->ev_call[0], h->stream);
   for (int64_t c = 0; c < nck; ++c) {
     U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
