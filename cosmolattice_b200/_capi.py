@@ -22,7 +22,8 @@ CLB_EUNSUPPORTED = -6
 CLB_ESTATE = -7
 
 # evolver ids, numbered as the reference's EvolverType (evolvers/evolvertype.h:37)
-EVOLVERS = {"LF": 0, "VV2": 1, "VV4": 2, "VV6": 3, "VV8": 4, "VV10": 5, "VV6_2": 6}
+EVOLVERS = {"LF": 0, "VV2": 1, "VV4": 2, "VV6": 3, "VV8": 4, "VV10": 5, "VV6_2": 6,
+            "PV2": 11, "PV4": 12, "PV6": 13, "PV8": 14, "PV10": 15, "PV6_2": 16}
 EVOLVER_NAMES = {v: k for k, v in EVOLVERS.items()}
 
 PREC_FP64 = 0

@@ -126,8 +126,9 @@ template <class R> R *F(clb_handle *h, int b) { return static_cast<R *>(h->fld[b
 template <class R> R *P(clb_handle *h, int b) { return static_cast<R *>(h->pi[b]); }
 
 // ---- kernel launchers (templated on storage type and field count) ----------------------------
-template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
-void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2)
+template <class R, int NS, class SH, int DRIFT, bool KICK, int RED>
+void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2,
+              double dtw0 = 0.0)
 {
   static bool attr_set = false;
   if (!attr_set) {
@@ -139,6 +140,7 @@ void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dt
   a.dtw = dtw;
   a.h1 = h1;
   a.h2 = h2;
+  a.dtw0 = dtw0;
   a.rs = h->rs;
   if (h->pdl_now)
     CLB_LAUNCH(h, kind,
@@ -153,14 +155,15 @@ void sweep_sh(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dt
   if (sizeof(R) == 4 && (DRIFT || KICK)) h->rs ^= 1; // the launch advanced the FP64 references
 }
 
-template <class R, int NS, bool DRIFT, bool KICK, int RED>
-void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2)
+template <class R, int NS, int DRIFT, bool KICK, int RED>
+void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, double h1, double h2,
+           double dtw0 = 0.0)
 {
   if constexpr (NS == 1) {
-    if (h->shape == 1) return sweep_sh<R, NS, ShapeQ, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
-    if (h->shape == 2) return sweep_sh<R, NS, ShapeH, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
+    if (h->shape == 1) return sweep_sh<R, NS, ShapeQ, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
+    if (h->shape == 2) return sweep_sh<R, NS, ShapeH, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
   }
-  sweep_sh<R, NS, ShapeW, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2);
+  sweep_sh<R, NS, ShapeW, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
 }
 
 template <class R, int NS> struct Launch {
@@ -177,6 +180,18 @@ template <class R, int NS> struct Launch {
       sweep<R, NS, true, true, 3>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, h1, h2);
     else
       sweep<R, NS, true, true, 0>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, h1, h2);
+    h->cf = nf;
+    h->cp = np;
+  }
+  // position-Verlet stage after the first: the previous stage's second drift (dtw0) and this
+  // stage's first drift (dtw), each rounded as the reference's, kick (hk), averages
+  static void fused_pv(clb_handle *h, double dtw0, double dtw, double hk, bool red)
+  {
+    const int nf = h->cf ^ 1, np = h->cp ^ 1;
+    if (red)
+      sweep<R, NS, 2, true, 3>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, hk, 0.0, dtw0);
+    else
+      sweep<R, NS, 2, true, 0>(h, K_FUSED, h->cf, h->cp, nf, np, dtw, hk, 0.0, dtw0);
     h->cf = nf;
     h->cp = np;
   }
@@ -371,6 +386,63 @@ template <class R, int NS> struct EvolveVV {
   }
 };
 
+// PositionVerlet::evolve, n steps (positionverlet.h:45-99).  A stage: drift(dt/2 w) at
+// pow(aI, alpha - 3), the first a half-drift, the half-step field averages, kick(w dt) at the
+// half-step a, the momentum averages, the a-kick (getSI), the second a half-drift, drift(dt/2 w) at
+// the new a, the field averages.
+template <class R, int NS> struct EvolvePV {
+  static void run(clb_handle *h, int64_t nsteps)
+  {
+    using L = Launch<R, NS>;
+    const double dt = h->cfg.dt;
+    const bool ex = h->cfg.expansion != 0;
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    if (nsteps <= 0) return;
+    if (h->cfg.path == CLB_PATH_REFERENCE) {
+      tail(h, T_PV_MODE, 0); // the drift coefficient of the current a
+      for (int64_t s = 0; s < nsteps; ++s)
+        for (size_t i = 0; i < S; ++i) {
+          const double w = wof(i);
+          L::drift(h, dt / 2 * w); // driftScalar
+          if (ex) tail(h, T_PV_MODE | T_PV_STORE_SI | T_PV_DRIFT_A1, L::reduce_fields(h, false), 0, w);
+          L::kick(h, w * dt); // kickScalar
+          if (ex) tail(h, T_PV_MODE | T_PV_STORE_PI2 | T_PV_KICK | T_PV_DRIFT_A2, L::reduce_pi2(h), w, 0);
+          L::drift(h, dt / 2 * w);
+          if (ex) tail(h, T_PV_MODE | T_STORE_FIELDS, L::reduce_fields(h, false), 0, 0, i + 1 == S ? s : -1);
+        }
+      return;
+    }
+    // Fused: one sweep per stage drifts (the previous stage's second drift and this stage's first,
+    // which act with the same a and pi), kicks and reduces the half-step field averages and <pi^2>;
+    // its tail books them, kicks a, finishes this stage's a-drift and starts the next one's.  Each
+    // step ends with its own drift sweep, whose averages are the integer-time ones.
+    const double w0 = wof(0);
+    tail(h, T_PV_MODE | (ex ? T_PV_DRIFT_A1 : 0u), 0, 0, w0);
+    h->pdl_now = h->pdl;
+    for (int64_t s = 0; s < nsteps; ++s)
+      for (size_t i = 0; i < S; ++i) {
+        const double w = wof(i);
+        const bool last = i + 1 == S;
+        if (i == 0)
+          L::fused(h, dt / 2 * w, w * dt, 0.0, ex);
+        else
+          L::fused_pv(h, dt / 2 * wof(i - 1), dt / 2 * w, w * dt, ex);
+        if (ex) {
+          uint32_t fl = T_PV_MODE | T_PV_STORE_SI | T_PV_STORE_PI2 | T_PV_KICK | T_PV_DRIFT_A2;
+          if (!last) fl |= T_PV_DRIFT_A1;
+          tail(h, fl, h->sweep_blocks, w, last ? 0.0 : wof(i + 1));
+        }
+        if (last) {
+          L::drift_fields(h, dt / 2 * w, ex);
+          if (ex) tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), h->sweep_blocks, 0, w0, s);
+        }
+      }
+    h->pdl_now = false;
+  }
+};
+
 // LeapFrog::evolve, n steps (leapfrog.h:42-89).
 template <class R, int NS> struct EvolveLF {
   static void run(clb_handle *h, int64_t nsteps)
@@ -502,8 +574,12 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_EINVAL;
   }
   std::vector<double> ws;
+  if (is_pv(cfg->evolver) && (u1 || su2)) {
+    g_err = "clb_create: position Verlet evolves the scalar-singlet models here";
+    return CLB_EUNSUPPORTED;
+  }
   if (cfg->evolver != CLB_LF) {
-    ws = vv_coefficients(cfg->evolver);
+    ws = is_pv(cfg->evolver) ? pv_coefficients(cfg->evolver) : vv_coefficients(cfg->evolver);
     if (ws.empty()) {
       g_err = "clb_create: The evolver type you specified was not implemented in the Evolver class";  // evolver.h:366-368
       return CLB_EUNSUPPORTED;
@@ -804,6 +880,8 @@ int clb_evolve(clb_handle *h, int64_t n)
   cudaEventRecord(h->ev_call[0], h->stream);
   if (h->cfg.evolver == CLB_LF)
     dispatch<EvolveLF>(h, n);
+  else if (is_pv(h->cfg.evolver))
+    dispatch<EvolvePV>(h, n);
   else
     dispatch<EvolveVV>(h, n);
   cudaEventRecord(h->ev_call[1], h->stream);

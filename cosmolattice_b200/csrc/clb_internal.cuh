@@ -18,8 +18,10 @@ constexpr int kMeasSlots = 16;
 struct DevState {
   double aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
   double pi2AvI, pi2AvSI, pi2AvSIM, grad2AvI, potAvI, potAvSI;
+  double grad2AvSI; // position Verlet: <grad^2> at the half step (positionverlet.h:258-266)
   // coefficients read by the sweeps
-  double drift_p; // pow(aSI, alpha - 3)              (velocityverlet.h:183)
+  double drift_p; // pow(aSI, alpha - 3) (velocityverlet.h:183); position Verlet pow(aI, alpha - 3)
+                  // (positionverlet.h:172)
   double kick_A;  // pow(aI, 1 + alpha)               (scalarsingletkernels.h:266)
   double kick_B;  // pow(aI, 3 + alpha)
   int32_t status; // 0 ok, 1 non-finite average seen
@@ -54,8 +56,15 @@ enum TailFlags : uint32_t {
   T_LF_CTOR = 1u << 10,     // aDotSI = aDotI - dt/2 F                 (leapfrog.h:35)
   T_CORRECT_ADOT = 1u << 11,// aDotI = sqrt(Friedmann RHS)             (modelinitializer.h:77-78)
   T_HIST_EARLY = 1u << 12,  // history row right after the field averages (LF step end)
-  T_STORE_PI2_B = 1u << 13  // a two-kick sweep's second momentum sums become the cached <pi^2>
+  T_STORE_PI2_B = 1u << 13, // a two-kick sweep's second momentum sums become the cached <pi^2>
                             // (after T_VV_KICK_HALF; the gauge sectors' tails)
+  // PositionVerlet (positionverlet.h:45-99, 160-276), applied after the flags above, in this order:
+  T_PV_STORE_SI = 1u << 14,  // grad2AvSI = <grad^2>; potAvSI = <V>      storeFieldsAveragesHalf (:258-266)
+  T_PV_STORE_PI2 = 1u << 15, // pi2AvIM = pi2AvI; pi2AvI = <pi^2>; pi2AvSI = mean  storeMomentaAverages (:238-256)
+  T_PV_KICK = 1u << 16,      // aDotI += dt getSI w                       kickScaleFactor (:160-163)
+  T_PV_DRIFT_A2 = 1u << 17,  // aI += dt/2 aDotI w; aSI = (aIM + aI)/2    driftScaleFactorSecondHalf (:225-234)
+  T_PV_DRIFT_A1 = 1u << 18,  // aIM = aI; aI += dt/2 aDotI w2; aSI = aI    driftScaleFactorFirstHalf (:209-222)
+  T_PV_MODE = 1u << 19       // drift coefficient pow(aI, alpha - 3), of the a before T_PV_DRIFT_A1
 };
 
 struct TailOp {

@@ -345,6 +345,18 @@ __device__ __forceinline__ double sf_kernel(const DevState &s, const SFParams &p
   return __dmul_rn(__dmul_rn(apow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
 }
 
+// ScaleFactorKernels::getSI (scalefactorkernels.h:83-119), scalar singlets: the half-step averages
+// pi2AvSI, grad2AvSI, potAvSI at aI.
+__device__ __forceinline__ double sf_kernel_si(const DevState &s, const SFParams &p)
+{
+  const double al = p.alpha;
+  const double Eks = __dmul_rn(0.5 * s.pi2AvSI, ipow_d(s.aI, -6));
+  const double Egs = __dmul_rn(0.5 * s.grad2AvSI, ipow_d(s.aI, -2));
+  const double br = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(al - 2, Eks), __dmul_rn(al, Egs)), __dmul_rn(al - 1, 0.0)),
+                              __dmul_rn(al + 1, s.potAvSI));
+  return __dmul_rn(__dmul_rn(apow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
+}
+
 // Scale-factor bookkeeping of one tail (the flags of TailOp, in schedule order) given the volume
 // sums of <pi^2>, <grad^2> and <V>; shared by the single-lattice and the batched tails.
 __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const SFParams &p, double pi2s, double g2s,
@@ -408,7 +420,31 @@ __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const 
     s.aI = __dadd_rn(s.aI, __dmul_rn(__dmul_rn(dt, s.aDotSI), op.w2));
     s.aSI = (s.aIM + s.aI) / 2.0;
   }
-  s.drift_p = apow(s.aSI, p.alpha - 3);
+  // PositionVerlet: the field averages at the half step, the momenta's, the a-kick, the second
+  // a half-drift of a stage and the first of the next one
+  if (fl & T_PV_STORE_SI) {
+    s.grad2AvSI = g2;
+    s.potAvSI = pot;
+  }
+  if (fl & T_PV_STORE_PI2) {
+    s.pi2AvSIM = s.pi2AvI; // pi2AvIM
+    s.pi2AvI = pi2;
+    s.pi2AvSI = 0.5 * (s.pi2AvI + s.pi2AvSIM);
+  }
+  if (fl & T_PV_KICK) s.aDotI = __dadd_rn(s.aDotI, __dmul_rn(__dmul_rn(dt, sf_kernel_si(s, p)), op.w));
+  if (fl & T_PV_DRIFT_A2) {
+    s.aI = __dadd_rn(s.aI, __dmul_rn(__dmul_rn(dt / 2.0, s.aDotI), op.w));
+    s.aSI = (s.aIM + s.aI) / 2.0;
+  }
+  if (fl & T_PV_DRIFT_A1) {
+    s.aIM = s.aI;
+    s.aI = __dadd_rn(s.aI, __dmul_rn(__dmul_rn(dt / 2.0, s.aDotI), op.w2));
+    s.aSI = s.aI;
+  }
+  if (fl & T_PV_MODE) // the next field drift happens before the first a half-drift of its stage
+    s.drift_p = apow((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI, p.alpha - 3);
+  else
+    s.drift_p = apow(s.aSI, p.alpha - 3);
   s.kick_A = apow(s.aI, 1 + p.alpha);
   s.kick_B = apow(s.aI, 3 + p.alpha);
   if (!isfinite(s.aI) || !isfinite(s.aDotI) || !isfinite(s.aDotSI) || !isfinite(s.pi2AvI) ||

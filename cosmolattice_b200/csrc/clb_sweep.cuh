@@ -70,6 +70,7 @@ struct SweepArgs {
   uint32_t tries;  // bound of each mbarrier wait
   double inv_dx2, c0, q, c0_quarter, q_half;
   double dtw, h1, h2;
+  double dtw0;     // DRIFT == 2: a first drift of the same kind before dtw's (position Verlet)
 };
 
 // VZ consecutive values from 16-byte-aligned shared memory.
@@ -144,13 +145,14 @@ struct Lphi4SplitCoef {
 
 template <int NS>
 __device__ __forceinline__ RefStep<NS> ref_step(const DevState *st, int rs, bool drift, bool kick, double dtw, double h1,
-                                                double h2, double c0, double q)
+                                                double h2, double c0, double q, double dtw0 = 0.0)
 {
   RefStep<NS> r;
   double phi[NS];
 #pragma unroll
   for (int f = 0; f < NS; ++f) {
     phi[f] = st->ref_phi[rs][f];
+    if (drift && dtw0 != 0.0) phi[f] = __dadd_rn(phi[f], __dmul_rn(st->drift_p, __dmul_rn(dtw0, st->ref_pi[rs][f])));
     if (drift) phi[f] = __dadd_rn(phi[f], __dmul_rn(st->drift_p, __dmul_rn(dtw, st->ref_pi[rs][f])));
     r.phi[f] = phi[f];
   }
@@ -166,10 +168,12 @@ __device__ __forceinline__ RefStep<NS> ref_step(const DevState *st, int rs, bool
   return r;
 }
 
-// DRIFT / KICK / RED as in k_scalar_sweep (clb_scalar.cuh); fout/pout are padded arrays.
+// DRIFT / KICK / RED as in k_scalar_sweep (clb_scalar.cuh), with DRIFT == 2 two successive drifts
+// (dtw0, then dtw) each rounded as the reference's (the end drift of a position-Verlet stage and the
+// first drift of the next); fout/pout are padded arrays.
 // FP32 storage holds fluctuations around the FP64 references (DevState::ref_*): FP32 arithmetic on
 // the fluctuations, with the reference terms of the volume sums added in FP64.
-template <class R, int NS, class SH, bool DRIFT, bool KICK, int RED>
+template <class R, int NS, class SH, int DRIFT, bool KICK, int RED>
 __global__ void __launch_bounds__(SH::THREADS)
     k_sweep(const __grid_constant__ CUtensorMap tmf, const __grid_constant__ CUtensorMap tmp, R *fout, R *pout,
             SweepArgs a, const DevState *__restrict__ st, double *__restrict__ partials, int *__restrict__ err)
@@ -222,10 +226,11 @@ __global__ void __launch_bounds__(SH::THREADS)
     return;
   }
 
-  R pdr = R(0), dtw = R(0), KA = R(0), KB = R(0);
+  R pdr = R(0), dtw = R(0), dtw0 = R(0), KA = R(0), KB = R(0);
   if (DRIFT) {
     pdr = (R)st->drift_p;
     dtw = (R)a.dtw;
+    if (DRIFT == 2) dtw0 = (R)a.dtw0;
   }
   if (KICK) {
     KA = (R)st->kick_A;
@@ -238,7 +243,7 @@ __global__ void __launch_bounds__(SH::THREADS)
   Lphi4SplitCoef spc{};
   const float h1f = (float)a.h1, h2f = (float)a.h2;
   if constexpr (SPLIT) {
-    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.c0, a.q);
+    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.c0, a.q, DRIFT == 2 ? a.dtw0 : 0.0);
     spc = Lphi4SplitCoef::make(rf.phi[0], a.c0);
     if ((DRIFT || KICK) && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
       DevState *sw = const_cast<DevState *>(st); // slot rs ^ 1 is read by no block of this launch
@@ -265,7 +270,10 @@ __global__ void __launch_bounds__(SH::THREADS)
       if (LOADP) tma_load_3d(box(s, f, 1), &tmp, &bars[s], z0, y0, f * N + p);
     }
   };
-  auto drift1 = [&](R phi, R pi) -> R { return DRIFT ? drift_val<R>(phi, pi, pdr, dtw) : phi; };
+  auto drift1 = [&](R phi, R pi) -> R {
+    if (DRIFT == 2) return drift_val<R>(drift_val<R>(phi, pi, pdr, dtw0), pi, pdr, dtw);
+    return DRIFT ? drift_val<R>(phi, pi, pdr, dtw) : phi;
+  };
   // VZ drifted values at box offset o of stage s, field f (and the raw pi values if wanted)
   auto dquad = [&](int s, int f, int o, R (&out)[VZ], R (*praw)[VZ]) {
     R fv[VZ];

@@ -30,4 +30,12 @@ inline std::vector<double> vv_coefficients(int ev)
   }
 }
 
+// Position-Verlet weights (PositionVerletParameters::getCoeffs, positionverletparameters.h:23-46):
+// the reference quotes the same numbers as for the velocity-Verlet scheme of the same order.
+inline bool is_pv(int ev) { return ev >= CLB_PV2 && ev <= CLB_PV6_2; }
+inline std::vector<double> pv_coefficients(int ev)
+{
+  return is_pv(ev) ? vv_coefficients(CLB_VV2 + (ev - CLB_PV2)) : std::vector<double>{};
+}
+
 } // namespace clb

@@ -28,16 +28,15 @@ class NotAnEvolverType(ValueError):
 
 
 def parse_evolver(value: str) -> int:
-    """EvolverType from a name or its integer (evolvertype.h:39-82); only LF and VV2-VV10 exist here."""
+    """EvolverType from a name or its integer (evolvertype.h:39-82); LF, VV2-VV10 and PV2-PV10 exist
+    here (position Verlet for the scalar-singlet models)."""
     v = str(value).strip()
     if v in EVOLVERS:
         return EVOLVERS[v]
     if v.isdigit() and int(v) in EVOLVERS.values():
         return int(v)
-    if v in ("RK2", "RK3_3", "RK3_4", "RK4_5", "PV2", "PV4", "PV6", "PV8", "PV10", "PV6_2") or (
-        v.isdigit() and 7 <= int(v) <= 16
-    ):
-        raise NotAnEvolverType(f"{v} is a reference evolver outside this library's hot path (LF, VV2-VV10).")
+    if v in ("RK2", "RK3_3", "RK3_4", "RK4_5") or (v.isdigit() and 7 <= int(v) <= 10):
+        raise NotAnEvolverType(f"{v} is a reference evolver outside this library's hot path (LF, VV2-VV10, PV2-PV10).")
     raise NotAnEvolverType(f"{v} is not an evolver type, abort.")
 
 

@@ -39,6 +39,14 @@ extern "C" {
 #define CLB_VV8    4
 #define CLB_VV10   5
 #define CLB_VV6_2  6
+/* position Verlet, PositionVerlet (positionverlet.h:45-99, positionverletparameters.h:23-46);
+   scalar-singlet models only (lphi4) */
+#define CLB_PV2    11
+#define CLB_PV4    12
+#define CLB_PV6    13
+#define CLB_PV8    14
+#define CLB_PV10   15
+#define CLB_PV6_2  16
 
 /* ---- arithmetic forms -------------------------------------------------------------------- */
 #define CLB_PREC_FP64       0 /* fields, momenta, stencils, reductions and expansion in FP64 */

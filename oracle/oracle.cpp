@@ -5,7 +5,8 @@
 //
 // It restates, in the reference's own operation order, the arithmetic of
 //   evolvers/velocityverlet.h:51-266, evolvers/velocityverletparameters.h:23-46,
-//   evolvers/leapfrog.h:29-277, evolvers/kernels/scalarsingletkernels.h:30-40,
+//   evolvers/leapfrog.h:29-277, evolvers/positionverlet.h:45-276,
+//   evolvers/positionverletparameters.h:23-46, evolvers/kernels/scalarsingletkernels.h:30-40,
 //   evolvers/kernels/scalefactorkernels.h:27-80, definitions/energies.h:37-239,
 //   definitions/averages.h:27-129, definitions/fieldfunctionals.h:52-67,
 //   definitions/gaugederivatives.h:36-73, definitions/hubbleconstraint.h:27-36,
@@ -70,6 +71,10 @@ std::vector<double> vvCoeffs(int ev)
   }
 }
 
+// Position-Verlet composition coefficients, positionverletparameters.h:23-46 (the same numbers).
+bool isPV(int ev) { return ev >= CLB_PV2 && ev <= CLB_PV6_2; }
+std::vector<double> pvCoeffs(int ev) { return isPV(ev) ? vvCoeffs(CLB_VV2 + (ev - CLB_PV2)) : std::vector<double>{}; }
+
 struct Oracle {
   clb_config cfg;
   clb_model_desc md;
@@ -81,6 +86,7 @@ struct Oracle {
   // ScaleFactorBase (scalefactorbase.h:20-21) and cached averages (scalarbase.h, abstractmodel.h:142)
   double aI = 1, aSI = 1, aIM = 1, aDotI = 0, aDotSI = 0, aDotSIM = 0;
   double pi2AvI = 0, pi2AvSI = 0, pi2AvSIM = 0, grad2AvI = 0, potAvI = 0, potAvSI = 0;
+  double pi2AvIM = 0, grad2AvSI = 0; // position Verlet (positionverlet.h:238-276)
   bool synced = true;   // LeapFrog::synced (leapfrog.h:31)
   bool initialized = false;
   std::vector<double> ws;
@@ -200,6 +206,17 @@ struct Oracle {
            ((((al - 2) * Eks + al * Egs) + (al - 1) * 0.0) + (al + 1) * potAvI);
   }
 
+  // ScaleFactorKernels::getSI (scalefactorkernels.h:83-119): the half-step averages at aI.
+  double sfKernelSI() const
+  {
+    const double al = md.alpha;
+    const double Eks = kineticS(pi2AvSI);
+    const double Egs = gradientS(grad2AvSI);
+    const double fm = md.fStar / md.MPl;
+    return std::pow(aI, 2 * al + 1) / 3.0 * (fm * fm) *
+           ((((al - 2) * Eks + al * Egs) + (al - 1) * 0.0) + (al + 1) * potAvSI);
+  }
+
   // ---- Sweeps
   // Kick: pi += h * [a^(1+alpha) lapl(phi) - a^(3+alpha) dV/dphi]  (scalarsingletkernels.h:30-40)
   void kick(double h)
@@ -222,6 +239,14 @@ struct Oracle {
   void drift(double c)
   {
     const double p = std::pow(aSI, md.alpha - 3);
+#pragma omp parallel for schedule(static)
+    for (size_t s = 0; s < (size_t)Ns * n3; ++s) fld[s] = fld[s] + p * (c * pi[s]);
+  }
+
+  // Position-Verlet drift: phi += pow(aI, alpha-3) * (c * pi)  (positionverlet.h:170-173)
+  void driftPV(double c)
+  {
+    const double p = std::pow(aI, md.alpha - 3);
 #pragma omp parallel for schedule(static)
     for (size_t s = 0; s < (size_t)Ns * n3; ++s) fld[s] = fld[s] + p * (c * pi[s]);
   }
@@ -275,6 +300,40 @@ struct Oracle {
       if (ex) {
         pi2AvI = avPi2();
         aDotI = aDotSI + (dt / 2) * sfKernel() * w;          // kickScaleFactorOne (:171-174)
+      }
+    }
+  }
+
+  // ---- PositionVerlet::evolve (positionverlet.h:45-99), self-consistent or no expansion
+  void evolvePV()
+  {
+    const double dt = cfg.dt;
+    const size_t P = ws.size();
+    const size_t stages = (P - 1) * 2 + 1;
+    const bool ex = cfg.expansion != 0;
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < P ? i : stages - i - 1];
+      driftPV(dt / 2 * w);                                   // driftScalar (:170-173)
+      if (ex) {
+        aIM = aI;                                            // driftScaleFactorFirstHalf (:209-222)
+        aI += dt / 2.0 * aDotI * w;
+        aSI = aI;
+        grad2AvSI = avGrad2();                               // storeFieldsAveragesHalf (:258-266)
+        potAvSI = avPot();
+      }
+      kick(w * dt);                                          // kickScalar (:132-135)
+      if (ex) {
+        pi2AvIM = pi2AvI;                                    // storeMomentaAverages (:238-256)
+        pi2AvI = avPi2();
+        pi2AvSI = 0.5 * (pi2AvI + pi2AvIM);
+        aDotI += dt * sfKernelSI() * w;                      // kickScaleFactor (:160-163)
+        aI += dt / 2.0 * aDotI * w;                          // driftScaleFactorSecondHalf (:225-234)
+        aSI = (aIM + aI) / 2.0;
+      }
+      driftPV(dt / 2 * w);
+      if (ex) {                                              // storeFieldsAveragesInt (:268-276)
+        grad2AvI = avGrad2();
+        potAvI = avPot();
       }
     }
   }
@@ -373,7 +432,7 @@ int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out
   o->fld.assign((size_t)o->Ns * o->n3, 0.0);
   o->pi.assign((size_t)o->Ns * o->n3, 0.0);
   if (cfg->evolver != CLB_LF) {
-    o->ws = vvCoeffs(cfg->evolver);
+    o->ws = isPV(cfg->evolver) ? pvCoeffs(cfg->evolver) : vvCoeffs(cfg->evolver);
     if (o->ws.empty()) { delete o; g_err = "unsupported evolver"; return CLB_EUNSUPPORTED; }
   }
   *out = reinterpret_cast<orc_handle *>(new Handle{CLB_MODEL_LPHI4, o});
@@ -448,6 +507,8 @@ int orc_evolve(orc_handle *h, int64_t n)
   for (int64_t s = 0; s < n; ++s) {
     if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
+    else if (isPV(o->cfg.evolver))
+      o->evolvePV();
     else
       o->evolveVV();
   }

@@ -167,3 +167,64 @@ def test_errors_surface_through_the_abi():
         lat.initialize()
     assert ei.value.code == _capi.CLB_ENONFINITE
     lat.close()
+
+
+# ---- position Verlet (PositionVerlet::evolve, positionverlet.h:45-99) --------------------------
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+@pytest.mark.parametrize("expansion", [True, False])
+def test_pv2_64_100_steps(path, expansion):
+    g, c, meas = run_pair(64, "PV2", expansion, 100, path=path)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("evolver", ["PV4", "PV6", "PV8", "PV10", "PV6_2"])
+def test_higher_order_pv(evolver):
+    g, c, meas = run_pair(24, evolver, True, 20)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_pv_two_fields_and_measure_cadence():
+    g, c, meas = run_pair(32, "PV4", True, 30, model="lphi4", measure_every=4)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+def test_pv_fp32_split_against_fp64(path):
+    g, c, meas = run_pair(48, "PV4", True, 50, precision="fp32", path=path)
+    (fg, pg, sg), (fc, pc, sc) = g, c
+    assert rel(fg, fc) < 1e-6
+    assert rel(fg - fg.mean(), fc - fc.mean()) < 1e-3
+    assert abs(sg["aI"] - sc["aI"]) / sc["aI"] < 1e-7
+    assert abs(meas["gpu"][-1]["friedmann"][0] - meas["cpu"][-1]["friedmann"][0]) < 1e-6
+
+
+def test_pv_history_rows_match_measurements():
+    # the fused path's step-end drift sweep books the integer-time field averages of each step
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = make_scalar_case(N=24, evolver="PV4", expansion=True)
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(6)
+    hist = lat.history()
+    lat.sync()
+    mm = lat.measure(1.0)
+    lat.close()
+    assert len(hist) == 6
+    assert abs(hist[-1][0] - mm["aI"]) <= 1e-15 * mm["aI"]
+    assert abs(hist[-1][1] - mm["aDotI"]) <= 1e-15 * abs(mm["aDotI"])
+
+
+def test_pv_rejected_for_gauge_models():
+    from conftest import make_u1_case
+
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, *_ = make_u1_case(N=8, evolver="PV2")
+    with pytest.raises(_capi.ClbError):
+        Lattice(m, rp)

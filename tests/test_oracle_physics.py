@@ -4,8 +4,8 @@ The reference's tests hold no golden vectors for the evolution (its only numeric
 couplings manager), so the oracle is pinned by physics with closed forms:
   (i)   free-field plane wave: the velocity-Verlet map of one lattice mode is x_n = A cos(n theta)
         with cos(theta) = 1 - (omega dt)^2 / 2 and omega^2 = sum_i (2/dx sin(pi n_i/N))^2;
-  (ii)  time reversibility of VV2/VV4 without expansion;
-  (iii) energy error of VVn convergent as dt^n without expansion;
+  (ii)  time reversibility of VV2/VV4 and PV2/PV4 without expansion;
+  (iii) energy error of VVn and PVn convergent as dt^n without expansion;
   (iv)  homogeneous lambda phi^4 with self-consistent expansion against scipy's solve_ivp of the
         background equations (velocityverlet.h, scalefactorkernels.h in the continuum-time limit).
 """
@@ -56,7 +56,7 @@ def test_free_plane_wave_closed_form(evolver):
     assert np.abs(fo.reshape(N, N, N) - expect).max() < 1e-12
 
 
-@pytest.mark.parametrize("evolver", ["VV2", "VV4"])
+@pytest.mark.parametrize("evolver", ["VV2", "VV4", "PV2", "PV4"])
 def test_time_reversibility(evolver):
     par, rp, m, f, p, sf = make_scalar_case(N=8, evolver=evolver, expansion=False, dt=0.02, amp=1e-2)
     (f1, p1, s1), _, _ = run_oracle(rp, m, f, p, sf, 30)
@@ -69,7 +69,7 @@ def test_time_reversibility(evolver):
     assert np.abs(p2 - p.ravel()).max() < 1e-13
 
 
-@pytest.mark.parametrize("evolver,order", [("VV2", 2), ("VV4", 4), ("VV6", 6)])
+@pytest.mark.parametrize("evolver,order", [("VV2", 2), ("VV4", 4), ("VV6", 6), ("PV2", 2), ("PV4", 4), ("PV6", 6)])
 def test_energy_error_order(evolver, order):
     errs = []
     for dt in (0.04, 0.02):
@@ -113,7 +113,7 @@ def test_homogeneous_background_with_expansion_vv6():
     assert max(errs) < 1e-11, errs
 
 
-@pytest.mark.parametrize("evolver", ["VV2", "LF"])
+@pytest.mark.parametrize("evolver", ["VV2", "LF", "PV2"])
 def test_homogeneous_background_second_order(evolver):
     e1 = _background_error(evolver, 0.004)[0]
     e2 = _background_error(evolver, 0.002)[0]
