@@ -50,6 +50,10 @@ class Config(C.Structure):
         ("precision", C.c_int32),
         ("path", C.c_int32),
         ("device", C.c_int32),
+        ("fixed_background", C.c_int32),
+        ("omega_eos", C.c_double),
+        ("H0", C.c_double),
+        ("t0", C.c_double),
     ]
 
 

@@ -313,9 +313,10 @@ bool encode_map(clb_handle *h, void *base, CUtensorMap *map, std::string &why)
   return true;
 }
 
-void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1)
+void tail(clb_handle *h, uint32_t flags, int nblocks, double w = 0, double w2 = 0, int64_t hist_row = -1,
+          double fa = 0, double fb = 0)
 {
-  TailOp op{flags, nblocks, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
+  TailOp op{flags, nblocks, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row, fa, fb};
   if (h->pdl_now)
     CLB_LAUNCH(h, K_TAIL, launch_pdl(k_tail, dim3(1), dim3(kTailThreads), 0, h->stream, (const double *)h->d_part, op,
                                      h->d_st, h->sp));
@@ -337,6 +338,12 @@ template <template <class, int> class Fn, class... Args> void dispatch(clb_handl
 
 // ---- schedules --------------------------------------------------------------------------------
 // VelocityVerlet::evolve, n steps (velocityverlet.h:51-114).
+// Fixed-background tail: the flags' scale-factor values from the closed form (no reduction).
+void fb_tail(clb_handle *h, uint32_t flags, double fa, double fb = 0.0)
+{
+  tail(h, flags, 0, 0, 0, -1, fa, fb);
+}
+
 template <class R, int NS> struct EvolveVV {
   static void run(clb_handle *h, int64_t nsteps)
   {
@@ -346,6 +353,45 @@ template <class R, int NS> struct EvolveVV {
     const std::vector<double> &ws = h->ws;
     const size_t P = ws.size(), S = 2 * P - 1;
     auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    if (h->fb) {
+      // fixed background (velocityverlet.h:74-118, 225-231): no a-kicks and no averages; the
+      // a-drift sets aI = a(t + w dt) and leaves aSI, which the field drift reads, as it was
+      const double t0 = h->cfg.t0;
+      if (h->cfg.path == CLB_PATH_REFERENCE) {
+        for (int64_t s = 0; s < nsteps; ++s) {
+          double tc = h->fb_t - t0;
+          for (size_t i = 0; i < S; ++i) {
+            const double w = wof(i);
+            L::kick(h, w * dt / 2);
+            fb_tail(h, T_FB_AIM | T_FB_AI, h->fb_a(tc + w * dt));
+            L::drift(h, dt * w);
+            L::kick(h, w * dt / 2);
+            tc += dt * w;
+          }
+          h->fb_t += dt;
+        }
+        return;
+      }
+      const int64_t total = nsteps * (int64_t)S;
+      L::kick(h, wof(0) * dt / 2);
+      h->pdl_now = h->pdl;
+      double tc = h->fb_t - t0;
+      for (int64_t k = 0; k < total; ++k) {
+        const size_t i = (size_t)(k % (int64_t)S);
+        const double w = wof(i);
+        const bool more = k + 1 < total;
+        const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+        fb_tail(h, T_FB_AIM | T_FB_AI, h->fb_a(tc + w * dt));
+        L::fused(h, dt * w, w * dt / 2, more ? wn * dt / 2 : 0.0, false);
+        tc += dt * w;
+        if (i + 1 == S) {
+          h->fb_t += dt;
+          tc = h->fb_t - t0;
+        }
+      }
+      h->pdl_now = false;
+      return;
+    }
     if (h->cfg.path == CLB_PATH_REFERENCE) {
       for (int64_t s = 0; s < nsteps; ++s)
         for (size_t i = 0; i < S; ++i) {
@@ -400,6 +446,59 @@ template <class R, int NS> struct EvolvePV {
     const size_t P = ws.size(), S = 2 * P - 1;
     auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
     if (nsteps <= 0) return;
+    if (h->fb) {
+      // fixed background (positionverlet.h:45-99, 207-235): a half-drifts from the closed form, no
+      // a-kick and no averages
+      const double t0 = h->cfg.t0;
+      if (h->cfg.path == CLB_PATH_REFERENCE) {
+        tail(h, T_PV_MODE, 0);
+        for (int64_t s = 0; s < nsteps; ++s) {
+          double tc = h->fb_t - t0;
+          for (size_t i = 0; i < S; ++i) {
+            const double w = wof(i);
+            L::drift(h, dt / 2 * w);
+            fb_tail(h, T_PV_MODE | T_FB_PV_HALF, 0.0, h->fb_a(tc + w * dt / 2.0));
+            L::kick(h, w * dt);
+            fb_tail(h, T_PV_MODE | T_FB_AI, h->fb_a(tc + w * dt));
+            L::drift(h, dt / 2 * w);
+            tc += dt * w;
+          }
+          h->fb_t += dt;
+        }
+        return;
+      }
+      // fused: every stage after the first of the call pairs the previous stage's second drift
+      // with its own first drift; one drift sweep closes the call
+      const int64_t total = nsteps * (int64_t)S;
+      double tc = h->fb_t - t0;
+      fb_tail(h, T_PV_MODE | T_FB_PV_HALF, 0.0, h->fb_a(tc + wof(0) * dt / 2.0));
+      h->pdl_now = h->pdl;
+      double wprev = 0.0;
+      for (int64_t k = 0; k < total; ++k) {
+        const size_t i = (size_t)(k % (int64_t)S);
+        const double w = wof(i);
+        if (k == 0)
+          L::fused(h, dt / 2 * w, w * dt, 0.0, false);
+        else
+          L::fused_pv(h, dt / 2 * wprev, dt / 2 * w, w * dt, false);
+        const double a_end = h->fb_a(tc + w * dt);
+        tc += dt * w;
+        if (i + 1 == S) {
+          h->fb_t += dt;
+          tc = h->fb_t - t0;
+        }
+        if (k + 1 < total) {
+          const double wn = wof((size_t)((k + 1) % (int64_t)S));
+          fb_tail(h, T_PV_MODE | T_FB_AI | T_FB_PV_HALF, a_end, h->fb_a(tc + wn * dt / 2.0));
+        } else {
+          fb_tail(h, T_PV_MODE | T_FB_AI, a_end);
+        }
+        wprev = w;
+      }
+      L::drift_fields(h, dt / 2 * wprev, false);
+      h->pdl_now = false;
+      return;
+    }
     if (h->cfg.path == CLB_PATH_REFERENCE) {
       tail(h, T_PV_MODE, 0); // the drift coefficient of the current a
       for (int64_t s = 0; s < nsteps; ++s)
@@ -451,6 +550,35 @@ template <class R, int NS> struct EvolveLF {
     const double dt = h->cfg.dt;
     const bool ex = h->cfg.expansion != 0;
     if (nsteps <= 0) return;
+    if (h->fb) {
+      // fixed background (leapfrog.h:55-89, 168-184): aI = a(t + dt), aSI = a(t + dt/2)
+      const double t0 = h->cfg.t0;
+      auto a_drift = [&]() {
+        const double tm = h->fb_t - t0;
+        fb_tail(h, T_FB_AIM | T_FB_AI | T_FB_ASI, h->fb_a(tm + dt), h->fb_a(tm + dt / 2.0));
+      };
+      if (h->cfg.path == CLB_PATH_REFERENCE) {
+        for (int64_t s = 0; s < nsteps; ++s) {
+          L::kick(h, (h->synced ? 0.5 : 1.0) * dt);
+          a_drift();
+          L::drift(h, dt);
+          h->fb_t += dt;
+          h->synced = false;
+        }
+        return;
+      }
+      L::kick(h, (h->synced ? 0.5 : 1.0) * dt);
+      a_drift();
+      for (int64_t s = 1; s < nsteps; ++s) {
+        h->fb_t += dt;
+        L::fused(h, dt, dt, 0.0, false);
+        a_drift();
+      }
+      L::drift_fields(h, dt, false);
+      h->fb_t += dt;
+      h->synced = false;
+      return;
+    }
     if (h->cfg.path == CLB_PATH_REFERENCE) {
       for (int64_t s = 0; s < nsteps; ++s) {
         const double weight = h->synced ? 0.5 : 1.0;
@@ -484,7 +612,7 @@ template <class R, int NS> struct SyncLF {
     using L = Launch<R, NS>;
     if (!h->synced) {
       L::kick(h, 0.5 * h->cfg.dt);
-      if (h->cfg.expansion) tail(h, T_STORE_PI2_I | T_LF_SYNC, L::reduce_pi2(h));
+      if (h->cfg.expansion && !h->fb) tail(h, T_STORE_PI2_I | T_LF_SYNC, L::reduce_pi2(h));
     }
     h->synced = true;
   }
@@ -495,7 +623,7 @@ template <class R, int NS> struct Init {
   {
     using L = Launch<R, NS>;
     uint32_t fl = T_STORE_ALL;
-    if (h->cfg.expansion && correct) fl |= T_CORRECT_ADOT;
+    if (h->cfg.expansion && correct && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
     if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
     tail(h, fl, L::reduce_fields(h, true));
   }
@@ -573,6 +701,16 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     g_err = "clb_create: fStar, omegaStar and MPl must be positive";
     return CLB_EINVAL;
   }
+  const bool fb = cfg->expansion && cfg->fixed_background;
+  if (fb && (u1 || su2)) {
+    g_err = "clb_create: the fixed background evolves the scalar-singlet models here";
+    return CLB_EUNSUPPORTED;
+  }
+  if (fb && !(std::fabs(cfg->H0) > 1e-8)) { // runParameterTolerance (fixedbackgroundexpansion.h:28-31)
+    g_err = "For models that do not involve cosmic defects, you need to specify a non-zero H0 to run a simulation with "
+            "fixed background. If you want to disable expansion, please set expansion = false in the input file.";
+    return CLB_EINVAL;
+  }
   std::vector<double> ws;
   if (is_pv(cfg->evolver) && (u1 || su2)) {
     g_err = "clb_create: position Verlet evolves the scalar-singlet models here";
@@ -607,6 +745,12 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_OK;
   }
   h->NS = md->n_scalars;
+  h->fb = fb;
+  if (fb) { // pEoS, H0 (fixedbackgroundexpansion.h:21-26)
+    h->fb_p = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
+    h->fb_H0 = cfg->H0;
+    h->fb_t = cfg->t0;
+  }
   h->fp32 = cfg->precision == CLB_PREC_FP32_SPLIT;
   h->esz = h->fp32 ? sizeof(float) : sizeof(double);
   h->ws = ws;
@@ -851,6 +995,7 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
   }
   dispatch<Init>(h, (int)correct_adot);
   h->synced = true;
+  h->fb_t = h->cfg.t0;
   int r = sync_and_check(h, "clb_initialize");
   if (r == CLB_OK) h->initialized = true;
   return r;
@@ -888,7 +1033,7 @@ int clb_evolve(clb_handle *h, int64_t n)
   int r = sync_and_check(h, "clb_evolve");
   float ms = 0;
   if (cudaEventElapsedTime(&ms, h->ev_call[0], h->ev_call[1]) == cudaSuccess) h->last_evolve_ms = ms;
-  if (r == CLB_OK && h->cfg.expansion) h->hist_rows = n;
+  if (r == CLB_OK && h->cfg.expansion && !h->fb) h->hist_rows = n;
   return r;
 }
 
@@ -960,6 +1105,7 @@ int clb_sync(clb_handle *h)
   if (h->u1) return u1_sync(h);
   if (h->su2) return su2_sync(h);
   if (h->cfg.evolver == CLB_LF) dispatch<SyncLF>(h);
+  if (h->fb) fb_tail(h, T_FB_ADOT, 0.0, h->fb_adot(h->fb_t - h->cfg.t0));
   return sync_and_check(h, "clb_sync");
 }
 

@@ -342,6 +342,10 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
   }
   *out = nullptr;
   const clb_config &c0 = cfgs[0];
+  if (c0.expansion && c0.fixed_background) {
+    g_berr = "clb_batch_create: the batched ensemble runs the self-consistent expansion";
+    return CLB_EUNSUPPORTED;
+  }
   std::vector<double> ws = vv_coefficients(c0.evolver);
   if (ws.empty()) {
     g_berr = "clb_batch_create: the batched ensemble runs the VV evolvers";

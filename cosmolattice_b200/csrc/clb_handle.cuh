@@ -9,6 +9,8 @@
 #include <cuda.h>
 #include <cufft.h>
 
+#include <cmath>
+
 #include <string>
 #include <vector>
 
@@ -47,6 +49,12 @@ struct clb_handle {
   size_t part_rows = 0;
   cudaStream_t stream = nullptr;
   std::vector<double> ws;
+  // fixed background: a(t - t0) = (1 + H0/p (t - t0))^p (fixedbackgroundexpansion.h:37-45); fb_t is
+  // the time t, t0 at clb_initialize and advanced by dt per step as the reference's main loop does
+  bool fb = false;
+  double fb_p = 0, fb_H0 = 0, fb_t = 0;
+  double fb_a(double dtm) const { return std::pow(1 + fb_H0 / fb_p * dtm, fb_p); }
+  double fb_adot(double dtm) const { return fb_H0 * std::pow(1 + fb_H0 / fb_p * dtm, fb_p - 1); }
   bool has_state = false, initialized = false, synced = true;
   ScalarArgs sa{};
   SweepArgs sw{};

@@ -64,7 +64,14 @@ enum TailFlags : uint32_t {
   T_PV_KICK = 1u << 16,      // aDotI += dt getSI w                       kickScaleFactor (:160-163)
   T_PV_DRIFT_A2 = 1u << 17,  // aI += dt/2 aDotI w; aSI = (aIM + aI)/2    driftScaleFactorSecondHalf (:225-234)
   T_PV_DRIFT_A1 = 1u << 18,  // aIM = aI; aI += dt/2 aDotI w2; aSI = aI    driftScaleFactorFirstHalf (:209-222)
-  T_PV_MODE = 1u << 19       // drift coefficient pow(aI, alpha - 3), of the a before T_PV_DRIFT_A1
+  T_PV_MODE = 1u << 19,      // drift coefficient pow(aI, alpha - 3), of the a before T_PV_DRIFT_A1
+  // Fixed background (FixedBackgroundExpansion, fixedbackgroundexpansion.h:37-45): a and aDot are
+  // the host's closed-form values fa, fb, applied after the flags above, in this order:
+  T_FB_AIM = 1u << 20,       // aIM = aI
+  T_FB_AI = 1u << 21,        // aI = fa
+  T_FB_ASI = 1u << 22,       // aSI = fb                                 (leapfrog.h:171-175)
+  T_FB_PV_HALF = 1u << 23,   // aIM = aI; aI = fb; aSI = aI              (positionverlet.h:209-216)
+  T_FB_ADOT = 1u << 24       // aDotI = fb                               (sync: velocityverlet.h:121)
 };
 
 struct TailOp {
@@ -74,6 +81,7 @@ struct TailOp {
   double w2;       // weight of T_VV_KICK_HALF / T_VV_DRIFT
   double *hist;    // per-step history rows (kHistCols doubles), or null
   int64_t hist_row;// row written after this tail, -1 for none
+  double fa, fb;   // fixed background: the values of T_FB_*
 };
 
 // Columns of the per-step history: a, aDot, <pi^2>, <grad^2>, <V> at the end of each step.

@@ -441,8 +441,17 @@ __device__ __forceinline__ void tail_apply(DevState &s, const TailOp &op, const 
     s.aI = __dadd_rn(s.aI, __dmul_rn(__dmul_rn(dt / 2.0, s.aDotI), op.w2));
     s.aSI = s.aI;
   }
+  if (fl & T_FB_AIM) s.aIM = s.aI;
+  if (fl & T_FB_AI) s.aI = op.fa;
+  if (fl & T_FB_ASI) s.aSI = op.fb;
+  if (fl & T_FB_PV_HALF) {
+    s.aIM = s.aI;
+    s.aI = op.fb;
+    s.aSI = s.aI;
+  }
+  if (fl & T_FB_ADOT) s.aDotI = op.fb;
   if (fl & T_PV_MODE) // the next field drift happens before the first a half-drift of its stage
-    s.drift_p = apow((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI, p.alpha - 3);
+    s.drift_p = apow((fl & (T_PV_DRIFT_A1 | T_FB_PV_HALF)) ? s.aIM : s.aI, p.alpha - 3);
   else
     s.drift_p = apow(s.aSI, p.alpha - 3);
   s.kick_A = apow(s.aI, 1 + p.alpha);

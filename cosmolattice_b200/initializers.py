@@ -42,9 +42,12 @@ def wave_numbers(N: int):
 
 
 def initial_scale_factor(model: Model, rp: RunParameters):
-    """(aI, aDotI) before fluctuations (scalefactorinitializer.h:58-65)."""
+    """(aI, aDotI) before fluctuations (scalefactorinitializer.h:37-65); a fixed background starts
+    at a = 1, aDot = H0 (in program units)."""
     if not rp.expansion:
         return 1.0, 0.0
+    if getattr(rp, "fixedBackground", False):
+        return 1.0, rp.H0 / model.omegaStar
     kin = 0.0
     for i in range(model.Ns):
         # Energies::kineticS with the default a = 1 in force at that point

@@ -43,6 +43,11 @@ class Lattice:
         cfg.precision = PRECISIONS[precision]
         cfg.path = PATHS[path]
         cfg.device = device
+        if getattr(rp, "fixedBackground", False):
+            cfg.fixed_background = 1
+            cfg.omega_eos = rp.omegaEoS
+            cfg.H0 = rp.H0 / model.omegaStar  # program units (fixedbackgroundexpansion.h:26)
+        cfg.t0 = getattr(rp, "t0", 0.0)
         self.cfg = cfg
         self._desc = model.desc()
         h = C.c_void_p()

@@ -145,6 +145,9 @@ class RunParameters:
         self.baseSeed = par.get_str("baseSeed", "0")
         self.outFn = par.get_str("outputfile", "./")
         self.fixedBackground = par.get_bool("fixedBackground", False) if self.expansion else False
+        # fixed background (runparameters.h:90-94): equation of state and initial Hubble rate (GeV)
+        self.omegaEoS = par.get_float("omegaEoS", 1.0 / 3.0) if self.fixedBackground else 1.0 / 3.0
+        self.H0 = par.get_float("H0", 0.0) if self.fixedBackground else 0.0
         self.a0 = par.get_float("a0", 1.0)
         self.deltaKBin = par.get_float("deltaKBin", 1.0)
         self.nBinsSpectra = int(math.floor(math.sqrt(3.0) / 2.0 * self.N / self.deltaKBin))  # runparameters.h:98
@@ -191,7 +194,10 @@ class RunParameters:
         if self.powerSpectrumVersion not in (1, 2, 3):
             raise RunParametersInconsistent(
                 f"powerSpectrumVersion {self.powerSpectrumVersion} is not a valid powerSpectrumVersion.")
-        if self.fixedBackground:
-            raise RunParametersInconsistent("fixedBackground expansion is outside this library's hot path.")
+        if self.fixedBackground and _almost_equal(self.H0, 0.0):
+            # FixedBackgroundExpansion ctor (fixedbackgroundexpansion.h:28-31), non-defect models
+            raise RunParametersInconsistent(
+                "For models that do not involve cosmic defects, you need to specify a non-zero H0 to run a simulation "
+                "with fixed background. If you want to disable expansion, please set expansion = false in the input file.")
         if self.withGWs:
             raise RunParametersInconsistent("GWs are outside this library's hot path.")

@@ -83,6 +83,13 @@ typedef struct clb_config {
   int32_t precision;  /* CLB_PREC_*                                                             */
   int32_t path;       /* CLB_PATH_*                                                             */
   int32_t device;     /* CUDA device ordinal                                                    */
+  /* Fixed background (runparameters.h:90-94; with expansion only; scalar-singlet models):
+   * a(t) = (1 + H0/p (t - t0))^p, aDot = H0 (1 + H0/p (t - t0))^(p - 1),
+   * p = 2 / (3 (1 + omega_eos) - 2 alpha)  (FixedBackgroundExpansion, fixedbackgroundexpansion.h:21-50) */
+  int32_t fixed_background; /* 0: self-consistent expansion (default), 1: fixed background           */
+  double omega_eos;         /* equation of state w                                                  */
+  double H0;                /* initial Hubble rate in program units (H0 / omega_*)                  */
+  double t0;                /* initial time (runparameters.h:68); t advances by dt per step         */
 } clb_config;
 
 typedef struct clb_model_desc {

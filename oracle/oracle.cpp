@@ -87,6 +87,11 @@ struct Oracle {
   double aI = 1, aSI = 1, aIM = 1, aDotI = 0, aDotSI = 0, aDotSIM = 0;
   double pi2AvI = 0, pi2AvSI = 0, pi2AvSIM = 0, grad2AvI = 0, potAvI = 0, potAvSI = 0;
   double pi2AvIM = 0, grad2AvSI = 0; // position Verlet (positionverlet.h:238-276)
+  // fixed background (fixedbackgroundexpansion.h:21-45): pEoS, H0 and the main loop's time t
+  bool fb = false;
+  double pEoS = 0, H0fb = 0, t = 0;
+  double aBg(double dtm) const { return std::pow(1 + H0fb / pEoS * dtm, pEoS); }
+  double aBgDot(double dtm) const { return H0fb * std::pow(1 + H0fb / pEoS * dtm, pEoS - 1); }
   bool synced = true;   // LeapFrog::synced (leapfrog.h:31)
   bool initialized = false;
   std::vector<double> ws;
@@ -281,6 +286,19 @@ struct Oracle {
     const size_t P = ws.size();
     const size_t stages = (P - 1) * 2 + 1;
     const bool ex = cfg.expansion != 0;
+    if (fb) { // velocityverlet.h:74-118 with driftScaleFactor's fixed branch (:225-231)
+      double tcurrent = t - cfg.t0;
+      for (size_t i = 0; i < stages; ++i) {
+        const double w = ws[i < P ? i : stages - i - 1];
+        kick(w * dt / 2);
+        aIM = aI;
+        aI = aBg(tcurrent + w * dt);
+        drift(dt * w);
+        kick(w * dt / 2);
+        tcurrent += dt * w;
+      }
+      return;
+    }
     for (size_t i = 0; i < stages; ++i) {
       const double w = ws[i < P ? i : stages - i - 1];
       if (ex) aDotSI = aDotI + (dt / 2) * sfKernel() * w;   // kickScaleFactorHalf (:165-169)
@@ -311,6 +329,21 @@ struct Oracle {
     const size_t P = ws.size();
     const size_t stages = (P - 1) * 2 + 1;
     const bool ex = cfg.expansion != 0;
+    if (fb) { // positionverlet.h:45-99 with the fixed branches of :207-235
+      double tcurrent = t - cfg.t0;
+      for (size_t i = 0; i < stages; ++i) {
+        const double w = ws[i < P ? i : stages - i - 1];
+        driftPV(dt / 2 * w);
+        aIM = aI;
+        aI = aBg(tcurrent + w * dt / 2.0);
+        aSI = aI;
+        kick(w * dt);
+        aI = aBg(tcurrent + w * dt);
+        driftPV(dt / 2 * w);
+        tcurrent += dt * w;
+      }
+      return;
+    }
     for (size_t i = 0; i < stages; ++i) {
       const double w = ws[i < P ? i : stages - i - 1];
       driftPV(dt / 2 * w);                                   // driftScalar (:170-173)
@@ -344,6 +377,15 @@ struct Oracle {
     const double dt = cfg.dt;
     const bool ex = cfg.expansion != 0;
     const double weight = synced ? 0.5 : 1.0;
+    if (fb) { // leapfrog.h:55-89 with driftScaleFactor's fixed branch (:168-175)
+      kick(weight * dt);
+      aIM = aI;
+      aI = aBg(t - cfg.t0 + dt);
+      aSI = aBg(t - cfg.t0 + dt / 2.0);
+      drift(dt);
+      synced = false;
+      return;
+    }
     kick(weight * dt);                                      // kickScalar (:131-134)
     if (ex) {
       pi2AvSIM = pi2AvSI;                                   // storeMomentaAverages (:239-245)
@@ -367,7 +409,9 @@ struct Oracle {
   // ---- LeapFrog::sync (leapfrog.h:96-116)
   void syncLF()
   {
-    if (!synced) {
+    if (!synced && fb) {
+      kick(0.5 * cfg.dt);
+    } else if (!synced) {
       kick(0.5 * cfg.dt);
       if (cfg.expansion) {
         pi2AvI = avPi2();
@@ -431,6 +475,12 @@ int orc_create(const clb_config *cfg, const clb_model_desc *md, orc_handle **out
   o->Ns = md->n_scalars;
   o->fld.assign((size_t)o->Ns * o->n3, 0.0);
   o->pi.assign((size_t)o->Ns * o->n3, 0.0);
+  o->fb = cfg->expansion && cfg->fixed_background;
+  if (o->fb) {
+    o->pEoS = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
+    o->H0fb = cfg->H0;
+  }
+  o->t = cfg->t0;
   if (cfg->evolver != CLB_LF) {
     o->ws = isPV(cfg->evolver) ? pvCoeffs(cfg->evolver) : vvCoeffs(cfg->evolver);
     if (o->ws.empty()) { delete o; g_err = "unsupported evolver"; return CLB_EUNSUPPORTED; }
@@ -487,12 +537,13 @@ int orc_initialize(orc_handle *h, int32_t correct_adot)
   if (isU1(h)) return oracle_models::u1_initialize(H(h)->impl, correct_adot);
   Oracle *o = S(h);
   o->setAllAverages();
-  if (o->cfg.expansion && correct_adot) {
+  if (o->cfg.expansion && correct_adot && !o->fb) { // modelinitializer.h:74-80
     double hl[3];
     o->hubble(hl);
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
+  o->t = o->cfg.t0;
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;
   return CLB_OK;
@@ -511,6 +562,7 @@ int orc_evolve(orc_handle *h, int64_t n)
       o->evolvePV();
     else
       o->evolveVV();
+    o->t += o->cfg.dt; // the main loop's t (cosmolattice.cpp:186-188)
   }
   return CLB_OK;
 }
@@ -521,6 +573,7 @@ int orc_sync(orc_handle *h)
   if (isU1(h)) return oracle_models::u1_sync(H(h)->impl);
   Oracle *o = S(h);
   if (o->cfg.evolver == CLB_LF) o->syncLF();
+  if (o->fb) o->aDotI = o->aBgDot(o->t - o->cfg.t0); // velocityverlet.h:121, leapfrog.h:114, positionverlet.h:106
   return CLB_OK;
 }
 

@@ -73,6 +73,11 @@ class OracleLattice:
         cfg.expansion = 1 if rp.expansion else 0
         cfg.precision = capi.PREC_FP64
         cfg.path = capi.PATH_REFERENCE
+        if getattr(rp, "fixedBackground", False):
+            cfg.fixed_background = 1
+            cfg.omega_eos = rp.omegaEoS
+            cfg.H0 = rp.H0 / model.omegaStar
+        cfg.t0 = getattr(rp, "t0", 0.0)
         self._desc = model.desc()
         h = C.c_void_p()
         rc = self.lib.orc_create(C.byref(cfg), C.byref(self._desc), C.byref(h))

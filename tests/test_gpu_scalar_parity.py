@@ -21,11 +21,12 @@ def rel(a, b):
 
 
 def run_pair(N, evolver, expansion, nsteps, model="lphi4_1f", path="fused", precision="fp64", measure_every=None,
-             dt=0.01, amp=1e-3):
+             dt=0.01, amp=1e-3, extra=None):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, expansion=expansion, model=model, dt=dt, amp=amp)
+    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, expansion=expansion, model=model, dt=dt, amp=amp,
+                                            extra=extra)
     gpu = Lattice(m, rp, precision=precision, path=path)
     cpu = OracleLattice(m, rp)
     meas = {"gpu": [], "cpu": []}
@@ -226,5 +227,50 @@ def test_pv_rejected_for_gauge_models():
     from cosmolattice_b200 import Lattice, _capi
 
     par, rp, m, *_ = make_u1_case(N=8, evolver="PV2")
+    with pytest.raises(_capi.ClbError):
+        Lattice(m, rp)
+
+
+# ---- fixed background (FixedBackgroundExpansion, fixedbackgroundexpansion.h:21-45) --------------
+
+# H0 = 0.5 in program units: omega_* = sqrt(lambda) phi_0 = 5.6964e18 GeV for the lphi4_1f case
+FB = {"fixedBackground": "true", "H0": 0.5 * 5.6964e18, "omegaEoS": 1.0 / 3.0}
+
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+@pytest.mark.parametrize("evolver", ["VV2", "VV4", "PV2", "PV4"])
+def test_fixed_background_parity(path, evolver):
+    g, c, meas = run_pair(32, evolver, True, 30, path=path, extra=FB, measure_every=7)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("path", ["fused", "reference"])
+def test_fixed_background_leapfrog_with_syncs(path):
+    g, c, meas = run_pair(32, "LF", True, 30, path=path, extra=FB, measure_every=7)
+    check_state(g, c)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_fixed_background_scale_factor_closed_form():
+    # a(t) = (1 + H0/p t)^p, aDot = H0 (1 + H0/p t)^(p-1), p = 2/(3(1 + w) - 2 alpha), at t = n dt
+    g, c, meas = run_pair(16, "VV2", True, 40, extra=FB)
+    (fg, pg, sg) = g
+    p = 2.0 / (3.0 * (1.0 + 1.0 / 3.0) - 2.0 * 1.0)
+    t = 0.0
+    for _ in range(40):
+        t += 0.01
+    a = (1 + 0.5 / p * t) ** p
+    ad = 0.5 * (1 + 0.5 / p * t) ** (p - 1)
+    assert abs(sg["aI"] - a) <= 1e-15 * a
+    assert abs(sg["aDotI"] - ad) <= 1e-15 * ad
+
+
+def test_fixed_background_rejected_for_gauge_and_batch():
+    from conftest import make_u1_case
+
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, *_ = make_u1_case(N=8, extra={"fixedBackground": "true", "H0": 1e18})
     with pytest.raises(_capi.ClbError):
         Lattice(m, rp)

@@ -130,3 +130,35 @@ def test_reference_vv4_weights_are_reproduced():
     e_a = _background_error("VV4", 0.004)[0]
     e_b = _background_error("VV4", 0.002)[0]
     assert 1e-8 < e_a < 2e-8 and abs(e_a - e_b) / e_a < 0.1
+
+
+def test_fixed_background_run_parameters():
+    # FixedBackgroundExpansion needs a non-zero H0 (fixedbackgroundexpansion.h:28-31); the initial
+    # a = 1 and aDot = H0 / omega_* (scalefactorinitializer.h:37-43)
+    from cosmolattice_b200.initializers import initial_scale_factor
+    from cosmolattice_b200.params import RunParametersInconsistent
+
+    with pytest.raises(RunParametersInconsistent):
+        make_scalar_case(N=8, extra={"fixedBackground": "true"})
+    par, rp, m, f, p, sf = make_scalar_case(N=8, extra={"fixedBackground": "true", "H0": 2.0e18, "omegaEoS": 0.0})
+    assert rp.fixedBackground and rp.omegaEoS == 0.0
+    assert initial_scale_factor(m, rp) == (1.0, 2.0e18 / m.omegaStar)
+
+
+def test_fixed_background_oracle_scale_factor():
+    # matter domination (w = 0, alpha = 1): p = 2, a = (1 + H0 t / 2)^2 exactly at t = n dt (PV2:
+    # its one weight is 1; the reference's PV4/VV4 weights sum to 1 - 2e-8, so their last stage
+    # ends 2e-8 dt short of t + dt, velocityverletparameters.h:26)
+    par, rp, m, f, p, sf = make_scalar_case(N=6, evolver="PV2", dt=0.02,
+                                            extra={"fixedBackground": "true", "H0": 0.3 * m_omega(), "omegaEoS": 0.0})
+    (fo, po, so), _, _ = run_oracle(rp, m, f, p, sf, 25)
+    t = 0.0
+    for _ in range(25):
+        t += 0.02
+    assert abs(so["aI"] - (1 + 0.3 / 2 * t) ** 2) <= 1e-15 * so["aI"]
+    assert abs(so["aDotI"] - 0.3 * (1 + 0.3 / 2 * t)) <= 1e-15 * so["aDotI"]
+
+
+def m_omega():
+    # omega_* of the lphi4_1f case: sqrt(lambda) phi_0 with lambda = 1
+    return 5.6964e18
