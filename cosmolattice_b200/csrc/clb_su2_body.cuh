@@ -54,6 +54,18 @@ template <class T> __device__ __forceinline__ D2<T> isig(int b, const D2<T> &d)
   if (b == 1) return D2<T>{d.v, C2<T>{-d.u.re, -d.u.im}};
   return D2<T>{cmul(I, d.u), cmul(C2<T>{0, -1}, d.v)};
 }
+// Divisions of the kernels: the FP64 form keeps the reference's rounding (a / b); the FP32 form,
+// bound to no rounding order, multiplies by the reciprocal (formed once per site for dx, dx^2 and
+// the field norms); the tangent-linear types divide as Tan does.
+template <class T> __device__ __forceinline__ T kdiv(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float kdiv<float>(float a, float b) { return a * (1.0f / b); }
+// the FP32 tangent-linear form: the value part as kdiv<float> forms it (bitwise the plain form)
+template <> __device__ __forceinline__ Tan<float> kdiv<Tan<float>>(Tan<float> a, Tan<float> b)
+{
+  const float r = 1.0f / b.v, q = a.v * r;
+  return Tan<float>(q, (a.d - q * b.d) * r);
+}
+
 template <class T> __device__ __forceinline__ T ipw(T x, int n)
 {
   if (n < 0) return T(1) / ipw(x, -n);
@@ -133,9 +145,9 @@ template <class S, class T> struct Site {
     const T c = F(comp, s);
     T t[3];
     for (int d = 0; d < 3; ++d) t[d] = (F(comp, pl(d)) + F(comp, mi(d))) - 2 * c;
-    return (T(1) / (dx * dx)) * ((t[0] + t[1]) + t[2]);
+    return kdiv(T(1), dx * dx) * ((t[0] + t[1]) + t[2]);
   }
-  __device__ __forceinline__ T fd(int comp, size_t t0, size_t t1) const { return (F(comp, t1) - F(comp, t0)) / dx; }
+  __device__ __forceinline__ T fd(int comp, size_t t0, size_t t1) const { return kdiv(F(comp, t1) - F(comp, t0), dx); }
   __device__ __forceinline__ Q4<T> plaq(int i, int j) const
   {
     return qmul(qmul(qmul(link(i, s), link(j, pl(i))), qdag(link(i, pl(j)))), qdag(link(j, s)));
@@ -208,7 +220,7 @@ template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<
   }
   const T dx2 = v.dx * v.dx;
   const C2<T> c = v.cs(v.s);
-  return C2<T>{((plus.re + minus.re) - 6 * c.re) / dx2, ((plus.im + minus.im) - 6 * c.im) / dx2};
+  return C2<T>{kdiv((plus.re + minus.re) - 6 * c.re, dx2), kdiv((plus.im + minus.im) - 6 * c.im, dx2)};
 }
 
 template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S, T> &v, T out[4])
@@ -228,10 +240,10 @@ template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S
   }
   const T dx2 = v.dx * v.dx;
   const D2<T> c = v.dbl(v.s);
-  out[0] = ((plus.u.re + minus.u.re) - 6 * c.u.re) / dx2;
-  out[1] = ((plus.u.im + minus.u.im) - 6 * c.u.im) / dx2;
-  out[2] = ((plus.v.re + minus.v.re) - 6 * c.v.re) / dx2;
-  out[3] = ((plus.v.im + minus.v.im) - 6 * c.v.im) / dx2;
+  out[0] = kdiv((plus.u.re + minus.u.re) - 6 * c.u.re, dx2);
+  out[1] = kdiv((plus.u.im + minus.u.im) - 6 * c.u.im, dx2);
+  out[2] = kdiv((plus.v.re + minus.v.re) - 6 * c.v.re, dx2);
+  out[3] = kdiv((plus.v.im + minus.v.im) - 6 * c.v.im, dx2);
 }
 
 // Kick coefficients pow(aI, 1+alpha), pow(aI, 3+alpha), its half and pow(aI, -1+alpha).
@@ -252,12 +264,12 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
     K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
     const C2<T> cl = covLapC(v);
     const T ndC = 4 * qH * ipw(nD, 2) * nC;
-    K[1] = A * cl.re - B2 * (ndC / nC * v.F(1, s));
-    K[2] = A * cl.im - B2 * (ndC / nC * v.F(2, s));
+    K[1] = A * cl.re - B2 * (kdiv(ndC, nC) * v.F(1, s));
+    K[2] = A * cl.im - B2 * (kdiv(ndC, nC) * v.F(2, s));
     T dl[4];
     covLapD(v, dl);
     const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
-    for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (ndD / nD * v.F(3 + c, s));
+    for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (kdiv(ndD, nD) * v.F(3 + c, s));
     const D2<T> D0 = v.dbl(s);
     const C2<T> C0 = v.cs(s);
     for (int i = 0; i < 3; ++i) {
@@ -266,19 +278,19 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
       for (int j = 0; j < 3; ++j) {
         const T g0 = v.fd(7 + j, s, v.pl(i));
         const T g1 = v.fd(7 + j, v.mi(j), v.plmi(i, j));
-        const T t = (g0 - g1) / v.dx;
+        const T t = kdiv(g0 - g1, v.dx);
         grad = j == 0 ? t : grad + t;
       }
       const T Jc = v.gC * cmul(conj_(v.wC(i)), C0).im;
       const T Jd = v.gD * sprod(v.wD(i), D0).im;
-      const T J = T(2.0) / v.dx * rfo2 * (Jc + Jd);
+      const T J = kdiv(T(2.0), v.dx) * rfo2 * (Jc + Jd);
       K[7 + i] = G * (lap - grad) - A * J;
     }
   }
   if constexpr (SECT != 1) {
     const D2<T> Dg = v.dbl(s);
-    const T normGrad = ipw(T(1) / v.dx, 3) / v.gS * G;
-    const T normSrc = (T(1) / v.dx) * A;
+    const T normGrad = kdiv(ipw(kdiv(T(1), v.dx), 3), v.gS) * G;
+    const T normSrc = kdiv(T(1), v.dx) * A;
     for (int i = 0; i < 3; ++i) {
       T gr[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
       bool first = true;
@@ -317,7 +329,7 @@ template <class S, class T> __device__ __forceinline__ T cGrad2(const Site<S, T>
   T acc = 0;
   for (int j = 0; j < 3; ++j) {
     const C2<T> d0 = csub(v.wC(j), c);
-    const C2<T> d{d0.re / v.dx, d0.im / v.dx};
+    const C2<T> d{kdiv(d0.re, v.dx), kdiv(d0.im, v.dx)};
     const T n2 = d.re * d.re + d.im * d.im;
     acc = j == 0 ? n2 : acc + n2;
   }
@@ -330,7 +342,7 @@ template <class S, class T> __device__ __forceinline__ T dGrad2(const Site<S, T>
   for (int j = 0; j < 3; ++j) {
     const D2<T> w = qapply(v.link(j, v.s), dscale(v.phaseD(j, v.s), v.dbl(v.pl(j))));
     const C2<T> du0 = csub(w.u, c.u), dv0 = csub(w.v, c.v);
-    const C2<T> du{du0.re / v.dx, du0.im / v.dx}, dv{dv0.re / v.dx, dv0.im / v.dx};
+    const C2<T> du{kdiv(du0.re, v.dx), kdiv(du0.im, v.dx)}, dv{kdiv(dv0.re, v.dx), kdiv(dv0.im, v.dx)};
     const T n2 = (du.re * du.re + du.im * du.im) + (dv.re * dv.re + dv.im * dv.im);
     acc = j == 0 ? n2 : acc + n2;
   }
@@ -347,7 +359,7 @@ template <class S, class T> __device__ __forceinline__ T aB2(const Site<S, T> &v
 }
 template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v)
 {
-  const T c = T(4.0) / (ipw(v.dx, 4) * ipw(v.gS, 2));
+  const T c = kdiv(T(4.0), ipw(v.dx, 4) * ipw(v.gS, 2));
   const T t10 = 2 - 2 * v.plaq(1, 0).w, t20 = 2 - 2 * v.plaq(2, 0).w, t21 = 2 - 2 * v.plaq(2, 1).w;
   return c * (t10 + (t20 + t21));
 }

@@ -62,11 +62,12 @@ __device__ __forceinline__ double u1_m(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double u1_a(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double u1_s(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double u1_d(double a, double b) { return __ddiv_rn(a, b); }
-// FP32 form: plain single-precision arithmetic (contraction allowed)
+// FP32 form: plain single-precision arithmetic (contraction allowed; a division by dx, dx^2 or
+// |phi| is a multiply by the reciprocal)
 __device__ __forceinline__ float u1_m(float a, float b) { return a * b; }
 __device__ __forceinline__ float u1_a(float a, float b) { return a + b; }
 __device__ __forceinline__ float u1_s(float a, float b) { return a - b; }
-__device__ __forceinline__ float u1_d(float a, float b) { return a / b; }
+__device__ __forceinline__ float u1_d(float a, float b) { return a * (1.0f / b); } // reciprocal formed once per site
 __device__ __forceinline__ void u1_sincos(double x, double *sn, double *cs) { sincos(x, sn, cs); }
 __device__ __forceinline__ void u1_sincos(float x, float *sn, float *cs) { sincosf(x, sn, cs); }
 
