@@ -712,8 +712,8 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_EINVAL;
   }
   std::vector<double> ws;
-  if (is_pv(cfg->evolver) && (u1 || su2)) {
-    g_err = "clb_create: position Verlet evolves the scalar-singlet models here";
+  if (is_pv(cfg->evolver) && su2) {
+    g_err = "clb_create: position Verlet evolves the scalar-singlet and lphi4U1 models here";
     return CLB_EUNSUPPORTED;
   }
   if (cfg->evolver != CLB_LF) {

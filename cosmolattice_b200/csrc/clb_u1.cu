@@ -10,6 +10,7 @@
 #include "clb_adjoint.cuh"
 #include "clb_handle.cuh"
 #include "clb_u1.cuh"
+#include "clb_vv.h"
 
 #include <algorithm>
 #include <cmath>
@@ -109,17 +110,20 @@ template <int NK, bool RF, bool RP> void kick(clb_handle *h, int kind, const U1K
   kick_t<NK, RF, RP, double>(h, kind, kc);
 }
 
-template <class S> void drift_t(clb_handle *h, double w)
+template <class S> void drift_t(clb_handle *h, double w, double dtd)
 {
   U1Sector *u = h->u1;
   CLB_LAUNCH(h, K_U1_DRIFT,
              k_u1_drift<S><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<S *>(u->f), static_cast<const S *>(u->p),
-                                                              h->n3, w, h->cfg.dt, u->d_st));
+                                                              h->n3, w, dtd, u->d_st));
 }
-void drift(clb_handle *h, double w)
+// field drifts of weight w over dt (the position Verlet's half drifts pass dt/2: halving is exact,
+// so ((pow dt)/2) w and ((pow w) dt)/2 of positionverlet.h:182-197 are the same numbers)
+void drift(clb_handle *h, double w, double dtd = -1.0)
 {
-  if (h->u1->fp32) return drift_t<float>(h, w);
-  drift_t<double>(h, w);
+  if (dtd < 0) dtd = h->cfg.dt;
+  if (h->u1->fp32) return drift_t<float>(h, w, dtd);
+  drift_t<double>(h, w, dtd);
 }
 
 // One measurement sweep of the live state into d_sums (unnormalised sums, kU1Meas slots).
@@ -428,6 +432,32 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
       }
     }
     h->synced = false;
+  } else if (is_pv(h->cfg.evolver)) {
+    // PositionVerlet::evolve (positionverlet.h:45-99): drift(dt/2 w), a first half-drift, kick(w dt)
+    // at the half-step a (its sweep also reduces the half-step field sums), the momentum sums, the
+    // a-kick and second half-drift, drift(dt/2 w); each step ends with a field-sum sweep.  The
+    // first a half-drift of a stage is booked in the tail before its first field drift, whose
+    // coefficient then comes from aIM.
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    const double w0 = wof(0);
+    tail(h, T_PV_MODE | (ex ? T_PV_DRIFT_A1 : 0u), false, 0, w0);
+    for (int64_t s = 0; s < nsteps; ++s)
+      for (size_t i = 0; i < S; ++i) {
+        const double w = wof(i);
+        const bool last = i + 1 == S;
+        drift(h, w, dt / 2);
+        kick_sweep(h, 1, ex, ex, lf_kick(dt, w));
+        if (ex)
+          tail(h, T_PV_MODE | T_PV_STORE_SI | T_PV_STORE_PI2 | T_PV_KICK | T_PV_DRIFT_A2 | (last ? 0u : T_PV_DRIFT_A1),
+               true, w, last ? 0.0 : wof(i + 1));
+        drift(h, w, dt / 2);
+        if (last && ex) {
+          kick_sweep(h, 0, true, false, U1Kick{});
+          tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), true, 0, w0, s);
+        }
+      }
   } else {
     vv_run(h, nsteps, nullptr);
   }
@@ -617,7 +647,8 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
                                                      int32_t nw, double *obs)
 {
   U1Sector *u = h->u1;
-  if (h->cfg.evolver == CLB_LF) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers");
+  if (h->cfg.evolver == CLB_LF || is_pv(h->cfg.evolver))
+    return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers");
   if (nsteps < 1 || K < 1) return h->fail(CLB_EINVAL, "clb_forward: nsteps and checkpoint_every must be >= 1");
   if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
   cudaError_t e = cudaStreamSynchronize(h->stream);

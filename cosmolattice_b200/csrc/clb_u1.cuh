@@ -33,7 +33,8 @@ struct U1State {
   double csPi2I, csPi2SI, csPi2SIM, csGrad2I;
   double u1Pi2I, u1Pi2SI, u1Pi2SIM, u1Mag2I;
   double potI, potSI;
-  double cs_drift; // pow(aSI, alpha - 3)        (velocityverlet.h:195)
+  double csGrad2SI, u1Mag2SI; // position Verlet: field averages at the half step (positionverlet.h:258-266)
+  double cs_drift; // pow(aSI, alpha - 3)        (velocityverlet.h:195); position Verlet pow(aI, ...)
   double u1_drift; // pow(aSI, alpha - 1)        (velocityverlet.h:207)
   double kA;       // pow(aI, 1 + alpha)         (complexscalarkernels.h:33, u1kernels.h:45)
   double kB2;      // pow(aI, 3 + alpha) / 2     (complexscalarkernels.h:34)
@@ -309,6 +310,20 @@ __device__ __forceinline__ double u1_sf_kernel(const U1State &s, const U1Params 
 }
 
 
+// ScaleFactorKernels::getSI with complex-scalar and U(1) energies (scalefactorkernels.h:83-119):
+// the half-step averages at aI.
+__device__ __forceinline__ double u1_sf_kernel_si(const U1State &s, const U1Params &p)
+{
+  const double al = p.alpha;
+  const double e4 = u1_m(p.el0, ipow_d(s.aI, -4));
+  const double Ekcs = u1_m(s.csPi2SI, ipow_d(s.aI, -6));
+  const double Egcs = u1_m(s.csGrad2SI, ipow_d(s.aI, -2));
+  const double Eel = u1_m(e4, s.u1Pi2SI), Emag = u1_m(e4, s.u1Mag2SI);
+  const double br = u1_a(u1_a(u1_a(u1_m(al - 2, Ekcs), u1_m(al, Egcs)), u1_m(al - 1, u1_a(Eel, Emag))),
+                         u1_m(al + 1, s.potSI));
+  return u1_m(u1_m(pow(s.aI, 2 * al + 1) / 3.0, p.fm2), br);
+}
+
 // One-thread tail: fixed-order sum of the kick-sweep partials and the scale-factor update, in
 // the order of the VelocityVerlet and LeapFrog schedules (same flags as the scalar tail).
 // Fixed-order sum of the kick-sweep partial rows (all threads of one 256-thread block; the
@@ -400,8 +415,33 @@ __device__ __forceinline__ void u1_tail_apply(U1State &s, const double (&v)[kU1R
     s.aI = u1_a(s.aI, u1_m(u1_m(dt, s.aDotSI), op.w2));
     s.aSI = (s.aIM + s.aI) / 2.0;
   }
-  s.cs_drift = pow(s.aSI, p.alpha - 3);
-  s.u1_drift = pow(s.aSI, p.alpha - 1);
+  // PositionVerlet (positionverlet.h:160-163, 207-276), as in the scalar tail
+  if (fl & T_PV_STORE_SI) {
+    s.csGrad2SI = csG;
+    s.u1Mag2SI = u1B;
+    s.potSI = pot;
+  }
+  if (fl & T_PV_STORE_PI2) {
+    s.csPi2SIM = s.csPi2I; // CSpi2AvIM
+    s.u1Pi2SIM = s.u1Pi2I;
+    s.csPi2I = csP;
+    s.u1Pi2I = u1P;
+    s.csPi2SI = 0.5 * (s.csPi2I + s.csPi2SIM);
+    s.u1Pi2SI = 0.5 * (s.u1Pi2I + s.u1Pi2SIM);
+  }
+  if (fl & T_PV_KICK) s.aDotI = u1_a(s.aDotI, u1_m(u1_m(dt, u1_sf_kernel_si(s, p)), op.w));
+  if (fl & T_PV_DRIFT_A2) {
+    s.aI = u1_a(s.aI, u1_m(u1_m(dt / 2.0, s.aDotI), op.w));
+    s.aSI = (s.aIM + s.aI) / 2.0;
+  }
+  if (fl & T_PV_DRIFT_A1) {
+    s.aIM = s.aI;
+    s.aI = u1_a(s.aI, u1_m(u1_m(dt / 2.0, s.aDotI), op.w2));
+    s.aSI = s.aI;
+  }
+  const double ad = (fl & T_PV_MODE) ? ((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI) : s.aSI;
+  s.cs_drift = pow(ad, p.alpha - 3);
+  s.u1_drift = pow(ad, p.alpha - 1);
   s.kA = pow(s.aI, 1 + p.alpha);
   s.kB2 = pow(s.aI, 3 + p.alpha) / 2;
   s.kG = pow(s.aI, -1 + p.alpha);

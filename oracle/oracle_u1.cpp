@@ -42,6 +42,7 @@ struct U1Oracle {
   double aI = 1, aSI = 1, aIM = 1, aDotI = 0, aDotSI = 0, aDotSIM = 0;
   double csPi2I = 0, csPi2SI = 0, csPi2SIM = 0, csGrad2I = 0;
   double u1Pi2I = 0, u1Pi2SI = 0, u1Pi2SIM = 0, u1Mag2I = 0;
+  double csPi2IM = 0, u1Pi2IM = 0, csGrad2SI = 0, u1Mag2SI = 0; // position Verlet (positionverlet.h:238-276)
   double potI = 0, potSI = 0;
   bool synced = true, initialized = false;
   std::vector<double> ws;
@@ -236,6 +237,16 @@ struct U1Oracle {
            ((((al - 2) * Ekcs + al * Egcs) + (al - 1) * (1.0 * (Eel + Emag))) + (al + 1) * potI);
   }
 
+  double sfKernelSI() const // ScaleFactorKernels::getSI (scalefactorkernels.h:83-119)
+  {
+    const double al = md.alpha;
+    const double Ekcs = kineticCS(csPi2SI), Egcs = gradientCS(csGrad2SI);
+    const double Eel = electricU1(u1Pi2SI), Emag = magneticU1(u1Mag2SI);
+    const double fm = md.fStar / md.MPl;
+    return std::pow(aI, 2 * al + 1) / 3.0 * (fm * fm) *
+           ((((al - 2) * Ekcs + al * Egcs) + (al - 1) * (Eel + Emag)) + (al + 1) * potSI);
+  }
+
   void setAllAverages() // averages.h:349-378
   {
     potI = avPot();
@@ -318,6 +329,45 @@ struct U1Oracle {
         csPi2I = avCsPi2();
         u1Pi2I = avU1Pi2();
         aDotI = aDotSI + (dt / 2) * sfKernel() * w;
+      }
+    }
+  }
+
+  // PositionVerlet::evolve (positionverlet.h:45-99): driftCS / driftU1Vector (:182-185, :194-197),
+  // kickCS / kickU1Vector (:138-157), the scale factor (:160-163, :207-235), averages (:238-276)
+  void evolvePV()
+  {
+    const double dt = cfg.dt;
+    const size_t Pn = ws.size(), stages = (Pn - 1) * 2 + 1;
+    const bool ex = cfg.expansion != 0;
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < Pn ? i : stages - i - 1];
+      drift(std::pow(aI, md.alpha - 3) * dt / 2 * w, std::pow(aI, md.alpha - 1) * w * dt / 2);
+      if (ex) {
+        aIM = aI;
+        aI += dt / 2.0 * aDotI * w;
+        aSI = aI;
+        csGrad2SI = avCsGrad2();
+        u1Mag2SI = avU1B2();
+        potSI = avPot();
+      }
+      kick(dt * w, dt * w);
+      if (ex) {
+        csPi2IM = csPi2I;
+        u1Pi2IM = u1Pi2I;
+        csPi2I = avCsPi2();
+        u1Pi2I = avU1Pi2();
+        csPi2SI = 0.5 * (csPi2I + csPi2IM);
+        u1Pi2SI = 0.5 * (u1Pi2I + u1Pi2IM);
+        aDotI += dt * sfKernelSI() * w;
+        aI += dt / 2.0 * aDotI * w;
+        aSI = (aIM + aI) / 2.0;
+      }
+      drift(std::pow(aI, md.alpha - 3) * dt / 2 * w, std::pow(aI, md.alpha - 1) * w * dt / 2);
+      if (ex) {
+        csGrad2I = avCsGrad2();
+        u1Mag2I = avU1B2();
+        potI = avPot();
       }
     }
   }
@@ -417,7 +467,7 @@ void *u1_create(const clb_config *cfg, const clb_model_desc *md, std::string &er
   o->F.assign(5 * o->n3, 0.0);
   o->P.assign(5 * o->n3, 0.0);
   if (cfg->evolver != CLB_LF) {
-    o->ws = oracle_vv_weights(cfg->evolver);
+    o->ws = oracle_vv_weights(cfg->evolver >= CLB_PV2 ? cfg->evolver - CLB_PV2 + CLB_VV2 : cfg->evolver);
     if (o->ws.empty()) {
       delete o;
       err = "unsupported evolver";
@@ -488,6 +538,8 @@ int u1_evolve(void *h, int64_t n)
   for (int64_t s = 0; s < n; ++s) {
     if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
+    else if (o->cfg.evolver >= CLB_PV2)
+      o->evolvePV();
     else
       o->evolveVV();
   }

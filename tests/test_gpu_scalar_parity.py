@@ -221,12 +221,12 @@ def test_pv_history_rows_match_measurements():
     assert abs(hist[-1][1] - mm["aDotI"]) <= 1e-15 * abs(mm["aDotI"])
 
 
-def test_pv_rejected_for_gauge_models():
-    from conftest import make_u1_case
+def test_pv_rejected_for_lphi4su2u1():
+    from conftest import make_su2_case
 
     from cosmolattice_b200 import Lattice, _capi
 
-    par, rp, m, *_ = make_u1_case(N=8, evolver="PV2")
+    par, rp, m, *_ = make_su2_case(N=6, evolver="PV2")
     with pytest.raises(_capi.ClbError):
         Lattice(m, rp)
 

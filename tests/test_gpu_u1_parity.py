@@ -219,3 +219,33 @@ def test_u1_fp32_form_tracks_fp64():
     assert ma["gauss_u1"][0] <= 1e-4
     assert abs(ma["gauss_u1"][2] - mb["gauss_u1"][2]) <= 1e-4 * mb["gauss_u1"][2]
     assert sdiff <= 1e-5
+
+
+# ---- position Verlet for lphi4U1 (PositionVerlet::evolve, positionverlet.h:45-99) -------------
+
+@pytest.mark.parametrize("evolver,expansion", [("PV2", True), ("PV2", False), ("PV4", True), ("PV6", True)])
+def test_lphi4u1_position_verlet(evolver, expansion):
+    g, c, meas = run_pair(16, evolver, expansion, 30, measure_every=7, links=0.05)
+    check_state(g, c, 16)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_lphi4u1_position_verlet_fp32_and_adjoint_guard():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_u1_case(N=16, evolver="PV4", dt=0.01, amp=2e-2)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        lat = Lattice(m, rp, precision=prec)
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.evolve(20)
+        lat.sync()
+        out[prec] = lat.measure(1.0)
+        if prec == "fp64":
+            with pytest.raises(_capi.ClbError):
+                lat.forward(4, 2, [0, 0, 1, 1, 0])  # the adjoint covers the VV evolvers
+        lat.close()
+    assert abs(out["fp32"]["aI"] - out["fp64"]["aI"]) <= 1e-7 * out["fp64"]["aI"]
+    for x, y in zip(out["fp32"]["energies"], out["fp64"]["energies"]):
+        assert abs(x - y) <= 1e-4 * abs(out["fp64"]["energies"][-1])
