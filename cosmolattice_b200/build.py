@@ -58,7 +58,24 @@ def build(force: bool = False, verbose: bool = False, out: str = None, defines=(
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
+    if out is None:
+        build_host(verbose)
     return lib
+
+
+HOST_SRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "host", "cosmolattice_b200.cpp")
+HOST_BIN = os.path.join(os.path.dirname(LIB), "cosmolattice_b200")
+
+
+def build_host(verbose: bool = False) -> str:
+    """The C++20 host program (the reference's main over the C ABI), linked next to the library."""
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-std=c++20", "-O2", "-Wall", HOST_SRC, "-o", HOST_BIN, "-L", os.path.dirname(LIB), "-lclb200",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return HOST_BIN
 
 
 if __name__ == "__main__":
