@@ -712,10 +712,6 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_EINVAL;
   }
   std::vector<double> ws;
-  if (is_pv(cfg->evolver) && su2) {
-    g_err = "clb_create: position Verlet evolves the scalar-singlet and lphi4U1 models here";
-    return CLB_EUNSUPPORTED;
-  }
   if (cfg->evolver != CLB_LF) {
     ws = is_pv(cfg->evolver) ? pv_coefficients(cfg->evolver) : vv_coefficients(cfg->evolver);
     if (ws.empty()) {

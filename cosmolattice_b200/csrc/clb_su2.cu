@@ -8,6 +8,7 @@
 
 #include "clb_handle.cuh"
 #include "clb_su2.cuh"
+#include "clb_vv.h"
 
 #include <cmath>
 #include <cstdlib>
@@ -216,8 +217,9 @@ template <class S> void drift_tan_t(clb_handle *h, double w, bool lf)
                                                                u->prm, w, lf ? 1 : 0, u->d_tst, u->tan_cd));
 }
 
-void drift(clb_handle *h, double w, bool lf)
+void drift(clb_handle *h, double w, bool lf, double dtd = -1.0)
 {
+  if (dtd < 0) dtd = h->cfg.dt;
   SU2Sector *u = h->su2;
   if (u->tangent) {
     if (u->fp32)
@@ -230,12 +232,12 @@ void drift(clb_handle *h, double w, bool lf)
     CLB_LAUNCH(h, K_U1_DRIFT, k_drift<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f),
                                                                                  static_cast<const float *>(u->p),
                                                                                  u->prm, w, lf ? 1 : 0, u->d_st,
-                                                                                 static_cast<float *>(u->ph)));
+                                                                                 static_cast<float *>(u->ph), dtd));
   else
     CLB_LAUNCH(h, K_U1_DRIFT, k_drift<double><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<double *>(u->f),
                                                                                   static_cast<const double *>(u->p),
                                                                                   u->prm, w, lf ? 1 : 0, u->d_st,
-                                                                                  static_cast<double *>(u->ph)));
+                                                                                  static_cast<double *>(u->ph), dtd));
 }
 
 // FP32 form: after the drift of every kUnitarizeEvery-th step the links are projected back to
@@ -461,6 +463,33 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
       }
     }
     h->synced = false;
+  } else if (is_pv(h->cfg.evolver)) {
+    // PositionVerlet::evolve (positionverlet.h:45-99), as for lphi4U1: drift(dt/2 w), kick(w dt)
+    // at the half-step a with the half-step field sums and the momentum sums, the a-kick and a
+    // half-drifts in the tails, drift(dt/2 w); a field-sum sweep ends each step
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    const double w0 = wof(0);
+    tail(h, T_PV_MODE | (ex ? T_PV_DRIFT_A1 : 0u), false, 0, w0);
+    for (int64_t s = 0; s < nsteps; ++s)
+      for (size_t i = 0; i < S; ++i) {
+        const double w = wof(i);
+        const bool last = i + 1 == S;
+        drift(h, w, false, dt / 2);
+        sweep(h, 1, ex, ex, lf_kick(dt, w));
+        if (ex)
+          tail(h, T_PV_MODE | T_PV_STORE_SI | T_PV_STORE_PI2 | T_PV_KICK | T_PV_DRIFT_A2 | (last ? 0u : T_PV_DRIFT_A1),
+               true, w, last ? 0.0 : wof(i + 1));
+        drift(h, w, false, dt / 2);
+        if (last) {
+          step_done(h);
+          if (ex) {
+            sweep(h, 0, true, false, Kick{});
+            tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), true, 0, w0, s);
+          }
+        }
+      }
   } else {
     const std::vector<double> &ws = h->ws;
     const size_t P = ws.size(), S = 2 * P - 1;
@@ -657,6 +686,8 @@ __attribute__((visibility("hidden"))) int su2_tangent_begin(clb_handle *h, const
                                                             const clb_scalefactor *sf_dot)
 {
   SU2Sector *u = h->su2;
+  if (is_pv(h->cfg.evolver))
+    return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers the LF and VV evolvers");
   if (n < 0 || n > 6 || (n > 0 && !couplings_dot))
     return h->fail(CLB_EINVAL, "clb_tangent_begin: up to 6 coupling derivatives");
   cudaError_t e = cudaStreamSynchronize(h->stream);

@@ -52,8 +52,9 @@ template <class T> struct StateT {
   T aI, aSI, aIM, aDotI, aDotSI, aDotSIM;
   T pi2[5], pi2SI[5], pi2SIM[5];
   T g2S, g2C, g2D, b2A, b2G, potI;
+  T g2S_SI, g2C_SI, g2D_SI, b2A_SI, b2G_SI, potSI; // position Verlet: half-step field averages
   T kA, kB, kB2, kG; // pow(aI, 1+alpha), pow(aI, 3+alpha), /2, pow(aI, -1+alpha)
-  T p3, p1;          // pow(aSI, alpha-3), pow(aSI, alpha-1)
+  T p3, p1;          // pow(aSI, alpha-3), pow(aSI, alpha-1); position Verlet: of aI
   int32_t status, pad;
 };
 using State = StateT<double>;
@@ -79,6 +80,12 @@ template <class A, class B, class Fn> inline void zip_state(StateT<A> &x, const 
   fn(x.b2A, y.b2A);
   fn(x.b2G, y.b2G);
   fn(x.potI, y.potI);
+  fn(x.g2S_SI, y.g2S_SI);
+  fn(x.g2C_SI, y.g2C_SI);
+  fn(x.g2D_SI, y.g2D_SI);
+  fn(x.b2A_SI, y.b2A_SI);
+  fn(x.b2G_SI, y.b2G_SI);
+  fn(x.potSI, y.potSI);
   fn(x.kA, y.kA);
   fn(x.kB, y.kB);
   fn(x.kB2, y.kB2);
@@ -206,12 +213,49 @@ __global__ void __launch_bounds__(256)
     s.aI += dt * s.aDotSI * op.w2;
     s.aSI = (s.aIM + s.aI) / 2.0;
   }
+  // PositionVerlet (positionverlet.h:160-163, 207-276), as in the scalar tail; getSI is the
+  // scale-factor kernel of the half-step averages at aI
+  if (fl & T_PV_STORE_SI) {
+    s.g2S_SI = v[5];
+    s.g2C_SI = v[6];
+    s.g2D_SI = v[7];
+    s.b2A_SI = v[8];
+    s.b2G_SI = v[9];
+    s.potSI = v[10];
+  }
+  if (fl & T_PV_STORE_PI2)
+    for (int g = 0; g < 5; ++g) {
+      s.pi2SIM[g] = s.pi2[g]; // pi2AvIM
+      s.pi2[g] = v[g];
+      s.pi2SI[g] = 0.5 * (s.pi2[g] + s.pi2SIM[g]);
+    }
+  if (fl & T_PV_KICK) {
+    StateT<T> si = s;
+    for (int g = 0; g < 5; ++g) si.pi2[g] = s.pi2SI[g];
+    si.g2S = s.g2S_SI;
+    si.g2C = s.g2C_SI;
+    si.g2D = s.g2D_SI;
+    si.b2A = s.b2A_SI;
+    si.b2G = s.b2G_SI;
+    si.potI = s.potSI;
+    s.aDotI += dt * sf_kernel(si, p) * op.w;
+  }
+  if (fl & T_PV_DRIFT_A2) {
+    s.aI += dt / 2.0 * s.aDotI * op.w;
+    s.aSI = (s.aIM + s.aI) / 2.0;
+  }
+  if (fl & T_PV_DRIFT_A1) {
+    s.aIM = s.aI;
+    s.aI += dt / 2.0 * s.aDotI * op.w2;
+    s.aSI = s.aI;
+  }
   s.kA = pow(s.aI, 1 + p.alpha);
   s.kB = pow(s.aI, 3 + p.alpha);
   s.kB2 = pow(s.aI, 3 + p.alpha) / 2;
   s.kG = pow(s.aI, -1 + p.alpha);
-  s.p3 = pow(s.aSI, p.alpha - 3);
-  s.p1 = pow(s.aSI, p.alpha - 1);
+  const T ad = (fl & T_PV_MODE) ? ((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI) : s.aSI;
+  s.p3 = pow(ad, p.alpha - 3);
+  s.p1 = pow(ad, p.alpha - 1);
   bool ok = finite_(s.aI) && finite_(s.aDotI) && finite_(s.aDotSI) && finite_(s.potI);
   for (int g = 0; g < 5; ++g) ok = ok && finite_(s.pi2[g]);
   if (!ok) s.status = 1;

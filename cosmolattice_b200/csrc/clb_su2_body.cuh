@@ -502,9 +502,10 @@ template <class S> __global__ void __launch_bounds__(256) k_phases(const S *__re
 template <class S>
 __global__ void __launch_bounds__(256)
     k_drift(S *__restrict__ f, const S *__restrict__ p, Params a, double w, int lf, const State *__restrict__ stp,
-            S *__restrict__ ph)
+            S *__restrict__ ph, double dtd)
 {
-  const double dt = a.dt, p3 = stp->p3, p1 = stp->p1;
+  // dtd: the time step of this drift (the position Verlet's half drifts pass dt/2)
+  const double dt = dtd, p3 = stp->p3, p1 = stp->p1;
   const double cC = lf ? p3 * dt : p3 * dt * w;
   const double cA = lf ? p1 * dt : p1 * w * dt;
   const double cG = lf ? p1 * a.dx * dt * a.gS : w * p1 * a.dx * dt * a.gS;

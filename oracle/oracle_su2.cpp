@@ -98,6 +98,8 @@ struct SU2Oracle {
   double pi2A = 0, pi2ASI = 0, pi2ASIM = 0, b2A = 0;
   double pi2G = 0, pi2GSI = 0, pi2GSIM = 0, b2G = 0;
   double potI = 0;
+  // position Verlet: field averages at the half step (positionverlet.h:258-266)
+  double g2S_SI = 0, g2C_SI = 0, g2D_SI = 0, b2A_SI = 0, b2G_SI = 0, potSI = 0;
   bool synced = true, initialized = false;
   std::vector<double> ws;
   std::string err;
@@ -341,10 +343,13 @@ struct SU2Oracle {
     kick(h);
   }
   // drifts (velocityverlet.h:181-222; leapfrog with w = 1)
-  void drift(double w, bool lf)
+  void drift(double w, bool lf) { driftWith(w, lf, cfg.dt, std::pow(aSI, md.alpha - 3), std::pow(aSI, md.alpha - 1)); }
+  // position Verlet (positionverlet.h:170-222): pow(aI, .) and dt/2, whose halving is exact, so
+  // pow (dt/2 w pi), ((pow dt)/2) w, ((pow w) dt)/2 and the link's (((w pow) dx) dt)/2 gQ are
+  // the numbers of the formulas below with dt -> dt/2
+  void driftPV(double w) { driftWith(w, false, cfg.dt / 2, std::pow(aI, md.alpha - 3), std::pow(aI, md.alpha - 1)); }
+  void driftWith(double w, bool lf, double dt, double p3, double p1)
   {
-    const double dt = cfg.dt, al = md.alpha;
-    const double p3 = std::pow(aSI, al - 3), p1 = std::pow(aSI, al - 1);
     const double cS = p3;                                 // S: pow * (dt w pi)
     const double cC = lf ? p3 * dt : p3 * dt * w;         // phi, Phi: pow dt w pi
     const double cA = lf ? p1 * dt : p1 * w * dt;         // A: pow w dt pi
@@ -487,6 +492,18 @@ struct SU2Oracle {
     return En{0.5 * pi2S * a6, 0.5 * g2S * a2, pi2C * a6, g2C * a2, pi2D * a6, g2D * a2,
               e4 * pi2A * 1.0,  e4 * b2A / 1.0, e4 * pi2G, e4 * b2G};
   }
+  double sfKernelSI() const // ScaleFactorKernels::getSI (scalefactorkernels.h:83-119)
+  {
+    const double al = md.alpha;
+    const double a6 = ipow(aI, -6), a2 = ipow(aI, -2), e4 = 0.5 * rof2() * ipow(aI, -4);
+    const En E{0.5 * pi2SSI * a6, 0.5 * g2S_SI * a2, pi2CSI * a6, g2C_SI * a2, pi2DSI * a6, g2D_SI * a2,
+               e4 * pi2ASI * 1.0,  e4 * b2A_SI / 1.0, e4 * pi2GSI, e4 * b2G_SI};
+    const double fm = md.fStar / md.MPl;
+    return std::pow(aI, 2 * al + 1) / 3.0 * (fm * fm) *
+           ((((al - 2) * ((E.ks + E.kc) + E.kd) + al * ((E.gs + E.gc) + E.gd)) +
+             (al - 1) * (((E.ea + E.ba) + E.eg) + E.bg)) +
+            (al + 1) * potSI);
+  }
   double sfKernel() const // scalefactorkernels.h:73-77
   {
     const double al = md.alpha;
@@ -536,6 +553,48 @@ struct SU2Oracle {
         storeMomenta();
         aDotI = aDotSI + (dt / 2) * sfKernel() * w;
       }
+    }
+  }
+  // PositionVerlet::evolve (positionverlet.h:45-99, 160-276)
+  void evolvePV()
+  {
+    const double dt = cfg.dt;
+    const size_t Pn = ws.size(), stages = (Pn - 1) * 2 + 1;
+    const bool ex = cfg.expansion != 0;
+    auto upd = [](double &I, double &SI, double &IM, double v) {
+      IM = I;
+      I = v;
+      SI = 0.5 * (I + IM);
+    };
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < Pn ? i : stages - i - 1];
+      driftPV(w);
+      if (ex) {
+        aIM = aI;
+        aI += dt / 2.0 * aDotI * w;
+        aSI = aI;
+        storeFields();
+        g2S_SI = g2S;
+        g2C_SI = g2C;
+        g2D_SI = g2D;
+        b2A_SI = b2A;
+        b2G_SI = b2G;
+        potSI = potI;
+      }
+      const double h[5] = {w * dt, dt * w, dt * w, dt * w, dt * w}; // positionverlet.h:132-157
+      kick(h);
+      if (ex) {
+        upd(pi2S, pi2SSI, pi2SSIM, avPiS());
+        upd(pi2C, pi2CSI, pi2CSIM, avPiC());
+        upd(pi2D, pi2DSI, pi2DSIM, avPiD());
+        upd(pi2A, pi2ASI, pi2ASIM, avPiA());
+        upd(pi2G, pi2GSI, pi2GSIM, avPiG());
+        aDotI += dt * sfKernelSI() * w;
+        aI += dt / 2.0 * aDotI * w;
+        aSI = (aIM + aI) / 2.0;
+      }
+      driftPV(w);
+      if (ex) storeFields();
     }
   }
   void lfStoreMomenta()
@@ -687,7 +746,7 @@ void *su2_create(const clb_config *cfg, const clb_model_desc *md, std::string &e
   o->F.assign((size_t)NF * o->n3, 0.0);
   o->P.assign((size_t)NP * o->n3, 0.0);
   if (cfg->evolver != CLB_LF) {
-    o->ws = oracle_vv_weights(cfg->evolver);
+    o->ws = oracle_vv_weights(cfg->evolver >= CLB_PV2 ? cfg->evolver - CLB_PV2 + CLB_VV2 : cfg->evolver);
     if (o->ws.empty()) {
       delete o;
       err = "unsupported evolver";
@@ -758,6 +817,8 @@ int su2_evolve(void *h, int64_t n)
   for (int64_t s = 0; s < n; ++s) {
     if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
+    else if (o->cfg.evolver >= CLB_PV2)
+      o->evolvePV();
     else
       o->evolveVV();
   }

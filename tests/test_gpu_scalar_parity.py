@@ -221,16 +221,6 @@ def test_pv_history_rows_match_measurements():
     assert abs(hist[-1][1] - mm["aDotI"]) <= 1e-15 * abs(mm["aDotI"])
 
 
-def test_pv_rejected_for_lphi4su2u1():
-    from conftest import make_su2_case
-
-    from cosmolattice_b200 import Lattice, _capi
-
-    par, rp, m, *_ = make_su2_case(N=6, evolver="PV2")
-    with pytest.raises(_capi.ClbError):
-        Lattice(m, rp)
-
-
 # ---- fixed background (FixedBackgroundExpansion, fixedbackgroundexpansion.h:21-45) --------------
 
 # H0 = 0.5 in program units: omega_* = sqrt(lambda) phi_0 = 5.6964e18 GeV for the lphi4_1f case

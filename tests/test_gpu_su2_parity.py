@@ -181,3 +181,32 @@ def test_su2_rejects_unsupported():
     ko, vo, co = spectrum(fg.reshape(22, 6, 6, 6)[3], rp.dx)
     assert c.tolist() == co.tolist() and np.abs(v - vo).max() <= 1e-10 * np.abs(vo).max()
     lat.close()
+
+
+# ---- position Verlet for lphi4SU2U1 (PositionVerlet::evolve, positionverlet.h:45-99) ----------
+
+@pytest.mark.parametrize("evolver,expansion", [("PV2", True), ("PV2", False), ("PV4", True)])
+def test_lphi4su2u1_position_verlet(evolver, expansion):
+    g, c, meas = run_pair(8, evolver, expansion, 20, measure_every=7, links=True)
+    check(g, c, meas)
+
+
+def test_lphi4su2u1_position_verlet_fp32_and_tangent_guard():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_su2_case(N=8, evolver="PV4", amp=3e-2)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        lat = Lattice(m, rp, precision=prec)
+        lat.set_state(f, p, sf)
+        if prec == "fp64":
+            with pytest.raises(_capi.ClbError):
+                lat.tangent_begin([0, 0, 0, 0, 1, 0])  # the tangent-linear form covers LF and VV
+        lat.initialize()
+        lat.evolve(20)
+        lat.sync()
+        out[prec] = lat.measure(1.0)
+        lat.close()
+    assert abs(out["fp32"]["aI"] - out["fp64"]["aI"]) <= 1e-7 * out["fp64"]["aI"]
+    for x, y in zip(out["fp32"]["energies"], out["fp64"]["energies"]):
+        assert abs(x - y) <= 1e-4 * abs(out["fp64"]["energies"][-1])
