@@ -702,10 +702,6 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_EINVAL;
   }
   const bool fb = cfg->expansion && cfg->fixed_background;
-  if (fb && (u1 || su2)) {
-    g_err = "clb_create: the fixed background evolves the scalar-singlet models here";
-    return CLB_EUNSUPPORTED;
-  }
   if (fb && !(std::fabs(cfg->H0) > 1e-8)) { // runParameterTolerance (fixedbackgroundexpansion.h:28-31)
     g_err = "For models that do not involve cosmic defects, you need to specify a non-zero H0 to run a simulation with "
             "fixed background. If you want to disable expansion, please set expansion = false in the input file.";
@@ -729,6 +725,12 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   h->md = *md;
   h->N = cfg->N;
   h->n3 = (size_t)cfg->N * cfg->N * cfg->N;
+  h->fb = fb;
+  if (fb) { // pEoS, H0 (fixedbackgroundexpansion.h:21-26)
+    h->fb_p = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
+    h->fb_H0 = cfg->H0;
+    h->fb_t = cfg->t0;
+  }
   if (u1 || su2) {
     h->ws = ws;
     const int r = u1 ? u1_create(h) : su2_create(h);
@@ -741,12 +743,6 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
     return CLB_OK;
   }
   h->NS = md->n_scalars;
-  h->fb = fb;
-  if (fb) { // pEoS, H0 (fixedbackgroundexpansion.h:21-26)
-    h->fb_p = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
-    h->fb_H0 = cfg->H0;
-    h->fb_t = cfg->t0;
-  }
   h->fp32 = cfg->precision == CLB_PREC_FP32_SPLIT;
   h->esz = h->fp32 ? sizeof(float) : sizeof(double);
   h->ws = ws;
@@ -984,6 +980,7 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
 {
   if (!h) return CLB_EINVAL;
   if (!h->has_state) return h->fail(CLB_ESTATE, "clb_initialize: no state uploaded");
+  h->fb_t = h->cfg.t0;
   if (h->u1 || h->su2) {
     const int r = h->u1 ? u1_initialize(h, correct_adot) : su2_initialize(h, correct_adot);
     if (r == CLB_OK) h->initialized = true;
@@ -1015,7 +1012,7 @@ int clb_evolve(clb_handle *h, int64_t n)
   }
   if (h->u1 || h->su2) {
     const int r = h->u1 ? u1_evolve(h, n) : su2_evolve(h, n);
-    if (r == CLB_OK && h->cfg.expansion) h->hist_rows = n;
+    if (r == CLB_OK && h->cfg.expansion && !h->fb) h->hist_rows = n;
     return r;
   }
   cudaEventRecord(h->ev_call[0], h->stream);

@@ -255,10 +255,11 @@ void step_done(clb_handle *h)
     CLB_LAUNCH(h, K_U1_DRIFT, k_unitarize<float><<<kSU2Blocks, 256, 0, h->stream>>>(static_cast<float *>(u->f), h->n3));
 }
 
-void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
+void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1,
+          double fa = 0, double fb = 0)
 {
   SU2Sector *u = h->su2;
-  TailOp op{flags, reduced ? kSU2Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
+  TailOp op{flags, reduced ? kSU2Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row, fa, fb};
   if (u->tangent)
     CLB_LAUNCH(h, K_TAIL, su2d::k_tail<Tan<double>><<<1, 256, 0, h->stream>>>(u->d_tpart, op, u->d_tst, u->prm));
   else
@@ -436,7 +437,7 @@ __attribute__((visibility("hidden"))) int su2_initialize(clb_handle *h, int32_t 
 {
   sweep(h, 0, true, true, Kick{});
   uint32_t fl = T_STORE_ALL;
-  if (h->cfg.expansion && correct_adot) fl |= T_CORRECT_ADOT;
+  if (h->cfg.expansion && correct_adot && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
   if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
   tail(h, fl, true);
   h->synced = true;
@@ -448,7 +449,61 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
   const double dt = h->cfg.dt;
   const bool ex = h->cfg.expansion != 0;
   cudaEventRecord(h->ev_call[0], h->stream);
-  if (h->cfg.evolver == CLB_LF) {
+  if (h->fb) {
+    // fixed background (velocityverlet.h:74-118, leapfrog.h:55-89, positionverlet.h:45-99 with the
+    // fixed branches): a from the closed form at the reference's stage times, no a-kicks and no
+    // averages; the VV a-drift leaves aSI, which its field drifts read, as it was
+    const double t0 = h->cfg.t0;
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    if (h->cfg.evolver == CLB_LF) {
+      for (int64_t s = 0; s < nsteps; ++s) {
+        sweep(h, 1, false, false, lf_kick(dt, h->synced ? 0.5 : 1.0));
+        const double tm = h->fb_t - t0;
+        tail(h, T_FB_AIM | T_FB_AI | T_FB_ASI, false, 0, 0, -1, h->fb_a(tm + dt), h->fb_a(tm + dt / 2.0));
+        drift(h, 1.0, true);
+        step_done(h);
+        h->fb_t += dt;
+        h->synced = false;
+      }
+    } else if (is_pv(h->cfg.evolver)) {
+      tail(h, T_PV_MODE, false);
+      for (int64_t s = 0; s < nsteps; ++s) {
+        double tc = h->fb_t - t0;
+        for (size_t i = 0; i < S; ++i) {
+          const double w = wof(i);
+          drift(h, w, false, dt / 2);
+          tail(h, T_PV_MODE | T_FB_PV_HALF, false, 0, 0, -1, 0.0, h->fb_a(tc + w * dt / 2.0));
+          sweep(h, 1, false, false, lf_kick(dt, w));
+          tail(h, T_PV_MODE | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
+          drift(h, w, false, dt / 2);
+          tc += dt * w;
+        }
+        step_done(h);
+        h->fb_t += dt;
+      }
+    } else {
+      const int64_t total = nsteps * (int64_t)S;
+      sweep(h, 1, false, false, vv_kick(dt, wof(0), 0.0));
+      double tc = h->fb_t - t0;
+      for (int64_t k = 0; k < total; ++k) {
+        const size_t i = (size_t)(k % (int64_t)S);
+        const double w = wof(i);
+        const bool more = k + 1 < total;
+        const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+        tail(h, T_FB_AIM | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
+        drift(h, w, false);
+        if (i + 1 == S) { step_done(h); }
+        sweep(h, more ? 2 : 1, false, false, vv_kick(dt, w, wn));
+        tc += dt * w;
+        if (i + 1 == S) {
+          h->fb_t += dt;
+          tc = h->fb_t - t0;
+        }
+      }
+    }
+  } else if (h->cfg.evolver == CLB_LF) {
     sweep(h, 1, false, ex, lf_kick(dt, h->synced ? 0.5 : 1.0));
     if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
     for (int64_t s = 0; s < nsteps; ++s) {
@@ -524,9 +579,10 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
 __attribute__((visibility("hidden"))) int su2_sync(clb_handle *h)
 {
   if (h->cfg.evolver == CLB_LF && !h->synced) {
-    sweep(h, 1, false, h->cfg.expansion != 0, lf_kick(h->cfg.dt, 0.5));
-    if (h->cfg.expansion) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
+    sweep(h, 1, false, h->cfg.expansion != 0 && !h->fb, lf_kick(h->cfg.dt, 0.5));
+    if (h->cfg.expansion && !h->fb) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
   }
+  if (h->fb) tail(h, T_FB_ADOT, false, 0, 0, -1, 0.0, h->fb_adot(h->fb_t - h->cfg.t0));
   h->synced = true;
   return check(h, "clb_sync");
 }
@@ -688,6 +744,7 @@ __attribute__((visibility("hidden"))) int su2_tangent_begin(clb_handle *h, const
   SU2Sector *u = h->su2;
   if (is_pv(h->cfg.evolver))
     return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers the LF and VV evolvers");
+  if (h->fb) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers the self-consistent expansion");
   if (n < 0 || n > 6 || (n > 0 && !couplings_dot))
     return h->fail(CLB_EINVAL, "clb_tangent_begin: up to 6 coupling derivatives");
   cudaError_t e = cudaStreamSynchronize(h->stream);

@@ -249,11 +249,21 @@ __global__ void __launch_bounds__(256)
     s.aI += dt / 2.0 * s.aDotI * op.w2;
     s.aSI = s.aI;
   }
+  // fixed background: the host's closed-form values (fixedbackgroundexpansion.h:37-45)
+  if (fl & T_FB_AIM) s.aIM = s.aI;
+  if (fl & T_FB_AI) s.aI = T(op.fa);
+  if (fl & T_FB_ASI) s.aSI = T(op.fb);
+  if (fl & T_FB_PV_HALF) {
+    s.aIM = s.aI;
+    s.aI = T(op.fb);
+    s.aSI = s.aI;
+  }
+  if (fl & T_FB_ADOT) s.aDotI = T(op.fb);
   s.kA = pow(s.aI, 1 + p.alpha);
   s.kB = pow(s.aI, 3 + p.alpha);
   s.kB2 = pow(s.aI, 3 + p.alpha) / 2;
   s.kG = pow(s.aI, -1 + p.alpha);
-  const T ad = (fl & T_PV_MODE) ? ((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI) : s.aSI;
+  const T ad = (fl & T_PV_MODE) ? ((fl & (T_PV_DRIFT_A1 | T_FB_PV_HALF)) ? s.aIM : s.aI) : s.aSI;
   s.p3 = pow(ad, p.alpha - 3);
   s.p1 = pow(ad, p.alpha - 1);
   bool ok = finite_(s.aI) && finite_(s.aDotI) && finite_(s.aDotSI) && finite_(s.potI);

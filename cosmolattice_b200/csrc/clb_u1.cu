@@ -139,10 +139,11 @@ void measure_sums(clb_handle *h)
   CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kU1Meas><<<1, 256, 0, h->stream>>>(u->d_part, kU1Blocks, u->d_sums));
 }
 
-void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1)
+void tail(clb_handle *h, uint32_t flags, bool reduced, double w = 0, double w2 = 0, int64_t hist_row = -1,
+          double fa = 0, double fb = 0)
 {
   U1Sector *u = h->u1;
-  TailOp op{flags, reduced ? kU1Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row};
+  TailOp op{flags, reduced ? kU1Blocks : 0, w, w2, hist_row >= 0 ? h->d_hist : nullptr, hist_row, fa, fb};
   CLB_LAUNCH(h, K_TAIL, k_u1_tail<<<1, 256, 0, h->stream>>>(u->d_part, op, u->d_st, u->prm));
 }
 
@@ -402,7 +403,7 @@ __attribute__((visibility("hidden"))) int u1_initialize(clb_handle *h, int32_t c
 {
   kick_sweep(h, 0, true, true, U1Kick{});
   uint32_t fl = T_STORE_ALL;
-  if (h->cfg.expansion && correct_adot) fl |= T_CORRECT_ADOT;
+  if (h->cfg.expansion && correct_adot && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
   if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
   tail(h, fl, true);
   h->synced = true;
@@ -414,7 +415,58 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
   const double dt = h->cfg.dt;
   const bool ex = h->cfg.expansion != 0;
   cudaEventRecord(h->ev_call[0], h->stream);
-  if (h->cfg.evolver == CLB_LF) {
+  if (h->fb) {
+    // fixed background (velocityverlet.h:74-118, leapfrog.h:55-89, positionverlet.h:45-99 with the
+    // fixed branches): a from the closed form at the reference's stage times, no a-kicks and no
+    // averages; the VV a-drift leaves aSI, which its field drifts read, as it was
+    const double t0 = h->cfg.t0;
+    const std::vector<double> &ws = h->ws;
+    const size_t P = ws.size(), S = 2 * P - 1;
+    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    if (h->cfg.evolver == CLB_LF) {
+      for (int64_t s = 0; s < nsteps; ++s) {
+        kick_sweep(h, 1, false, false, lf_kick(dt, h->synced ? 0.5 : 1.0));
+        const double tm = h->fb_t - t0;
+        tail(h, T_FB_AIM | T_FB_AI | T_FB_ASI, false, 0, 0, -1, h->fb_a(tm + dt), h->fb_a(tm + dt / 2.0));
+        drift(h, 1.0);
+        h->fb_t += dt;
+        h->synced = false;
+      }
+    } else if (is_pv(h->cfg.evolver)) {
+      tail(h, T_PV_MODE, false);
+      for (int64_t s = 0; s < nsteps; ++s) {
+        double tc = h->fb_t - t0;
+        for (size_t i = 0; i < S; ++i) {
+          const double w = wof(i);
+          drift(h, w, dt / 2);
+          tail(h, T_PV_MODE | T_FB_PV_HALF, false, 0, 0, -1, 0.0, h->fb_a(tc + w * dt / 2.0));
+          kick_sweep(h, 1, false, false, lf_kick(dt, w));
+          tail(h, T_PV_MODE | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
+          drift(h, w, dt / 2);
+          tc += dt * w;
+        }
+        h->fb_t += dt;
+      }
+    } else {
+      const int64_t total = nsteps * (int64_t)S;
+      kick_sweep(h, 1, false, false, vv_kick(dt, wof(0), 0.0));
+      double tc = h->fb_t - t0;
+      for (int64_t k = 0; k < total; ++k) {
+        const size_t i = (size_t)(k % (int64_t)S);
+        const double w = wof(i);
+        const bool more = k + 1 < total;
+        const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+        tail(h, T_FB_AIM | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
+        drift(h, w);
+        kick_sweep(h, more ? 2 : 1, false, false, vv_kick(dt, w, wn));
+        tc += dt * w;
+        if (i + 1 == S) {
+          h->fb_t += dt;
+          tc = h->fb_t - t0;
+        }
+      }
+    }
+  } else if (h->cfg.evolver == CLB_LF) {
     // LeapFrog::evolve: kick (1/2 dt after a sync), <pi^2>, a kick and drift, field drifts, field averages
     const double weight = h->synced ? 0.5 : 1.0;
     kick_sweep(h, 1, false, ex, lf_kick(dt, weight));
@@ -472,9 +524,10 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
 __attribute__((visibility("hidden"))) int u1_sync(clb_handle *h)
 {
   if (h->cfg.evolver == CLB_LF && !h->synced) {
-    kick_sweep(h, 1, false, h->cfg.expansion != 0, lf_kick(h->cfg.dt, 0.5));
-    if (h->cfg.expansion) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
+    kick_sweep(h, 1, false, h->cfg.expansion != 0 && !h->fb, lf_kick(h->cfg.dt, 0.5));
+    if (h->cfg.expansion && !h->fb) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
   }
+  if (h->fb) tail(h, T_FB_ADOT, false, 0, 0, -1, 0.0, h->fb_adot(h->fb_t - h->cfg.t0));
   h->synced = true;
   return check(h, "clb_sync");
 }
@@ -649,6 +702,7 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   U1Sector *u = h->u1;
   if (h->cfg.evolver == CLB_LF || is_pv(h->cfg.evolver))
     return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers");
+  if (h->fb) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the self-consistent expansion");
   if (nsteps < 1 || K < 1) return h->fail(CLB_EINVAL, "clb_forward: nsteps and checkpoint_every must be >= 1");
   if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
   cudaError_t e = cudaStreamSynchronize(h->stream);

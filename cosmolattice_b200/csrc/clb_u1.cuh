@@ -439,7 +439,17 @@ __device__ __forceinline__ void u1_tail_apply(U1State &s, const double (&v)[kU1R
     s.aI = u1_a(s.aI, u1_m(u1_m(dt / 2.0, s.aDotI), op.w2));
     s.aSI = s.aI;
   }
-  const double ad = (fl & T_PV_MODE) ? ((fl & T_PV_DRIFT_A1) ? s.aIM : s.aI) : s.aSI;
+  // fixed background: the host's closed-form values (fixedbackgroundexpansion.h:37-45)
+  if (fl & T_FB_AIM) s.aIM = s.aI;
+  if (fl & T_FB_AI) s.aI = op.fa;
+  if (fl & T_FB_ASI) s.aSI = op.fb;
+  if (fl & T_FB_PV_HALF) {
+    s.aIM = s.aI;
+    s.aI = op.fb;
+    s.aSI = s.aI;
+  }
+  if (fl & T_FB_ADOT) s.aDotI = op.fb;
+  const double ad = (fl & T_PV_MODE) ? ((fl & (T_PV_DRIFT_A1 | T_FB_PV_HALF)) ? s.aIM : s.aI) : s.aSI;
   s.cs_drift = pow(ad, p.alpha - 3);
   s.u1_drift = pow(ad, p.alpha - 1);
   s.kA = pow(s.aI, 1 + p.alpha);

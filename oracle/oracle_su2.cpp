@@ -100,6 +100,12 @@ struct SU2Oracle {
   double potI = 0;
   // position Verlet: field averages at the half step (positionverlet.h:258-266)
   double g2S_SI = 0, g2C_SI = 0, g2D_SI = 0, b2A_SI = 0, b2G_SI = 0, potSI = 0;
+  // fixed background (fixedbackgroundexpansion.h:21-45): pEoS, H0, the main loop's time t
+  bool fb = false;
+  double pEoS = 0, H0fb = 0, t = 0;
+  double aBg(double d) const { return std::pow(1 + H0fb / pEoS * d, pEoS); }
+  double aBgDot(double d) const { return H0fb * std::pow(1 + H0fb / pEoS * d, pEoS - 1); }
+
   bool synced = true, initialized = false;
   std::vector<double> ws;
   std::string err;
@@ -610,6 +616,44 @@ struct SU2Oracle {
     upd(pi2A, pi2ASI, pi2ASIM, avPiA());
     upd(pi2G, pi2GSI, pi2GSIM, avPiG());
   }
+  // fixed background, as in the U(1) oracle: VV (aSI left as it was), leapfrog and position Verlet
+  // with a from the closed form, no a-kicks or averages; one step from time t
+  void evolveFB()
+  {
+    const double dt = cfg.dt;
+    if (cfg.evolver == CLB_LF) {
+      lf_kick(synced ? 0.5 : 1.0);
+      aIM = aI;
+      aI = aBg(t - cfg.t0 + dt);
+      aSI = aBg(t - cfg.t0 + dt / 2.0);
+      drift(1.0, true);
+      synced = false;
+      return;
+    }
+    const size_t Pn = ws.size(), stages = (Pn - 1) * 2 + 1;
+    double tc = t - cfg.t0;
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < Pn ? i : stages - i - 1];
+      if (cfg.evolver >= CLB_PV2) {
+        driftPV(w);
+        aIM = aI;
+        aI = aBg(tc + w * dt / 2.0);
+        aSI = aI;
+        const double h[5] = {w * dt, dt * w, dt * w, dt * w, dt * w};
+        kick(h);
+        aI = aBg(tc + w * dt);
+        driftPV(w);
+      } else {
+        vv_kick(w);
+        aIM = aI;
+        aI = aBg(tc + w * dt);
+        drift(w, false);
+        vv_kick(w);
+      }
+      tc += dt * w;
+    }
+  }
+
   void evolveLF()
   {
     const double dt = cfg.dt;
@@ -745,6 +789,12 @@ void *su2_create(const clb_config *cfg, const clb_model_desc *md, std::string &e
   o->n3 = (size_t)cfg->N * cfg->N * cfg->N;
   o->F.assign((size_t)NF * o->n3, 0.0);
   o->P.assign((size_t)NP * o->n3, 0.0);
+  o->fb = cfg->expansion && cfg->fixed_background;
+  if (o->fb) {
+    o->pEoS = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
+    o->H0fb = cfg->H0;
+  }
+  o->t = cfg->t0;
   if (cfg->evolver != CLB_LF) {
     o->ws = oracle_vv_weights(cfg->evolver >= CLB_PV2 ? cfg->evolver - CLB_PV2 + CLB_VV2 : cfg->evolver);
     if (o->ws.empty()) {
@@ -796,7 +846,8 @@ int su2_initialize(void *h, int32_t correct_adot)
 {
   SU2Oracle *o = static_cast<SU2Oracle *>(h);
   o->setAllAverages();
-  if (o->cfg.expansion && correct_adot) {
+  o->t = o->cfg.t0;
+  if (o->cfg.expansion && correct_adot && !o->fb) {
     double hl[3];
     o->hubble(hl);
     o->aDotI = std::sqrt(hl[2]);
@@ -815,12 +866,15 @@ int su2_evolve(void *h, int64_t n)
     return CLB_ESTATE;
   }
   for (int64_t s = 0; s < n; ++s) {
-    if (o->cfg.evolver == CLB_LF)
+    if (o->fb)
+      o->evolveFB();
+    else if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
     else if (o->cfg.evolver >= CLB_PV2)
       o->evolvePV();
     else
       o->evolveVV();
+    o->t += o->cfg.dt;
   }
   return CLB_OK;
 }
@@ -828,6 +882,12 @@ int su2_evolve(void *h, int64_t n)
 int su2_sync(void *h)
 {
   SU2Oracle *o = static_cast<SU2Oracle *>(h);
+  if (o->fb) {
+    if (o->cfg.evolver == CLB_LF && !o->synced) o->lf_kick(0.5);
+    o->synced = true;
+    o->aDotI = o->aBgDot(o->t - o->cfg.t0);
+    return CLB_OK;
+  }
   if (o->cfg.evolver == CLB_LF) o->syncLF();
   return CLB_OK;
 }

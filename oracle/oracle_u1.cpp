@@ -43,6 +43,12 @@ struct U1Oracle {
   double csPi2I = 0, csPi2SI = 0, csPi2SIM = 0, csGrad2I = 0;
   double u1Pi2I = 0, u1Pi2SI = 0, u1Pi2SIM = 0, u1Mag2I = 0;
   double csPi2IM = 0, u1Pi2IM = 0, csGrad2SI = 0, u1Mag2SI = 0; // position Verlet (positionverlet.h:238-276)
+  // fixed background (fixedbackgroundexpansion.h:21-45): pEoS, H0, the main loop's time t
+  bool fb = false;
+  double pEoS = 0, H0fb = 0, t = 0;
+  double aBg(double d) const { return std::pow(1 + H0fb / pEoS * d, pEoS); }
+  double aBgDot(double d) const { return H0fb * std::pow(1 + H0fb / pEoS * d, pEoS - 1); }
+
   double potI = 0, potSI = 0;
   bool synced = true, initialized = false;
   std::vector<double> ws;
@@ -372,6 +378,45 @@ struct U1Oracle {
     }
   }
 
+  // fixed background: the VV (velocityverlet.h:74-118, 225-231; aSI is left as it was), the leapfrog
+  // (leapfrog.h:55-89, 168-175) and position Verlet (positionverlet.h:45-99, 207-235) with a from
+  // the closed form and no a-kicks or averages; one step from time t
+  void evolveFB()
+  {
+    const double dt = cfg.dt, al = md.alpha;
+    if (cfg.evolver == CLB_LF) {
+      const double weight = synced ? 0.5 : 1.0;
+      kick(weight * dt, weight * dt);
+      aIM = aI;
+      aI = aBg(t - cfg.t0 + dt);
+      aSI = aBg(t - cfg.t0 + dt / 2.0);
+      drift(std::pow(aSI, al - 3) * dt, std::pow(aSI, al - 1) * dt);
+      synced = false;
+      return;
+    }
+    const size_t Pn = ws.size(), stages = (Pn - 1) * 2 + 1;
+    double tc = t - cfg.t0;
+    for (size_t i = 0; i < stages; ++i) {
+      const double w = ws[i < Pn ? i : stages - i - 1];
+      if (cfg.evolver >= CLB_PV2) {
+        drift(std::pow(aI, al - 3) * dt / 2 * w, std::pow(aI, al - 1) * w * dt / 2);
+        aIM = aI;
+        aI = aBg(tc + w * dt / 2.0);
+        aSI = aI;
+        kick(dt * w, dt * w);
+        aI = aBg(tc + w * dt);
+        drift(std::pow(aI, al - 3) * dt / 2 * w, std::pow(aI, al - 1) * w * dt / 2);
+      } else {
+        kick(dt / 2 * w, dt * w / 2);
+        aIM = aI;
+        aI = aBg(tc + w * dt);
+        drift(std::pow(aSI, al - 3) * dt * w, std::pow(aSI, al - 1) * w * dt);
+        kick(dt / 2 * w, dt * w / 2);
+      }
+      tc += dt * w;
+    }
+  }
+
   void evolveLF()
   {
     const double dt = cfg.dt;
@@ -466,6 +511,12 @@ void *u1_create(const clb_config *cfg, const clb_model_desc *md, std::string &er
   o->n3 = (size_t)cfg->N * cfg->N * cfg->N;
   o->F.assign(5 * o->n3, 0.0);
   o->P.assign(5 * o->n3, 0.0);
+  o->fb = cfg->expansion && cfg->fixed_background;
+  if (o->fb) {
+    o->pEoS = 2.0 / (3.0 * (1.0 + cfg->omega_eos) - 2.0 * md->alpha);
+    o->H0fb = cfg->H0;
+  }
+  o->t = cfg->t0;
   if (cfg->evolver != CLB_LF) {
     o->ws = oracle_vv_weights(cfg->evolver >= CLB_PV2 ? cfg->evolver - CLB_PV2 + CLB_VV2 : cfg->evolver);
     if (o->ws.empty()) {
@@ -517,7 +568,8 @@ int u1_initialize(void *h, int32_t correct_adot)
 {
   U1Oracle *o = static_cast<U1Oracle *>(h);
   o->setAllAverages();
-  if (o->cfg.expansion && correct_adot) {
+  o->t = o->cfg.t0;
+  if (o->cfg.expansion && correct_adot && !o->fb) {
     double hl[3];
     o->hubble(hl);
     o->aDotI = std::sqrt(hl[2]);
@@ -536,12 +588,15 @@ int u1_evolve(void *h, int64_t n)
     return CLB_ESTATE;
   }
   for (int64_t s = 0; s < n; ++s) {
-    if (o->cfg.evolver == CLB_LF)
+    if (o->fb)
+      o->evolveFB();
+    else if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
     else if (o->cfg.evolver >= CLB_PV2)
       o->evolvePV();
     else
       o->evolveVV();
+    o->t += o->cfg.dt;
   }
   return CLB_OK;
 }
@@ -549,6 +604,12 @@ int u1_evolve(void *h, int64_t n)
 int u1_sync(void *h)
 {
   U1Oracle *o = static_cast<U1Oracle *>(h);
+  if (o->fb) {
+    if (o->cfg.evolver == CLB_LF && !o->synced) o->kick(0.5 * o->cfg.dt, 0.5 * o->cfg.dt);
+    o->synced = true;
+    o->aDotI = o->aBgDot(o->t - o->cfg.t0);
+    return CLB_OK;
+  }
   if (o->cfg.evolver == CLB_LF) o->syncLF();
   return CLB_OK;
 }

@@ -254,13 +254,3 @@ def test_fixed_background_scale_factor_closed_form():
     ad = 0.5 * (1 + 0.5 / p * t) ** (p - 1)
     assert abs(sg["aI"] - a) <= 1e-15 * a
     assert abs(sg["aDotI"] - ad) <= 1e-15 * ad
-
-
-def test_fixed_background_rejected_for_gauge_and_batch():
-    from conftest import make_u1_case
-
-    from cosmolattice_b200 import Lattice, _capi
-
-    par, rp, m, *_ = make_u1_case(N=8, extra={"fixedBackground": "true", "H0": 1e18})
-    with pytest.raises(_capi.ClbError):
-        Lattice(m, rp)

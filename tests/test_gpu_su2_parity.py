@@ -38,11 +38,11 @@ def random_links(f, rng, s=0.1):
     return f
 
 
-def run_pair(N, evolver, expansion, nsteps, measure_every=None, links=False):
+def run_pair(N, evolver, expansion, nsteps, measure_every=None, links=False, extra=None):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = make_su2_case(N=N, evolver=evolver, expansion=expansion, amp=3e-2)
+    par, rp, m, f, p, sf = make_su2_case(N=N, evolver=evolver, expansion=expansion, amp=3e-2, extra=extra)
     if links:
         f = random_links(f, np.random.default_rng(4))
     gpu = Lattice(m, rp)
@@ -210,3 +210,23 @@ def test_lphi4su2u1_position_verlet_fp32_and_tangent_guard():
     assert abs(out["fp32"]["aI"] - out["fp64"]["aI"]) <= 1e-7 * out["fp64"]["aI"]
     for x, y in zip(out["fp32"]["energies"], out["fp64"]["energies"]):
         assert abs(x - y) <= 1e-4 * abs(out["fp64"]["energies"][-1])
+
+
+# ---- fixed background for lphi4SU2U1 (fixedbackgroundexpansion.h:21-45) ------------------------
+
+@pytest.mark.parametrize("evolver", ["VV2", "LF", "PV2"])
+def test_lphi4su2u1_fixed_background(evolver):
+    fb = {"fixedBackground": "true", "H0": 2.0e18, "omegaEoS": 0.0}
+    g, c, meas = run_pair(8, evolver, True, 20, measure_every=7, links=True, extra=fb)
+    check(g, c, meas)
+
+
+def test_lphi4su2u1_fixed_background_rejects_the_tangent_form():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_su2_case(N=6, extra={"fixedBackground": "true", "H0": 2.0e18})
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    with pytest.raises(_capi.ClbError):
+        lat.tangent_begin([0, 0, 0, 0, 1, 0])
+    lat.close()

@@ -28,11 +28,11 @@ def rel_comp(a, b, N):
     return max(out)
 
 
-def run_pair(N, evolver, expansion, nsteps, measure_every=None, dt=0.01, amp=2e-2, links=0.0):
+def run_pair(N, evolver, expansion, nsteps, measure_every=None, dt=0.01, amp=2e-2, links=0.0, extra=None):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = make_u1_case(N=N, evolver=evolver, expansion=expansion, dt=dt, amp=amp)
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver=evolver, expansion=expansion, dt=dt, amp=amp, extra=extra)
     if links:
         rng = np.random.default_rng(11)
         f = f.copy()
@@ -249,3 +249,25 @@ def test_lphi4u1_position_verlet_fp32_and_adjoint_guard():
     assert abs(out["fp32"]["aI"] - out["fp64"]["aI"]) <= 1e-7 * out["fp64"]["aI"]
     for x, y in zip(out["fp32"]["energies"], out["fp64"]["energies"]):
         assert abs(x - y) <= 1e-4 * abs(out["fp64"]["energies"][-1])
+
+
+# ---- fixed background for lphi4U1 (fixedbackgroundexpansion.h:21-45) ---------------------------
+
+@pytest.mark.parametrize("evolver", ["VV2", "VV4", "LF", "PV2"])
+def test_lphi4u1_fixed_background(evolver):
+    fb = {"fixedBackground": "true", "H0": 2.0e18, "omegaEoS": 1.0 / 3.0}
+    g, c, meas = run_pair(16, evolver, True, 30, measure_every=7, links=0.05, extra=fb)
+    check_state(g, c, 16)
+    check_meas(meas["gpu"], meas["cpu"])
+
+
+def test_lphi4u1_fixed_background_rejects_the_adjoint():
+    from cosmolattice_b200 import Lattice, _capi
+
+    par, rp, m, f, p, sf = make_u1_case(N=8, extra={"fixedBackground": "true", "H0": 2.0e18})
+    lat = Lattice(m, rp)
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    with pytest.raises(_capi.ClbError):
+        lat.forward(4, 2, [0, 0, 1, 1, 0])  # the adjoint covers the self-consistent expansion
+    lat.close()
