@@ -29,7 +29,7 @@ class NotAnEvolverType(ValueError):
 
 def parse_evolver(value: str) -> int:
     """EvolverType from a name or its integer (evolvertype.h:39-82); LF, VV2-VV10 and PV2-PV10 exist
-    here (position Verlet for the scalar-singlet models)."""
+    here."""
     v = str(value).strip()
     if v in EVOLVERS:
         return EVOLVERS[v]

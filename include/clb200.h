@@ -40,7 +40,7 @@ extern "C" {
 #define CLB_VV10   5
 #define CLB_VV6_2  6
 /* position Verlet, PositionVerlet (positionverlet.h:45-99, positionverletparameters.h:23-46);
-   scalar-singlet models only (lphi4) */
+   every model; the adjoint pair and the tangent-linear form take the VV and LF evolvers */
 #define CLB_PV2    11
 #define CLB_PV4    12
 #define CLB_PV6    13
@@ -83,7 +83,8 @@ typedef struct clb_config {
   int32_t precision;  /* CLB_PREC_*                                                             */
   int32_t path;       /* CLB_PATH_*                                                             */
   int32_t device;     /* CUDA device ordinal                                                    */
-  /* Fixed background (runparameters.h:90-94; with expansion only; scalar-singlet models):
+  /* Fixed background (runparameters.h:90-94; with expansion only; every model, not the adjoint
+   * pair or the tangent-linear form):
    * a(t) = (1 + H0/p (t - t0))^p, aDot = H0 (1 + H0/p (t - t0))^(p - 1),
    * p = 2 / (3 (1 + omega_eos) - 2 alpha)  (FixedBackgroundExpansion, fixedbackgroundexpansion.h:21-50) */
   int32_t fixed_background; /* 0: self-consistent expansion (default), 1: fixed background           */
