@@ -26,6 +26,12 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def c_round(x: float) -> int:
+    """C's round(): halves go away from zero (measurer.h:48-53 counts output steps with it);
+    Python's round() sends them to the even neighbour instead."""
+    return int(np.copysign(np.floor(abs(x) + 0.5), x))
+
+
 class Lattice:
     """One lattice of one model on one GPU (a clb_handle)."""
 
@@ -308,8 +314,8 @@ class Measurer:
         self.model = model
         self.rp = rp
         self.outdir = outdir if outdir is not None else rp.outFn
-        self.outputFreq = max(1, int(round(rp.tOutFreq / rp.dt)))
-        self.spectraFreq = max(1, int(round(rp.tOutInfreq / rp.dt)))  # measurer.h:48-53
+        self.outputFreq = max(1, c_round(rp.tOutFreq / rp.dt))
+        self.spectraFreq = max(1, c_round(rp.tOutInfreq / rp.dt))  # measurer.h:48-53
         self.e0 = None
         self.files: Dict[str, object] = {}
         self.history: List[Dict[str, object]] = []
@@ -470,7 +476,7 @@ def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fu
             measurer.measure_spectra(t, lattice)
         # advance to the next measurement in one device call
         n = min(measurer.outputFreq - (i % measurer.outputFreq), measurer.spectraFreq - (i % measurer.spectraFreq))
-        n_left = int(round((rp.tMax - t) / rp.dt))
+        n_left = c_round((rp.tMax - t) / rp.dt)
         n = max(1, min(n, n_left))
         evolver.evolve_n(n)
         t += n * rp.dt

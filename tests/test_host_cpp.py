@@ -40,6 +40,7 @@ def test_host_rejects_missing_parameters():
 def test_host_matches_python_over_the_abi(tmp_path, evolver, extra):
     from cosmolattice_b200 import Lattice, ParameterParser, RunParameters, lphi4_1f
     from cosmolattice_b200.initializers import device_ic_params
+    from cosmolattice_b200.lattice import c_round
 
     params = dict(PARAMS, evolver=evolver, **extra)
     seed = 7
@@ -56,7 +57,7 @@ def test_host_matches_python_over_the_abi(tmp_path, evolver, extra):
     p, aI, aD = device_ic_params(m, rp, seed=seed)
     lat.generate_state(p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
     lat.initialize(correct_adot=True)
-    out_freq = int(round(rp.tOutFreq / rp.dt))
+    out_freq = c_round(rp.tOutFreq / rp.dt)
     rows_en, rows_sf = [], []
     t, i, e0 = rp.t0, 0, None
     while t < rp.tMax - rp.dt / 2.0:
@@ -67,7 +68,7 @@ def test_host_matches_python_over_the_abi(tmp_path, evolver, extra):
                 e0 = mm["energies"][-1]
             rows_en.append([t] + mm["energies"])
             rows_sf.append([t, mm["aI"], mm["aDotI"], mm["hubble"]])
-        n = max(1, min(out_freq - i % out_freq, int(round((rp.tMax - t) / rp.dt))))
+        n = max(1, min(out_freq - i % out_freq, c_round((rp.tMax - t) / rp.dt)))
         lat.evolve(n)
         t += n * rp.dt
         i += n

@@ -94,3 +94,11 @@ def test_couplings_manager_golden():
         cm.set_effective_charges([1, 1, 2, 3, 4, 5], [1, 2, 3, 4])
     with pytest.raises(CouplingsManager.NotEnoughCouplings):
         cm.set_effective_charges([1, 2, 3, 4, 5], [1, 3, 4])
+
+
+def test_output_cadence_rounds_halves_away_from_zero():
+    """measurer.h:48-53 counts output steps with C's round(): 2.5 steps -> 3, not Python's 2."""
+    from cosmolattice_b200.lattice import c_round
+
+    assert [c_round(x) for x in (2.5, 3.5, 0.5, 2.49, 10.000000000000002, -2.5)] == [3, 4, 1, 2, 10, -3]
+    assert round(2.5) == 2  # the rounding this replaces
