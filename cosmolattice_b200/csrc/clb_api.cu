@@ -1001,7 +1001,8 @@ int clb_evolve(clb_handle *h, int64_t n)
   if (n < 0) return h->fail(CLB_EINVAL, "clb_evolve: negative step count");
   if (n == 0) return CLB_OK;
   h->hist_rows = 0;
-  if (h->cfg.expansion && n > h->hist_cap) {
+  // a fixed background writes no history rows (a(t) is closed-form), so it needs no buffer
+  if (h->cfg.expansion && !h->fb && n > h->hist_cap) {
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e == cudaSuccess && h->d_hist) e = cudaFree(h->d_hist);
     h->d_hist = nullptr;
