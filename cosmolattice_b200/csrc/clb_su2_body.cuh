@@ -251,7 +251,13 @@ template <class T> struct Coef {
   T A, B, B2, G;
 };
 
-// SECT: 0 all components, 1 S, phi, Phi and A (K[0..9]), 2 the SU(2) field (K[10..18]).
+// SECT: 0 all components; 1 S, phi, Phi and A (K[0..9]); 2 the SU(2) field (K[10..18]);
+// 3 S, phi and Phi (K[0..6]); 4 A (K[7..9]).  Each component's kernel is the same expression in
+// every SECT that holds it.
+__host__ __device__ constexpr bool sect_scalars(int sect) { return sect == 0 || sect == 1 || sect == 3; }
+__host__ __device__ constexpr bool sect_u1(int sect) { return sect == 0 || sect == 1 || sect == 4; }
+__host__ __device__ constexpr bool sect_su2(int sect) { return sect == 0 || sect == 2; }
+
 template <int SECT = 0, class S, class T>
 __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP])
 {
@@ -259,7 +265,7 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
   const size_t s = v.s;
   const T A = C.A, B = C.B, B2 = C.B2, G = C.G;
   const T qG = v.qG, qH = v.qH, c4 = v.c4, rfo2 = (T)a.rfo2;
-  if constexpr (SECT != 2) {
+  if constexpr (sect_scalars(SECT)) {
     const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
     K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
     const C2<T> cl = covLapC(v);
@@ -270,6 +276,8 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
     covLapD(v, dl);
     const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
     for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (kdiv(ndD, nD) * v.F(3 + c, s));
+  }
+  if constexpr (sect_u1(SECT)) {
     const D2<T> D0 = v.dbl(s);
     const C2<T> C0 = v.cs(s);
     for (int i = 0; i < 3; ++i) {
@@ -287,7 +295,7 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
       K[7 + i] = G * (lap - grad) - A * J;
     }
   }
-  if constexpr (SECT != 1) {
+  if constexpr (sect_su2(SECT)) {
     const D2<T> Dg = v.dbl(s);
     const T normGrad = kdiv(ipw(kdiv(T(1), v.dx), 3), v.gS) * G;
     const T normSrc = kdiv(T(1), v.dx) * A;
@@ -363,18 +371,19 @@ template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v
   const T t10 = 2 - 2 * v.plaq(1, 0).w, t20 = 2 - 2 * v.plaq(2, 0).w, t21 = 2 - 2 * v.plaq(2, 1).w;
   return c * (t10 + (t20 + t21));
 }
-// momentum sums of the five sectors (FP64) from momentum values q[19]; G1 = 4: the first four
-// sectors only (q[0..9] read), G0 = 4: the SU(2) sector only (q[10..18] read)
+// First momentum component of sector g (0 S, 1 phi, 2 Phi, 3 A, 4 SU(2)); g = 5: one past the last.
+__host__ __device__ constexpr int sector_c0(int g) { return g == 0 ? 0 : g == 1 ? 1 : g == 2 ? 3 : g == 3 ? 7 : g == 4 ? 10 : NP; }
+
+// momentum sums of sectors [G0, G1) (FP64) from momentum values q[19], reading only their
+// components q[sector_c0(G0) .. sector_c0(G1))
 template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s(const R *qs, double out[5])
 {
   double q[NP];
-  for (int c = (G0 == 4 ? 10 : 0); c < (G1 == 4 ? 10 : NP); ++c) q[c] = (double)qs[c];
-  if (G0 == 0) {
-    out[0] = q[0] * q[0];
-    out[1] = q[1] * q[1] + q[2] * q[2];
-    out[2] = ((q[3] * q[3] + q[4] * q[4]) + q[5] * q[5]) + q[6] * q[6];
-    out[3] = (q[7] * q[7] + q[8] * q[8]) + q[9] * q[9];
-  }
+  for (int c = sector_c0(G0); c < sector_c0(G1); ++c) q[c] = (double)qs[c];
+  if (G0 <= 0 && G1 > 0) out[0] = q[0] * q[0];
+  if (G0 <= 1 && G1 > 1) out[1] = q[1] * q[1] + q[2] * q[2];
+  if (G0 <= 2 && G1 > 2) out[2] = ((q[3] * q[3] + q[4] * q[4]) + q[5] * q[5]) + q[6] * q[6];
+  if (G0 <= 3 && G1 > 3) out[3] = (q[7] * q[7] + q[8] * q[8]) + q[9] * q[9];
   if (G1 == 5) {
     double acc = 0;
     for (int i = 0; i < 3; ++i) {
@@ -403,10 +412,12 @@ __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c
 #ifndef CLB_SU2_KICK_MINB_F64
 #define CLB_SU2_KICK_MINB_F64 3
 #endif
-// SECT (as kernels()): 0 every sector in one sweep; 1 and 2 the two halves of a split sweep, run
-// one after the other over the same grid.  Each half updates, reduces and writes only its own
-// components and partial slots (1: sectors S, phi, Phi, A, the field sums but <B^2> of SU(2);
-// 2: the SU(2) sector and its <B^2>), so the halves hold fewer registers than the whole.
+// SECT (as kernels()): 0 every sector in one sweep; 1 and 2 the two halves of a split sweep, or
+// 3, 4 and 2 the three parts of a three-way split, run one after the other over the same grid.
+// Each part updates, reduces and writes only its own components and partial slots (1: sectors S,
+// phi, Phi, A, the field sums but <B^2> of SU(2); 2: the SU(2) sector and its <B^2>; 3: sectors
+// S, phi, Phi, their gradient sums and <V>; 4: sector A and its <B^2>), so the parts hold fewer
+// registers than the whole.  The kicks read the fields only, so the parts' order is free.
 // The halves of a split sweep (192^3, ms per step, same call): FP64 8.17 whole, 6.23 halves at
 // three blocks, 5.73 at four; FP32 4.66 whole, 3.31 halves at four blocks, 3.64 at five.
 #ifndef CLB_SU2_HALF_MINB_F32
@@ -421,8 +432,9 @@ __global__ void __launch_bounds__(128, SECT == 0 ? (sizeof(S) == 4 ? CLB_SU2_KIC
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
            double *__restrict__ partials, const S *__restrict__ ph)
 {
-  constexpr int C0 = SECT == 2 ? 10 : 0, C1 = SECT == 1 ? 10 : NP; // momentum components [C0, C1)
-  constexpr int G0 = SECT == 2 ? 4 : 0, G1 = SECT == 1 ? 4 : 5;    // sectors [G0, G1)
+  constexpr int G0 = SECT == 2 ? 4 : SECT == 4 ? 3 : 0;                   // sectors [G0, G1)
+  constexpr int G1 = SECT == 1 || SECT == 4 ? 4 : SECT == 3 ? 3 : 5;
+  constexpr int C0 = sector_c0(G0), C1 = sector_c0(G1);                    // momentum components [C0, C1)
   __shared__ double smem[(128 / 32) * kRed];
   const State st = *stp;
   double acc[kRed];
@@ -450,22 +462,23 @@ __global__ void __launch_bounds__(128, SECT == 0 ? (sizeof(S) == 4 ? CLB_SU2_KIC
       for (int g = G0; g < G1; ++g) acc[g] += t[g];
     }
     if (RF) {
-      if (SECT != 2) {
+      if (sect_scalars(SECT)) {
         acc[5] += (double)sGrad2(v);
         acc[6] += (double)cGrad2(v);
         acc[7] += (double)dGrad2(v);
-        acc[8] += (double)aB2(v);
       }
-      if (SECT != 1) acc[9] += (double)gB2(v);
-      if (SECT != 2) acc[10] += (double)v.pot();
+      if (sect_u1(SECT)) acc[8] += (double)aB2(v);
+      if (sect_su2(SECT)) acc[9] += (double)gB2(v);
+      if (sect_scalars(SECT)) acc[10] += (double)v.pot();
     }
   }
   if (RF || RP) {
     block_reduce<kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
       for (int k = 0; k < kRed; ++k) {
-        const bool mine = k < 5 || k >= 11 ? ((k < 5 ? k : k - 11) >= G0 && (k < 5 ? k : k - 11) < G1)
-                                           : (k == 9 ? SECT != 1 : SECT != 2);
+        const int g = k < 5 ? k : k >= 11 ? k - 11 : -1; // momentum slot of sector g
+        const bool mine = g >= 0 ? (g >= G0 && g < G1)
+                                 : (k == 8 ? sect_u1(SECT) : k == 9 ? sect_su2(SECT) : sect_scalars(SECT));
         if (mine) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
       }
   }
