@@ -35,8 +35,10 @@ struct SU2Sector {
   // kick sweeps: 0 one sweep, 1 two halves, 2 three parts (CLB_SU2_SPLIT overrides).  su2_create
   // takes three parts for FP64 and halves for FP32, by timing at 192^3 VV2 (ms per step): FP64
   // 8.14 whole, 5.74 halves, 4.93 three parts; FP32 3.98, 2.97, 3.06.  Every form gives the same
-  // state to the last bit.
+  // state to the last bit.  The tangent-linear sweep takes three parts in both (128^3 VV2, ms per
+  // step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
   int split = 2;
+  int tan_split = 2;
   int64_t steps_since_unitarize = 0;
   Params prm{};
   // tangent-linear form: d(state) along the coupling direction tan_cd, active while tangent
@@ -171,7 +173,11 @@ template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, con
                                                                                   u->tan_cd, u->d_tpart))
 #define CLB_SU2T(NK, RF, RP)                                                                                            \
   do {                                                                                                                 \
-    if (NK > 0 && u->split) {                                                                                          \
+    if (NK > 0 && u->tan_split == 2) {                                                                                 \
+      CLB_SU2T1(NK, RF, RP, 3);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 4);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 2);                                                                                        \
+    } else if (NK > 0 && u->tan_split) {                                                                               \
       CLB_SU2T1(NK, RF, RP, 1);                                                                                        \
       CLB_SU2T1(NK, RF, RP, 2);                                                                                        \
     } else {                                                                                                           \
@@ -319,7 +325,7 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
   u->esz = u->fp32 ? sizeof(float) : sizeof(double);
   u->split = u->fp32 ? 1 : 2;
-  if (const char *env = std::getenv("CLB_SU2_SPLIT")) u->split = std::max(0, std::min(2, std::atoi(env)));
+  if (const char *env = std::getenv("CLB_SU2_SPLIT")) u->split = u->tan_split = std::max(0, std::min(2, std::atoi(env)));
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;
   ok = ok && cudaMalloc(&u->p, NP * h->n3 * u->esz) == cudaSuccess;

@@ -673,16 +673,14 @@ __global__ void __launch_bounds__(128)
 template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s_tan(const R *qs, const R *dqs, double out[5])
 {
   double q[NP], d[NP];
-  for (int c = (G0 == 4 ? 10 : 0); c < (G1 == 4 ? 10 : NP); ++c) {
+  for (int c = sector_c0(G0); c < sector_c0(G1); ++c) {
     q[c] = (double)qs[c];
     d[c] = (double)dqs[c];
   }
-  if (G0 == 0) {
-    out[0] = 2 * (q[0] * d[0]);
-    out[1] = 2 * (q[1] * d[1] + q[2] * d[2]);
-    out[2] = 2 * (((q[3] * d[3] + q[4] * d[4]) + q[5] * d[5]) + q[6] * d[6]);
-    out[3] = 2 * ((q[7] * d[7] + q[8] * d[8]) + q[9] * d[9]);
-  }
+  if (G0 <= 0 && G1 > 0) out[0] = 2 * (q[0] * d[0]);
+  if (G0 <= 1 && G1 > 1) out[1] = 2 * (q[1] * d[1] + q[2] * d[2]);
+  if (G0 <= 2 && G1 > 2) out[2] = 2 * (((q[3] * d[3] + q[4] * d[4]) + q[5] * d[5]) + q[6] * d[6]);
+  if (G0 <= 3 && G1 > 3) out[3] = 2 * ((q[7] * d[7] + q[8] * d[8]) + q[9] * d[9]);
   if (G1 == 5) {
     double acc = 0;
     for (int c = 10; c < NP; ++c) acc += 8 * (q[c] * d[c]);
@@ -692,15 +690,16 @@ template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s_
 
 // Tangent kick sweep: k_kick on (p, dp) with kernels and field sums in Tan<S>; partials
 // [block][2 kRed]: the kRed sums of k_kick, then their tangents.
-// SECT as k_kick: 0 whole, 1 and 2 the halves of a split sweep.
+// SECT as k_kick: 0 whole; 1 and 2 the halves, or 3, 4 and 2 the three parts, of a split sweep.
 template <class S, int NK, bool RF, bool RP, int SECT = 0>
 __global__ void __launch_bounds__(128)
     k_kick_tan(const S *__restrict__ f, const S *__restrict__ df, S *__restrict__ p, S *__restrict__ dp, Params a,
                Kick kc, const TState *__restrict__ stp, CoupDot cd, double *__restrict__ partials)
 {
   using T = Tan<S>;
-  constexpr int C0 = SECT == 2 ? 10 : 0, C1 = SECT == 1 ? 10 : NP;
-  constexpr int G0 = SECT == 2 ? 4 : 0, G1 = SECT == 1 ? 4 : 5;
+  constexpr int G0 = SECT == 2 ? 4 : SECT == 4 ? 3 : 0;                   // sectors [G0, G1)
+  constexpr int G1 = SECT == 1 || SECT == 4 ? 4 : SECT == 3 ? 3 : 5;
+  constexpr int C0 = sector_c0(G0), C1 = sector_c0(G1);                    // momentum components [C0, C1)
   __shared__ double smem[(128 / 32) * 2 * kRed];
   const Coef<T> C{T(stp->kA), T(stp->kB), T(stp->kB2), T(stp->kG)};
   double acc[2 * kRed];
@@ -744,23 +743,24 @@ __global__ void __launch_bounds__(128)
         acc[5 + k] += (double)r.v;
         acc[kRed + 5 + k] += (double)r.d;
       };
-      if (SECT != 2) {
+      if (sect_scalars(SECT)) {
         addf(0, sGrad2(v));
         addf(1, cGrad2(v));
         addf(2, dGrad2(v));
-        addf(3, aB2(v));
       }
-      if (SECT != 1) addf(4, gB2(v));
-      if (SECT != 2) addf(5, v.pot());
+      if (sect_u1(SECT)) addf(3, aB2(v));
+      if (sect_su2(SECT)) addf(4, gB2(v));
+      if (sect_scalars(SECT)) addf(5, v.pot());
     }
   }
   if (RF || RP) {
     block_reduce<2 * kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
       for (int k = 0; k < 2 * kRed; ++k) {
-        const int j = k % kRed; // value and tangent slots alike
-        const bool mine = j < 5 || j >= 11 ? ((j < 5 ? j : j - 11) >= G0 && (j < 5 ? j : j - 11) < G1)
-                                           : (j == 9 ? SECT != 1 : SECT != 2);
+        const int j = k % kRed;                          // value and tangent slots alike
+        const int g = j < 5 ? j : j >= 11 ? j - 11 : -1; // momentum slot of sector g
+        const bool mine = g >= 0 ? (g >= G0 && g < G1)
+                                 : (j == 8 ? sect_u1(SECT) : j == 9 ? sect_su2(SECT) : sect_scalars(SECT));
         if (mine) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
       }
   }
