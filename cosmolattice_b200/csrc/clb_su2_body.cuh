@@ -426,9 +426,20 @@ __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c
 #ifndef CLB_SU2_HALF_MINB_F64
 #define CLB_SU2_HALF_MINB_F64 4
 #endif
+// the FP64 three-part sweep's S, phi, Phi part (SECT 3) and A part (SECT 4); four blocks timed
+// best at 192^3 (ms per step): 4.99, against 5.37 with three for SECT 3 and 5.04 with five for SECT 4
+#ifndef CLB_SU2_P3_MINB_F64
+#define CLB_SU2_P3_MINB_F64 CLB_SU2_HALF_MINB_F64
+#endif
+#ifndef CLB_SU2_P4_MINB_F64
+#define CLB_SU2_P4_MINB_F64 CLB_SU2_HALF_MINB_F64
+#endif
 template <class S, int NK, bool RF, bool RP, int SECT = 0>
-__global__ void __launch_bounds__(128, SECT == 0 ? (sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
-                                                  : (sizeof(S) == 4 ? CLB_SU2_HALF_MINB_F32 : CLB_SU2_HALF_MINB_F64))
+__global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
+                                       : sizeof(S) == 4 ? CLB_SU2_HALF_MINB_F32
+                                       : SECT == 3      ? CLB_SU2_P3_MINB_F64
+                                       : SECT == 4      ? CLB_SU2_P4_MINB_F64
+                                                        : CLB_SU2_HALF_MINB_F64)
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
            double *__restrict__ partials, const S *__restrict__ ph)
 {
