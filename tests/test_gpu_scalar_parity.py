@@ -254,3 +254,38 @@ def test_fixed_background_scale_factor_closed_form():
     ad = 0.5 * (1 + 0.5 / p * t) ** (p - 1)
     assert abs(sg["aI"] - a) <= 1e-15 * a
     assert abs(sg["aDotI"] - ad) <= 1e-15 * ad
+
+
+KNOBS = ("CLB_SWEEP_SHAPE", "CLB_SWEEP_XS", "CLB_SWEEP_RING_KB", "CLB_PDL")
+
+
+@pytest.mark.parametrize("precision,tol,atol", [("fp64", 1e-12, 1e-13), ("fp32", 1e-6, 1e-9)])
+def test_sweep_launch_knobs_compute_the_same_step(monkeypatch, precision, tol, atol):
+    # Block shape, x-run (64, 8 and 4 planes per block), ring depth and dependent launch change only
+    # how the sweep is scheduled: the state after 20 VV2 steps matches the default's within the
+    # reordering of the volume sums' block partials (1e-12 FP64; FP32 storage 1e-6).  The FP32
+    # form sums each plane in FP32 first, in an order set by the tile shape, so its a(t) moves in
+    # the 12th digit (2.8e-12 between two shapes), far inside its 1e-7 bar against FP64.
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = make_scalar_case(N=64, evolver="VV2", expansion=True, amp=1e-2)
+    settings = [{}, {"CLB_SWEEP_SHAPE": "0"}, {"CLB_SWEEP_SHAPE": "1"}, {"CLB_SWEEP_SHAPE": "2"},
+                {"CLB_SWEEP_XS": "1"}, {"CLB_SWEEP_XS": "8"}, {"CLB_SWEEP_XS": "16"},
+                {"CLB_SWEEP_RING_KB": "64"}, {"CLB_PDL": "0"}]
+    out = []
+    for env in settings:
+        for k in KNOBS:
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        lat = Lattice(m, rp, precision=precision)
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.evolve(20)
+        out.append(lat.get_state())
+        lat.close()
+    f0, p0, s0 = out[0]
+    for env, (fs, ps, ss) in zip(settings[1:], out[1:]):
+        assert np.abs(fs - f0).max() <= tol * np.abs(f0).max(), env
+        assert np.abs(ps - p0).max() <= tol * np.abs(p0).max(), env
+        assert abs(ss["aI"] - s0["aI"]) <= atol * s0["aI"], env
