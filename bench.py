@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--N", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the shortened runs of the other workloads in the default line")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--config", default="lphi4", choices=["lphi4", "lphi4U1-adjoint", "batched", "lphi4SU2U1"],
                     help="lphi4: the headline 512^3 scalar workload; lphi4U1-adjoint: 128^3 VV4 gauge "
@@ -69,6 +71,16 @@ def workload_params(N, steps):
         "lambda": 1.0, "initial_amplitudes": "5.6964e18", "initial_momenta": "0",
         "fluct_amplitude": 1e-3, "kCutOff": 16.0, "baseSeed": "bench-512",
         "tMax": steps * 0.01,
+    }
+
+
+def headline_config(N, K, world):
+    """The `config` object of the headline line, the same for both arms."""
+    return {
+        "workload": f"lphi4 1 real scalar {N}^3 VV2, self-consistent expansion, {K} steps, FP64",
+        "lattice": N, "evolver": "VV2", "dt": 0.01, "kIR": 64.0 / N, "expansion": True,
+        "l2": "inputs larger than L2 (state %.1f GiB)" % (2 * N ** 3 * 8 / 2 ** 30),
+        "parallelism": "replicas" if world > 1 else "single GPU",
     }
 
 
@@ -685,6 +697,233 @@ def main_su2(args):
     print(json.dumps(line))
 
 
+def run_configs(local, cpu_cores_ok=True):
+    """Shortened but full-size runs of the other workloads, each with its throughput, its roofline
+    on the algorithmic bytes per site-update (state read once and written once per stage) and its
+    clocks, for the default bench line:
+      lphi4_64     lphi4 64^3 kIR = 1 VV2, all 5000 steps on the GPU (FP64, FP32 split) and on the
+                   CPU oracle, with the GPU-vs-CPU differences at the end;
+      batched      384 lphi4 lattices of 32^3-96^3, 200 steps, batched (FP32, FP64) against the same
+                   members one at a time;
+      lphi4U1      128^3 VV4 dt = 0.005 g = 0.5: 100 plain steps (FP64, FP32) and one adjoint
+                   gradient over them with checkpoints every 10 steps, its cost over the forward;
+      lphi4SU2U1   384^3 VV2 dt = 0.005: 20 steps FP64 and FP32 from a device-drawn start state,
+                   with the Gauss ratios at the start and end."""
+    import numpy as np
+    import torch
+
+    from cosmolattice_b200 import MODELS, Lattice, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import device_initial_state, scalar_initial_state, u1_initial_state
+
+    peak, peak_kind = measured_peaks()
+    out = {}
+
+    def roof(bytes_per_step, ms_per_step, what):
+        ach = bytes_per_step / (ms_per_step * 1e-3) / 1e9
+        return {"bound": "hbm", "basis": what, "achieved": round(ach, 1), "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": round(ach / peak, 4)}
+
+    def sf_of(aI, aD):
+        return {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD}
+
+    # ---- lphi4 64^3, 5000 steps ----
+    t0 = time.perf_counter()
+    par = ParameterParser(params={"N": 64, "kIR": 1.0, "dt": 0.01, "evolver": "VV2", "expansion": "true",
+                                  "lambda": 1.0, "initial_amplitudes": "5.6964e18", "initial_momenta": "0",
+                                  "fluct_amplitude": 1e-3, "kCutOff": 16.0, "baseSeed": "cfg0"})
+    rp = RunParameters(par)
+    m = MODELS["lphi4_1f"](par, rp)
+    f, p, aI, aD = scalar_initial_state(m, rp)
+    K0 = 5000
+    res = {}
+    for prec in ("fp64", "fp32"):
+        lat = Lattice(m, rp, precision=prec, device=local)
+        lat.set_state(f, p, sf_of(aI, aD))
+        lat.initialize()
+        lat.sync()
+        e0 = lat.measure(1.0)["energies"][-1]
+        with ClockSampler(local) as clk:
+            lat.evolve(K0)
+        ms = lat.last_evolve_ms()
+        lat.sync()
+        res[prec] = (ms, lat.measure(e0), lat.get_state(), clk.summary())
+        lat.close()
+    from oracle.oracle import OracleLattice, num_threads
+
+    o = OracleLattice(m, rp)
+    o.set_state(f, p, sf_of(aI, aD))
+    o.initialize()
+    o.sync()
+    e0c = o.measure(1.0)["energies"][-1]
+    tc = time.perf_counter()
+    o.evolve(K0)
+    cpu_s = time.perf_counter() - tc
+    o.sync()
+    mc, sc = o.measure(e0c), o.get_state()
+    o.close()
+    sites = 64 ** 3
+    ms64, m64, s64, clk64 = res["fp64"]
+    ms32, m32 = res["fp32"][0], res["fp32"][1]
+    fl = float(np.abs(s64[0] - sc[0]).max() / np.abs(sc[0] - sc[0].mean()).max())
+    out["lphi4_64"] = {
+        "workload": "lphi4 64^3 kIR=1 dt=0.01 VV2, expansion, amplitude 1e-3, 5000 steps",
+        "fp64": {"value": sites * K0 / (ms64 * 1e-3), "ms_per_step": ms64 / K0,
+                 "roofline": roof(32 * sites, ms64 / K0, "32 B/site/step FP64 (state in L2: above HBM is possible)")},
+        "fp32": {"value": sites * K0 / (ms32 * 1e-3), "ms_per_step": ms32 / K0},
+        "cpu": {"value": sites * K0 / cpu_s, "seconds": cpu_s, "cores": num_threads(), "kind": "port"},
+        "gpu_over_cpu": (sites * K0 / (ms64 * 1e-3)) / (sites * K0 / cpu_s),
+        "gpu_vs_cpu_after_5000_steps": {
+            "a_rel": abs(s64[2]["aI"] - sc[2]["aI"]) / sc[2]["aI"],
+            "friedmann_abs": abs(m64["friedmann"][0] - mc["friedmann"][0]),
+            "energy_rel": max(abs(x - y) / abs(y) for x, y in zip(m64["energies"], mc["energies"]) if y != 0),
+            "field_rel_to_fluctuations": fl},
+        "fp32_vs_fp64": {"friedmann_abs": abs(m32["friedmann"][0] - m64["friedmann"][0]),
+                         "energy_rel": max(abs(x - y) / abs(y) for x, y in zip(m32["energies"], m64["energies"]) if y != 0)},
+        "clocks": clk64, "seconds": time.perf_counter() - t0}
+
+    # ---- batched ensemble: 384 members, 200 steps ----
+    from cosmolattice_b200.batch import LatticeBatch
+
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(20261203)
+    cases = []
+    for i in range(384):
+        N = int(rng.choice([32, 48, 64, 96]))
+        lam = float(np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+        amp = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2))))
+        par = ParameterParser(params={
+            "N": N, "kIR": 1.0, "dt": 0.01, "evolver": "VV2", "expansion": "true", "lambda": 1.0,
+            "lambda_prog": lam, "initial_amplitudes": "5.6964e18", "initial_momenta": "0",
+            "fluct_amplitude": amp, "kCutOff": N / 4.0, "baseSeed": f"ens-{i}"})
+        rpi = RunParameters(par)
+        mi = MODELS["lphi4_1f"](par, rpi)
+        fi, pi_, a_, d_ = scalar_initial_state(mi, rpi)
+        cases.append((mi, rpi, fi, pi_, sf_of(a_, d_)))
+    bsites = sum(c[1].N ** 3 for c in cases)
+    KB = 200
+    bres = {}
+    for prec in ("fp32", "fp64"):
+        bt = LatticeBatch([(c[0], c[1]) for c in cases], precision=prec, device=local)
+        for i, c in enumerate(cases):
+            bt.set_state(i, c[2], c[3], c[4])
+        bt.initialize()
+        bt.evolve(5)
+        with ClockSampler(local) as clk:
+            bt.evolve(KB)
+        bres[prec] = (bt.last_evolve_ms(), clk.summary(), bt.tuning())
+        bt.close()
+    seq_ms = 0.0
+    for c in cases:
+        lat = Lattice(c[0], c[1], precision="fp32", device=local)
+        lat.set_state(c[2], c[3], c[4])
+        lat.initialize()
+        lat.evolve(3)
+        lat.evolve(KB)
+        seq_ms += lat.last_evolve_ms()
+        lat.close()
+    b32, b64 = bres["fp32"][0], bres["fp64"][0]
+    out["batched"] = {
+        "workload": "384 lphi4 lattices, N in {32,48,64,96}, lambda log-uniform [0.5,2], amplitude log-uniform "
+                    "[1e-4,1e-2], VV2 dt=0.01, expansion, 200 steps",
+        "total_sites": bsites,
+        "fp32": {"value": bsites * KB / (b32 * 1e-3), "ms_per_step": b32 / KB,
+                 "roofline": roof(16 * bsites, b32 / KB, "16 B/site/step FP32 storage, whole step")},
+        "fp64": {"value": bsites * KB / (b64 * 1e-3), "ms_per_step": b64 / KB,
+                 "roofline": roof(32 * bsites, b64 / KB, "32 B/site/step FP64, whole step")},
+        "one_at_a_time_fp32": {"value": bsites * KB / (seq_ms * 1e-3), "ms_per_step": seq_ms / KB},
+        "batched_speedup": seq_ms / b32,
+        "tuning": bres["fp32"][2], "clocks": bres["fp32"][1], "seconds": time.perf_counter() - t0}
+    del cases
+
+    # ---- lphi4U1 128^3 VV4: 100 steps and one gradient (K = 10) ----
+    from cosmolattice_b200.adjoint import GAUGE_FRACTION, u1_gradients
+
+    t0 = time.perf_counter()
+    par = ParameterParser(params={
+        "N": 128, "kIR": 1.0, "dt": 0.005, "evolver": "VV4", "expansion": "true", "lambda": 1.0, "lambda_prog": 1.0,
+        "cmplx_field_initial_norm": "5.6964e18", "cmplx_momentum_initial_norm": "0", "gU1s": 0.5,
+        "CSU1_charges": 1, "fluct_amplitude": 1e-3, "kCutOff": 32.0, "baseSeed": "cfg3"})
+    rp = RunParameters(par)
+    m = MODELS["lphi4U1"](par, rp)
+    state = u1_initial_state(m, rp)
+    f, p, aI, aD = state
+    K3 = 100
+    ures = {}
+    for prec in ("fp64", "fp32"):
+        lat = Lattice(m, rp, precision=prec, device=local)
+        lat.set_state(f, p, sf_of(aI, aD))
+        lat.initialize()
+        lat.evolve(3)
+        with ClockSampler(local) as clk:
+            lat.evolve(K3)
+        ures[prec] = (lat.last_evolve_ms(), clk.summary())
+        lat.close()
+    lat = Lattice(m, rp, device=local)
+    u1_gradients(m, rp, K3, 10, GAUGE_FRACTION, params=(), lattice=lat, state=state)  # warm
+    O, _, rec = u1_gradients(m, rp, K3, 10, GAUGE_FRACTION, params=(), lattice=lat, state=state)
+    lat.close()
+    sites = 128 ** 3
+    u64, u32 = ures["fp64"][0], ures["fp32"][0]
+    grad_s = rec["forward_s"] + rec["backward_s"]
+    out["lphi4U1"] = {
+        "workload": "lphi4U1 128^3 VV4 dt=0.005 g=0.5 lambda=1 amplitude 1e-3, expansion, 100 steps; "
+                    "gradient of the final gauge-energy fraction, checkpoints every 10 steps",
+        "fp64": {"value": sites * K3 / (u64 * 1e-3), "ms_per_step": u64 / K3,
+                 "roofline": roof(3 * 160 * sites, u64 / K3, "160 B/site/stage FP64, 3 stages")},
+        "fp32": {"value": sites * K3 / (u32 * 1e-3), "ms_per_step": u32 / K3, "speedup_vs_fp64": u64 / u32,
+                 "roofline": roof(3 * 80 * sites, u32 / K3, "80 B/site/stage FP32 storage, 3 stages")},
+        "gradient": {"observable": O, "forward_s": rec["forward_s"], "backward_s": rec["backward_s"],
+                     "gradient_over_plain_forward": grad_s * 1e3 / u64},
+        "clocks": ures["fp64"][1], "seconds": time.perf_counter() - t0}
+    del state, f, p
+
+    # ---- lphi4SU2U1 384^3 VV2, 20 steps ----
+    t0 = time.perf_counter()
+    par = ParameterParser(params={
+        "N": 384, "kIR": 1.0, "dt": 0.005, "evolver": "VV2", "expansion": "true", "lambda": 1.0, "qG": 50, "qH": 50,
+        "initial_amplitudes": 0.0, "initial_momenta": 0.0, "cmplx_field_initial_norm": 0.0,
+        "cmplx_momentum_initial_norm": 0.0, "SU2Doublet_initial_norm": "5.25151e18",
+        "SU2Doublet_initial_momenta_norm": 0.0, "gU1s": 0.35, "gSU2s": 0.6, "fluct_amplitude": 1e-3,
+        "kCutOff": 96.0, "baseSeed": "cfg4"})
+    rp = RunParameters(par)
+    m = MODELS["lphi4SU2U1"](par, rp)
+    K4 = 20
+    sres = {}
+    for prec in ("fp64", "fp32"):
+        lat = Lattice(m, rp, precision=prec, device=local)
+        device_initial_state(lat, m, rp, seed=4)
+        lat.initialize()
+        lat.sync()
+        m0 = lat.measure(1.0)
+        lat.evolve(2)
+        with ClockSampler(local) as clk:
+            lat.evolve(K4)
+        ms = lat.last_evolve_ms()
+        lat.sync()
+        m1 = lat.measure(m0["energies"][-1])
+        sres[prec] = (ms, m0, m1, clk.summary())
+        lat.close()
+    torch.cuda.empty_cache()
+    sites = 384 ** 3
+    s64, s32 = sres["fp64"], sres["fp32"]
+    out["lphi4SU2U1"] = {
+        "workload": "lphi4SU2U1 384^3 VV2 dt=0.005 gSU2=0.6 gU1=0.35 lambda=1 qG=qH=50, expansion, 20 steps "
+                    "(device-drawn start state)",
+        "fp64": {"value": sites * K4 / (s64[0] * 1e-3), "ms_per_step": s64[0] / K4,
+                 "roofline": roof(656 * sites, s64[0] / K4, "656 B/site/step FP64 (41 reals read and written)")},
+        "fp32": {"value": sites * K4 / (s32[0] * 1e-3), "ms_per_step": s32[0] / K4, "speedup_vs_fp64": s64[0] / s32[0],
+                 "roofline": roof(328 * sites, s32[0] / K4, "328 B/site/step FP32 storage")},
+        "gauss_su2": {"fp64": [s64[1]["gauss_su2"][0], s64[2]["gauss_su2"][0]],
+                      "fp32": [s32[1]["gauss_su2"][0], s32[2]["gauss_su2"][0]], "order": "start, end"},
+        "gauss_u1": {"fp64": [s64[1]["gauss_u1"][0], s64[2]["gauss_u1"][0]],
+                     "fp32": [s32[1]["gauss_u1"][0], s32[2]["gauss_u1"][0]], "order": "start, end"},
+        "fp32_vs_fp64": {"a_rel": abs(s32[2]["aI"] - s64[2]["aI"]) / s64[2]["aI"],
+                         "energy_diff_over_etot": max(abs(x - y) for x, y in zip(s32[2]["energies"], s64[2]["energies"]))
+                         / abs(s64[2]["energies"][-1])},
+        "clocks": s64[3], "seconds": time.perf_counter() - t0}
+    return out
+
+
 def main():
     args = parse_args()
     if args.config == "lphi4SU2U1":
@@ -744,6 +983,10 @@ def main():
         cpu = cpu_baseline(rp, model, fields, momenta, sf, args.cpu_seconds)
     if rank != 0:
         return
+    configs = None
+    if world == 1 and not args.no_configs:
+        del fields, momenta
+        configs = run_configs(local)
     peak, peak_kind = measured_peaks()
     f64, f32 = r64["m1"], r32["m1"]
     launches = sum(v["launches"] for v in r64["stats"].values())
@@ -760,12 +1003,7 @@ def main():
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded Gaussian vacuum fluctuations, BASELINE recipe)",
-        "config": {
-            "workload": f"lphi4 1 real scalar {N}^3 VV2, self-consistent expansion, {K} steps, FP64 fused path",
-            "lattice": N, "evolver": "VV2", "dt": 0.01, "kIR": 64.0 / N, "expansion": True,
-            "l2": "inputs larger than L2 (state %.1f GiB)" % (2 * sites * 8 / 2 ** 30),
-            "parallelism": "replicas" if world > 1 else "single GPU",
-        },
+        "config": headline_config(N, K, world),
         "roofline": roofline(r64["stats"], N, "fp64", peak, peak_kind),
         "ms_per_step_kernel_events_pass": r64["ms_prof"] / K,
         "fp64_reference_order": {"ms_per_step": tref, "value": world * sites / (tref * 1e-3),
@@ -798,6 +1036,7 @@ def main():
         "clocks_mixed": r32["clocks"],
         "cpu_baseline": cpu,
         "history_rows": r64["hist_rows"],
+        "configs": configs,
     }
     print(json.dumps(line))
 
@@ -821,8 +1060,7 @@ def main_reference(args):
         "value": cpu["value"], "unit": "site-updates/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": N ** 3 / cpu["value"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian vacuum fluctuations, BASELINE recipe)",
-        "config": {"workload": f"lphi4 1 real scalar {N}^3 VV2, self-consistent expansion, {K} steps, FP64",
-                   "lattice": N, "evolver": "VV2"},
+        "config": headline_config(N, K, world),
         "impl": "reference",
         "cpu_baseline": cpu,
         "e2e": {"value": cpu["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

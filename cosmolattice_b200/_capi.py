@@ -9,7 +9,11 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libclb200.so")
+# The library built with the scalar-singlet model header named by CLB200_SCALAR_MODEL (lib/<name>/),
+# or the package library (lphi4).
+_SCALAR_MODEL = os.environ.get("CLB200_SCALAR_MODEL", "lphi4")
+LIB_PATH = (os.path.join(_HERE, "lib", "libclb200.so") if _SCALAR_MODEL == "lphi4"
+            else os.path.join(_HERE, "lib", _SCALAR_MODEL, "libclb200.so"))
 
 # status codes
 CLB_OK = 0
@@ -18,6 +22,7 @@ CLB_ECUDA = -2
 CLB_ENOMEM = -3
 CLB_ENONFINITE = -4
 CLB_ETIMEOUT = -5
+CLB_INIT_RESTART = 2
 CLB_EUNSUPPORTED = -6
 CLB_ESTATE = -7
 

@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
   // by dx^2 and by m_A^-1 are multiplies by reciprocals
   const double inv_r2 = 1.0 / g.r2, cJ = g.kA * g.J0 * inv_r2, cD = g.AD * g.inv_n3 * (2.0 * a.gQ / a.dx);
   const double two_dx = 2.0 / a.dx, dJ = g.dkA * g.J0 * a.gQ;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+  for_sites(a.N, n3, a.order, [&](size_t s) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
     // the JVP direction at a site: M^{-1} (hA lambda_A + hB lambda_B)
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
       qbar[c * n3 + s] = qb[c];
       pbar_out[c * n3 + s] = pb[c];
     }
-  }
+  });
   block_reduce<kAdjSlots, 256>(acc, smem);
   if (threadIdx.x == 0) {
 #pragma unroll

@@ -110,10 +110,13 @@ void setup_geometry(clb_handle *h, int blocks_per_sm)
   const int N = h->N;
   const int gx = (N + h->bz - 1) / h->bz, gy = (N + h->by - 1) / h->by;
   // Many short x-runs (about 32 planes) beat few long ones: a block's plane rate is bounded by its
-  // own pipeline, so throughput comes from many blocks cycling through the SMs.
-  (void)blocks_per_sm;
+  // own pipeline, so throughput comes from many blocks cycling through the SMs.  A small lattice
+  // has few (z, y) tiles (64^3: 8), so its runs are shortened, down to one plane, until the grid
+  // fills two waves of resident blocks (the extra halo planes then come from L2).
   int xs = std::max(1, (N + kPlanesPerBlock - 1) / kPlanesPerBlock);
-  xs = std::max(1, std::min(xs, std::max(1, N / 4)));
+  const int waves = 2 * 148 * std::max(1, blocks_per_sm);
+  if ((long long)gx * gy * xs < waves) xs = std::max(xs, std::min(N, (waves + gx * gy - 1) / (gx * gy)));
+  xs = std::max(1, std::min(xs, N));
   if (const char *env = std::getenv("CLB_SWEEP_XS")) xs = std::max(1, std::min(N, std::atoi(env)));
   int LX = (N + xs - 1) / xs;
   xs = (N + LX - 1) / LX;
@@ -233,8 +236,8 @@ template <class R, int NS> struct Launch {
   {
     CLB_LAUNCH(h, K_MEASURE,
                k_measure_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->pd,
-                                                                        h->sa.inv_dx2, h->sa.c0_quarter,
-                                                                        h->sa.q_half, am, h->d_st, h->rs, h->d_part));
+                                                                        h->sa.inv_dx2, h->sa.mc, am, h->d_st,
+                                                                        h->rs, h->d_part));
     CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeasSlots><<<1, 256, 0, h->stream>>>(h->d_part, kElemBlocks, h->d_sums));
   }
 };
@@ -623,8 +626,8 @@ template <class R, int NS> struct Init {
   {
     using L = Launch<R, NS>;
     uint32_t fl = T_STORE_ALL;
-    if (h->cfg.expansion && correct && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
-    if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
+    if (h->cfg.expansion && correct == 1 && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
+    if (h->cfg.expansion && h->cfg.evolver == CLB_LF && correct != CLB_INIT_RESTART) fl |= T_LF_CTOR;
     tail(h, fl, L::reduce_fields(h, true));
   }
 };
@@ -750,10 +753,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   ScalarArgs &a = h->sa;
   a.N = h->N;
   a.inv_dx2 = 1.0 / (cfg->dx * cfg->dx);
-  a.c0 = md->couplings[0];
-  a.q = md->couplings[1];
-  a.c0_quarter = 0.25 * md->couplings[0];
-  a.q_half = 0.5 * md->couplings[1];
+  a.mc = ScalarModel::couplings(md->couplings);
   // ring depth: as many plane stages as fit in ~48 KiB, at least 3 (planes x, x+1 and one in flight)
   // sweep shape: default per storage type and field count, CLB_SWEEP_SHAPE=0/1/2 overrides (one field)
   h->shape = (h->NS == 1) ? (h->fp32 ? kDefaultShapeFP32 : kDefaultShapeFP64) : 0;
@@ -778,11 +778,11 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   w.LX = a.LX;
   w.S = h->S;
   w.tries = kWaitTries;
+  // Lowers the bound of the sweeps' tile-load waits, so a test can make a wait run out and check
+  // that the call reports CLB_ETIMEOUT (0: every wait gives up at once).
+  if (const char *env = std::getenv("CLB_WAIT_TRIES")) w.tries = (uint32_t)std::strtoul(env, nullptr, 10);
   w.inv_dx2 = a.inv_dx2;
-  w.c0 = a.c0;
-  w.q = a.q;
-  w.c0_quarter = a.c0_quarter;
-  w.q_half = a.q_half;
+  w.mc = a.mc;
   const double fm = md->fStar / md->MPl;
   h->sp = SFParams{md->alpha, fm * fm, cfg->dt, 1.0 / (double)h->n3};
   h->part_rows = (size_t)std::max(h->sweep_blocks, kElemBlocks);
@@ -981,13 +981,19 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
   if (!h) return CLB_EINVAL;
   if (!h->has_state) return h->fail(CLB_ESTATE, "clb_initialize: no state uploaded");
   h->fb_t = h->cfg.t0;
+  if (correct_adot < 0 || correct_adot > CLB_INIT_RESTART)
+    return h->fail(CLB_EINVAL, "clb_initialize: mode must be 0, 1 or CLB_INIT_RESTART");
+  if (correct_adot == CLB_INIT_RESTART && h->fb)
+    return h->fail(CLB_EUNSUPPORTED, "clb_initialize: a restart with a fixed background is not supported");
   if (h->u1 || h->su2) {
     const int r = h->u1 ? u1_initialize(h, correct_adot) : su2_initialize(h, correct_adot);
     if (r == CLB_OK) h->initialized = true;
     return r;
   }
+  if (correct_adot == CLB_INIT_RESTART && h->fb)
+    return h->fail(CLB_EUNSUPPORTED, "clb_initialize: a restart with a fixed background is not supported");
   dispatch<Init>(h, (int)correct_adot);
-  h->synced = true;
+  h->synced = !(correct_adot == CLB_INIT_RESTART && h->cfg.evolver == CLB_LF); // leapfrog.h:30-31
   h->fb_t = h->cfg.t0;
   int r = sync_and_check(h, "clb_initialize");
   if (r == CLB_OK) h->initialized = true;

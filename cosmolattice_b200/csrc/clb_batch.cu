@@ -396,8 +396,7 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
     L.N = N;
     L.off = off;
     L.inv_dx2 = 1.0 / (cfgs[i].dx * cfgs[i].dx);
-    L.c0 = mds[i].couplings[0];
-    L.c0q = 0.25 * mds[i].couplings[0];
+    L.mc = ScalarModel::couplings(mds[i].couplings);
     const double fm = mds[i].fStar / mds[i].MPl;
     L.sp = SFParams{mds[i].alpha, fm * fm, c0.dt, 1.0 / ((double)N * N * N)};
     const long long n3 = (long long)N * N * N;

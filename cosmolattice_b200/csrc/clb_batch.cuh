@@ -1,7 +1,8 @@
 // clb_batch.cuh - sm_100a kernels of the batched lphi4 ensemble (many independent lattices).
 //
-// Every member is one real scalar with V = c0/4 phi^4 (models/lphi4.h:154-206 with the daughter
-// field removed) on its own N^3 periodic lattice; the members share dt, evolver and expansion
+// Every member is one real scalar singlet of the model header the library is built with (lphi4:
+// V = c0/4 phi^4, models/lphi4.h:154-206 with the daughter field removed) on its own N^3 periodic
+// lattice; the members share dt, evolver and expansion
 // mode and differ in N, dx, c0, initial state and scale factor.  One launch of k_batch_sweep
 // advances all members by one fused VV stage (the same drift + two-kick sweep as the single
 // lattice path: velocityverlet.h:51-114, 129-196); k_batch_tail then updates each member's scale
@@ -22,7 +23,8 @@ struct BatchLat {
   int N, gx, gy, gz, LX; // sweep grid of this member: (z, y) tiles of BZ x BY, x runs of LX planes
   int first_block, nblocks;
   long long off;         // element offset of the member's arrays
-  double inv_dx2, c0, c0q;
+  double inv_dx2;
+  ModelCouplings mc; // the member's couplings in the model header's form
   SFParams sp;
 };
 
@@ -84,10 +86,10 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
 
   // the member's reference step (split form) and its coefficients
   RefStep<1> rf{};
-  Lphi4SplitCoef spc{};
+  ModelFluct spc{};
   if constexpr (SPLIT) {
-    rf = ref_step<1>(st, rs, DRIFT, KICK, dtw_d, h1, h2, lt.c0, 0.0);
-    spc = Lphi4SplitCoef::make(rf.phi[0], lt.c0);
+    rf = ref_step<1>(st, rs, DRIFT, KICK, dtw_d, h1, h2, lt.mc);
+    spc = ModelFluct::make(rf.phi[0], lt.mc);
     if ((DRIFT || KICK) && local == 0 && tid == 0) {
       st->ref_phi[rs ^ 1][0] = rf.phi[0];
       st->ref_pi[rs ^ 1][0] = rf.pi_next[0];
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
   }
   const R pd = DRIFT ? (R)st->drift_p : R(0), dtw = DRIFT ? (R)dtw_d : R(0);
   const R KA = KICK ? (R)st->kick_A : R(0), KB = KICK ? (R)st->kick_B : R(0);
-  const R inv_dx2 = (R)lt.inv_dx2, c0 = (R)lt.c0, c0q = (R)lt.c0q, two = R(2);
+  const R inv_dx2 = (R)lt.inv_dx2, two = R(2);
   const float h1f = (float)h1, h2f = (float)h2;
 
   auto sidx = [&](int x, int yy, int zz) -> size_t { return ((size_t)x * N + yy) * N + zz; };
@@ -189,7 +191,14 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
             const float zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : tile[b][ty + 1][zt];
             if (KICK) {
               const float lap = inv_dx2 * ((((nxt[k] + prev[k]) - 2.f * c) + ((ynb + ymb) - 2.f * c)) + ((znb + zmb) - 2.f * c));
-              const float K = KA * lap - KB * spc.ddV(c);
+              float ddv;
+              if constexpr (kModelFluct) {
+                ddv = spc.dV(c);
+              } else {
+                const double cd[1] = {rf.phi[0] + (double)c};
+                ddv = (float)(SPot<double, 1>::dV(0, cd, lt.mc) - rf.dV[0]);
+              }
+              const float K = KA * lap - KB * ddv;
               const float pm = fmaf(h1f, K, piC[k]);
               outp[k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
               if (RED & 1) {
@@ -203,7 +212,12 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
             if (RED & 2) {
               const float gx = nxt[k] - c, gy = ynb - c, gz = znb - c;
               s_g2 += (gx * gx + gy * gy + gz * gz) * inv_dx2;
-              s_dv += spc.dVpot(c);
+              if constexpr (kModelFluct) {
+                s_dv += spc.V(c);
+              } else {
+                const double cd[1] = {rf.phi[0] + (double)c};
+                s_dv += (float)(SPot<double, 1>::V(cd, lt.mc) - rf.V);
+              }
             }
           }
           acc_p += (double)s_p;
@@ -224,7 +238,7 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
               const R tzv = A::sub(A::add(znb, zmb), A::mul(two, c));
               const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
               const R cv[1] = {c};
-              const R K = A::sub(A::mul(KA, lap), A::mul(KB, Lphi4<R, 1>::dV(0, cv, c0, R(0))));
+              const R K = A::sub(A::mul(KA, lap), A::mul(KB, SPot<R, 1>::dV(0, cv, lt.mc)));
               const KickOut<R> ko = kick_val<R>(piC[k], K, h1, h2);
               outp[k] = ko.next;
               if (RED & 1) acc_pi2 += ko.mid * ko.mid;
@@ -235,7 +249,7 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
               const R gx = A::sub(nxt[k], c), gy = A::sub(ynb, c), gz = A::sub(znb, c);
               acc_g2 += (double)A::mul(A::add(A::add(A::mul(gx, gx), A::mul(gy, gy)), A::mul(gz, gz)), inv_dx2);
               const R cv[1] = {c};
-              acc_v += (double)Lphi4<R, 1>::V(cv, c0q, R(0));
+              acc_v += (double)SPot<R, 1>::V(cv, lt.mc);
             }
           }
         }
@@ -337,7 +351,8 @@ __global__ void __launch_bounds__(256)
     acc[3] += c * c;
     acc[4] += m;
     acc[5] += m * m;
-    acc[6] += lt.c0q * c * c * c * c;
+    const double cv[1] = {c};
+    acc[6] += SPot<double, 1>::V(cv, lt.mc);
   }
   block_reduce<7, 256>(acc, smem);
   if (threadIdx.x == 0)

@@ -1,19 +1,25 @@
 // clb_noalloc.cu - volume averages of caller-owned device lattices with no device allocation.
 //
-// Some callers cannot call cudaMalloc: a host runtime that owns the whole device memory pool,
-// code running while a CUDA graph is being captured (an allocation would break the capture), or
-// an embedding that forbids allocation after start-up.  clb_scalar_averages_noalloc serves them:
-// the caller passes device pointers for the inputs and the output, and the per-block partial sums
-// of the reduction live in the file-scope array below instead of a cudaMalloc'd buffer.
+// Some callers cannot call cudaMalloc: a host runtime that owns the whole device memory pool and
+// hands out no more, or an embedding that forbids device allocation after start-up (a long-running
+// service with a fixed memory budget).  clb_scalar_averages_noalloc serves them: the caller passes
+// device pointers for the inputs and the output, and the per-block partial sums of the reduction
+// live in the file-scope array below instead of a cudaMalloc'd buffer.
 //
 // The array is sized for kNoAllocMaxRows block rows (192 KiB); every GPU that loads the library
 // holds it until the process exits.  All calls share it and it keeps the last call's contents;
 // each call's blocks overwrite exactly the rows the same call then sums, so nothing has to start
 // at zero.  Calls that overlap on the GPU (other streams, other host threads) race on the array.
+//
+// Set-up: the first call on a device (more exactly, in a device context) looks up the array's
+// device address with cudaGetSymbolAddress, with that device current, and caches it beside the
+// context it belongs to; a new context on the device (after cudaDeviceReset) is looked up again.
 
 #include "../../include/clb200.h"
 #include "clb_internal.cuh"
 #include "clb_scalar.cuh"
+
+#include <cuda.h>
 
 #include <algorithm>
 #include <mutex>
@@ -38,6 +44,22 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxRows * kRe
 
 std::mutex g_mu;
 double *g_dev_ptr[kNoAllocMaxDevices] = {};
+CUcontext g_dev_ctx[kNoAllocMaxDevices] = {};
+
+// The driver's cuCtxGetCurrent, through the runtime's entry-point query (no -lcuda link).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+CtxGetCurrentFn ctx_get_current()
+{
+  static CtxGetCurrentFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  return fn;
+}
 
 // Fixed-order sum of the block rows, divided by N^3, into the caller's three outputs.
 __global__ void __launch_bounds__(256)
@@ -53,7 +75,7 @@ __global__ void __launch_bounds__(256)
     for (int k = 0; k < kRedSlots; ++k) out[k] = v[k] * inv_n3;
 }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device, looked up once per device context.
 cudaError_t scratch_on_current_device(double **ptr)
 {
   int dev = 0;
@@ -61,11 +83,22 @@ cudaError_t scratch_on_current_device(double **ptr)
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_mu);
+  // cudaGetSymbolAddress makes the device's primary context current if none is; the context is
+  // read after it, so the cache entry names the context the address belongs to.
+  if (g_dev_ptr[dev]) {
+    CUcontext ctx = nullptr;
+    CtxGetCurrentFn get = ctx_get_current();
+    if (!get || get(&ctx) != CUDA_SUCCESS || ctx != g_dev_ctx[dev]) g_dev_ptr[dev] = nullptr;
+  }
   if (!g_dev_ptr[dev]) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess) return e;
+    CUcontext ctx = nullptr;
+    CtxGetCurrentFn get = ctx_get_current();
+    if (get) (void)get(&ctx);
     g_dev_ptr[dev] = static_cast<double *>(p);
+    g_dev_ctx[dev] = ctx;
   }
   *ptr = g_dev_ptr[dev];
   return cudaSuccess;
@@ -101,8 +134,16 @@ extern "C" int clb_scalar_averages_noalloc(const double *d_fields, const double 
     set_global_error("clb_scalar_averages_noalloc: dx must be positive");
     return CLB_EINVAL;
   }
+  // A launch error left by earlier work in the process stays with its owner: report it without
+  // clearing it, so the error that the launches below return is this call's own.
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    set_global_error(std::string("clb_scalar_averages_noalloc: an earlier CUDA error is pending: ") +
+                     cudaGetErrorString(e));
+    return CLB_ECUDA;
+  }
   double *partials = nullptr;
-  cudaError_t e = scratch_on_current_device(&partials);
+  e = scratch_on_current_device(&partials);
   if (e != cudaSuccess) {
     set_global_error(std::string("clb_scalar_averages_noalloc: scratch address: ") + cudaGetErrorString(e));
     return CLB_ECUDA;
@@ -116,10 +157,8 @@ extern "C" int clb_scalar_averages_noalloc(const double *d_fields, const double 
   a.N = N;
   a.LX = LX;
   a.inv_dx2 = 1.0 / (dx * dx);
-  a.c0 = c0;
-  a.q = q;
-  a.c0_quarter = 0.25 * c0;
-  a.q_half = 0.5 * q;
+  const double coup[CLB_MAX_COUPLINGS] = {c0, q};
+  a.mc = ScalarModel::couplings(coup);
   const dim3 grid(gx, gy, xs);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n_scalars == 1)

@@ -13,49 +13,46 @@
 
 #include "clb_internal.cuh"
 
+#ifndef CLB_SCALAR_MODEL
+#define CLB_SCALAR_MODEL_HEADER "models/lphi4.h"
+#define CLB_SCALAR_MODEL lphi4
+#endif
+#include CLB_SCALAR_MODEL_HEADER
+
 namespace clb {
+
+using ScalarModel = clb_models::CLB_SCALAR_MODEL;
+using ModelCouplings = ScalarModel::Couplings;
 
 struct ScalarArgs {
   int N;
   int LX;           // x planes per block
   double inv_dx2;   // 1 / (dx dx)                      (gaugederivatives.h:38)
-  double c0;        // lphi4 quartic coefficient (1 in the reference header)
-  double q;         // lphi4 interaction q
-  double c0_quarter;// 0.25 * c0                         (lphi4.h:163)
-  double q_half;    // 0.5 * q                           (lphi4.h:176)
+  ModelCouplings mc; // the model header's couplings (models/lphi4.h: c0, q, c0/4, q/2)
   double dtw;       // dt * w of the drift              (velocityverlet.h:183)
   double h1;        // first kick weight  (w dt / 2)    (velocityverlet.h:131)
   double h2;        // second kick weight (w' dt / 2), 0 when the sweep ends on a half kick
 };
 
-// ---- lphi4 potential (models/lphi4.h:154-226) in the pinned rounding order -------------------
-template <class R, int NS> struct Lphi4 {
-  using A = Ar<R>;
-  static __device__ __forceinline__ R p2(R x) { return A::mul(x, x); }
-  static __device__ __forceinline__ R p3(R x) { return A::mul(A::mul(x, x), x); }
-  static __device__ __forceinline__ R p4(R x) { return A::mul(A::mul(A::mul(x, x), x), x); }
-  // potDeriv(Tag<f>)
-  static __device__ __forceinline__ R dV(int f, const R (&v)[NS], R c0, R q)
+// ---- the scalar-singlet model's potential ----------------------------------------------------
+// The potential, its derivatives and its terms come from a model header shaped like the
+// reference's (potentialTerms / potDeriv / potDeriv2 per Tag: models/model_api.h), chosen when the
+// library is built, as the reference chooses its model when it compiles (CMakeLists.txt:133-146).
+// SPot evaluates the header's terms at one site in the arithmetic of Ar<R>: FP64 pins every
+// rounding (the order the header writes, which the oracle shares).
+template <class R, int NS> struct SPot {
+  using M = ScalarModel;
+  static __device__ __forceinline__ R dV(int f, const R (&v)[NS], const ModelCouplings &c)
   {
-    if constexpr (NS == 1) {
-      return A::mul(c0, p3(v[0]));
-    } else {
-      if (f == 0) return A::add(A::mul(c0, p3(v[0])), A::mul(A::mul(q, v[0]), p2(v[1])));
-      return A::mul(A::mul(q, v[1]), p2(v[0]));
-    }
+    return clb_models::pot_deriv<M, Ar<R>>(f, v, c);
   }
-  // sum of potentialTerms
-  static __device__ __forceinline__ R V(const R (&v)[NS], R c0q, R qh)
+  static __device__ __forceinline__ R V(const R (&v)[NS], const ModelCouplings &c)
   {
-    R r = A::mul(c0q, p4(v[0]));
-    if constexpr (NS == 2) r = A::add(r, A::mul(qh, p2(A::mul(v[0], v[1]))));
-    return r;
+    return clb_models::potential<M, Ar<R>>(v, c);
   }
-  static __device__ __forceinline__ R Vterm(int k, const R (&v)[NS], R c0q, R qh)
+  static __device__ __forceinline__ R Vterm(int k, const R (&v)[NS], const ModelCouplings &c)
   {
-    if (k == 0) return A::mul(c0q, p4(v[0]));
-    if constexpr (NS == 2) return A::mul(qh, p2(A::mul(v[0], v[1])));
-    return R(0);
+    return clb_models::potential_term<M, Ar<R>>(k, v, c);
   }
 };
 
@@ -103,7 +100,7 @@ __global__ void __launch_bounds__(BZ *BY)
                    double *__restrict__ partials)
 {
   using A = Ar<R>;
-  using Pot = Lphi4<R, NS>;
+  using Pot = SPot<R, NS>;
   __shared__ R tile[3][NS][BY + 2][BZ + 2];
   __shared__ double red_smem[(BZ * BY / 32) * kRedSlots];
 
@@ -131,7 +128,6 @@ __global__ void __launch_bounds__(BZ *BY)
     KB = (R)st->kick_B;
   }
   const R inv_dx2 = (R)a.inv_dx2;
-  const R c0 = (R)a.c0, q = (R)a.q, c0q = (R)a.c0_quarter, qh = (R)a.q_half;
   const R two = R(2);
 
   auto sidx = [&](int x, int yy, int zz) -> size_t { return ((size_t)x * N + yy) * N + zz; };
@@ -191,7 +187,7 @@ __global__ void __launch_bounds__(BZ *BY)
             const R tyv = A::sub(A::add(tile[b][f][ty + 2][tz + 1], tile[b][f][ty][tz + 1]), A::mul(two, c));
             const R tzv = A::sub(A::add(tile[b][f][ty + 1][tz + 2], tile[b][f][ty + 1][tz]), A::mul(two, c));
             const R lap = A::mul(inv_dx2, A::add(A::add(tx, tyv), tzv));
-            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cur, c0, q)));
+            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cur, a.mc)));
             const KickOut<R> ko = kick_val<R>(piC[f], K, a.h1, a.h2);
             pout[f * n3 + s] = ko.next;
             if (RED & 1) site_pi2 = f == 0 ? ko.mid * ko.mid : site_pi2 + ko.mid * ko.mid;
@@ -209,7 +205,7 @@ __global__ void __launch_bounds__(BZ *BY)
           }
         }
         if (RED & 1) acc_pi2 += site_pi2;
-        if (RED & 2) acc_v += (double)Pot::V(cur, c0q, qh);
+        if (RED & 2) acc_v += (double)Pot::V(cur, a.mc);
       }
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
@@ -281,11 +277,11 @@ __global__ void __launch_bounds__(256)
     k_measure(const R *fld, const R *pi, ScalarArgs a, double am, double *__restrict__ partials)
 {
   using A = Ar<R>;
-  using Pot = Lphi4<R, NS>;
+  using Pot = SPot<R, NS>;
   __shared__ double smem[(256 / 32) * kMeasSlots];
   const int N = a.N;
   const size_t n3 = (size_t)N * N * N;
-  const R inv_dx2 = (R)a.inv_dx2, c0q = (R)a.c0_quarter, qh = (R)a.q_half;
+  const R inv_dx2 = (R)a.inv_dx2;
   double acc[kMeasSlots];
 #pragma unroll
   for (int k = 0; k < kMeasSlots; ++k) acc[k] = 0;
@@ -313,7 +309,7 @@ __global__ void __launch_bounds__(256)
       acc[6 * f + 5] += m * m;
     }
 #pragma unroll
-    for (int k = 0; k < NS; ++k) acc[6 * NS + k] += (double)Pot::Vterm(k, v, c0q, qh);
+    for (int k = 0; k < NS; ++k) acc[6 * NS + k] += (double)Pot::Vterm(k, v, a.mc);
   }
   block_reduce<kMeasSlots, 256>(acc, smem);
   if (threadIdx.x == 0)

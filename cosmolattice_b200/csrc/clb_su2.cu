@@ -79,6 +79,7 @@ Params su2_params(const clb_handle *h)
   a.fm2 = fm * fm;
   a.dt = c.dt;
   a.inv_n3 = 1.0 / (double)h->n3;
+  a.order = gauge_site_order(c.N, true);
   return a;
 }
 
@@ -453,10 +454,10 @@ __attribute__((visibility("hidden"))) int su2_initialize(clb_handle *h, int32_t 
 {
   sweep(h, 0, true, true, Kick{});
   uint32_t fl = T_STORE_ALL;
-  if (h->cfg.expansion && correct_adot && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
-  if (h->cfg.expansion && h->cfg.evolver == CLB_LF) fl |= T_LF_CTOR;
+  if (h->cfg.expansion && correct_adot == 1 && !h->fb) fl |= T_CORRECT_ADOT; // modelinitializer.h:74-80
+  if (h->cfg.expansion && h->cfg.evolver == CLB_LF && correct_adot != CLB_INIT_RESTART) fl |= T_LF_CTOR;
   tail(h, fl, true);
-  h->synced = true;
+  h->synced = !(correct_adot == CLB_INIT_RESTART && h->cfg.evolver == CLB_LF); // leapfrog.h:30-31
   return check(h, "clb_initialize");
 }
 

@@ -44,6 +44,7 @@ struct Params {
   double qG, qH, gC, gD, gS, c4;
   double rfo2, rof2; // (fStar/omegaStar)^2 and its inverse
   double alpha, fm2, dt, inv_n3;
+  int order; // site order of the kick sweeps (for_sites)
 };
 
 // Scale factor, the cached averages of the five sectors (S, phi, Phi, A, SU(2)) and the sweep

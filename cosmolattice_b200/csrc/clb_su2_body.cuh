@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
   const State st = *stp;
   double acc[kRed];
   for (int k = 0; k < kRed; ++k) acc[k] = 0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
+  for_sites(a.N, a.n3, a.order, [&](size_t s) {
     Site<S, S> v = make_site<S, S>(f, a, s);
     v.ph = ph;
     S q[NP];
@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
       if (sect_su2(SECT)) acc[9] += (double)gB2(v);
       if (sect_scalars(SECT)) acc[10] += (double)v.pot();
     }
-  }
+  });
   if (RF || RP) {
     block_reduce<kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
@@ -715,7 +715,7 @@ __global__ void __launch_bounds__(128)
   const Coef<T> C{T(stp->kA), T(stp->kB), T(stp->kB2), T(stp->kG)};
   double acc[2 * kRed];
   for (int k = 0; k < 2 * kRed; ++k) acc[k] = 0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n3; s += (size_t)gridDim.x * blockDim.x) {
+  for_sites(a.N, a.n3, a.order, [&](size_t s) {
     const Site<S, T> v = make_site_tan<S>(f, df, a, s, cd);
     S q[NP], dq[NP];
     for (int c = C0; c < C1; ++c) {
@@ -763,7 +763,7 @@ __global__ void __launch_bounds__(128)
       if (sect_su2(SECT)) addf(4, gB2(v));
       if (sect_scalars(SECT)) addf(5, v.pot());
     }
-  }
+  });
   if (RF || RP) {
     block_reduce<2 * kRed, 128>(acc, smem);
     if (threadIdx.x == 0)

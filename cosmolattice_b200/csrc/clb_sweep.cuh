@@ -62,13 +62,21 @@ template <class R, class SH> struct TileGeom {
   static constexpr int SLOT = ((BYTES + 127) / 128) * 128; // TMA smem destinations 128-byte aligned
 };
 
+// Bound of each wait in a sweep's drain after an abort (copies already issued always complete).
+constexpr uint32_t kDrainTries = 1u << 26;
+
+template <bool B> struct BoolTag {
+  static constexpr bool value = B;
+};
+
 struct SweepArgs {
   Pad pd;
   int LX;          // planes per block
   int S;           // ring stages
   int rs;          // FP32 split storage: reference slot read by this launch
   uint32_t tries;  // bound of each mbarrier wait
-  double inv_dx2, c0, q, c0_quarter, q_half;
+  double inv_dx2;
+  ModelCouplings mc; // the model header's couplings
   double dtw, h1, h2;
   double dtw0;     // DRIFT == 2: a first drift of the same kind before dtw's (position Verlet)
 };
@@ -83,12 +91,15 @@ template <class R, int VZ> __device__ __forceinline__ void ldv(const R *p, R (&v
       v[k] = t.x;
       v[k + 1] = t.y;
     }
-  } else if constexpr (VZ == 4) {
-    const float4 t = *reinterpret_cast<const float4 *>(p);
-    v[0] = t.x;
-    v[1] = t.y;
-    v[2] = t.z;
-    v[3] = t.w;
+  } else if constexpr (VZ % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 4) {
+      const float4 t = *reinterpret_cast<const float4 *>(p + k);
+      v[k] = t.x;
+      v[k + 1] = t.y;
+      v[k + 2] = t.z;
+      v[k + 3] = t.w;
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < VZ; k += 2) {
@@ -105,8 +116,9 @@ template <class R, int VZ> __device__ __forceinline__ void stv(R *p, const R (&v
   if constexpr (sizeof(R) == 8) {
 #pragma unroll
     for (int k = 0; k < VZ; k += 2) *reinterpret_cast<double2 *>(p + k) = double2{v[k], v[k + 1]};
-  } else if constexpr (VZ == 4) {
-    *reinterpret_cast<float4 *>(p) = float4{v[0], v[1], v[2], v[3]};
+  } else if constexpr (VZ % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < VZ; k += 4) *reinterpret_cast<float4 *>(p + k) = float4{v[k], v[k + 1], v[k + 2], v[k + 3]};
   } else {
 #pragma unroll
     for (int k = 0; k < VZ; k += 2) *reinterpret_cast<float2 *>(p + k) = float2{v[k], v[k + 1]};
@@ -120,32 +132,26 @@ template <int NS> struct RefStep {
   double V; // potential at the reference point
 };
 
-// lphi4 with one field about a reference phi_r: exact polynomial differences in the fluctuation s,
-//   dV(phi_r + s) - dV(phi_r) = s (a1 + s (a2 + c0 s)),      a1 = 3 c0 phi_r^2, a2 = 3 c0 phi_r
-//   V(phi_r + s) - V(phi_r)   = s (b1 + s (b2 + s (b3 + c0/4 s))), b1 = c0 phi_r^3, b2 = 3/2 c0 phi_r^2,
-//                                                               b3 = c0 phi_r
-// evaluated in FP32 (relative precision of the fluctuation's own force and energy).
-struct Lphi4SplitCoef {
-  float a1, a2, c0, b1, b2, b3, c0q;
-  __host__ __device__ static Lphi4SplitCoef make(double phi_r, double c0)
-  {
-    Lphi4SplitCoef k;
-    k.a1 = (float)(3.0 * c0 * phi_r * phi_r);
-    k.a2 = (float)(3.0 * c0 * phi_r);
-    k.c0 = (float)c0;
-    k.b1 = (float)(c0 * phi_r * phi_r * phi_r);
-    k.b2 = (float)(1.5 * c0 * phi_r * phi_r);
-    k.b3 = (float)(c0 * phi_r);
-    k.c0q = (float)(0.25 * c0);
-    return k;
-  }
-  __device__ __forceinline__ float ddV(float s) const { return s * fmaf(s, fmaf(c0, s, a2), a1); }
-  __device__ __forceinline__ float dVpot(float s) const { return s * fmaf(s, fmaf(s, fmaf(c0q, s, b3), b2), b1); }
+// The model's FP32 fluctuation form (models/model_api.h), if its header has one: with one field,
+// the force and energy of a fluctuation s about the FP64 reference, evaluated in FP32.  Without
+// it (NoFluct) the split form takes both differences in FP64.
+struct NoFluct {
+  template <class C> __host__ __device__ static NoFluct make(double, const C &) { return {}; }
+  __device__ float dV(float) const { return 0.f; } // never called: the FP64 differences are taken
+  __device__ float V(float) const { return 0.f; }
 };
+template <class M, bool> struct FluctOf {
+  using type = NoFluct;
+};
+template <class M> struct FluctOf<M, true> {
+  using type = typename M::Fluct;
+};
+constexpr bool kModelFluct = clb_models::HasFluct<ScalarModel>::value;
+using ModelFluct = typename FluctOf<ScalarModel, kModelFluct>::type;
 
 template <int NS>
 __device__ __forceinline__ RefStep<NS> ref_step(const DevState *st, int rs, bool drift, bool kick, double dtw, double h1,
-                                                double h2, double c0, double q, double dtw0 = 0.0)
+                                                double h2, const ModelCouplings &mc, double dtw0 = 0.0)
 {
   RefStep<NS> r;
   double phi[NS];
@@ -156,10 +162,10 @@ __device__ __forceinline__ RefStep<NS> ref_step(const DevState *st, int rs, bool
     if (drift) phi[f] = __dadd_rn(phi[f], __dmul_rn(st->drift_p, __dmul_rn(dtw, st->ref_pi[rs][f])));
     r.phi[f] = phi[f];
   }
-  r.V = Lphi4<double, NS>::V(phi, 0.25 * c0, 0.5 * q);
+  r.V = SPot<double, NS>::V(phi, mc);
 #pragma unroll
   for (int f = 0; f < NS; ++f) {
-    r.dV[f] = Lphi4<double, NS>::dV(f, phi, c0, q);
+    r.dV[f] = SPot<double, NS>::dV(f, phi, mc);
     const double Kr = -__dmul_rn(st->kick_B, r.dV[f]);
     const double p0 = st->ref_pi[rs][f];
     r.pi_mid[f] = kick ? __dadd_rn(p0, __dmul_rn(h1, Kr)) : p0;
@@ -179,7 +185,7 @@ __global__ void __launch_bounds__(SH::THREADS)
             SweepArgs a, const DevState *__restrict__ st, double *__restrict__ partials, int *__restrict__ err)
 {
   using A = Ar<R>;
-  using Pot = Lphi4<R, NS>;
+  using Pot = SPot<R, NS>;
   using TG = TileGeom<R, SH>;
   constexpr int VZ = SH::VZ;
   constexpr bool LOADP = DRIFT || KICK || (RED & 1);
@@ -237,14 +243,13 @@ __global__ void __launch_bounds__(SH::THREADS)
     KB = (R)st->kick_B;
   }
   const R inv_dx2 = (R)a.inv_dx2;
-  const R c0 = (R)a.c0, q = (R)a.q, c0q = (R)a.c0_quarter, qh = (R)a.q_half;
   const R two = R(2);
   RefStep<NS> rf{};
-  Lphi4SplitCoef spc{};
+  ModelFluct spc{};
   const float h1f = (float)a.h1, h2f = (float)a.h2;
   if constexpr (SPLIT) {
-    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.c0, a.q, DRIFT == 2 ? a.dtw0 : 0.0);
-    spc = Lphi4SplitCoef::make(rf.phi[0], a.c0);
+    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.mc, DRIFT == 2 ? a.dtw0 : 0.0);
+    spc = ModelFluct::make(rf.phi[0], a.mc);
     if ((DRIFT || KICK) && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
       DevState *sw = const_cast<DevState *>(st); // slot rs ^ 1 is read by no block of this launch
 #pragma unroll
@@ -295,15 +300,29 @@ __global__ void __launch_bounds__(SH::THREADS)
     const R fv = box(s, f, 0)[o];
     return LOADP ? drift1(fv, box(s, f, 1)[o]) : fv;
   };
+  // neighbour values of the current plane (stage s): y - 1, y + 1 rows and the z - 1, z + VZ cells,
+  // each drifted as it is read
+  auto neighbours = [&](int s, int f, R (&ym)[VZ], R (&yp)[VZ], R &zm, R &zp) {
+    dquad(s, f, toff - BOXZ, ym, nullptr);
+    dquad(s, f, toff + BOXZ, yp, nullptr);
+    zm = dscalar(s, f, toff - 1);
+    zp = dscalar(s, f, toff + VZ);
+  };
 
   __syncthreads();
   if (tid == 0)
     for (int j = 0; j < min(S, nplanes); ++j) issue(j);
 
-  int issued = min(S, nplanes), waited = 0; // tracked by thread 0 for the drain on abort
+  // Thread 0 tracks the planes issued and the first plane whose wait did not complete, for the
+  // drain on abort: a wait that gave up leaves its copy in flight.
+  int issued = min(S, nplanes), waited = 0;
+  bool gave_up = false;
   auto wait_plane = [&](int j) {
-    if (!mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1), a.tries)) abort_flag = 1;
-    if (tid == 0) waited = j + 1;
+    if (!mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1), a.tries)) {
+      abort_flag = 1;
+      gave_up = true;
+    }
+    if (tid == 0 && !gave_up) waited = j + 1;
   };
 
   // periodic ghost copies this thread writes (they depend on y and z only): y row -1 / N, z column -1 / N
@@ -319,7 +338,9 @@ __global__ void __launch_bounds__(SH::THREADS)
   for (int f = 0; f < NS; ++f) dquad(0, f, toff, prev[f], nullptr);
   wait_plane(1);
 #pragma unroll
-  for (int f = 0; f < NS; ++f) dquad(1 % S, f, toff, cur[f], LOADP ? &piC[f] : nullptr);
+  for (int f = 0; f < NS; ++f) {
+    dquad(1 % S, f, toff, cur[f], LOADP ? &piC[f] : nullptr);
+  }
   __syncthreads();
   if (abort_flag) goto drain;
   if (tid == 0 && S < nplanes) {
@@ -342,76 +363,84 @@ __global__ void __launch_bounds__(SH::THREADS)
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
         dquad(sn, f, toff, nxt[f], LOADP ? &piN[f] : nullptr);
-        dquad(sb, f, toff - BOXZ, ym[f], nullptr);
-        dquad(sb, f, toff + BOXZ, yp[f], nullptr);
-        zmv[f] = dscalar(sb, f, toff - 1);
-        zpv[f] = dscalar(sb, f, toff + VZ);
+        neighbours(sb, f, ym[f], yp[f], zmv[f], zpv[f]);
       }
       R outp[NS][VZ];
       if constexpr (SPLIT) {
-        // FP32 fluctuations about the FP64 references: FP32 arithmetic throughout, per-plane FP32
-        // partial sums folded into FP64 accumulators (the reference terms are added at the end).
-        // Not bound to the reference's operation order: the Laplacian is (sum of the six
-        // neighbours) - 6 c with 1/dx^2 folded into the kick coefficient, and the gradient sum is
-        // scaled once per plane.
-        float s_p[NS], s_p2 = 0.f, s_g2 = 0.f, s_dv = 0.f;
-        const float KAd = KA * inv_dx2;
+        // Full tiles (every site of the thread inside the lattice) take a copy of the plane's
+        // arithmetic without the per-site predicates of the volume sums.
+        auto split_plane = [&](auto full_tag) {
+          constexpr bool FULL = decltype(full_tag)::value;
+          // FP32 fluctuations about the FP64 references: FP32 arithmetic throughout, per-plane FP32
+          // partial sums folded into FP64 accumulators (the reference terms are added at the end).
+          // Not bound to the reference's operation order: the Laplacian is (sum of the six
+          // neighbours) - 6 c with 1/dx^2 folded into the kick coefficient, and the gradient sum is
+          // scaled once per plane.
+          float s_p[NS], s_p2 = 0.f, s_g2 = 0.f, s_dv = 0.f;
+          const float KAd = KA * inv_dx2;
 #pragma unroll
-        for (int f = 0; f < NS; ++f) s_p[f] = 0.f;
+          for (int f = 0; f < NS; ++f) s_p[f] = 0.f;
 #pragma unroll
-        for (int k = 0; k < VZ; ++k) {
-          const bool vk = k < nvalid;
-          float cv[NS];
-          double cd[NS];
+          for (int k = 0; k < VZ; ++k) {
+            const bool vk = FULL || k < nvalid; // FULL: every site of the thread is inside
+            float cv[NS];
+            constexpr bool FL = NS == 1 && kModelFluct; // the header's FP32 fluctuation form
+            double cd[NS];                                // otherwise the full field values in FP64
 #pragma unroll
-          for (int f = 0; f < NS; ++f) {
-            cv[f] = cur[f][k];
-            if constexpr (NS > 1) cd[f] = rf.phi[f] + (double)cur[f][k];
-          }
+            for (int f = 0; f < NS; ++f) {
+              cv[f] = cur[f][k];
+              if constexpr (!FL) cd[f] = rf.phi[f] + (double)cur[f][k];
+            }
+            (void)cd;
 #pragma unroll
-          for (int f = 0; f < NS; ++f) {
-            const float c = cur[f][k];
-            const float zn = k + 1 < VZ ? cur[f][k + 1 < VZ ? k + 1 : 0] : zpv[f];
-            const float zm = k > 0 ? cur[f][k > 0 ? k - 1 : 0] : zmv[f];
-            if (KICK) {
-              const float nsum = ((nxt[f][k] + prev[f][k]) + (yp[f][k] + ym[f][k])) + (zn + zm);
-              const float lap = fmaf(-6.f, c, nsum); // times 1/dx^2 in KAd
-              float ddv;
-              if constexpr (NS == 1)
-                ddv = spc.ddV(c);
-              else
-                ddv = (float)(Lphi4<double, NS>::dV(f, cd, a.c0, a.q) - rf.dV[f]);
-              const float K = KAd * lap - KB * ddv;
-              const float pm = fmaf(h1f, K, piC[f][k]);
-              outp[f][k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
-              if ((RED & 1) && vk) {
-                s_p[f] += pm;
-                s_p2 = fmaf(pm, pm, s_p2);
+            for (int f = 0; f < NS; ++f) {
+              const float c = cur[f][k];
+              const float zn = k + 1 < VZ ? cur[f][k + 1 < VZ ? k + 1 : 0] : zpv[f];
+              const float zm = k > 0 ? cur[f][k > 0 ? k - 1 : 0] : zmv[f];
+              if (KICK) {
+                const float nsum = ((nxt[f][k] + prev[f][k]) + (yp[f][k] + ym[f][k])) + (zn + zm);
+                const float lap = fmaf(-6.f, c, nsum); // times 1/dx^2 in KAd
+                float ddv;
+                if constexpr (FL)
+                  ddv = spc.dV(c);
+                else
+                  ddv = (float)(SPot<double, NS>::dV(f, cd, a.mc) - rf.dV[f]);
+                const float K = KAd * lap - KB * ddv;
+                const float pm = fmaf(h1f, K, piC[f][k]);
+                outp[f][k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
+                if ((RED & 1) && vk) {
+                  s_p[f] += pm;
+                  s_p2 = fmaf(pm, pm, s_p2);
+                }
+              } else if ((RED & 1) && vk) {
+                s_p[f] += piC[f][k];
+                s_p2 = fmaf(piC[f][k], piC[f][k], s_p2);
               }
-            } else if ((RED & 1) && vk) {
-              s_p[f] += piC[f][k];
-              s_p2 = fmaf(piC[f][k], piC[f][k], s_p2);
+              if ((RED & 2) && vk) {
+                const float gx = nxt[f][k] - c, gy = yp[f][k] - c, gz = zn - c;
+                s_g2 += gx * gx + gy * gy + gz * gz; // times 1/dx^2 per plane
+              }
             }
             if ((RED & 2) && vk) {
-              const float gx = nxt[f][k] - c, gy = yp[f][k] - c, gz = zn - c;
-              s_g2 += gx * gx + gy * gy + gz * gz; // times 1/dx^2 per plane
+              if constexpr (FL)
+                s_dv += spc.V(cv[0]);
+              else
+                s_dv += (float)(SPot<double, NS>::V(cd, a.mc) - rf.V);
             }
           }
-          if ((RED & 2) && vk) {
-            if constexpr (NS == 1)
-              s_dv += spc.dVpot(cv[0]);
-            else
-              s_dv += (float)(Lphi4<double, NS>::V(cd, a.c0_quarter, a.q_half) - rf.V);
-          }
-        }
-        if (RED) {
+          if (RED) {
 #pragma unroll
-          for (int f = 0; f < NS; ++f) acc_p[f] += (double)s_p[f];
-          acc_pi2 += (double)s_p2;
-          acc_g2 += (double)s_g2 * a.inv_dx2;
-          acc_v += (double)s_dv;
-          cnt += nvalid;
-        }
+            for (int f = 0; f < NS; ++f) acc_p[f] += (double)s_p[f];
+            acc_pi2 += (double)s_p2;
+            acc_g2 += (double)s_g2 * a.inv_dx2;
+            acc_v += (double)s_dv;
+            cnt += nvalid;
+          }
+        };
+        if (nvalid == VZ)
+          split_plane(BoolTag<true>{});
+        else
+          split_plane(BoolTag<false>{});
       } else {
 #pragma unroll
       for (int k = 0; k < VZ; ++k) {
@@ -429,7 +458,7 @@ __global__ void __launch_bounds__(SH::THREADS)
             const R tyv = A::sub(A::add(yp[f][k], ym[f][k]), A::mul(two, c));
             const R tzv = A::sub(A::add(zn, zm), A::mul(two, c));
             const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
-            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cv, c0, q)));
+            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cv, a.mc)));
             const KickOut<R> ko = kick_val<R>(piC[f][k], K, a.h1, a.h2);
             outp[f][k] = ko.next;
             if (RED & 1) site_pi2 = f == 0 ? ko.mid * ko.mid : site_pi2 + ko.mid * ko.mid;
@@ -443,7 +472,7 @@ __global__ void __launch_bounds__(SH::THREADS)
           }
         }
         if ((RED & 1) && k < nvalid) acc_pi2 += site_pi2;
-        if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, c0q, qh);
+        if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, a.mc);
       }
       }
       // stores: the thread's VZ sites, then the periodic ghost copies of boundary sites
@@ -515,11 +544,12 @@ __global__ void __launch_bounds__(SH::THREADS)
   }
 
 drain:
-  // A wait gave up: flag it, then let thread 0 wait (bounded) for the copies still in flight so no
-  // TMA write lands in shared memory after the block has left.
+  // A wait gave up: flag it, then let thread 0 wait for the copies still in flight so no TMA write
+  // lands in shared memory after the block has left.  The drain has its own fixed bound, far above
+  // the time a tile load takes, so a small a.tries cannot cut it short.
   if (tid == 0) {
     atomicOr(err, 1);
-    for (int j = waited; j < issued; ++j) (void)mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1), a.tries);
+    for (int j = waited; j < issued; ++j) (void)mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1), kDrainTries);
   }
 }
 
@@ -557,15 +587,15 @@ __global__ void __launch_bounds__(256)
 // Measurement sums (same slots as k_measure) over the padded layout.
 template <class R, int NS>
 __global__ void __launch_bounds__(256)
-    k_measure_pad(const R *fld, const R *pi, Pad pd, double inv_dx2d, double c0qd, double qhd, double am,
+    k_measure_pad(const R *fld, const R *pi, Pad pd, double inv_dx2d, ModelCouplings mc, double am,
                   const DevState *__restrict__ st, int rs, double *__restrict__ partials)
 {
   constexpr bool SPLIT = sizeof(R) == 4;
   using A = Ar<R>;
-  using Pot = Lphi4<R, NS>;
+  using Pot = SPot<R, NS>;
   __shared__ double smem[(256 / 32) * kMeasSlots];
   const int N = pd.N;
-  const R inv_dx2 = (R)inv_dx2d, c0q = (R)c0qd, qh = (R)qhd;
+  const R inv_dx2 = (R)inv_dx2d;
   double acc[kMeasSlots];
 #pragma unroll
   for (int k = 0; k < kMeasSlots; ++k) acc[k] = 0;
@@ -597,7 +627,7 @@ __global__ void __launch_bounds__(256)
       }
 #pragma unroll
       for (int k = 0; k < NS; ++k)
-        acc[6 * NS + k] += SPLIT ? Lphi4<double, NS>::Vterm(k, vd, c0qd, qhd) : (double)Pot::Vterm(k, v, c0q, qh);
+        acc[6 * NS + k] += SPLIT ? SPot<double, NS>::Vterm(k, vd, mc) : (double)Pot::Vterm(k, v, mc);
     }
   }
   block_reduce<kMeasSlots, 256>(acc, smem);

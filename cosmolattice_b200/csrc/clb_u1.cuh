@@ -51,6 +51,7 @@ struct U1Params {
   double J0;    // 2/dx (fStar/omegaStar)^2            (mattercurrents.h:29, 70)
   double el0;   // 0.5 (omegaStar/fStar)^2             (energies.h:70, 80)
   double alpha, fm2, dt, inv_n3;
+  int order; // site order of the kick and adjoint sweeps (for_sites)
 };
 
 // Kick factors of up to two successive kicks with the same kernel: complex scalar (dt/2 w, or
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
   double acc[kU1Red];
 #pragma unroll
   for (int k = 0; k < kU1Red; ++k) acc[k] = 0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
+  for_sites(a.N, n3, a.order, [&](size_t s) {
     long long op[3], om[3];
     u1_offsets(a.N, s, op, om);
     U1Site<T> o;
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
 #pragma unroll
       for (int c = 0; c < 5; ++c) p[c * n3 + s] = (S)q[c];
     }
-  }
+  });
   if (RF || RP) {
     block_reduce<kU1Red, 256>(acc, smem);
     if (threadIdx.x == 0) {

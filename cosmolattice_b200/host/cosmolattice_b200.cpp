@@ -1,78 +1,54 @@
-// cosmolattice_b200.cpp - C++20 host of the lphi4 model over the libclb200 C ABI.
+// cosmolattice_b200.cpp - C++20 host of the lphi4, lphi4U1 and lphi4SU2U1 models over the libclb200
+// C ABI.
 //
-// The reference's main (source/cosmolattice.cpp:134-201) for the lphi4 header (models/lphi4.h): the
-// run parameters and model keys of a reference parameter file, the initial state drawn on the GPU
-// (clb_generate_state, the FluctuationsGenerator recipe), clb_initialize (ModelInitializer's scale
-// factor and aDot correction, modelinitializer.h:47-81), then the time loop
-//   while (t < tMax - dt/2) { measure every round(tOutputFreq/dt) steps (after sync); evolve; }
-// writing average_energies.txt, average_energy_conservation.txt, average_scale_factor.txt and
-// average_scalar_<i>.txt as the reference's MeasurementsSaver does (15 significant digits,
-// measurementssaverstd.h:61-82).  Steps between two measurements go to the GPU in one clb_evolve.
+// The reference's main (source/cosmolattice.cpp:134-201) for one model header (models.h; the key
+// `model` names it, where the reference picks it at compile time): the run parameters and model
+// keys of a reference parameter file; the initial state drawn on the GPU (clb_generate_state, the
+// FluctuationsGenerator recipe and the Gauss solves), then clb_initialize (ModelInitializer's scale
+// factor and aDot correction, modelinitializer.h:47-81) - or, with restart = true, the state of a
+// restart file (SimulationManager::loadSim, simulationmanager.h:69-100); then the time loop
+//   while (t < tMax - dt/2) { sync and measure every round(tOutputFreq/dt) steps, spectra every
+//   round(tOutputInfreq/dt) steps; evolve; backup every round(tBackupFreq/dt) steps }
+// writing the measurers' files: average_energies.txt, average_energy_conservation.txt,
+// average_scale_factor.txt, the means files of every field, the Gauss-law files of the gauge
+// fields (measurementssaverstd.h:61-82, 15 significant digits) and spectra_<name>.txt
+// (spectrumsaverstd.h:54-96).  Steps between two measurements go to the GPU in one clb_evolve.
 //
 // Usage: cosmolattice_b200 [input.in] [key=value ...]
-// Keys (runparameters.h:60-236, lphi4.h:120-226): N, kIR or lSide, dt, tMax, t0, evolver,
-// expansion, fixedBackground, omegaEoS, H0, a0, tOutputFreq, kCutOff, outputfile, print_headers,
-// lambda, q, lambda_prog, initial_amplitudes (1 or 2 values: one or two fields), initial_momenta,
-// fluct_amplitude, MPl; host keys: precision (fp64 | fp32), path (fused | reference), deviceSeed
-// (the Philox key; default: FNV-1a of baseSeed).
+// Keys (runparameters.h:60-236 and the model headers, models.h): N, kIR or lSide, dt, tMax, t0,
+// evolver, expansion, fixedBackground, omegaEoS, H0, a0, tOutputFreq, tOutputInfreq, kCutOff,
+// outputfile, print_headers, PS_type, PS_version, deltaKBin, restart, restartFile, tBackupFreq,
+// backupPath, saveFile, and the model's keys; host keys: model (lphi4 | lphi4U1 | lphi4SU2U1),
+// precision (fp64 | fp32), path (fused | reference), deviceSeed (the Philox key; default: FNV-1a
+// of baseSeed).
+//
+// Restart files use the layout of cosmolattice_b200/restart.py (HDF5 is not available): a magic,
+// a header, each sector's field then momentum arrays in the reference's save order, the six
+// scale-factor values and tSave, and the parameter lines.
 
 #include "../../include/clb200.h"
+#include "models.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <map>
-#include <sstream>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 namespace {
 
+using host::HostModel;
+using host::Params;
+
 constexpr double kPi = 3.14159265358979323846;
-constexpr double kReducedPlanckGeV = 2.435e18;
-
-// ParameterParser: "key = value" lines ('#' starts a comment), later keys override earlier ones.
-struct Params {
-  std::map<std::string, std::string> kv;
-
-  void add_line(std::string line)
-  {
-    if (auto c = line.find('#'); c != std::string::npos) line.erase(c);
-    const auto eq = line.find('=');
-    if (eq == std::string::npos) return;
-    auto trim = [](std::string s) {
-      const auto a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
-      return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
-    };
-    const std::string k = trim(line.substr(0, eq)), v = trim(line.substr(eq + 1));
-    if (!k.empty()) kv[k] = v;
-  }
-  bool has(const std::string &k) const { return kv.count(k) != 0; }
-  std::string str(const std::string &k, const std::string &d) const { return has(k) ? kv.at(k) : d; }
-  double num(const std::string &k, double d) const { return has(k) ? std::stod(kv.at(k)) : d; }
-  double num(const std::string &k) const
-  {
-    if (!has(k)) throw std::runtime_error("Parameter " + k + " is missing.");
-    return std::stod(kv.at(k));
-  }
-  std::vector<double> nums(const std::string &k) const
-  {
-    std::vector<double> out;
-    if (!has(k)) return out;
-    std::istringstream is(kv.at(k));
-    for (double x; is >> x;) out.push_back(x);
-    return out;
-  }
-  bool flag(const std::string &k, bool d) const
-  {
-    if (!has(k)) return d;
-    const std::string v = kv.at(k);
-    return v == "true" || v == "1" || v == "True" || v == "TRUE";
-  }
-};
 
 int evolver_id(const std::string &v) // evolvertype.h:39-82
 {
@@ -97,19 +73,102 @@ void check(clb_handle *h, int rc, const char *what)
   if (rc != CLB_OK) throw std::runtime_error(std::string(what) + ": " + clb_last_error(h));
 }
 
+std::string fmt15(double v)
+{
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "%.15g", v);
+  return buf;
+}
+
 struct Out {
   std::ofstream f;
-  void row(const std::vector<double> &v)
+  void row(const std::vector<double> &v, const char *sep = "    ")
   {
-    char buf[64];
-    for (size_t i = 0; i < v.size(); ++i) {
-      std::snprintf(buf, sizeof(buf), "%.15g", v[i]);
-      f << (i ? "    " : "") << buf;
-    }
+    for (size_t i = 0; i < v.size(); ++i) f << (i ? sep : "") << fmt15(v[i]);
     f << '\n';
     f.flush();
   }
 };
+
+std::string join(const std::vector<std::string> &v, const char *sep = "    ")
+{
+  std::string s;
+  for (size_t i = 0; i < v.size(); ++i) s += (i ? sep : "") + v[i];
+  return s;
+}
+
+// ---- restart files (the layout of cosmolattice_b200/restart.py) -------------------------------
+const char kMagic[16] = {'C', 'L', 'B', '2', '0', '0', '-', 'R', 'E', 'S', 'T', 'A', 'R', 'T', 0, 0};
+
+// (first field, field count, first momentum, momentum count) per sector, in the reference's save
+// order (simulationmanager.h:112-125)
+std::vector<std::array<int, 4>> sectors(const HostModel &m)
+{
+  if (m.kind == CLB_MODEL_LPHI4SU2U1) return {{0, 1, 0, 1}, {1, 2, 1, 2}, {3, 4, 3, 4}, {7, 3, 7, 3}, {10, 12, 10, 9}};
+  if (m.kind == CLB_MODEL_LPHI4U1) return {{0, 2, 0, 2}, {2, 3, 2, 3}};
+  std::vector<std::array<int, 4>> s;
+  for (int i = 0; i < m.n_scalars; ++i) s.push_back({i, 1, i, 1});
+  return s;
+}
+
+void save_sim(clb_handle *h, const HostModel &m, int N, double t, const Params &par, const std::string &path)
+{
+  int32_t nf = 0, np = 0;
+  clb_num_components(h, &nf, &np);
+  const size_t n3 = (size_t)N * N * N;
+  std::vector<double> f((size_t)nf * n3), p((size_t)np * n3);
+  clb_scalefactor sf{};
+  check(h, clb_get_state(h, f.data(), p.data(), &sf), "clb_get_state");
+  const auto secs = sectors(m);
+  const std::string tmp = path + ".part";
+  {
+    std::ofstream o(tmp, std::ios::binary);
+    if (!o) throw std::runtime_error("cannot write " + tmp);
+    o.write(kMagic, 16);
+    const int64_t hdr[8] = {1, m.kind, N, nf, np, (int64_t)n3, (int64_t)secs.size(), 0};
+    o.write(reinterpret_cast<const char *>(hdr), sizeof(hdr));
+    for (const auto &s : secs) {
+      o.write(reinterpret_cast<const char *>(f.data() + (size_t)s[0] * n3), (std::streamsize)(s[1] * n3 * 8));
+      o.write(reinterpret_cast<const char *>(p.data() + (size_t)s[2] * n3), (std::streamsize)(s[3] * n3 * 8));
+    }
+    const double sc[7] = {sf.aSI, sf.aI, sf.aIM, sf.aDotSI, sf.aDotI, sf.aDotSIM, t};
+    o.write(reinterpret_cast<const char *>(sc), sizeof(sc));
+    std::string text;
+    for (const auto &[k, v] : par.kv) text += k + " = " + v + "\n";
+    const int64_t len = (int64_t)text.size();
+    o.write(reinterpret_cast<const char *>(&len), 8);
+    o.write(text.data(), len);
+    if (!o) throw std::runtime_error("write failed: " + tmp);
+  }
+  std::filesystem::rename(tmp, path);
+}
+
+double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &path)
+{
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::runtime_error("cannot read restart file " + path);
+  char magic[16];
+  in.read(magic, 16);
+  int64_t hdr[8];
+  in.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
+  if (!in || std::memcmp(magic, kMagic, 16) != 0 || hdr[0] != 1)
+    throw std::runtime_error(path + ": not a restart file of this format");
+  if (hdr[1] != m.kind || hdr[2] != N)
+    throw std::runtime_error(path + ": saved for another model or lattice size");
+  const size_t n3 = (size_t)hdr[5];
+  std::vector<double> f((size_t)hdr[3] * n3), p((size_t)hdr[4] * n3);
+  for (const auto &s : sectors(m)) {
+    in.read(reinterpret_cast<char *>(f.data() + (size_t)s[0] * n3), (std::streamsize)(s[1] * n3 * 8));
+    in.read(reinterpret_cast<char *>(p.data() + (size_t)s[2] * n3), (std::streamsize)(s[3] * n3 * 8));
+  }
+  double sc[7];
+  in.read(reinterpret_cast<char *>(sc), sizeof(sc));
+  if (!in) throw std::runtime_error(path + ": truncated");
+  const clb_scalefactor sf{sc[1], sc[0], sc[2], sc[4], sc[3], sc[5]};
+  check(h, clb_set_state(h, f.data(), p.data(), &sf), "clb_set_state");
+  check(h, clb_initialize(h, CLB_INIT_RESTART), "clb_initialize");
+  return sc[6];
+}
 
 } // namespace
 
@@ -131,33 +190,21 @@ try {
   double dx;
   if (par.has("kIR")) dx = 2 * kPi / (N * par.num("kIR"));
   else dx = par.num("lSide") / N;
+  const double kIR = 2 * kPi / (N * dx);
   const double t0 = par.num("t0", 0.0), tMax = par.num("tMax");
   const bool expansion = par.flag("expansion", true);
   const bool fixedBg = expansion && par.flag("fixedBackground", false);
-  const double tOut = par.num("tOutputFreq", 10 * dt);
-  const int outFreq = std::max(1, (int)std::lround(tOut / dt)); // measurer.h:48-53
+  const int outFreq = std::max(1, (int)std::lround(par.num("tOutputFreq", 10 * dt) / dt)); // measurer.h:48-53
+  const int specFreq = std::max(1, (int)std::lround(par.num("tOutputInfreq", 100 * dt) / dt));
+  const int backupFreq = par.has("tBackupFreq") ? std::max(1, (int)std::lround(par.num("tBackupFreq") / dt)) : 0;
   double kCut = par.num("kCutOff", -1.0);
   if (kCut < 0) kCut = 2 * std::sqrt(3.0) * kPi / dx;
   const std::string outdir = par.str("outputfile", "./");
+  const int psType = (int)par.num("PS_type", 1), psVersion = (int)par.num("PS_version", 1);
+  const double dk = par.num("deltaKBin", 1.0);
+  const int nbins = (int)std::floor(std::sqrt(3.0) / 2.0 * N / dk); // runparameters.h:98
 
-  // ---- the lphi4 header (models/lphi4.h:120-226): alpha = 1, fStar = phi0, omegaStar = sqrt(lambda) phi0
-  std::vector<double> phi0 = par.nums("initial_amplitudes"), pi0 = par.nums("initial_momenta");
-  if (phi0.empty() || phi0.size() > 2) throw std::runtime_error("initial_amplitudes takes one or two values");
-  const int Ns = (int)phi0.size();
-  pi0.resize(Ns, 0.0);
-  const double lambda = par.num("lambda"), q = Ns == 2 ? par.num("q", 0.0) : 0.0;
-  const double c0 = par.num("lambda_prog", 1.0);
-  const double fStar = phi0[0], omegaStar = std::sqrt(lambda) * fStar, MPl = par.num("MPl", kReducedPlanckGeV);
-  std::vector<double> f0(Ns), p0(Ns), m2(Ns);
-  for (int i = 0; i < Ns; ++i) {
-    f0[i] = phi0[i] / fStar;
-    p0[i] = pi0[i] / fStar / omegaStar;
-  }
-  // pot0 and masses2 at the homogeneous point (abstractmodel.h:220-248, lphi4.h:154-206)
-  double pot0 = 0.25 * c0 * std::pow(f0[0], 4);
-  if (Ns == 2) pot0 += 0.5 * q * std::pow(f0[0] * f0[1], 2);
-  m2[0] = 3 * c0 * std::pow(f0[0], 2) + (Ns == 2 ? q * std::pow(f0[1], 2) : 0.0);
-  if (Ns == 2) m2[1] = q * std::pow(f0[0], 2);
+  const HostModel m = host::make_model(par.str("model", "lphi4"), par);
 
   clb_config cfg{};
   cfg.N = N;
@@ -171,101 +218,136 @@ try {
   if (fixedBg) {
     cfg.fixed_background = 1;
     cfg.omega_eos = par.num("omegaEoS", 1.0 / 3.0);
-    cfg.H0 = par.num("H0") / omegaStar;
+    cfg.H0 = par.num("H0") / m.omegaStar;
   }
-  clb_model_desc md{};
-  md.kind = CLB_MODEL_LPHI4;
-  md.n_scalars = Ns;
-  md.alpha = 1.0;
-  md.fStar = fStar;
-  md.omegaStar = omegaStar;
-  md.MPl = MPl;
-  md.couplings[0] = c0;
-  md.couplings[1] = q;
+  const clb_model_desc md = m.desc();
   clb_handle *h = nullptr;
   check(nullptr, clb_create(&cfg, &md, &h), "clb_create");
+  std::unique_ptr<clb_handle, void (*)(clb_handle *)> guard(h, clb_destroy);
 
-  // ---- ScaleFactorInitializer (scalefactorinitializer.h:37-65) and the fluctuations on the GPU
-  double aDot = 0.0;
-  if (fixedBg) aDot = cfg.H0;
-  else if (expansion) {
-    double kin = 0;
-    for (int i = 0; i < Ns; ++i) kin += 0.5 * std::pow(pi0[i] / fStar / omegaStar, 2);
-    aDot = fStar / MPl * std::sqrt((kin + pot0) / 3.0);
+  double t = t0;
+  if (par.flag("restart", false)) {
+    t = load_sim(h, m, N, par.str("restartFile", outdir + "/" + m.name + "_backup.clb"));
+  } else {
+    // ScaleFactorInitializer (scalefactorinitializer.h:37-65) and the fluctuations on the GPU
+    double aDot = 0.0;
+    if (fixedBg) aDot = cfg.H0;
+    else if (expansion) aDot = m.fStar / m.MPl * std::sqrt((m.kin0 + m.pot0) / 3.0);
+    const double a0 = fixedBg ? 1.0 : (expansion ? par.num("a0", 1.0) : 1.0);
+    clb_ic_params ic{};
+    ic.seed = par.has("deviceSeed") ? std::stoull(par.str("deviceSeed", "0")) : fnv1a(par.str("baseSeed", "0"));
+    ic.amplitude = m.fluct_amplitude >= 0 ? m.fluct_amplitude : m.omegaStar / m.fStar;
+    ic.k_cutoff = kCut;
+    ic.adot = aDot;
+    for (size_t i = 0; i < m.m2.size() && i < CLB_IC_MAX; ++i) {
+      ic.mass2[i] = m.m2[i];
+      ic.fld0[i] = m.f0[i];
+      ic.pi0[i] = m.p0[i];
+    }
+    for (int i = 0; i < 4; ++i) ic.charge[i] = m.charge[i];
+    clb_scalefactor sf{a0, a0, a0, aDot, aDot, 0.0};
+    check(h, clb_generate_state(h, &ic, &sf), "clb_generate_state");
+    check(h, clb_initialize(h, 1), "clb_initialize");
   }
-  const double a0 = fixedBg ? 1.0 : (expansion ? par.num("a0", 1.0) : 1.0);
-  clb_ic_params ic{};
-  ic.seed = par.has("deviceSeed") ? std::stoull(par.str("deviceSeed", "0")) : fnv1a(par.str("baseSeed", "0"));
-  ic.amplitude = par.num("fluct_amplitude", omegaStar / fStar);
-  ic.k_cutoff = kCut;
-  ic.adot = aDot;
-  for (int i = 0; i < Ns; ++i) {
-    ic.mass2[i] = m2[i];
-    ic.fld0[i] = f0[i];
-    ic.pi0[i] = p0[i];
-  }
-  clb_scalefactor sf{a0, a0, a0, aDot, aDot, 0.0};
-  check(h, clb_generate_state(h, &ic, &sf), "clb_generate_state");
-  check(h, clb_initialize(h, 1), "clb_initialize");
 
-  // ---- output files (measurementssaverstd.h:61-82)
+  // ---- output files (measurementssaverstd.h:61-82, spectrumsaverstd.h:54-96)
   const bool headers = par.flag("print_headers", false);
+  const bool append = par.flag("appendToFiles", false);
   auto open = [&](const std::string &name, const std::string &hdr) {
     Out o;
-    o.f.open(outdir + "/average_" + name + ".txt");
-    if (!o.f) throw std::runtime_error("cannot write " + outdir + "/average_" + name + ".txt");
-    if (headers) o.f << '#' << hdr << '\n';
+    const std::string path = outdir + "/" + name + ".txt";
+    o.f.open(path, append ? std::ios::app : std::ios::out);
+    if (!o.f) throw std::runtime_error("cannot write " + path);
+    if (headers && !append) o.f << hdr << '\n';
     return o;
   };
-  std::string eh = "t";
-  for (int i = 0; i < Ns; ++i) eh += "    E^kin_scal" + std::to_string(i) + "    E^grad_scal" + std::to_string(i);
-  for (int k = 0; k < Ns; ++k) eh += "    Vpot_term_" + std::to_string(k);
-  eh += "    E_tot";
-  Out en = open("energies", eh);
-  Out cons = open("energy_conservation", expansion ? "t    rel_diff_friedmann    LHS_friedmann    RHS_friedmann"
-                                                   : "t    energy_cons");
+  Out en = open("average_energies", "#" + join(m.energy_headers));
+  Out cons = open("average_energy_conservation", expansion ? "#t    rel_diff_friedmann    LHS_friedmann    RHS_friedmann"
+                                                           : "#t    energy_cons");
   Out sfo;
-  if (expansion) sfo = open("scale_factor", "t    a    aDot    H");
-  std::vector<Out> means;
-  for (int i = 0; i < Ns; ++i)
-    means.push_back(open("scalar_" + std::to_string(i), "t    <phi>    <pi>    <phi^2>    <pi^2>    rms(phi)    rms(pi)"));
+  if (expansion) sfo = open("average_scale_factor", "#t    a    aDot    H");
+  std::vector<Out> means, gauss;
+  for (const auto &name : m.mean_files)
+    means.push_back(open("average_" + name, "#" + join(name.find("U1") != std::string::npos ||
+                                                               name.find("norm_SU2_") != std::string::npos
+                                                           ? host::means_header_eb()
+                                                           : host::means_header())));
+  for (const auto &name : m.gauss_files)
+    gauss.push_back(open("average_" + name, "#t    av|LHS-RHS|_over_av|LHS+RHS|    av|LHS|    av|RHS|"));
+  std::vector<Out> spec;
+  for (const auto &s : m.spectra) {
+    std::string hdr = "1:binCentralValue";
+    for (size_t c = 0; c < s.columns.size(); ++c) hdr += " " + std::to_string(c + 2) + ":PS";
+    spec.push_back(open("spectra_" + s.name, hdr));
+  }
 
   // ---- the time loop (cosmolattice.cpp:168-201)
-  double t = t0, e0 = 0.0;
+  double e0 = 0.0;
   bool have_e0 = false;
+  std::vector<double> bins(nbins), acc(nbins);
   for (int64_t i = 0; t < tMax - dt / 2.0;) {
-    if (i % outFreq == 0) {
-      check(h, clb_sync(h), "clb_sync");
-      clb_measurement m{};
-      check(h, clb_measure(h, have_e0 ? e0 : 1.0, &m), "clb_measure");
+    const bool freq = i % outFreq == 0, infreq = i % specFreq == 0;
+    if (freq || infreq) check(h, clb_sync(h), "clb_sync");
+    if (freq) {
+      clb_measurement mm{};
+      check(h, clb_measure(h, have_e0 ? e0 : 1.0, &mm), "clb_measure");
       if (!have_e0) {
-        e0 = m.energies[m.n_energies - 1];
+        e0 = mm.energies[mm.n_energies - 1];
         have_e0 = true;
-        if (!expansion) m.friedmann[0] = 0.0;
+        if (!expansion) mm.friedmann[0] = 0.0;
       }
       std::vector<double> row{t};
-      row.insert(row.end(), m.energies, m.energies + m.n_energies);
+      row.insert(row.end(), mm.energies, mm.energies + mm.n_energies);
       en.row(row);
-      if (expansion) cons.row({t, m.friedmann[0], m.friedmann[1], m.friedmann[2]});
-      else cons.row({t, m.friedmann[0]});
-      if (expansion) sfo.row({t, m.aI, m.aDotI, m.hubble});
-      for (int f = 0; f < Ns; ++f) {
+      if (expansion) cons.row({t, mm.friedmann[0], mm.friedmann[1], mm.friedmann[2]});
+      else cons.row({t, mm.friedmann[0]});
+      if (expansion) sfo.row({t, mm.aI, mm.aDotI, mm.hubble});
+      for (size_t f = 0; f < means.size() && (int)f < mm.n_means; ++f) {
         std::vector<double> r{t};
-        r.insert(r.end(), m.means[f], m.means[f] + 6);
+        r.insert(r.end(), mm.means[f], mm.means[f] + 6);
         means[f].row(r);
       }
+      if (!gauss.empty()) gauss[0].row({t, mm.gauss_u1[0], mm.gauss_u1[1], mm.gauss_u1[2]});
+      if (gauss.size() > 1) gauss[1].row({t, mm.gauss_su2[0], mm.gauss_su2[1], mm.gauss_su2[2]});
     }
-    int64_t n = outFreq - i % outFreq;
+    if (infreq) {
+      for (size_t s = 0; s < m.spectra.size(); ++s) {
+        std::vector<std::vector<double>> cols;
+        for (const auto &group : m.spectra[s].columns) {
+          std::fill(acc.begin(), acc.end(), 0.0);
+          for (const auto &[which, comp] : group) {
+            check(h, clb_spectrum(h, which, comp, psType, psVersion, dk, nbins, 1, nullptr, bins.data(), nullptr),
+                  "clb_spectrum");
+            for (int b = 0; b < nbins; ++b) acc[b] += bins[b];
+          }
+          cols.push_back(acc);
+        }
+        for (int b = 0; b < nbins; ++b) {
+          std::vector<double> r{(b + 0.5) * dk * kIR};
+          for (const auto &c : cols) r.push_back(c[b]);
+          spec[s].row(r, " ");
+        }
+        spec[s].f << '\n';
+        spec[s].f.flush();
+      }
+    }
+    int64_t n = std::min(outFreq - i % outFreq, specFreq - i % specFreq);
+    if (backupFreq) n = std::min(n, backupFreq - i % backupFreq);
     const int64_t n_left = std::llround((tMax - t) / dt);
     n = std::max<int64_t>(1, std::min(n, n_left));
     check(h, clb_evolve(h, n), "clb_evolve");
     t += n * dt;
     i += n;
+    if (backupFreq && i % backupFreq == 0) { // simulationmanager.h:143-149
+      const std::string path = par.str("backupPath", outdir) + "/" + m.name + "_backup.clb";
+      if (std::filesystem::exists(path)) std::filesystem::rename(path, path + "~");
+      save_sim(h, m, N, t, par, path);
+    }
   }
+  if (par.has("saveFile")) save_sim(h, m, N, t, par, par.str("saveFile", ""));
   double ms = 0;
   clb_last_evolve_ms(h, &ms);
-  std::printf("lphi4 N=%d %s: t = %.6g, last evolve %.3f ms\n", N, par.str("evolver", "LF").c_str(), t, ms);
-  clb_destroy(h);
+  std::printf("%s N=%d %s: t = %.6g, last evolve %.3f ms\n", m.name.c_str(), N, par.str("evolver", "LF").c_str(), t, ms);
   return 0;
 } catch (const std::exception &e) {
   std::fprintf(stderr, "cosmolattice_b200: %s\n", e.what());

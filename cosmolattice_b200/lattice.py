@@ -117,8 +117,10 @@ class Lattice:
         sfd = {k: getattr(sf, k) for k, _ in _capi.ScaleFactor._fields_}
         return f, p, sfd
 
-    def initialize(self, correct_adot: bool = True) -> None:
-        self._check(self.lib.clb_initialize(self.h, 1 if correct_adot else 0))
+    def initialize(self, correct_adot: bool = True, restart: bool = False) -> None:
+        """clb_initialize; restart: the state is a restarted one (CLB_INIT_RESTART)."""
+        mode = _capi.CLB_INIT_RESTART if restart else (1 if correct_adot else 0)
+        self._check(self.lib.clb_initialize(self.h, mode))
 
     def evolve(self, n_steps: int) -> None:
         self._check(self.lib.clb_evolve(self.h, int(n_steps)))
@@ -326,19 +328,28 @@ class Measurer:
         """Names of the per-field means files, in the order of the measurement's means rows
         (scalarsingletmeasurer.h, complexscalarmeasurer.h:40-52, u1measurer.h:45-55)."""
         m = self.model
+        if getattr(m, "NSU2", 0):  # + su2doubletmeasurer.h:42, su2measurer.h:39
+            return ["scalar_0", "cmplx_scalar_0_0", "cmplx_scalar_0_1", "norm_cmplx_scalar_0", "norm_SU2Doublet_0",
+                    "norm_U1_0", "norm_SU2_0"]
         if getattr(m, "NU1", 0):
             return ["cmplx_scalar_0_0", "cmplx_scalar_0_1", "norm_cmplx_scalar_0", "norm_U1_0"]
         return [f"scalar_{i}" for i in range(m.Ns)]
 
     def _headers(self):
+        # energiesmeasurer.h:127-150: singlets, complex scalars, SU(2) doublets, U(1), SU(2), the
+        # potential terms, E_tot
         m = self.model
         en = ["t"]
         for i in range(m.Ns):
             en += [f"E^kin_scal{i}", f"E^grad_scal{i}"]
         for i in range(getattr(m, "NCs", 0)):
             en += [f"E^kin_cmplxscal{i}", f"E^grad_cmplxscal{i}"]
+        for i in range(getattr(m, "NSU2Doublet", 0)):
+            en += ["E^kin_SU2matter", "E^grad_SU2matter"]
         for i in range(getattr(m, "NU1", 0)):
             en += [f"E^kin_U1{i}", f"E^grad_U1{i}"]
+        for i in range(getattr(m, "NSU2", 0)):
+            en += ["E^kin_SU2", "E^grad_SU2"]
         en += [f"Vpot_term_{k}" for k in range(m.NPotTerms)] + ["E_tot"]
         cons = ["t"] + (["rel_diff_friedmann", "LHS_friedmann", "RHS_friedmann"] if self.rp.expansion else ["energy_cons"])
         means = ["t", "<phi>", "<pi>", "<phi^2>", "<pi^2>", "rms(phi)", "rms(pi)"]
@@ -347,10 +358,13 @@ class Measurer:
             "energies": en,
             "energy_conservation": cons,
             "scale_factor": ["t", "a", "aDot", "H"],
-            **{name: (means_eb if name.startswith("norm_U1") else means) for name in self._mean_files()},
+            **{name: (means_eb if name.startswith(("norm_U1", "norm_SU2_")) else means) for name in self._mean_files()},
         }
+        gauss = ["t", "av|LHS-RHS|_over_av|LHS+RHS|", "av|LHS|", "av|RHS|"]
         if getattr(m, "NU1", 0):
-            h["gauss_U1_0"] = ["t", "av|LHS-RHS|_over_av|LHS+RHS|", "av|LHS|", "av|RHS|"]
+            h["gauss_U1_0"] = gauss
+        if getattr(m, "NSU2", 0):
+            h["gauss_SU2_0"] = gauss
         return h
 
     def _write(self, name: str, values: List[float]) -> None:
@@ -383,7 +397,7 @@ class Measurer:
         if getattr(m, "NSU2", 0):
             return [("scalar_0", [(0, 0)], [(1, 0)]),
                     ("norm_cmplx_scalar_0", [(0, 1), (0, 2)], [(1, 1), (1, 2)]),
-                    ("norm_SU2Doublet_0", [(0, c) for c in range(3, 7)], [(1, c) for c in range(3, 7)]),
+                    ("norm_SU2Doublet_scalar_0", [(0, c) for c in range(3, 7)], [(1, c) for c in range(3, 7)]),
                     ("norm_U1_0", [(1, 7), (1, 8), (1, 9)], None)]
         if getattr(m, "NU1", 0):
             return [("norm_cmplx_scalar_0", [(0, 0), (0, 1)], [(1, 0), (1, 1)]),
@@ -444,6 +458,8 @@ class Measurer:
             self._write(name, [t] + row)
         if getattr(self.model, "NU1", 0):
             self._write("gauss_U1_0", [t] + m["gauss_u1"])
+        if getattr(self.model, "NSU2", 0):
+            self._write("gauss_SU2_0", [t] + m["gauss_su2"])
         return m
 
     def close(self) -> None:
@@ -452,14 +468,18 @@ class Measurer:
         self.files = {}
 
 
-def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fused", outdir: Optional[str] = None):
-    """The reference main loop (source/cosmolattice.cpp:168-201) over the GPU library."""
+def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fused", outdir: Optional[str] = None,
+        lattice_factory=None):
+    """The reference main loop (source/cosmolattice.cpp:168-201) over the GPU library.
+    lattice_factory(model, rp), if given, makes the lattice the loop drives instead (an object with
+    Lattice's set_state / initialize / evolve / sync / measure / spectrum)."""
     from .models import MODELS
     from .params import RunParameters
 
     rp = RunParameters(par)
     model = MODELS[model_name](par, rp)
-    lattice = Lattice(model, rp, precision=precision, path=path)
+    lattice = (lattice_factory(model, rp) if lattice_factory is not None
+               else Lattice(model, rp, precision=precision, path=path))
     measurer = Measurer(model, rp, outdir)
     ModelInitializer(model, rp.lSide, rp.baseSeed).initialize(model, rp, lattice)
     evolver = Evolver(model, rp, lattice)

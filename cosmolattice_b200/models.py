@@ -187,6 +187,61 @@ class lphi4_1f(lphi4):
     NPotTerms = 1
 
 
+class tanh2(Model):
+    """models/tanh2.h: an inflaton phi with a T-model potential and a daughter field chi,
+    V = (M/phi_i)^2 tanh^2(phi phi_i/M) / 2 + q/2 phi^2 chi^2 in program variables.
+
+    Keys: M, Lambda4, q, initial_amplitudes (2 values, GeV), initial_momenta (2 values).
+    Rescaling (tanh2.h constructor): alpha = 0, fStar = phi_i = initial_amplitudes[0],
+    omegaStar = sqrt(Lambda4 / M^2).  The device kernels take the potential from the tanh2 model
+    header (cosmolattice_b200/csrc/models/tanh2.h): the library built with it
+    (lib/tanh2/libclb200.so) runs this model, selected by CLB200_SCALAR_MODEL=tanh2.
+    """
+
+    name = "tanh2"
+    scalar_header = "tanh2"
+    kind = _capi.MODEL_LPHI4  # the scalar-singlet kind: the header the library is built with
+    Ns = 2
+    NPotTerms = 2
+
+    def __init__(self, par: ParameterParser, rp: RunParameters):
+        super().__init__(par, rp)
+        self.M = par.get_float("M")
+        self.Lambda4 = par.get_float("Lambda4")
+        self.q = par.get_float("q")
+        self.fldS0 = par.get_floats("initial_amplitudes", self.Ns)
+        self.piS0 = par.get_floats("initial_momenta", self.Ns, [0.0] * self.Ns)
+        phii = self.fldS0[0]
+        self.alpha = 0.0
+        self.fStar = phii
+        self.omegaStar = math.sqrt(self.Lambda4 / self.M ** 2)
+        self.mu = self.M / phii
+        if par.has("fluct_amplitude"):
+            self.fluct_amplitude = par.get_float("fluct_amplitude")
+        self.set_initial_potential_and_masses_from_potential()
+
+    def potential_terms(self, k, phi):
+        if k == 0:
+            return self.mu ** 2 * math.tanh(phi[0] / self.mu) ** 2 / 2
+        return 0.5 * self.q * phi[0] ** 2 * phi[1] ** 2
+
+    def pot_deriv(self, n, phi):
+        if n == 0:
+            x = phi[0] / self.mu
+            return 2 * self.mu * math.tanh(x) ** 2 / math.sinh(2 * x) + self.q * phi[0] * phi[1] ** 2
+        return self.q * phi[1] * phi[0] ** 2
+
+    def pot_deriv2(self, n, phi):
+        if n == 0:
+            x = phi[0] / self.mu
+            return (4 * (2 - math.cosh(2 * x)) * math.tanh(x) ** 2 / math.sinh(2 * x) ** 2
+                    + self.q * phi[1] ** 2)
+        return self.q * phi[0] ** 2
+
+    def couplings(self):
+        return [self.mu, self.q]
+
+
 class lphi4U1(Model):
     """models/lphi4U1.h: one complex scalar charged under one U(1), V = |phi|^4 in program variables.
 
@@ -343,4 +398,4 @@ class lphi4SU2U1(Model):
         return [self.qG, self.qH, self.gQ_C, self.gQ_D, self.gQ_S, self.c4]
 
 
-MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f, "lphi4U1": lphi4U1, "lphi4SU2U1": lphi4SU2U1}
+MODELS = {"lphi4": lphi4, "lphi4_1f": lphi4_1f, "lphi4U1": lphi4U1, "lphi4SU2U1": lphi4SU2U1, "tanh2": tanh2}

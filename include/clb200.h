@@ -188,9 +188,14 @@ int clb_generate_state(clb_handle *h, const clb_ic_params *p, const clb_scalefac
 int clb_get_state(clb_handle *h, double *fields, double *momenta, clb_scalefactor *sf);
 
 /* Finish initialisation: volume averages of the state (Averages::setAllAverages, averages.h:349-392),
- * and with self-consistent expansion aDot_I = sqrt(Friedmann RHS) if correct_adot != 0
+ * and with self-consistent expansion aDot_I = sqrt(Friedmann RHS) if correct_adot == 1
  * (modelinitializer.h:74-80).  Then applies the evolver constructor: for LF,
- * aDot_SI = aDot_I - dt/2 F (leapfrog.h:35) and the synced flag. */
+ * aDot_SI = aDot_I - dt/2 F (leapfrog.h:35) and the synced flag.
+ * correct_adot == CLB_INIT_RESTART: the state is a restarted one (SimulationManager::loadSim,
+ * simulationmanager.h:69-100, then the evolver's constructor with doWeRestart set): averages only,
+ * no aDot correction, and the leapfrog starts unsynced, its momenta at the half step
+ * (leapfrog.h:30-36); not with a fixed background (CLB_EUNSUPPORTED). */
+#define CLB_INIT_RESTART 2
 int clb_initialize(clb_handle *h, int32_t correct_adot);
 
 /* Advance n_steps time steps of dt: n_steps calls of Evolver::evolve (evolver.h:102-124). */
@@ -354,9 +359,9 @@ int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t s
 int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
- * For callers that cannot call cudaMalloc: a runtime that owns the whole device memory pool, code
- * issued while a CUDA graph is being captured, or an embedding that forbids allocation after
- * start-up.  Computes, for FP64 scalar-singlet lattices already in device memory, the volume
+ * For callers that cannot call cudaMalloc: a host runtime that owns the whole device memory pool
+ * and hands out no more, or an embedding that forbids device allocation after start-up (a service
+ * with a fixed memory budget).  Computes, for FP64 scalar-singlet lattices already in device memory, the volume
  * averages d_out[0] = <sum_f pi_f^2>, d_out[1] = <sum_f grad^2 phi_f>, d_out[2] = <V> (lphi4:
  * V = c0/4 phi^4 + q/2 phi^2 chi^2), the same sums clb_initialize and clb_measure form.
  * d_fields / d_momenta: n_scalars x N^3 doubles each (layout of clb_set_state) on the current
@@ -364,8 +369,9 @@ int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out);
  * Allocates nothing: the block partials live in a fixed 192 KiB device array that every GPU
  * loading the library keeps until exit, so N is limited to 1024 (larger N returns CLB_EINVAL with
  * the reason in clb_last_error(NULL)).  The first call on a device looks up that array's address
- * (cudaGetSymbolAddress) with the device current; make that first call before any stream capture.
- * Calls return once their work is enqueued.  All calls share the array: calls that overlap on the
+ * (cudaGetSymbolAddress) with the device current, and again in a new context after a
+ * cudaDeviceReset; make that first call before any stream capture.  A CUDA error left pending by
+ * earlier work is reported (CLB_ECUDA) and left in place.  Calls return once their work is enqueued.  All calls share the array: calls that overlap on the
  * GPU (other streams or host threads) race and must be serialised by the caller. */
 int clb_scalar_averages_noalloc(const double *d_fields, const double *d_momenta, int32_t N, int32_t n_scalars,
                                 double dx, double c0, double q, double *d_out, void *stream);

@@ -108,10 +108,20 @@ struct Oracle {
   double c0() const { return md.couplings[0]; }
   double q() const { return md.couplings[1]; }
 
-  // potentialTerms(Tag<0>) = 0.25 * pow<4>(phi);  Tag<1> = 0.5 * q * pow<2>(phi * chi)
+  // The scalar-singlet model: 0 lphi4 (above), 1 tanh2 (models/tanh2.h), set by orc_set_scalar_model.
+  // tanh2 couplings: mu = M / phi_i = couplings[0], q = couplings[1]; x = phi / mu.
+  int scalar_model = 0;
+  double mu() const { return md.couplings[0]; }
+
+  // lphi4 potentialTerms(Tag<0>) = 0.25 * pow<4>(phi);  Tag<1> = 0.5 * q * pow<2>(phi * chi)
+  // tanh2 potentialTerms(Tag<0>) = pow<2>(M/phi_i) pow<2>(tanh(phi phi_i/M)) / 2 (tanh2.h)
   double potTerm(int k, size_t s) const
   {
     const double p = fld[s];
+    if (k == 0 && scalar_model == 1) {
+      const double t = std::tanh(p * (1.0 / mu()));
+      return ((mu() * mu()) * (t * t)) * 0.5;
+    }
     if (k == 0) return (0.25 * c0()) * ipow(p, 4);
     const double c = fld[n3 + s];
     return (0.5 * q()) * ipow(p * c, 2);
@@ -123,12 +133,20 @@ struct Oracle {
     return v;
   }
   // potDeriv(Tag<0>) = pow<3>(phi) + q * phi * pow<2>(chi);  Tag<1> = q * chi * pow<2>(phi)
+  // tanh2 potDeriv(Tag<0>) = 2 (M/phi_i) pow<2>(tanh(x)) / sinh(2 x) + q phi chi^2 (tanh2.h)
   double potDeriv(int f, size_t s) const
   {
     const double p = fld[s];
-    if (Ns == 1) return c0() * ipow(p, 3);
+    double d0;
+    if (scalar_model == 1) {
+      const double x = p * (1.0 / mu()), t = std::tanh(x);
+      d0 = ((2 * mu()) * (t * t)) / std::sinh(2 * x);
+    } else {
+      d0 = c0() * ipow(p, 3);
+    }
+    if (Ns == 1) return d0;
     const double c = fld[n3 + s];
-    if (f == 0) return c0() * ipow(p, 3) + (q() * p) * ipow(c, 2);
+    if (f == 0) return d0 + (q() * p) * ipow(c, 2);
     return (q() * c) * ipow(p, 2);
   }
 
@@ -499,6 +517,15 @@ void orc_destroy(orc_handle *h)
   else
     delete S(h);
   delete H(h);
+}
+
+// Selects the scalar-singlet potential restated above: 0 lphi4, 1 tanh2 (scalar-singlet handles).
+int orc_set_scalar_model(orc_handle *h, int32_t id)
+{
+  if (!h || (id != 0 && id != 1)) return CLB_EINVAL;
+  if (isU1(h) || isSU2(h)) return CLB_EUNSUPPORTED;
+  S(h)->scalar_model = id;
+  return CLB_OK;
 }
 
 int orc_set_state(orc_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)

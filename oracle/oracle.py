@@ -43,6 +43,7 @@ def load():
             "orc_sync": (C.c_int, [H]),
             "orc_measure": (C.c_int, [H, C.c_double, C.POINTER(capi.Measurement)]),
             "orc_num_threads": (C.c_int, []),
+            "orc_set_scalar_model": (C.c_int, [H, C.c_int32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -84,6 +85,8 @@ class OracleLattice:
         if rc != 0:
             raise RuntimeError(self.lib.orc_last_error(None).decode())
         self.h = h
+        if getattr(model, "scalar_header", "lphi4") == "tanh2":  # the tanh2 potential restated in oracle.cpp
+            self._check(self.lib.orc_set_scalar_model(self.h, 1))
         self.n_components = getattr(model, "n_components", model.Ns)
         self.n_momentum_components = getattr(model, "n_momentum_components", self.n_components)
 

@@ -92,3 +92,32 @@ def gpu_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+# Per-site parity metrics.  The state is a homogeneous value plus small fluctuations (phi ~ 1 with
+# fluctuations ~1e-3 in the scalar cases), so an error bar relative to an array's maximum checks
+# the fluctuations only to that ratio.  Two bars see them:
+#   fluct: max |a - b| over a component, relative to max |b - <b>| (the fluctuations' own scale);
+#   site:  max |a - b| / |b| over the sites where |b| >= SITE_FLOOR * max |b| (a true per-site
+#          relative error; below the floor a value's relative error measures only its smallness).
+SITE_FLOOR = 1e-1
+
+
+def site_metrics(a, b, nc, floor=SITE_FLOOR):
+    """(site, fluct) errors of a against b, each the worst over the nc components."""
+    import numpy as np
+
+    a = np.asarray(a).reshape(nc, -1)
+    b = np.asarray(b).reshape(nc, -1)
+    site = fluct = 0.0
+    for c in range(nc):
+        sc = np.abs(b[c]).max()
+        if sc == 0:
+            continue
+        d = np.abs(a[c] - b[c])
+        m = np.abs(b[c]) >= floor * sc
+        site = max(site, float((d[m] / np.abs(b[c][m])).max()))
+        fs = np.abs(b[c] - b[c].mean()).max()
+        if fs > 0:
+            fluct = max(fluct, float(d.max() / fs))
+    return site, fluct

@@ -54,3 +54,23 @@ def test_version_and_error_without_gpu():
     cfg.evolver = 1
     cfg.dt = 0.0
     assert lib.clb_create(ctypes.byref(cfg), ctypes.byref(md), ctypes.byref(h)) == _capi.CLB_EINVAL
+
+
+def test_scalar_model_variants_export_the_same_symbols():
+    # each scalar-singlet model header the build compiles besides lphi4 (csrc/models/) gives a
+    # complete library of its own
+    from cosmolattice_b200.build import SCALAR_VARIANTS, variant_lib
+
+    for name in SCALAR_VARIANTS:
+        lib = ctypes.CDLL(variant_lib(name))
+        missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
+        assert not missing, (name, missing)
+
+
+def test_model_headers_have_the_reference_shape():
+    # every model header defines potentialTerms, potDeriv and potDeriv2 per Tag, like the
+    # reference's headers (models/lphi4.h:154-226, models/tanh2.h)
+    for name in ("lphi4", "tanh2"):
+        text = open(os.path.join(ROOT, "cosmolattice_b200", "csrc", "models", f"{name}.h")).read()
+        for fn in ("potentialTerms", "potDeriv", "potDeriv2"):
+            assert f"{fn}(Tag<0>" in text and f"{fn}(Tag<1>" in text, (name, fn)

@@ -1,18 +1,24 @@
 """Parity of the CUDA lphi4SU2U1 path with the FP64 CPU oracle (B200).
 
-Same bars as the other sectors: per-site fields and momenta within 1e-12 relative (to each
-component's max |value|) after 100 steps; a(t), aDot, energies, means and the Gauss averages
+Same bars as lphi4U1: per-site fields and momenta after 100 steps within 1e-12 of each
+component's max |value|, within 2e-12 of its fluctuations max |x - <x>|, and within 1e-11 of each
+site's own value where it exceeds 1e-1 of that max (conftest.site_metrics; measured 9e-13); the
+same with the 384^3 workload's couplings and time step at 64^3; a(t), aDot, energies, means and the Gauss averages
 within 1e-10 relative, the Gauss ratios within 1e-8 relative (difference of nearly equal
 terms).  Both Gauss laws are preserved per site on the GPU too.
 """
+import math
+
 import numpy as np
 import pytest
 
-from conftest import make_su2_case
+from conftest import make_su2_case, site_metrics
 
 pytestmark = pytest.mark.gpu
 
 SITE_TOL = 1e-12
+FLUCT_TOL = 2e-12
+SITE_REL_TOL = 1e-11
 AVG_TOL = 1e-10
 RATIO_TOL = 1e-8
 
@@ -38,11 +44,11 @@ def random_links(f, rng, s=0.1):
     return f
 
 
-def run_pair(N, evolver, expansion, nsteps, measure_every=None, links=False, extra=None):
+def run_pair(N, evolver, expansion, nsteps, measure_every=None, links=False, extra=None, amp=3e-2):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = make_su2_case(N=N, evolver=evolver, expansion=expansion, amp=3e-2, extra=extra)
+    par, rp, m, f, p, sf = make_su2_case(N=N, evolver=evolver, expansion=expansion, amp=amp, extra=extra)
     if links:
         f = random_links(f, np.random.default_rng(4))
     gpu = Lattice(m, rp)
@@ -75,6 +81,10 @@ def check(g, c, meas):
     (fg, pg, sg), (fc, pc, sc) = g, c
     assert rel_comp(fg, fc, 22) < SITE_TOL, rel_comp(fg, fc, 22)
     assert rel_comp(pg, pc, 19) < SITE_TOL, rel_comp(pg, pc, 19)
+    for what, a, b, nc in (("fields", fg, fc, 22), ("momenta", pg, pc, 19)):
+        site, fluct = site_metrics(a, b, nc)
+        assert site < SITE_REL_TOL, (what, "per-site", site)
+        assert fluct < FLUCT_TOL, (what, "fluctuations", fluct)
     for k in ("aI", "aDotI"):
         assert abs(sg[k] - sc[k]) <= AVG_TOL * max(abs(sc[k]), 1e-300), (k, sg[k], sc[k])
     for a, b in zip(meas["gpu"], meas["cpu"]):
@@ -85,8 +95,14 @@ def check(g, c, meas):
             assert abs(a["friedmann"][k] - b["friedmann"][k]) <= AVG_TOL * abs(b["friedmann"][k]) + 1e-300
         assert len(a["means"]) == len(b["means"]) == 7
         for ra, rb in zip(a["means"], b["means"]):
+            # the mean of |B| of SU(2) takes sqrt(B^2) per site as the reference does
+            # (su2measurer.h:62); near unit links B^2 can round below zero, and both sides then
+            # report NaN in the same place
+            assert [math.isnan(x) for x in ra] == [math.isnan(y) for y in rb], (ra, rb)
             scales = [max(abs(rb[0]), rb[4]), max(abs(rb[1]), rb[5]), abs(rb[2]), abs(rb[3])]
             for x, y, s in zip(ra[:4], rb[:4], scales):
+                if math.isnan(y):
+                    continue
                 assert abs(x - y) <= AVG_TOL * max(s, 1e-300) + 1e-30, (ra, rb)
         for key in ("gauss_u1", "gauss_su2"):
             ga, gb = a[key], b[key]
@@ -98,6 +114,13 @@ def check(g, c, meas):
 @pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV2", False), ("VV4", True), ("LF", True)])
 def test_lphi4su2u1_100_steps(evolver, expansion):
     g, c, meas = run_pair(8, evolver, expansion, 100)
+    check(g, c, meas)
+
+
+def test_lphi4su2u1_workload_couplings_64_vv2_100_steps():
+    # the 384^3 workload's couplings (gSU2 = 0.6, gU1 = 0.35, qG = qH = 50, lambda = 1), time step
+    # (0.005), evolver (VV2), expansion and amplitude (1e-3) on a 64^3 lattice, 100 steps
+    g, c, meas = run_pair(64, "VV2", True, 100, amp=1e-3)
     check(g, c, meas)
 
 

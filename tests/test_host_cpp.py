@@ -77,3 +77,109 @@ def test_host_matches_python_over_the_abi(tmp_path, evolver, extra):
     assert host_en.shape == py_en.shape and host_sf.shape == py_sf.shape
     assert np.allclose(host_en, py_en, rtol=1e-13, atol=0)
     assert np.allclose(host_sf, py_sf, rtol=1e-13, atol=0)
+
+
+GAUGE = {
+    "lphi4U1": {"N": 12, "kIR": 1.0, "dt": 0.01, "tMax": 0.3, "tOutputFreq": 0.05, "tOutputInfreq": 0.1,
+                "evolver": "VV2", "expansion": "true", "lambda": 1.0, "cmplx_field_initial_norm": "5.6964e18",
+                "gU1s": 0.5, "fluct_amplitude": 1e-2, "kCutOff": 3.0, "baseSeed": "host"},
+    "lphi4SU2U1": {"N": 8, "kIR": 1.0, "dt": 0.005, "tMax": 0.15, "tOutputFreq": 0.025, "tOutputInfreq": 0.05,
+                   "evolver": "VV2", "expansion": "true", "lambda": 1.0, "qG": 50, "qH": 50,
+                   "SU2Doublet_initial_norm": "5.25151e18", "gU1s": 0.35, "gSU2s": 0.6, "fluct_amplitude": 1e-2,
+                   "kCutOff": 2.0, "baseSeed": "host"},
+}
+
+
+def _python_files(model_name, params, seed, outdir):
+    """The same run driven from Python over the ABI: device initial state with the same seed, the
+    reference's cadence, files written by lattice.Measurer."""
+    from cosmolattice_b200 import MODELS, Lattice, ParameterParser, RunParameters
+    from cosmolattice_b200.initializers import device_ic_params
+    from cosmolattice_b200.lattice import Measurer, c_round
+
+    par = ParameterParser(params=dict(params, print_headers="true"))
+    rp = RunParameters(par)
+    m = MODELS[model_name](par, rp)
+    lat = Lattice(m, rp)
+    p, aI, aD = device_ic_params(m, rp, seed=seed)
+    lat.generate_state(p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
+    lat.initialize(correct_adot=True)
+    meas = Measurer(m, rp, outdir)
+    t, i = rp.t0, 0
+    while t < rp.tMax - rp.dt / 2.0:
+        if i % meas.outputFreq == 0 or i % meas.spectraFreq == 0:
+            lat.sync()
+        if i % meas.outputFreq == 0:
+            meas.measure(i, t, lat)
+        if i % meas.spectraFreq == 0:
+            meas.measure_spectra(t, lat)
+        n = min(meas.outputFreq - i % meas.outputFreq, meas.spectraFreq - i % meas.spectraFreq)
+        n = max(1, min(n, c_round((rp.tMax - t) / rp.dt)))
+        lat.evolve(n)
+        t += n * rp.dt
+        i += n
+    meas.close()
+    lat.close()
+
+
+def _numbers(path):
+    rows = []
+    for line in open(path):
+        if line.strip() and not line.startswith("#") and not line.startswith("1:"):
+            rows.append([float(x) for x in line.split()])
+    return np.array(rows)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", list(GAUGE))
+def test_host_gauge_models_match_python(tmp_path, model):
+    # every file the host writes for the gauge models (energies, Friedmann, scale factor, the means
+    # of every field, both Gauss laws, the spectra) equals the Python-driven run's file of the same
+    # name, line by line, within 1e-13 of each column's largest value (NaN where the reference's
+    # sqrt of a rounded-negative SU(2) B^2 gives one, on both sides)
+    params = GAUGE[model]
+    seed = 11
+    hdir, pdir = tmp_path / "host", tmp_path / "py"
+    hdir.mkdir()
+    args = [f"{k}={v}" for k, v in params.items()] + [f"model={model}", f"outputfile={hdir}", f"deviceSeed={seed}",
+                                                      "print_headers=true"]
+    r = subprocess.run([built()] + args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    _python_files(model, params, seed, str(pdir))
+    hfiles, pfiles = sorted(os.listdir(hdir)), sorted(os.listdir(pdir))
+    assert hfiles == pfiles
+    for name in hfiles:
+        assert open(hdir / name).readline() == open(pdir / name).readline(), name  # same header
+        a, b = _numbers(hdir / name), _numbers(pdir / name)
+        assert a.shape == b.shape, name
+        assert np.array_equal(np.isnan(a), np.isnan(b)), name
+        # each column within 1e-13 of its largest magnitude: the two hosts form the initial-state
+        # masses in their own operation order, so values that average to zero differ by 1e-19
+        scale = np.nanmax(np.abs(b), axis=0, keepdims=True)
+        assert np.all(np.nan_to_num(np.abs(a - b)) <= 1e-13 * scale), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model,evolver", [("lphi4", "VV2"), ("lphi4U1", "LF"), ("lphi4SU2U1", "VV2")])
+def test_host_restart_continues_the_run(tmp_path, model, evolver):
+    # a run saved half way (saveFile) and restarted from the file (restart = true) writes, for the
+    # second half, the rows that the uninterrupted run writes
+    params = dict(GAUGE.get(model, PARAMS), evolver=evolver)
+    dt = float(params["dt"])
+    t_half = 10 * dt
+    base = [f"{k}={v}" for k, v in params.items() if k != "tMax"] + [f"model={model}", "deviceSeed=5",
+                                                                      f"tOutputFreq={5 * dt}", f"tOutputInfreq={5 * dt}"]
+    whole, first, second = tmp_path / "whole", tmp_path / "first", tmp_path / "second"
+    for d in (whole, first, second):
+        d.mkdir()
+    path = tmp_path / "half.clb"
+    runs = [base + [f"tMax={2 * t_half}", f"outputfile={whole}"],
+            base + [f"tMax={t_half}", f"outputfile={first}", f"saveFile={path}"],
+            base + [f"tMax={2 * t_half}", f"outputfile={second}", "restart=true", f"restartFile={path}"]]
+    for args in runs:
+        r = subprocess.run([built()] + args, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+    a = _numbers(whole / "average_energies.txt")
+    b = _numbers(second / "average_energies.txt")
+    assert len(b) == 2 and np.allclose(a[-2:, 0], b[:, 0], rtol=1e-15)  # t = 10 dt, 15 dt
+    assert np.allclose(a[-2:], b, rtol=1e-11, atol=0)

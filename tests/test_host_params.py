@@ -102,3 +102,48 @@ def test_output_cadence_rounds_halves_away_from_zero():
 
     assert [c_round(x) for x in (2.5, 3.5, 0.5, 2.49, 10.000000000000002, -2.5)] == [3, 4, 1, 2, 10, -3]
     assert round(2.5) == 2  # the rounding this replaces
+
+
+def test_restart_file_round_trip(tmp_path):
+    # save_sim / load_sim over a stand-in lattice (no GPU): every array, the six scale-factor
+    # values and the time come back bitwise, in the reference's sector order, and a file of
+    # another model or size is refused
+    import numpy as np
+
+    from conftest import make_su2_case
+    from cosmolattice_b200 import restart
+
+    par, rp, m, f, p, sf = make_su2_case(N=4)
+    sf = dict(sf, aDotSIM=0.25)
+
+    class Stand:
+        def __init__(self):
+            self.rp = rp
+            self.state = None
+            self.mode = None
+
+        def get_state(self):
+            return f.ravel(), p.ravel(), dict(sf)
+
+        def set_state(self, F, P, s):
+            self.state = (F.copy(), P.copy(), dict(s))
+
+        def initialize(self, restart=False):
+            self.mode = restart
+
+    path = str(tmp_path / "run.clb")
+    restart.save_sim(path, Stand(), m, 1.5, {"N": 4, "dt": 0.005})
+    st = Stand()
+    t, text = restart.load_sim(path, st, m)
+    F, P, s = st.state
+    assert t == 1.5 and "dt = 0.005" in text and st.mode is True
+    assert np.array_equal(F.ravel(), f.ravel()) and np.array_equal(P.ravel(), p.ravel())
+    assert all(s[k] == sf[k] for k in restart.SCALARS)
+    # sector order on disk: S field, S momentum, phi fields, phi momenta, ...
+    raw = np.fromfile(path, dtype="<f8", offset=80, count=2 * 64)
+    assert np.array_equal(raw[:64], f.reshape(22, -1)[0]) and np.array_equal(raw[64:], p.reshape(19, -1)[0])
+    par2, rp2, m2, *_ = make_su2_case(N=6)
+    st2 = Stand()
+    st2.rp = rp2
+    with pytest.raises(ValueError):
+        restart.load_sim(path, st2, m2)

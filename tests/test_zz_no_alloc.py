@@ -1,7 +1,7 @@
 """clb_scalar_averages_noalloc: averages of caller-owned device arrays with no device allocation.
 
-It serves callers that cannot call cudaMalloc (a runtime owning the whole memory pool, work
-issued during CUDA-graph capture, embeddings that forbid allocation after start-up).  The
+It serves callers that cannot call cudaMalloc (a host runtime owning the whole device memory
+pool, embeddings that forbid device allocation after start-up).  The
 caller owns the input and output buffers (allocated here by torch); the entry point's block
 partials live in its fixed device array.  Its results must match what the allocating path
 (clb_measure) reports for the same state, within the parity suite's 1e-10 average tolerance, on
