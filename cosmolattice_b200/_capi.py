@@ -144,6 +144,23 @@ class BatchTuning(C.Structure):
     ]
 
 
+class BatchForm(C.Structure):
+    """clb_batch_form."""
+
+    _fields_ = [
+        ("persistent", C.c_int32),
+        ("tile_z", C.c_int32),
+        ("tile_y", C.c_int32),
+        ("sites_per_thread", C.c_int32),
+        ("planes_x", C.c_int32),
+        ("clusters", C.c_int32),
+        ("cluster_blocks", C.c_int32),
+        ("candidates", C.c_int32),
+        ("ms_graph", C.c_double),
+        ("ms_persistent", C.c_double),
+    ]
+
+
 class AdjointGrad(C.Structure):
     """clb_adjoint_grad."""
 
@@ -186,6 +203,11 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_cuda_stream": (C.c_void_p, [H]),
             "clb_spectrum": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
                                        C.c_int32, dp, dp, C.POINTER(C.c_int64)]),
+            "clb_gws_enable": (C.c_int, [H]),
+            "clb_gws_set_state": (C.c_int, [H, dp, dp]),
+            "clb_gws_get_state": (C.c_int, [H, dp, dp]),
+            "clb_gw_spectrum": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                                          dp, dp, C.POINTER(C.c_int64), dp]),
             "clb_forward": (C.c_int, [H, C.c_int64, C.c_int32, dp, C.c_int32, dp]),
             "clb_backward": (C.c_int, [H, C.c_int32, dp, dp, C.POINTER(AdjointGrad)]),
             "clb_generate_state": (C.c_int, [H, C.POINTER(ICParams), C.POINTER(ScaleFactor)]),
@@ -211,6 +233,8 @@ def _declare(lib: C.CDLL, prefix: str) -> None:
             "clb_batch_autotune": (C.c_int, [H, C.c_int32, C.POINTER(BatchTuning)]),
             "clb_batch_set_tuning": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "clb_batch_get_tuning": (C.c_int, [H, C.POINTER(BatchTuning)]),
+            "clb_batch_set_persistent": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+            "clb_batch_get_form": (C.c_int, [H, C.POINTER(BatchForm)]),
         }
         for name, (res, args) in more.items():
             fn = getattr(lib, name)
@@ -278,5 +302,11 @@ EXPORTED = [
     "clb_batch_autotune",
     "clb_batch_set_tuning",
     "clb_batch_get_tuning",
+    "clb_batch_set_persistent",
+    "clb_batch_get_form",
     "clb_scalar_averages_noalloc",
+    "clb_gws_enable",
+    "clb_gws_set_state",
+    "clb_gws_get_state",
+    "clb_gw_spectrum",
 ]

@@ -113,3 +113,15 @@ class LatticeBatch:
         t = _capi.BatchTuning()
         self._check(self.lib.clb_batch_get_tuning(self.h, C.byref(t)))
         return self._tuning_dict(t)
+
+    def set_persistent(self, tile_z: int, tile_y: int, planes_x: int, sites_per_thread: int = 1) -> None:
+        """Run every evolve call as one persistent launch of thread-block clusters with this tile."""
+        self._check(self.lib.clb_batch_set_persistent(self.h, int(tile_z), int(tile_y), int(sites_per_thread),
+                                                      int(planes_x)))
+
+    def form(self) -> Dict[str, object]:
+        """clb_batch_form: persistent or per-stage graph form, the persistent tile and cluster count,
+        and the autotuner's per-step times of both forms."""
+        f = _capi.BatchForm()
+        self._check(self.lib.clb_batch_get_form(self.h, C.byref(f)))
+        return {k: getattr(f, k) for k, _ in _capi.BatchForm._fields_}

@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libclb200.so")
 
-SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_su2.cu", "clb_batch.cu", "clb_noalloc.cu", "clb_ic.cu"]
+SOURCES = ["clb_api.cu", "clb_u1.cu", "clb_su2.cu", "clb_batch.cu", "clb_noalloc.cu", "clb_ic.cu", "clb_gws.cu"]
 # per-unit flags: the lphi4SU2U1 unit writes the reference's rounding order as plain expressions
 UNIT_FLAGS = {"clb_su2.cu": ["-fmad=false"]}
 # every source and header under csrc/: an edit to any of them makes the library stale

@@ -77,6 +77,13 @@ const void *su2_tangent_component(clb_handle *h, int which, int comp, bool *f32,
 const double *u1_component(clb_handle *h, int which, int comp, bool *gauge);
 const double *su2_component(clb_handle *h, int which, int comp, bool *gauge);
 
+// gravitational waves of the scalar singlets (clb_gws.cu)
+void gw_kick_step(clb_handle *h);
+void gw_drift(clb_handle *h);
+void gw_sync(clb_handle *h);
+void gw_set_synced(clb_handle *h, bool s);
+void gw_destroy(clb_handle *h);
+
 // Records a handle-less failure for clb_last_error(NULL); used by entry points in other units.
 __attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_err = m; }
 } // namespace clb
@@ -236,7 +243,7 @@ template <class R, int NS> struct Launch {
   {
     CLB_LAUNCH(h, K_MEASURE,
                k_measure_pad<R, NS><<<kElemBlocks, 256, 0, h->stream>>>(F<R>(h, h->cf), P<R>(h, h->cp), h->pd,
-                                                                        h->sa.inv_dx2, h->sa.mc, am, h->d_st,
+                                                                        h->sa.inv_dx2, h->sa.cs.mc, am, h->d_st,
                                                                         h->rs, h->d_part));
     CLB_LAUNCH(h, K_MEASURE, k_sum_partials<kMeasSlots><<<1, 256, 0, h->stream>>>(h->d_part, kElemBlocks, h->d_sums));
   }
@@ -413,8 +420,12 @@ template <class R, int NS> struct EvolveVV {
     // Fused: the second kick of a stage and the first kick of the next one act with the same
     // kernel K(phi', a) (no field or a update in between), so one sweep drifts phi, forms
     // pi_mid = pi + h1 K and pi_next = pi_mid + h2 K, and reduces <pi_mid^2>, <grad^2>, <V>.
+    // With GWs (evolver.h:102-124): a GW kick before each step at the step's fields and a_I, and
+    // a GW drift after it with the a_SI of its last stage; both after the step's last sweep and
+    // before the tail that moves a on to the next step's first stage.
     const int64_t total = nsteps * (int64_t)S;
     const double w0 = wof(0);
+    if (h->gw) gw_kick_step(h);
     if (ex) tail(h, T_VV_KICK_HALF, 0, 0, w0); // kickScaleFactorHalf
     L::kick(h, w0 * dt / 2);                  // kickScalar with a(t) before the drift
     if (ex) tail(h, T_VV_DRIFT, 0, 0, w0);     // driftScaleFactor
@@ -425,6 +436,8 @@ template <class R, int NS> struct EvolveVV {
       const bool more = k + 1 < total;
       const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
       L::fused(h, dt * w, w * dt / 2, more ? wn * dt / 2 : 0.0, ex);
+      if (h->gw && i + 1 == S) gw_drift(h);
+      if (h->gw && i + 1 == S && more) gw_kick_step(h); // a_I of the step's end, before the tail drifts a
       if (ex) {
         uint32_t fl = T_STORE_PI2_I | T_STORE_FIELDS | T_VV_KICK_ONE;
         if (more) fl |= T_VV_KICK_HALF | T_VV_DRIFT;
@@ -753,7 +766,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   ScalarArgs &a = h->sa;
   a.N = h->N;
   a.inv_dx2 = 1.0 / (cfg->dx * cfg->dx);
-  a.mc = ScalarModel::couplings(md->couplings);
+  a.cs.mc = ScalarModel::couplings(md->couplings);
   // ring depth: as many plane stages as fit in ~48 KiB, at least 3 (planes x, x+1 and one in flight)
   // sweep shape: default per storage type and field count, CLB_SWEEP_SHAPE=0/1/2 overrides (one field)
   h->shape = (h->NS == 1) ? (h->fp32 ? kDefaultShapeFP32 : kDefaultShapeFP64) : 0;
@@ -782,7 +795,7 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   // that the call reports CLB_ETIMEOUT (0: every wait gives up at once).
   if (const char *env = std::getenv("CLB_WAIT_TRIES")) w.tries = (uint32_t)std::strtoul(env, nullptr, 10);
   w.inv_dx2 = a.inv_dx2;
-  w.mc = a.mc;
+  w.cs = a.cs;
   const double fm = md->fStar / md->MPl;
   h->sp = SFParams{md->alpha, fm * fm, cfg->dt, 1.0 / (double)h->n3};
   h->part_rows = (size_t)std::max(h->sweep_blocks, kElemBlocks);
@@ -833,6 +846,7 @@ void clb_destroy(clb_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   u1_destroy(h);
   su2_destroy(h);
+  gw_destroy(h);
   for (int b = 0; b < 2; ++b) {
     if (h->fld[b]) cudaFree(h->fld[b]);
     if (h->pi[b]) cudaFree(h->pi[b]);
@@ -994,6 +1008,7 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
     return h->fail(CLB_EUNSUPPORTED, "clb_initialize: a restart with a fixed background is not supported");
   dispatch<Init>(h, (int)correct_adot);
   h->synced = !(correct_adot == CLB_INIT_RESTART && h->cfg.evolver == CLB_LF); // leapfrog.h:30-31
+  if (h->gw) gw_set_synced(h, correct_adot != CLB_INIT_RESTART);           // evolver.h:52
   h->fb_t = h->cfg.t0;
   int r = sync_and_check(h, "clb_initialize");
   if (r == CLB_OK) h->initialized = true;
@@ -1104,6 +1119,7 @@ int clb_sync(clb_handle *h)
   if (!h->initialized) return h->fail(CLB_ESTATE, "clb_sync: call clb_initialize first");
   if (h->u1) return u1_sync(h);
   if (h->su2) return su2_sync(h);
+  if (h->gw) gw_sync(h); // evolver.h:134-137, before the matter sync
   if (h->cfg.evolver == CLB_LF) dispatch<SyncLF>(h);
   if (h->fb) fb_tail(h, T_FB_ADOT, 0.0, h->fb_adot(h->fb_t - h->cfg.t0));
   return sync_and_check(h, "clb_sync");

@@ -37,8 +37,20 @@ constexpr int kNTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 constexpr int kRuns[] = {8, 16, 32, 64, 1024};
 constexpr int kDefaultTile = 1, kDefaultRun = 32; // 32 x 8 tiles, 32-plane runs
 
-// Tuned configurations by ensemble (precision, device and sorted member sizes), for the process.
-std::map<std::string, std::pair<int, int>> g_tuned;
+// Shapes compiled for the persistent form (block z and y threads, z sites per thread); x-runs as
+// kRuns.  Clusters of kClusterCTAs blocks (the portable maximum).
+constexpr TileShape kPersist[] = {{32, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 4, 1}};
+constexpr int kNPersist = sizeof(kPersist) / sizeof(kPersist[0]);
+constexpr int kClusterCTAs = 8;
+
+// Tuned configurations by ensemble (precision, device and sorted member sizes), for the process:
+// graph-form tile and run, then whether the persistent form won, with its shape and run.
+struct Tuned {
+  int tile, run;
+  bool persist;
+  int ptile, prun;
+};
+std::map<std::string, Tuned> g_tuned;
 
 } // namespace
 
@@ -75,6 +87,12 @@ struct clb_batch {
     int64_t launches; // kernels in the graph
   };
   std::map<std::tuple<int64_t, int, int>, Graph> graphs; // (steps, cf, rs) -> graph
+  // the persistent form (k_batch_persist): shape index into kPersist, x-run, cluster count
+  bool persist = false;
+  int ptile = 0, prun = 8, pclusters = 0;
+  BatchLat *d_plat = nullptr; // member descriptors with the persistent tile grid
+  int *d_members = nullptr, *d_offsets = nullptr;
+  clb_batch_form form{};
   std::string err;
   int fail(int code, const std::string &m)
   {
@@ -222,7 +240,7 @@ void sweep(clb_batch *b, bool drift, bool kick, int red, double dtw, double h1, 
 // the handle's stream with CUDA events, and keeps the fastest.  The timing sweeps read the current
 // state and write only the idle state buffers, the next reference slot and the partials, so the
 // state is unchanged.
-int autotune(clb_batch *b, int reps)
+int autotune_graph(clb_batch *b, int reps)
 {
   const double dt = b->cfg.dt, w = b->ws[0];
   cudaError_t e = cudaSuccess;
@@ -258,7 +276,6 @@ int autotune(clb_batch *b, int reps)
   drop_graphs(b);
   b->tuned = true;
   b->tuning = tuning_of(bt, br, count, best, def);
-  g_tuned[tune_key(b)] = {bt, br};
   return CLB_OK;
 }
 
@@ -269,9 +286,16 @@ void btail(clb_batch *b, uint32_t flags, bool reduced, double w = 0, double w2 =
   ++b->launches;
 }
 
-// The fused VV schedule of EvolveVV (clb_api.cu) over all members.
+cudaError_t persist_run(clb_batch *b, int64_t nsteps);
+
+// The fused VV schedule of EvolveVV (clb_api.cu) over all members: one launch of the persistent
+// form, or a sweep and a tail launch per stage.
 void evolve_launches(clb_batch *b, int64_t nsteps)
 {
+  if (b->persist) {
+    persist_run(b, nsteps);
+    return;
+  }
   const double dt = b->cfg.dt;
   const bool ex = b->cfg.expansion != 0;
   const std::vector<double> &ws = b->ws;
@@ -294,6 +318,267 @@ void evolve_launches(clb_batch *b, int64_t nsteps)
       btail(b, fl, true, w, wn);
     }
   }
+}
+
+// ---- persistent form ----------------------------------------------------------------------------
+template <class R, int BZ, int BY, int VZ> struct Persist {
+  static cudaLaunchConfig_t config(clb_batch *b, int clusters, cudaLaunchAttribute *at)
+  {
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterCTAs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t c{};
+    c.gridDim = dim3((unsigned)(clusters * kClusterCTAs));
+    c.blockDim = dim3(BZ, BY);
+    c.dynamicSmemBytes = 0;
+    c.stream = b->stream;
+    c.attrs = at;
+    c.numAttrs = 1;
+    return c;
+  }
+  static int max_clusters(clb_batch *b)
+  {
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t c = config(b, 148, at);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_batch_persist<BZ, BY, VZ, R>, &c) != cudaSuccess) return 0;
+    return n;
+  }
+  static cudaError_t launch(clb_batch *b, const PersistArgs &a)
+  {
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t c = config(b, b->pclusters, at);
+    R *f0 = static_cast<R *>(b->f[0]), *f1 = static_cast<R *>(b->f[1]);
+    R *p0 = static_cast<R *>(b->p[0]), *p1 = static_cast<R *>(b->p[1]);
+    return cudaLaunchKernelEx(&c, k_batch_persist<BZ, BY, VZ, R>, f0, p0, f1, p1, (const BatchLat *)b->d_plat,
+                              b->d_st, (const int *)b->d_members, (const int *)b->d_offsets, a);
+  }
+};
+
+// Calls F with the Persist instantiation of shape t for the ensemble's precision.
+template <class F> auto with_persist(const clb_batch *b, int t, F &&f)
+{
+#define CLB_PS(R)                                                                                                        switch (t) {                                                                                                           case 0: return f(Persist<R, 32, 8, 1>{});                                                                             case 1: return f(Persist<R, 16, 8, 2>{});                                                                             case 2: return f(Persist<R, 16, 8, 4>{});                                                                             default: return f(Persist<R, 32, 4, 1>{});                                                                            }
+  if (b->fp32) {
+    CLB_PS(float)
+  } else {
+    CLB_PS(double)
+  }
+#undef CLB_PS
+}
+
+bool persist_fits(const clb_batch *b, int t)
+{
+  for (const BatchLat &L : b->lat)
+    if (L.N % kPersist[t].vz) return false;
+  return true;
+}
+
+// The persistent form's member table for shape t and x-run `run`: each member's tile grid, and the
+// members dealt to as many clusters as the device holds at once (at most one per member), longest
+// first to the least-loaded cluster.  A member's cost is its CTA's share of tiles per stage (the
+// sites of ceil(tiles / 8) tiles) plus a fixed per-stage cost of the cluster barriers and tail.
+cudaError_t persist_layout(clb_batch *b, int t, int run)
+{
+  const TileShape sh = kPersist[t];
+  int nc = with_persist(b, t, [&](auto P) { return decltype(P)::max_clusters(b); });
+  if (nc < 1) return cudaErrorInvalidConfiguration;
+  nc = std::min(nc, b->n);
+  std::vector<BatchLat> L = b->lat;
+  std::vector<std::pair<double, int>> cost;
+  for (int i = 0; i < b->n; ++i) {
+    BatchLat &l = L[(size_t)i];
+    l.gx = (l.N + sh.bz * sh.vz - 1) / (sh.bz * sh.vz);
+    l.gy = (l.N + sh.by - 1) / sh.by;
+    l.LX = std::min(l.N, run);
+    l.gz = (l.N + l.LX - 1) / l.LX;
+    l.first_block = 0;
+    l.nblocks = l.gx * l.gy * l.gz;
+    const double per_cta = (double)((l.nblocks + kClusterCTAs - 1) / kClusterCTAs) * sh.bz * sh.vz * sh.by * l.LX;
+    cost.push_back({per_cta + 4096.0, i});
+  }
+  std::stable_sort(cost.begin(), cost.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+  std::vector<double> load((size_t)nc, 0.0);
+  std::vector<std::vector<int>> lists((size_t)nc);
+  for (const auto &c : cost) {
+    const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[k] += c.first;
+    lists[k].push_back(c.second);
+  }
+  std::vector<int> members, offsets{0};
+  for (const auto &l : lists) {
+    members.insert(members.end(), l.begin(), l.end());
+    offsets.push_back((int)members.size());
+  }
+  cudaError_t e = cudaMemcpyAsync(b->d_plat, L.data(), L.size() * sizeof(BatchLat), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_members, members.data(), members.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_offsets, offsets.data(), offsets.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return e;
+  b->ptile = t;
+  b->prun = run;
+  b->pclusters = nc;
+  return cudaSuccess;
+}
+
+// One k_batch_persist launch for nsteps steps; the buffer parity and reference slot advance as the
+// per-stage launches would (a first kick sweep, then one drift sweep per stage).
+cudaError_t persist_run(clb_batch *b, int64_t nsteps)
+{
+  PersistArgs a{};
+  const std::vector<double> &ws = b->ws;
+  const size_t P = ws.size(), S = 2 * P - 1;
+  for (size_t i = 0; i < S; ++i) a.w[i] = ws[i < P ? i : S - i - 1];
+  a.dt = b->cfg.dt;
+  a.expansion = b->cfg.expansion != 0;
+  a.stages = (int)S;
+  a.nsteps = nsteps;
+  a.cf0 = b->cf;
+  a.rs0 = b->rs;
+  const cudaError_t e = with_persist(b, b->ptile, [&](auto Q) { return decltype(Q)::launch(b, a); });
+  ++b->launches;
+  const int64_t sweeps = nsteps * (int64_t)S;
+  if (sweeps % 2) b->cf ^= 1;
+  if (b->fp32 && (sweeps + 1) % 2) b->rs ^= 1;
+  return e;
+}
+
+// The state a timing launch starts from: the live buffers, the members' DevStates, the parity.
+struct Snapshot {
+  void *f = nullptr, *p = nullptr;
+  DevState *st = nullptr;
+  int cf = 0, rs = 0;
+  ~Snapshot()
+  {
+    for (void *q : {f, p, (void *)st})
+      if (q) cudaFree(q);
+  }
+};
+
+cudaError_t snap_take(clb_batch *b, Snapshot &s)
+{
+  const size_t bytes = (size_t)b->total_elems * b->esz;
+  cudaError_t e = cudaMalloc(&s.f, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&s.p, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&s.st, (size_t)b->n * sizeof(DevState));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s.f, b->f[b->cf], bytes, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s.p, b->p[b->cf], bytes, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s.st, b->d_st, (size_t)b->n * sizeof(DevState), cudaMemcpyDeviceToDevice, b->stream);
+  s.cf = b->cf;
+  s.rs = b->rs;
+  return e;
+}
+
+cudaError_t snap_put(clb_batch *b, const Snapshot &s)
+{
+  const size_t bytes = (size_t)b->total_elems * b->esz;
+  b->cf = s.cf;
+  b->rs = s.rs;
+  cudaError_t e = cudaMemcpyAsync(b->f[b->cf], s.f, bytes, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->p[b->cf], s.p, bytes, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_st, s.st, (size_t)b->n * sizeof(DevState), cudaMemcpyDeviceToDevice, b->stream);
+  return e;
+}
+
+// Milliseconds per step of a `steps`-step evolve call in the current form: captured as a graph,
+// launched once to warm up and once timed (CUDA events on the handle's stream), each launch from
+// the snapshot.
+cudaError_t time_form(clb_batch *b, const Snapshot &sn, int64_t steps, double &ms)
+{
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  cudaError_t e = snap_put(b, sn);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  const int64_t l0 = b->launches;
+  evolve_launches(b, steps);
+  const int64_t nl = b->launches - l0;
+  b->launches = l0;
+  e = cudaStreamEndCapture(b->stream, &g);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+  if (g) cudaGraphDestroy(g);
+  for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
+    if ((e = snap_put(b, sn)) != cudaSuccess) break;
+    cudaEventRecord(b->ev[0], b->stream);
+    e = cudaGraphLaunch(x, b->stream);
+    b->launches += nl;
+    cudaEventRecord(b->ev[1], b->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b->ev[1]);
+  }
+  float t = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, b->ev[0], b->ev[1]);
+  ms = t / (double)steps;
+  if (x) cudaGraphExecDestroy(x);
+  const cudaError_t e2 = snap_put(b, sn);
+  return e != cudaSuccess ? e : e2;
+}
+
+// CLB_BATCH_PERSISTENT: "0" keeps the per-stage graph form, "1" the persistent form, unset lets
+// the autotuner choose.
+int persistent_choice()
+{
+  const char *env = std::getenv("CLB_BATCH_PERSISTENT");
+  if (env && env[0] == '0') return 0;
+  if (env && env[0] == '1') return 1;
+  return -1;
+}
+
+bool persist_allowed(const clb_batch *b) { return 2 * b->ws.size() - 1 <= (size_t)kMaxStages; }
+
+// The full autotuner: the graph form's sweep configuration (autotune_graph), then whole evolve
+// calls of kFormSteps steps in that form and in the persistent form for every compiled shape and
+// x-run, each from a snapshot of the state (restored afterwards), keeping the fastest form.
+constexpr int64_t kFormSteps = 8;
+int autotune(clb_batch *b, int reps)
+{
+  int r = autotune_graph(b, reps);
+  if (r != CLB_OK) return r;
+  const int choice = persist_allowed(b) ? persistent_choice() : 0;
+  b->form = clb_batch_form{};
+  b->persist = false;
+  if (choice != 0) {
+    Snapshot sn;
+    cudaError_t e = snap_take(b, sn);
+    double best = 1e300, ms = 0;
+    int bt = -1, br = 0;
+    if (e == cudaSuccess && choice < 0) {
+      e = time_form(b, sn, kFormSteps, ms);
+      b->form.ms_graph = ms;
+    }
+    int maxN = 0;
+    for (const BatchLat &L : b->lat) maxN = std::max(maxN, L.N);
+    for (int t = 0; t < kNPersist && e == cudaSuccess; ++t) {
+      if (!persist_fits(b, t)) continue;
+      for (int run : {8, 16, 32}) {
+        if (run != 8 && run / 2 >= maxN) continue;
+        if ((e = persist_layout(b, t, run)) != cudaSuccess) break;
+        b->persist = true;
+        e = time_form(b, sn, kFormSteps, ms);
+        b->persist = false;
+        if (e != cudaSuccess) break;
+        ++b->form.candidates;
+        if (ms < best) {
+          best = ms;
+          bt = t;
+          br = run;
+        }
+      }
+    }
+    if (e == cudaSuccess && bt >= 0) {
+      e = persist_layout(b, bt, br);
+      b->form.ms_persistent = best;
+      b->persist = choice == 1 || best < b->form.ms_graph;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_autotune: forms");
+  }
+  g_tuned[tune_key(b)] = Tuned{b->tile, b->run, b->persist, b->ptile, b->prun};
+  return CLB_OK;
 }
 
 int check(clb_batch *b, const char *where)
@@ -326,7 +611,7 @@ void clb_batch_destroy(clb_batch *b)
     if (b->p[i]) cudaFree(b->p[i]);
   }
   for (void *q : {(void *)b->d_lat, (void *)b->d_blk, (void *)b->d_st, (void *)b->d_part, (void *)b->d_sums,
-                  (void *)b->d_stage})
+                  (void *)b->d_stage, (void *)b->d_plat, (void *)b->d_members, (void *)b->d_offsets})
     if (q) cudaFree(q);
   for (auto e : b->ev)
     if (e) cudaEventDestroy(e);
@@ -414,6 +699,9 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
          cudaMemset(b->f[i], 0, bytes) == cudaSuccess && cudaMemset(b->p[i], 0, bytes) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_lat, (size_t)n * sizeof(BatchLat)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_st, (size_t)n * sizeof(DevState)) == cudaSuccess;
+  ok = ok && cudaMalloc(&b->d_plat, (size_t)n * sizeof(BatchLat)) == cudaSuccess;
+  ok = ok && cudaMalloc(&b->d_members, (size_t)n * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&b->d_offsets, (size_t)(n + 1) * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_sums, 8 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_stage, b->stage_n * sizeof(double)) == cudaSuccess;
   ok = ok && cudaEventCreate(&b->ev[0]) == cudaSuccess && cudaEventCreate(&b->ev[1]) == cudaSuccess;
@@ -421,10 +709,14 @@ int clb_batch_create(const clb_config *cfgs, const clb_model_desc *mds, int32_t 
     // a configuration tuned earlier in this process for the same ensemble, else the default
     auto it = g_tuned.find(tune_key(b));
     const bool cached = it != g_tuned.end();
-    ok = layout(b, cached ? it->second.first : kDefaultTile, cached ? it->second.second : kDefaultRun) == cudaSuccess;
-    if (cached) {
+    ok = layout(b, cached ? it->second.tile : kDefaultTile, cached ? it->second.run : kDefaultRun) == cudaSuccess;
+    if (ok && cached) {
       b->tuned = true;
       b->tuning = tuning_of(b->tile, b->run, 0, 0.0, 0.0);
+      if (it->second.persist) {
+        ok = persist_layout(b, it->second.ptile, it->second.prun) == cudaSuccess;
+        b->persist = true;
+      }
     }
   }
   if (ok) {
@@ -561,6 +853,12 @@ int clb_batch_evolve(clb_batch *b, int64_t nsteps)
     } else {
       b->tuned = true;
       b->tuning = tuning_of(b->tile, b->run, 0, 0.0, 0.0);
+      if (persist_allowed(b) && persistent_choice() == 1) {
+        const int t = persist_fits(b, 0) ? 0 : 3;
+        const cudaError_t e = persist_layout(b, t, 8);
+        if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_evolve: persistent layout");
+        b->persist = true;
+      }
     }
   }
   const auto key = std::make_tuple(nsteps, b->cf, b->rs);
@@ -714,6 +1012,51 @@ int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t s
   drop_graphs(b);
   b->tuned = true;
   b->tuning = tuning_of(t, planes_x, 0, 0.0, 0.0);
+  b->persist = false;
+  return CLB_OK;
+}
+
+int clb_batch_set_persistent(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x)
+{
+  if (!b) return CLB_EINVAL;
+  if (!persist_allowed(b)) return b->fail(CLB_EUNSUPPORTED, "clb_batch_set_persistent: too many stages per step");
+  int t = -1;
+  for (int k = 0; k < kNPersist; ++k)
+    if (kPersist[k].bz * kPersist[k].vz == tile_z && kPersist[k].by == tile_y && kPersist[k].vz == sites_per_thread)
+      t = k;
+  if (t < 0) return b->fail(CLB_EINVAL, "clb_batch_set_persistent: not a compiled tile (see clb_batch_form)");
+  if (!persist_fits(b, t))
+    return b->fail(CLB_EINVAL, "clb_batch_set_persistent: every member's N must be a multiple of sites_per_thread");
+  if (planes_x < 1) return b->fail(CLB_EINVAL, "clb_batch_set_persistent: planes_x must be >= 1");
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = persist_layout(b, t, planes_x);
+  if (e != cudaSuccess) return b->cuda_fail(e, "clb_batch_set_persistent");
+  drop_graphs(b);
+  if (!b->tuned) {
+    b->tuned = true;
+    b->tuning = tuning_of(b->tile, b->run, 0, 0.0, 0.0);
+  }
+  b->persist = true;
+  return CLB_OK;
+}
+
+int clb_batch_get_form(clb_batch *b, clb_batch_form *out)
+{
+  if (!b || !out) return CLB_EINVAL;
+  clb_batch_form f = b->form;
+  f.persistent = b->persist ? 1 : 0;
+  if (b->persist) {
+    const TileShape sh = kPersist[b->ptile];
+    f.tile_z = sh.bz * sh.vz;
+    f.tile_y = sh.by;
+    f.sites_per_thread = sh.vz;
+    f.planes_x = b->prun;
+    f.clusters = b->pclusters;
+    f.cluster_blocks = kClusterCTAs;
+  } else {
+    f.tile_z = f.tile_y = f.sites_per_thread = f.planes_x = f.clusters = f.cluster_blocks = 0;
+  }
+  *out = f;
   return CLB_OK;
 }
 

@@ -17,6 +17,8 @@
 #include "clb_scalar.cuh"
 #include "clb_sweep.cuh"
 
+#include <cooperative_groups.h>
+
 namespace clb {
 
 struct BatchLat {
@@ -53,21 +55,19 @@ template <class R, int VZ> __device__ __forceinline__ void stg_v(R *p, const R (
     stv<R, VZ>(p, v);
 }
 
+// One tile of one member: the member's block `local` of its (z, y, x-run) grid, with the block's
+// sums of the averages in v (thread 0).  k_batch_sweep runs one tile per block; the persistent
+// k_batch_persist runs a cluster's share of a member's tiles one after another.
 template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
-__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ == 1 ? 1 : 2))
-    k_batch_sweep(const R *fin, const R *pin, R *fout, R *pout, const BatchLat *__restrict__ lats,
-                  const int *__restrict__ blk_lat, DevState *__restrict__ sts, int rs, double dtw_d, double h1,
-                  double h2, double *__restrict__ partials)
+__device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, R *pout, const BatchLat &lt,
+                                           DevState *__restrict__ st, int local, int rs, double dtw_d, double h1,
+                                           double h2, double (&vout)[kRedSlots])
 {
   using A = Ar<R>;
   constexpr bool SPLIT = sizeof(R) == 4;
   constexpr int TZ = BZ * VZ; // z sites per tile
   __shared__ R tile[3][BY + 2][TZ + 2];
   __shared__ double red_smem[(BZ * BY / 32) * kRedSlots];
-  const int L = blk_lat[blockIdx.x];
-  const BatchLat lt = lats[L];
-  DevState *st = sts + L;
-  const int local = blockIdx.x - lt.first_block;
   const int bx = local % lt.gx, by = (local / lt.gx) % lt.gy, bz = local / (lt.gx * lt.gy);
   const int N = lt.N;
   fin += lt.off;
@@ -276,10 +276,26 @@ __global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ
     }
     double v[kRedSlots] = {acc_pi2, acc_g2, acc_v};
     block_reduce<kRedSlots, BZ * BY>(v, red_smem);
-    if (tid == 0) {
 #pragma unroll
-      for (int k = 0; k < kRedSlots; ++k) partials[(size_t)blockIdx.x * kRedSlots + k] = v[k];
-    }
+    for (int k = 0; k < kRedSlots; ++k) vout[k] = v[k];
+  }
+  __syncthreads(); // the next tile of the same block reuses the shared tile and scratch
+}
+
+template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
+__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ == 1 ? 1 : 2))
+    k_batch_sweep(const R *fin, const R *pin, R *fout, R *pout, const BatchLat *__restrict__ lats,
+                  const int *__restrict__ blk_lat, DevState *__restrict__ sts, int rs, double dtw_d, double h1,
+                  double h2, double *__restrict__ partials)
+{
+  const int L = blk_lat[blockIdx.x];
+  const BatchLat lt = lats[L];
+  double v[kRedSlots] = {0, 0, 0};
+  batch_tile<BZ, BY, VZ, R, DRIFT, KICK, RED>(fin, pin, fout, pout, lt, sts + L, blockIdx.x - lt.first_block, rs,
+                                              dtw_d, h1, h2, v);
+  if (RED && threadIdx.x == 0 && threadIdx.y == 0) {
+#pragma unroll
+    for (int k = 0; k < kRedSlots; ++k) partials[(size_t)blockIdx.x * kRedSlots + k] = v[k];
   }
 }
 
@@ -305,6 +321,124 @@ __global__ void __launch_bounds__(256)
   o.hist = nullptr;
   tail_apply(s, o, lt.sp, v[0], v[1], v[2]);
   sts[blockIdx.x] = s;
+}
+
+// ---- the whole evolve call as one persistent launch --------------------------------------------
+// A thread-block cluster (CS CTAs, co-scheduled by the hardware) owns a list of members and takes
+// each through every step of the call before the next: per stage its CTAs sweep their share of
+// the member's tiles (tile t to CTA t % CS, in order), the cluster synchronises, CTA 0 adds the
+// CTAs' sums in rank order through distributed shared memory and applies the member's
+// scale-factor bookkeeping (tail_apply), and the cluster synchronises again before the next sweep
+// reads the new state.  No CTA waits on another cluster: members are independent, and within a
+// cluster every CTA runs the same loops and so the same barrier sequence.  The schedule is the
+// graph form's (evolve_launches, clb_batch.cu): a first half kick, then one fused sweep per stage.
+constexpr int kMaxStages = 31; // VV10
+
+// One tile as its own (not inlined) function: the persistent kernel calls three tile variants, and
+// inlined into its member and stage loops they would share one register allocation.
+template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
+__device__ __noinline__ void persist_tile(const R *fin, const R *pin, R *fout, R *pout, const BatchLat &lt,
+                                          DevState *st, int local, int rs, double dtw_d, double h1, double h2,
+                                          double (&vout)[kRedSlots])
+{
+  batch_tile<BZ, BY, VZ, R, DRIFT, KICK, RED>(fin, pin, fout, pout, lt, st, local, rs, dtw_d, h1, h2, vout);
+}
+
+struct PersistArgs {
+  double dt;
+  int expansion;
+  int stages;           // sweeps per step
+  long long nsteps;
+  double w[kMaxStages]; // stage weights
+  int cf0, rs0;         // buffer parity and FP32 reference slot at the call's start (all members)
+};
+
+template <int BZ, int BY, int VZ, class R>
+__global__ void __launch_bounds__(BZ *BY, CLB_BATCH_MINB * 256 / (BZ * BY) / (VZ == 1 ? 1 : 2))
+    k_batch_persist(R *f0, R *p0, R *f1, R *p1, const BatchLat *__restrict__ lats, DevState *__restrict__ sts,
+                    const int *__restrict__ members, const int *__restrict__ offsets, PersistArgs a)
+{
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int crank = (int)cl.block_rank(), csize = (int)cl.num_blocks();
+  const int cid = blockIdx.x / csize;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  __shared__ double part[kRedSlots]; // this CTA's sums of the current stage
+  R *F[2] = {f0, f1}, *P[2] = {p0, p1};
+  const double dt = a.dt;
+  for (int mi = offsets[cid]; mi < offsets[cid + 1]; ++mi) {
+    const int L = members[mi];
+    const BatchLat lt = lats[L];
+    DevState *st = sts + L;
+    int cf = a.cf0, rs = a.rs0;
+    auto clear = [&]() {
+      if (lead)
+#pragma unroll
+        for (int k = 0; k < kRedSlots; ++k) part[k] = 0.0;
+    };
+    auto add = [&](const double (&v)[kRedSlots]) {
+      if (lead)
+#pragma unroll
+        for (int k = 0; k < kRedSlots; ++k) part[k] += v[k];
+    };
+    auto tail = [&](uint32_t flags, bool reduced, double w, double w2) {
+      cl.sync(); // every CTA's sweep writes and sums are complete and visible
+      if (crank == 0 && lead) {
+        double v[kRedSlots] = {0, 0, 0};
+        if (reduced)
+          for (int r = 0; r < csize; ++r) {
+            const double *pr = cl.map_shared_rank(part, r);
+#pragma unroll
+            for (int k = 0; k < kRedSlots; ++k) v[k] += pr[k];
+          }
+        DevState sv = *st;
+        const TailOp op{flags, 0, w, w2, nullptr, -1, 0.0, 0.0};
+        tail_apply(sv, op, lt.sp, v[0], v[1], v[2]);
+        *st = sv;
+      }
+      cl.sync(); // the member's state is written before any CTA reads it, and `part` is free again
+    };
+    const int ntiles = lt.nblocks;
+    const bool ex = a.expansion != 0;
+    // the first half kick of the call (kickScaleFactorHalf, kickScalar, driftScaleFactor)
+    if (ex) tail(T_VV_KICK_HALF, false, 0.0, a.w[0]);
+    for (int t = crank; t < ntiles; t += csize) {
+      double v[kRedSlots] = {0, 0, 0};
+      persist_tile<BZ, BY, VZ, R, false, true, 0>(F[cf], P[cf], F[cf], P[cf], lt, st, t, rs, 0.0, a.w[0] * dt / 2, 0.0, v);
+    }
+    if (sizeof(R) == 4) rs ^= 1;
+    if (ex)
+      tail(T_VV_DRIFT, false, 0.0, a.w[0]);
+    else
+      cl.sync();
+    const long long total = a.nsteps * a.stages;
+    for (long long k = 0; k < total; ++k) {
+      const int i = (int)(k % a.stages);
+      const double w = a.w[i];
+      const bool more = k + 1 < total;
+      const double wn = more ? a.w[(int)((k + 1) % a.stages)] : 0.0;
+      clear();
+      for (int t = crank; t < ntiles; t += csize) {
+        double v[kRedSlots] = {0, 0, 0};
+        if (ex)
+          persist_tile<BZ, BY, VZ, R, true, true, 3>(F[cf], P[cf], F[cf ^ 1], P[cf ^ 1], lt, st, t, rs, dt * w,
+                                                   w * dt / 2, more ? wn * dt / 2 : 0.0, v);
+        else
+          persist_tile<BZ, BY, VZ, R, true, true, 0>(F[cf], P[cf], F[cf ^ 1], P[cf ^ 1], lt, st, t, rs, dt * w,
+                                                   w * dt / 2, more ? wn * dt / 2 : 0.0, v);
+        add(v);
+      }
+      cf ^= 1;
+      if (sizeof(R) == 4) rs ^= 1;
+      if (ex) {
+        uint32_t fl = T_STORE_PI2_I | T_STORE_FIELDS | T_VV_KICK_ONE;
+        if (more) fl |= T_VV_KICK_HALF | T_VV_DRIFT;
+        tail(fl, true, w, wn);
+      } else {
+        cl.sync();
+      }
+    }
+  }
 }
 
 // Host FP64 arrays <-> member storage: dst = (R)(src - off) and back (FP32: off = the member's

@@ -17,7 +17,9 @@
 namespace clb {
 struct U1Sector;
 struct SU2Sector;
+struct GWSector;
 }
+using clb::GWSector;
 using clb::U1Sector;
 using clb::SU2Sector;
 using namespace clb;
@@ -64,6 +66,7 @@ struct clb_handle {
   std::string err;
   U1Sector *u1 = nullptr;   // complex scalar + U(1) sector state (clb_u1.cu), null for other models
   SU2Sector *su2 = nullptr; // lphi4SU2U1 state (clb_su2.cu), null for other models
+  GWSector *gw = nullptr;   // gravitational waves of the scalar singlets (clb_gws.cu), null when off
 
   // instrumentation: launch counts always; per-launch CUDA events on the stream when prof
   bool prof = false;
@@ -119,13 +122,14 @@ namespace {
 
 enum KKind {
   K_FUSED, K_KICK, K_DRIFT_SWEEP, K_DRIFT, K_RED_PI2, K_RED_FIELDS, K_TAIL, K_MEASURE, K_CONVERT, K_SPECTRUM,
-  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_U1_ADJ, K_INIT, K_NKINDS
+  K_U1_KICK, K_U1_DRIFT, K_U1_REDUCE, K_U1_ADJ, K_INIT, K_GW, K_NKINDS
 };
 const char *const kKindNames[K_NKINDS] = {"scalar_fused_sweep", "scalar_kick_sweep", "scalar_drift_sweep",
                                           "scalar_drift",       "reduce_pi2",        "reduce_fields",
                                           "tail",               "measure",           "convert",
                                           "spectrum",           "gauge_kick_sweep",  "gauge_drift",
-                                          "gauge_reduce",       "u1_adjoint_sweep",  "initial_conditions"};
+                                          "gauge_reduce",       "u1_adjoint_sweep",  "initial_conditions",
+                                          "gw_sweep"};
 
 cudaEvent_t take_event(clb_handle *h)
 {

@@ -158,7 +158,7 @@ extern "C" int clb_scalar_averages_noalloc(const double *d_fields, const double 
   a.LX = LX;
   a.inv_dx2 = 1.0 / (dx * dx);
   const double coup[CLB_MAX_COUPLINGS] = {c0, q};
-  a.mc = ScalarModel::couplings(coup);
+  a.cs.mc = ScalarModel::couplings(coup);
   const dim3 grid(gx, gy, xs);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n_scalars == 1)

@@ -23,12 +23,20 @@ namespace clb {
 
 using ScalarModel = clb_models::CLB_SCALAR_MODEL;
 using ModelCouplings = ScalarModel::Couplings;
+// The handle and the kernel arguments hold a model's couplings in a fixed 8-double slot, so the
+// handle has one layout whichever header a build uses (the units that do not read the potential
+// are shared between the builds).
+static_assert(sizeof(ModelCouplings) <= 8 * sizeof(double), "a model header's Couplings holds at most 8 doubles");
+union CouplingSlot {
+  ModelCouplings mc;
+  double pad[8];
+};
 
 struct ScalarArgs {
   int N;
   int LX;           // x planes per block
   double inv_dx2;   // 1 / (dx dx)                      (gaugederivatives.h:38)
-  ModelCouplings mc; // the model header's couplings (models/lphi4.h: c0, q, c0/4, q/2)
+  CouplingSlot cs;   // the model header's couplings (models/lphi4.h: c0, q, c0/4, q/2) in cs.mc
   double dtw;       // dt * w of the drift              (velocityverlet.h:183)
   double h1;        // first kick weight  (w dt / 2)    (velocityverlet.h:131)
   double h2;        // second kick weight (w' dt / 2), 0 when the sweep ends on a half kick
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(BZ *BY)
             const R tyv = A::sub(A::add(tile[b][f][ty + 2][tz + 1], tile[b][f][ty][tz + 1]), A::mul(two, c));
             const R tzv = A::sub(A::add(tile[b][f][ty + 1][tz + 2], tile[b][f][ty + 1][tz]), A::mul(two, c));
             const R lap = A::mul(inv_dx2, A::add(A::add(tx, tyv), tzv));
-            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cur, a.mc)));
+            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cur, a.cs.mc)));
             const KickOut<R> ko = kick_val<R>(piC[f], K, a.h1, a.h2);
             pout[f * n3 + s] = ko.next;
             if (RED & 1) site_pi2 = f == 0 ? ko.mid * ko.mid : site_pi2 + ko.mid * ko.mid;
@@ -205,7 +213,7 @@ __global__ void __launch_bounds__(BZ *BY)
           }
         }
         if (RED & 1) acc_pi2 += site_pi2;
-        if (RED & 2) acc_v += (double)Pot::V(cur, a.mc);
+        if (RED & 2) acc_v += (double)Pot::V(cur, a.cs.mc);
       }
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
@@ -309,7 +317,7 @@ __global__ void __launch_bounds__(256)
       acc[6 * f + 5] += m * m;
     }
 #pragma unroll
-    for (int k = 0; k < NS; ++k) acc[6 * NS + k] += (double)Pot::Vterm(k, v, a.mc);
+    for (int k = 0; k < NS; ++k) acc[6 * NS + k] += (double)Pot::Vterm(k, v, a.cs.mc);
   }
   block_reduce<kMeasSlots, 256>(acc, smem);
   if (threadIdx.x == 0)

@@ -13,10 +13,11 @@
 #include "clb_sweep.cuh"
 
 namespace clb {
+// The non-template kernels are static: every unit that includes this header gets its own copies.
 
 // Padded component -> real input of an in-place R2C transform (row pitch 2 (N/2 + 1) doubles).
 template <class R>
-__global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, double *__restrict__ dst, Pad pd, double off)
+static __global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, double *__restrict__ dst, Pad pd, double off)
 {
   const int N = pd.N;
   const long long pitch = 2LL * (N / 2 + 1);
@@ -29,7 +30,7 @@ __global__ void __launch_bounds__(256) k_spec_gather(const R *__restrict__ src, 
 }
 
 // Unpadded N^3 component (x slowest) -> real input of an in-place R2C transform.
-__global__ void __launch_bounds__(256) k_spec_gather_plain(const double *__restrict__ src, double *__restrict__ dst, int N)
+static __global__ void __launch_bounds__(256) k_spec_gather_plain(const double *__restrict__ src, double *__restrict__ dst, int N)
 {
   const long long pitch = 2LL * (N / 2 + 1);
   for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
@@ -41,7 +42,7 @@ __global__ void __launch_bounds__(256) k_spec_gather_plain(const double *__restr
 
 // Unpadded N^3 component of storage type R -> real input of an in-place R2C transform.
 template <class R>
-__global__ void __launch_bounds__(256) k_spec_gather_raw(const R *__restrict__ src, double *__restrict__ dst, int N)
+static __global__ void __launch_bounds__(256) k_spec_gather_raw(const R *__restrict__ src, double *__restrict__ dst, int N)
 {
   const long long pitch = 2LL * (N / 2 + 1);
   for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(256) k_spec_gather_raw(const R *__restrict__ s
 // Tangent of the binned sum of |f_k|^2: per bin sum w 2 Re(conj(f_k) t_k) of the transforms of
 // a component (fk) and of its tangent (tk), with k_spec_bin's bins and weights; partial rows in
 // k_spec_bin's layout (the |n| and count slots left 0).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_spec_bin_cross(const double2 *__restrict__ fk, const double2 *__restrict__ tk, int N, double dk, int nbins,
                      int fold, double *__restrict__ part_val, unsigned long long *__restrict__ part_cnt)
 {
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(256)
 // Gradient of sum_b g_b (sum over bin b of |f_k|^2), step 1: each mode of the half spectrum times
 // the weight g of its bin (k_spec_bin's bin rule; modes outside the bins: 0).  A C2R transform of
 // the result, times 2, is the gradient with respect to the real component.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_spec_weight(double2 *__restrict__ fk, int N, double dk, int nbins, int fold, const double *__restrict__ gbin)
 {
   const int nzh = N / 2 + 1;
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // Real output of an in-place C2R transform (row pitch 2 (N/2 + 1)) times scale -> N^3 array.
-__global__ void __launch_bounds__(256) k_spec_extract(const double *__restrict__ src, double *__restrict__ dst, int N, double scale)
+static __global__ void __launch_bounds__(256) k_spec_extract(const double *__restrict__ src, double *__restrict__ dst, int N, double scale)
 {
   const long long pitch = 2LL * (N / 2 + 1);
   for (long long r = blockIdx.x; r < (long long)N * N; r += gridDim.x) {
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) k_spec_extract(const double *__restrict__
 
 // One block per group of (kx, ky) rows; shared-memory histograms of sum w |f|^2, sum w |n| and the
 // integer mode count, written as one partial row per block.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_spec_bin(const double2 *__restrict__ fk, int N, double dk, int nbins, int fold, double *__restrict__ part_val,
                unsigned long long *__restrict__ part_cnt)
 {
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // Fixed-order sum of the block partial rows, one thread per bin.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_spec_sum(const double *__restrict__ part_val, const unsigned long long *__restrict__ part_cnt, int nblk, int nbins,
                double *__restrict__ out_val, double *__restrict__ out_n, unsigned long long *__restrict__ out_cnt)
 {

@@ -76,7 +76,7 @@ struct SweepArgs {
   int rs;          // FP32 split storage: reference slot read by this launch
   uint32_t tries;  // bound of each mbarrier wait
   double inv_dx2;
-  ModelCouplings mc; // the model header's couplings
+  CouplingSlot cs; // the model header's couplings (cs.mc)
   double dtw, h1, h2;
   double dtw0;     // DRIFT == 2: a first drift of the same kind before dtw's (position Verlet)
 };
@@ -248,8 +248,8 @@ __global__ void __launch_bounds__(SH::THREADS)
   ModelFluct spc{};
   const float h1f = (float)a.h1, h2f = (float)a.h2;
   if constexpr (SPLIT) {
-    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.mc, DRIFT == 2 ? a.dtw0 : 0.0);
-    spc = ModelFluct::make(rf.phi[0], a.mc);
+    rf = ref_step<NS>(st, a.rs, DRIFT, KICK, a.dtw, a.h1, a.h2, a.cs.mc, DRIFT == 2 ? a.dtw0 : 0.0);
+    spc = ModelFluct::make(rf.phi[0], a.cs.mc);
     if ((DRIFT || KICK) && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
       DevState *sw = const_cast<DevState *>(st); // slot rs ^ 1 is read by no block of this launch
 #pragma unroll
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(SH::THREADS)
                 if constexpr (FL)
                   ddv = spc.dV(c);
                 else
-                  ddv = (float)(SPot<double, NS>::dV(f, cd, a.mc) - rf.dV[f]);
+                  ddv = (float)(SPot<double, NS>::dV(f, cd, a.cs.mc) - rf.dV[f]);
                 const float K = KAd * lap - KB * ddv;
                 const float pm = fmaf(h1f, K, piC[f][k]);
                 outp[f][k] = h2f != 0.f ? fmaf(h2f, K, pm) : pm;
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(SH::THREADS)
               if constexpr (FL)
                 s_dv += spc.V(cv[0]);
               else
-                s_dv += (float)(SPot<double, NS>::V(cd, a.mc) - rf.V);
+                s_dv += (float)(SPot<double, NS>::V(cd, a.cs.mc) - rf.V);
             }
           }
           if (RED) {
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(SH::THREADS)
             const R tyv = A::sub(A::add(yp[f][k], ym[f][k]), A::mul(two, c));
             const R tzv = A::sub(A::add(zn, zm), A::mul(two, c));
             const R lap = A::mul(inv_dx2, A::add(A::add(txv, tyv), tzv));
-            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cv, a.mc)));
+            const R K = A::sub(A::mul(KA, lap), A::mul(KB, Pot::dV(f, cv, a.cs.mc)));
             const KickOut<R> ko = kick_val<R>(piC[f][k], K, a.h1, a.h2);
             outp[f][k] = ko.next;
             if (RED & 1) site_pi2 = f == 0 ? ko.mid * ko.mid : site_pi2 + ko.mid * ko.mid;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(SH::THREADS)
           }
         }
         if ((RED & 1) && k < nvalid) acc_pi2 += site_pi2;
-        if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, a.mc);
+        if ((RED & 2) && k < nvalid) acc_v += (double)Pot::V(cv, a.cs.mc);
       }
       }
       // stores: the thread's VZ sites, then the periodic ghost copies of boundary sites

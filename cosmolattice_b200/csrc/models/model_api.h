@@ -4,8 +4,9 @@
 // A model header defines one struct M with
 //   static constexpr const char *name;
 //   static constexpr int NScalarsMax;           the singlet count of the header (1 or 2 used)
-//   struct Couplings;                           the program-unit couplings the terms read (FP64;
-//                                               a term of storage type R rounds them to R)
+//   struct Couplings;                           the program-unit couplings the terms read (FP64,
+//                                               at most 8 doubles; a term of storage type R rounds
+//                                               them to R)
 //   static Couplings couplings(const double *c);   from clb_model_desc::couplings
 //   template <class A, class R, int NS> static R potentialTerms(Tag<k>, const R (&phi)[NS], const Couplings<R> &);
 //   template <class A, class R, int NS> static R potDeriv(Tag<f>, const R (&phi)[NS], const Couplings<R> &);

@@ -8,6 +8,7 @@ so a driver reads like source/cosmolattice.cpp.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from typing import Dict, List, Optional
 
@@ -234,6 +235,42 @@ class Lattice:
     def tangent_end(self) -> None:
         self._check(self.lib.clb_tangent_end(self.h))
 
+    # ---- gravitational waves (clb_gws_*; the reference's GW sector with doLFforGWs) ----
+    def gws_enable(self) -> None:
+        self._check(self.lib.clb_gws_enable(self.h))
+
+    def gws_set_state(self, u=None, pi=None) -> None:
+        n = 5 * self.rp.N ** 3
+        args = []
+        for a in (u, pi):
+            if a is None:
+                args.append(None)
+            else:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                if a.size != n:
+                    raise ValueError("GW arrays hold 5 x N^3 values")
+                args.append(a)
+        self._check(self.lib.clb_gws_set_state(self.h, *[_dp(a) if a is not None else None for a in args]))
+
+    def gws_get_state(self):
+        n = 5 * self.rp.N ** 3
+        u, p = np.empty(n), np.empty(n)
+        self._check(self.lib.clb_gws_get_state(self.h, _dp(u), _dp(p)))
+        return u, p
+
+    def gw_spectrum(self, prj_type: int = 2, ps_type: int = 1, ps_version: int = 1, dk: float = 1.0,
+                    nbins: Optional[int] = None, fold: bool = True):
+        """(k, d(rho_GW/rho)/dlog k per bin, mode counts, rho_GW/rho) of clb_gw_spectrum."""
+        if nbins is None:
+            nbins = int(math.floor(math.sqrt(3.0) / 2.0 * self.rp.N / dk))
+        k, v = np.empty(nbins), np.empty(nbins)
+        c = np.empty(nbins, dtype=np.int64)
+        frac = C.c_double()
+        self._check(self.lib.clb_gw_spectrum(self.h, int(prj_type), int(ps_type), int(ps_version), float(dk), nbins,
+                                             1 if fold else 0, _dp(k), _dp(v),
+                                             c.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(frac)))
+        return k, v, c, frac.value
+
     def history(self) -> np.ndarray:
         """Per-step rows (a, aDot, <pi^2>, <grad^2>, <V>) of the last evolve call."""
         n = C.c_int64()
@@ -440,6 +477,37 @@ class Measurer:
             fh.write("\n")
             fh.flush()
 
+    def measure_gws(self, t: float, lattice: Lattice) -> None:
+        """GWsMeasurer::measureSpectra (gwsmeasurer.h:41-53): spectra_energy_gws.txt (the bin
+        centre times kIR and d(rho_GW/rho)/dlog k) and average_energies_gws.txt (t, rhoGW/rho,
+        rhoGW)."""
+        if not self.outdir:
+            return
+        rp = self.rp
+        k, v, c, frac = lattice.gw_spectrum(prj_type=rp.GWprojectorType, ps_type=rp.powerSpectrumType,
+                                            ps_version=rp.powerSpectrumVersion, dk=rp.deltaKBin, nbins=rp.nBinsSpectra)
+        key = "spectra_energy_gws"
+        if key not in self.files:
+            fh = open(os.path.join(self.outdir, key + ".txt"), "a" if rp.appendMode else "w")
+            if rp.printHeaders and not rp.appendMode:
+                fh.write("1:binCentralValue 2:PS\n")
+            self.files[key] = fh
+        fh = self.files[key]
+        centres = (np.arange(rp.nBinsSpectra) + 0.5) * rp.deltaKBin * rp.kIR
+        for b in range(rp.nBinsSpectra):
+            fh.write(f"{centres[b]:.15g} {v[b]:.15g}\n")
+        fh.write("\n")
+        fh.flush()
+        rho = lattice.measure(self.e0 if self.e0 is not None else 1.0)["energies"][-1]
+        if "energies_gws" not in self.files:
+            path = os.path.join(self.outdir, "average_energies_gws.txt")
+            fh = open(path, "a" if rp.appendMode else "w")
+            if rp.printHeaders and not rp.appendMode:
+                fh.write("#t    rhoGW_over_rho    rhoGW\n")
+            self.files["energies_gws"] = fh
+        self.files["energies_gws"].write(f"{t:.15g}    {frac:.15g}    {frac * rho:.15g}\n")
+        self.files["energies_gws"].flush()
+
     def measure(self, n: int, t: float, lattice: Lattice) -> Dict[str, object]:
         first = self.e0 is None
         m = lattice.measure(self.e0 if self.e0 is not None else 1.0)
@@ -480,6 +548,8 @@ def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fu
     model = MODELS[model_name](par, rp)
     lattice = (lattice_factory(model, rp) if lattice_factory is not None
                else Lattice(model, rp, precision=precision, path=path))
+    if rp.withGWs:
+        lattice.gws_enable()
     measurer = Measurer(model, rp, outdir)
     ModelInitializer(model, rp.lSide, rp.baseSeed).initialize(model, rp, lattice)
     evolver = Evolver(model, rp, lattice)
@@ -494,6 +564,8 @@ def run(par, model_name: str = "lphi4", precision: str = "fp64", path: str = "fu
             measurer.measure(i, t, lattice)
         if infreq:
             measurer.measure_spectra(t, lattice)
+            if rp.withGWs:
+                measurer.measure_gws(t, lattice)
         # advance to the next measurement in one device call
         n = min(measurer.outputFreq - (i % measurer.outputFreq), measurer.spectraFreq - (i % measurer.spectraFreq))
         n_left = c_round((rp.tMax - t) / rp.dt)

@@ -158,6 +158,8 @@ class RunParameters:
         self.powerSpectrumType = par.get_int("PS_type", 1)
         self.powerSpectrumVersion = par.get_int("PS_version", 1)
         self.withGWs = par.get_bool("withGWs", False)
+        self.doLFforGWs = par.get_bool("doLFforGWs", True)      # runparameters.h:121
+        self.GWprojectorType = par.get_int("GWprojectorType", 2)  # runparameters.h:122-123
 
         # lSide = 2 pi / kIR = N dx (runparameters.h:155-186)
         hasK = not _almost_equal(kIR, -1)
@@ -199,5 +201,8 @@ class RunParameters:
             raise RunParametersInconsistent(
                 "For models that do not involve cosmic defects, you need to specify a non-zero H0 to run a simulation "
                 "with fixed background. If you want to disable expansion, please set expansion = false in the input file.")
-        if self.withGWs:
-            raise RunParametersInconsistent("GWs are outside this library's hot path.")
+        if self.withGWs and not self.doLFforGWs:
+            raise RunParametersInconsistent("GWs run as the reference's default leapfrog over the matter evolver "
+                                            "(doLFforGWs = true) here.")
+        if self.withGWs and self.GWprojectorType not in (1, 2, 3):
+            raise RunParametersInconsistent(f"GWprojectorType {self.GWprojectorType} is not 1, 2 or 3.")

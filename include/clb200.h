@@ -358,6 +358,56 @@ int clb_batch_autotune(clb_batch *b, int32_t reps, clb_batch_tuning *out);
 int clb_batch_set_tuning(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x);
 int clb_batch_get_tuning(clb_batch *b, clb_batch_tuning *out);
 
+/* The form an evolve call takes.  Per-stage form: one sweep and one tail launch per VV stage,
+ * captured as one CUDA graph per call (the tile of clb_batch_tuning).  Persistent form: the whole
+ * call is one launch of thread-block clusters (cluster_blocks blocks each, co-scheduled), each
+ * cluster taking its members, longest first to the least-loaded cluster, through every step; per
+ * stage the cluster sweeps a member's tiles, synchronises on the hardware cluster barrier and
+ * applies the member's scale-factor update from its sums in a fixed order.  The call is captured
+ * as a one-launch graph.  There is no software wait in it (no flags, no spins).
+ * The autotuner (clb_batch_autotune, or the first evolve) times whole 8-step calls of both forms
+ * from a snapshot of the state, which it restores, and keeps the faster; CLB_BATCH_PERSISTENT=0 or
+ * 1 in the environment fixes the form.  clb_batch_set_tuning selects the per-stage form,
+ * clb_batch_set_persistent the persistent form with the given tile: (tile_z, tile_y,
+ * sites_per_thread) one of (32, 8, 1), (32, 8, 2), (64, 8, 4) and (32, 4, 1), with planes_x
+ * x-planes per tile.  The fields do not depend on the form; the volume sums are summed in a
+ * form-dependent order. */
+typedef struct clb_batch_form {
+  int32_t persistent;        /* 1: persistent form, 0: per-stage graph form                   */
+  int32_t tile_z, tile_y;    /* persistent form's tile (0 in the per-stage form)              */
+  int32_t sites_per_thread;
+  int32_t planes_x;
+  int32_t clusters;          /* clusters launched                                             */
+  int32_t cluster_blocks;    /* blocks per cluster                                            */
+  int32_t candidates;        /* persistent configurations timed (0: set, cached or default)   */
+  double ms_graph;           /* per step, timed by the autotuner (0: not timed)               */
+  double ms_persistent;      /* per step, the fastest persistent configuration (0: not timed) */
+} clb_batch_form;
+
+int clb_batch_set_persistent(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x);
+int clb_batch_get_form(clb_batch *b, clb_batch_form *out);
+
+/* ---- gravitational waves of the scalar singlets -------------------------------------------------
+ * The GW sector of the reference (GWsKernels::get, evolvers/kernels/gwskernels.h:27-33; the
+ * scalar-singlet source of PITensor.h; Evolver::evolve/sync with the default doLFforGWs, a leapfrog
+ * staggered over the matter evolver, evolvers/evolver.h:102-138; GWsInitializer, zero at the
+ * start).  The field is the traceless symmetric u_ij as five components (u_11, u_12, u_13, u_22,
+ * u_23; u_33 = -u_11 - u_22), its momenta likewise.
+ * clb_gws_enable: after clb_create, before clb_initialize; scalar-singlet models with the VV
+ * evolvers on the fused path and self-consistent or no expansion (else CLB_EUNSUPPORTED).
+ * clb_gws_set_state / clb_gws_get_state: 5 x N^3 doubles each (either may be NULL).
+ * clb_gw_spectrum: the GW energy spectrum d(rho_GW/rho)/dlog k (PowerSpectrumMeasurer::
+ * powerSpectrumGW, measurements/powerspectrum.h:51-71) with the TT projector of
+ * GWProjectorType1/2/3 (definitions/gwsprojector.h; prj_type 1, 2 or 3), the bins and PS_type /
+ * PS_version of clb_spectrum; rho_gw_over_rho (may be NULL): its sum over the bins times
+ * dk / k (GWsMeasurer, measurements/gwsmeasurer.h:41-53).  Measures the energies first, as the
+ * reference's Energies::rho does (which refreshes the cached averages).  Call it after clb_sync. */
+int clb_gws_enable(clb_handle *h);
+int clb_gws_set_state(clb_handle *h, const double *u, const double *pi);
+int clb_gws_get_state(clb_handle *h, double *u, double *pi);
+int clb_gw_spectrum(clb_handle *h, int32_t prj_type, int32_t ps_type, int32_t ps_version, double dk, int32_t nbins,
+                    int32_t fold, double *k_out, double *value_out, int64_t *count_out, double *rho_gw_over_rho);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ----------------------------
  * For callers that cannot call cudaMalloc: a host runtime that owns the whole device memory pool
  * and hands out no more, or an embedding that forbids device allocation after start-up (a service

@@ -274,6 +274,49 @@ struct Oracle {
     for (size_t s = 0; s < (size_t)Ns * n3; ++s) fld[s] = fld[s] + p * (c * pi[s]);
   }
 
+  // ---- gravitational waves (evolver.h:102-138 with the default doLFforGWs: a leapfrog staggered
+  // over the matter evolver).  Five components of the traceless symmetric u_ij (11, 12, 13, 22,
+  // 23; u_33 = -u_11 - u_22, as gwsprojector.h reads them), zero at the start (gwsinitializer.h).
+  // Kick (leapfrog.h:136-139, gwskernels.h:27-33): pi_u += (w dt) [a^(1+alpha) lapl u
+  // + a^(1+alpha) 2 Pi], Pi the traceless part of sum_a forwDiff_i phi_a forwDiff_j phi_a
+  // (PITensor.h scalar-singlet source; forwDiff (f(x+i) - f(x)) / dx, gaugederivatives.h:70-73;
+  // lapl as gaugederivatives.h:42-46).  Drift (leapfrog.h:198-201): u += pow(aSI, alpha-3) (dt pi_u).
+  bool gws = false, gwSynced = true;
+  std::vector<double> gu, gpi;
+  void gwKick(double w)
+  {
+    const double A = std::pow(aI, 1 + md.alpha);
+    const double h = w * cfg.dt;
+    const double dx = cfg.dx;
+#pragma omp parallel for schedule(static)
+    for (int x = 0; x < N; ++x)
+      for (int y = 0; y < N; ++y)
+        for (int z = 0; z < N; ++z) {
+          const size_t s = at(x, y, z);
+          const size_t nb[3] = {at(up(x), y, z), at(x, up(y), z), at(x, y, up(z))};
+          double P[6] = {0, 0, 0, 0, 0, 0}; // 00, 01, 02, 11, 12, 22
+          for (int f = 0; f < Ns; ++f) {
+            const double *F0 = fld.data() + (size_t)f * n3;
+            double g[3];
+            for (int i = 0; i < 3; ++i) g[i] = (F0[nb[i]] - F0[s]) / dx;
+            const double t[6] = {g[0] * g[0], g[0] * g[1], g[0] * g[2], g[1] * g[1], g[1] * g[2], g[2] * g[2]};
+            for (int k = 0; k < 6; ++k) P[k] = f == 0 ? t[k] : P[k] + t[k];
+          }
+          const double third = ((P[0] + P[3]) + P[5]) * (1.0 / 3.0);
+          const double S[5] = {P[0] - third, P[1], P[2], P[3] - third, P[4]};
+          for (int c = 0; c < 5; ++c) {
+            const double K = A * lapl(gu.data() + (size_t)c * n3, x, y, z) + (A * 2) * S[c];
+            gpi[c * n3 + s] = gpi[c * n3 + s] + h * K;
+          }
+        }
+  }
+  void gwDrift()
+  {
+    const double p = std::pow(aSI, md.alpha - 3);
+#pragma omp parallel for schedule(static)
+    for (size_t s = 0; s < 5 * n3; ++s) gu[s] = gu[s] + p * (cfg.dt * gpi[s]);
+  }
+
   // ---- Averages::setAllAverages (averages.h:349-358)
   void setAllAverages()
   {
@@ -528,6 +571,35 @@ int orc_set_scalar_model(orc_handle *h, int32_t id)
   return CLB_OK;
 }
 
+// Gravitational waves of a scalar-singlet handle: enable (zero u and pi_u), set and get the five
+// components of each (5 x N^3 doubles, the order of u_11, u_12, u_13, u_22, u_23).
+int orc_gws_enable(orc_handle *h)
+{
+  if (!h || isU1(h) || isSU2(h)) return CLB_EUNSUPPORTED;
+  Oracle *o = S(h);
+  o->gws = true;
+  o->gwSynced = true;
+  o->gu.assign(5 * o->n3, 0.0);
+  o->gpi.assign(5 * o->n3, 0.0);
+  return CLB_OK;
+}
+int orc_gws_set_state(orc_handle *h, const double *u, const double *pi)
+{
+  if (!h || isU1(h) || isSU2(h) || !S(h)->gws) return CLB_ESTATE;
+  Oracle *o = S(h);
+  if (u) std::memcpy(o->gu.data(), u, o->gu.size() * sizeof(double));
+  if (pi) std::memcpy(o->gpi.data(), pi, o->gpi.size() * sizeof(double));
+  return CLB_OK;
+}
+int orc_gws_get_state(orc_handle *h, double *u, double *pi)
+{
+  if (!h || isU1(h) || isSU2(h) || !S(h)->gws) return CLB_ESTATE;
+  Oracle *o = S(h);
+  if (u) std::memcpy(u, o->gu.data(), o->gu.size() * sizeof(double));
+  if (pi) std::memcpy(pi, o->gpi.data(), o->gpi.size() * sizeof(double));
+  return CLB_OK;
+}
+
 int orc_set_state(orc_handle *h, const double *fields, const double *momenta, const clb_scalefactor *sf)
 {
   if (isSU2(h)) return oracle_models::su2_set_state(H(h)->impl, fields, momenta, sf);
@@ -570,6 +642,7 @@ int orc_initialize(orc_handle *h, int32_t correct_adot)
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
+  o->gwSynced = true;
   o->t = o->cfg.t0;
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;
@@ -583,12 +656,17 @@ int orc_evolve(orc_handle *h, int64_t n)
   Oracle *o = S(h);
   if (!o->initialized) { o->err = "evolve before initialize"; return CLB_ESTATE; }
   for (int64_t s = 0; s < n; ++s) {
+    if (o->gws) { // evolver.h:104-107
+      o->gwKick(o->gwSynced ? 0.5 : 1.0);
+      o->gwSynced = false;
+    }
     if (o->cfg.evolver == CLB_LF)
       o->evolveLF();
     else if (isPV(o->cfg.evolver))
       o->evolvePV();
     else
       o->evolveVV();
+    if (o->gws) o->gwDrift(); // evolver.h:123
     o->t += o->cfg.dt; // the main loop's t (cosmolattice.cpp:186-188)
   }
   return CLB_OK;
@@ -599,6 +677,10 @@ int orc_sync(orc_handle *h)
   if (isSU2(h)) return oracle_models::su2_sync(H(h)->impl);
   if (isU1(h)) return oracle_models::u1_sync(H(h)->impl);
   Oracle *o = S(h);
+  if (o->gws && !o->gwSynced) { // evolver.h:134-137
+    o->gwKick(0.5);
+    o->gwSynced = true;
+  }
   if (o->cfg.evolver == CLB_LF) o->syncLF();
   if (o->fb) o->aDotI = o->aBgDot(o->t - o->cfg.t0); // velocityverlet.h:121, leapfrog.h:114, positionverlet.h:106
   return CLB_OK;

@@ -44,6 +44,9 @@ def load():
             "orc_measure": (C.c_int, [H, C.c_double, C.POINTER(capi.Measurement)]),
             "orc_num_threads": (C.c_int, []),
             "orc_set_scalar_model": (C.c_int, [H, C.c_int32]),
+            "orc_gws_enable": (C.c_int, [H]),
+            "orc_gws_set_state": (C.c_int, [H, dp, dp]),
+            "orc_gws_get_state": (C.c_int, [H, dp, dp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -89,6 +92,17 @@ class OracleLattice:
             self._check(self.lib.orc_set_scalar_model(self.h, 1))
         self.n_components = getattr(model, "n_components", model.Ns)
         self.n_momentum_components = getattr(model, "n_momentum_components", self.n_components)
+
+    def gws_enable(self):
+        self._check(self.lib.orc_gws_enable(self.h))
+
+    def gws_get_state(self):
+        import numpy as np
+
+        n = 5 * self.rp.N ** 3
+        u, p = np.empty(n), np.empty(n)
+        self._check(self.lib.orc_gws_get_state(self.h, _dp(u), _dp(p)))
+        return u, p
 
     def close(self):
         if getattr(self, "h", None):

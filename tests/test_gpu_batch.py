@@ -174,6 +174,9 @@ def test_autotuner_picks_a_timed_configuration():
     # the timing sweeps left the state alone: a second handle without tuning runs the same steps
     bt2 = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp32")
     bt2.set_tuning(t["tile_z"], t["tile_y"], t["planes_x"], t["sites_per_thread"])
+    f = bt.form()
+    if f["persistent"]:  # the autotuner kept the persistent form: the second handle takes it too
+        bt2.set_persistent(f["tile_z"], f["tile_y"], f["planes_x"], f["sites_per_thread"])
     for i, c in enumerate(cases):
         bt2.set_state(i, c[3], c[4], c[5])
     bt2.initialize()
@@ -200,3 +203,113 @@ def test_fp32_vector_tiles_track_fp64():
         assert rel(fa, fb) < 1e-6
         assert abs(sa["aI"] - sb["aI"]) / sb["aI"] < 1e-7
         assert abs(m32[i]["friedmann"][0] - m64[i]["friedmann"][0]) < 1e-6
+
+
+# ---- persistent form: the whole evolve call as one launch of thread-block clusters ----------------
+def run_persistent(cases, precision, steps, shape, chunks=1):
+    from cosmolattice_b200.batch import LatticeBatch
+
+    bt = LatticeBatch([(c[2], c[1]) for c in cases], precision=precision)
+    bt.set_persistent(*shape)
+    for i, c in enumerate(cases):
+        bt.set_state(i, c[3], c[4], c[5])
+    bt.initialize()
+    m0 = [bt.measure(i) for i in range(len(cases))]
+    form = bt.form()
+    launches = []
+    for _ in range(chunks):
+        l0 = bt.kernel_launches()
+        bt.evolve(steps // chunks)
+        launches.append(bt.kernel_launches() - l0)
+    out = [bt.get_state(i) for i in range(len(cases))]
+    m1 = [bt.measure(i, m0[i]["energies"][-1]) for i in range(len(cases))]
+    bt.close()
+    return out, m0, m1, form, launches
+
+
+# (tile z sites, tile y, x-planes, z sites per thread): every compiled shape, x-runs shorter than,
+# equal to and longer than the members
+PERSIST_SHAPES = [(32, 8, 8, 1), (32, 4, 3, 1), (32, 8, 64, 1), (32, 8, 16, 2), (64, 8, 8, 4)]
+
+
+@pytest.mark.parametrize("shape", PERSIST_SHAPES)
+@pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV4", True), ("VV2", False)])
+def test_persistent_form_matches_oracle_per_member(shape, evolver, expansion):
+    # FP64: every member within 1e-12 per site of the oracle run on its own, over two evolve calls
+    # (the second starts from the other buffer parity), each call one kernel launch
+    cases = members(evolver, expansion) if shape[3] == 1 else members4(evolver, expansion)
+    out, m0, m1, form, launches = run_persistent(cases, "fp64", 30, shape, chunks=2)
+    assert form["persistent"] == 1 and form["clusters"] == len(cases) and form["cluster_blocks"] == 8
+    assert (form["tile_z"], form["tile_y"], form["planes_x"], form["sites_per_thread"]) == shape
+    assert launches == [1, 1]
+    for i, c in enumerate(cases):
+        (fo, po, so), mo0, mo1 = run_oracle(c, 30)
+        fg, pg, sg = out[i]
+        assert rel(fg, fo) < 1e-12 and rel(pg, po) < 1e-12, (shape, i, rel(fg, fo), rel(pg, po))
+        assert abs(sg["aI"] - so["aI"]) <= 1e-10 * so["aI"]
+        assert abs(sg["aDotI"] - so["aDotI"]) <= 1e-10 * abs(so["aDotI"]) + 1e-300
+        for a, b in zip(m1[i]["energies"], mo1["energies"]):
+            assert abs(a - b) <= 1e-10 * abs(b) + 1e-300
+
+
+def test_persistent_form_many_members_per_cluster():
+    # more members than the device holds clusters at once: each cluster takes several members in
+    # turn; every member within 1e-12 of the per-stage form (FP64)
+    from cosmolattice_b200.batch import LatticeBatch
+
+    rng = np.random.default_rng(3)
+    specs = [(int(rng.choice([8, 12, 16, 20])), float(np.exp(rng.uniform(np.log(0.5), np.log(2.0)))),
+              float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2)))), f"m{k}") for k in range(400)]
+    cases = [make_scalar_case(N=N, evolver="VV2", expansion=True, dt=0.01, seed=s, amp=a, extra={"lambda_prog": l})
+             for N, l, a, s in specs]
+    ref, _, _ = run_batch(cases, "fp64", 12, tuning=(32, 8, 32, 1))
+    out, _, m1, form, launches = run_persistent(cases, "fp64", 12, (32, 8, 8, 1))
+    print("form", form)
+    assert form["clusters"] < len(cases) and launches == [1]
+    for i in range(len(cases)):
+        assert rel(out[i][0], ref[i][0]) < 1e-13 and rel(out[i][1], ref[i][1]) < 1e-13, i
+        assert abs(out[i][2]["aI"] - ref[i][2]["aI"]) <= 1e-13 * ref[i][2]["aI"]
+    # spot-check members against the oracle
+    for i in (0, 199, 399):
+        st, _, _ = run_oracle(cases[i], 12)
+        assert rel(out[i][0], st[0]) < 1e-12 and rel(out[i][1], st[1]) < 1e-12
+
+
+def test_persistent_fp32_tracks_fp64():
+    # the FP32 split form in the persistent launch: every member within the FP32 bounds of its FP64
+    # run, and equal to the per-stage FP32 form up to the order of the volume sums
+    cases = members4("VV2")
+    g32, _, m32, _, _ = run_persistent(cases, "fp32", 60, (64, 8, 8, 4))
+    g64, _, m64 = run_batch(cases, "fp64", 60, tuning=(32, 8, 32, 1))
+    s32, _, _ = run_batch(cases, "fp32", 60, tuning=(64, 16, 16, 4))
+    for i in range(len(cases)):
+        (fa, pa, sa), (fb, pb, sb) = g32[i], g64[i]
+        assert rel(fa, fb) < 1e-6
+        assert rel(fa - fa.mean(), fb - fb.mean()) < 1e-3
+        assert abs(sa["aI"] - sb["aI"]) <= 1e-7 * sb["aI"]
+        assert abs(m32[i]["friedmann"][0] - m64[i]["friedmann"][0]) <= 1e-6
+        assert rel(fa, s32[i][0]) < 1e-6 and rel(pa, s32[i][1]) < 1e-5
+
+
+def test_autotuner_times_both_forms_and_leaves_the_state():
+    from cosmolattice_b200.batch import LatticeBatch
+
+    cases = members4("VV2")
+    bt = LatticeBatch([(c[2], c[1]) for c in cases], precision="fp32")
+    for i, c in enumerate(cases):
+        bt.set_state(i, c[3], c[4], c[5])
+    bt.initialize()
+    f0 = [bt.get_state(i) for i in range(len(cases))]
+    bt.autotune(2)
+    f = bt.form()
+    print("form", f)
+    assert f["candidates"] >= 4 and f["ms_graph"] > 0 and f["ms_persistent"] > 0
+    assert f["persistent"] == (1 if f["ms_persistent"] < f["ms_graph"] else 0)
+    f1 = [bt.get_state(i) for i in range(len(cases))]
+    for a, b in zip(f0, f1):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    l0 = bt.kernel_launches()
+    bt.evolve(5)
+    # per-stage form: the first half kick (tail, sweep, tail), then a sweep and a tail per step
+    assert bt.kernel_launches() - l0 == (1 if f["persistent"] else 3 + 2 * 5)
+    bt.close()

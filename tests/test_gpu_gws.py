@@ -1,0 +1,164 @@
+"""Gravitational waves of the scalar singlets (clb_gws_*, clb_gw_spectrum) on the B200.
+
+Against the oracle's restatement (the reference's default: a leapfrog for the GWs staggered over
+the VV matter evolver, evolver.h:102-138; the kernel of gwskernels.h:27-33 with the PITensor.h
+source): the GW field and momenta per site within 1e-12 of each component's max after 30 steps
+taken in three calls with syncs between them, the matter state as in the scalar parity tests.
+The GW energy spectrum against a numpy restatement of the TT projectors (gwsprojector.h) on the
+same momenta: 1e-10 per populated bin, counts bit-exact.  A longitudinal-plus-trace tensor
+projects to zero.  Parity with TempLat is unpinned: its ConstructSymTraceless, forwDiff and the
+spectrum's integrate() are not on disk (the stated choices are in clb_gws.cu).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import make_scalar_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(model, evolver, precision="fp64", N=24):
+    from cosmolattice_b200 import Lattice
+    from oracle.oracle import OracleLattice
+
+    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, model=model, amp=3e-2)
+    gpu, cpu = Lattice(m, rp, precision=precision), OracleLattice(m, rp)
+    for lat in (gpu, cpu):
+        lat.gws_enable()
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        for _ in range(3):
+            lat.evolve(10)
+            lat.sync()
+    return rp, m, gpu, cpu
+
+
+@pytest.mark.parametrize("model,evolver", [("lphi4_1f", "VV2"), ("lphi4_1f", "VV4"), ("lphi4", "VV2")])
+def test_gw_evolution_matches_oracle(model, evolver):
+    rp, m, gpu, cpu = _pair(model, evolver)
+    ug, pg = gpu.gws_get_state()
+    uc, pc = cpu.gws_get_state()
+    (fg, _, sg), (fc, _, sc) = gpu.get_state(), cpu.get_state()
+    gpu.close()
+    cpu.close()
+    assert np.abs(pc).max() > 0 and np.abs(uc).max() > 0
+    for a, b in ((ug, uc), (pg, pc)):
+        for c in range(5):
+            x, y = a.reshape(5, -1)[c], b.reshape(5, -1)[c]
+            assert np.abs(x - y).max() <= 1e-12 * np.abs(y).max(), c
+    assert np.abs(fg - fc).max() <= 1e-12 * np.abs(fc).max()
+    assert abs(sg["aI"] - sc["aI"]) <= 1e-12 * sc["aI"]
+
+
+@pytest.mark.parametrize("prj", [1, 2, 3])
+@pytest.mark.parametrize("ps_type", [1, 2])
+def test_gw_spectrum_matches_numpy(prj, ps_type):
+    from oracle.spectrum import gw_spectrum
+
+    rp, m, gpu, cpu = _pair("lphi4_1f", "VV2")
+    cpu.close()
+    N = rp.N
+    k, v, cnt, frac = gpu.gw_spectrum(prj_type=prj, ps_type=ps_type)
+    mm = gpu.measure(1.0)
+    _, pi = gpu.gws_get_state()
+    gpu.close()
+    fac = (m.fStar / m.MPl) ** 2 / (4 * mm["aI"] ** 6 * mm["energies"][-1])
+    ko, vo, co = gw_spectrum(pi.reshape(5, N, N, N), rp.dx, prj_type=prj, ps_type=ps_type, factor=fac)
+    assert cnt.tolist() == co.tolist()
+    band = vo > 1e-8 * vo.max()
+    assert band.sum() > 3
+    assert np.all(np.abs(v - vo)[band] <= 1e-10 * vo[band])
+    assert np.allclose(k, ko, rtol=1e-12)
+    ntil = ko / rp.kIR
+    assert abs(frac - sum(vo[b] * 1.0 / ntil[b] for b in range(len(vo)) if co[b] > 0 and ntil[b] > 0)) <= 1e-10 * frac
+
+
+def test_longitudinal_and_trace_parts_project_to_zero():
+    # pi_ij = kL_i kL_j f(k) + delta_ij g(k), stored traceless, in Fourier space with the type-1
+    # lattice momenta: the TT projector annihilates it, so its spectrum is rounding only, while a
+    # transverse-traceless tensor of the same size keeps its power
+    from cosmolattice_b200 import Lattice
+
+    N = 16
+    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver="VV2", amp=1e-2)
+    rng = np.random.default_rng(5)
+    nx = np.fft.fftfreq(N, 1.0 / N)
+    kL = [np.sin(2 * math.pi / N * nx)[:, None, None], np.sin(2 * math.pi / N * nx)[None, :, None],
+          np.sin(2 * math.pi / N * nx)[None, None, :]]
+    fk = np.fft.fftn(rng.normal(size=(N, N, N)))
+    gk = np.fft.fftn(rng.normal(size=(N, N, N)))
+
+    def comp(i, j):
+        return np.real(np.fft.ifftn(kL[i] * kL[j] * fk + (gk if i == j else 0)))
+
+    t = [[comp(i, j) for j in range(3)] for i in range(3)]
+    tr3 = (t[0][0] + t[1][1] + t[2][2]) / 3
+    pi_long = np.stack([t[0][0] - tr3, t[0][1], t[0][2], t[1][1] - tr3, t[1][2]])
+    # transverse-traceless: modes with k along z only, u_11 = -u_22 = h(k), u_12 = h2(k)
+    hz = np.fft.fftn(rng.normal(size=(N, N, N)))
+    sel = (nx[:, None, None] == 0) & (nx[None, :, None] == 0) & (nx[None, None, :] != 0)
+    h1 = np.real(np.fft.ifftn(np.where(sel, hz, 0)))
+    pi_tt = np.stack([h1, h1, np.zeros_like(h1), -h1, np.zeros_like(h1)])
+    out = {}
+    for name, arr in (("long", pi_long), ("tt", pi_tt)):
+        lat = Lattice(m, rp)
+        lat.gws_enable()
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.gws_set_state(np.zeros(5 * N ** 3), arr.ravel())
+        _, v, _, _ = lat.gw_spectrum(prj_type=1)
+        out[name] = v
+        lat.close()
+    scale = np.abs(pi_long).max() ** 2 / np.abs(pi_tt).max() ** 2
+    assert out["tt"].max() > 0
+    # rounding: the longitudinal tensor's projected power is ~1e-17 of its unprojected size
+    assert out["long"].max() <= 1e-13 * scale * out["tt"].max()
+
+
+def test_fp32_gws_track_fp64():
+    rp, m, g64, cpu = _pair("lphi4_1f", "VV2")
+    cpu.close()
+    _, v64, _, f64 = g64.gw_spectrum()
+    g64.close()
+    rp, m, g32, cpu = _pair("lphi4_1f", "VV2", precision="fp32")
+    cpu.close()
+    _, v32, _, f32 = g32.gw_spectrum()
+    g32.close()
+    band = v64 > 1e-6 * v64.max()
+    assert np.all(np.abs(v32 - v64)[band] <= 1e-4 * v64[band])
+    assert abs(f32 - f64) <= 1e-4 * f64
+
+
+def test_gws_reject_other_evolvers_and_models():
+    from cosmolattice_b200 import Lattice, _capi
+    from conftest import make_u1_case
+
+    for ev in ("LF", "PV2"):
+        par, rp, m, f, p, sf = make_scalar_case(N=8, evolver=ev)
+        lat = Lattice(m, rp)
+        with pytest.raises(_capi.ClbError) as ei:
+            lat.gws_enable()
+        assert ei.value.code == _capi.CLB_EUNSUPPORTED
+        lat.close()
+    par, rp, m, f, p, sf = make_u1_case(N=8)
+    lat = Lattice(m, rp)
+    with pytest.raises(_capi.ClbError):
+        lat.gws_enable()
+    lat.close()
+
+
+def test_run_writes_gw_files(tmp_path):
+    from cosmolattice_b200 import ParameterParser, run
+
+    params = {"N": 16, "kIR": 1.0, "dt": 0.01, "evolver": "VV2", "expansion": "true", "lambda": 1.0,
+              "tMax": 0.3, "tOutputFreq": 0.1, "tOutputInfreq": 0.1, "kCutOff": 4, "fluct_amplitude": 3e-2,
+              "initial_amplitudes": "5.6964e18", "initial_momenta": "0", "withGWs": "true", "print_headers": "true"}
+    _, lat = run(ParameterParser(params=params), "lphi4_1f", outdir=str(tmp_path))
+    lat.close()
+    lines = open(tmp_path / "average_energies_gws.txt").read().splitlines()
+    assert lines[0] == "#t    rhoGW_over_rho    rhoGW" and len(lines) == 4
+    vals = np.array([list(map(float, l.split())) for l in lines[1:]])
+    assert vals[0, 1] == 0.0 and np.all(vals[1:, 1] > 0)  # the GWs start at zero and grow
+    assert (tmp_path / "spectra_energy_gws.txt").exists()

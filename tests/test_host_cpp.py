@@ -154,8 +154,12 @@ def test_host_gauge_models_match_python(tmp_path, model):
         assert a.shape == b.shape, name
         assert np.array_equal(np.isnan(a), np.isnan(b)), name
         # each column within 1e-13 of its largest magnitude: the two hosts form the initial-state
-        # masses in their own operation order, so values that average to zero differ by 1e-19
+        # masses in their own operation order, so values that average to zero differ by 1e-19.
+        # The Gauss files' violation column is itself a ratio of rounding residue (~1e-12) to the
+        # charge scale: it is held to 1e-13 absolute instead.
         scale = np.nanmax(np.abs(b), axis=0, keepdims=True)
+        if "gauss" in name:
+            scale[0, 1] = 1.0
         assert np.all(np.nan_to_num(np.abs(a - b)) <= 1e-13 * scale), name
 
 

@@ -147,3 +147,15 @@ def test_restart_file_round_trip(tmp_path):
     st2.rp = rp2
     with pytest.raises(ValueError):
         restart.load_sim(path, st2, m2)
+
+
+def test_gw_parameters():
+    # withGWs, doLFforGWs and GWprojectorType (runparameters.h:120-123): the GWs run as the
+    # reference's default leapfrog over the matter evolver
+    base = {"N": 8, "kIR": 1.0, "dt": 0.01, "withGWs": "true"}
+    rp = RunParameters(ParameterParser(params=base))
+    assert rp.withGWs and rp.doLFforGWs and rp.GWprojectorType == 2
+    with pytest.raises(RunParametersInconsistent):
+        RunParameters(ParameterParser(params=dict(base, doLFforGWs="false")))
+    with pytest.raises(RunParametersInconsistent):
+        RunParameters(ParameterParser(params=dict(base, GWprojectorType=4)))
