@@ -114,9 +114,10 @@ void sweep_tile(clb_batch *b, bool drift, bool kick, int red, double dtw, double
   const R *fin = static_cast<const R *>(b->f[b->cf]), *pin = static_cast<const R *>(b->p[b->cf]);
   R *fout = static_cast<R *>(b->f[drift ? b->cf ^ 1 : b->cf]), *pout = static_cast<R *>(b->p[drift ? b->cf ^ 1 : b->cf]);
   const dim3 grid(b->total_blocks), block(BZ, BY);
+  constexpr int SM = Ring<BZ, BY, VZ, R>::BYTES;
 #define CLB_BS(D, K, RD)                                                                                               \
-  k_batch_sweep<BZ, BY, VZ, R, D, K, RD><<<grid, block, 0, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk,    \
-                                                                          b->d_st, b->rs, dtw, h1, h2, b->d_part)
+  k_batch_sweep<BZ, BY, VZ, R, D, K, RD><<<grid, block, SM, b->stream>>>(fin, pin, fout, pout, b->d_lat, b->d_blk,   \
+                                                                           b->d_st, b->rs, dtw, h1, h2, b->d_part)
   if (drift && kick && red)
     CLB_BS(true, true, 3);
   else if (drift && kick)
@@ -126,6 +127,37 @@ void sweep_tile(clb_batch *b, bool drift, bool kick, int red, double dtw, double
   else
     CLB_BS(false, false, 3);
 #undef CLB_BS
+}
+
+// Rings above the default 48 KB of dynamic shared memory need the kernel's opt-in (set once per
+// kernel, outside any stream capture: at layout time).
+template <int BZ, int BY, int VZ, class R> cudaError_t ring_attr()
+{
+  constexpr int SM = Ring<BZ, BY, VZ, R>::BYTES;
+  if (SM <= 48 * 1024) return cudaSuccess;
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_batch_sweep<BZ, BY, VZ, R, true, true, 3>, a, SM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_sweep<BZ, BY, VZ, R, true, true, 0>, a, SM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_sweep<BZ, BY, VZ, R, false, true, 0>, a, SM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_sweep<BZ, BY, VZ, R, false, false, 3>, a, SM);
+  return e;
+}
+
+template <class R> cudaError_t ring_attr_tile(int t)
+{
+  switch (t) {
+  case 0: return ring_attr<32, 4, 1, R>();
+  case 1: return ring_attr<32, 8, 1, R>();
+  case 2: return ring_attr<32, 16, 1, R>();
+  case 3: return ring_attr<64, 4, 1, R>();
+  case 4: return ring_attr<16, 8, 2, R>();
+  case 5: return ring_attr<16, 16, 2, R>();
+  case 6: return ring_attr<32, 8, 2, R>();
+  case 7: return ring_attr<8, 16, 4, R>();
+  case 8: return ring_attr<8, 32, 4, R>();
+  case 9: return ring_attr<16, 8, 4, R>();
+  default: return ring_attr<16, 16, 4, R>();
+  }
 }
 
 // One sweep with the current configuration; advance = false leaves the buffer parity and the
@@ -157,6 +189,8 @@ void sweep_launch(clb_batch *b, bool drift, bool kick, int red, double dtw, doub
 cudaError_t layout(clb_batch *b, int tile, int run)
 {
   const TileShape t = kTiles[tile];
+  const cudaError_t ea = b->fp32 ? ring_attr_tile<float>(tile) : ring_attr_tile<double>(tile);
+  if (ea != cudaSuccess) return ea;
   int blocks = 0;
   b->blk_lat.clear();
   for (int i = 0; i < b->n; ++i) {
@@ -322,6 +356,7 @@ void evolve_launches(clb_batch *b, int64_t nsteps)
 
 // ---- persistent form ----------------------------------------------------------------------------
 template <class R, int BZ, int BY, int VZ> struct Persist {
+  static_assert(Ring<BZ, BY, VZ, R>::BYTES <= 48 * 1024, "persistent shapes keep the default shared-memory limit");
   static cudaLaunchConfig_t config(clb_batch *b, int clusters, cudaLaunchAttribute *at)
   {
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -331,7 +366,7 @@ template <class R, int BZ, int BY, int VZ> struct Persist {
     cudaLaunchConfig_t c{};
     c.gridDim = dim3((unsigned)(clusters * kClusterCTAs));
     c.blockDim = dim3(BZ, BY);
-    c.dynamicSmemBytes = 0;
+    c.dynamicSmemBytes = Ring<BZ, BY, VZ, R>::BYTES; // at most 48 KB for the persistent shapes
     c.stream = b->stream;
     c.attrs = at;
     c.numAttrs = 1;

@@ -30,23 +30,21 @@ struct BatchLat {
   SFParams sp;
 };
 
-// DRIFT / KICK / RED as in k_sweep; one block = one (BZ VZ) x BY (z, y) tile of one member, each
-// thread owning VZ consecutive z sites (vector loads and stores; every member's N a multiple of
-// VZ), marching over LX x-planes.  Tile shape, VZ and LX are chosen by the batch autotuner.
-// fin/pin are never written; fout/pout alias them only without DRIFT.
-// Register budget: that of four resident 256-thread blocks per SM (64 registers) for one site per
-// thread (1.43x over the unbounded build at 32 x 8), twice that for vector sites (their VZ-wide
-// planes spill at 64).
-#ifndef CLB_BATCH_MINB
-#define CLB_BATCH_MINB 4
-#endif
-template <class R, int VZ> __device__ __forceinline__ void ldg_v(const R *p, R (&v)[VZ])
+// Asynchronous global -> shared copies (cp.async, sm_80+): 4, 8 or 16 bytes, both addresses
+// aligned to the size.  A commit closes a group; wait_group<K> returns when at most K of this
+// thread's groups are still in flight.
+template <int B> __device__ __forceinline__ void cp_async(void *dst, const void *src)
 {
-  if constexpr (VZ == 1)
-    v[0] = p[0];
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
   else
-    ldv<R, VZ>(p, v);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(B) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+// VZ consecutive values to global memory (vector stores when VZ > 1; aligned: N % VZ == 0).
 template <class R, int VZ> __device__ __forceinline__ void stg_v(R *p, const R (&v)[VZ])
 {
   if constexpr (VZ == 1)
@@ -55,18 +53,61 @@ template <class R, int VZ> __device__ __forceinline__ void stg_v(R *p, const R (
     stv<R, VZ>(p, v);
 }
 
+// VZ consecutive elements (VZ * sizeof(R) bytes, aligned to that size on both sides).
+template <class R, int VZ> __device__ __forceinline__ void cp_run(R *dst, const R *src)
+{
+  constexpr int BYTES = VZ * (int)sizeof(R), CH = BYTES >= 16 ? 16 : BYTES;
+#pragma unroll
+  for (int o = 0; o < BYTES; o += CH)
+    cp_async<CH>(reinterpret_cast<char *>(dst) + o, reinterpret_cast<const char *>(src) + o);
+}
+
+// The shared-memory ring of one tile: D slots, each one x-plane of fields and one of momenta,
+// (BY + 2) rows (the y halos in rows 0 and BY + 1) of ROW elements: the z-left halo in column
+// VZ - 1, the tile's sites from column VZ (aligned for VZ-wide copies), the z-right halo after
+// them.  D: as many planes as fit in 32 KB, 3 to 8; the loads run D - 2 planes ahead of the plane
+// whose x-neighbour is read.
+template <int BZ, int BY, int VZ, class R> struct Ring {
+  static constexpr int TZ = BZ * VZ;
+  static constexpr int ROW = TZ + 2 * VZ;
+  static constexpr int PLANE = (BY + 2) * ROW;
+  static constexpr int PLANE_BYTES = 2 * PLANE * (int)sizeof(R);
+  static constexpr int FIT = 32768 / PLANE_BYTES;
+  static constexpr int D = FIT > 8 ? 8 : (FIT < 3 ? 3 : FIT);
+  static constexpr int BYTES = D * PLANE_BYTES;
+};
+
+// DRIFT / KICK / RED as in k_sweep; one block = one (BZ VZ) x BY (z, y) tile of one member, each
+// thread owning VZ consecutive z sites (every member's N a multiple of VZ), marching over LX
+// x-planes.  Tile shape, VZ and LX are chosen by the batch autotuner.
+// Each x-plane of the tile (with its y and z halos) is copied to a slot of the shared-memory ring
+// (Ring) by cp.async, D - 2 planes ahead of use, so that several planes of loads are in flight
+// per thread while one is computed.  The drift is applied where a value is read (a neighbour's
+// drifted value is recomputed from its field and momentum: the same inputs give the same value).
+// fin/pin are never written; fout/pout alias them only without DRIFT (the in-place kick writes
+// only momenta of the block's own sites, which only this thread reads).
+// Register budget: that of four resident 256-thread blocks per SM (64 registers) for one site per
+// thread, twice that for vector sites.
+#ifndef CLB_BATCH_MINB
+#define CLB_BATCH_MINB 4
+#endif
+
 // One tile of one member: the member's block `local` of its (z, y, x-run) grid, with the block's
 // sums of the averages in v (thread 0).  k_batch_sweep runs one tile per block; the persistent
-// k_batch_persist runs a cluster's share of a member's tiles one after another.
+// k_batch_persist runs a cluster's share of a member's tiles one after another.  The ring is the
+// kernel's dynamic shared memory (Ring::BYTES).
 template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
 __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, R *pout, const BatchLat &lt,
                                            DevState *__restrict__ st, int local, int rs, double dtw_d, double h1,
                                            double h2, double (&vout)[kRedSlots])
 {
   using A = Ar<R>;
+  using RG = Ring<BZ, BY, VZ, R>;
   constexpr bool SPLIT = sizeof(R) == 4;
-  constexpr int TZ = BZ * VZ; // z sites per tile
-  __shared__ R tile[3][BY + 2][TZ + 2];
+  constexpr int TZ = RG::TZ, ROW = RG::ROW, PL = RG::PLANE, D = RG::D, L = D - 1;
+  extern __shared__ __align__(16) unsigned char clb_batch_ring[];
+  R *const ringF = reinterpret_cast<R *>(clb_batch_ring);
+  R *const ringP = ringF + D * PL;
   __shared__ double red_smem[(BZ * BY / 32) * kRedSlots];
   const int bx = local % lt.gx, by = (local / lt.gx) % lt.gy, bz = local / (lt.gx * lt.gy);
   const int N = lt.N;
@@ -101,83 +142,82 @@ __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, 
   const float h1f = (float)h1, h2f = (float)h2;
 
   auto sidx = [&](int x, int yy, int zz) -> size_t { return ((size_t)x * N + yy) * N + zz; };
-  auto ld1 = [&](size_t s) -> R {
-    R v = fin[s];
-    if (DRIFT) v = drift_val<R>(v, pin[s], pd, dtw);
-    return v;
-  };
-  auto ldq = [&](size_t s, R (&out)[VZ]) { // VZ drifted values
-    ldg_v<R, VZ>(fin + s, out);
-    if (DRIFT) {
-      R pv[VZ];
-      ldg_v<R, VZ>(pin + s, pv);
-#pragma unroll
-      for (int k = 0; k < VZ; ++k) out[k] = drift_val<R>(out[k], pv[k], pd, dtw);
+  auto wrapx = [&](int xx) { return xx >= N ? xx - N : (xx < 0 ? xx + N : xx); };
+  constexpr bool LOADP = DRIFT || KICK || (RED & 1);
+  const bool hym = ty == 0, hyp = ty == hy - 1, hzm = tz == 0, hzp = zt + VZ == hz;
+  const int ctr = (ty + 1) * ROW + VZ + zt; // the thread's first site in a slot
+  // Plane j of the tile's sequence (x = x0 - 1 + j) into slot j % D: the thread's own sites, and
+  // for the computed planes x0 .. x1 - 1 the halo values it owns; momenta where they are read.
+  auto issue = [&](int j) {
+    const int xp = x0 - 1 + j;
+    if (valid && xp <= x1) {
+      const int xs = wrapx(xp);
+      const bool halo = xp >= x0 && xp < x1;
+      R *F = ringF + (j % D) * PL, *P = ringP + (j % D) * PL;
+      const size_t s = sidx(xs, y, z);
+      cp_run<R, VZ>(F + ctr, fin + s);
+      if (LOADP) cp_run<R, VZ>(P + ctr, pin + s);
+      if (halo) {
+        if (hym) {
+          cp_run<R, VZ>(F + VZ + zt, fin + sidx(xs, ym, z));
+          if (DRIFT) cp_run<R, VZ>(P + VZ + zt, pin + sidx(xs, ym, z));
+        }
+        if (hyp) {
+          cp_run<R, VZ>(F + (hy + 1) * ROW + VZ + zt, fin + sidx(xs, yp, z));
+          if (DRIFT) cp_run<R, VZ>(P + (hy + 1) * ROW + VZ + zt, pin + sidx(xs, yp, z));
+        }
+        if (hzm) {
+          cp_run<R, 1>(F + ctr - 1, fin + sidx(xs, y, zm));
+          if (DRIFT) cp_run<R, 1>(P + ctr - 1, pin + sidx(xs, y, zm));
+        }
+        if (hzp) {
+          cp_run<R, 1>(F + ctr + VZ, fin + sidx(xs, y, zp));
+          if (DRIFT) cp_run<R, 1>(P + ctr + VZ, pin + sidx(xs, y, zp));
+        }
+      }
     }
+    cp_async_commit(); // one group per plane, empty past the run
+  };
+  // the drifted field at element e of slot j
+  auto fval = [&](int j, int e) -> R {
+    const R f = ringF[(j % D) * PL + e];
+    return DRIFT ? drift_val<R>(f, ringP[(j % D) * PL + e], pd, dtw) : f;
   };
 
   double acc_pi2 = 0, acc_g2 = 0, acc_v = 0, acc_p = 0;
   long long cnt = 0;
-  constexpr bool LOADP = DRIFT || KICK || (RED & 1);
-  // One plane's values for this thread: its VZ sites, the in-plane halo values it owns, momenta.
-  struct Plane {
-    R c[VZ], pi[VZ], hm[VZ], hp[VZ], zl, zr;
-  };
-  const bool hym = ty == 0, hyp = ty == hy - 1, hzm = tz == 0, hzp = zt + VZ == hz;
-  auto load = [&](int xp, bool tile_too, Plane &q) {
-    const size_t s = sidx(xp, y, z);
-    ldg_v<R, VZ>(fin + s, q.c);
-    if (LOADP) ldg_v<R, VZ>(pin + s, q.pi);
-    if (DRIFT) {
-#pragma unroll
-      for (int k = 0; k < VZ; ++k) q.c[k] = drift_val<R>(q.c[k], q.pi[k], pd, dtw);
-    }
-    if (tile_too) {
-      if (hym) ldq(sidx(xp, ym, z), q.hm);
-      if (hyp) ldq(sidx(xp, yp, z), q.hp);
-      if (hzm) q.zl = ld1(sidx(xp, y, zm));
-      if (hzp) q.zr = ld1(sidx(xp, y, zp));
-    }
-  };
-  auto store = [&](int tb, const Plane &q) {
-#pragma unroll
-    for (int k = 0; k < VZ; ++k) {
-      tile[tb][ty + 1][1 + zt + k] = q.c[k];
-      if (hym) tile[tb][0][1 + zt + k] = q.hm[k];
-      if (hyp) tile[tb][hy + 1][1 + zt + k] = q.hp[k];
-    }
-    if (hzm) tile[tb][ty + 1][0] = q.zl;
-    if (hzp) tile[tb][ty + 1][hz + 1] = q.zr;
-  };
-  auto wrapx = [&](int xx) { return xx >= N ? xx - N : xx; };
   R prev[VZ], cur[VZ], nxt[VZ], piC[VZ], piN[VZ];
 #pragma unroll
   for (int k = 0; k < VZ; ++k) prev[k] = cur[k] = nxt[k] = piC[k] = piN[k] = R(0);
   if (x0 < x1) {
-    // prologue: planes x0 - 1 (centre), x0 and x0 + 1; loads run two planes ahead of the compute
-    Plane q0{}, q1{};
+    // prologue: planes x0 - 1 .. x0 + L - 1 in flight; the first two into registers
+#pragma unroll 1
+    for (int j = 0; j <= L; ++j) issue(j);
+    cp_async_wait<L - 1>();
+    __syncthreads();
     if (valid) {
-      ldq(sidx(x0 == 0 ? N - 1 : x0 - 1, y, z), prev);
-      load(x0, true, q0);
-      load(wrapx(x0 + 1), x0 + 1 < x1, q1);
-      store(0, q0);
-      if (x0 + 1 < x1) store(1, q1);
 #pragma unroll
       for (int k = 0; k < VZ; ++k) {
-        cur[k] = q0.c[k];
-        piC[k] = q0.pi[k];
-        nxt[k] = q1.c[k];
-        piN[k] = q1.pi[k];
+        prev[k] = fval(0, ctr + k);
+        cur[k] = fval(1, ctr + k);
+        if (LOADP) piC[k] = ringP[(1 % D) * PL + ctr + k];
       }
     }
-    __syncthreads();
-    int b = 0;
+#pragma unroll 1
     for (int x = x0; x < x1; ++x) {
-      const int b2 = b == 0 ? 2 : b - 1; // buffer of plane x + 2 (held plane x - 1)
-      const bool has2 = x + 2 <= x1, tile2 = x + 2 < x1;
-      Plane q2{};
-      if (valid && has2) load(wrapx(x + 2), tile2, q2);
+      const int j = x - x0 + 1; // plane x's sequence index; x + 1 is j + 1
+      cp_async_wait<L - 2>();   // planes up to x + 1 have landed (this thread's copies)
+      __syncthreads();          // ... and every thread's; slot (j + L) % D = (j - 1) % D is free
+      issue(j + L);
       if (valid) {
+        const R *F = ringF + (j % D) * PL;
+        const R *P = ringP + (j % D) * PL;
+#pragma unroll
+        for (int k = 0; k < VZ; ++k) {
+          nxt[k] = fval(j + 1, ctr + k);
+          if (LOADP) piN[k] = ringP[((j + 1) % D) * PL + ctr + k];
+        }
+        auto nb = [&](int e) -> R { return DRIFT ? drift_val<R>(F[e], P[e], pd, dtw) : F[e]; };
         const size_t s = sidx(x, y, z);
         R outp[VZ];
         if (DRIFT) stg_v<R, VZ>(fout + s, cur);
@@ -186,9 +226,9 @@ __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, 
 #pragma unroll
           for (int k = 0; k < VZ; ++k) {
             const float c = cur[k];
-            const float ynb = tile[b][ty + 2][1 + zt + k], ymb = tile[b][ty][1 + zt + k];
-            const float znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : tile[b][ty + 1][1 + zt + VZ];
-            const float zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : tile[b][ty + 1][zt];
+            const float ynb = nb(ctr + ROW + k), ymb = nb(ctr - ROW + k);
+            const float znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : nb(ctr + VZ);
+            const float zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : nb(ctr - 1);
             if (KICK) {
               const float lap = inv_dx2 * ((((nxt[k] + prev[k]) - 2.f * c) + ((ynb + ymb) - 2.f * c)) + ((znb + zmb) - 2.f * c));
               float ddv;
@@ -229,9 +269,9 @@ __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, 
 #pragma unroll
           for (int k = 0; k < VZ; ++k) {
             const R c = cur[k];
-            const R ynb = tile[b][ty + 2][1 + zt + k], ymb = tile[b][ty][1 + zt + k];
-            const R znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : tile[b][ty + 1][1 + zt + VZ];
-            const R zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : tile[b][ty + 1][zt];
+            const R ynb = nb(ctr + ROW + k), ymb = nb(ctr - ROW + k);
+            const R znb = k + 1 < VZ ? cur[k + 1 < VZ ? k + 1 : 0] : nb(ctr + VZ);
+            const R zmb = k > 0 ? cur[k > 0 ? k - 1 : 0] : nb(ctr - 1);
             if (KICK) {
               const R txv = A::sub(A::add(nxt[k], prev[k]), A::mul(two, c));
               const R tyv = A::sub(A::add(ynb, ymb), A::mul(two, c));
@@ -259,14 +299,10 @@ __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, 
           prev[k] = cur[k];
           cur[k] = nxt[k];
           piC[k] = piN[k];
-          nxt[k] = q2.c[k];
-          piN[k] = q2.pi[k];
         }
-        if (tile2) store(b2, q2);
       }
-      __syncthreads();
-      b = b == 2 ? 0 : b + 1;
     }
+    cp_async_wait<0>(); // only empty groups remain past the run
   }
   if (RED) {
     if constexpr (SPLIT) {
@@ -279,7 +315,7 @@ __device__ __forceinline__ void batch_tile(const R *fin, const R *pin, R *fout, 
 #pragma unroll
     for (int k = 0; k < kRedSlots; ++k) vout[k] = v[k];
   }
-  __syncthreads(); // the next tile of the same block reuses the shared tile and scratch
+  __syncthreads(); // the next tile of the same block reuses the ring and the scratch
 }
 
 template <int BZ, int BY, int VZ, class R, bool DRIFT, bool KICK, int RED>
