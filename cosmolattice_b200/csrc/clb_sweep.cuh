@@ -301,7 +301,8 @@ __global__ void __launch_bounds__(SH::THREADS)
     return LOADP ? drift1(fv, box(s, f, 1)[o]) : fv;
   };
   // neighbour values of the current plane (stage s): y - 1, y + 1 rows and the z - 1, z + VZ cells,
-  // each drifted as it is read
+  // each drifted as it is read (a drift of each plane once, written back to shared memory by its
+  // owners, measured no faster: the stores and the halo work cost what the drifts saved)
   auto neighbours = [&](int s, int f, R (&ym)[VZ], R (&yp)[VZ], R &zm, R &zp) {
     dquad(s, f, toff - BOXZ, ym, nullptr);
     dquad(s, f, toff + BOXZ, yp, nullptr);
@@ -315,10 +316,12 @@ __global__ void __launch_bounds__(SH::THREADS)
 
   // Thread 0 tracks the planes issued and the first plane whose wait did not complete, for the
   // drain on abort: a wait that gave up leaves its copy in flight.
+  // Plane j sits in ring stage j % S with barrier parity (j / S) & 1; the loop keeps both as running
+  // counters (no division by the run-time ring depth per plane).
   int issued = min(S, nplanes), waited = 0;
   bool gave_up = false;
-  auto wait_plane = [&](int j) {
-    if (!mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1), a.tries)) {
+  auto wait_plane = [&](int j, int stage, uint32_t parity) {
+    if (!mbar_wait(&bars[stage], parity, a.tries)) {
       abort_flag = 1;
       gave_up = true;
     }
@@ -333,13 +336,13 @@ __global__ void __launch_bounds__(SH::THREADS)
   const bool has_ghost = nvalid > 0 && (ghost_y != -2 || kz_first >= 0 || kz_last >= 0);
 
   R prev[NS][VZ], cur[NS][VZ], nxt[NS][VZ], piC[NS][VZ], piN[NS][VZ];
-  wait_plane(0);
+  wait_plane(0, 0, 0u); // S >= 3: planes 0, 1 and 2 are in stages 0, 1 and 2 of the first lap
 #pragma unroll
   for (int f = 0; f < NS; ++f) dquad(0, f, toff, prev[f], nullptr);
-  wait_plane(1);
+  wait_plane(1, 1, 0u);
 #pragma unroll
   for (int f = 0; f < NS; ++f) {
-    dquad(1 % S, f, toff, cur[f], LOADP ? &piC[f] : nullptr);
+    dquad(1, f, toff, cur[f], LOADP ? &piC[f] : nullptr);
   }
   __syncthreads();
   if (abort_flag) goto drain;
@@ -355,10 +358,16 @@ __global__ void __launch_bounds__(SH::THREADS)
     for (int f = 0; f < NS; ++f) acc_p[f] = 0;
     long long cnt = 0; // FP32 split: sites summed by this thread
     long long pbase = (long long)x0 * pd.plane;
+    int sb = 1, sn = 2;  // stages of planes j and j + 1
+    uint32_t par_n = 0u; // barrier parity of plane j + 1
     for (int x = x0; x < x1; ++x, pbase += pd.plane) {
       const int j = x - x0 + 1;
-      const int sb = j % S, sn = (j + 1) % S;
-      wait_plane(j + 1);
+      // the drifted plane x is known here: store it first, so the registers are free long before
+      // the rotation below overwrites them
+      if (DRIFT && nvalid == VZ)
+#pragma unroll
+        for (int f = 0; f < NS; ++f) stv<R, VZ>(fout + ((long long)f * pd.comp + pbase + ioff), cur[f]);
+      wait_plane(j + 1, sn, par_n);
       R ym[NS][VZ], yp[NS][VZ], zmv[NS], zpv[NS];
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
@@ -480,8 +489,7 @@ __global__ void __launch_bounds__(SH::THREADS)
       for (int f = 0; f < NS; ++f) {
         const long long o = (long long)f * pd.comp + pbase + ioff;
         if (nvalid == VZ) {
-          if (DRIFT) stv<R, VZ>(fout + o, cur[f]);
-          if (KICK) stv<R, VZ>(pout + o, outp[f]);
+          if (KICK) stv<R, VZ>(pout + o, outp[f]); // fields stored at the top of the iteration
         } else {
 #pragma unroll
           for (int k = 0; k < VZ; ++k)
@@ -521,6 +529,11 @@ __global__ void __launch_bounds__(SH::THREADS)
           cur[f][k] = nxt[f][k];
           if (LOADP) piC[f][k] = piN[f][k];
         }
+      sb = sn;
+      if (++sn == S) {
+        sn = 0;
+        par_n ^= 1u;
+      }
     }
     griddep_launch(); // planes done: the tail may be scheduled
     if (RED) {
