@@ -36,7 +36,7 @@ constexpr int kElemBlocks = 148 * 8; // elementwise grid: 8 resident 256-thread 
 constexpr uint32_t kWaitTries = 1u << 24; // bound of each mbarrier wait in the sweeps
 constexpr size_t kStageMin = (size_t)1 << 23; // host-transfer staging: >= 64 MiB of doubles
 constexpr int kDefaultShapeFP64 = 0;          // ShapeW
-constexpr int kDefaultShapeFP32 = 2;          // ShapeH
+constexpr int kDefaultShapeFP32 = 4;          // ShapeK
 constexpr int kPlanesPerBlock = 32;           // x-run length of one sweep block
 
 } // namespace
@@ -172,6 +172,8 @@ void sweep(clb_handle *h, int kind, int fb, int pb, int fo, int po, double dtw, 
   if constexpr (NS == 1) {
     if (h->shape == 1) return sweep_sh<R, NS, ShapeQ, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
     if (h->shape == 2) return sweep_sh<R, NS, ShapeH, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
+    if (h->shape == 3) return sweep_sh<R, NS, ShapeL, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
+    if (h->shape == 4) return sweep_sh<R, NS, ShapeK, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
   }
   sweep_sh<R, NS, ShapeW, DRIFT, KICK, RED>(h, kind, fb, pb, fo, po, dtw, h1, h2, dtw0);
 }
@@ -768,14 +770,19 @@ int clb_create(const clb_config *cfg, const clb_model_desc *md, clb_handle **out
   a.inv_dx2 = 1.0 / (cfg->dx * cfg->dx);
   a.cs.mc = ScalarModel::couplings(md->couplings);
   // ring depth: as many plane stages as fit in ~48 KiB, at least 3 (planes x, x+1 and one in flight)
-  // sweep shape: default per storage type and field count, CLB_SWEEP_SHAPE=0/1/2 overrides (one field)
+  // sweep shape: default per storage type and field count, CLB_SWEEP_SHAPE=0..4 overrides (one field)
   h->shape = (h->NS == 1) ? (h->fp32 ? kDefaultShapeFP32 : kDefaultShapeFP64) : 0;
   if (const char *env = std::getenv("CLB_SWEEP_SHAPE")) {
     const int v = std::atoi(env);
-    if (h->NS == 1 && v >= 0 && v <= 2) h->shape = v;
+    if (h->NS == 1 && v >= 0 && v <= 4) h->shape = v;
   }
-  h->bz = 64;
-  h->by = h->shape == 1 ? 16 : 8;
+  {
+    // sites per block along z and y of ShapeW, ShapeQ, ShapeH, ShapeL, ShapeK
+    static const int kShapeBZ[5] = {64, 64, 64, 128, 128};
+    static const int kShapeBY[5] = {8, 16, 8, 8, 4};
+    h->bz = kShapeBZ[h->shape];
+    h->by = kShapeBY[h->shape];
+  }
   if (const char *env = std::getenv("CLB_PDL")) h->pdl = std::atoi(env) != 0;
   const size_t box_bytes = (size_t)(h->bz + 2 * (16 / (int)h->esz)) * (size_t)(h->by + 2) * h->esz;
   const size_t slot = ((box_bytes + 127) / 128) * 128;

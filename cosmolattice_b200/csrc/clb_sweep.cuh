@@ -53,6 +53,8 @@ template <int TZ_, int TY_, int VZ_> struct Shape {
 using ShapeW = Shape<32, 8, 2>;  // 64 x 8 sites, 2 per thread
 using ShapeQ = Shape<16, 16, 4>; // 64 x 16 sites, 4 per thread
 using ShapeH = Shape<16, 8, 4>;  // 64 x 8 sites, 4 per thread, 128 threads
+using ShapeL = Shape<32, 8, 4>;  // 128 x 8 sites, 4 per thread, 256 threads
+using ShapeK = Shape<32, 4, 4>;  // 128 x 4 sites, 4 per thread, 128 threads
 
 template <class R, class SH> struct TileGeom {
   static constexpr int G = 16 / (int)sizeof(R);

@@ -281,6 +281,7 @@ def test_sweep_launch_knobs_compute_the_same_step(monkeypatch, precision, tol, a
 
     par, rp, m, f, p, sf = make_scalar_case(N=64, evolver="VV2", expansion=True, amp=1e-2)
     settings = [{}, {"CLB_SWEEP_SHAPE": "0"}, {"CLB_SWEEP_SHAPE": "1"}, {"CLB_SWEEP_SHAPE": "2"},
+                {"CLB_SWEEP_SHAPE": "3"}, {"CLB_SWEEP_SHAPE": "4"},
                 {"CLB_SWEEP_XS": "1"}, {"CLB_SWEEP_XS": "8"}, {"CLB_SWEEP_XS": "16"},
                 {"CLB_SWEEP_RING_KB": "64"}, {"CLB_PDL": "0"}]
     out = []
