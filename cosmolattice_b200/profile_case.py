@@ -3,7 +3,8 @@
     python -m cosmolattice_b200.profile_case --N 256 --steps 10 --precision fp64 --path fused
     python -m cosmolattice_b200.profile_case --model lphi4U1 --N 128 --steps 5
     python -m cosmolattice_b200.profile_case --model lphi4SU2U1 --N 96 --steps 3 [--precision fp32]
-    python -m cosmolattice_b200.profile_case --model batch --members 64 --steps 5 --precision fp32
+    python -m cosmolattice_b200.profile_case --model batch --members 64 --steps 5 --precision fp32 [--tile 32,16,32,4]
+    python -m cosmolattice_b200.profile_case --N 128 --steps 4 --gws
     python -m cosmolattice_b200.profile_case --model lphi4U1 --N 96 --steps 4 --mode adjoint
     python -m cosmolattice_b200.profile_case --model lphi4SU2U1 --N 64 --steps 2 --mode tangent
 
@@ -64,6 +65,9 @@ def _batch(args):
         rp = RunParameters(par)
         cases.append((lphi4_1f(par, rp), rp))
     bt = LatticeBatch(cases, precision=args.precision)
+    if args.tile:  # a fixed sweep configuration instead of the autotuner's
+        tz, ty, px, vz = (int(v) for v in args.tile.split(","))
+        bt.set_tuning(tz, ty, px, vz)
     for i, (m, rp) in enumerate(cases):
         n = rp.N ** 3
         bt.set_state(i, 1.0 + 1e-3 * rng.standard_normal(n), 1e-3 * rng.standard_normal(n),
@@ -87,6 +91,8 @@ def main(argv=None):
     ap.add_argument("--evolver", default="VV2")
     ap.add_argument("--model", default="lphi4", choices=["lphi4", "lphi4U1", "lphi4SU2U1", "batch"])
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--tile", default="", help="batch: tile_z,tile_y,planes_x,sites_per_thread (no autotuning)")
+    ap.add_argument("--gws", action="store_true", help="lphi4: evolve the GW sector too")
     ap.add_argument("--mode", default="evolve", choices=["evolve", "adjoint", "tangent"],
                     help="adjoint: clb_forward + clb_backward (lphi4U1); tangent: the tangent-linear "
                          "form along g_SU2 (lphi4SU2U1)")
@@ -122,6 +128,8 @@ def main(argv=None):
     f = 1.0 + 1e-3 * rng.standard_normal(N ** 3)
     p = 1e-3 * rng.standard_normal(N ** 3)
     lat = Lattice(model, rp, precision=args.precision, path=args.path)
+    if args.gws:
+        lat.gws_enable()
     lat.set_state(f, p, {"aI": 1.0, "aSI": 1.0, "aIM": 1.0, "aDotI": 0.5, "aDotSI": 0.5})
     lat.initialize()
     t0 = time.perf_counter()
