@@ -218,4 +218,27 @@ template <class Fn> __device__ __forceinline__ void for_sites(int N, size_t n3, 
   }
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80+): 4, 8 or 16 bytes, both addresses
+// aligned to the size.  A commit closes a group; wait_group<K> returns when at most K of this
+// thread's groups are still in flight.
+template <int B> __device__ __forceinline__ void cp_async(void *dst, const void *src)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+// VZ consecutive elements (VZ * sizeof(R) bytes, aligned to that size on both sides).
+template <class R, int VZ> __device__ __forceinline__ void cp_run(R *dst, const R *src)
+{
+  constexpr int BYTES = VZ * (int)sizeof(R), CH = BYTES >= 16 ? 16 : BYTES;
+#pragma unroll
+  for (int o = 0; o < BYTES; o += CH)
+    cp_async<CH>(reinterpret_cast<char *>(dst) + o, reinterpret_cast<const char *>(src) + o);
+}
+
 } // namespace clb

@@ -282,6 +282,126 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
   }
 }
 
+// ---- the kick on staged planes ----------------------------------------------------------------
+// One block per (z, y) tile of BZ x BY sites (one per thread) and an x-run of LX planes; the
+// blocks take tiles in turn (grid-stride over tiles, so the partial rows are the grid's).  Each
+// x-plane of the five field components, with a one-cell halo in y and z (corners included: the
+// curl term reads x + i - j), is copied by cp.async into a ring of D shared-memory slots, D - 3
+// planes ahead of the plane being kicked, whose x - 1 and x + 1 neighbours stay in the ring.  The
+// site arithmetic is u1_site's, on a view of the ring: the component stride is the ring's and the
+// neighbour offsets are ring offsets, so every site's kernel values are bitwise those of
+// k_u1_kick; only the order of the volume sums differs.
+template <class S> struct U1Ring {
+  static constexpr int BZ = 32, BY = 8, THREADS = BZ * BY;
+  static constexpr int ROW = BZ + 2, PLANE = (BY + 2) * ROW; // one component's plane with halos
+  static constexpr int D = sizeof(S) == 8 ? 6 : 8;           // ring slots
+  static constexpr int CS = D * PLANE;                       // component stride in the ring
+  static constexpr int BYTES = 5 * CS * (int)sizeof(S);
+};
+
+template <int NK, bool RF, bool RP, class S>
+__global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
+    k_u1_kick_tile(const S *__restrict__ f, S *__restrict__ p, U1Params a, U1Kick kc, const U1State *__restrict__ st,
+                   double *__restrict__ partials, int LX)
+{
+  using RG = U1Ring<S>;
+  constexpr int BZ = RG::BZ, BY = RG::BY, ROW = RG::ROW, PL = RG::PLANE, D = RG::D, L = D - 2;
+  static_assert(L >= 2, "two planes ahead at least");
+  extern __shared__ __align__(16) unsigned char u1_ring_raw[];
+  S *const ring = reinterpret_cast<S *>(u1_ring_raw); // [5][D][BY + 2][ROW]
+  __shared__ double smem[(256 / 32) * kU1Red];
+  using T = S;
+  const int N = a.N;
+  const size_t n3 = a.n3;
+  U1Params av = a;
+  av.n3 = (size_t)RG::CS; // u1_site reads component c of ring index t at ring[c * CS + t]
+  const T kA = (T)st->kA, kB2 = (T)st->kB2, kG = (T)st->kG;
+  const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
+  const int gz = (N + BZ - 1) / BZ, gy = (N + BY - 1) / BY, gxr = (N + LX - 1) / LX;
+  const long long ntiles = (long long)gz * gy * gxr;
+  auto wrap = [&](int v) { return v < 0 ? v + N : (v >= N ? v - N : v); };
+  double acc[kU1Red];
+#pragma unroll
+  for (int k = 0; k < kU1Red; ++k) acc[k] = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int z0 = (int)(tile % gz) * BZ, y0 = (int)((tile / gz) % gy) * BY, x0 = (int)(tile / ((long long)gz * gy)) * LX;
+    const int x1 = min(N, x0 + LX), hz = min(BZ, N - z0), hy = min(BY, N - y0);
+    const bool valid = tz < hz && ty < hy;
+    // plane j of the run (x = x0 - 1 + j, up to x1) into slot j % D: the (hy + 2) x (hz + 2) box
+    auto issue = [&](int j) {
+      const int xp = x0 - 1 + j;
+      if (xp <= x1) {
+        const size_t xs = (size_t)wrap(xp);
+        S *slot = ring + (j % D) * PL;
+        for (int cell = threadIdx.x; cell < PL; cell += RG::THREADS) {
+          const int r = cell / ROW, c = cell - r * ROW;
+          if (r > hy + 1 || c > hz + 1) continue;
+          const size_t g = (xs * N + (size_t)wrap(y0 - 1 + r)) * N + (size_t)wrap(z0 - 1 + c);
+#pragma unroll
+          for (int comp = 0; comp < 5; ++comp) cp_async<(int)sizeof(S)>(slot + comp * RG::CS + cell, f + comp * n3 + g);
+        }
+      }
+      cp_async_commit(); // one group per plane, empty past the run
+    };
+#pragma unroll 1
+    for (int j = 0; j <= L; ++j) issue(j);
+#pragma unroll 1
+    for (int x = x0; x < x1; ++x) {
+      const int j = x - x0 + 1;
+      cp_async_wait<L - 2>(); // planes up to x + 1 have landed (this thread's copies)
+      __syncthreads();        // ... and every thread's; slot (j + L) % D, plane x - 2's, is free
+      issue(j + L);
+      if (valid) {
+        const int sc = j % D, sp = (j + 1) % D, sm = (j - 1) % D;
+        const size_t t = (size_t)sc * PL + (size_t)(ty + 1) * ROW + (size_t)(tz + 1);
+        const long long op[3] = {(long long)(sp - sc) * PL, ROW, 1};
+        const long long om[3] = {(long long)(sm - sc) * PL, -ROW, -1};
+        U1Site<T> o;
+        u1_site<(NK > 0)>(ring, av, t, op, om, kA, kB2, kG, o);
+        if (RF) {
+          acc[2] += (double)u1_cs_grad2(o, (T)a.dx);
+          acc[3] += (double)u1_b2(o);
+          acc[4] += (double)u1_pot(o, (T)a.c4);
+        }
+        const size_t g = ((size_t)x * N + (size_t)(y0 + ty)) * N + (size_t)(z0 + tz);
+        double q[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) q[c] = (double)p[c * n3 + g];
+#pragma unroll
+        for (int k = 0; k < (NK > 0 ? NK : 1); ++k) {
+          if (NK > 0) {
+            q[0] = u1_a(q[0], u1_m(kc.hc[k], (double)o.Kr));
+            q[1] = u1_a(q[1], u1_m(kc.hc[k], (double)o.Ki));
+#pragma unroll
+            for (int i = 0; i < 3; ++i) q[2 + i] = u1_a(q[2 + i], u1_m(kc.hu[k], (double)o.KA[i]));
+            if (sizeof(S) == 4) {
+#pragma unroll
+              for (int c = 0; c < 5; ++c) q[c] = (double)(S)q[c]; // the stored value after this kick
+            }
+          }
+          if (RP) {
+            acc[k == 0 ? 0 : 5] += u1_a(u1_m(q[0], q[0]), u1_m(q[1], q[1]));
+            acc[k == 0 ? 1 : 6] += u1_a(u1_a(u1_m(q[2], q[2]), u1_m(q[3], q[3])), u1_m(q[4], q[4]));
+          }
+        }
+        if (NK > 0) {
+#pragma unroll
+          for (int c = 0; c < 5; ++c) p[c * n3 + g] = (S)q[c];
+        }
+      }
+    }
+    cp_async_wait<0>(); // only empty groups remain past the run
+    __syncthreads();    // the next tile refills the ring
+  }
+  if (RF || RP) {
+    block_reduce<kU1Red, 256>(acc, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < kU1Red; ++k) partials[(size_t)blockIdx.x * kU1Red + k] = acc[k];
+    }
+  }
+}
+
 // Drifts phi += ((pow(aSI, alpha-3) dt) w) pi_phi and A += ((pow(aSI, alpha-1) w) dt) pi_A
 // (velocityverlet.h:193-210; the leapfrog's forms leapfrog.h:203-217 are w = 1).
 template <class S>

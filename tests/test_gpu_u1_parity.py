@@ -290,3 +290,37 @@ def test_gradient_workload_geometry_128_vv4_100_steps():
     g, c, meas = run_pair(N, "VV4", True, 100, dt=0.005, amp=1e-3, extra={"gU1s": 0.5})
     check_state(g, c, N)
     check_meas(meas["gpu"], meas["cpu"])
+
+
+@pytest.mark.parametrize("N,evolver,expansion,precision", [(20, "VV2", False, "fp64"), (36, "VV4", False, "fp64"),
+                                                           (36, "LF", True, "fp64"), (20, "VV2", True, "fp32"),
+                                                           (36, "PV2", False, "fp32")])
+def test_staged_kick_equals_site_kick(monkeypatch, N, evolver, expansion, precision):
+    # the kick on staged planes (k_u1_kick_tile, the default) and the site-by-site kick (CLB_U1_TILE=0)
+    # evaluate every site with the same arithmetic: without expansion (no volume sums feed back) the
+    # states agree bitwise; with expansion a(t) takes the sums in another order, 1e-13.  N = 20 and
+    # 36 leave partial tiles in z (32 sites) and y (8 rows); x-runs of 16 and 5 planes.
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = make_u1_case(N=N, evolver=evolver, expansion=expansion, amp=3e-2)
+    out = []
+    for env in ({"CLB_U1_TILE": "0"}, {}, {"CLB_U1_TILE_LX": "5"}):
+        monkeypatch.delenv("CLB_U1_TILE", raising=False)
+        monkeypatch.delenv("CLB_U1_TILE_LX", raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        lat = Lattice(m, rp, precision=precision)
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.evolve(12)
+        lat.sync()
+        out.append(lat.get_state())
+        lat.close()
+    (f0, p0, s0) = out[0]
+    for fg, pg, sg in out[1:]:
+        if not expansion:
+            assert np.array_equal(fg, f0) and np.array_equal(pg, p0)
+        else:
+            assert np.abs(fg - f0).max() <= 1e-13 * np.abs(f0).max()
+            assert np.abs(pg - p0).max() <= 1e-13 * np.abs(p0).max()
+            assert abs(sg["aI"] - s0["aI"]) <= 1e-14 * s0["aI"]
