@@ -231,6 +231,159 @@ __global__ void __launch_bounds__(256, CLB_U1_ADJ_MINB)
   }
 }
 
+// The same sweep on staged planes: each x-plane of the state (f, p) and of the incoming cotangent
+// lambda_A, with a one-cell y/z halo (corners included), is copied by cp.async into a ring of D
+// shared-memory slots ahead of use; the JVP direction at a cell is formed from the ring as k_u1_adj
+// forms it from global memory, and u1_pieces runs on ring indices, so every site's values are
+// those of k_u1_adj.  32 x 4-site tiles, one site per thread, two 128-thread blocks per SM (the
+// registers of one 256-thread block: no spills); the blocks take tiles in turn, so the partial rows
+// are the grid's.
+template <class S> struct U1AdjRing {
+  static constexpr int BZ = 32, BY = 4, THREADS = BZ * BY;
+  static constexpr int ROW = BZ + 2, PLANE = (BY + 2) * ROW;
+  static constexpr int D = 4, CS = D * PLANE;
+  static constexpr int BYTES = 5 * CS * (2 * (int)sizeof(S) + (int)sizeof(double));
+};
+
+template <class S>
+__global__ void __launch_bounds__(128, 2)
+    k_u1_adj_tile(const S *__restrict__ f, const S *__restrict__ p, const double *__restrict__ pbar_in,
+                  double *__restrict__ qbar, double *__restrict__ pbar_out, U1Params a, U1AdjArgs g,
+                  double *__restrict__ partials, int LX)
+{
+  using RG = U1AdjRing<S>;
+  constexpr int BZ = RG::BZ, BY = RG::BY, ROW = RG::ROW, PL = RG::PLANE, D = RG::D, CS = RG::CS, L = D - 2;
+  extern __shared__ __align__(16) unsigned char adj_ring_raw[];
+  double *const rL = reinterpret_cast<double *>(adj_ring_raw); // [5][D][BY + 2][ROW] lambda_A
+  S *const rF = reinterpret_cast<S *>(rL + 5 * CS);             // fields
+  S *const rP = rF + 5 * CS;                                   // momenta
+  __shared__ double smem[(128 / 32) * kAdjSlots];
+  const int N = a.N;
+  const size_t n3 = a.n3;
+  double acc[kAdjSlots];
+#pragma unroll
+  for (int k = 0; k < kAdjSlots; ++k) acc[k] = 0;
+  const double two_n3 = 2.0 * g.inv_n3;
+  const double cP = (g.ApiA + g.ApiB) * two_n3, cE = (g.AEA + g.AEB) * two_n3;
+  const double kJ = g.kA * g.J0 * a.gQ;
+  const double inv_r2 = 1.0 / g.r2, cJ = g.kA * g.J0 * inv_r2, cD = g.AD * g.inv_n3 * (2.0 * a.gQ / a.dx);
+  const double two_dx = 2.0 / a.dx, dJ = g.dkA * g.J0 * a.gQ;
+  const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
+  const int gz = (N + BZ - 1) / BZ, gy = (N + BY - 1) / BY, gxr = (N + LX - 1) / LX;
+  const long long ntiles = (long long)gz * gy * gxr;
+  auto wrap = [&](int v) { return v < 0 ? v + N : (v >= N ? v - N : v); };
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int z0 = (int)(tile % gz) * BZ, y0 = (int)((tile / gz) % gy) * BY, x0 = (int)(tile / ((long long)gz * gy)) * LX;
+    const int x1 = min(N, x0 + LX), hz = min(BZ, N - z0), hy = min(BY, N - y0);
+    const bool valid = tz < hz && ty < hy;
+    auto issue = [&](int j) {
+      const int xp = x0 - 1 + j;
+      if (xp <= x1) {
+        const size_t xs = (size_t)wrap(xp);
+        const int so = (j % D) * PL;
+        for (int cell = threadIdx.x; cell < PL; cell += RG::THREADS) {
+          const int r = cell / ROW, c = cell - r * ROW;
+          if (r > hy + 1 || c > hz + 1) continue;
+          const size_t y = (xs * N + (size_t)wrap(y0 - 1 + r)) * N + (size_t)wrap(z0 - 1 + c);
+#pragma unroll
+          for (int comp = 0; comp < 5; ++comp) {
+            cp_async<(int)sizeof(S)>(rF + comp * CS + so + cell, f + comp * n3 + y);
+            cp_async<(int)sizeof(S)>(rP + comp * CS + so + cell, p + comp * n3 + y);
+            cp_async<8>(rL + comp * CS + so + cell, pbar_in + comp * n3 + y);
+          }
+        }
+      }
+      cp_async_commit();
+    };
+    // the JVP direction at ring index y: M^{-1} (hA lambda_A + hB lambda_B), as k_u1_adj's ld
+    auto ld = [&](int c, size_t y) -> TD {
+      const double lA = rL[c * CS + y];
+      const int sec = c < 2 ? 0 : 1;
+      const double lB = lA + (sec == 0 ? cP : cE) * (double)rP[c * CS + y];
+      const double w = g.hA[sec] * lA + g.hB[sec] * lB;
+      return TD((double)rF[c * CS + y], sec == 0 ? w : g.r2 * w);
+    };
+#pragma unroll 1
+    for (int j = 0; j <= L; ++j) issue(j);
+#pragma unroll 1
+    for (int x = x0; x < x1; ++x) {
+      const int j = x - x0 + 1;
+      cp_async_wait<L - 2>();
+      __syncthreads();
+      issue(j + L);
+      if (valid) {
+        const int sc = j % D, sp = (j + 1) % D, sm = (j - 1) % D;
+        const size_t t = (size_t)sc * PL + (size_t)(ty + 1) * ROW + (size_t)(tz + 1);
+        const long long op[3] = {(long long)(sp - sc) * PL, ROW, 1};
+        const long long om[3] = {(long long)(sm - sc) * PL, -ROW, -1};
+        const size_t s = ((size_t)x * N + (size_t)(y0 + ty)) * N + (size_t)(z0 + tz);
+        U1Pieces o;
+        u1_pieces(ld, a, t, op, om, o);
+        TD K[5];
+        K[0] = g.kA * o.cl[0] - g.kB2 * o.dv[0];
+        K[1] = g.kA * o.cl[1] - g.kB2 * o.dv[1];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) K[2 + i] = g.kG * o.cc[i] - kJ * o.im[i];
+        double lA[5], lB[5], qb[5], pc[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          lA[c] = rL[c * CS + t];
+          pc[c] = (double)rP[c * CS + t];
+          lB[c] = lA[c] + (c < 2 ? cP : cE) * pc[c];
+          qb[c] = qbar[c * n3 + s];
+        }
+        qb[0] += K[0].d;
+        qb[1] += K[1].d;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) qb[2 + i] += K[2 + i].d * inv_r2;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) qb[c] += g.AD * (-two_n3) * o.cl[c].v + g.AV * g.inv_n3 * o.dv[c].v;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+          qb[2 + i] += cD * o.im[i].v + g.AB * (-two_n3) * o.cc[i].v;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const double da = g.dkA * o.cl[c].v - g.dkB2 * o.dv[c].v;
+          acc[0] += g.hA[0] * lA[c] * da;
+          acc[1] += g.hB[0] * lB[c] * da;
+          acc[3] += (g.hA[0] * lA[c] + g.hB[0] * lB[c]) * (-g.kB2 * 4.0 * o.vn[c]);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const double da = g.dkG * o.cc[i].v - dJ * o.im[i].v;
+          acc[0] += g.hA[1] * lA[2 + i] * da;
+          acc[1] += g.hB[1] * lB[2 + i] * da;
+          const double Ai = (double)rF[(2 + i) * CS + t];
+          const double wi = g.r2 * (g.hA[1] * lA[2 + i] + g.hB[1] * lB[2 + i]);
+          acc[2] += -cJ * (Ai * o.im[i].d + wi * o.im[i].v);
+          acc[4] += two_dx * Ai * o.im[i].v;
+        }
+        acc[5] += o.n4;
+        double pb[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          const bool phi = c < 2;
+          const double p1 = pc[c] - g.hB[phi ? 0 : 1] * K[c].v;
+          pb[c] = lB[c] + (phi ? g.cdf : g.cda) * qb[c];
+          acc[phi ? 6 : 7] += p1 * qb[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          qbar[c * n3 + s] = qb[c];
+          pbar_out[c * n3 + s] = pb[c];
+        }
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+  block_reduce<kAdjSlots, 128>(acc, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < kAdjSlots; ++k) partials[(size_t)blockIdx.x * kAdjSlots + k] = acc[k];
+  }
+}
+
 // Copies the U(1) scalar state into row r of the per-boundary record (adjoint recompute).
 __global__ void k_u1_record(const U1State *__restrict__ st, U1State *__restrict__ rec, int64_t r) { rec[r] = *st; }
 

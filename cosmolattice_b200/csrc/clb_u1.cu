@@ -27,6 +27,7 @@ constexpr int kU1Blocks = 148 * 8; // grid-stride sweeps: 8 resident 256-thread 
 struct U1Sector {
   void *f = nullptr, *p = nullptr; // 5 x N^3 each, FP64 or FP32 (esz bytes per value)
   int tile_lx = 8;                  // x-run of the staged kick; 0: the site-by-site kick
+  int adj_lx = 16;                  // x-run of the staged adjoint sweep (CLB_U1_ADJ_LX)
   bool fp32 = false;
   size_t esz = 8;
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
@@ -200,6 +201,19 @@ struct SegSave {
 template <int NK, bool RED, class S> void kick_save_t(clb_handle *h, const U1Kick &kc, char *slot, size_t half)
 {
   U1Sector *u = h->u1;
+  if (u->tile_lx > 0) {
+    static bool attr = false; // the ring is above the default 48 KB of dynamic shared memory
+    if (!attr) {
+      cudaFuncSetAttribute(k_u1_kick_tile<NK, RED, RED, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           U1Ring<S>::BYTES);
+      attr = true;
+    }
+    CLB_LAUNCH(h, K_U1_KICK,
+               k_u1_kick_tile<NK, RED, RED, S, true, true><<<kU1Blocks, 256, U1Ring<S>::BYTES, h->stream>>>(
+                   static_cast<const S *>(u->f), static_cast<S *>(u->p), u->prm, kc, u->d_st, u->d_part, u->tile_lx,
+                   reinterpret_cast<S *>(slot), reinterpret_cast<S *>(slot + half)));
+    return;
+  }
   CLB_LAUNCH(h, K_U1_KICK,
              k_u1_kick<NK, RED, RED, S, true, true><<<kU1Blocks, 256, 0, h->stream>>>(
                  static_cast<const S *>(u->f), static_cast<S *>(u->p), u->prm, kc, u->d_st, u->d_part,
@@ -293,6 +307,7 @@ __attribute__((visibility("hidden"))) int u1_create(clb_handle *h)
   if (const char *env = std::getenv("CLB_U1_TILE")) u->tile_lx = std::atoi(env) == 0 ? 0 : u->tile_lx;
   if (const char *env = std::getenv("CLB_U1_TILE_LX"))
     if (u->tile_lx > 0) u->tile_lx = std::max(1, std::atoi(env));
+  if (const char *env = std::getenv("CLB_U1_ADJ_LX")) u->adj_lx = std::max(1, std::atoi(env));
   const size_t bytes = 5 * h->n3 * u->esz;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, bytes) == cudaSuccess && cudaMalloc(&u->p, bytes) == cudaSuccess;
@@ -676,6 +691,16 @@ template <class T>
 void adj_launch(clb_handle *h, const void *f, const void *p, const double *pin, double *pout, const U1AdjArgs &g)
 {
   U1Sector *u = h->u1;
+  if (u->tile_lx > 0) { // the sweep on staged planes (CLB_U1_TILE=0: site by site)
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_u1_adj_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, U1AdjRing<T>::BYTES);
+      attr = true;
+    }
+    k_u1_adj_tile<T><<<kU1Blocks, U1AdjRing<T>::THREADS, U1AdjRing<T>::BYTES, h->stream>>>(
+        static_cast<const T *>(f), static_cast<const T *>(p), pin, u->qbar, pout, u->prm, g, u->d_apart, u->adj_lx);
+    return;
+  }
   k_u1_adj<T><<<kU1Blocks, 256, 0, h->stream>>>(static_cast<const T *>(f), static_cast<const T *>(p), pin, u->qbar,
                                                  pout, u->prm, g, u->d_apart);
 }

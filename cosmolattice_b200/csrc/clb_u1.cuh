@@ -299,10 +299,12 @@ template <class S> struct U1Ring {
   static constexpr int BYTES = 5 * CS * (int)sizeof(S);
 };
 
-template <int NK, bool RF, bool RP, class S>
+// SAVE and FAST as in k_u1_kick (the adjoint's segment recompute).
+template <int NK, bool RF, bool RP, class S, bool SAVE = false, bool FAST = false>
 __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
     k_u1_kick_tile(const S *__restrict__ f, S *__restrict__ p, U1Params a, U1Kick kc, const U1State *__restrict__ st,
-                   double *__restrict__ partials, int LX)
+                   double *__restrict__ partials, int LX, S *__restrict__ save_f = nullptr,
+                   S *__restrict__ save_p = nullptr)
 {
   using RG = U1Ring<S>;
   constexpr int BZ = RG::BZ, BY = RG::BY, ROW = RG::ROW, PL = RG::PLANE, D = RG::D, L = D - 2;
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
   extern __shared__ __align__(16) unsigned char u1_ring_raw[];
   S *const ring = reinterpret_cast<S *>(u1_ring_raw); // [5][D][BY + 2][ROW]
   __shared__ double smem[(256 / 32) * kU1Red];
-  using T = S;
+  using T = typename std::conditional<FAST && sizeof(S) == 8, FD, S>::type;
   const int N = a.N;
   const size_t n3 = a.n3;
   U1Params av = a;
@@ -377,6 +379,13 @@ __global__ void __launch_bounds__(256, CLB_U1_KICK_MINB)
             if (sizeof(S) == 4) {
 #pragma unroll
               for (int c = 0; c < 5; ++c) q[c] = (double)(S)q[c]; // the stored value after this kick
+            }
+            if (SAVE && k == 0) {
+#pragma unroll
+              for (int c = 0; c < 5; ++c) {
+                save_p[c * n3 + g] = (S)q[c];
+                save_f[c * n3 + g] = ring[c * RG::CS + t];
+              }
             }
           }
           if (RP) {

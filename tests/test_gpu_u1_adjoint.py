@@ -237,3 +237,26 @@ def test_energy_observable_after_spectrum_observable():
     assert O1 == O0
     for prm in g0:
         assert g1[prm] == g0[prm]
+
+
+@pytest.mark.parametrize("N,evolver,expansion", [(20, "VV2", True), (36, "VV4", True), (20, "VV2", False)])
+def test_staged_sweeps_give_the_site_by_site_gradient(monkeypatch, N, evolver, expansion):
+    # the kicks and the adjoint sweep on staged planes (the default) and site by site
+    # (CLB_U1_TILE=0) evaluate every site alike; the volume sums and the dot products are added in
+    # another order, so the observable and the gradients agree to 1e-12.  N = 20 and 36 leave
+    # partial tiles in z and y; x-runs of 16 and 5 planes for the adjoint sweep.
+    from cosmolattice_b200.adjoint import u1_gradients
+
+    par, rp, m, f, p, sf = case(N, evolver, expansion, 0.01)
+    out = []
+    for env in ({"CLB_U1_TILE": "0"}, {}, {"CLB_U1_ADJ_LX": "5"}):
+        for k in ("CLB_U1_TILE", "CLB_U1_ADJ_LX"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        out.append(u1_gradients(m, rp, 12, 5))
+    O0, g0, _ = out[0]
+    for O, g, _ in out[1:]:
+        assert abs(O - O0) <= 1e-12 * abs(O0)
+        for prm in ("amp", "c4", "gQ"):
+            assert abs(g[prm] - g0[prm]) <= 1e-12 * abs(g0[prm]), (prm, g[prm], g0[prm])
