@@ -813,14 +813,26 @@ def run_configs(local, cpu_cores_ok=True):
         bres[prec] = (bt.last_evolve_ms(), clk.summary(), bt.tuning(), bt.form())
         bt.close()
     seq_ms = 0.0
+    by_n = {}  # N -> [members, summed ms over KB steps]
     for c in cases:
         lat = Lattice(c[0], c[1], precision="fp32", device=local)
         lat.set_state(c[2], c[3], c[4])
         lat.initialize()
         lat.evolve(3)
         lat.evolve(KB)
-        seq_ms += lat.last_evolve_ms()
+        ms = lat.last_evolve_ms()
+        seq_ms += ms
+        by_n.setdefault(c[1].N, [0, 0.0])
+        by_n[c[1].N][0] += 1
+        by_n[c[1].N][1] += ms
         lat.close()
+    # per member size: the single-lattice handle's ms per step and its fraction of the HBM roofline
+    # on 16 B/site/step, to tell the handle's small-lattice overhead from the batch sweep's quality
+    one_by_n = {}
+    for n_, (cnt, ms) in sorted(by_n.items()):
+        per = ms / cnt / KB
+        one_by_n[str(n_)] = {"members": cnt, "ms_per_step": per,
+                             "roofline": roof(16 * n_ ** 3, per, "16 B/site/step FP32 storage, one lattice")}
     b32, b64 = bres["fp32"][0], bres["fp64"][0]
     out["batched"] = {
         "workload": "384 lphi4 lattices, N in {32,48,64,96}, lambda log-uniform [0.5,2], amplitude log-uniform "
@@ -830,7 +842,8 @@ def run_configs(local, cpu_cores_ok=True):
                  "roofline": roof(16 * bsites, b32 / KB, "16 B/site/step FP32 storage, whole step")},
         "fp64": {"value": bsites * KB / (b64 * 1e-3), "ms_per_step": b64 / KB,
                  "roofline": roof(32 * bsites, b64 / KB, "32 B/site/step FP64, whole step")},
-        "one_at_a_time_fp32": {"value": bsites * KB / (seq_ms * 1e-3), "ms_per_step": seq_ms / KB},
+        "one_at_a_time_fp32": {"value": bsites * KB / (seq_ms * 1e-3), "ms_per_step": seq_ms / KB,
+                               "by_N": one_by_n},
         "batched_speedup": seq_ms / b32,
         "tuning": bres["fp32"][2], "form": {"fp32": bres["fp32"][3], "fp64": bres["fp64"][3]},
         "clocks": bres["fp32"][1], "seconds": time.perf_counter() - t0}
