@@ -384,6 +384,21 @@ __global__ void __launch_bounds__(128, 2)
   }
 }
 
+// The cotangent of a momentum average <|pi_phi|^2> (or <sum pi_A^2>) with cotangent X adds
+// 2 X / N^3 p to the momenta's cotangent: pbar += cphi p on the complex-scalar components and
+// cA p on the gauge ones (set: pbar = that instead).  The leapfrog adjoint adds these after a
+// boundary's sweep, once the scale-factor chain has given them.
+template <class S>
+__global__ void __launch_bounds__(256)
+    k_u1_pbar_axpy(double *__restrict__ pbar, const S *__restrict__ p, size_t n3, double cphi, double cA, int set)
+{
+  const size_t n = 5 * n3, n2 = 2 * n3;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = (i < n2 ? cphi : cA) * (double)p[i];
+    pbar[i] = set ? v : pbar[i] + v;
+  }
+}
+
 // Copies the U(1) scalar state into row r of the per-boundary record (adjoint recompute).
 __global__ void k_u1_record(const U1State *__restrict__ st, U1State *__restrict__ rec, int64_t r) { rec[r] = *st; }
 

@@ -47,6 +47,12 @@ struct U1Sector {
   double *qbar = nullptr, *pbar[2] = {nullptr, nullptr};
   double *d_apart = nullptr, *d_asums = nullptr;
   int64_t fwd_steps = -1, fwd_K = 0;
+  // leapfrog: the forward's first kick weight (1/2 right after a sync), and whether it started
+  // right after clb_initialize, where the previous half step's <pi^2> is that of the start momenta
+  double fwd_w0 = 0.5;
+  bool fwd_fresh = false;
+  bool lf_fresh = false;      // no step since clb_initialize (not a restart)
+  bool init_corrected = false; // clb_initialize set aDot = sqrt(RHS)
   double fwd_w[5] = {0, 0, 0, 0, 0};
   double fwd_avg[5] = {0, 0, 0, 0, 0}; // final <|pi_phi|^2>, <|D phi|^2>, <pi_A^2>, <B^2>, <V>
   double fwd_a = 1, fwd_obs = 0;
@@ -230,7 +236,8 @@ template <class S> void kick_save_s(clb_handle *h, int nk, bool red, const U1Kic
 // VelocityVerlet::evolve over nsteps with merged kicks (as u1_evolve).  With sv, the state and the
 // scalar record at every stage boundary are kept: the merged sweep writes the state between its
 // two kicks, and its tail is split at the boundary so the record can be taken there.
-void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
+// hist: per-step history rows (clb_evolve sizes that buffer; the adjoint's runs write none).
+void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv, bool hist = true)
 {
   const double dt = h->cfg.dt;
   const bool ex = h->cfg.expansion != 0;
@@ -257,7 +264,7 @@ void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
       if (ex) {
         uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
         if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
-        tail(h, fl, true, w, wn, i + 1 == S ? k / (int64_t)S : -1);
+        tail(h, fl, true, w, wn, hist && i + 1 == S ? k / (int64_t)S : -1);
       }
     } else {
       char *slot = sv->seg + (size_t)(k + 1) * 2 * sv->half;
@@ -276,6 +283,39 @@ void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
       }
     }
   }
+}
+
+// LeapFrog::evolve over nsteps (as u1_evolve's leapfrog branch, the same launches, no history rows).  With sv, the
+// state before every kick (boundary b: the fields of step b and the momenta half a step earlier)
+// goes to boundary slot b, the scalar state after the step's kick tail to record row b, and the
+// end state to slot nsteps.
+void lf_run(clb_handle *h, int64_t nsteps, const SegSave *sv)
+{
+  const double dt = h->cfg.dt;
+  const bool ex = h->cfg.expansion != 0;
+  const double w0 = h->synced ? 0.5 : 1.0;
+  auto slot = [&](int64_t b) { return sv->seg + (size_t)b * 2 * sv->half; };
+  for (int64_t s = 0; s < nsteps; ++s) {
+    if (sv) copy_state(h, slot(s), slot(s) + sv->half, false);
+    if (s == 0) {
+      kick_sweep(h, 1, false, ex, lf_kick(dt, w0));
+      if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
+    } else {
+      kick_sweep(h, 1, ex, ex, lf_kick(dt, 1.0));
+      if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
+    }
+    if (sv) k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, s);
+    drift(h, 1.0);
+  }
+  if (ex) {
+    kick_sweep(h, 0, true, false, U1Kick{});
+    tail(h, T_STORE_FIELDS | T_HIST_EARLY, true);
+  }
+  if (sv) {
+    copy_state(h, slot(nsteps), slot(nsteps) + sv->half, false);
+    k_u1_record<<<1, 1, 0, h->stream>>>(h->u1->d_st, sv->rec, nsteps);
+  }
+  h->synced = false;
 }
 
 int check(clb_handle *h, const char *where)
@@ -443,6 +483,8 @@ __attribute__((visibility("hidden"))) int u1_initialize(clb_handle *h, int32_t c
   if (h->cfg.expansion && h->cfg.evolver == CLB_LF && correct_adot != CLB_INIT_RESTART) fl |= T_LF_CTOR;
   tail(h, fl, true);
   h->synced = !(correct_adot == CLB_INIT_RESTART && h->cfg.evolver == CLB_LF); // leapfrog.h:30-31
+  h->u1->lf_fresh = correct_adot != CLB_INIT_RESTART;
+  h->u1->init_corrected = (fl & T_CORRECT_ADOT) != 0;
   return check(h, "clb_initialize");
 }
 
@@ -451,6 +493,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
   const double dt = h->cfg.dt;
   const bool ex = h->cfg.expansion != 0;
   cudaEventRecord(h->ev_call[0], h->stream);
+  h->u1->lf_fresh = false;
   if (h->fb) {
     // fixed background (velocityverlet.h:74-118, leapfrog.h:55-89, positionverlet.h:45-99 with the
     // fixed branches): a from the closed form at the reference's stage times, no a-kicks and no
@@ -560,6 +603,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
 __attribute__((visibility("hidden"))) int u1_sync(clb_handle *h)
 {
   if (h->cfg.evolver == CLB_LF && !h->synced) {
+    h->u1->lf_fresh = false;
     kick_sweep(h, 1, false, h->cfg.expansion != 0 && !h->fb, lf_kick(h->cfg.dt, 0.5));
     if (h->cfg.expansion && !h->fb) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
   }
@@ -746,8 +790,9 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
                                                      int32_t nw, double *obs)
 {
   U1Sector *u = h->u1;
-  if (h->cfg.evolver == CLB_LF || is_pv(h->cfg.evolver))
-    return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers");
+  const bool lf = h->cfg.evolver == CLB_LF;
+  if (is_pv(h->cfg.evolver))
+    return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers and the leapfrog");
   if (h->fb) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the self-consistent expansion");
   if (nsteps < 1 || K < 1) return h->fail(CLB_EINVAL, "clb_forward: nsteps and checkpoint_every must be >= 1");
   if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
@@ -755,7 +800,7 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   if (e != cudaSuccess) return h->cuda_fail(e, "clb_forward");
   const size_t bytes = 5 * h->n3 * u->esz, dbytes = 5 * h->n3 * sizeof(double);
   const int64_t nck = (nsteps + K - 1) / K;
-  const int64_t S = 2 * (int64_t)h->ws.size() - 1;
+  const int64_t S = lf ? 1 : 2 * (int64_t)h->ws.size() - 1; // boundaries per step
   const int64_t seg_states = std::min<int64_t>(K, nsteps) * S + 1;
   // the storage of the previous pair is kept when its layout fits (same checkpoint count and
   // segment length); the observable is reset either way
@@ -779,12 +824,23 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
     u->seg_cap = seg_states;
   }
   cudaEventRecord(h->ev_call[0], h->stream);
+  u->fwd_w0 = h->synced ? 0.5 : 1.0;
+  u->fwd_fresh = lf && u->lf_fresh;
+  u->lf_fresh = false;
   for (int64_t c = 0; c < nck; ++c) {
     U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
     if ((e = copy_state(h, ck.f, ck.p, false)) != cudaSuccess) return h->cuda_fail(e, "clb_forward");
     if ((e = cudaMemcpyAsync(&ck.st, u->d_st, sizeof(U1State), cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
       return h->cuda_fail(e, "clb_forward");
-    vv_run(h, std::min<int64_t>(K, nsteps - c * K), nullptr); // the merged schedule of clb_evolve
+    if (lf)
+      lf_run(h, std::min<int64_t>(K, nsteps - c * K), nullptr); // the launches of clb_evolve
+    else
+      vv_run(h, std::min<int64_t>(K, nsteps - c * K), nullptr, false); // the merged schedule of clb_evolve
+  }
+  if (lf) { // LeapFrog::sync: the observable is measured at integer-time momenta
+    const bool ex = h->cfg.expansion != 0;
+    kick_sweep(h, 1, false, ex, lf_kick(h->cfg.dt, 0.5));
+    if (ex) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
   }
   cudaEventRecord(h->ev_call[1], h->stream);
   {
@@ -836,11 +892,205 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
 // first kick of the stage starting there, part B: the second kick of the stage ending there).
 // With through_init the start state is taken as produced by clb_initialize(correct_adot = 1),
 // whose aDot = sqrt(Friedmann RHS) (modelinitializer.h:77-78) is differentiated too.
+namespace {
+// pbar += (2 X_phi / N^3) p_phi, (2 X_A / N^3) p_A: the cotangents X of the two momentum averages
+// of the momenta p (storage type of the state), or pbar = that (set).
+void pbar_axpy(clb_handle *h, double *pbar, const void *p, double Xphi, double XA, bool set)
+{
+  U1Sector *u = h->u1;
+  const double c = 2.0 * u->prm.inv_n3;
+  if (u->fp32)
+    k_u1_pbar_axpy<float><<<kU1Blocks, 256, 0, h->stream>>>(pbar, static_cast<const float *>(p), h->n3, c * Xphi,
+                                                             c * XA, set ? 1 : 0);
+  else
+    k_u1_pbar_axpy<double><<<kU1Blocks, 256, 0, h->stream>>>(pbar, static_cast<const double *>(p), h->n3, c * Xphi,
+                                                              c * XA, set ? 1 : 0);
+}
+
+// The backward pass of the leapfrog (LeapFrog::evolve, leapfrog.h:42-89, then sync, :96-116).
+// Boundary n is the state before step n's kick: fields f_n, momenta p_{n-1/2}; boundary N the
+// state before the sync.  One adjoint sweep per boundary: part A is the kick at f_n (w dt; dt/2
+// for the sync, 1/2 of dt for a first step right after a sync), part B the drift of step n - 1
+// (no kick: hB = 0).  The scale-factor chain of step n - 1 (a-drift, aDot kick with
+// F(a_{n-1}; <.>)) is reversed on the host after boundary n's sweep; its <pi^2> inputs are the
+// means of the averages of p_{n-3/2} and p_{n-1/2} (leapfrog.h:152-167), so the cotangent of
+// boundary n's momentum average is complete only then, and is added to the sweep's output by
+// pbar_axpy.  The sweep's dot products do not depend on it (hB = 0).
+int u1_backward_lf(clb_handle *h, int32_t through_init, double *fields_bar, double *momenta_bar,
+                   clb_adjoint_grad *out)
+{
+  U1Sector *u = h->u1;
+  const U1Params &prm = u->prm;
+  const bool ex = h->cfg.expansion != 0;
+  const double dt = h->cfg.dt, al = prm.alpha, el = prm.el0, inv = prm.inv_n3;
+  const size_t bytes = 5 * h->n3 * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  double thg = 0, thc = 0, Sd[kAdjSlots];
+  int cur = 0, r = CLB_OK;
+  // seed at the synced end state: O = sum_k w_k E_k / E_tot, or a spectrum observable
+  double E[kAvgN], Et = 0, Ew = 0, Aend[kAvgN] = {0, 0, 0, 0, 0}, abar = 0;
+  {
+    const double a = u->fwd_a;
+    energies_of(prm, a, u->fwd_avg, E);
+    for (int k = 0; k < kAvgN; ++k) {
+      Et += E[k];
+      Ew += u->fwd_w[k] * E[k];
+    }
+    double Ebar[kAvgN];
+    for (int k = 0; k < kAvgN; ++k) Ebar[k] = u->seed_which >= 0 ? 0.0 : (u->fwd_w[k] - Ew / Et) / Et;
+    Aend[0] = Ebar[0] * std::pow(a, -6);
+    Aend[1] = Ebar[1] * std::pow(a, -2);
+    Aend[2] = Ebar[2] * el * std::pow(a, -4);
+    Aend[3] = Ebar[3] * el * std::pow(a, -4);
+    Aend[4] = Ebar[4];
+    abar = ex ? Ebar[0] * u->fwd_avg[0] * -6 * std::pow(a, -7) + Ebar[1] * u->fwd_avg[1] * -2 * std::pow(a, -3) +
+                    (Ebar[2] * u->fwd_avg[2] + Ebar[3] * u->fwd_avg[3]) * el * -4 * std::pow(a, -5)
+              : 0.0;
+    if (u->seed_which >= 0) abar = ex ? u->seed_abar : 0.0;
+  }
+  // cotangents of the synced end state: fields (qbar), momenta p_N (the sync kick's lambda_A)
+  const U1Sector::Ckpt &end = u->ckpt.back();
+  if ((e = cudaMemsetAsync(u->qbar, 0, bytes, h->stream)) != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+  pbar_axpy(h, u->pbar[cur], end.p, Aend[0], Aend[2], true);
+  if (u->seed_which >= 0) {
+    double *dst = (u->seed_which == 0 ? u->qbar : u->pbar[cur]) + (size_t)u->seed_comp * h->n3;
+    if ((e = cudaMemcpyAsync(dst, u->seed, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+  }
+  double fieldA[3] = {Aend[1], Aend[3], Aend[4]}; // <|D phi|^2>, <B^2>, <V> cotangents at the next boundary's fields
+  double adbar = 0;                               // cotangent of aDot_{n-1/2} (the sync's aDot enters no energy)
+  double piHalf[2] = {0, 0};                      // part of the cotangent of <pi^2>(p_{n-1/2}) from step n's F
+  const int64_t N = u->fwd_steps, K = u->fwd_K;
+  const int64_t nck = (int64_t)u->ckpt.size() - 1;
+  const size_t half = 5 * h->n3 * u->esz;
+  SegSave sv{u->seg, half, u->d_rec};
+  auto segf = [&](int64_t b) -> void * { return u->seg + (size_t)b * 2 * half; };
+  auto segp = [&](int64_t b) -> void * { return u->seg + (size_t)b * 2 * half + half; };
+  std::vector<U1State> rec((size_t)u->seg_cap);
+  for (int64_t c = nck - 1; c >= 0; --c) {
+    const int64_t s0 = c * K, s1 = std::min(N, s0 + K), nb = s1 - s0;
+    U1Sector::Ckpt &ck = u->ckpt[(size_t)c];
+    if ((e = copy_state(h, ck.f, ck.p, true)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(u->d_st, &ck.st, sizeof(U1State), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+    h->synced = c == 0 && u->fwd_w0 == 0.5;
+    lf_run(h, nb, &sv);
+    e = cudaMemcpyAsync(rec.data(), u->d_rec, (size_t)(nb + 1) * sizeof(U1State), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+    // a_n at boundary b: before step b's a-drift; the segment's end from its last step
+    auto a_at = [&](int64_t b) { return ex ? (b < nb ? rec[(size_t)b].aIM : rec[(size_t)nb - 1].aI) : rec[0].aI; };
+    for (int64_t b = nb; b >= (c == 0 ? 0 : 1); --b) {
+      const int64_t n = s0 + b;
+      const double an = a_at(b);
+      U1AdjArgs g = adj_base(prm, an);
+      const double wA = n == N ? 0.5 : (n == 0 ? u->fwd_w0 : 1.0);
+      g.hA[0] = g.hA[1] = wA * dt;
+      double aS = 0;
+      if (b >= 1) {
+        aS = rec[(size_t)b - 1].aSI;
+        g.cdf = dt * std::pow(aS, al - 3);
+        g.cda = dt * std::pow(aS, al - 1);
+      }
+      double piPrev[2] = {piHalf[0], piHalf[1]}; // cotangent of <pi^2>(p_{n-1/2}) so far
+      if (n == 0 && ex && u->fwd_fresh) {
+        // clb_initialize's aDot_{-1/2} = aDot_0 - dt/2 F(a_0, <.>_0) (leapfrog.h:35) and, through_init,
+        // aDot_0 = sqrt(RHS(a_0, <.>_0)) (modelinitializer.h:77-80); <pi^2>_0 of the start momenta,
+        // the field averages of f_0
+        const U1State &R0 = ck.st;
+        double A0[kAvgN], Ain[kAvgN] = {0, 0, 0, 0, 0};
+        averages_of(R0, A0);
+        const double a0 = an, ad0bar = adbar;
+        const SFGrad gc = sf_grad(prm, a0, A0);
+        const double Fc = -dt / 2.0 * ad0bar;
+        abar += Fc * gc.da;
+        for (int k = 0; k < kAvgN; ++k) Ain[k] += Fc * gc.dA[k];
+        if (through_init && u->init_corrected) {
+          const double C = std::pow(a0, 2 * al + 2) / 3.0 * prm.fm2, dC = (2 * al + 2) * std::pow(a0, 2 * al + 1) / 3.0 * prm.fm2;
+          const double rho = A0[0] * std::pow(a0, -6) + A0[1] * std::pow(a0, -2) + el * std::pow(a0, -4) * (A0[2] + A0[3]) + A0[4];
+          const double drho = A0[0] * -6 * std::pow(a0, -7) + A0[1] * -2 * std::pow(a0, -3) + el * -4 * std::pow(a0, -5) * (A0[2] + A0[3]);
+          const double RHSbar = ad0bar / (2 * R0.aDotI);
+          abar += RHSbar * (dC * rho + C * drho);
+          Ain[0] += RHSbar * C * std::pow(a0, -6);
+          Ain[1] += RHSbar * C * std::pow(a0, -2);
+          Ain[2] += RHSbar * C * el * std::pow(a0, -4);
+          Ain[3] += RHSbar * C * el * std::pow(a0, -4);
+          Ain[4] += RHSbar * C;
+        }
+        fieldA[0] += Ain[1];
+        fieldA[1] += Ain[3];
+        fieldA[2] += Ain[4];
+        piPrev[0] += Ain[0];
+        piPrev[1] += Ain[2];
+        adbar = through_init && u->init_corrected ? 0.0 : ad0bar; // then the cotangent of aDotI at the start
+      }
+      g.AD = fieldA[0];
+      g.AB = fieldA[1];
+      g.AV = fieldA[2];
+      if ((r = adj_sweep(h, segf(b), segp(b), u->pbar[cur], u->pbar[cur ^ 1], g, Sd)) != CLB_OK) return r;
+      cur ^= 1;
+      thg += Sd[2] + g.AD * inv * Sd[4];
+      thc += Sd[3] + g.AV * inv * Sd[5];
+      if (ex) abar += Sd[0]; // a_n in the kick coefficients
+      for (double &x : fieldA) x = 0;
+      piHalf[0] = piHalf[1] = 0;
+      if (b >= 1 && ex) {
+        // step n - 1 backwards: f_n = f_{n-1} + dt D(aS) p (the sweep's dots 6, 7), a_n = a_{n-1} +
+        // dt aDot_{n-1/2}, aS = (a_{n-1} + a_n)/2, aDot_{n-1/2} = aDot_{n-3/2} + dt F(a_{n-1}; <.>)
+        const double aSbar = dt * ((al - 3) * std::pow(aS, al - 4) * Sd[6] + (al - 1) * std::pow(aS, al - 2) * Sd[7]);
+        const double abar_n = abar + aSbar / 2;
+        adbar += dt * abar_n;
+        abar = abar_n + aSbar / 2;
+        const U1State &R = rec[(size_t)b - 1];
+        double A[kAvgN];
+        averages_of(R, A); // <pi^2> the mean over p_{n-3/2}, p_{n-1/2}; the fields' of f_{n-1}
+        const SFGrad g1 = sf_grad(prm, R.aIM, A);
+        const double Fbar = dt * adbar;
+        abar += Fbar * g1.da;
+        piPrev[0] += 0.5 * Fbar * g1.dA[0];
+        piPrev[1] += 0.5 * Fbar * g1.dA[2];
+        piHalf[0] = 0.5 * Fbar * g1.dA[0];
+        piHalf[1] = 0.5 * Fbar * g1.dA[2];
+        fieldA[0] = Fbar * g1.dA[1];
+        fieldA[1] = Fbar * g1.dA[3];
+        fieldA[2] = Fbar * g1.dA[4];
+      }
+      // the momentum average of this boundary's momenta p_{n-1/2} (step n's <pi^2> of the previous
+      // half step, and step n - 1's own; at n = 0 the start momenta's only right after
+      // clb_initialize, where the stored average is theirs)
+      if (ex && (b >= 1 || u->fwd_fresh)) pbar_axpy(h, u->pbar[cur], segp(b), piPrev[0], piPrev[1], false);
+    }
+  }
+  {
+    const U1Sector::Ckpt &fin = u->ckpt.back();
+    if ((e = copy_state(h, fin.f, fin.p, true)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(u->d_st, &fin.st, sizeof(U1State), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "clb_backward");
+  }
+  h->synced = true;
+  if (fields_bar) e = cudaMemcpyAsync(fields_bar, u->qbar, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && momenta_bar) e = cudaMemcpyAsync(momenta_bar, u->pbar[cur], bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "clb_backward");
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->dO_dcouplings[0] = thc;
+    out->dO_dcouplings[1] = thg;
+    out->dO_dscalefactor[0] = ex ? abar : 0.0;
+    // aDotI at the start (after clb_initialize; a later start: the half-step aDot before it)
+    out->dO_dscalefactor[1] = ex ? adbar : 0.0;
+    out->observable = u->fwd_obs;
+  }
+  return check(h, "clb_backward");
+}
+} // namespace
+
 __attribute__((visibility("hidden"))) int u1_backward(clb_handle *h, int32_t through_init, double *fields_bar,
                                                       double *momenta_bar, clb_adjoint_grad *out)
 {
   U1Sector *u = h->u1;
   if (u->fwd_steps < 0) return h->fail(CLB_ESTATE, "clb_backward: call clb_forward first");
+  if (h->cfg.evolver == CLB_LF) return u1_backward_lf(h, through_init, fields_bar, momenta_bar, out);
   const U1Params &prm = u->prm;
   const bool ex = h->cfg.expansion != 0;
   const double dt = h->cfg.dt, al = prm.alpha, el = prm.el0;

@@ -257,8 +257,10 @@ void *clb_cuda_stream(clb_handle *h);
  * a caller's finite-difference loop around Evolver::evolve (evolvers/evolver.h:102-127) and
  * EnergiesMeasurer::measure (measurements/energiesmeasurer.h:45-122).
  *
- * clb_forward runs nsteps VV steps from the current (initialized) state, storing the full state
- * every checkpoint_every steps, and returns the observable
+ * clb_forward runs nsteps VV or leapfrog steps from the current (initialized) state, storing the
+ * full state every checkpoint_every steps (the leapfrog then syncs, LeapFrog::sync
+ * evolvers/leapfrog.h:96-116, so that O is taken at integer-time momenta), and returns the
+ * observable
  *     O = sum_k w_k E_k / E_tot
  * over the energy components E_k in clb_measurement order without E_tot (lphi4U1: E_kin and
  * E_grad of the complex scalar, E_el, E_mag, V; n_weights <= 5).  clb_backward then returns dO
@@ -267,9 +269,13 @@ void *clb_cuda_stream(clb_handle *h);
  * their explicit appearance in the evolution.  With through_init = 1 the start state is taken as
  * made by clb_initialize(h, 1), whose aDot = sqrt(Friedmann RHS) is differentiated as well (the
  * aDot cotangent is then 0).  The backward pass recomputes each segment from its checkpoint;
- * device memory: (nsteps/checkpoint_every + 1) states plus checkpoint_every x stages + 1 states.
- * lphi4U1 with the VV evolvers; other models and the leapfrog return CLB_EUNSUPPORTED.  After
- * clb_backward the handle holds the forward's end state again. */
+ * device memory: (nsteps/checkpoint_every + 1) states plus checkpoint_every x stages + 1 states
+ * (stages: 1 for the leapfrog).  lphi4U1 with the VV evolvers and the leapfrog; the position
+ * Verlet, a fixed background and other models return CLB_EUNSUPPORTED.  A leapfrog forward that
+ * starts right after clb_initialize differentiates its first step's <pi^2> of the previous half
+ * step (the start momenta's) and the initial aDot_{-1/2} = aDot_0 - dt/2 F (leapfrog.h:35);
+ * started later, that stored average is a constant and dO_dscalefactor[1] is the cotangent of the
+ * stored half-step aDot.  After clb_backward the handle holds the forward's end state again. */
 typedef struct clb_adjoint_grad {
   double observable;         /* O of the forward pass                                       */
   double dO_dcouplings[8];   /* clb_model_desc.couplings order (lphi4U1: [0] c4, [1] gQ)     */

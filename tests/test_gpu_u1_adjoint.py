@@ -49,7 +49,8 @@ def fd(param, N, evolver, expansion, dt, n, oracle=False):
     return (up - dn) / (2 * h)
 
 
-@pytest.mark.parametrize("evolver,expansion,K", [("VV2", True, 7), ("VV4", True, 5), ("VV2", False, 40)])
+@pytest.mark.parametrize("evolver,expansion,K", [("VV2", True, 7), ("VV4", True, 5), ("VV2", False, 40),
+                                                 ("LF", True, 7), ("LF", True, 30), ("LF", False, 40)])
 def test_gradients_match_gpu_finite_differences(evolver, expansion, K):
     from cosmolattice_b200.adjoint import u1_gradients
 
@@ -73,15 +74,15 @@ def test_gradients_match_oracle_finite_differences():
         assert abs(grads[prm] - ref) <= REL * abs(ref), (prm, grads[prm], ref)
 
 
-@pytest.mark.parametrize("expansion", [True, False])
-def test_state_cotangent_directional_derivative(expansion):
+@pytest.mark.parametrize("evolver,expansion", [("VV2", True), ("VV2", False), ("LF", True), ("LF", False)])
+def test_state_cotangent_directional_derivative(evolver, expansion):
     # <fields_bar, v_f> + <momenta_bar, v_p> + aI_bar da + aDot_bar dadot equals the derivative of
     # O along a random start-state direction (no initial aDot correction: through_init = 0)
     from cosmolattice_b200 import Lattice
     from cosmolattice_b200.adjoint import GAUGE_FRACTION, observable_from_measurement
 
     N, dt, n = 10, 0.01, 25
-    par, rp, m, f, p, sf = case(N, "VV2", expansion, dt)
+    par, rp, m, f, p, sf = case(N, evolver, expansion, dt)
     rng = np.random.default_rng(5)
     f = f.copy()
     f[2:] = rng.normal(0, 0.05, f[2:].shape)
@@ -101,6 +102,7 @@ def test_state_cotangent_directional_derivative(expansion):
             out = (O,) + lat.backward(through_init=False)
         else:
             lat.evolve(n)
+            lat.sync()  # the leapfrog's momenta to integer time, as clb_forward ends
             out = observable_from_measurement(lat.measure(1.0))
         lat.close()
         return out
@@ -135,7 +137,7 @@ def test_forward_matches_evolve_bitwise_and_restores_state():
 def test_adjoint_rejects_unsupported():
     from cosmolattice_b200 import Lattice, _capi
 
-    par, rp, m, f, p, sf = case(8, "LF", True, 0.01)
+    par, rp, m, f, p, sf = case(8, "PV2", True, 0.01)
     lat = Lattice(m, rp)
     lat.set_state(f, p, sf)
     lat.initialize()
@@ -180,6 +182,8 @@ SPEC_CASES = [
     ("VV2", 0, 0, {"ps_type": 1, "ps_version": 1, "dk": 1.0, "fold": True, "nbins": 10}),
     ("VV4", 1, 3, {"ps_type": 2, "ps_version": 2, "dk": 1.0, "fold": True, "nbins": 10}),
     ("VV2", 1, 1, {"ps_type": 1, "ps_version": 2, "dk": 1.5, "fold": False, "nbins": 4}),
+    ("LF", 1, 0, {"ps_type": 1, "ps_version": 1, "dk": 1.0, "fold": True, "nbins": 10}),
+    ("LF", 0, 2, {"ps_type": 2, "ps_version": 2, "dk": 1.0, "fold": True, "nbins": 10}),
 ]
 
 
