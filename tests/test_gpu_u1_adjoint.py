@@ -155,7 +155,8 @@ def test_adjoint_rejects_unsupported():
     lat.close()
 
 
-def test_fp32_form_gradients_track_fp64():
+@pytest.mark.parametrize("evolver", ["VV4", "LF"])
+def test_fp32_form_gradients_track_fp64(evolver):
     # FP32 storage forward (FP64 increments and sums), FP64 cotangents: the observable and its
     # gradients follow the FP64 pair to the FP32 trajectory error (bounds: 1e-5 on O, 1e-3 on
     # each gradient relative to the largest one).
@@ -163,7 +164,7 @@ def test_fp32_form_gradients_track_fp64():
     from cosmolattice_b200.adjoint import u1_gradients
 
     N, dt, n, K = 12, 0.01, 30, 5
-    par, rp, m, f, p, sf = case(N, "VV4", True, dt)
+    par, rp, m, f, p, sf = case(N, evolver, True, dt)
     O64, g64, _ = u1_gradients(m, rp, n, K)
     lat = Lattice(m, rp, precision="fp32")
     O32, g32, _ = u1_gradients(m, rp, n, K, lattice=lat)
