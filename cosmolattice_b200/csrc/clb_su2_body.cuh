@@ -135,6 +135,11 @@ template <class S, class T> struct Site {
     return 2 * qH * ipw(nD * normC(s), 2);
   }
   __device__ __forceinline__ T pot() const { return (potTerm(0) + potTerm(1)) + potTerm(2); }
+  // pot() from |Phi|, |phi| and S at this site, formed as potTerm forms them
+  __device__ __forceinline__ T pot_at(T nD, T nC, T Sv) const
+  {
+    return (c4 * ipw(nD, 4) + qG * ipw(nD * Sv, 2)) + 2 * qH * ipw(nD * nC, 2);
+  }
   __device__ __forceinline__ size_t pl(int i) const { return s + op[i]; }
   __device__ __forceinline__ size_t mi(int i) const { return s + om[i]; }
   __device__ __forceinline__ size_t plmi(int i, int j) const { return i == j ? s : s + op[i] + om[j]; }
@@ -209,11 +214,31 @@ __device__ __forceinline__ Site<S, Tan<S>> make_site_tan(const S *f, const S *df
 }
 
 // ---- momentum kernels at one site (momentum-component order) ----------------------------------
-template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<S, T> &v)
+// Direction d's term of the gradient energies cGrad2 and dGrad2 below, from the forward product w
+// (the phi or Phi value at x + d parallel transported to x) and the value c at x.
+template <class S, class T> __device__ __forceinline__ T cgrad_term(const Site<S, T> &v, const C2<T> &w, const C2<T> &c)
+{
+  const C2<T> d0 = csub(w, c);
+  const C2<T> d{kdiv(d0.re, v.dx), kdiv(d0.im, v.dx)};
+  return d.re * d.re + d.im * d.im;
+}
+template <class S, class T> __device__ __forceinline__ T dgrad_term(const Site<S, T> &v, const D2<T> &w, const D2<T> &c)
+{
+  const C2<T> du0 = csub(w.u, c.u), dv0 = csub(w.v, c.v);
+  const C2<T> du{kdiv(du0.re, v.dx), kdiv(du0.im, v.dx)}, dv{kdiv(dv0.re, v.dx), kdiv(dv0.im, v.dx)};
+  return (du.re * du.re + du.im * du.im) + (dv.re * dv.re + dv.im * dv.im);
+}
+
+// g2: also form cGrad2 (covLapC) or dGrad2 (covLapD) from the same forward products.
+template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<S, T> &v, T *g2 = nullptr)
 {
   C2<T> plus{0, 0}, minus{0, 0};
   for (int d = 0; d < 3; ++d) {
     const C2<T> w = cmul(v.phaseC(d, v.s), v.cs(v.pl(d)));
+    if (g2) {
+      const T n2 = cgrad_term(v, w, v.cs(v.s));
+      *g2 = d == 0 ? n2 : *g2 + n2;
+    }
     const C2<T> m = cmul(conj_(v.phaseC(d, v.mi(d))), v.cs(v.mi(d)));
     plus = d == 0 ? w : cadd(plus, w);
     minus = d == 0 ? m : cadd(minus, m);
@@ -223,11 +248,15 @@ template <class S, class T> __device__ __forceinline__ C2<T> covLapC(const Site<
   return C2<T>{kdiv((plus.re + minus.re) - 6 * c.re, dx2), kdiv((plus.im + minus.im) - 6 * c.im, dx2)};
 }
 
-template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S, T> &v, T out[4])
+template <class S, class T> __device__ __forceinline__ void covLapD(const Site<S, T> &v, T out[4], T *g2 = nullptr)
 {
   D2<T> plus{}, minus{};
   for (int d = 0; d < 3; ++d) {
     const D2<T> w = qapply(v.link(d, v.s), dscale(v.phaseD(d, v.s), v.dbl(v.pl(d))));
+    if (g2) {
+      const T n2 = dgrad_term(v, w, v.dbl(v.s));
+      *g2 = d == 0 ? n2 : *g2 + n2;
+    }
     const size_t sm = v.mi(d);
     const D2<T> m = qapply(qdag(v.link(d, sm)), dscale(conj_(v.phaseD(d, sm)), v.dbl(sm)));
     if (d == 0) {
@@ -258,8 +287,20 @@ __host__ __device__ constexpr bool sect_scalars(int sect) { return sect == 0 || 
 __host__ __device__ constexpr bool sect_u1(int sect) { return sect == 0 || sect == 1 || sect == 4; }
 __host__ __device__ constexpr bool sect_su2(int sect) { return sect == 0 || sect == 2; }
 
-template <int SECT = 0, class S, class T>
-__device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP])
+// Per-site terms of the volume averages a kick sweep reduces with RF (fieldfunctionals.h):
+// gradient energies of S, phi and Phi, B^2 of A and of SU(2), and V.  They equal, to the last
+// bit, what sGrad2, cGrad2, dGrad2, aB2, gB2 and Site::pot give at the site.
+template <class T> struct SiteAvg {
+  T g2S, g2C, g2D, b2A, b2G, pot;
+};
+template <class S, class T> __device__ __forceinline__ T sGrad2(const Site<S, T> &v);
+template <class S, class T> __device__ __forceinline__ T aB2(const Site<S, T> &v, const T (*g)[3] = nullptr);
+template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v, const T *pw = nullptr);
+
+// AVG: also form the SiteAvg terms of the sectors in SECT into *av, from the covariant products,
+// differences and plaquettes the kernels form anyway.
+template <int SECT = 0, bool AVG = false, class S, class T>
+__device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T K[NP], SiteAvg<T> *av = nullptr)
 {
   const Params &a = *v.a;
   const size_t s = v.s;
@@ -268,23 +309,29 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
   if constexpr (sect_scalars(SECT)) {
     const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
     K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
-    const C2<T> cl = covLapC(v);
+    const C2<T> cl = covLapC(v, AVG ? &av->g2C : nullptr);
     const T ndC = 4 * qH * ipw(nD, 2) * nC;
     K[1] = A * cl.re - B2 * (kdiv(ndC, nC) * v.F(1, s));
     K[2] = A * cl.im - B2 * (kdiv(ndC, nC) * v.F(2, s));
     T dl[4];
-    covLapD(v, dl);
+    covLapD(v, dl, AVG ? &av->g2D : nullptr);
     const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
     for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (kdiv(ndD, nD) * v.F(3 + c, s));
+    if constexpr (AVG) {
+      av->g2S = sGrad2(v);
+      av->pot = v.pot_at(nD, nC, Sv);
+    }
   }
   if constexpr (sect_u1(SECT)) {
     const D2<T> D0 = v.dbl(s);
     const C2<T> C0 = v.cs(s);
+    T g0s[3][3]; // g0s[i][j]: forward difference of A_j along i
     for (int i = 0; i < 3; ++i) {
       const T lap = v.lapl(7 + i);
       T grad = 0;
       for (int j = 0; j < 3; ++j) {
         const T g0 = v.fd(7 + j, s, v.pl(i));
+        g0s[i][j] = g0;
         const T g1 = v.fd(7 + j, v.mi(j), v.plmi(i, j));
         const T t = kdiv(g0 - g1, v.dx);
         grad = j == 0 ? t : grad + t;
@@ -294,17 +341,20 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
       const T J = kdiv(T(2.0), v.dx) * rfo2 * (Jc + Jd);
       K[7 + i] = G * (lap - grad) - A * J;
     }
+    if constexpr (AVG) av->b2A = aB2(v, g0s);
   }
   if constexpr (sect_su2(SECT)) {
     const D2<T> Dg = v.dbl(s);
     const T normGrad = kdiv(ipw(kdiv(T(1), v.dx), 3), v.gS) * G;
     const T normSrc = kdiv(T(1), v.dx) * A;
+    T pw[3]; // plaq(1, 0).w, plaq(2, 0).w, plaq(2, 1).w
     for (int i = 0; i < 3; ++i) {
       T gr[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
       bool first = true;
       for (int j = 0; j < 3; ++j) {
         if (j == i) continue;
         const Q4<T> P = v.plaq(i, j), Pb = v.plaqBack(i, j);
+        if (j < i) pw[i + j - 1] = P.w;
         const T pv[3] = {P.x, P.y, P.z}, bv[3] = {Pb.x, Pb.y, Pb.z};
         for (int c = 0; c < 3; ++c) {
           gr[c] = first ? pv[c] : gr[c] + pv[c];
@@ -318,6 +368,7 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
         K[10 + 3 * i + c] = -normGrad * (gr[c] - gb[c]) - normSrc * J;
       }
     }
+    if constexpr (AVG) av->b2G = gB2(v, pw);
   }
 }
 
@@ -336,9 +387,7 @@ template <class S, class T> __device__ __forceinline__ T cGrad2(const Site<S, T>
   const C2<T> c = v.cs(v.s);
   T acc = 0;
   for (int j = 0; j < 3; ++j) {
-    const C2<T> d0 = csub(v.wC(j), c);
-    const C2<T> d{kdiv(d0.re, v.dx), kdiv(d0.im, v.dx)};
-    const T n2 = d.re * d.re + d.im * d.im;
+    const T n2 = cgrad_term(v, v.wC(j), c);
     acc = j == 0 ? n2 : acc + n2;
   }
   return acc;
@@ -348,29 +397,44 @@ template <class S, class T> __device__ __forceinline__ T dGrad2(const Site<S, T>
   const D2<T> c = v.dbl(v.s);
   T acc = 0;
   for (int j = 0; j < 3; ++j) {
-    const D2<T> w = qapply(v.link(j, v.s), dscale(v.phaseD(j, v.s), v.dbl(v.pl(j))));
-    const C2<T> du0 = csub(w.u, c.u), dv0 = csub(w.v, c.v);
-    const C2<T> du{kdiv(du0.re, v.dx), kdiv(du0.im, v.dx)}, dv{kdiv(dv0.re, v.dx), kdiv(dv0.im, v.dx)};
-    const T n2 = (du.re * du.re + du.im * du.im) + (dv.re * dv.re + dv.im * dv.im);
+    const T n2 = dgrad_term(v, qapply(v.link(j, v.s), dscale(v.phaseD(j, v.s), v.dbl(v.pl(j)))), c);
     acc = j == 0 ? n2 : acc + n2;
   }
   return acc;
 }
+// aB2's g and gB2's pw: the differences and plaquettes as kernels() formed them
 template <class S, class T> __device__ __forceinline__ T Fij(const Site<S, T> &v, int i, int j)
 {
   return v.fd(7 + j, v.s, v.pl(i)) - v.fd(7 + i, v.s, v.pl(j));
 }
-template <class S, class T> __device__ __forceinline__ T aB2(const Site<S, T> &v)
+template <class S, class T> __device__ __forceinline__ T aB2(const Site<S, T> &v, const T (*g)[3])
 {
-  const T f21 = Fij(v, 1, 0), f31 = Fij(v, 2, 0), f32 = Fij(v, 2, 1);
+  auto F = [&](int i, int j) { return g ? g[i][j] - g[j][i] : Fij(v, i, j); };
+  const T f21 = F(1, 0), f31 = F(2, 0), f32 = F(2, 1);
   return f21 * f21 + (f31 * f31 + f32 * f32);
 }
-template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v)
+template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v, const T *pw)
 {
   const T c = kdiv(T(4.0), ipw(v.dx, 4) * ipw(v.gS, 2));
-  const T t10 = 2 - 2 * v.plaq(1, 0).w, t20 = 2 - 2 * v.plaq(2, 0).w, t21 = 2 - 2 * v.plaq(2, 1).w;
+  const T t10 = 2 - 2 * (pw ? pw[0] : v.plaq(1, 0).w), t20 = 2 - 2 * (pw ? pw[1] : v.plaq(2, 0).w),
+          t21 = 2 - 2 * (pw ? pw[2] : v.plaq(2, 1).w);
   return c * (t10 + (t20 + t21));
 }
+// The SiteAvg terms of the sectors in SECT, formed on their own (a sweep that does not kick).
+template <int SECT, class S, class T> __device__ __forceinline__ SiteAvg<T> site_avg(const Site<S, T> &v)
+{
+  SiteAvg<T> av{};
+  if constexpr (sect_scalars(SECT)) {
+    av.g2S = sGrad2(v);
+    av.g2C = cGrad2(v);
+    av.g2D = dGrad2(v);
+    av.pot = v.pot();
+  }
+  if constexpr (sect_u1(SECT)) av.b2A = aB2(v);
+  if constexpr (sect_su2(SECT)) av.b2G = gB2(v);
+  return av;
+}
+
 // First momentum component of sector g (0 S, 1 phi, 2 Phi, 3 A, 4 SU(2)); g = 5: one past the last.
 __host__ __device__ constexpr int sector_c0(int g) { return g == 0 ? 0 : g == 1 ? 1 : g == 2 ? 3 : g == 3 ? 7 : g == 4 ? 10 : NP; }
 
@@ -455,9 +519,10 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
     v.ph = ph;
     S q[NP];
     for (int c = C0; c < C1; ++c) q[c] = p[(size_t)c * a.n3 + s];
+    SiteAvg<S> av; // with RF: formed by kernels() when the sweep kicks, else by site_avg()
     if (NK > 0) {
       S K[NP];
-      kernels<SECT>(v, Coef<S>{(S)st.kA, (S)st.kB, (S)st.kB2, (S)st.kG}, K);
+      kernels<SECT, RF>(v, Coef<S>{(S)st.kA, (S)st.kB, (S)st.kB2, (S)st.kG}, K, &av);
       for (int k = 0; k < NK; ++k) {
         for (int c = C0; c < C1; ++c) q[c] = (S)((double)q[c] + kc.h[k][sector(c)] * (double)K[c]);
         if (RP) {
@@ -472,15 +537,16 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
       pi2s<G0, G1>(q, t);
       for (int g = G0; g < G1; ++g) acc[g] += t[g];
     }
+    if (RF && NK == 0) av = site_avg<SECT>(v);
     if (RF) {
       if (sect_scalars(SECT)) {
-        acc[5] += (double)sGrad2(v);
-        acc[6] += (double)cGrad2(v);
-        acc[7] += (double)dGrad2(v);
+        acc[5] += (double)av.g2S;
+        acc[6] += (double)av.g2C;
+        acc[7] += (double)av.g2D;
       }
-      if (sect_u1(SECT)) acc[8] += (double)aB2(v);
-      if (sect_su2(SECT)) acc[9] += (double)gB2(v);
-      if (sect_scalars(SECT)) acc[10] += (double)v.pot();
+      if (sect_u1(SECT)) acc[8] += (double)av.b2A;
+      if (sect_su2(SECT)) acc[9] += (double)av.b2G;
+      if (sect_scalars(SECT)) acc[10] += (double)av.pot;
     }
   });
   if (RF || RP) {
@@ -731,9 +797,10 @@ __global__ void __launch_bounds__(128)
         acc[kRed + base + g] += td[g];
       }
     };
+    SiteAvg<T> av;
     if (NK > 0) {
       T K[NP];
-      kernels<SECT>(v, C, K);
+      kernels<SECT, RF>(v, C, K, &av);
       for (int k = 0; k < NK; ++k) {
         for (int c = C0; c < C1; ++c) {
           const double h = kc.h[k][sector(c)];
@@ -749,19 +816,20 @@ __global__ void __launch_bounds__(128)
     } else if (RP) {
       add_pi(0);
     }
+    if (RF && NK == 0) av = site_avg<SECT>(v);
     if (RF) {
       auto addf = [&](int k, T r) {
         acc[5 + k] += (double)r.v;
         acc[kRed + 5 + k] += (double)r.d;
       };
       if (sect_scalars(SECT)) {
-        addf(0, sGrad2(v));
-        addf(1, cGrad2(v));
-        addf(2, dGrad2(v));
+        addf(0, av.g2S);
+        addf(1, av.g2C);
+        addf(2, av.g2D);
       }
-      if (sect_u1(SECT)) addf(3, aB2(v));
-      if (sect_su2(SECT)) addf(4, gB2(v));
-      if (sect_scalars(SECT)) addf(5, v.pot());
+      if (sect_u1(SECT)) addf(3, av.b2A);
+      if (sect_su2(SECT)) addf(4, av.b2G);
+      if (sect_scalars(SECT)) addf(5, av.pot);
     }
   });
   if (RF || RP) {
