@@ -1,19 +1,23 @@
-// clb_gws.cu - gravitational waves sourced by the scalar singlets.
+// clb_gws.cu - the gravitational-wave sector: its C ABI, the scalar singlets' source, and the
+// energy spectrum.  The kick and drift kernels are in clb_gws.cuh; the gauge models' sources are in
+// clb_u1.cu (lphi4U1) and clb_su2.cu (lphi4SU2U1).
 //
 // The GW field is the traceless symmetric u_ij stored as five components (u_11, u_12, u_13, u_22,
 // u_23; u_33 = -u_11 - u_22, the storage gwsprojector.h reads), zero at the start
 // (GWsInitializer, gwsinitializer.h).  With the reference's default (doLFforGWs, runparameters.h:121)
 // it advances as a leapfrog staggered over the matter evolver (Evolver::evolve, evolver.h:102-124):
-//   before each matter step  pi_u += (w dt) K(u, phi; a_I),  w = 1/2 after a sync, else 1
+//   before each matter step  pi_u += (w dt) K(u, source; a_I),  w = 1/2 after a sync, else 1
 //   after it                 u += pow(a_SI, alpha - 3) (dt pi_u)
 // and Evolver::sync (evolver.h:132-138) kicks by dt/2 to integer time before a measurement.  The
 // kernel (GWsKernels::get, gwskernels.h:27-33) is
 //   K = a^(1+alpha) lapl(u) + a^(1+alpha) 2 Pi,
 // with lapl the seven-point Laplacian of each component (gaugederivatives.h:42-46) and Pi the
-// scalar-singlet source sum_a forwDiff_i phi_a forwDiff_j phi_a (PITensor.h), of which the five
-// stored components take the traceless part (Pi_11 - tr/3, Pi_12, Pi_13, Pi_22 - tr/3, Pi_23;
-// TempLat's ConstructSymTraceless is not vendored: a stated choice, and the TT projection of the
-// measurement removes the trace either way).  FP64 pins every rounding in the order above; the
+// anisotropic tensor of PITensor.h: the scalar singlets' sum_a forwDiff_i phi_a forwDiff_j phi_a,
+// the complex scalars' 2 Re[D_i phi conj(D_j phi)] and the U(1) electric and magnetic terms.  The
+// five stored components take its traceless part (Pi_11 - tr/3, Pi_12, Pi_13, Pi_22 - tr/3,
+// Pi_23; TempLat's ConstructSymTraceless is not vendored: a stated choice, and the TT projection
+// of the measurement removes the trace either way).  The SU(2) doublet and the SU(2) gauge field
+// source no GWs in PITensor.h, and none here.  FP64 pins every rounding in the order above; the
 // oracle restates it.
 //
 // The energy spectrum (PowerSpectrumMeasurer::powerSpectrumGW, powerspectrum.h:51-71;
@@ -22,6 +26,7 @@
 // (fStar/MPl)^2 / (4 a^6 rho).  The zero mode, where the lattice momentum vanishes and the
 // projector is undefined, contributes nothing.
 #include "../../include/clb200.h"
+#include "clb_gws.cuh"
 #include "clb_handle.cuh"
 #include "clb_internal.cuh"
 #include "clb_scalar.cuh"
@@ -32,36 +37,19 @@
 #include <string>
 #include <vector>
 
-namespace clb {
-struct GWSector {
-  void *u = nullptr, *pi = nullptr; // 5 x N^3 each, the handle's storage type
-  bool synced = true;                // momenta at integer time (after clb_initialize or a sync)
-  double *d_fk = nullptr;            // five in-place D2Z buffers of the spectrum
-};
-} // namespace clb
-
 namespace {
 
-constexpr int kGWBlocks = 148 * 8;
 constexpr int kGWSpecBlocks = 148 * 2;
 
-// pi_u += h K(u, phi; a_I) at every site (FP64 in the order of the file header).
-template <class R, int NS>
-__global__ void __launch_bounds__(256) k_gw_kick(const R *__restrict__ u, R *__restrict__ piu, const R *__restrict__ fld,
-                                                 Pad pd, double inv_dx2d, double dxd, double hd,
-                                                 const DevState *__restrict__ st)
-{
-  using A = Ar<R>;
-  const int N = pd.N;
-  const size_t n3 = (size_t)N * N * N;
-  const R kA = (R)st->kick_A, h = (R)hd, inv_dx2 = (R)inv_dx2d, dx = (R)dxd, two = R(2), third = R(1.0 / 3.0);
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n3; s += (size_t)gridDim.x * blockDim.x) {
-    const int z = (int)(s % N), y = (int)((s / N) % N), x = (int)(s / ((size_t)N * N));
-    const int xp = x + 1 == N ? 0 : x + 1, xm = x == 0 ? N - 1 : x - 1;
-    const int yp = y + 1 == N ? 0 : y + 1, ym = y == 0 ? N - 1 : y - 1;
-    const int zp = z + 1 == N ? 0 : z + 1, zm = z == 0 ? N - 1 : z - 1;
-    // the source from forward differences of the singlets (padded layout)
-    R P[6];
+// The scalar-singlet source of PITensor.h: Pi_ij = sum_a forwDiff_i phi_a forwDiff_j phi_a, from the
+// padded field layout.
+template <class R, int NS> struct ScalarGWSource {
+  const R *fld;
+  Pad pd;
+  R dx;
+  __device__ __forceinline__ void operator()(size_t, int x, int y, int z, int xp, int yp, int zp, R (&P)[6]) const
+  {
+    using A = Ar<R>;
 #pragma unroll
     for (int f = 0; f < NS; ++f) {
       const R *F = fld + (size_t)f * pd.comp;
@@ -72,32 +60,8 @@ __global__ void __launch_bounds__(256) k_gw_kick(const R *__restrict__ u, R *__r
 #pragma unroll
       for (int k = 0; k < 6; ++k) P[k] = f == 0 ? t[k] : A::add(P[k], t[k]);
     }
-    const R tr3 = A::mul(A::add(A::add(P[0], P[3]), P[5]), third);
-    const R S[5] = {A::sub(P[0], tr3), P[1], P[2], A::sub(P[3], tr3), P[4]};
-    const R kA2 = A::mul(kA, two);
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      const R *U = u + (size_t)c * n3;
-      const R uc = U[s];
-      const R tx = A::sub(A::add(U[((size_t)xp * N + y) * N + z], U[((size_t)xm * N + y) * N + z]), A::mul(two, uc));
-      const R ty = A::sub(A::add(U[((size_t)x * N + yp) * N + z], U[((size_t)x * N + ym) * N + z]), A::mul(two, uc));
-      const R tz = A::sub(A::add(U[((size_t)x * N + y) * N + zp], U[((size_t)x * N + y) * N + zm]), A::mul(two, uc));
-      const R lap = A::mul(inv_dx2, A::add(A::add(tx, ty), tz));
-      const R K = A::add(A::mul(kA, lap), A::mul(kA2, S[c]));
-      piu[(size_t)c * n3 + s] = A::add(piu[(size_t)c * n3 + s], A::mul(h, K));
-    }
   }
-}
-
-// u += pow(a_SI, alpha - 3) (dt pi_u)
-template <class R>
-__global__ void __launch_bounds__(256) k_gw_drift(R *__restrict__ u, const R *__restrict__ piu, size_t n, double dtd,
-                                                  const DevState *__restrict__ st)
-{
-  const R pd = (R)st->drift_p, dt = (R)dtd;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    u[i] = drift_val<R>(u[i], piu[i], pd, dt);
-}
+};
 
 // The TT-projected power of one mode (GWProjectorType1/2/3::eval, gwsprojector.h).
 struct Cx {
@@ -215,16 +179,26 @@ bool gw_ok(const clb_handle *h) { return h->gw != nullptr; }
 
 namespace clb {
 
+// The gauge models' GW kick and drift (clb_u1.cu, clb_su2.cu).
+void u1_gw_kick(clb_handle *h, double w);
+void u1_gw_drift(clb_handle *h);
+void su2_gw_kick(clb_handle *h, double w);
+void su2_gw_drift(clb_handle *h);
+bool su2_tangent_active(const clb_handle *h);
+
 // Runs one GW kick (weight w of dt) at the handle's current fields and a_I.
 __attribute__((visibility("hidden"))) void gw_kick(clb_handle *h, double w)
 {
   GWSector *g = h->gw;
+  g->synced = false;
+  if (h->u1) return u1_gw_kick(h, w);
+  if (h->su2) return su2_gw_kick(h, w);
   const double inv_dx2 = 1.0 / (h->cfg.dx * h->cfg.dx);
   const double hd = w * h->cfg.dt;
 #define CLB_GWK(R, NS)                                                                                                 \
-  CLB_LAUNCH(h, K_GW, k_gw_kick<R, NS><<<kGWBlocks, 256, 0, h->stream>>>(                                            \
-                          static_cast<const R *>(g->u), static_cast<R *>(g->pi), static_cast<const R *>(h->fld[h->cf]), \
-                          h->pd, inv_dx2, h->cfg.dx, hd, h->d_st))
+  CLB_LAUNCH(h, K_GW, (k_gw_kick<R, ScalarGWSource<R, NS>><<<kGWBlocks, 256, 0, h->stream>>>(                        \
+                          static_cast<const R *>(g->u), static_cast<R *>(g->pi), h->N, inv_dx2, hd, &h->d_st->kick_A, \
+                          ScalarGWSource<R, NS>{static_cast<const R *>(h->fld[h->cf]), h->pd, (R)h->cfg.dx})))
   if (h->fp32) {
     if (h->NS == 1) CLB_GWK(float, 1);
     else CLB_GWK(float, 2);
@@ -233,22 +207,23 @@ __attribute__((visibility("hidden"))) void gw_kick(clb_handle *h, double w)
     else CLB_GWK(double, 2);
   }
 #undef CLB_GWK
-  g->synced = false;
 }
 
 // Runs one GW drift with the a_SI of the matter step just taken.
 __attribute__((visibility("hidden"))) void gw_drift(clb_handle *h)
 {
+  if (h->u1) return u1_gw_drift(h);
+  if (h->su2) return su2_gw_drift(h);
   GWSector *g = h->gw;
   const size_t n = 5 * h->n3;
   if (h->fp32)
     CLB_LAUNCH(h, K_GW, k_gw_drift<float><<<kGWBlocks, 256, 0, h->stream>>>(static_cast<float *>(g->u),
                                                                            static_cast<const float *>(g->pi), n,
-                                                                           h->cfg.dt, h->d_st));
+                                                                           h->cfg.dt, &h->d_st->drift_p));
   else
     CLB_LAUNCH(h, K_GW, k_gw_drift<double><<<kGWBlocks, 256, 0, h->stream>>>(static_cast<double *>(g->u),
                                                                              static_cast<const double *>(g->pi), n,
-                                                                             h->cfg.dt, h->d_st));
+                                                                             h->cfg.dt, &h->d_st->drift_p));
 }
 
 // The GW kick before a matter step (evolver.h:104-107): half a step after a sync, else a whole one.
@@ -281,13 +256,16 @@ int clb_gws_enable(clb_handle *h)
 {
   if (!h) return CLB_EINVAL;
   if (h->gw) return CLB_OK;
-  if (h->u1 || h->su2) return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: GWs are sourced by the scalar singlets here");
+  const bool gauge = h->u1 || h->su2;
   if (h->cfg.evolver == CLB_LF || (h->cfg.evolver >= CLB_PV2 && h->cfg.evolver <= CLB_PV6_2) ||
-      h->cfg.path != CLB_PATH_FUSED || h->fb)
+      (!gauge && h->cfg.path != CLB_PATH_FUSED) || h->fb)
     return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: GWs run with the VV evolvers on the fused path, with "
                                      "self-consistent or no expansion");
+  if (h->su2 && su2_tangent_active(h))
+    return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: not with the tangent-linear form running");
   auto *g = new GWSector();
-  const size_t bytes = 5 * h->n3 * h->esz;
+  g->fp32 = gauge ? h->cfg.precision == CLB_PREC_FP32_SPLIT : h->fp32;
+  const size_t bytes = 5 * h->n3 * (g->fp32 ? sizeof(float) : sizeof(double));
   cudaError_t e = cudaMalloc(&g->u, bytes);
   if (e == cudaSuccess) e = cudaMalloc(&g->pi, bytes);
   if (e == cudaSuccess) e = cudaMemset(g->u, 0, bytes);
@@ -313,7 +291,7 @@ int clb_gws_set_state(clb_handle *h, const double *u, const double *pi)
     if (!src) continue;
     e = cudaMemcpyAsync(tmp, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) break;
-    if (h->fp32)
+    if (h->gw->fp32)
       k_gw_copy<double, float><<<kGWBlocks, 256, 0, h->stream>>>(tmp, static_cast<float *>(dst), n);
     else
       e = cudaMemcpyAsync(dst, tmp, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
@@ -335,7 +313,7 @@ int clb_gws_get_state(clb_handle *h, double *u, double *pi)
     double *dst = k == 0 ? u : pi;
     const void *src = k == 0 ? h->gw->u : h->gw->pi;
     if (!dst) continue;
-    if (h->fp32)
+    if (h->gw->fp32)
       k_gw_copy<float, double><<<kGWBlocks, 256, 0, h->stream>>>(static_cast<const float *>(src), tmp, n);
     else
       e = cudaMemcpyAsync(tmp, src, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
@@ -374,7 +352,7 @@ int clb_gw_spectrum(clb_handle *h, int32_t prj_type, int32_t ps_type, int32_t ps
   }
   for (int c = 0; c < 5; ++c) {
     double *dst = h->gw->d_fk + (size_t)c * comp_n;
-    if (h->fp32)
+    if (h->gw->fp32)
       CLB_LAUNCH(h, K_SPECTRUM, k_spec_gather_raw<float><<<kGWBlocks, 256, 0, h->stream>>>(
                                     static_cast<const float *>(h->gw->pi) + (size_t)c * h->n3, dst, N));
     else

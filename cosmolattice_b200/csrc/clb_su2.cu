@@ -6,6 +6,7 @@
 // (leapfrog.h:42-116) with every sector of the model; the second kick of a VV stage and the first
 // of the next share one sweep (no field or a(t) change in between), as in the other sectors.
 
+#include "clb_gws.cuh"
 #include "clb_handle.cuh"
 #include "clb_su2.cuh"
 #include "clb_vv.h"
@@ -51,6 +52,31 @@ struct SU2Sector {
 
 // FP32 form: links re-unitarised every this many steps
 constexpr int64_t kUnitarizeEvery = 10;
+
+namespace {
+// PITensor.h's GW source for lphi4SU2U1: the singlet S (component 0), the complex scalar phi
+// (1, 2) and the U(1) field (7..9, momenta 7..9), in the order scalarSinglet + complexScalar +
+// electricU1 + magneticU1; the doublet and the SU(2) field source none.
+template <class R> struct SU2GWSource {
+  const R *f, *p;
+  size_t n3;
+  int N;
+  R dx, ndxg, rfo2;
+  const double *aI;
+  __device__ __forceinline__ void operator()(size_t s, int x, int y, int z, int xp, int yp, int zp, R (&P)[6]) const
+  {
+    using A = Ar<R>;
+    const size_t nb[3] = {((size_t)xp * N + y) * N + z, ((size_t)x * N + yp) * N + z, ((size_t)x * N + y) * N + zp};
+    const R c = f[s];
+    R g[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] = A::sub(f[nb[i]], c) / dx;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) P[k] = A::mul(g[gw_pair_i(k)], g[gw_pair_j(k)]);
+    gw_gauge_tensor<R>(f + n3, f + 2 * n3, f + 7 * n3, p + 7 * n3, n3, nb, s, dx, ndxg, (R)*aI, rfo2, false, P);
+  }
+};
+} // namespace
 
 namespace {
 
@@ -461,6 +487,77 @@ __attribute__((visibility("hidden"))) int su2_initialize(clb_handle *h, int32_t 
   return check(h, "clb_initialize");
 }
 
+void gw_kick_step(clb_handle *h);
+void gw_drift(clb_handle *h);
+void gw_sync(clb_handle *h);
+
+__attribute__((visibility("hidden"))) bool su2_tangent_active(const clb_handle *h) { return h->su2->tangent; }
+
+// The GW kick (weight w of dt) with the lphi4SU2U1 source, at the current fields, momenta and a_I.
+__attribute__((visibility("hidden"))) void su2_gw_kick(clb_handle *h, double w)
+{
+  SU2Sector *u = h->su2;
+  GWSector *g = h->gw;
+  const double r = h->md.fStar / h->md.omegaStar; // pow<2>(fStar / omegaStar)
+  const double inv_dx2 = 1.0 / (h->cfg.dx * h->cfg.dx), hd = w * h->cfg.dt;
+  const double ndxg = -u->prm.dx * u->prm.gC;     // the phase of Site::phaseC
+  auto go = [&](auto zero) {
+    using R = decltype(zero);
+    const SU2GWSource<R> src{static_cast<const R *>(u->f), static_cast<const R *>(u->p), h->n3, h->N, (R)h->cfg.dx,
+                             (R)ndxg, (R)(r * r), &u->d_st->aI};
+    CLB_LAUNCH(h, K_GW, (k_gw_kick<R, SU2GWSource<R>><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<const R *>(g->u), static_cast<R *>(g->pi), h->N, inv_dx2, hd, &u->d_st->kA, src)));
+  };
+  if (u->fp32) go(0.0f);
+  else go(0.0);
+}
+
+// The GW drift with the a_SI of the matter step just taken (State::p3 = pow(a_SI, alpha - 3)).
+__attribute__((visibility("hidden"))) void su2_gw_drift(clb_handle *h)
+{
+  SU2Sector *u = h->su2;
+  GWSector *g = h->gw;
+  const size_t n = 5 * h->n3;
+  if (u->fp32)
+    CLB_LAUNCH(h, K_GW, k_gw_drift<float><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<float *>(g->u), static_cast<const float *>(g->pi), n, h->cfg.dt, &u->d_st->p3));
+  else
+    CLB_LAUNCH(h, K_GW, k_gw_drift<double><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<double *>(g->u), static_cast<const double *>(g->pi), n, h->cfg.dt, &u->d_st->p3));
+}
+
+namespace {
+// VelocityVerlet::evolve over nsteps with merged kicks; the history rows start at row0.
+void vv_steps(clb_handle *h, int64_t nsteps, int64_t row0)
+{
+  const double dt = h->cfg.dt;
+  const bool ex = h->cfg.expansion != 0;
+  const std::vector<double> &ws = h->ws;
+  const size_t P = ws.size(), S = 2 * P - 1;
+  auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+  const int64_t total = nsteps * (int64_t)S;
+  const double w0 = wof(0);
+  if (ex) tail(h, T_VV_KICK_HALF, false, 0, w0);
+  sweep(h, 1, false, ex, vv_kick(dt, w0, 0.0));
+  if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w0);
+  for (int64_t k = 0; k < total; ++k) {
+    const size_t i = (size_t)(k % (int64_t)S);
+    const double w = wof(i);
+    const bool more = k + 1 < total;
+    const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+    drift(h, w, false);
+    if (i + 1 == S) step_done(h);
+    sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
+    if (ex) {
+      uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
+      if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
+      tail(h, fl, true, w, wn, i + 1 == S ? row0 + k / (int64_t)S : -1);
+    }
+  }
+}
+
+} // namespace
+
 __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nsteps)
 {
   const double dt = h->cfg.dt;
@@ -562,29 +659,17 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
           }
         }
       }
-  } else {
-    const std::vector<double> &ws = h->ws;
-    const size_t P = ws.size(), S = 2 * P - 1;
-    auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
-    const int64_t total = nsteps * (int64_t)S;
-    const double w0 = wof(0);
-    if (ex) tail(h, T_VV_KICK_HALF, false, 0, w0);
-    sweep(h, 1, false, ex, vv_kick(dt, w0, 0.0));
-    if (ex) tail(h, T_STORE_PI2_I | T_VV_DRIFT, true, 0, w0);
-    for (int64_t k = 0; k < total; ++k) {
-      const size_t i = (size_t)(k % (int64_t)S);
-      const double w = wof(i);
-      const bool more = k + 1 < total;
-      const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
-      drift(h, w, false);
-      if (i + 1 == S) step_done(h);
-      sweep(h, more ? 2 : 1, ex, ex, vv_kick(dt, w, wn));
-      if (ex) {
-        uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
-        if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
-        tail(h, fl, true, w, wn, i + 1 == S ? k / (int64_t)S : -1);
-      }
+  } else if (h->gw) {
+    // the GW leapfrog around each matter step (evolver.h:102-124): its kick reads the gauge
+    // momenta at integer time, which the merged sweep between two steps never stores, so the steps
+    // run one by one (the schedule of one-step clb_evolve calls)
+    for (int64_t s = 0; s < nsteps; ++s) {
+      gw_kick_step(h);
+      vv_steps(h, 1, s);
+      gw_drift(h);
     }
+  } else {
+    vv_steps(h, nsteps, 0);
   }
   cudaEventRecord(h->ev_call[1], h->stream);
   const int r = check(h, "clb_evolve");
@@ -595,6 +680,7 @@ __attribute__((visibility("hidden"))) int su2_evolve(clb_handle *h, int64_t nste
 
 __attribute__((visibility("hidden"))) int su2_sync(clb_handle *h)
 {
+  if (h->gw) gw_sync(h); // evolver.h:134-137, before the matter sync
   if (h->cfg.evolver == CLB_LF && !h->synced) {
     sweep(h, 1, false, h->cfg.expansion != 0 && !h->fb, lf_kick(h->cfg.dt, 0.5));
     if (h->cfg.expansion && !h->fb) tail(h, T_STORE_PI2_I | T_LF_SYNC, true);
@@ -762,6 +848,7 @@ __attribute__((visibility("hidden"))) int su2_tangent_begin(clb_handle *h, const
   if (is_pv(h->cfg.evolver))
     return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers the LF and VV evolvers");
   if (h->fb) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form covers the self-consistent expansion");
+  if (h->gw) return h->fail(CLB_EUNSUPPORTED, "clb_tangent_begin: the tangent-linear form runs without the GW sector");
   if (n < 0 || n > 6 || (n > 0 && !couplings_dot))
     return h->fail(CLB_EINVAL, "clb_tangent_begin: up to 6 coupling derivatives");
   cudaError_t e = cudaStreamSynchronize(h->stream);

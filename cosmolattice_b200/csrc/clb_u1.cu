@@ -8,6 +8,7 @@
 // a step are reduced by the next step's kick sweep, which reads the same fields.
 
 #include "clb_adjoint.cuh"
+#include "clb_gws.cuh"
 #include "clb_handle.cuh"
 #include "clb_u1.cuh"
 #include "clb_vv.h"
@@ -22,7 +23,22 @@ namespace clb {
 
 namespace {
 constexpr int kU1Blocks = 148 * 8; // grid-stride sweeps: 8 resident 256-thread blocks per SM
-}
+
+// PITensor.h's GW source for lphi4U1: the complex scalar (components 0, 1) and the U(1) field
+// (components 2..4, momenta 2..4); no singlets.
+template <class R> struct U1GWSource {
+  const R *f, *p;
+  size_t n3;
+  int N;
+  R dx, ndxg, rfo2;
+  const double *aI;
+  __device__ __forceinline__ void operator()(size_t s, int x, int y, int z, int xp, int yp, int zp, R (&P)[6]) const
+  {
+    const size_t nb[3] = {((size_t)xp * N + y) * N + z, ((size_t)x * N + yp) * N + z, ((size_t)x * N + y) * N + zp};
+    gw_gauge_tensor<R>(f, f + n3, f + 2 * n3, p + 2 * n3, n3, nb, s, dx, ndxg, (R)*aI, rfo2, true, P);
+  }
+};
+} // namespace
 
 struct U1Sector {
   void *f = nullptr, *p = nullptr; // 5 x N^3 each, FP64 or FP32 (esz bytes per value)
@@ -236,8 +252,9 @@ template <class S> void kick_save_s(clb_handle *h, int nk, bool red, const U1Kic
 // VelocityVerlet::evolve over nsteps with merged kicks (as u1_evolve).  With sv, the state and the
 // scalar record at every stage boundary are kept: the merged sweep writes the state between its
 // two kicks, and its tail is split at the boundary so the record can be taken there.
-// hist: per-step history rows (clb_evolve sizes that buffer; the adjoint's runs write none).
-void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv, bool hist = true)
+// hist: per-step history rows (clb_evolve sizes that buffer; the adjoint's runs write none), the
+// first at row row0.
+void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv, bool hist = true, int64_t row0 = 0)
 {
   const double dt = h->cfg.dt;
   const bool ex = h->cfg.expansion != 0;
@@ -264,7 +281,7 @@ void vv_run(clb_handle *h, int64_t nsteps, const SegSave *sv, bool hist = true)
       if (ex) {
         uint32_t fl = T_STORE_FIELDS | T_STORE_PI2_I | T_VV_KICK_ONE;
         if (more) fl |= T_VV_KICK_HALF | T_STORE_PI2_B | T_VV_DRIFT;
-        tail(h, fl, true, w, wn, hist && i + 1 == S ? k / (int64_t)S : -1);
+        tail(h, fl, true, w, wn, hist && i + 1 == S ? row0 + k / (int64_t)S : -1);
       }
     } else {
       char *slot = sv->seg + (size_t)(k + 1) * 2 * sv->half;
@@ -332,6 +349,42 @@ int check(clb_handle *h, const char *where)
 }
 
 } // namespace
+
+void gw_kick_step(clb_handle *h);
+void gw_drift(clb_handle *h);
+void gw_sync(clb_handle *h);
+
+// The GW kick (weight w of dt) with the lphi4U1 source, at the current fields, momenta and a_I.
+__attribute__((visibility("hidden"))) void u1_gw_kick(clb_handle *h, double w)
+{
+  U1Sector *u = h->u1;
+  GWSector *g = h->gw;
+  const double r = h->md.fStar / h->md.omegaStar; // pow<2>(fStar / omegaStar)
+  const double inv_dx2 = 1.0 / (h->cfg.dx * h->cfg.dx), hd = w * h->cfg.dt;
+  auto go = [&](auto zero) {
+    using R = decltype(zero);
+    const U1GWSource<R> src{static_cast<const R *>(u->f), static_cast<const R *>(u->p), h->n3, h->N, (R)h->cfg.dx,
+                            (R)u->prm.ndxg, (R)(r * r), &u->d_st->aI};
+    CLB_LAUNCH(h, K_GW, (k_gw_kick<R, U1GWSource<R>><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<const R *>(g->u), static_cast<R *>(g->pi), h->N, inv_dx2, hd, &u->d_st->kA, src)));
+  };
+  if (u->fp32) go(0.0f);
+  else go(0.0);
+}
+
+// The GW drift with the a_SI of the matter step just taken (U1State::cs_drift = pow(a_SI, alpha - 3)).
+__attribute__((visibility("hidden"))) void u1_gw_drift(clb_handle *h)
+{
+  U1Sector *u = h->u1;
+  GWSector *g = h->gw;
+  const size_t n = 5 * h->n3;
+  if (u->fp32)
+    CLB_LAUNCH(h, K_GW, k_gw_drift<float><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<float *>(g->u), static_cast<const float *>(g->pi), n, h->cfg.dt, &u->d_st->cs_drift));
+  else
+    CLB_LAUNCH(h, K_GW, k_gw_drift<double><<<kGWBlocks, 256, 0, h->stream>>>(
+                            static_cast<double *>(g->u), static_cast<const double *>(g->pi), n, h->cfg.dt, &u->d_st->cs_drift));
+}
 
 __attribute__((visibility("hidden"))) int u1_create(clb_handle *h)
 {
@@ -589,6 +642,15 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
           tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), true, 0, w0, s);
         }
       }
+  } else if (h->gw) {
+    // the GW leapfrog around each matter step (evolver.h:102-124): its kick reads the gauge
+    // momenta at integer time, which the merged sweep between two steps never stores, so the steps
+    // run one by one (the schedule of one-step clb_evolve calls)
+    for (int64_t s = 0; s < nsteps; ++s) {
+      gw_kick_step(h);
+      vv_run(h, 1, nullptr, true, s);
+      gw_drift(h);
+    }
   } else {
     vv_run(h, nsteps, nullptr);
   }
@@ -602,6 +664,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
 // LeapFrog::sync (leapfrog.h:96-116); a no-op on the VV.
 __attribute__((visibility("hidden"))) int u1_sync(clb_handle *h)
 {
+  if (h->gw) gw_sync(h); // evolver.h:134-137, before the matter sync
   if (h->cfg.evolver == CLB_LF && !h->synced) {
     h->u1->lf_fresh = false;
     kick_sweep(h, 1, false, h->cfg.expansion != 0 && !h->fb, lf_kick(h->cfg.dt, 0.5));
@@ -794,6 +857,7 @@ __attribute__((visibility("hidden"))) int u1_forward(clb_handle *h, int64_t nste
   if (is_pv(h->cfg.evolver))
     return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the VV evolvers and the leapfrog");
   if (h->fb) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint covers the self-consistent expansion");
+  if (h->gw) return h->fail(CLB_EUNSUPPORTED, "clb_forward: the adjoint runs without the GW sector");
   if (nsteps < 1 || K < 1) return h->fail(CLB_EINVAL, "clb_forward: nsteps and checkpoint_every must be >= 1");
   if (nw < 0 || nw > kAvgN || (nw > 0 && !w)) return h->fail(CLB_EINVAL, "clb_forward: up to 5 energy weights");
   cudaError_t e = cudaStreamSynchronize(h->stream);

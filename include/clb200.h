@@ -393,14 +393,17 @@ typedef struct clb_batch_form {
 int clb_batch_set_persistent(clb_batch *b, int32_t tile_z, int32_t tile_y, int32_t sites_per_thread, int32_t planes_x);
 int clb_batch_get_form(clb_batch *b, clb_batch_form *out);
 
-/* ---- gravitational waves of the scalar singlets -------------------------------------------------
+/* ---- gravitational waves -------------------------------------------------------------------------
  * The GW sector of the reference (GWsKernels::get, evolvers/kernels/gwskernels.h:27-33; the
- * scalar-singlet source of PITensor.h; Evolver::evolve/sync with the default doLFforGWs, a leapfrog
- * staggered over the matter evolver, evolvers/evolver.h:102-138; GWsInitializer, zero at the
- * start).  The field is the traceless symmetric u_ij as five components (u_11, u_12, u_13, u_22,
- * u_23; u_33 = -u_11 - u_22), its momenta likewise.
- * clb_gws_enable: after clb_create, before clb_initialize; scalar-singlet models with the VV
- * evolvers on the fused path and self-consistent or no expansion (else CLB_EUNSUPPORTED).
+ * sources of PITensor.h: scalar singlets, complex scalars through their U(1) covariant forward
+ * differences, U(1) electric and magnetic fields; Evolver::evolve/sync with the default
+ * doLFforGWs, a leapfrog staggered over the matter evolver, evolvers/evolver.h:102-138;
+ * GWsInitializer, zero at the start).  The field is the traceless symmetric u_ij as five
+ * components (u_11, u_12, u_13, u_22, u_23; u_33 = -u_11 - u_22), its momenta likewise.
+ * clb_gws_enable: after clb_create, before clb_initialize; every model with the VV evolvers, the
+ * scalar singlets on the fused path, and self-consistent or no expansion (else CLB_EUNSUPPORTED).
+ * A gauge handle with GWs takes no clb_forward and no clb_tangent_begin (CLB_EUNSUPPORTED), and
+ * the reverse.
  * clb_gws_set_state / clb_gws_get_state: 5 x N^3 doubles each (either may be NULL).
  * clb_gw_spectrum: the GW energy spectrum d(rho_GW/rho)/dlog k (PowerSpectrumMeasurer::
  * powerSpectrumGW, measurements/powerspectrum.h:51-71) with the TT projector of

@@ -575,7 +575,9 @@ int orc_set_scalar_model(orc_handle *h, int32_t id)
 // components of each (5 x N^3 doubles, the order of u_11, u_12, u_13, u_22, u_23).
 int orc_gws_enable(orc_handle *h)
 {
-  if (!h || isU1(h) || isSU2(h)) return CLB_EUNSUPPORTED;
+  if (!h) return CLB_EINVAL;
+  if (isSU2(h)) return oracle_models::su2_gws_enable(H(h)->impl);
+  if (isU1(h)) return oracle_models::u1_gws_enable(H(h)->impl);
   Oracle *o = S(h);
   o->gws = true;
   o->gwSynced = true;
@@ -583,9 +585,24 @@ int orc_gws_enable(orc_handle *h)
   o->gpi.assign(5 * o->n3, 0.0);
   return CLB_OK;
 }
+// the GW sector of a gauge handle (null for a scalar-singlet handle)
+static oracle_models::GWs *gauge_gws(orc_handle *h)
+{
+  if (isSU2(h)) return oracle_models::su2_gws(H(h)->impl);
+  if (isU1(h)) return oracle_models::u1_gws(H(h)->impl);
+  return nullptr;
+}
+
 int orc_gws_set_state(orc_handle *h, const double *u, const double *pi)
 {
-  if (!h || isU1(h) || isSU2(h) || !S(h)->gws) return CLB_ESTATE;
+  if (!h) return CLB_EINVAL;
+  if (oracle_models::GWs *g = gauge_gws(h)) {
+    if (!g->on) return CLB_ESTATE;
+    if (u) std::memcpy(g->u.data(), u, g->u.size() * sizeof(double));
+    if (pi) std::memcpy(g->pi.data(), pi, g->pi.size() * sizeof(double));
+    return CLB_OK;
+  }
+  if (!S(h)->gws) return CLB_ESTATE;
   Oracle *o = S(h);
   if (u) std::memcpy(o->gu.data(), u, o->gu.size() * sizeof(double));
   if (pi) std::memcpy(o->gpi.data(), pi, o->gpi.size() * sizeof(double));
@@ -593,7 +610,14 @@ int orc_gws_set_state(orc_handle *h, const double *u, const double *pi)
 }
 int orc_gws_get_state(orc_handle *h, double *u, double *pi)
 {
-  if (!h || isU1(h) || isSU2(h) || !S(h)->gws) return CLB_ESTATE;
+  if (!h) return CLB_EINVAL;
+  if (oracle_models::GWs *g = gauge_gws(h)) {
+    if (!g->on) return CLB_ESTATE;
+    if (u) std::memcpy(u, g->u.data(), g->u.size() * sizeof(double));
+    if (pi) std::memcpy(pi, g->pi.data(), g->pi.size() * sizeof(double));
+    return CLB_OK;
+  }
+  if (!S(h)->gws) return CLB_ESTATE;
   Oracle *o = S(h);
   if (u) std::memcpy(u, o->gu.data(), o->gu.size() * sizeof(double));
   if (pi) std::memcpy(pi, o->gpi.data(), o->gpi.size() * sizeof(double));

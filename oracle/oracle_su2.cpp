@@ -109,6 +109,7 @@ struct SU2Oracle {
   bool synced = true, initialized = false;
   std::vector<double> ws;
   std::string err;
+  oracle_models::GWs gw; // the GW sector (PITensor.h source: S, phi and A)
 
   double qG() const { return md.couplings[0]; }
   double qH() const { return md.couplings[1]; }
@@ -126,6 +127,25 @@ struct SU2Oracle {
 
   size_t at(int x, int y, int z) const { return ((size_t)x * N + y) * N + z; }
   int wrap(int i) const { return i < 0 ? i + N : (i >= N ? i - N : i); }
+
+  // PITensor.h's anisotropic tensor of lphi4SU2U1 at (x, y, z): the singlet S, then the complex
+  // scalar phi and the U(1) field; the doublet and the SU(2) field source none
+  void gwTensor(int x, int y, int z, double (&T)[6]) const
+  {
+    const size_t s = at(x, y, z);
+    const size_t nbp[3] = {at(wrap(x + 1), y, z), at(x, wrap(y + 1), z), at(x, y, wrap(z + 1))};
+    double g[3];
+    for (int i = 0; i < 3; ++i) g[i] = (f(0)[nbp[i]] - f(0)[s]) / cfg.dx;
+    const int I[6] = {0, 0, 0, 1, 1, 2}, J[6] = {0, 1, 2, 1, 2, 2};
+    for (int k = 0; k < 6; ++k) T[k] = g[I[k]] * g[J[k]];
+    const double *const A[3] = {f(7), f(8), f(9)};
+    const double *const pA[3] = {p(7), p(8), p(9)};
+    oracle_models::gw_gauge_tensor(f(1), f(2), A, pA, nbp, s, cfg.dx, gC(), aI, rfo2(), false, T);
+  }
+  void gwKick(double w)
+  {
+    gw.kick(N, cfg.dx, aI, md.alpha, w * cfg.dt, [&](int x, int y, int z, double (&T)[6]) { gwTensor(x, y, z, T); });
+  }
   size_t nb(int x, int y, int z, int d1, int s1, int d2 = 0, int s2 = 0) const
   {
     int c[3] = {x, y, z};
@@ -853,10 +873,19 @@ int su2_initialize(void *h, int32_t correct_adot)
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
+  o->gw.synced = true;
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;
   return CLB_OK;
 }
+
+int su2_gws_enable(void *h)
+{
+  SU2Oracle *o = static_cast<SU2Oracle *>(h);
+  o->gw.enable(o->n3);
+  return CLB_OK;
+}
+GWs *su2_gws(void *h) { return &static_cast<SU2Oracle *>(h)->gw; }
 
 int su2_evolve(void *h, int64_t n)
 {
@@ -866,6 +895,10 @@ int su2_evolve(void *h, int64_t n)
     return CLB_ESTATE;
   }
   for (int64_t s = 0; s < n; ++s) {
+    if (o->gw.on) { // evolver.h:104-107
+      o->gwKick(o->gw.synced ? 0.5 : 1.0);
+      o->gw.synced = false;
+    }
     if (o->fb)
       o->evolveFB();
     else if (o->cfg.evolver == CLB_LF)
@@ -874,6 +907,7 @@ int su2_evolve(void *h, int64_t n)
       o->evolvePV();
     else
       o->evolveVV();
+    if (o->gw.on) o->gw.drift(std::pow(o->aSI, o->md.alpha - 3), o->cfg.dt); // evolver.h:123
     o->t += o->cfg.dt;
   }
   return CLB_OK;
@@ -882,6 +916,10 @@ int su2_evolve(void *h, int64_t n)
 int su2_sync(void *h)
 {
   SU2Oracle *o = static_cast<SU2Oracle *>(h);
+  if (o->gw.on && !o->gw.synced) { // evolver.h:134-137
+    o->gwKick(0.5);
+    o->gw.synced = true;
+  }
   if (o->fb) {
     if (o->cfg.evolver == CLB_LF && !o->synced) o->lf_kick(0.5);
     o->synced = true;

@@ -51,6 +51,7 @@ struct U1Oracle {
 
   double potI = 0, potSI = 0;
   bool synced = true, initialized = false;
+  oracle_models::GWs gw; // the GW sector (PITensor.h source: phi and A)
   std::vector<double> ws;
   std::string err;
 
@@ -223,6 +224,19 @@ struct U1Oracle {
     const double f21 = Fij(1, 0, x, y, z), f31 = Fij(2, 0, x, y, z), f32 = Fij(2, 1, x, y, z);
     return f21 * f21 + (f31 * f31 + f32 * f32);
   }
+  // PITensor.h's anisotropic tensor of lphi4U1 at (x, y, z): the complex scalar and the U(1) field
+  void gwTensor(int x, int y, int z, double (&T)[6]) const
+  {
+    const size_t nbp[3] = {nb(x, y, z, 0, +1), nb(x, y, z, 1, +1), nb(x, y, z, 2, +1)};
+    const double *const A[3] = {f(2), f(3), f(4)};
+    const double *const pA[3] = {P.data() + 2 * n3, P.data() + 3 * n3, P.data() + 4 * n3};
+    oracle_models::gw_gauge_tensor(f(0), f(1), A, pA, nbp, at(x, y, z), cfg.dx, gQ(), aI, rfo2(), true, T);
+  }
+  void gwKick(double w)
+  {
+    gw.kick(N, cfg.dx, aI, md.alpha, w * cfg.dt, [&](int x, int y, int z, double (&T)[6]) { gwTensor(x, y, z, T); });
+  }
+
   double avCsGrad2() { return average([&](int x, int y, int z) { return csGrad2(x, y, z); }); }
   double avU1B2() { return average([&](int x, int y, int z) { return u1B2(x, y, z); }); }
   double avPot() { return average([&](int x, int y, int z) { return pot(at(x, y, z)); }); }
@@ -575,10 +589,19 @@ int u1_initialize(void *h, int32_t correct_adot)
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
+  o->gw.synced = true;
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;
   return CLB_OK;
 }
+
+int u1_gws_enable(void *h)
+{
+  U1Oracle *o = static_cast<U1Oracle *>(h);
+  o->gw.enable(o->n3);
+  return CLB_OK;
+}
+GWs *u1_gws(void *h) { return &static_cast<U1Oracle *>(h)->gw; }
 
 int u1_evolve(void *h, int64_t n)
 {
@@ -588,6 +611,10 @@ int u1_evolve(void *h, int64_t n)
     return CLB_ESTATE;
   }
   for (int64_t s = 0; s < n; ++s) {
+    if (o->gw.on) { // evolver.h:104-107
+      o->gwKick(o->gw.synced ? 0.5 : 1.0);
+      o->gw.synced = false;
+    }
     if (o->fb)
       o->evolveFB();
     else if (o->cfg.evolver == CLB_LF)
@@ -596,6 +623,7 @@ int u1_evolve(void *h, int64_t n)
       o->evolvePV();
     else
       o->evolveVV();
+    if (o->gw.on) o->gw.drift(std::pow(o->aSI, o->md.alpha - 3), o->cfg.dt); // evolver.h:123
     o->t += o->cfg.dt;
   }
   return CLB_OK;
@@ -604,6 +632,10 @@ int u1_evolve(void *h, int64_t n)
 int u1_sync(void *h)
 {
   U1Oracle *o = static_cast<U1Oracle *>(h);
+  if (o->gw.on && !o->gw.synced) { // evolver.h:134-137
+    o->gwKick(0.5);
+    o->gw.synced = true;
+  }
   if (o->fb) {
     if (o->cfg.evolver == CLB_LF && !o->synced) o->kick(0.5 * o->cfg.dt, 0.5 * o->cfg.dt);
     o->synced = true;

@@ -1,4 +1,5 @@
-"""Gravitational waves of the scalar singlets (clb_gws_*, clb_gw_spectrum) on the B200.
+"""Gravitational waves (clb_gws_*, clb_gw_spectrum) on the B200: the scalar singlets' sector, and
+the gauge models' (lphi4U1, lphi4SU2U1) with the complex-scalar and U(1) sources of PITensor.h.
 
 Against the oracle's restatement (the reference's default: a leapfrog for the GWs staggered over
 the VV matter evolver, evolver.h:102-138; the kernel of gwskernels.h:27-33 with the PITensor.h
@@ -142,11 +143,147 @@ def test_gws_reject_other_evolvers_and_models():
             lat.gws_enable()
         assert ei.value.code == _capi.CLB_EUNSUPPORTED
         lat.close()
+    par, rp, m, f, p, sf = make_u1_case(N=8, evolver="LF")
+    lat = Lattice(m, rp)
+    with pytest.raises(_capi.ClbError) as ei:
+        lat.gws_enable()
+    assert ei.value.code == _capi.CLB_EUNSUPPORTED
+    lat.close()
+
+
+def test_gauge_gws_refuse_the_adjoint_and_tangent_forms():
+    # the adjoint pair and the tangent-linear form do not advance the GW sector, so neither runs
+    # beside it
+    from cosmolattice_b200 import Lattice, _capi
+    from conftest import make_su2_case, make_u1_case
+
     par, rp, m, f, p, sf = make_u1_case(N=8)
     lat = Lattice(m, rp)
-    with pytest.raises(_capi.ClbError):
-        lat.gws_enable()
+    lat.gws_enable()
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    with pytest.raises(_capi.ClbError) as ei:
+        lat.forward(4, 2, [0, 0, 1, 1, 0])
+    assert ei.value.code == _capi.CLB_EUNSUPPORTED
     lat.close()
+    par, rp, m, f, p, sf = make_su2_case(N=8)
+    for order in ("gws_first", "tangent_first"):
+        lat = Lattice(m, rp)
+        lat.set_state(f, p, sf)
+        if order == "gws_first":
+            lat.gws_enable()
+            with pytest.raises(_capi.ClbError) as ei:
+                lat.tangent_begin([0, 0, 0, 0, 1, 0])
+        else:
+            lat.tangent_begin([0, 0, 0, 0, 1, 0])
+            with pytest.raises(_capi.ClbError) as ei:
+                lat.gws_enable()
+        assert ei.value.code == _capi.CLB_EUNSUPPORTED
+        lat.close()
+
+
+def _gauge_case(model, evolver, N):
+    from conftest import make_su2_case, make_u1_case
+
+    if model == "lphi4U1":
+        return make_u1_case(N=N, evolver=evolver, amp=3e-2)
+    return make_su2_case(N=N, evolver=evolver, amp=3e-2)
+
+
+def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True):
+    from cosmolattice_b200 import Lattice
+    from oracle.oracle import OracleLattice
+
+    par, rp, m, f, p, sf = _gauge_case(model, evolver, N)
+    gpu, cpu = Lattice(m, rp, precision=precision), OracleLattice(m, rp)
+    for lat in (gpu, cpu):
+        if gws:
+            lat.gws_enable()
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        for _ in range(3):
+            lat.evolve(10)
+            lat.sync()
+    return rp, m, gpu, cpu
+
+
+@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4U1", "VV4"), ("lphi4SU2U1", "VV2")])
+def test_gauge_gw_evolution_matches_oracle(model, evolver):
+    # the complex scalar, U(1) electric and magnetic (and for lphi4SU2U1 singlet) sources of
+    # PITensor.h: GW field and momenta per component within 1e-12 of the component's max after 30
+    # steps in three calls with syncs, against the oracle's restatement
+    rp, m, gpu, cpu = _gauge_pair(model, evolver)
+    ug, pg = gpu.gws_get_state()
+    uc, pc = cpu.gws_get_state()
+    sg, sc = gpu.get_state()[2], cpu.get_state()[2]
+    gpu.close()
+    cpu.close()
+    assert np.abs(pc).max() > 0 and np.abs(uc).max() > 0
+    worst = 0.0
+    for a, b in ((ug, uc), (pg, pc)):
+        for c in range(5):
+            x, y = a.reshape(5, -1)[c], b.reshape(5, -1)[c]
+            worst = max(worst, np.abs(x - y).max() / np.abs(y).max())
+    print(model, evolver, "GW rel. error", worst)
+    assert worst <= 1e-12
+    assert abs(sg["aI"] - sc["aI"]) <= 1e-12 * sc["aI"]
+
+
+@pytest.mark.parametrize("model", ["lphi4U1", "lphi4SU2U1"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gauge_gws_leave_the_matter_evolution_bitwise(model, precision):
+    # the GWs do not act back, and their per-step schedule is that of one-step evolve calls: the
+    # matter state and the scale factor equal those of a run without GWs to the last bit
+    from cosmolattice_b200 import Lattice
+
+    par, rp, m, f, p, sf = _gauge_case(model, "VV2", 12)
+    out = []
+    for gws in (True, False):
+        lat = Lattice(m, rp, precision=precision)
+        if gws:
+            lat.gws_enable()
+        lat.set_state(f, p, sf)
+        lat.initialize()
+        lat.evolve(7)
+        lat.sync()
+        lat.evolve(5)
+        out.append(lat.get_state())
+        lat.close()
+    (fa, pa, sa), (fb, pb, sb) = out
+    assert np.array_equal(fa, fb) and np.array_equal(pa, pb) and sa == sb
+
+
+def test_fp32_gauge_gws_track_fp64():
+    rp, m, g64, cpu = _gauge_pair("lphi4U1", "VV2")
+    cpu.close()
+    u64, p64 = g64.gws_get_state()
+    g64.close()
+    rp, m, g32, cpu = _gauge_pair("lphi4U1", "VV2", precision="fp32")
+    cpu.close()
+    u32, p32 = g32.gws_get_state()
+    g32.close()
+    rel = max(np.abs(a - b).max() / np.abs(b).max() for a, b in ((u32, u64), (p32, p64)))
+    print("fp32 gauge GW rel. error", rel)
+    assert rel <= 3e-4
+
+
+def test_gauge_gw_spectrum_matches_numpy():
+    from oracle.spectrum import gw_spectrum
+
+    rp, m, gpu, cpu = _gauge_pair("lphi4U1", "VV2")
+    cpu.close()
+    N = rp.N
+    k, v, cnt, frac = gpu.gw_spectrum(prj_type=1, ps_type=1)
+    mm = gpu.measure(1.0)
+    _, pi = gpu.gws_get_state()
+    gpu.close()
+    fac = (m.fStar / m.MPl) ** 2 / (4 * mm["aI"] ** 6 * mm["energies"][-1])
+    ko, vo, co = gw_spectrum(pi.reshape(5, N, N, N), rp.dx, prj_type=1, ps_type=1, factor=fac)
+    assert cnt.tolist() == co.tolist()
+    band = vo > 1e-8 * vo.max()
+    assert band.sum() > 3
+    assert np.all(np.abs(v - vo)[band] <= 1e-10 * vo[band])
+    assert frac > 0
 
 
 def test_run_writes_gw_files(tmp_path):
