@@ -610,15 +610,24 @@ template <class R, int NS> struct EvolveLF {
     }
     // Fused: drift of step n and kick of step n+1 in one sweep; the sweep's reductions are the
     // field averages of phi_{n+1} and <pi_{n+3/2}^2>, which the tail books in LeapFrog order.
+    // With GWs (evolver.h:102-124): the GW kick of step n+1 reads phi_{n+1} and a_I of step n+1,
+    // and the GW drift of step n the a_SI of step n; both hold between the fused sweep and its
+    // tail, which drifts a on.
     const double weight = h->synced ? 0.5 : 1.0;
+    if (h->gw) gw_kick_step(h);
     L::kick(h, weight * dt);
     if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, L::reduce_pi2(h));
     for (int64_t s = 1; s < nsteps; ++s) {
       L::fused(h, dt, dt, 0.0, ex);
+      if (h->gw) {
+        gw_drift(h);
+        gw_kick_step(h);
+      }
       if (ex)
         tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, h->sweep_blocks, 0, 0, s - 1);
     }
     L::drift_fields(h, dt, ex);
+    if (h->gw) gw_drift(h);
     if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY, h->sweep_blocks, 0, 0, nsteps - 1);
     h->synced = false;
   }

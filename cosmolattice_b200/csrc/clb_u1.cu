@@ -600,12 +600,17 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
     }
   } else if (h->cfg.evolver == CLB_LF) {
     // LeapFrog::evolve: kick (1/2 dt after a sync), <pi^2>, a kick and drift, field drifts, field averages
+    // With GWs (evolver.h:102-124): a GW kick before each step's kick (the step's fields, the
+    // momenta half a step back, a_I) and a GW drift after its drift (its a_SI)
     const double weight = h->synced ? 0.5 : 1.0;
+    if (h->gw) gw_kick_step(h);
     kick_sweep(h, 1, false, ex, lf_kick(dt, weight));
     if (ex) tail(h, T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true);
     for (int64_t s = 0; s < nsteps; ++s) {
       drift(h, 1.0);
+      if (h->gw) gw_drift(h);
       if (s + 1 < nsteps) {
+        if (h->gw) gw_kick_step(h);
         kick_sweep(h, 1, ex, ex, lf_kick(dt, 1.0));
         if (ex) tail(h, T_STORE_FIELDS | T_HIST_EARLY | T_STORE_PI2_LF | T_LF_KICK | T_LF_DRIFT, true, 0, 0, s);
       } else {

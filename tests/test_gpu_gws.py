@@ -36,7 +36,7 @@ def _pair(model, evolver, precision="fp64", N=24):
     return rp, m, gpu, cpu
 
 
-@pytest.mark.parametrize("model,evolver", [("lphi4_1f", "VV2"), ("lphi4_1f", "VV4"), ("lphi4", "VV2")])
+@pytest.mark.parametrize("model,evolver", [("lphi4_1f", "VV2"), ("lphi4_1f", "VV4"), ("lphi4", "VV2"), ("lphi4_1f", "LF")])
 def test_gw_evolution_matches_oracle(model, evolver):
     rp, m, gpu, cpu = _pair(model, evolver)
     ug, pg = gpu.gws_get_state()
@@ -136,14 +136,14 @@ def test_gws_reject_other_evolvers_and_models():
     from cosmolattice_b200 import Lattice, _capi
     from conftest import make_u1_case
 
-    for ev in ("LF", "PV2"):
+    for ev in ("PV2",):
         par, rp, m, f, p, sf = make_scalar_case(N=8, evolver=ev)
         lat = Lattice(m, rp)
         with pytest.raises(_capi.ClbError) as ei:
             lat.gws_enable()
         assert ei.value.code == _capi.CLB_EUNSUPPORTED
         lat.close()
-    par, rp, m, f, p, sf = make_u1_case(N=8, evolver="LF")
+    par, rp, m, f, p, sf = make_u1_case(N=8, evolver="PV2")
     lat = Lattice(m, rp)
     with pytest.raises(_capi.ClbError) as ei:
         lat.gws_enable()
@@ -207,7 +207,8 @@ def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True):
     return rp, m, gpu, cpu
 
 
-@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4U1", "VV4"), ("lphi4SU2U1", "VV2")])
+@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4U1", "VV4"), ("lphi4SU2U1", "VV2"),
+                                           ("lphi4U1", "LF"), ("lphi4SU2U1", "LF")])
 def test_gauge_gw_evolution_matches_oracle(model, evolver):
     # the complex scalar, U(1) electric and magnetic (and for lphi4SU2U1 singlet) sources of
     # PITensor.h: GW field and momenta per component within 1e-12 of the component's max after 30
@@ -229,14 +230,14 @@ def test_gauge_gw_evolution_matches_oracle(model, evolver):
     assert abs(sg["aI"] - sc["aI"]) <= 1e-12 * sc["aI"]
 
 
-@pytest.mark.parametrize("model", ["lphi4U1", "lphi4SU2U1"])
+@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4SU2U1", "VV2"), ("lphi4U1", "LF")])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_gauge_gws_leave_the_matter_evolution_bitwise(model, precision):
+def test_gauge_gws_leave_the_matter_evolution_bitwise(model, evolver, precision):
     # the GWs do not act back, and their per-step schedule is that of one-step evolve calls: the
     # matter state and the scale factor equal those of a run without GWs to the last bit
     from cosmolattice_b200 import Lattice
 
-    par, rp, m, f, p, sf = _gauge_case(model, "VV2", 12)
+    par, rp, m, f, p, sf = _gauge_case(model, evolver, 12)
     out = []
     for gws in (True, False):
         lat = Lattice(m, rp, precision=precision)
