@@ -1018,6 +1018,7 @@ int clb_initialize(clb_handle *h, int32_t correct_adot)
   if (h->u1 || h->su2) {
     const int r = h->u1 ? u1_initialize(h, correct_adot) : su2_initialize(h, correct_adot);
     if (r == CLB_OK) h->initialized = true;
+    if (h->gw) gw_set_synced(h, correct_adot != CLB_INIT_RESTART); // evolver.h:52
     return r;
   }
   if (correct_adot == CLB_INIT_RESTART && h->fb)

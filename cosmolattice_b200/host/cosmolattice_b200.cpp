@@ -157,7 +157,14 @@ double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &pat
     throw std::runtime_error(path + ": saved for another model or lattice size");
   const size_t n3 = (size_t)hdr[5];
   std::vector<double> f((size_t)hdr[3] * n3), p((size_t)hdr[4] * n3);
-  for (const auto &s : sectors(m)) {
+  const auto secs = sectors(m);
+  // header word 7, bit 0: the five GW field and momentum pairs follow the scalar singlets; this
+  // host runs no GW sector, so it steps over them (loadSim reads them only for a model with GWs)
+  const size_t gw_at = m.kind == CLB_MODEL_LPHI4SU2U1 ? 1 : m.kind == CLB_MODEL_LPHI4U1 ? 0 : secs.size();
+  for (size_t k = 0; k <= secs.size(); ++k) {
+    if ((hdr[7] & 1) && k == gw_at) in.seekg((std::streamoff)(10 * n3 * 8), std::ios::cur);
+    if (k == secs.size()) break;
+    const auto &s = secs[k];
     in.read(reinterpret_cast<char *>(f.data() + (size_t)s[0] * n3), (std::streamsize)(s[1] * n3 * 8));
     in.read(reinterpret_cast<char *>(p.data() + (size_t)s[2] * n3), (std::streamsize)(s[3] * n3 * 8));
   }

@@ -238,6 +238,9 @@ class Lattice:
     # ---- gravitational waves (clb_gws_*; the reference's GW sector with doLFforGWs) ----
     def gws_enable(self) -> None:
         self._check(self.lib.clb_gws_enable(self.h))
+        self.gws_on = True
+
+    gws_on = False  # the GW sector is enabled on this lattice
 
     def gws_set_state(self, u=None, pi=None) -> None:
         n = 5 * self.rp.N ** 3

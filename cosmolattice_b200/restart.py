@@ -6,10 +6,13 @@ variables go, in the same order, into a plain binary file:
 
     magic      16 bytes  b"CLB200-RESTART\\0\\0"
     header     8 x int64 version (1), model kind (clb_model_desc.kind), N, field components,
-                         momentum components, sites per array (N^3), number of sectors, 0
+                         momentum components, sites per array (N^3), number of sectors, flags
+                         (bit 0: the GW arrays are present)
     sectors    for each sector in the reference's save order (scalar singlets, complex scalars,
                SU(2) doublets, U(1) fields, SU(2) fields): its field components, then its momentum
-               components, each N^3 float64 values in the order of clb_get_state
+               components, each N^3 float64 values in the order of clb_get_state; with the GW flag,
+               after the scalar singlets (simulationmanager.h:112-114), the five GW field
+               components each followed by its momentum component, N^3 float64 values each
     scalars    7 x float64   aSI, aI, aIM, aDotSI, aDotI, aDotSIM, tSave
     parameters int64 length, then the UTF-8 "key = value" lines of the run's parameters
 
@@ -44,19 +47,42 @@ def sectors(model) -> List[Tuple[str, range, range]]:
     return [(f"scalar_{i}", range(i, i + 1), range(i, i + 1)) for i in range(model.Ns)]
 
 
+FLAG_GWS = 1
+
+
+def _gw_slot(secs) -> int:
+    """Index of the first sector after the scalar singlets: where the GW arrays go."""
+    k = 0
+    while k < len(secs) and secs[k][0].startswith("scalar_"):
+        k += 1
+    return k
+
+
 def save_sim(path: str, lattice, model, t: float, params: Dict[str, object] = None) -> None:
-    """saveSim: the lattice's state, scale factor and time (and the run's parameters) to path."""
+    """saveSim: the lattice's state, its GWs if enabled, scale factor and time (and the run's
+    parameters) to path."""
     f, p, sf = lattice.get_state()
     N = lattice.rp.N
     n3 = N ** 3
     F = f.reshape(-1, n3)
     P = p.reshape(-1, n3)
     secs = sectors(model)
+    gws = getattr(lattice, "gws_on", False)
+    if gws:
+        gu, gp = (a.reshape(5, n3) for a in lattice.gws_get_state())
     tmp = path + ".part"
     with open(tmp, "wb") as fh:
         fh.write(MAGIC)
-        fh.write(struct.pack("<8q", VERSION, int(model.kind), N, F.shape[0], P.shape[0], n3, len(secs), 0))
-        for _, fc, pc in secs:
+        fh.write(struct.pack("<8q", VERSION, int(model.kind), N, F.shape[0], P.shape[0], n3, len(secs),
+                             FLAG_GWS if gws else 0))
+        for k in range(len(secs) + 1):
+            if gws and k == _gw_slot(secs):
+                for c in range(5):
+                    fh.write(np.ascontiguousarray(gu[c], dtype="<f8").tobytes())
+                    fh.write(np.ascontiguousarray(gp[c], dtype="<f8").tobytes())
+            if k == len(secs):
+                break
+            _, fc, pc = secs[k]
             for c in fc:
                 fh.write(np.ascontiguousarray(F[c], dtype="<f8").tobytes())
             for c in pc:
@@ -74,18 +100,20 @@ def _open(path: str):
     try:
         if fh.read(16) != MAGIC:
             raise ValueError(f"{path}: not a restart file")
-        version, kind, N, nf, npm, n3, nsec, _ = struct.unpack("<8q", fh.read(64))
+        version, kind, N, nf, npm, n3, nsec, flags = struct.unpack("<8q", fh.read(64))
         if version != VERSION:
             raise ValueError(f"{path}: restart format version {version}, expected {VERSION}")
     except Exception:
         fh.close()
         raise
-    return fh, {"kind": kind, "N": N, "n_fields": nf, "n_momenta": npm, "n3": n3, "n_sectors": nsec}
+    return fh, {"kind": kind, "N": N, "n_fields": nf, "n_momenta": npm, "n3": n3, "n_sectors": nsec,
+                "gws": bool(flags & FLAG_GWS)}
 
 
 def load_sim(path: str, lattice, model):
-    """loadSim: the state of path into lattice (same model and N), then the cached averages.
-    Returns (t, parameter text)."""
+    """loadSim: the state of path into lattice (same model and N), its GWs if the lattice has them
+    enabled (loadSim reads them only then; a lattice with GWs needs a file with them), then the
+    cached averages.  Returns (t, parameter text)."""
     fh, hdr = _open(path)
     with fh:
         N = lattice.rp.N
@@ -94,8 +122,19 @@ def load_sim(path: str, lattice, model):
         if hdr["kind"] != int(model.kind) or hdr["N"] != N:
             raise ValueError(f"{path}: saved model kind {hdr['kind']} at N = {hdr['N']}, this run is kind "
                              f"{int(model.kind)} at N = {N}")
+        gws = getattr(lattice, "gws_on", False)
+        if gws and not hdr["gws"]:
+            raise ValueError(f"{path}: the run has GWs, the restart file has none")
         n3 = hdr["n3"]
-        for _, fc, pc in sectors(model):
+        secs = sectors(model)
+        gu = gp = None
+        for k in range(len(secs) + 1):
+            if hdr["gws"] and k == _gw_slot(secs):
+                pair = np.frombuffer(fh.read(8 * 10 * n3), dtype="<f8").reshape(5, 2, n3)
+                gu, gp = pair[:, 0].copy(), pair[:, 1].copy()
+            if k == len(secs):
+                break
+            _, fc, pc = secs[k]
             for c in fc:
                 F[c] = np.frombuffer(fh.read(8 * n3), dtype="<f8")
             for c in pc:
@@ -105,6 +144,8 @@ def load_sim(path: str, lattice, model):
         text = fh.read(ln).decode()
     sf = dict(zip(SCALARS, vals[:6]))
     lattice.set_state(F, P, sf)
+    if gws:
+        lattice.gws_set_state(gu.ravel(), gp.ravel())
     lattice.initialize(restart=True)
     return vals[6], text
 

@@ -660,13 +660,13 @@ int orc_initialize(orc_handle *h, int32_t correct_adot)
   if (isU1(h)) return oracle_models::u1_initialize(H(h)->impl, correct_adot);
   Oracle *o = S(h);
   o->setAllAverages();
-  if (o->cfg.expansion && correct_adot && !o->fb) { // modelinitializer.h:74-80
+  if (o->cfg.expansion && correct_adot == 1 && !o->fb) { // modelinitializer.h:74-80
     double hl[3];
     o->hubble(hl);
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
-  o->gwSynced = true;
+  o->gwSynced = correct_adot != CLB_INIT_RESTART; // Evolver's GWsynced(!doWeRestart), evolver.h:52
   o->t = o->cfg.t0;
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;

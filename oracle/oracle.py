@@ -96,6 +96,13 @@ class OracleLattice:
     def gws_enable(self):
         self._check(self.lib.orc_gws_enable(self.h))
 
+    def gws_set_state(self, u, pi):
+        import numpy as np
+
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        pi = np.ascontiguousarray(pi, dtype=np.float64)
+        self._check(self.lib.orc_gws_set_state(self.h, _dp(u), _dp(pi)))
+
     def gws_get_state(self):
         import numpy as np
 
@@ -135,8 +142,10 @@ class OracleLattice:
         self._check(self.lib.orc_get_state(self.h, _dp(f), _dp(p), C.byref(sf)))
         return f, p, {k: getattr(sf, k) for k, _ in self.capi.ScaleFactor._fields_}
 
-    def initialize(self, correct_adot=True):
-        self._check(self.lib.orc_initialize(self.h, 1 if correct_adot else 0))
+    def initialize(self, correct_adot=True, restart=False):
+        """orc_initialize; restart: no aDot correction and the GW leapfrog unsynced (mode 2, as
+        CLB_INIT_RESTART)."""
+        self._check(self.lib.orc_initialize(self.h, 2 if restart else (1 if correct_adot else 0)))
 
     def evolve(self, n):
         self._check(self.lib.orc_evolve(self.h, int(n)))

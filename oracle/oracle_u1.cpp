@@ -583,13 +583,13 @@ int u1_initialize(void *h, int32_t correct_adot)
   U1Oracle *o = static_cast<U1Oracle *>(h);
   o->setAllAverages();
   o->t = o->cfg.t0;
-  if (o->cfg.expansion && correct_adot && !o->fb) {
+  if (o->cfg.expansion && correct_adot == 1 && !o->fb) {
     double hl[3];
     o->hubble(hl);
     o->aDotI = std::sqrt(hl[2]);
   }
   o->synced = true;
-  o->gw.synced = true;
+  o->gw.synced = correct_adot != CLB_INIT_RESTART; // evolver.h:52
   if (o->cfg.evolver == CLB_LF && o->cfg.expansion) o->aDotSI = o->aDotI - o->cfg.dt / 2.0 * o->sfKernel();
   o->initialized = true;
   return CLB_OK;

@@ -72,3 +72,70 @@ def test_restart_with_fixed_background_is_refused(tmp_path):
         restart.load_sim(path, lat, m)
     assert ei.value.code == _capi.CLB_EUNSUPPORTED
     lat.close()
+
+
+@pytest.mark.parametrize("model", ["lphi4_1f", "lphi4U1"])
+def test_restart_carries_the_gws(tmp_path, model):
+    # saveSim/loadSim with GWs (simulationmanager.h:76-77, 112-113): the GW field and momenta come
+    # back bitwise, and after the restart the GW leapfrog starts unsynced (GWsynced(!doWeRestart),
+    # evolver.h:52); 10 more steps match the oracle restarted from the same arrays within 1e-12 of
+    # each component's maximum.  A lattice with GWs refuses a file without them.
+    from cosmolattice_b200 import Lattice, restart
+    from oracle.oracle import OracleLattice
+
+    case = make_scalar_case(N=12, amp=3e-2) if model == "lphi4_1f" else make_u1_case(N=12, amp=3e-2)
+    par, rp, m, f, p, sf = case
+    lat = Lattice(m, rp)
+    lat.gws_enable()
+    lat.set_state(f, p, sf)
+    lat.initialize()
+    lat.evolve(10)
+    lat.sync()
+    u0, p0 = lat.gws_get_state()
+    F0, P0, S0 = lat.get_state()
+    path = str(tmp_path / "gw.clb")
+    restart.save_sim(path, lat, m, 10 * rp.dt)
+    lat.close()
+
+    again = Lattice(m, rp)
+    again.gws_enable()
+    restart.load_sim(path, again, m)
+    u1, p1 = again.gws_get_state()
+    assert np.array_equal(u0, u1) and np.array_equal(p0, p1)
+    again.evolve(10)
+    again.sync()
+    ug, pg = again.gws_get_state()
+    again.close()
+
+    cpu = OracleLattice(m, rp)
+    cpu.gws_enable()
+    cpu.set_state(F0, P0, S0)
+    cpu.gws_set_state(u0, p0)
+    cpu.initialize(restart=True)
+    cpu.evolve(10)
+    cpu.sync()
+    uc, pc = cpu.gws_get_state()
+    cpu.close()
+    for a, b in ((ug, uc), (pg, pc)):
+        for c in range(5):
+            x, y = a.reshape(5, -1)[c], b.reshape(5, -1)[c]
+            assert np.abs(x - y).max() <= 1e-12 * np.abs(y).max(), c
+
+    plain = Lattice(m, rp)
+    plain.set_state(f, p, sf)
+    plain.initialize()
+    path2 = str(tmp_path / "plain.clb")
+    restart.save_sim(path2, plain, m, 0.0)
+    plain.close()
+    withgw = Lattice(m, rp)
+    withgw.gws_enable()
+    with pytest.raises(ValueError):
+        restart.load_sim(path2, withgw, m)
+    withgw.close()
+    # a run without GWs reads a file with them, as loadSim reads the GW datasets only for a model
+    # with GWs
+    nogw = Lattice(m, rp)
+    restart.load_sim(path, nogw, m)
+    Fn, Pn, _ = nogw.get_state()
+    nogw.close()
+    assert np.array_equal(Fn, F0) and np.array_equal(Pn, P0)

@@ -159,3 +159,60 @@ def test_gw_parameters():
         RunParameters(ParameterParser(params=dict(base, doLFforGWs="false")))
     with pytest.raises(RunParametersInconsistent):
         RunParameters(ParameterParser(params=dict(base, GWprojectorType=4)))
+
+
+def test_restart_file_carries_the_gws(tmp_path):
+    # with GWs the five field/momentum pairs sit right after the scalar singlets (for lphi4SU2U1,
+    # after S; simulationmanager.h:112-114) and come back bitwise; a lattice without GWs steps
+    # over them
+    import numpy as np
+
+    from conftest import make_su2_case
+    from cosmolattice_b200 import restart
+
+    par, rp, m, f, p, sf = make_su2_case(N=4)
+    sf = dict(sf, aDotSIM=0.25)
+    n3 = rp.N ** 3
+    rng = np.random.default_rng(3)
+    gu, gp = rng.standard_normal(5 * n3), rng.standard_normal(5 * n3)
+
+    class Stand:
+        def __init__(self, gws):
+            self.rp = rp
+            self.gws_on = gws
+            self.state = self.gw = None
+
+        def get_state(self):
+            return f.ravel(), p.ravel(), dict(sf)
+
+        def gws_get_state(self):
+            return gu, gp
+
+        def set_state(self, F, P, s):
+            self.state = (F.copy(), P.copy(), dict(s))
+
+        def gws_set_state(self, u, pi):
+            self.gw = (u.copy(), pi.copy())
+
+        def initialize(self, restart=False):
+            pass
+
+    path = str(tmp_path / "gw.clb")
+    restart.save_sim(path, Stand(True), m, 2.0)
+    raw = np.fromfile(path, dtype="<f8", count=(16 + 64) // 8 + 2 * n3 + 10 * n3)
+    body = raw[(16 + 64) // 8:]
+    F, P = f.reshape(22, n3), p.reshape(19, n3)
+    assert np.array_equal(body[:n3], F[0]) and np.array_equal(body[n3:2 * n3], P[0])  # S, pi_S
+    pairs = body[2 * n3:].reshape(5, 2, n3)
+    assert np.array_equal(pairs[:, 0].ravel(), gu) and np.array_equal(pairs[:, 1].ravel(), gp)
+    st = Stand(True)
+    t, _ = restart.load_sim(path, st, m)
+    assert t == 2.0 and np.array_equal(st.gw[0], gu) and np.array_equal(st.gw[1], gp)
+    assert np.array_equal(st.state[0], F) and np.array_equal(st.state[1], P)
+    plain = Stand(False)
+    restart.load_sim(path, plain, m)
+    assert plain.gw is None and np.array_equal(plain.state[0], F) and np.array_equal(plain.state[1], P)
+    path2 = str(tmp_path / "nogw.clb")
+    restart.save_sim(path2, Stand(False), m, 2.0)
+    with pytest.raises(ValueError):
+        restart.load_sim(path2, Stand(True), m)
