@@ -12,19 +12,22 @@
 // writing the measurers' files: average_energies.txt, average_energy_conservation.txt,
 // average_scale_factor.txt, the means files of every field, the Gauss-law files of the gauge
 // fields (measurementssaverstd.h:61-82, 15 significant digits) and spectra_<name>.txt
-// (spectrumsaverstd.h:54-96).  Steps between two measurements go to the GPU in one clb_evolve.
+// (spectrumsaverstd.h:54-96); with withGWs, spectra_energy_gws.txt and average_energies_gws.txt at
+// the spectra cadence (gwsmeasurer.h:41-53).  Steps between two measurements go to the GPU in one
+// clb_evolve.
 //
 // Usage: cosmolattice_b200 [input.in] [key=value ...]
 // Keys (runparameters.h:60-236 and the model headers, models.h): N, kIR or lSide, dt, tMax, t0,
 // evolver, expansion, fixedBackground, omegaEoS, H0, a0, tOutputFreq, tOutputInfreq, kCutOff,
 // outputfile, print_headers, PS_type, PS_version, deltaKBin, restart, restartFile, tBackupFreq,
-// backupPath, saveFile, and the model's keys; host keys: model (lphi4 | lphi4U1 | lphi4SU2U1),
-// precision (fp64 | fp32), path (fused | reference), deviceSeed (the Philox key; default: FNV-1a
-// of baseSeed).
+// backupPath, saveFile, withGWs, doLFforGWs, GWprojectorType, and the model's keys; host keys:
+// model (lphi4 | lphi4U1 | lphi4SU2U1), precision (fp64 | fp32), path (fused | reference),
+// deviceSeed (the Philox key; default: FNV-1a of baseSeed).
 //
 // Restart files use the layout of cosmolattice_b200/restart.py (HDF5 is not available): a magic,
-// a header, each sector's field then momentum arrays in the reference's save order, the six
-// scale-factor values and tSave, and the parameter lines.
+// a header, each sector's field then momentum arrays in the reference's save order (with GWs, their
+// five field/momentum pairs after the scalar singlets), the six scale-factor values and tSave, and
+// the parameter lines.
 
 #include "../../include/clb200.h"
 #include "models.h"
@@ -111,23 +114,41 @@ std::vector<std::array<int, 4>> sectors(const HostModel &m)
   return s;
 }
 
-void save_sim(clb_handle *h, const HostModel &m, int N, double t, const Params &par, const std::string &path)
+// Index of the first sector after the scalar singlets, where the GW arrays sit (simulationmanager.h:112-114).
+size_t gw_slot(const HostModel &m, size_t nsec)
+{
+  return m.kind == CLB_MODEL_LPHI4SU2U1 ? 1 : m.kind == CLB_MODEL_LPHI4U1 ? 0 : nsec;
+}
+
+void save_sim(clb_handle *h, const HostModel &m, int N, double t, const Params &par, const std::string &path, bool gws)
 {
   int32_t nf = 0, np = 0;
   clb_num_components(h, &nf, &np);
   const size_t n3 = (size_t)N * N * N;
-  std::vector<double> f((size_t)nf * n3), p((size_t)np * n3);
+  std::vector<double> f((size_t)nf * n3), p((size_t)np * n3), gu, gp;
   clb_scalefactor sf{};
   check(h, clb_get_state(h, f.data(), p.data(), &sf), "clb_get_state");
+  if (gws) {
+    gu.resize(5 * n3);
+    gp.resize(5 * n3);
+    check(h, clb_gws_get_state(h, gu.data(), gp.data()), "clb_gws_get_state");
+  }
   const auto secs = sectors(m);
   const std::string tmp = path + ".part";
   {
     std::ofstream o(tmp, std::ios::binary);
     if (!o) throw std::runtime_error("cannot write " + tmp);
     o.write(kMagic, 16);
-    const int64_t hdr[8] = {1, m.kind, N, nf, np, (int64_t)n3, (int64_t)secs.size(), 0};
+    const int64_t hdr[8] = {1, m.kind, N, nf, np, (int64_t)n3, (int64_t)secs.size(), gws ? 1 : 0};
     o.write(reinterpret_cast<const char *>(hdr), sizeof(hdr));
-    for (const auto &s : secs) {
+    for (size_t k = 0; k <= secs.size(); ++k) {
+      if (gws && k == gw_slot(m, secs.size()))
+        for (int c = 0; c < 5; ++c) { // each GW field component, then its momentum
+          o.write(reinterpret_cast<const char *>(gu.data() + (size_t)c * n3), (std::streamsize)(n3 * 8));
+          o.write(reinterpret_cast<const char *>(gp.data() + (size_t)c * n3), (std::streamsize)(n3 * 8));
+        }
+      if (k == secs.size()) break;
+      const auto &s = secs[k];
       o.write(reinterpret_cast<const char *>(f.data() + (size_t)s[0] * n3), (std::streamsize)(s[1] * n3 * 8));
       o.write(reinterpret_cast<const char *>(p.data() + (size_t)s[2] * n3), (std::streamsize)(s[3] * n3 * 8));
     }
@@ -143,7 +164,7 @@ void save_sim(clb_handle *h, const HostModel &m, int N, double t, const Params &
   std::filesystem::rename(tmp, path);
 }
 
-double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &path)
+double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &path, bool gws)
 {
   std::ifstream in(path, std::ios::binary);
   if (!in) throw std::runtime_error("cannot read restart file " + path);
@@ -156,13 +177,25 @@ double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &pat
   if (hdr[1] != m.kind || hdr[2] != N)
     throw std::runtime_error(path + ": saved for another model or lattice size");
   const size_t n3 = (size_t)hdr[5];
-  std::vector<double> f((size_t)hdr[3] * n3), p((size_t)hdr[4] * n3);
+  std::vector<double> f((size_t)hdr[3] * n3), p((size_t)hdr[4] * n3), gu, gp;
   const auto secs = sectors(m);
-  // header word 7, bit 0: the five GW field and momentum pairs follow the scalar singlets; this
-  // host runs no GW sector, so it steps over them (loadSim reads them only for a model with GWs)
-  const size_t gw_at = m.kind == CLB_MODEL_LPHI4SU2U1 ? 1 : m.kind == CLB_MODEL_LPHI4U1 ? 0 : secs.size();
+  // header word 7, bit 0: the five GW field and momentum pairs follow the scalar singlets; a run
+  // without GWs steps over them (loadSim reads them only for a model with GWs)
+  const bool file_gws = (hdr[7] & 1) != 0;
+  if (gws && !file_gws) throw std::runtime_error(path + ": the run has GWs, the restart file has none");
   for (size_t k = 0; k <= secs.size(); ++k) {
-    if ((hdr[7] & 1) && k == gw_at) in.seekg((std::streamoff)(10 * n3 * 8), std::ios::cur);
+    if (file_gws && k == gw_slot(m, secs.size())) {
+      if (gws) {
+        gu.resize(5 * n3);
+        gp.resize(5 * n3);
+        for (int c = 0; c < 5; ++c) {
+          in.read(reinterpret_cast<char *>(gu.data() + (size_t)c * n3), (std::streamsize)(n3 * 8));
+          in.read(reinterpret_cast<char *>(gp.data() + (size_t)c * n3), (std::streamsize)(n3 * 8));
+        }
+      } else {
+        in.seekg((std::streamoff)(10 * n3 * 8), std::ios::cur);
+      }
+    }
     if (k == secs.size()) break;
     const auto &s = secs[k];
     in.read(reinterpret_cast<char *>(f.data() + (size_t)s[0] * n3), (std::streamsize)(s[1] * n3 * 8));
@@ -173,6 +206,7 @@ double load_sim(clb_handle *h, const HostModel &m, int N, const std::string &pat
   if (!in) throw std::runtime_error(path + ": truncated");
   const clb_scalefactor sf{sc[1], sc[0], sc[2], sc[4], sc[3], sc[5]};
   check(h, clb_set_state(h, f.data(), p.data(), &sf), "clb_set_state");
+  if (gws) check(h, clb_gws_set_state(h, gu.data(), gp.data()), "clb_gws_set_state");
   check(h, clb_initialize(h, CLB_INIT_RESTART), "clb_initialize");
   return sc[6];
 }
@@ -210,6 +244,12 @@ try {
   const int psType = (int)par.num("PS_type", 1), psVersion = (int)par.num("PS_version", 1);
   const double dk = par.num("deltaKBin", 1.0);
   const int nbins = (int)std::floor(std::sqrt(3.0) / 2.0 * N / dk); // runparameters.h:98
+  // GWs (runparameters.h:120-123): the reference's default leapfrog over the matter evolver
+  const bool withGWs = par.flag("withGWs", false);
+  const int gwPrj = (int)par.num("GWprojectorType", 2);
+  if (withGWs && !par.flag("doLFforGWs", true))
+    throw std::runtime_error("the GWs run as a leapfrog over the matter evolver (doLFforGWs = true) here");
+  if (withGWs && (gwPrj < 1 || gwPrj > 3)) throw std::runtime_error("GWprojectorType is 1, 2 or 3");
 
   const HostModel m = host::make_model(par.str("model", "lphi4"), par);
 
@@ -231,10 +271,11 @@ try {
   clb_handle *h = nullptr;
   check(nullptr, clb_create(&cfg, &md, &h), "clb_create");
   std::unique_ptr<clb_handle, void (*)(clb_handle *)> guard(h, clb_destroy);
+  if (withGWs) check(h, clb_gws_enable(h), "clb_gws_enable");
 
   double t = t0;
   if (par.flag("restart", false)) {
-    t = load_sim(h, m, N, par.str("restartFile", outdir + "/" + m.name + "_backup.clb"));
+    t = load_sim(h, m, N, par.str("restartFile", outdir + "/" + m.name + "_backup.clb"), withGWs);
   } else {
     // ScaleFactorInitializer (scalefactorinitializer.h:37-65) and the fluctuations on the GPU
     double aDot = 0.0;
@@ -287,6 +328,12 @@ try {
     for (size_t c = 0; c < s.columns.size(); ++c) hdr += " " + std::to_string(c + 2) + ":PS";
     spec.push_back(open("spectra_" + s.name, hdr));
   }
+  // GWsMeasurer::measureSpectra (gwsmeasurer.h:41-53)
+  Out gwspec, gwen;
+  if (withGWs) {
+    gwspec = open("spectra_energy_gws", "1:binCentralValue 2:PS");
+    gwen = open("average_energies_gws", "#t    rhoGW_over_rho    rhoGW");
+  }
 
   // ---- the time loop (cosmolattice.cpp:168-201)
   double e0 = 0.0;
@@ -337,6 +384,18 @@ try {
         spec[s].f << '\n';
         spec[s].f.flush();
       }
+      if (withGWs) {
+        double frac = 0.0;
+        check(h, clb_gw_spectrum(h, gwPrj, psType, psVersion, dk, nbins, 1, nullptr, bins.data(), nullptr, &frac),
+              "clb_gw_spectrum");
+        for (int b = 0; b < nbins; ++b) gwspec.row({(b + 0.5) * dk * kIR, bins[b]}, " ");
+        gwspec.f << '\n';
+        gwspec.f.flush();
+        clb_measurement mm{};
+        check(h, clb_measure(h, have_e0 ? e0 : 1.0, &mm), "clb_measure");
+        const double rho = mm.energies[mm.n_energies - 1];
+        gwen.row({t, frac, frac * rho});
+      }
     }
     int64_t n = std::min(outFreq - i % outFreq, specFreq - i % specFreq);
     if (backupFreq) n = std::min(n, backupFreq - i % backupFreq);
@@ -348,10 +407,10 @@ try {
     if (backupFreq && i % backupFreq == 0) { // simulationmanager.h:143-149
       const std::string path = par.str("backupPath", outdir) + "/" + m.name + "_backup.clb";
       if (std::filesystem::exists(path)) std::filesystem::rename(path, path + "~");
-      save_sim(h, m, N, t, par, path);
+      save_sim(h, m, N, t, par, path, withGWs);
     }
   }
-  if (par.has("saveFile")) save_sim(h, m, N, t, par, par.str("saveFile", ""));
+  if (par.has("saveFile")) save_sim(h, m, N, t, par, par.str("saveFile", ""), withGWs);
   double ms = 0;
   clb_last_evolve_ms(h, &ms);
   std::printf("%s N=%d %s: t = %.6g, last evolve %.3f ms\n", m.name.c_str(), N, par.str("evolver", "LF").c_str(), t, ms);

@@ -1,5 +1,6 @@
 """The C++20 host program (cosmolattice_b200/host/cosmolattice_b200.cpp): the reference's main loop
-(source/cosmolattice.cpp:134-201) for lphi4 over the C ABI.
+(source/cosmolattice.cpp:134-201) for lphi4, lphi4U1 and lphi4SU2U1 (with or without GWs) over the
+C ABI.
 
 CPU: it is built with the library and rejects an incomplete parameter set before any CUDA call.
 GPU: its output files equal, row by row, the measurements of the same run driven from Python over
@@ -101,6 +102,8 @@ def _python_files(model_name, params, seed, outdir):
     rp = RunParameters(par)
     m = MODELS[model_name](par, rp)
     lat = Lattice(m, rp)
+    if rp.withGWs:
+        lat.gws_enable()
     p, aI, aD = device_ic_params(m, rp, seed=seed)
     lat.generate_state(p, {"aI": aI, "aSI": aI, "aIM": aI, "aDotI": aD, "aDotSI": aD})
     lat.initialize(correct_adot=True)
@@ -113,6 +116,8 @@ def _python_files(model_name, params, seed, outdir):
             meas.measure(i, t, lat)
         if i % meas.spectraFreq == 0:
             meas.measure_spectra(t, lat)
+            if rp.withGWs:
+                meas.measure_gws(t, lat)
         n = min(meas.outputFreq - i % meas.outputFreq, meas.spectraFreq - i % meas.spectraFreq)
         n = max(1, min(n, c_round((rp.tMax - t) / rp.dt)))
         lat.evolve(n)
@@ -161,6 +166,46 @@ def test_host_gauge_models_match_python(tmp_path, model):
         if "gauss" in name:
             scale[0, 1] = 1.0
         assert np.all(np.nan_to_num(np.abs(a - b)) <= 1e-13 * scale), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4SU2U1", "LF")])
+def test_host_gws_match_python(tmp_path, model, evolver):
+    # withGWs: the host's spectra_energy_gws.txt and average_energies_gws.txt (gwsmeasurer.h:41-53)
+    # equal the Python-driven run's, line by line, within 1e-13 of each column's largest value; a
+    # restart file saved with GWs carries them (restart = true needs them when withGWs is set)
+    params = dict(GAUGE[model], evolver=evolver, withGWs="true")
+    seed = 13
+    hdir, pdir = tmp_path / "host", tmp_path / "py"
+    hdir.mkdir()
+    save = tmp_path / "gw.clb"
+    args = [f"{k}={v}" for k, v in params.items()] + [f"model={model}", f"outputfile={hdir}", f"deviceSeed={seed}",
+                                                      "print_headers=true", f"saveFile={save}"]
+    r = subprocess.run([built()] + args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    _python_files(model, params, seed, str(pdir))
+    for name in ("spectra_energy_gws.txt", "average_energies_gws.txt"):
+        assert open(hdir / name).readline() == open(pdir / name).readline(), name
+        a, b = _numbers(hdir / name), _numbers(pdir / name)
+        assert a.shape == b.shape and len(a) > 2, name
+        scale = np.nanmax(np.abs(b), axis=0, keepdims=True)
+        assert np.all(np.abs(a - b) <= 1e-13 * scale), name
+    assert _numbers(hdir / "average_energies_gws.txt")[-1, 1] > 0  # the GWs grew from zero
+    hdr = np.fromfile(save, dtype="<i8", count=10)
+    assert hdr[2 + 7] & 1  # the GW flag of the header's last word
+    # a restart with GWs reads them back; without a GW flag in the file it is refused
+    plain = tmp_path / "plain.clb"
+    r = subprocess.run([built()] + [a for a in args if not a.startswith(("withGWs", "saveFile"))] +
+                       [f"saveFile={plain}"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    for path, ok in ((save, True), (plain, False)):
+        rdir = tmp_path / ("r_ok" if ok else "r_no")
+        rdir.mkdir()
+        rr = subprocess.run([built()] + [a for a in args if not a.startswith(("outputfile", "saveFile", "tMax"))] +
+                            [f"outputfile={rdir}", "restart=true", f"restartFile={path}",
+                             f"tMax={float(params['tMax']) + 5 * float(params['dt'])}"],
+                            capture_output=True, text=True, timeout=300)
+        assert (rr.returncode == 0) == ok, rr.stderr
 
 
 @pytest.mark.gpu
