@@ -384,7 +384,10 @@ template <class R, int NS> struct EvolveVV {
         }
         return;
       }
+      // With GWs, as in the fused loop below: after a step's last sweep, the GW drift (the a_SI
+      // that the fixed background leaves as it was) and the next step's GW kick (its a_I)
       const int64_t total = nsteps * (int64_t)S;
+      if (h->gw) gw_kick_step(h);
       L::kick(h, wof(0) * dt / 2);
       h->pdl_now = h->pdl;
       double tc = h->fb_t - t0;
@@ -395,6 +398,8 @@ template <class R, int NS> struct EvolveVV {
         const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
         fb_tail(h, T_FB_AIM | T_FB_AI, h->fb_a(tc + w * dt));
         L::fused(h, dt * w, w * dt / 2, more ? wn * dt / 2 : 0.0, false);
+        if (h->gw && i + 1 == S) gw_drift(h);
+        if (h->gw && i + 1 == S && more) gw_kick_step(h);
         tc += dt * w;
         if (i + 1 == S) {
           h->fb_t += dt;
@@ -585,14 +590,21 @@ template <class R, int NS> struct EvolveLF {
         }
         return;
       }
+      // GW hooks as in the self-consistent fused leapfrog below
+      if (h->gw) gw_kick_step(h);
       L::kick(h, (h->synced ? 0.5 : 1.0) * dt);
       a_drift();
       for (int64_t s = 1; s < nsteps; ++s) {
         h->fb_t += dt;
         L::fused(h, dt, dt, 0.0, false);
+        if (h->gw) {
+          gw_drift(h);
+          gw_kick_step(h);
+        }
         a_drift();
       }
       L::drift_fields(h, dt, false);
+      if (h->gw) gw_drift(h);
       h->fb_t += dt;
       h->synced = false;
       return;

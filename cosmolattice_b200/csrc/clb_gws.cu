@@ -257,9 +257,9 @@ int clb_gws_enable(clb_handle *h)
   if (!h) return CLB_EINVAL;
   if (h->gw) return CLB_OK;
   const bool gauge = h->u1 || h->su2;
-  if ((h->cfg.evolver >= CLB_PV2 && h->cfg.evolver <= CLB_PV6_2) || (!gauge && h->cfg.path != CLB_PATH_FUSED) || h->fb)
+  if ((h->cfg.evolver >= CLB_PV2 && h->cfg.evolver <= CLB_PV6_2) || (!gauge && h->cfg.path != CLB_PATH_FUSED))
     return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: GWs run with the VV evolvers and the leapfrog on the fused "
-                                     "path, with self-consistent or no expansion");
+                                     "path");
   if (h->su2 && su2_tangent_active(h))
     return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: not with the tangent-linear form running");
   auto *g = new GWSector();

@@ -557,10 +557,12 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
     auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
     if (h->cfg.evolver == CLB_LF) {
       for (int64_t s = 0; s < nsteps; ++s) {
+        if (h->gw) gw_kick_step(h); // evolver.h:102-124, as in the self-consistent leapfrog
         kick_sweep(h, 1, false, false, lf_kick(dt, h->synced ? 0.5 : 1.0));
         const double tm = h->fb_t - t0;
         tail(h, T_FB_AIM | T_FB_AI | T_FB_ASI, false, 0, 0, -1, h->fb_a(tm + dt), h->fb_a(tm + dt / 2.0));
         drift(h, 1.0);
+        if (h->gw) gw_drift(h);
         h->fb_t += dt;
         h->synced = false;
       }
@@ -580,22 +582,34 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
         h->fb_t += dt;
       }
     } else {
-      const int64_t total = nsteps * (int64_t)S;
-      kick_sweep(h, 1, false, false, vv_kick(dt, wof(0), 0.0));
-      double tc = h->fb_t - t0;
-      for (int64_t k = 0; k < total; ++k) {
-        const size_t i = (size_t)(k % (int64_t)S);
-        const double w = wof(i);
-        const bool more = k + 1 < total;
-        const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
-        tail(h, T_FB_AIM | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
-        drift(h, w);
-        kick_sweep(h, more ? 2 : 1, false, false, vv_kick(dt, w, wn));
-        tc += dt * w;
-        if (i + 1 == S) {
-          h->fb_t += dt;
-          tc = h->fb_t - t0;
+      auto vv_fb = [&](int64_t n) {
+        const int64_t total = n * (int64_t)S;
+        kick_sweep(h, 1, false, false, vv_kick(dt, wof(0), 0.0));
+        double tc = h->fb_t - t0;
+        for (int64_t k = 0; k < total; ++k) {
+          const size_t i = (size_t)(k % (int64_t)S);
+          const double w = wof(i);
+          const bool more = k + 1 < total;
+          const double wn = more ? wof((size_t)((k + 1) % (int64_t)S)) : 0.0;
+          tail(h, T_FB_AIM | T_FB_AI, false, 0, 0, -1, h->fb_a(tc + w * dt));
+          drift(h, w);
+          kick_sweep(h, more ? 2 : 1, false, false, vv_kick(dt, w, wn));
+          tc += dt * w;
+          if (i + 1 == S) {
+            h->fb_t += dt;
+            tc = h->fb_t - t0;
+          }
         }
+      };
+      if (h->gw) {
+        // one step at a time, as in the self-consistent VV with GWs
+        for (int64_t s = 0; s < nsteps; ++s) {
+          gw_kick_step(h);
+          vv_fb(1);
+          gw_drift(h);
+        }
+      } else {
+        vv_fb(nsteps);
       }
     }
   } else if (h->cfg.evolver == CLB_LF) {

@@ -20,11 +20,14 @@ from conftest import make_scalar_case
 pytestmark = pytest.mark.gpu
 
 
-def _pair(model, evolver, precision="fp64", N=24):
+FB = {"fixedBackground": "true", "H0": 2.0e18}  # a fixed radiation-like background
+
+
+def _pair(model, evolver, precision="fp64", N=24, extra=None):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, model=model, amp=3e-2)
+    par, rp, m, f, p, sf = make_scalar_case(N=N, evolver=evolver, model=model, amp=3e-2, extra=extra)
     gpu, cpu = Lattice(m, rp, precision=precision), OracleLattice(m, rp)
     for lat in (gpu, cpu):
         lat.gws_enable()
@@ -36,9 +39,11 @@ def _pair(model, evolver, precision="fp64", N=24):
     return rp, m, gpu, cpu
 
 
-@pytest.mark.parametrize("model,evolver", [("lphi4_1f", "VV2"), ("lphi4_1f", "VV4"), ("lphi4", "VV2"), ("lphi4_1f", "LF")])
-def test_gw_evolution_matches_oracle(model, evolver):
-    rp, m, gpu, cpu = _pair(model, evolver)
+@pytest.mark.parametrize("model,evolver,fb", [("lphi4_1f", "VV2", False), ("lphi4_1f", "VV4", False),
+                                             ("lphi4", "VV2", False), ("lphi4_1f", "LF", False),
+                                             ("lphi4_1f", "VV2", True), ("lphi4_1f", "LF", True)])
+def test_gw_evolution_matches_oracle(model, evolver, fb):
+    rp, m, gpu, cpu = _pair(model, evolver, extra=FB if fb else None)
     ug, pg = gpu.gws_get_state()
     uc, pc = cpu.gws_get_state()
     (fg, _, sg), (fc, _, sc) = gpu.get_state(), cpu.get_state()
@@ -182,19 +187,19 @@ def test_gauge_gws_refuse_the_adjoint_and_tangent_forms():
         lat.close()
 
 
-def _gauge_case(model, evolver, N):
+def _gauge_case(model, evolver, N, extra=None):
     from conftest import make_su2_case, make_u1_case
 
     if model == "lphi4U1":
-        return make_u1_case(N=N, evolver=evolver, amp=3e-2)
-    return make_su2_case(N=N, evolver=evolver, amp=3e-2)
+        return make_u1_case(N=N, evolver=evolver, amp=3e-2, extra=extra)
+    return make_su2_case(N=N, evolver=evolver, amp=3e-2, extra=extra)
 
 
-def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True):
+def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True, extra=None):
     from cosmolattice_b200 import Lattice
     from oracle.oracle import OracleLattice
 
-    par, rp, m, f, p, sf = _gauge_case(model, evolver, N)
+    par, rp, m, f, p, sf = _gauge_case(model, evolver, N, extra)
     gpu, cpu = Lattice(m, rp, precision=precision), OracleLattice(m, rp)
     for lat in (gpu, cpu):
         if gws:
@@ -207,13 +212,15 @@ def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True):
     return rp, m, gpu, cpu
 
 
-@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4U1", "VV4"), ("lphi4SU2U1", "VV2"),
-                                           ("lphi4U1", "LF"), ("lphi4SU2U1", "LF")])
-def test_gauge_gw_evolution_matches_oracle(model, evolver):
+@pytest.mark.parametrize("model,evolver,fb", [("lphi4U1", "VV2", False), ("lphi4U1", "VV4", False),
+                                             ("lphi4SU2U1", "VV2", False), ("lphi4U1", "LF", False),
+                                             ("lphi4SU2U1", "LF", False), ("lphi4U1", "VV2", True),
+                                             ("lphi4U1", "LF", True), ("lphi4SU2U1", "VV2", True)])
+def test_gauge_gw_evolution_matches_oracle(model, evolver, fb):
     # the complex scalar, U(1) electric and magnetic (and for lphi4SU2U1 singlet) sources of
     # PITensor.h: GW field and momenta per component within 1e-12 of the component's max after 30
-    # steps in three calls with syncs, against the oracle's restatement
-    rp, m, gpu, cpu = _gauge_pair(model, evolver)
+    # steps in three calls with syncs, against the oracle's restatement (fb: a fixed background)
+    rp, m, gpu, cpu = _gauge_pair(model, evolver, extra=FB if fb else None)
     ug, pg = gpu.gws_get_state()
     uc, pc = cpu.gws_get_state()
     sg, sc = gpu.get_state()[2], cpu.get_state()[2]
@@ -225,19 +232,20 @@ def test_gauge_gw_evolution_matches_oracle(model, evolver):
         for c in range(5):
             x, y = a.reshape(5, -1)[c], b.reshape(5, -1)[c]
             worst = max(worst, np.abs(x - y).max() / np.abs(y).max())
-    print(model, evolver, "GW rel. error", worst)
+    print(model, evolver, "fixed background" if fb else "", "GW rel. error", worst)
     assert worst <= 1e-12
     assert abs(sg["aI"] - sc["aI"]) <= 1e-12 * sc["aI"]
 
 
-@pytest.mark.parametrize("model,evolver", [("lphi4U1", "VV2"), ("lphi4SU2U1", "VV2"), ("lphi4U1", "LF")])
+@pytest.mark.parametrize("model,evolver,fb", [("lphi4U1", "VV2", False), ("lphi4SU2U1", "VV2", False),
+                                             ("lphi4U1", "LF", False), ("lphi4SU2U1", "VV2", True)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_gauge_gws_leave_the_matter_evolution_bitwise(model, evolver, precision):
+def test_gauge_gws_leave_the_matter_evolution_bitwise(model, evolver, fb, precision):
     # the GWs do not act back, and their per-step schedule is that of one-step evolve calls: the
     # matter state and the scale factor equal those of a run without GWs to the last bit
     from cosmolattice_b200 import Lattice
 
-    par, rp, m, f, p, sf = _gauge_case(model, evolver, 12)
+    par, rp, m, f, p, sf = _gauge_case(model, evolver, 12, FB if fb else None)
     out = []
     for gws in (True, False):
         lat = Lattice(m, rp, precision=precision)
