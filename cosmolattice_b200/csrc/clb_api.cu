@@ -491,7 +491,13 @@ template <class R, int NS> struct EvolvePV {
         return;
       }
       // fused: every stage after the first of the call pairs the previous stage's second drift
-      // with its own first drift; one drift sweep closes the call
+      // with its own first drift; one drift sweep closes the call.  With GWs the steps run one per
+      // call, the integer-time state between them being what the GW kick reads (evolver.h:102-124).
+      if (h->gw && nsteps > 1) {
+        for (int64_t s = 0; s < nsteps; ++s) run(h, 1);
+        return;
+      }
+      if (h->gw) gw_kick_step(h);
       const int64_t total = nsteps * (int64_t)S;
       double tc = h->fb_t - t0;
       fb_tail(h, T_PV_MODE | T_FB_PV_HALF, 0.0, h->fb_a(tc + wof(0) * dt / 2.0));
@@ -519,6 +525,7 @@ template <class R, int NS> struct EvolvePV {
         wprev = w;
       }
       L::drift_fields(h, dt / 2 * wprev, false);
+      if (h->gw) gw_drift(h);
       h->pdl_now = false;
       return;
     }
@@ -540,7 +547,11 @@ template <class R, int NS> struct EvolvePV {
     // which act with the same a and pi), kicks and reduces the half-step field averages and <pi^2>;
     // its tail books them, kicks a, finishes this stage's a-drift and starts the next one's.  Each
     // step ends with its own drift sweep, whose averages are the integer-time ones.
+    // With GWs (evolver.h:102-124): the GW kick before each step (a_I before the step's first a
+    // half-drift) and the GW drift after the step's closing drift sweep (its a_SI), both before the
+    // tail that starts the next step's a half-drift.
     const double w0 = wof(0);
+    if (h->gw) gw_kick_step(h);
     tail(h, T_PV_MODE | (ex ? T_PV_DRIFT_A1 : 0u), 0, 0, w0);
     h->pdl_now = h->pdl;
     for (int64_t s = 0; s < nsteps; ++s)
@@ -558,6 +569,10 @@ template <class R, int NS> struct EvolvePV {
         }
         if (last) {
           L::drift_fields(h, dt / 2 * w, ex);
+          if (h->gw) {
+            gw_drift(h);
+            if (s + 1 < nsteps) gw_kick_step(h);
+          }
           if (ex) tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), h->sweep_blocks, 0, w0, s);
         }
       }

@@ -32,6 +32,7 @@
 #include "clb_scalar.cuh"
 #include "clb_spectrum.cuh"
 #include "clb_sweep.cuh"
+#include "clb_vv.h"
 
 #include <cmath>
 #include <string>
@@ -216,14 +217,15 @@ __attribute__((visibility("hidden"))) void gw_drift(clb_handle *h)
   if (h->su2) return su2_gw_drift(h);
   GWSector *g = h->gw;
   const size_t n = 5 * h->n3;
+  const bool pv = is_pv(h->cfg.evolver);
   if (h->fp32)
-    CLB_LAUNCH(h, K_GW, k_gw_drift<float><<<kGWBlocks, 256, 0, h->stream>>>(static_cast<float *>(g->u),
-                                                                           static_cast<const float *>(g->pi), n,
-                                                                           h->cfg.dt, &h->d_st->drift_p));
+    CLB_LAUNCH(h, K_GW, launch_gw_drift<float>(static_cast<float *>(g->u), static_cast<const float *>(g->pi), n,
+                                               h->cfg.dt, &h->d_st->drift_p, &h->d_st->aSI, h->md.alpha, pv,
+                                               h->stream));
   else
-    CLB_LAUNCH(h, K_GW, k_gw_drift<double><<<kGWBlocks, 256, 0, h->stream>>>(static_cast<double *>(g->u),
-                                                                             static_cast<const double *>(g->pi), n,
-                                                                             h->cfg.dt, &h->d_st->drift_p));
+    CLB_LAUNCH(h, K_GW, launch_gw_drift<double>(static_cast<double *>(g->u), static_cast<const double *>(g->pi), n,
+                                                h->cfg.dt, &h->d_st->drift_p, &h->d_st->aSI, h->md.alpha, pv,
+                                                h->stream));
 }
 
 // The GW kick before a matter step (evolver.h:104-107): half a step after a sync, else a whole one.
@@ -257,9 +259,8 @@ int clb_gws_enable(clb_handle *h)
   if (!h) return CLB_EINVAL;
   if (h->gw) return CLB_OK;
   const bool gauge = h->u1 || h->su2;
-  if ((h->cfg.evolver >= CLB_PV2 && h->cfg.evolver <= CLB_PV6_2) || (!gauge && h->cfg.path != CLB_PATH_FUSED))
-    return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: GWs run with the VV evolvers and the leapfrog on the fused "
-                                     "path");
+  if (!gauge && h->cfg.path != CLB_PATH_FUSED)
+    return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: the scalar singlets' GWs run on the fused path");
   if (h->su2 && su2_tangent_active(h))
     return h->fail(CLB_EUNSUPPORTED, "clb_gws_enable: not with the tangent-linear form running");
   auto *g = new GWSector();

@@ -74,6 +74,29 @@ __global__ void __launch_bounds__(256) k_gw_drift(R *__restrict__ u, const R *__
     u[i] = drift_val<R>(u[i], piu[i], pd, dt);
 }
 
+// The same drift with the coefficient formed here from a_SI (aSI points at the device copy; the
+// position-Verlet tails keep a_SI as the reference does, positionverlet.h:213-235, but their drift
+// coefficient is a_I's).
+template <class R>
+__global__ void __launch_bounds__(256) k_gw_drift_a(R *__restrict__ u, const R *__restrict__ piu, size_t n, double dtd,
+                                                    const double *__restrict__ aSI, double alpha)
+{
+  const R pd = (R)apow(*aSI, alpha - 3), dt = (R)dtd;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    u[i] = drift_val<R>(u[i], piu[i], pd, dt);
+}
+
+// Launches the GW drift: with the tails' coefficient pd (VV, leapfrog), or from a_SI (position Verlet).
+template <class R>
+inline void launch_gw_drift(R *u, const R *piu, size_t n, double dt, const double *pd, const double *aSI, double alpha,
+                            bool from_aSI, cudaStream_t stream)
+{
+  if (from_aSI)
+    k_gw_drift_a<R><<<kGWBlocks, 256, 0, stream>>>(u, piu, n, dt, aSI, alpha);
+  else
+    k_gw_drift<R><<<kGWBlocks, 256, 0, stream>>>(u, piu, n, dt, pd);
+}
+
 // The gauge part of the anisotropic tensor (PITensor.h:58-111) at site s, added to P in the
 // reference's order: P_ij += 2 Re[D_i phi conj(D_j phi)] (complex scalar), then the U(1) electric
 // and magnetic terms -1/a^2/(fStar/omegaStar)^2 pi_A,i pi_A,j and ... B_i B_j.  phi (fr, fi at the

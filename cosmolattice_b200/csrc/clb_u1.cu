@@ -372,18 +372,22 @@ __attribute__((visibility("hidden"))) void u1_gw_kick(clb_handle *h, double w)
   else go(0.0);
 }
 
-// The GW drift with the a_SI of the matter step just taken (U1State::cs_drift = pow(a_SI, alpha - 3)).
+// The GW drift with the a_SI of the matter step just taken (U1State::cs_drift = pow(a_SI, alpha - 3)
+// on the VV and the leapfrog).
 __attribute__((visibility("hidden"))) void u1_gw_drift(clb_handle *h)
 {
   U1Sector *u = h->u1;
   GWSector *g = h->gw;
   const size_t n = 5 * h->n3;
+  const bool pv = is_pv(h->cfg.evolver); // cs_drift is then a_I's: the drift forms a_SI's
   if (u->fp32)
-    CLB_LAUNCH(h, K_GW, k_gw_drift<float><<<kGWBlocks, 256, 0, h->stream>>>(
-                            static_cast<float *>(g->u), static_cast<const float *>(g->pi), n, h->cfg.dt, &u->d_st->cs_drift));
+    CLB_LAUNCH(h, K_GW, launch_gw_drift<float>(static_cast<float *>(g->u), static_cast<const float *>(g->pi), n,
+                                               h->cfg.dt, &u->d_st->cs_drift, &u->d_st->aSI, h->md.alpha, pv,
+                                               h->stream));
   else
-    CLB_LAUNCH(h, K_GW, k_gw_drift<double><<<kGWBlocks, 256, 0, h->stream>>>(
-                            static_cast<double *>(g->u), static_cast<const double *>(g->pi), n, h->cfg.dt, &u->d_st->cs_drift));
+    CLB_LAUNCH(h, K_GW, launch_gw_drift<double>(static_cast<double *>(g->u), static_cast<const double *>(g->pi), n,
+                                                h->cfg.dt, &u->d_st->cs_drift, &u->d_st->aSI, h->md.alpha, pv,
+                                                h->stream));
 }
 
 __attribute__((visibility("hidden"))) int u1_create(clb_handle *h)
@@ -569,6 +573,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
     } else if (is_pv(h->cfg.evolver)) {
       tail(h, T_PV_MODE, false);
       for (int64_t s = 0; s < nsteps; ++s) {
+        if (h->gw) gw_kick_step(h); // evolver.h:102-124
         double tc = h->fb_t - t0;
         for (size_t i = 0; i < S; ++i) {
           const double w = wof(i);
@@ -579,6 +584,7 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
           drift(h, w, dt / 2);
           tc += dt * w;
         }
+        if (h->gw) gw_drift(h);
         h->fb_t += dt;
       }
     } else {
@@ -644,7 +650,11 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
     const std::vector<double> &ws = h->ws;
     const size_t P = ws.size(), S = 2 * P - 1;
     auto wof = [&](size_t i) { return ws[i < P ? i : S - i - 1]; };
+    // With GWs (evolver.h:102-124): the GW kick before each step (a_I before the step's first a
+    // half-drift) and the GW drift after its last field drift (its a_SI), both before the tail that
+    // starts the next step's a half-drift.
     const double w0 = wof(0);
+    if (h->gw) gw_kick_step(h);
     tail(h, T_PV_MODE | (ex ? T_PV_DRIFT_A1 : 0u), false, 0, w0);
     for (int64_t s = 0; s < nsteps; ++s)
       for (size_t i = 0; i < S; ++i) {
@@ -656,6 +666,10 @@ __attribute__((visibility("hidden"))) int u1_evolve(clb_handle *h, int64_t nstep
           tail(h, T_PV_MODE | T_PV_STORE_SI | T_PV_STORE_PI2 | T_PV_KICK | T_PV_DRIFT_A2 | (last ? 0u : T_PV_DRIFT_A1),
                true, w, last ? 0.0 : wof(i + 1));
         drift(h, w, dt / 2);
+        if (last && h->gw) {
+          gw_drift(h);
+          if (s + 1 < nsteps) gw_kick_step(h);
+        }
         if (last && ex) {
           kick_sweep(h, 0, true, false, U1Kick{});
           tail(h, T_PV_MODE | T_STORE_FIELDS | (s + 1 < nsteps ? T_PV_DRIFT_A1 : 0u), true, 0, w0, s);

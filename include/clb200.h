@@ -400,8 +400,8 @@ int clb_batch_get_form(clb_batch *b, clb_batch_form *out);
  * doLFforGWs, a leapfrog staggered over the matter evolver, evolvers/evolver.h:102-138;
  * GWsInitializer, zero at the start).  The field is the traceless symmetric u_ij as five
  * components (u_11, u_12, u_13, u_22, u_23; u_33 = -u_11 - u_22), its momenta likewise.
- * clb_gws_enable: after clb_create, before clb_initialize; every model with the VV evolvers or the
- * leapfrog (the scalar singlets on the fused path), with any expansion (else CLB_EUNSUPPORTED).
+ * clb_gws_enable: after clb_create, before clb_initialize; every model, evolver and expansion (the
+ * scalar singlets on the fused path; else CLB_EUNSUPPORTED).
  * A gauge handle with GWs takes no clb_forward and no clb_tangent_begin (CLB_EUNSUPPORTED), and
  * the reverse.
  * clb_gws_set_state / clb_gws_get_state: 5 x N^3 doubles each (either may be NULL).

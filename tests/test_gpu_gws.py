@@ -41,7 +41,9 @@ def _pair(model, evolver, precision="fp64", N=24, extra=None):
 
 @pytest.mark.parametrize("model,evolver,fb", [("lphi4_1f", "VV2", False), ("lphi4_1f", "VV4", False),
                                              ("lphi4", "VV2", False), ("lphi4_1f", "LF", False),
-                                             ("lphi4_1f", "VV2", True), ("lphi4_1f", "LF", True)])
+                                             ("lphi4_1f", "PV2", False), ("lphi4_1f", "PV4", False),
+                                             ("lphi4_1f", "VV2", True), ("lphi4_1f", "LF", True),
+                                             ("lphi4_1f", "PV2", True)])
 def test_gw_evolution_matches_oracle(model, evolver, fb):
     rp, m, gpu, cpu = _pair(model, evolver, extra=FB if fb else None)
     ug, pg = gpu.gws_get_state()
@@ -137,19 +139,12 @@ def test_fp32_gws_track_fp64():
     assert abs(f32 - f64) <= 1e-4 * f64
 
 
-def test_gws_reject_other_evolvers_and_models():
+def test_gws_refuse_the_scalar_reference_path():
+    # the scalar singlets' GWs ride the fused path's loops; the reference-order path has none
     from cosmolattice_b200 import Lattice, _capi
-    from conftest import make_u1_case
 
-    for ev in ("PV2",):
-        par, rp, m, f, p, sf = make_scalar_case(N=8, evolver=ev)
-        lat = Lattice(m, rp)
-        with pytest.raises(_capi.ClbError) as ei:
-            lat.gws_enable()
-        assert ei.value.code == _capi.CLB_EUNSUPPORTED
-        lat.close()
-    par, rp, m, f, p, sf = make_u1_case(N=8, evolver="PV2")
-    lat = Lattice(m, rp)
+    par, rp, m, f, p, sf = make_scalar_case(N=8)
+    lat = Lattice(m, rp, path="reference")
     with pytest.raises(_capi.ClbError) as ei:
         lat.gws_enable()
     assert ei.value.code == _capi.CLB_EUNSUPPORTED
@@ -214,8 +209,10 @@ def _gauge_pair(model, evolver, precision="fp64", N=12, gws=True, extra=None):
 
 @pytest.mark.parametrize("model,evolver,fb", [("lphi4U1", "VV2", False), ("lphi4U1", "VV4", False),
                                              ("lphi4SU2U1", "VV2", False), ("lphi4U1", "LF", False),
-                                             ("lphi4SU2U1", "LF", False), ("lphi4U1", "VV2", True),
-                                             ("lphi4U1", "LF", True), ("lphi4SU2U1", "VV2", True)])
+                                             ("lphi4SU2U1", "LF", False), ("lphi4U1", "PV2", False),
+                                             ("lphi4SU2U1", "PV4", False), ("lphi4U1", "VV2", True),
+                                             ("lphi4U1", "LF", True), ("lphi4SU2U1", "VV2", True),
+                                             ("lphi4U1", "PV2", True), ("lphi4SU2U1", "PV2", True)])
 def test_gauge_gw_evolution_matches_oracle(model, evolver, fb):
     # the complex scalar, U(1) electric and magnetic (and for lphi4SU2U1 singlet) sources of
     # PITensor.h: GW field and momenta per component within 1e-12 of the component's max after 30
