@@ -34,10 +34,11 @@ struct SU2Sector {
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   void *ph = nullptr;        // U(1) link phases (12 x N^3, storage type), kept by the drifts
   // kick sweeps: 0 one sweep, 1 two halves, 2 three parts (CLB_SU2_SPLIT overrides).  su2_create
-  // takes three parts for FP64 and halves for FP32, by timing at 192^3 VV2 (ms per step): FP64
-  // 8.14 whole, 5.74 halves, 4.93 three parts; FP32 3.98, 2.97, 3.06.  Every form gives the same
-  // state to the last bit.  The tangent-linear sweep takes three parts in both (128^3 VV2, ms per
-  // step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
+  // takes three parts in both precisions, by timing at 384^3 VV2 since the kick forms the field
+  // averages from its own products (ms per step): FP64 83.0 whole, 58.3 halves, 45.5 three parts;
+  // FP32 44.0, 26.9, 23.4 (at 192^3: FP64 9.20, 6.53, 5.16; FP32 4.93, 3.18, 2.90).  Every form
+  // gives the same state to the last bit.  The tangent-linear sweep takes three parts in both
+  // (128^3 VV2, ms per step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
   int split = 2;
   int tan_split = 2;
   int64_t steps_since_unitarize = 0;
@@ -351,7 +352,7 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   u->prm = su2_params(h);
   u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
   u->esz = u->fp32 ? sizeof(float) : sizeof(double);
-  u->split = u->fp32 ? 1 : 2;
+  u->split = 2;
   if (const char *env = std::getenv("CLB_SU2_SPLIT")) u->split = u->tan_split = std::max(0, std::min(2, std::atoi(env)));
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;
