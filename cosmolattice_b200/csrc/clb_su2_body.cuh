@@ -768,8 +768,17 @@ template <int G0 = 0, int G1 = 5, class R> __device__ __forceinline__ void pi2s_
 // Tangent kick sweep: k_kick on (p, dp) with kernels and field sums in Tan<S>; partials
 // [block][2 kRed]: the kRed sums of k_kick, then their tangents.
 // SECT as k_kick: 0 whole; 1 and 2 the halves, or 3, 4 and 2 the three parts, of a split sweep.
+// Resident blocks per SM of the tangent kick parts: three in FP64, four in FP32, timed at 256^3 VV2
+// (ms per tangent step, 1 / 2 / 3 / 4 blocks): FP64 39.2, 39.3, 37.9, 39.3; FP32 23.2, 23.3, 21.9,
+// 21.4.  The value part stays the plain evolution's bitwise either way.
+#ifndef CLB_SU2_TAN_MINB_F64
+#define CLB_SU2_TAN_MINB_F64 3
+#endif
+#ifndef CLB_SU2_TAN_MINB_F32
+#define CLB_SU2_TAN_MINB_F32 4
+#endif
 template <class S, int NK, bool RF, bool RP, int SECT = 0>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_TAN_MINB_F32 : CLB_SU2_TAN_MINB_F64)
     k_kick_tan(const S *__restrict__ f, const S *__restrict__ df, S *__restrict__ p, S *__restrict__ dp, Params a,
                Kick kc, const TState *__restrict__ stp, CoupDot cd, double *__restrict__ partials)
 {
