@@ -33,12 +33,13 @@ struct SU2Sector {
   double *d_part = nullptr, *d_sums = nullptr;
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   void *ph = nullptr;        // U(1) link phases (12 x N^3, storage type), kept by the drifts
-  // kick sweeps: 0 one sweep, 1 two halves, 2 three parts (CLB_SU2_SPLIT overrides).  su2_create
-  // takes three parts in both precisions, by timing at 384^3 VV2 since the kick forms the field
-  // averages from its own products (ms per step): FP64 83.0 whole, 58.3 halves, 45.5 three parts;
-  // FP32 44.0, 26.9, 23.4 (at 192^3: FP64 9.20, 6.53, 5.16; FP32 4.93, 3.18, 2.90).  Every form
-  // gives the same state to the last bit.  The tangent-linear sweep takes three parts in both
-  // (128^3 VV2, ms per step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
+  // kick sweeps: 0 one sweep, 1 two halves, 2 three parts, 3 four parts (S and phi; Phi; A; SU(2);
+  // the tangent sweep takes three then) (CLB_SU2_SPLIT overrides).  su2_create takes four parts in
+  // FP64 and three in FP32, by timing at 384^3 VV2 since the kick forms the field averages from its
+  // own products (ms per step): FP64 83.0 whole, 58.3 halves, 45.2 three parts, 40.9 four parts;
+  // FP32 44.0, 26.9, 23.3, 23.3 (at 192^3: FP64 9.20, 6.53, 5.10, 4.73; FP32 4.93, 3.18, 2.90,
+  // 2.93).  Every form gives the same state to the last bit.  The tangent-linear sweep takes three
+  // parts in both (128^3 VV2, ms per step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
   int split = 2;
   int tan_split = 2;
   int64_t steps_since_unitarize = 0;
@@ -154,7 +155,12 @@ template <class S> void sweep_t(clb_handle *h, int nk, bool rf, bool rp, const K
                           f, p, u->prm, kc, u->d_st, u->d_part, static_cast<const S *>(u->ph)))
 #define CLB_SU2K(NK, RF, RP)                                                                                            \
   do {                                                                                                                 \
-    if (NK > 0 && u->split == 2) {                                                                                     \
+    if (NK > 0 && u->split == 3) {                                                                                     \
+      CLB_SU2K1(NK, RF, RP, 5);                                                                                        \
+      CLB_SU2K1(NK, RF, RP, 6);                                                                                        \
+      CLB_SU2K1(NK, RF, RP, 4);                                                                                        \
+      CLB_SU2K1(NK, RF, RP, 2);                                                                                        \
+    } else if (NK > 0 && u->split == 2) {                                                                              \
       CLB_SU2K1(NK, RF, RP, 3);                                                                                        \
       CLB_SU2K1(NK, RF, RP, 4);                                                                                        \
       CLB_SU2K1(NK, RF, RP, 2);                                                                                        \
@@ -352,8 +358,11 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   u->prm = su2_params(h);
   u->fp32 = h->cfg.precision == CLB_PREC_FP32_SPLIT;
   u->esz = u->fp32 ? sizeof(float) : sizeof(double);
-  u->split = 2;
-  if (const char *env = std::getenv("CLB_SU2_SPLIT")) u->split = u->tan_split = std::max(0, std::min(2, std::atoi(env)));
+  u->split = u->fp32 ? 2 : 3;
+  if (const char *env = std::getenv("CLB_SU2_SPLIT")) {
+    u->split = std::max(0, std::min(3, std::atoi(env)));
+    u->tan_split = std::min(2, u->split);
+  }
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;
   ok = ok && cudaMalloc(&u->p, NP * h->n3 * u->esz) == cudaSuccess;

@@ -281,11 +281,27 @@ template <class T> struct Coef {
 };
 
 // SECT: 0 all components; 1 S, phi, Phi and A (K[0..9]); 2 the SU(2) field (K[10..18]);
-// 3 S, phi and Phi (K[0..6]); 4 A (K[7..9]).  Each component's kernel is the same expression in
-// every SECT that holds it.
-__host__ __device__ constexpr bool sect_scalars(int sect) { return sect == 0 || sect == 1 || sect == 3; }
+// 3 S, phi and Phi (K[0..6]); 4 A (K[7..9]); 5 S and phi (K[0..2]); 6 Phi (K[3..6]).  Each
+// component's kernel is the same expression in every SECT that holds it.
+__host__ __device__ constexpr bool sect_sphi(int sect) { return sect == 0 || sect == 1 || sect == 3 || sect == 5; }
+__host__ __device__ constexpr bool sect_dbl(int sect) { return sect == 0 || sect == 1 || sect == 3 || sect == 6; }
+__host__ __device__ constexpr bool sect_scalars(int sect) { return sect_sphi(sect) || sect_dbl(sect); }
 __host__ __device__ constexpr bool sect_u1(int sect) { return sect == 0 || sect == 1 || sect == 4; }
 __host__ __device__ constexpr bool sect_su2(int sect) { return sect == 0 || sect == 2; }
+// momentum sectors [sect_g0, sect_g1) of SECT (0 S, 1 phi, 2 Phi, 3 A, 4 SU(2))
+__host__ __device__ constexpr int sect_g0(int sect) { return sect == 2 ? 4 : sect == 4 ? 3 : sect == 6 ? 2 : 0; }
+__host__ __device__ constexpr int sect_g1(int sect)
+{
+  return sect == 1 || sect == 4 ? 4 : sect == 3 || sect == 6 ? 3 : sect == 5 ? 2 : 5;
+}
+// whether SECT writes partial slot k of a kick sweep: the momentum sums of its sectors (k < 5 and
+// k >= 11), the gradient sums of S, phi (5, 6) and Phi (7), B^2 of A (8) and SU(2) (9), V (10,
+// with S and phi)
+__host__ __device__ constexpr bool sect_owns(int sect, int k)
+{
+  return k < 5 || k >= 11 ? ((k < 5 ? k : k - 11) >= sect_g0(sect) && (k < 5 ? k : k - 11) < sect_g1(sect))
+         : k == 7 ? sect_dbl(sect) : k == 8 ? sect_u1(sect) : k == 9 ? sect_su2(sect) : sect_sphi(sect);
+}
 
 // Per-site terms of the volume averages a kick sweep reduces with RF (fieldfunctionals.h):
 // gradient energies of S, phi and Phi, B^2 of A and of SU(2), and V.  They equal, to the last
@@ -308,16 +324,20 @@ __device__ __forceinline__ void kernels(const Site<S, T> &v, const Coef<T> &C, T
   const T qG = v.qG, qH = v.qH, c4 = v.c4, rfo2 = (T)a.rfo2;
   if constexpr (sect_scalars(SECT)) {
     const T nD = v.normD(s), nC = v.normC(s), Sv = v.F(0, s);
-    K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
-    const C2<T> cl = covLapC(v, AVG ? &av->g2C : nullptr);
-    const T ndC = 4 * qH * ipw(nD, 2) * nC;
-    K[1] = A * cl.re - B2 * (kdiv(ndC, nC) * v.F(1, s));
-    K[2] = A * cl.im - B2 * (kdiv(ndC, nC) * v.F(2, s));
-    T dl[4];
-    covLapD(v, dl, AVG ? &av->g2D : nullptr);
-    const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
-    for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (kdiv(ndD, nD) * v.F(3 + c, s));
-    if constexpr (AVG) {
+    if constexpr (sect_sphi(SECT)) {
+      K[0] = A * v.lapl(0) - B * (2 * qG * ipw(nD, 2) * Sv);
+      const C2<T> cl = covLapC(v, AVG ? &av->g2C : nullptr);
+      const T ndC = 4 * qH * ipw(nD, 2) * nC;
+      K[1] = A * cl.re - B2 * (kdiv(ndC, nC) * v.F(1, s));
+      K[2] = A * cl.im - B2 * (kdiv(ndC, nC) * v.F(2, s));
+    }
+    if constexpr (sect_dbl(SECT)) {
+      T dl[4];
+      covLapD(v, dl, AVG ? &av->g2D : nullptr);
+      const T ndD = c4 * (4 * ipw(nD, 3)) + nD * (2 * qG * ipw(Sv, 2) + 4 * qH * ipw(nC, 2));
+      for (int c = 0; c < 4; ++c) K[3 + c] = A * dl[c] - B2 * (kdiv(ndD, nD) * v.F(3 + c, s));
+    }
+    if constexpr (AVG && sect_sphi(SECT)) {
       av->g2S = sGrad2(v);
       av->pot = v.pot_at(nD, nC, Sv);
     }
@@ -424,12 +444,12 @@ template <class S, class T> __device__ __forceinline__ T gB2(const Site<S, T> &v
 template <int SECT, class S, class T> __device__ __forceinline__ SiteAvg<T> site_avg(const Site<S, T> &v)
 {
   SiteAvg<T> av{};
-  if constexpr (sect_scalars(SECT)) {
+  if constexpr (sect_sphi(SECT)) {
     av.g2S = sGrad2(v);
     av.g2C = cGrad2(v);
-    av.g2D = dGrad2(v);
     av.pot = v.pot();
   }
+  if constexpr (sect_dbl(SECT)) av.g2D = dGrad2(v);
   if constexpr (sect_u1(SECT)) av.b2A = aB2(v);
   if constexpr (sect_su2(SECT)) av.b2G = gB2(v);
   return av;
@@ -507,8 +527,7 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
            double *__restrict__ partials, const S *__restrict__ ph)
 {
-  constexpr int G0 = SECT == 2 ? 4 : SECT == 4 ? 3 : 0;                   // sectors [G0, G1)
-  constexpr int G1 = SECT == 1 || SECT == 4 ? 4 : SECT == 3 ? 3 : 5;
+  constexpr int G0 = sect_g0(SECT), G1 = sect_g1(SECT);                   // sectors [G0, G1)
   constexpr int C0 = sector_c0(G0), C1 = sector_c0(G1);                    // momentum components [C0, C1)
   __shared__ double smem[(128 / 32) * kRed];
   const State st = *stp;
@@ -539,25 +558,21 @@ __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_K
     }
     if (RF && NK == 0) av = site_avg<SECT>(v);
     if (RF) {
-      if (sect_scalars(SECT)) {
+      if (sect_sphi(SECT)) {
         acc[5] += (double)av.g2S;
         acc[6] += (double)av.g2C;
-        acc[7] += (double)av.g2D;
       }
+      if (sect_dbl(SECT)) acc[7] += (double)av.g2D;
       if (sect_u1(SECT)) acc[8] += (double)av.b2A;
       if (sect_su2(SECT)) acc[9] += (double)av.b2G;
-      if (sect_scalars(SECT)) acc[10] += (double)av.pot;
+      if (sect_sphi(SECT)) acc[10] += (double)av.pot;
     }
   });
   if (RF || RP) {
     block_reduce<kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
-      for (int k = 0; k < kRed; ++k) {
-        const int g = k < 5 ? k : k >= 11 ? k - 11 : -1; // momentum slot of sector g
-        const bool mine = g >= 0 ? (g >= G0 && g < G1)
-                                 : (k == 8 ? sect_u1(SECT) : k == 9 ? sect_su2(SECT) : sect_scalars(SECT));
-        if (mine) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
-      }
+      for (int k = 0; k < kRed; ++k)
+        if (sect_owns(SECT, k)) partials[(size_t)blockIdx.x * kRed + k] = acc[k];
   }
 }
 
@@ -783,8 +798,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_TAN_MINB_F32 : C
                Kick kc, const TState *__restrict__ stp, CoupDot cd, double *__restrict__ partials)
 {
   using T = Tan<S>;
-  constexpr int G0 = SECT == 2 ? 4 : SECT == 4 ? 3 : 0;                   // sectors [G0, G1)
-  constexpr int G1 = SECT == 1 || SECT == 4 ? 4 : SECT == 3 ? 3 : 5;
+  constexpr int G0 = sect_g0(SECT), G1 = sect_g1(SECT);                   // sectors [G0, G1)
   constexpr int C0 = sector_c0(G0), C1 = sector_c0(G1);                    // momentum components [C0, C1)
   __shared__ double smem[(128 / 32) * 2 * kRed];
   const Coef<T> C{T(stp->kA), T(stp->kB), T(stp->kB2), T(stp->kG)};
@@ -831,26 +845,21 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? CLB_SU2_TAN_MINB_F32 : C
         acc[5 + k] += (double)r.v;
         acc[kRed + 5 + k] += (double)r.d;
       };
-      if (sect_scalars(SECT)) {
+      if (sect_sphi(SECT)) {
         addf(0, av.g2S);
         addf(1, av.g2C);
-        addf(2, av.g2D);
       }
+      if (sect_dbl(SECT)) addf(2, av.g2D);
       if (sect_u1(SECT)) addf(3, av.b2A);
       if (sect_su2(SECT)) addf(4, av.b2G);
-      if (sect_scalars(SECT)) addf(5, av.pot);
+      if (sect_sphi(SECT)) addf(5, av.pot);
     }
   });
   if (RF || RP) {
     block_reduce<2 * kRed, 128>(acc, smem);
     if (threadIdx.x == 0)
-      for (int k = 0; k < 2 * kRed; ++k) {
-        const int j = k % kRed;                          // value and tangent slots alike
-        const int g = j < 5 ? j : j >= 11 ? j - 11 : -1; // momentum slot of sector g
-        const bool mine = g >= 0 ? (g >= G0 && g < G1)
-                                 : (j == 8 ? sect_u1(SECT) : j == 9 ? sect_su2(SECT) : sect_scalars(SECT));
-        if (mine) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
-      }
+      for (int k = 0; k < 2 * kRed; ++k) // value and tangent slots alike
+        if (sect_owns(SECT, k % kRed)) partials[(size_t)blockIdx.x * 2 * kRed + k] = acc[k];
   }
 }
 

@@ -259,14 +259,15 @@ def test_lphi4su2u1_fixed_background_rejects_the_tangent_form():
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_kick_split_is_bitwise_the_whole_sweep(monkeypatch, evolver, precision):
     # CLB_SU2_SPLIT: 0 one kick sweep, 1 two halves (S, phi, Phi, A; SU(2)), 2 three parts (S, phi,
-    # Phi; A; SU(2)).  Each component's kernel and each partial slot's sum run the same arithmetic
-    # over the same sites in every form, so states, a(t) and energies agree to the last bit.
+    # Phi; A; SU(2)), 3 four parts (S, phi; Phi; A; SU(2)).  Each component's kernel and each partial
+    # slot's sum run the same arithmetic over the same sites in every form, so states, a(t) and
+    # energies agree to the last bit.
     from cosmolattice_b200 import Lattice
 
     par, rp, m, f, p, sf = make_su2_case(N=12, evolver=evolver, expansion=True, amp=3e-2)
     f = random_links(f, np.random.default_rng(8), 0.05)
     res = {}
-    for split in ("0", "1", "2"):
+    for split in ("0", "1", "2", "3"):
         monkeypatch.setenv("CLB_SU2_SPLIT", split)
         lat = Lattice(m, rp, precision=precision)
         lat.set_state(f, p, sf)
@@ -277,7 +278,7 @@ def test_kick_split_is_bitwise_the_whole_sweep(monkeypatch, evolver, precision):
         res[split] = (lat.get_state(), lat.measure(1.0))
         lat.close()
     (f0, p0, s0), m0 = res["0"]
-    for split in ("1", "2"):
+    for split in ("1", "2", "3"):
         (fs, ps, ss), ms = res[split]
         assert np.array_equal(fs, f0) and np.array_equal(ps, p0), split
         assert ss == s0, split
