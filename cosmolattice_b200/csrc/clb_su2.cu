@@ -33,15 +33,15 @@ struct SU2Sector {
   double *d_part = nullptr, *d_sums = nullptr;
   double *d_stage = nullptr; // one FP64 component, for FP32 conversions
   void *ph = nullptr;        // U(1) link phases (12 x N^3, storage type), kept by the drifts
-  // kick sweeps: 0 one sweep, 1 two halves, 2 three parts, 3 four parts (S and phi; Phi; A; SU(2);
-  // the tangent sweep takes three then) (CLB_SU2_SPLIT overrides).  su2_create takes four parts in
-  // FP64 and three in FP32, by timing at 384^3 VV2 since the kick forms the field averages from its
-  // own products (ms per step): FP64 83.0 whole, 58.3 halves, 45.2 three parts, 40.9 four parts;
-  // FP32 44.0, 26.9, 23.3, 23.3 (at 192^3: FP64 9.20, 6.53, 5.10, 4.73; FP32 4.93, 3.18, 2.90,
-  // 2.93).  Every form gives the same state to the last bit.  The tangent-linear sweep takes three
-  // parts in both (128^3 VV2, ms per step: FP64 4.71 halves, 4.12 three parts; FP32 2.74, 2.54).
+  // kick sweeps: 0 one sweep, 1 two halves, 2 three parts, 3 four parts (S and phi; Phi; A; SU(2))
+  // (CLB_SU2_SPLIT sets both forms).  su2_create takes four parts in FP64 and three in FP32, by
+  // timing at 384^3 VV2 since the kick forms the field averages from its own products (ms per
+  // step): FP64 83.0 whole, 58.3 halves, 45.2 three parts, 40.9 four parts; FP32 44.0, 26.9, 23.3,
+  // 23.3 (at 192^3: FP64 9.20, 6.53, 5.10, 4.73; FP32 4.93, 3.18, 2.90, 2.93).  The tangent-linear
+  // sweep takes four parts in both (256^3 VV2, ms per tangent step, three / four parts: FP64 37.9,
+  // 31.4; FP32 21.5, 19.5).  Every form gives the same state to the last bit.
   int split = 2;
-  int tan_split = 2;
+  int tan_split = 3;
   int64_t steps_since_unitarize = 0;
   Params prm{};
   // tangent-linear form: d(state) along the coupling direction tan_cd, active while tangent
@@ -207,7 +207,12 @@ template <class S> void sweep_tan_t(clb_handle *h, int nk, bool rf, bool rp, con
                                                                                   u->tan_cd, u->d_tpart))
 #define CLB_SU2T(NK, RF, RP)                                                                                            \
   do {                                                                                                                 \
-    if (NK > 0 && u->tan_split == 2) {                                                                                 \
+    if (NK > 0 && u->tan_split == 3) {                                                                                 \
+      CLB_SU2T1(NK, RF, RP, 5);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 6);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 4);                                                                                        \
+      CLB_SU2T1(NK, RF, RP, 2);                                                                                        \
+    } else if (NK > 0 && u->tan_split == 2) {                                                                          \
       CLB_SU2T1(NK, RF, RP, 3);                                                                                        \
       CLB_SU2T1(NK, RF, RP, 4);                                                                                        \
       CLB_SU2T1(NK, RF, RP, 2);                                                                                        \
@@ -361,7 +366,7 @@ __attribute__((visibility("hidden"))) int su2_create(clb_handle *h)
   u->split = u->fp32 ? 2 : 3;
   if (const char *env = std::getenv("CLB_SU2_SPLIT")) {
     u->split = std::max(0, std::min(3, std::atoi(env)));
-    u->tan_split = std::min(2, u->split);
+    u->tan_split = u->split;
   }
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&u->f, NF * h->n3 * u->esz) == cudaSuccess;

@@ -245,7 +245,7 @@ def test_plain_evolution_after_tangent_end_is_bitwise(precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_tangent_kick_split_is_bitwise_the_whole_sweep(monkeypatch, precision):
-    # The tangent sweep runs whole, in halves or in three parts (CLB_SU2_SPLIT 0, 1, 2) with the
+    # The tangent sweep runs whole, in halves, three or four parts (CLB_SU2_SPLIT 0, 1, 2, 3) with the
     # same per-component arithmetic, so state and tangent agree to the last bit.
     from cosmolattice_b200 import Lattice
     from cosmolattice_b200.initializers import su2u1_initial_state_tangent
@@ -253,7 +253,7 @@ def test_tangent_kick_split_is_bitwise_the_whole_sweep(monkeypatch, precision):
     par, rp, m, f, p, sf = case(8, "VV2", True)
     df, dp, cd = su2u1_initial_state_tangent(m, rp, "gSU2", (f, p))
     out = {}
-    for split in ("0", "1", "2"):
+    for split in ("0", "1", "2", "3"):
         monkeypatch.setenv("CLB_SU2_SPLIT", split)
         lat = Lattice(m, rp, precision=precision)
         lat.set_state(f, p, sf)
@@ -262,6 +262,6 @@ def test_tangent_kick_split_is_bitwise_the_whole_sweep(monkeypatch, precision):
         lat.evolve(12)
         out[split] = (lat.get_state(), lat.tangent_get_state())
         lat.close()
-    for split in ("1", "2"):
+    for split in ("1", "2", "3"):
         for (a, b) in zip(out[split], out["0"]):
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2], split
