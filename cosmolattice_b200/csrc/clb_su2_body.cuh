@@ -518,11 +518,20 @@ __device__ __forceinline__ int sector(int c) { return c == 0 ? 0 : c < 3 ? 1 : c
 #ifndef CLB_SU2_P4_MINB_F64
 #define CLB_SU2_P4_MINB_F64 CLB_SU2_HALF_MINB_F64
 #endif
+// the FP64 four-part sweep's S and phi part (SECT 5) and Phi part (SECT 6)
+#ifndef CLB_SU2_P5_MINB_F64
+#define CLB_SU2_P5_MINB_F64 CLB_SU2_HALF_MINB_F64
+#endif
+#ifndef CLB_SU2_P6_MINB_F64
+#define CLB_SU2_P6_MINB_F64 CLB_SU2_HALF_MINB_F64
+#endif
 template <class S, int NK, bool RF, bool RP, int SECT = 0>
 __global__ void __launch_bounds__(128, SECT == 0   ? (sizeof(S) == 4 ? CLB_SU2_KICK_MINB_F32 : CLB_SU2_KICK_MINB_F64)
                                        : sizeof(S) == 4 ? CLB_SU2_HALF_MINB_F32
                                        : SECT == 3      ? CLB_SU2_P3_MINB_F64
                                        : SECT == 4      ? CLB_SU2_P4_MINB_F64
+                                       : SECT == 5      ? CLB_SU2_P5_MINB_F64
+                                       : SECT == 6      ? CLB_SU2_P6_MINB_F64
                                                         : CLB_SU2_HALF_MINB_F64)
     k_kick(const S *__restrict__ f, S *__restrict__ p, Params a, Kick kc, const State *__restrict__ stp,
            double *__restrict__ partials, const S *__restrict__ ph)
